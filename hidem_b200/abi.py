@@ -1,0 +1,248 @@
+"""ctypes mirror of ``include/hidem_b200.h`` and loader of ``libhidem_b200.so``.
+
+The library is the product: there is no Python or CPU fallback. ``load()`` raises when
+the in-tree shared object is missing (build it with ``python -m hidem_b200.build``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libhidem_b200.so"
+
+HIDEM_OK = 0
+STATUS_NAMES = {0: "HIDEM_OK", 1: "HIDEM_ERR_ARG", 2: "HIDEM_ERR_CUDA", 3: "HIDEM_ERR_STATE",
+                4: "HIDEM_ERR_CAPACITY", 5: "HIDEM_ERR_IO", 6: "HIDEM_ERR_DEVICE",
+                7: "HIDEM_ERR_NOT_FOUND"}
+PREC_FP64 = 0
+PREC_MIXED = 1
+TYPE_FIXED = 0x40
+TYPE_FRONT = 0x80
+
+_d = C.c_double
+_i32 = C.c_int32
+_i64 = C.c_int64
+_p = C.c_void_p
+
+
+class HidemParams(C.Structure):
+    _fields_ = [
+        ("dt", _d), ("scale", _d), ("E", _d), ("beamWidth", _d), ("damping", _d),
+        ("dampingRotation", _d), ("attractDistance", _d), ("attractScaleForce", _d),
+        ("maxLoad", _d), ("bendBreak", _d), ("breakTime", _d),
+        ("g", _d), ("rhoIce", _d), ("rhoWater", _d), ("waterLevel", _d),
+        ("airDrag", _d), ("waterDrag", _d), ("bedDrag", _d), ("bedStiffness", _d),
+        ("bedInteract", _d), ("maxVel", _d), ("maxRot", _d),
+        ("lowerLimit", _d * 3), ("upperLimit", _d * 3),
+        ("boundaryMin", _i32 * 3), ("boundaryMax", _i32 * 3),
+        ("searchDistanceScale", _d), ("gridRegenInterval", _i32), ("firstBalanceTimestep", _i32),
+        ("maxRadius", _d),
+        ("useBed", _i32), ("bedHeight", _d), ("bedFriction", _d),
+        ("useVelocityLimit", _i32), ("useBoundary", _i32), ("useFixed", _i32),
+        ("useFrontPressure", _i32), ("precision", _i32),
+    ]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class HidemParticleSoA(C.Structure):
+    _fields_ = [("xCord", _p), ("yCord", _p), ("zCord", _p),
+                ("xTheta", _p), ("yTheta", _p), ("zTheta", _p),
+                ("xDiff", _p), ("yDiff", _p), ("zDiff", _p),
+                ("uDiff", _p), ("vDiff", _p), ("wDiff", _p),
+                ("radius", _p), ("owners", _p), ("type", _p), ("globalKeys", _p)]
+
+
+class HidemLinkSoA(C.Structure):
+    _fields_ = [("owners", _p), ("state", _p), ("globalKeys", _p), ("globalKeyEndA", _p),
+                ("globalKeyEndB", _p), ("initialLen", _p), ("particleLinkNum", _p),
+                ("CT", _p * 6)]
+
+
+class HidemStats(C.Structure):
+    _fields_ = [("step", _i64), ("num_particles", _i64), ("num_links", _i64),
+                ("num_neighbour_pairs", _i64), ("max_neighbours", _i64),
+                ("max_links_per_particle", _i64), ("grid_dims", _i64 * 3), ("grid_min", _d * 3),
+                ("regen_count", _i64), ("last_regen_step", _i64), ("accumulated_dist", _d),
+                ("search_distance", _d), ("interact_distance", _d), ("broken_links", _i64),
+                ("kernel_launches", _i64)]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+# field order of the reference (HiDEMLib/HiDEMParticleData.h:45-51, HiDEMLinkData.h:39-50)
+PARTICLE_FIELDS = ["xCord", "yCord", "zCord", "xTheta", "yTheta", "zTheta", "xDiff", "yDiff",
+                   "zDiff", "uDiff", "vDiff", "wDiff", "radius", "owners", "type", "globalKeys"]
+LP_PARTICLE_FIELDS = ["xTheta", "yTheta", "zTheta", "xDiff", "yDiff", "zDiff", "uDiff", "vDiff",
+                      "wDiff", "radius"]
+LINK_FIELDS = ["owners", "state", "globalKeys", "globalKeyEndA", "globalKeyEndB", "initialLen",
+               "particleLinkNum"]
+SIDE_FIELDS = ["CT0", "CT1", "CT2", "CT3", "CT4", "CT5"]
+
+
+def lp_dtype(precision: int):
+    return np.float32 if precision == PREC_MIXED else np.float64
+
+
+def particle_dtypes(precision: int) -> dict:
+    lp = lp_dtype(precision)
+    d = {k: lp for k in LP_PARTICLE_FIELDS}
+    d.update(xCord=np.float64, yCord=np.float64, zCord=np.float64, owners=np.int32,
+             type=np.uint8, globalKeys=np.int64)
+    return d
+
+
+def link_dtypes(precision: int) -> dict:
+    lp = lp_dtype(precision)
+    d = dict(owners=np.int32, state=np.uint8, globalKeys=np.int64, globalKeyEndA=np.int64,
+             globalKeyEndB=np.int64, initialLen=lp, particleLinkNum=np.int32)
+    d.update({k: lp for k in SIDE_FIELDS})
+    return d
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def particle_soa(arrays: dict, precision: int, n: int | None = None) -> HidemParticleSoA:
+    """A particle SoA struct pointing into `arrays` (numpy, checked for dtype / size)."""
+    s = HidemParticleSoA()
+    dts = particle_dtypes(precision)
+    for k in PARTICLE_FIELDS:
+        a = arrays.get(k)
+        if a is None:
+            continue
+        if a.dtype != dts[k] or not a.flags.c_contiguous:
+            raise TypeError(f"particle field {k}: need contiguous {np.dtype(dts[k])}, got {a.dtype}")
+        if n is not None and a.shape[0] != n:
+            raise ValueError(f"particle field {k}: {a.shape[0]} elements, expected {n}")
+        setattr(s, k, _ptr(a))
+    return s
+
+
+def link_soa(arrays: dict, precision: int, L: int | None = None) -> HidemLinkSoA:
+    s = HidemLinkSoA()
+    dts = link_dtypes(precision)
+    for k in LINK_FIELDS:
+        a = arrays.get(k)
+        if a is None:
+            continue
+        if a.dtype != dts[k] or not a.flags.c_contiguous:
+            raise TypeError(f"link field {k}: need contiguous {np.dtype(dts[k])}, got {a.dtype}")
+        if L is not None and a.shape[0] != L:
+            raise ValueError(f"link field {k}: {a.shape[0]} elements, expected {L}")
+        setattr(s, k, _ptr(a))
+    for i, k in enumerate(SIDE_FIELDS):
+        a = arrays.get(k)
+        if a is None:
+            continue
+        if a.dtype != dts[k] or not a.flags.c_contiguous:
+            raise TypeError(f"side field {k}: need contiguous {np.dtype(dts[k])}, got {a.dtype}")
+        if L is not None and a.shape[0] != 2 * L:
+            raise ValueError(f"side field {k}: {a.shape[0]} elements, expected {2 * L}")
+        s.CT[i] = _ptr(a)
+    return s
+
+
+def empty_particles(n: int, precision: int) -> dict:
+    return {k: np.zeros(n, dt) for k, dt in particle_dtypes(precision).items()}
+
+
+def empty_links(L: int, precision: int) -> dict:
+    out = {}
+    for k, dt in link_dtypes(precision).items():
+        out[k] = np.zeros(2 * L if k in SIDE_FIELDS else L, dt)
+    return out
+
+
+_lib = None
+
+# (name, restype, argtypes)
+_PROTOS = [
+    ("hidem_abi_version", C.c_int, []),
+    ("hidem_create_error", C.c_char_p, []),
+    ("hidem_params_default", None, [C.POINTER(HidemParams)]),
+    ("hidem_create", C.c_int, [C.POINTER(HidemParams), C.c_int, C.POINTER(C.c_void_p)]),
+    ("hidem_destroy", None, [C.c_void_p]),
+    ("hidem_last_error", C.c_char_p, [C.c_void_p]),
+    ("hidem_set_particles", C.c_int, [C.c_void_p, C.POINTER(HidemParticleSoA), _i64]),
+    ("hidem_set_links", C.c_int, [C.c_void_p, C.POINTER(HidemLinkSoA), _i64]),
+    ("hidem_set_timestep", C.c_int, [C.c_void_p, _i64]),
+    ("hidem_set_params", C.c_int, [C.c_void_p, C.POINTER(HidemParams)]),
+    ("hidem_grid_service", C.c_int, [C.c_void_p]),
+    ("hidem_regenerate", C.c_int, [C.c_void_p]),
+    ("hidem_compute_forces", C.c_int, [C.c_void_p]),
+    ("hidem_integrate", C.c_int, [C.c_void_p]),
+    ("hidem_link_update", C.c_int, [C.c_void_p]),
+    ("hidem_finalize_ts", C.c_int, [C.c_void_p]),
+    ("hidem_step", C.c_int, [C.c_void_p, C.c_int32]),
+    ("hidem_synchronize", C.c_int, [C.c_void_p]),
+    ("hidem_get_stream", C.c_void_p, [C.c_void_p]),
+    ("hidem_get_particles", C.c_int, [C.c_void_p, C.POINTER(HidemParticleSoA)]),
+    ("hidem_get_links", C.c_int, [C.c_void_p, C.POINTER(HidemLinkSoA)]),
+    ("hidem_get_forces", C.c_int, [C.c_void_p, C.c_void_p * 6]),
+    ("hidem_get_cells", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(_i64), C.POINTER(_d)]),
+    ("hidem_get_neighbours", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64,
+                                       C.POINTER(_i64)]),
+    ("hidem_get_break_events", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64,
+                                         C.POINTER(_i64)]),
+    ("hidem_get_stats", C.c_int, [C.c_void_p, C.POINTER(HidemStats)]),
+    ("hidem_lattice_fcc", C.c_int, [_i32, _i32, _i32, _d, _d, C.POINTER(_d), _d, C.c_uint64,
+                                    _i32, C.POINTER(HidemParticleSoA)]),
+    ("hidem_links_by_distance", C.c_int, [C.POINTER(HidemParticleSoA), _i64, _i32, _d,
+                                          C.POINTER(HidemLinkSoA), _i64, C.POINTER(_i64)]),
+]
+
+EXPORTED = [name for name, _, _ in _PROTOS]
+
+
+def load():
+    """Load the in-tree library (once). Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: the CUDA path has no fallback; build it with "
+            "`python -m hidem_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, res, args in _PROTOS:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class HidemError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def default_params(**overrides) -> HidemParams:
+    p = HidemParams()
+    load().hidem_params_default(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise KeyError(f"unknown parameter {k}")
+        cur = getattr(p, k)
+        if hasattr(cur, "__len__"):
+            for i, x in enumerate(v):
+                cur[i] = x
+        else:
+            setattr(p, k, v)
+    return p

@@ -1,0 +1,1219 @@
+// C ABI of libhidem_b200: the context, the HiDEMLib-shaped step operations and the
+// host side of the rebuild (HiDEMLib::gridService) policy.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+using namespace hidem;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct SideSet {
+    uint32_t *partner = nullptr;
+    void *ct[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    uint8_t *state = nullptr;
+    void *L0 = nullptr;
+    int32_t *link = nullptr;
+    long long cap = 0;
+};
+
+}  // namespace
+
+struct hidem_ctx {
+    hidem_params P{};
+    int mixed = 1;
+    size_t lp = 4;  // bytes of lp / ct
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    Consts<float> cf{};
+    Consts<double> cd{};
+    double searchDistance = 0, interactDist = 0;
+
+    long long n = 0, L = 0;
+    long long step = 0, startStep = 0;
+    bool haveParticles = false, haveLinks = false, built = false;
+
+    // particles (slot order), double buffered
+    void *rec[2] = {nullptr, nullptr};
+    int cur = 0;  // record buffer holding the current state
+    int ord = 0;  // which of type/orig/cellOf matches the current slot order
+    uint8_t *type[2] = {nullptr, nullptr};
+    int32_t *orig[2] = {nullptr, nullptr};
+    int32_t *cellOf[2] = {nullptr, nullptr};
+    int32_t *slotOf = nullptr;
+    int32_t *perm = nullptr;
+    void *force = nullptr;
+
+    // grid
+    GridInfo grid{};
+    int32_t *cellCount = nullptr, *cellStart = nullptr, *cursor = nullptr;
+    long long cellCap = 0;
+    int *scanSums32 = nullptr;
+    long long *scanSums64 = nullptr;
+    long long scanCap = 0;
+    double *boundsPartial = nullptr, *boundsOut = nullptr;
+
+    // contact list + per-slot counts
+    uint32_t *counts = nullptr;
+    int *blockWidth = nullptr;
+    long long *nOff = nullptr, *sOff = nullptr, *offTotal = nullptr;
+    int32_t *nbr = nullptr;
+    long long nbrCap = 0;
+    long long numPairs = 0, maxNeigh = 0, maxLinksPP = 0;
+
+    // links (input order)
+    int32_t *linkA = nullptr, *linkB = nullptr;
+    void *L0link = nullptr;
+    int32_t *plStart = nullptr, *plLink = nullptr;
+    uint8_t *plEnd = nullptr;
+    int32_t *sideSlot[2] = {nullptr, nullptr};
+    SideSet side[2];
+    int curSide = 0;  // always 0: rebuild swaps the new layout into side[0]
+    std::vector<int64_t> linkOwners, linkKeys, linkKeyA, linkKeyB;
+    std::vector<int32_t> linkNum;
+
+    // particle metadata kept on the host (input order)
+    std::vector<int32_t> owners;
+    std::vector<int64_t> keys;
+
+    // events and reductions
+    int2 *events = nullptr;
+    unsigned long long *eventCount = nullptr;
+    long long eventCap = 0, eventsRead = 0;
+    unsigned long long *diffMax = nullptr;
+    int *errorFlag = nullptr;
+
+    double accumulatedDist = 0;
+    long long regenCount = 0, lastRegen = -1;
+    long long launches = 0;
+    int smCount = 148;
+};
+
+namespace {
+
+hidem_status fail(hidem_ctx *c, hidem_status s, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return s;
+}
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(ctx, HIDEM_ERR_CUDA, "%s failed: %s (%s:%d)", #call,                 \
+                        cudaGetErrorString(e_), __FILE__, __LINE__);                         \
+    } while (0)
+
+#define TRY(expr)                            \
+    do {                                     \
+        hidem_status s_ = (expr);            \
+        if (s_ != HIDEM_OK) return s_;       \
+    } while (0)
+
+template <class T>
+hidem_status dalloc(hidem_ctx *ctx, T **p, long long count) {
+    if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    if (count <= 0) count = 1;
+    CK(cudaMalloc((void **)p, sizeof(T) * (size_t)count));
+    return HIDEM_OK;
+}
+hidem_status dalloc_bytes(hidem_ctx *ctx, void **p, size_t bytes) {
+    if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    if (bytes == 0) bytes = 16;
+    CK(cudaMalloc(p, bytes));
+    return HIDEM_OK;
+}
+template <class T>
+void dfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+// Derived constants of the sample main (HiDEM/MeshBlock/MainMeshBlock.cpp:69-156) in lp
+// precision, and the search distances of HiDEMLib::setup (HiDEMLib.h:757-761).
+template <class LP>
+void derive(const hidem_params &P, Consts<LP> &c, double &searchDistance, double &interactDist) {
+    LP scale = (LP)P.scale;
+    LP s2 = scale * scale;
+    LP dt = (LP)P.dt;
+    LP E = (LP)P.E;
+    LP beamWidth = (LP)P.beamWidth * scale;
+    LP rhoWater = (LP)P.rhoWater, rhoIce = (LP)P.rhoIce, g = (LP)P.g;
+    c.invDt = (LP)(1.0 / (double)dt);
+    c.attractDistance = (LP)P.attractDistance * scale;
+    c.attractScaleForce = (LP)P.attractScaleForce;
+    c.damping = (LP)P.damping * s2;
+    c.dampingRotation = (LP)P.dampingRotation * s2;
+    c.scaleE = E * scale;
+    c.E = E;
+    c.W2 = beamWidth * beamWidth;
+    c.W4 = beamWidth * beamWidth * beamWidth * beamWidth;
+    c.G = (LP)((double)E / 2.0);
+    c.bendBreak = (LP)P.bendBreak;
+    c.maxLoad = (LP)P.maxLoad;
+    c.dt = dt;
+    c.invDt2 = (LP)(1.0 / (2.0 * (double)dt));
+    c.dtSqr = (LP)std::pow((double)dt, 2.0);
+    c.invDtSqr = (LP)(1.0 / std::pow((double)dt, 2.0));
+    c.g = g;
+    c.lift = (rhoWater - rhoIce) / rhoIce * g;
+    c.rhoIce = rhoIce;
+    c.rhoWater = rhoWater;
+    c.waterLevel = (LP)P.waterLevel;
+    c.airDrag = (LP)P.airDrag * s2;
+    c.waterDrag = (LP)P.waterDrag * s2;
+    c.bedDrag = (LP)P.bedDrag * s2;
+    c.bedFriction = (LP)P.bedFriction;
+    c.bedHeight = (LP)P.bedHeight;
+    c.bedInteract = (LP)P.bedInteract * scale;
+    c.bedStiffness = (LP)P.bedStiffness * s2;
+    c.scale = scale;
+    c.maxVel = (LP)P.maxVel;
+    c.maxRot = (LP)P.maxRot;
+    c.breakTime = (LP)P.breakTime;
+    for (int k = 0; k < 3; ++k) {
+        c.lower[k] = P.lowerLimit[k];
+        c.upper[k] = P.upperLimit[k];
+        c.bmin[k] = P.boundaryMin[k] != 0;
+        c.bmax[k] = P.boundaryMax[k] != 0;
+    }
+    c.useBed = P.useBed != 0;
+    c.useVel = P.useVelocityLimit != 0;
+    c.useBnd = P.useBoundary != 0;
+    c.useFixed = P.useFixed != 0;
+    c.useFront = P.useFrontPressure != 0;
+    LP maxRadius = (LP)P.maxRadius;
+    LP maxParticleDist = (LP)((double)maxRadius * 2.0);
+    searchDistance = P.searchDistanceScale * (double)maxParticleDist;
+    interactDist = searchDistance - (double)maxParticleDist;
+}
+
+hidem_status check_params(hidem_ctx *ctx, const hidem_params *p) {
+    if (!p) return fail(ctx, HIDEM_ERR_ARG, "params is NULL");
+    if (p->precision != HIDEM_PREC_FP64 && p->precision != HIDEM_PREC_MIXED)
+        return fail(ctx, HIDEM_ERR_ARG, "unknown precision %d", p->precision);
+    if (!(p->dt > 0)) return fail(ctx, HIDEM_ERR_ARG, "dt must be > 0");
+    if (!(p->maxRadius > 0)) return fail(ctx, HIDEM_ERR_ARG, "maxRadius must be > 0");
+    if (!(p->searchDistanceScale > 1))
+        return fail(ctx, HIDEM_ERR_ARG, "searchDistanceScale must be > 1");
+    return HIDEM_OK;
+}
+
+hidem_status apply_params(hidem_ctx *ctx, const hidem_params *p) {
+    TRY(check_params(ctx, p));
+    ctx->P = *p;
+    ctx->mixed = p->precision == HIDEM_PREC_MIXED;
+    ctx->lp = ctx->mixed ? 4 : 8;
+    double sd, id;
+    derive<float>(*p, ctx->cf, sd, id);
+    derive<double>(*p, ctx->cd, ctx->searchDistance, ctx->interactDist);
+    if (ctx->mixed) {
+        ctx->searchDistance = sd;
+        ctx->interactDist = id;
+    }
+    return HIDEM_OK;
+}
+
+hidem_status check_device_error(hidem_ctx *ctx) {
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, ctx->errorFlag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (flag) {
+        CK(cudaMemsetAsync(ctx->errorFlag, 0, sizeof(int), ctx->stream));
+        const char *what = flag == 1   ? "particle outside the grid bounds"
+                           : flag == 2 ? "more than 65535 contacts for one particle"
+                           : flag == 3 ? "more than 65535 link ends for one particle"
+                                       : "device check failed";
+        return fail(ctx, HIDEM_ERR_DEVICE, "device check %d: %s", flag, what);
+    }
+    return HIDEM_OK;
+}
+
+template <class LP>
+PRec<LP> *recp(hidem_ctx *ctx, int b) {
+    return static_cast<PRec<LP> *>(ctx->rec[b]);
+}
+
+template <class LP>
+SideView<LP> side_view(SideSet &s) {
+    SideView<LP> v;
+    v.partner = s.partner;
+    for (int k = 0; k < 6; ++k) v.ct[k] = static_cast<LP *>(s.ct[k]);
+    v.state = s.state;
+    v.L0 = static_cast<LP *>(s.L0);
+    v.link = s.link;
+    return v;
+}
+
+hidem_status side_alloc(hidem_ctx *ctx, SideSet &s, long long cap) {
+    if (s.cap >= cap && s.partner) return HIDEM_OK;
+    if (cap <= 0) cap = 1;
+    TRY(dalloc(ctx, &s.partner, cap));
+    for (int k = 0; k < 6; ++k) TRY(dalloc_bytes(ctx, &s.ct[k], ctx->lp * (size_t)cap));
+    TRY(dalloc(ctx, &s.state, cap));
+    TRY(dalloc_bytes(ctx, &s.L0, ctx->lp * (size_t)cap));
+    TRY(dalloc(ctx, &s.link, cap));
+    s.cap = cap;
+    return HIDEM_OK;
+}
+
+void side_free(SideSet &s) {
+    dfree(s.partner);
+    for (int k = 0; k < 6; ++k) dfree(s.ct[k]);
+    dfree(s.state);
+    dfree(s.L0);
+    dfree(s.link);
+    s.cap = 0;
+}
+
+long long nblocks32(long long n) { return (n + 31) / 32; }
+
+hidem_status ensure_scan(hidem_ctx *ctx, long long n) {
+    long long need = (n + 1023) / 1024 + 1;
+    if (ctx->scanCap >= need) return HIDEM_OK;
+    TRY(dalloc(ctx, &ctx->scanSums32, need));
+    TRY(dalloc(ctx, &ctx->scanSums64, need));
+    ctx->scanCap = need;
+    return HIDEM_OK;
+}
+
+// --------------------------------------------------------------- rebuild
+
+// CombinedAccel::generateNeighbours + generateLinks (+ LinkAccelSide::sortSideData):
+// bounds, cell colours, counting sort into cell order (inside a cell by input index),
+// permutation of the particle records, contact list, link-end layout.
+template <class LP>
+hidem_status rebuild(hidem_ctx *ctx) {
+    cudaStream_t st = ctx->stream;
+    const int n = (int)ctx->n;
+    const int cur = ctx->cur, nxt = 1 - cur;
+
+    // 1. bounds (ParticleData::getLimits)
+    const int nbB = std::min<long long>(std::max<long long>(1, (n + 255) / 256), 4 * ctx->smCount);
+    launch_bounds<LP>(recp<LP>(ctx, cur), n, ctx->boundsPartial, nbB, ctx->boundsOut, st);
+    ctx->launches += 2;
+    double b[6];
+    CK(cudaMemcpyAsync(b, ctx->boundsOut, sizeof b, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (!(b[0] <= b[3] && b[1] <= b[4] && b[2] <= b[5]))
+        return fail(ctx, HIDEM_ERR_DEVICE, "non-finite particle coordinates");
+
+    // 2. grid (NeighbourGrid::generateNeighbourGrid, NeighbourGrid.cpp:72-114)
+    GridInfo &g = ctx->grid;
+    g.xMin = b[0];
+    g.yMin = b[1];
+    g.zMin = b[2];
+    g.h = ctx->searchDistance;
+    double ex = std::floor((b[3] - b[0]) / g.h), ey = std::floor((b[4] - b[1]) / g.h),
+           ez = std::floor((b[5] - b[2]) / g.h);
+    if (ex > 2e9 || ey > 2e9 || ez > 2e9)
+        return fail(ctx, HIDEM_ERR_CAPACITY, "grid extent too large");
+    g.X = 1 + (int)ex;
+    g.Y = 1 + (int)ey;
+    g.Z = 1 + (int)ez;
+    g.total = (long long)g.X * g.Y * g.Z;
+    if (g.total >= (1ll << 31))
+        return fail(ctx, HIDEM_ERR_CAPACITY, "grid has %lld cells (limit 2^31)", g.total);
+    int k = 0;
+    for (int zD = -1; zD < 2; ++zD)
+        for (int yD = -1; yD < 2; ++yD)
+            for (int xD = -1; xD < 2; ++xD)
+                g.off[k++] = (long long)xD + (long long)yD * g.X + (long long)zD * g.X * g.Y;
+    if (ctx->cellCap < g.total) {
+        long long cap = g.total + g.total / 4 + 1024;
+        TRY(dalloc(ctx, &ctx->cellCount, cap));
+        TRY(dalloc(ctx, &ctx->cellStart, cap));
+        TRY(dalloc(ctx, &ctx->cursor, cap));
+        ctx->cellCap = cap;
+    }
+    TRY(ensure_scan(ctx, std::max<long long>(g.total, nblocks32(n) + 1)));
+
+    // 3. colours + counting sort (colourParticles / generateIterationList)
+    CK(cudaMemsetAsync(ctx->cellCount, 0, sizeof(int) * (size_t)g.total, st));
+    CK(cudaMemsetAsync(ctx->cursor, 0, sizeof(int) * (size_t)g.total, st));
+    const int od = ctx->ord, nd = 1 - od;
+    launch_cells<LP>(recp<LP>(ctx, cur), n, g, ctx->cellOf[od], ctx->cellCount, ctx->errorFlag, st);
+    ctx->launches += 1;
+    ctx->launches += launch_scan<int, int>(ctx->cellCount, g.total, 1, ctx->cellStart,
+                                           ctx->scanSums32, nullptr, st);
+    launch_scatter(ctx->cellOf[od], n, ctx->cellStart, ctx->cursor, ctx->perm, st);
+    launch_sort_cells(ctx->cellStart, ctx->cellCount, g.total, ctx->orig[od], ctx->perm, st);
+    launch_permute<LP>(ctx->perm, n, recp<LP>(ctx, cur), recp<LP>(ctx, nxt), ctx->type[od],
+                       ctx->type[nd], ctx->orig[od], ctx->orig[nd], ctx->cellOf[od],
+                       ctx->cellOf[nd], ctx->slotOf, st);
+    ctx->launches += 3;
+    ctx->cur = nxt;
+    ctx->ord = nd;
+    const int c = nd;   // slot-order arrays
+    const int rc = nxt; // record buffer
+
+    // 4. contact list (NeighAccel::generateNeighbours: count pass, widths, fill pass)
+    const long long nb32 = nblocks32(n);
+    launch_nbr_count<LP>(recp<LP>(ctx, rc), n, ctx->cellOf[c], g, ctx->cellStart, ctx->cellCount,
+                         ctx->interactDist, ctx->counts, ctx->blockWidth, ctx->errorFlag, st);
+    ctx->launches += 1;
+    ctx->launches += launch_scan<int, long long>(ctx->blockWidth, nb32, 32ll, ctx->nOff,
+                                                 ctx->scanSums64, ctx->offTotal, st);
+    long long nTotal = 0;
+    CK(cudaMemcpyAsync(&nTotal, ctx->offTotal, sizeof nTotal, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    TRY(check_device_error(ctx));
+    if (nTotal > ctx->nbrCap) {
+        long long cap = nTotal + nTotal / 8 + 1024;
+        TRY(dalloc(ctx, &ctx->nbr, cap));
+        ctx->nbrCap = cap;
+    }
+    launch_nbr_fill<LP>(recp<LP>(ctx, rc), n, ctx->cellOf[c], g, ctx->cellStart, ctx->cellCount,
+                        ctx->interactDist, ctx->nOff, ctx->nbr, st);
+    ctx->launches += 1;
+
+    // 5. link ends in the new slot order (LinkAccelSide::generateLinks + sortSideData)
+    launch_side_count(ctx->orig[c], n, ctx->plStart, ctx->counts, ctx->blockWidth, ctx->errorFlag, st);
+    ctx->launches += 1;
+    ctx->launches += launch_scan<int, long long>(ctx->blockWidth, nb32, 32ll, ctx->sOff,
+                                                 ctx->scanSums64, ctx->offTotal, st);
+    long long sTotal = 0;
+    CK(cudaMemcpyAsync(&sTotal, ctx->offTotal, sizeof sTotal, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    TRY(check_device_error(ctx));
+    if (sTotal >= (1ll << 31))
+        return fail(ctx, HIDEM_ERR_CAPACITY, "%lld link-end slots (limit 2^31)", sTotal);
+    // side[0] / sideSlot[0] hold the current layout; the new one is built in [1], then swapped
+    TRY(side_alloc(ctx, ctx->side[1], std::max<long long>(sTotal, 2 * ctx->L)));
+    if (ctx->L > 0) {
+        launch_side_fill<LP>(ctx->orig[c], n, ctx->slotOf, ctx->plStart, ctx->plLink, ctx->plEnd,
+                             ctx->linkA, ctx->linkB, static_cast<const LP *>(ctx->L0link),
+                             ctx->sideSlot[0], side_view<LP>(ctx->side[0]), ctx->sOff,
+                             side_view<LP>(ctx->side[1]), ctx->sideSlot[1], st);
+        ctx->launches += 1;
+    }
+    std::swap(ctx->sideSlot[0], ctx->sideSlot[1]);
+    std::swap(ctx->side[0], ctx->side[1]);
+
+    // statistics (host copies of the counts)
+    std::vector<uint32_t> cnt((size_t)n);
+    CK(cudaMemcpyAsync(cnt.data(), ctx->counts, sizeof(uint32_t) * (size_t)n,
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    long long pairs = 0, mn = 0, ml = 0;
+    for (int i = 0; i < n; ++i) {
+        long long a = cnt[i] & 0xffffu, s = cnt[i] >> 16;
+        pairs += a;
+        mn = std::max(mn, a);
+        ml = std::max(ml, s);
+    }
+    ctx->numPairs = pairs;
+    ctx->maxNeigh = mn;
+    ctx->maxLinksPP = ml;
+    ctx->built = true;
+    ctx->regenCount += 1;
+    ctx->lastRegen = ctx->step;
+    CK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+hidem_status do_rebuild(hidem_ctx *ctx) {
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    return ctx->mixed ? rebuild<float>(ctx) : rebuild<double>(ctx);
+}
+
+// max over particles of max(0, x/y/zDiff) -> accumulated displacement
+// (HiDEMLib::accumulateDist, HiDEMLib.h:463-474), from three device words.
+template <class LP>
+double curr_dist(const unsigned long long w[3]) {
+    LP m[3];
+    for (int k = 0; k < 3; ++k) {
+        if (sizeof(LP) == 4) {
+            uint32_t u = (uint32_t)w[k];
+            float f;
+            std::memcpy(&f, &u, 4);
+            m[k] = (LP)f;
+        } else {
+            double d;
+            std::memcpy(&d, &w[k], 8);
+            m[k] = (LP)d;
+        }
+    }
+    LP root = std::sqrt((m[0] * m[0]) + (m[1] * m[1]) + (m[2] * m[2]));
+    return (double)((LP)10 * root);
+}
+
+hidem_status read_diff_max(hidem_ctx *ctx, double *currDist) {
+    unsigned long long w[3];
+    CK(cudaMemcpyAsync(w, ctx->diffMax, sizeof w, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *currDist = ctx->mixed ? curr_dist<float>(w) : curr_dist<double>(w);
+    return HIDEM_OK;
+}
+
+hidem_status reduce_diff_now(hidem_ctx *ctx) {
+    CK(cudaMemsetAsync(ctx->diffMax, 0, 3 * sizeof(unsigned long long), ctx->stream));
+    int nb = std::min<long long>(std::max<long long>(1, (ctx->n + 255) / 256), 4 * ctx->smCount);
+    if (ctx->mixed)
+        launch_max_diff<float>(recp<float>(ctx, ctx->cur), (int)ctx->n, ctx->diffMax, nb, ctx->stream);
+    else
+        launch_max_diff<double>(recp<double>(ctx, ctx->cur), (int)ctx->n, ctx->diffMax, nb, ctx->stream);
+    ctx->launches += 1;
+    return HIDEM_OK;
+}
+
+// HiDEMLib::gridService (HiDEMLib.h:533-628) on one rank. `diffReady` says the
+// device words already hold this step's maxima (computed by the previous fused step).
+hidem_status grid_service(hidem_ctx *ctx, bool diffReady) {
+    const long long t = ctx->step;
+    bool regen = (t == ctx->startStep);
+    if (ctx->P.gridRegenInterval != -1) {
+        regen = ctx->P.gridRegenInterval > 0 && (t % ctx->P.gridRegenInterval) == 0;
+    } else if (t % 10 == 0) {
+        if (!diffReady) TRY(reduce_diff_now(ctx));
+        double cd = 0;
+        TRY(read_diff_max(ctx, &cd));
+        ctx->accumulatedDist += cd;
+        if (ctx->accumulatedDist >= ctx->interactDist / 2.0) regen = true;
+    }
+    if (t == ctx->P.firstBalanceTimestep) regen = true;
+    if (!ctx->built) regen = true;
+    if (regen) {
+        ctx->accumulatedDist = 0;
+        TRY(do_rebuild(ctx));
+    }
+    return HIDEM_OK;
+}
+
+template <class LP>
+StepArgs<LP> step_args(hidem_ctx *ctx) {
+    StepArgs<LP> a{};
+    a.in = recp<LP>(ctx, ctx->cur);
+    a.out = recp<LP>(ctx, 1 - ctx->cur);
+    a.type = ctx->type[ctx->ord];
+    a.counts = ctx->counts;
+    a.nOff = ctx->nOff;
+    a.nbr = ctx->nbr;
+    a.sOff = ctx->sOff;
+    SideSet &s = ctx->side[ctx->curSide];
+    a.sPartner = s.partner;
+    for (int k = 0; k < 6; ++k) a.ct[k] = static_cast<LP *>(s.ct[k]);
+    a.sState = s.state;
+    a.sL0 = static_cast<const LP *>(s.L0);
+    a.sLink = s.link;
+    a.force = static_cast<LP *>(ctx->force);
+    a.n = (int)ctx->n;
+    a.step = ctx->step;
+    a.diffMax = ctx->diffMax;
+    a.events = ctx->events;
+    a.eventCount = ctx->eventCount;
+    a.eventCap = ctx->eventCap;
+    a.errorFlag = ctx->errorFlag;
+    return a;
+}
+
+template <class LP>
+const Consts<LP> &consts(hidem_ctx *ctx);
+template <>
+const Consts<float> &consts<float>(hidem_ctx *ctx) { return ctx->cf; }
+template <>
+const Consts<double> &consts<double>(hidem_ctx *ctx) { return ctx->cd; }
+
+// HiDEMDefLinkBreakFunc gate of the sample main: t * dt > breakTime, in lp
+// (MainMeshBlock.cpp:312).
+template <class LP>
+bool break_active(hidem_ctx *ctx, long long t) {
+    const Consts<LP> &c = consts<LP>(ctx);
+    return (LP)((LP)t * c.dt) > c.breakTime;
+}
+
+template <class LP>
+hidem_status link_update_now(hidem_ctx *ctx, long long tagStep) {
+    SideSet &s = ctx->side[ctx->curSide];
+    launch_link_break<LP>(consts<LP>(ctx), recp<LP>(ctx, ctx->cur), ctx->slotOf, ctx->linkA,
+                          ctx->linkB, ctx->sideSlot[ctx->curSide], s.state,
+                          static_cast<const LP *>(s.L0), ctx->L, tagStep, ctx->events,
+                          ctx->eventCount, ctx->eventCap, ctx->stream);
+    if (ctx->L > 0) ctx->launches += 1;
+    return HIDEM_OK;
+}
+
+// n whole timesteps, one fused kernel each (MainMeshBlock.cpp:274-323).
+template <class LP>
+hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
+    bool pending = false;      // link update of step-1 not applied yet
+    long long pendingStep = 0;
+    bool diffReady = false;
+    for (int s = 0; s < nsteps; ++s) {
+        const long long t = ctx->step;
+        if (ctx->P.gridRegenInterval == -1 && t % 10 == 0) {
+            // gridService reads the maxima of the diffs at the start of step t
+            TRY(grid_service(ctx, diffReady));
+        } else {
+            TRY(grid_service(ctx, false));
+        }
+        diffReady = false;
+        StepArgs<LP> a = step_args<LP>(ctx);
+        a.breakPending = pending ? 1 : 0;
+        a.breakStep = pendingStep;
+        a.reduceDiff = (ctx->P.gridRegenInterval == -1 && (t + 1) % 10 == 0) ? 1 : 0;
+        if (a.reduceDiff) {
+            CK(cudaMemsetAsync(ctx->diffMax, 0, 3 * sizeof(unsigned long long), ctx->stream));
+            diffReady = true;
+        }
+        launch_step<LP>(consts<LP>(ctx), a, true, ctx->stream);
+        ctx->launches += 1;
+        ctx->cur = 1 - ctx->cur;  // the slot order (type / orig / cellOf) is unchanged
+        pending = break_active<LP>(ctx, t);
+        pendingStep = t;
+        ctx->step = t + 1;  // finalizeTs
+    }
+    if (pending) TRY(link_update_now<LP>(ctx, pendingStep));
+    CK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+int hidem_abi_version(void) { return HIDEM_B200_ABI_VERSION; }
+
+const char *hidem_create_error(void) { return g_create_error.c_str(); }
+
+void hidem_params_default(hidem_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->dt = 0.0001;
+    p->scale = 1.0;
+    p->E = 1e+09;
+    p->beamWidth = 0.6;
+    p->damping = 1000.0;
+    p->dampingRotation = 1000.0;
+    p->attractDistance = 0.0;
+    p->attractScaleForce = 0.0;
+    p->maxLoad = 0.35;
+    p->bendBreak = 0.35;
+    p->breakTime = 10.0;
+    p->g = 9.81;
+    p->rhoIce = 910.0;
+    p->rhoWater = 1030.0;
+    p->waterLevel = 0.0;
+    p->airDrag = 1.0;
+    p->waterDrag = 10.0;
+    p->bedDrag = 1000.0;
+    p->bedStiffness = 2e+08;
+    p->bedInteract = 2.0;
+    p->maxVel = 20.0;
+    p->maxRot = 5.0;
+    p->searchDistanceScale = 1.4;
+    p->gridRegenInterval = -1;
+    p->firstBalanceTimestep = 2000;
+    p->maxRadius = 0.5;
+    p->bedHeight = 0.0;
+    p->bedFriction = 1.0;
+    p->precision = HIDEM_PREC_MIXED;
+}
+
+hidem_status hidem_create(const hidem_params *params, int device, hidem_ctx **out) {
+    g_create_error.clear();
+    if (!out) {
+        g_create_error = "out is NULL";
+        return HIDEM_ERR_ARG;
+    }
+    *out = nullptr;
+    hidem_ctx *ctx = new hidem_ctx();
+    hidem_status s = apply_params(ctx, params);
+    if (s != HIDEM_OK) {
+        g_create_error = ctx->err;
+        delete ctx;
+        return s;
+    }
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || device < 0 || device >= count) {
+        g_create_error = std::string("no CUDA device ") + std::to_string(device) + ": " +
+                         (e != cudaSuccess ? cudaGetErrorString(e) : "index out of range");
+        delete ctx;
+        return HIDEM_ERR_CUDA;
+    }
+    ctx->device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smCount, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("CUDA setup failed: ") + cudaGetErrorString(e);
+        delete ctx;
+        return HIDEM_ERR_CUDA;
+    }
+    s = dalloc(ctx, &ctx->errorFlag, 1);
+    if (s == HIDEM_OK) s = dalloc(ctx, &ctx->diffMax, 3);
+    if (s == HIDEM_OK) s = dalloc(ctx, &ctx->eventCount, 1);
+    if (s == HIDEM_OK) s = dalloc(ctx, &ctx->boundsPartial, 6 * 4 * ctx->smCount + 6);
+    if (s == HIDEM_OK) s = dalloc(ctx, &ctx->boundsOut, 6);
+    if (s == HIDEM_OK) s = dalloc(ctx, &ctx->offTotal, 1);
+    if (s == HIDEM_OK) {
+        cudaMemsetAsync(ctx->errorFlag, 0, sizeof(int), ctx->stream);
+        cudaMemsetAsync(ctx->eventCount, 0, sizeof(unsigned long long), ctx->stream);
+        e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) s = fail(ctx, HIDEM_ERR_CUDA, "%s", cudaGetErrorString(e));
+    }
+    if (s != HIDEM_OK) {
+        g_create_error = ctx->err;
+        hidem_destroy(ctx);
+        return s;
+    }
+    *out = ctx;
+    return HIDEM_OK;
+}
+
+void hidem_destroy(hidem_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int b = 0; b < 2; ++b) {
+        dfree(ctx->rec[b]);
+        dfree(ctx->type[b]);
+        dfree(ctx->orig[b]);
+        dfree(ctx->cellOf[b]);
+        dfree(ctx->sideSlot[b]);
+        side_free(ctx->side[b]);
+    }
+    dfree(ctx->slotOf);
+    dfree(ctx->perm);
+    dfree(ctx->force);
+    dfree(ctx->cellCount);
+    dfree(ctx->cellStart);
+    dfree(ctx->cursor);
+    dfree(ctx->scanSums32);
+    dfree(ctx->scanSums64);
+    dfree(ctx->boundsPartial);
+    dfree(ctx->boundsOut);
+    dfree(ctx->counts);
+    dfree(ctx->blockWidth);
+    dfree(ctx->nOff);
+    dfree(ctx->sOff);
+    dfree(ctx->offTotal);
+    dfree(ctx->nbr);
+    dfree(ctx->linkA);
+    dfree(ctx->linkB);
+    dfree(ctx->L0link);
+    dfree(ctx->plStart);
+    dfree(ctx->plLink);
+    dfree(ctx->plEnd);
+    dfree(ctx->events);
+    dfree(ctx->eventCount);
+    dfree(ctx->diffMax);
+    dfree(ctx->errorFlag);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *hidem_last_error(const hidem_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+hidem_status hidem_set_params(hidem_ctx *ctx, const hidem_params *params) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (params && params->precision != ctx->P.precision)
+        return fail(ctx, HIDEM_ERR_ARG, "precision cannot change after creation");
+    return apply_params(ctx, params);
+}
+
+hidem_status hidem_set_timestep(hidem_ctx *ctx, int64_t step) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (step < 0) return fail(ctx, HIDEM_ERR_ARG, "negative timestep");
+    ctx->step = step;
+    ctx->startStep = step;
+    ctx->built = false;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, int64_t n) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!p || n <= 0) return fail(ctx, HIDEM_ERR_ARG, "need at least one particle");
+    if (n >= (1ll << 31) - 64) return fail(ctx, HIDEM_ERR_CAPACITY, "n = %lld exceeds int32 indexing", (long long)n);
+    if (!p->xCord || !p->yCord || !p->zCord || !p->radius)
+        return fail(ctx, HIDEM_ERR_ARG, "xCord/yCord/zCord/radius are required");
+    CK(cudaSetDevice(ctx->device));
+    const size_t lp = ctx->lp;
+    const size_t recBytes = ctx->mixed ? sizeof(PRec<float>) : sizeof(PRec<double>);
+    std::vector<unsigned char> host(recBytes * (size_t)n, 0);
+    auto lpval = [&](const void *arr, int64_t i) -> double {
+        if (!arr) return 0.0;
+        return lp == 4 ? (double)static_cast<const float *>(arr)[i] : static_cast<const double *>(arr)[i];
+    };
+    for (int64_t i = 0; i < n; ++i) {
+        unsigned char *r = host.data() + recBytes * (size_t)i;
+        double xyz[3] = {p->xCord[i], p->yCord[i], p->zCord[i]};
+        std::memcpy(r, xyz, 24);
+        const void *d[6] = {p->xDiff, p->yDiff, p->zDiff, p->uDiff, p->vDiff, p->wDiff};
+        const void *th[3] = {p->xTheta, p->yTheta, p->zTheta};
+        if (ctx->mixed) {
+            PRec<float> q;
+            std::memcpy(&q, r, 24);
+            for (int k = 0; k < 6; ++k) q.d[k] = d[k] ? static_cast<const float *>(d[k])[i] : 0.f;
+            q.r = static_cast<const float *>(p->radius)[i];
+            for (int k = 0; k < 3; ++k) q.th[k] = th[k] ? static_cast<const float *>(th[k])[i] : 0.f;
+            std::memcpy(r, &q, sizeof q);
+        } else {
+            PRec<double> q{};
+            std::memcpy(&q, r, 24);
+            for (int k = 0; k < 6; ++k) q.d[k] = lpval(d[k], i);
+            q.r = static_cast<const double *>(p->radius)[i];
+            for (int k = 0; k < 3; ++k) q.th[k] = lpval(th[k], i);
+            std::memcpy(r, &q, sizeof q);
+        }
+    }
+    for (int b = 0; b < 2; ++b) {
+        TRY(dalloc_bytes(ctx, &ctx->rec[b], recBytes * (size_t)n));
+        TRY(dalloc(ctx, &ctx->type[b], n));
+        TRY(dalloc(ctx, &ctx->orig[b], n));
+        TRY(dalloc(ctx, &ctx->cellOf[b], n));
+    }
+    TRY(dalloc(ctx, &ctx->slotOf, n));
+    TRY(dalloc(ctx, &ctx->perm, n));
+    TRY(dalloc_bytes(ctx, &ctx->force, 6 * lp * (size_t)n));
+    TRY(dalloc(ctx, &ctx->counts, n));
+    const long long nb32 = nblocks32(n);
+    TRY(dalloc(ctx, &ctx->blockWidth, nb32 + 1));
+    TRY(dalloc(ctx, &ctx->nOff, nb32 + 1));
+    TRY(dalloc(ctx, &ctx->sOff, nb32 + 1));
+    ctx->cur = 0;
+    ctx->ord = 0;
+    CK(cudaMemcpyAsync(ctx->rec[0], host.data(), host.size(), cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<uint8_t> ty((size_t)n, 0);
+    if (p->type) std::memcpy(ty.data(), p->type, (size_t)n);
+    std::vector<int32_t> ident((size_t)n);
+    for (int64_t i = 0; i < n; ++i) ident[i] = (int32_t)i;
+    CK(cudaMemcpyAsync(ctx->type[0], ty.data(), (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->orig[0], ident.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->slotOf, ident.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->counts, 0, 4 * (size_t)n, ctx->stream));
+    CK(cudaMemsetAsync(ctx->force, 0, 6 * lp * (size_t)n, ctx->stream));
+    ctx->owners.assign((size_t)n, 0);
+    if (p->owners) std::memcpy(ctx->owners.data(), p->owners, 4 * (size_t)n);
+    ctx->keys.resize((size_t)n);
+    for (int64_t i = 0; i < n; ++i) ctx->keys[i] = p->globalKeys ? p->globalKeys[i] : i;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->n = n;
+    ctx->haveParticles = true;
+    ctx->built = false;
+    ctx->startStep = ctx->step;
+    // a link set refers to particle indices of the previous particle set
+    ctx->haveLinks = false;
+    ctx->L = 0;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "set particles before links");
+    if (L < 0 || (L > 0 && (!l || !l->globalKeyEndA || !l->globalKeyEndB || !l->initialLen || !l->state)))
+        return fail(ctx, HIDEM_ERR_ARG, "link arrays globalKeyEndA/B, initialLen, state are required");
+    if (2 * L >= (1ll << 31)) return fail(ctx, HIDEM_ERR_CAPACITY, "L = %lld exceeds int32 side indexing", (long long)L);
+    CK(cudaSetDevice(ctx->device));
+    const long long n = ctx->n;
+    const size_t lp = ctx->lp;
+    // globalKey -> input index (LinkData::makeLocalPartEnds, PLiB/LinkData.h:91-115)
+    std::vector<std::pair<int64_t, int32_t>> km((size_t)n);
+    for (long long i = 0; i < n; ++i) km[i] = {ctx->keys[i], (int32_t)i};
+    std::sort(km.begin(), km.end());
+    auto find = [&](int64_t key) -> int32_t {
+        auto it = std::lower_bound(km.begin(), km.end(), std::make_pair(key, (int32_t)-1));
+        if (it == km.end() || it->first != key) return -1;
+        return it->second;
+    };
+    std::vector<int32_t> A((size_t)L), B((size_t)L);
+    for (long long i = 0; i < L; ++i) {
+        A[i] = find(l->globalKeyEndA[i]);
+        B[i] = find(l->globalKeyEndB[i]);
+        if (A[i] < 0 || B[i] < 0)
+            return fail(ctx, HIDEM_ERR_NOT_FOUND, "link %lld: dangling end (keys %lld, %lld)", i,
+                        (long long)l->globalKeyEndA[i], (long long)l->globalKeyEndB[i]);
+        if (A[i] == B[i]) return fail(ctx, HIDEM_ERR_ARG, "link %lld joins a particle to itself", i);
+    }
+    // per-particle link ends in ascending link index (LinkAccelSide::generateLinks)
+    std::vector<int32_t> start((size_t)n + 1, 0);
+    for (long long i = 0; i < L; ++i) {
+        start[A[i] + 1]++;
+        start[B[i] + 1]++;
+    }
+    for (long long i = 0; i < n; ++i) start[i + 1] += start[i];
+    std::vector<int32_t> plink((size_t)(2 * L + 1)), cursor(start.begin(), start.end() - 1);
+    std::vector<uint8_t> pend((size_t)(2 * L + 1));
+    for (long long i = 0; i < L; ++i) {
+        int32_t a = cursor[A[i]]++;
+        plink[a] = (int32_t)i;
+        pend[a] = 0;
+        int32_t b = cursor[B[i]]++;
+        plink[b] = (int32_t)i;
+        pend[b] = 1;
+    }
+    // flat initial side layout: side 2l+e
+    std::vector<int32_t> sslot((size_t)(2 * L + 1));
+    for (long long s = 0; s < 2 * L; ++s) sslot[s] = (int32_t)s;
+    std::vector<uint8_t> sstate((size_t)(2 * L + 1));
+    for (long long i = 0; i < L; ++i) sstate[2 * i] = sstate[2 * i + 1] = l->state[i];
+
+    TRY(dalloc(ctx, &ctx->linkA, L));
+    TRY(dalloc(ctx, &ctx->linkB, L));
+    TRY(dalloc_bytes(ctx, &ctx->L0link, lp * (size_t)std::max<long long>(L, 1)));
+    TRY(dalloc(ctx, &ctx->plStart, n + 1));
+    TRY(dalloc(ctx, &ctx->plLink, 2 * L));
+    TRY(dalloc(ctx, &ctx->plEnd, 2 * L));
+    for (int b = 0; b < 2; ++b) TRY(dalloc(ctx, &ctx->sideSlot[b], 2 * L));
+    side_free(ctx->side[0]);
+    side_free(ctx->side[1]);
+    TRY(side_alloc(ctx, ctx->side[0], 2 * L));
+    ctx->curSide = 0;
+    TRY(dalloc(ctx, &ctx->events, std::max<long long>(L, 1)));
+    ctx->eventCap = std::max<long long>(L, 1);
+    ctx->eventsRead = 0;
+    cudaStream_t st = ctx->stream;
+    if (L > 0) {
+        CK(cudaMemcpyAsync(ctx->linkA, A.data(), 4 * (size_t)L, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->linkB, B.data(), 4 * (size_t)L, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->L0link, l->initialLen, lp * (size_t)L, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->plLink, plink.data(), 4 * (size_t)(2 * L), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->plEnd, pend.data(), (size_t)(2 * L), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->sideSlot[0], sslot.data(), 4 * (size_t)(2 * L), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->side[0].state, sstate.data(), (size_t)(2 * L), cudaMemcpyHostToDevice, st));
+        for (int k = 0; k < 6; ++k) {
+            if (l->CT[k])
+                CK(cudaMemcpyAsync(ctx->side[0].ct[k], l->CT[k], lp * (size_t)(2 * L), cudaMemcpyHostToDevice, st));
+            else
+                CK(cudaMemsetAsync(ctx->side[0].ct[k], 0, lp * (size_t)(2 * L), st));
+        }
+    }
+    CK(cudaMemcpyAsync(ctx->plStart, start.data(), 4 * (size_t)(n + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->eventCount, 0, sizeof(unsigned long long), st));
+    ctx->linkOwners.assign((size_t)L, 0);
+    ctx->linkKeys.resize((size_t)L);
+    ctx->linkKeyA.assign(l ? l->globalKeyEndA : nullptr, l ? l->globalKeyEndA + L : nullptr);
+    ctx->linkKeyB.assign(l ? l->globalKeyEndB : nullptr, l ? l->globalKeyEndB + L : nullptr);
+    ctx->linkNum.assign((size_t)L, 0);
+    for (long long i = 0; i < L; ++i) {
+        if (l->owners) ctx->linkOwners[i] = l->owners[i];
+        ctx->linkKeys[i] = l->globalKeys ? l->globalKeys[i] : i;
+        if (l->particleLinkNum) ctx->linkNum[i] = l->particleLinkNum[i];
+    }
+    CK(cudaStreamSynchronize(st));
+    ctx->L = L;
+    ctx->haveLinks = true;
+    ctx->built = false;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_grid_service(hidem_ctx *ctx) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    CK(cudaSetDevice(ctx->device));
+    return grid_service(ctx, false);
+}
+
+hidem_status hidem_regenerate(hidem_ctx *ctx) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    CK(cudaSetDevice(ctx->device));
+    ctx->accumulatedDist = 0;
+    return do_rebuild(ctx);
+}
+
+hidem_status hidem_compute_forces(hidem_ctx *ctx) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->built) TRY(do_rebuild(ctx));
+    if (ctx->mixed) {
+        StepArgs<float> a = step_args<float>(ctx);
+        launch_step<float>(ctx->cf, a, false, ctx->stream);
+    } else {
+        StepArgs<double> a = step_args<double>(ctx);
+        launch_step<double>(ctx->cd, a, false, ctx->stream);
+    }
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+hidem_status hidem_integrate(hidem_ctx *ctx) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->mixed)
+        launch_integrate<float>(ctx->cf, recp<float>(ctx, ctx->cur), ctx->type[ctx->ord],
+                                static_cast<const float *>(ctx->force), (int)ctx->n, ctx->stream);
+    else
+        launch_integrate<double>(ctx->cd, recp<double>(ctx, ctx->cur), ctx->type[ctx->ord],
+                                 static_cast<const double *>(ctx->force), (int)ctx->n, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+hidem_status hidem_link_update(hidem_ctx *ctx) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    CK(cudaSetDevice(ctx->device));
+    TRY(ctx->mixed ? link_update_now<float>(ctx, ctx->step) : link_update_now<double>(ctx, ctx->step));
+    CK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+hidem_status hidem_finalize_ts(hidem_ctx *ctx) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    ctx->step += 1;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_step(hidem_ctx *ctx, int32_t nsteps) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (nsteps < 0) return fail(ctx, HIDEM_ERR_ARG, "negative step count");
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    CK(cudaSetDevice(ctx->device));
+    return ctx->mixed ? run_steps<float>(ctx, nsteps) : run_steps<double>(ctx, nsteps);
+}
+
+hidem_status hidem_synchronize(hidem_ctx *ctx) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_device_error(ctx);
+}
+
+void *hidem_get_stream(hidem_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+hidem_status hidem_get_particles(hidem_ctx *ctx, hidem_particle_soa *out) {
+    if (!ctx || !out) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    CK(cudaSetDevice(ctx->device));
+    const long long n = ctx->n;
+    const size_t recBytes = ctx->mixed ? sizeof(PRec<float>) : sizeof(PRec<double>);
+    std::vector<unsigned char> host(recBytes * (size_t)n);
+    std::vector<int32_t> orig((size_t)n);
+    std::vector<uint8_t> ty((size_t)n);
+    CK(cudaMemcpyAsync(host.data(), ctx->rec[ctx->cur], host.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(orig.data(), ctx->orig[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ty.data(), ctx->type[ctx->ord], (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (long long s = 0; s < n; ++s) {
+        const long long i = orig[s];
+        const unsigned char *r = host.data() + recBytes * (size_t)s;
+        if (ctx->mixed) {
+            PRec<float> q;
+            std::memcpy(&q, r, sizeof q);
+            if (out->xCord) out->xCord[i] = q.x;
+            if (out->yCord) out->yCord[i] = q.y;
+            if (out->zCord) out->zCord[i] = q.z;
+            void *d[6] = {out->xDiff, out->yDiff, out->zDiff, out->uDiff, out->vDiff, out->wDiff};
+            for (int k = 0; k < 6; ++k) if (d[k]) static_cast<float *>(d[k])[i] = q.d[k];
+            void *th[3] = {out->xTheta, out->yTheta, out->zTheta};
+            for (int k = 0; k < 3; ++k) if (th[k]) static_cast<float *>(th[k])[i] = q.th[k];
+            if (out->radius) static_cast<float *>(out->radius)[i] = q.r;
+        } else {
+            PRec<double> q;
+            std::memcpy(&q, r, sizeof q);
+            if (out->xCord) out->xCord[i] = q.x;
+            if (out->yCord) out->yCord[i] = q.y;
+            if (out->zCord) out->zCord[i] = q.z;
+            void *d[6] = {out->xDiff, out->yDiff, out->zDiff, out->uDiff, out->vDiff, out->wDiff};
+            for (int k = 0; k < 6; ++k) if (d[k]) static_cast<double *>(d[k])[i] = q.d[k];
+            void *th[3] = {out->xTheta, out->yTheta, out->zTheta};
+            for (int k = 0; k < 3; ++k) if (th[k]) static_cast<double *>(th[k])[i] = q.th[k];
+            if (out->radius) static_cast<double *>(out->radius)[i] = q.r;
+        }
+        if (out->type) out->type[i] = ty[s];
+    }
+    if (out->owners) std::memcpy(out->owners, ctx->owners.data(), 4 * (size_t)n);
+    if (out->globalKeys) std::memcpy(out->globalKeys, ctx->keys.data(), 8 * (size_t)n);
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_links(hidem_ctx *ctx, hidem_link_soa *out) {
+    if (!ctx || !out) return HIDEM_ERR_ARG;
+    if (!ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "no links set");
+    CK(cudaSetDevice(ctx->device));
+    const long long L = ctx->L;
+    if (L == 0) return HIDEM_OK;
+    SideSet &s = ctx->side[ctx->curSide];
+    const long long cap = s.cap;
+    std::vector<int32_t> slot((size_t)(2 * L));
+    std::vector<uint8_t> st((size_t)cap);
+    CK(cudaMemcpyAsync(slot.data(), ctx->sideSlot[ctx->curSide], 4 * (size_t)(2 * L), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(st.data(), s.state, (size_t)cap, cudaMemcpyDeviceToHost, ctx->stream));
+    const size_t lp = ctx->lp;
+    std::vector<unsigned char> ct((size_t)cap * lp);
+    for (int k = 0; k < 6; ++k) {
+        if (!out->CT[k]) continue;
+        CK(cudaMemcpyAsync(ct.data(), s.ct[k], ct.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        unsigned char *dst = static_cast<unsigned char *>(out->CT[k]);
+        for (long long q = 0; q < 2 * L; ++q) std::memcpy(dst + lp * q, ct.data() + lp * (size_t)slot[q], lp);
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (out->state) for (long long i = 0; i < L; ++i) out->state[i] = st[slot[2 * i]];
+    if (out->initialLen) CK(cudaMemcpy(out->initialLen, ctx->L0link, lp * (size_t)L, cudaMemcpyDeviceToHost));
+    if (out->owners) for (long long i = 0; i < L; ++i) out->owners[i] = (int32_t)ctx->linkOwners[i];
+    if (out->globalKeys) std::memcpy(out->globalKeys, ctx->linkKeys.data(), 8 * (size_t)L);
+    if (out->globalKeyEndA) std::memcpy(out->globalKeyEndA, ctx->linkKeyA.data(), 8 * (size_t)L);
+    if (out->globalKeyEndB) std::memcpy(out->globalKeyEndB, ctx->linkKeyB.data(), 8 * (size_t)L);
+    if (out->particleLinkNum) std::memcpy(out->particleLinkNum, ctx->linkNum.data(), 4 * (size_t)L);
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_forces(hidem_ctx *ctx, void *force[6]) {
+    if (!ctx || !force) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    CK(cudaSetDevice(ctx->device));
+    const long long n = ctx->n;
+    const size_t lp = ctx->lp;
+    std::vector<unsigned char> f(6 * lp * (size_t)n);
+    std::vector<int32_t> orig((size_t)n);
+    CK(cudaMemcpyAsync(f.data(), ctx->force, f.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(orig.data(), ctx->orig[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 6; ++k) {
+        if (!force[k]) continue;
+        unsigned char *dst = static_cast<unsigned char *>(force[k]);
+        for (long long s = 0; s < n; ++s)
+            std::memcpy(dst + lp * (size_t)orig[s], f.data() + lp * (size_t)(k * n + s), lp);
+    }
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_cells(hidem_ctx *ctx, int32_t *ix, int32_t *iy, int32_t *iz, int64_t dims[3],
+                             double mins[3]) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HIDEM_ERR_STATE, "no neighbour structure built yet");
+    CK(cudaSetDevice(ctx->device));
+    const long long n = ctx->n;
+    const GridInfo &g = ctx->grid;
+    std::vector<int32_t> cell((size_t)n), orig((size_t)n);
+    // cellOf follows the slot order of the current record buffer
+    CK(cudaMemcpyAsync(cell.data(), ctx->cellOf[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(orig.data(), ctx->orig[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (long long s = 0; s < n; ++s) {
+        long long c = cell[s], i = orig[s];
+        if (ix) ix[i] = (int32_t)(c % g.X);
+        if (iy) iy[i] = (int32_t)((c / g.X) % g.Y);
+        if (iz) iz[i] = (int32_t)(c / ((long long)g.X * g.Y));
+    }
+    if (dims) {
+        dims[0] = g.X;
+        dims[1] = g.Y;
+        dims[2] = g.Z;
+    }
+    if (mins) {
+        mins[0] = g.xMin;
+        mins[1] = g.yMin;
+        mins[2] = g.zMin;
+    }
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_neighbours(hidem_ctx *ctx, int32_t *counts, int32_t *list, int64_t cap,
+                                  int64_t *total) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->built) return fail(ctx, HIDEM_ERR_STATE, "no neighbour structure built yet");
+    CK(cudaSetDevice(ctx->device));
+    const long long n = ctx->n;
+    const long long nb32 = nblocks32(n);
+    std::vector<uint32_t> cnt((size_t)n);
+    std::vector<int32_t> orig((size_t)n);
+    std::vector<long long> off((size_t)nb32);
+    CK(cudaMemcpyAsync(cnt.data(), ctx->counts, 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(orig.data(), ctx->orig[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(off.data(), ctx->nOff, 8 * (size_t)nb32, cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<int32_t> nbr((size_t)std::max<long long>(ctx->nbrCap, 1));
+    CK(cudaMemcpyAsync(nbr.data(), ctx->nbr, 4 * (size_t)ctx->nbrCap, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<int32_t> slotOf((size_t)n);
+    for (long long s = 0; s < n; ++s) slotOf[orig[s]] = (int32_t)s;
+    long long acc = 0;
+    for (long long i = 0; i < n; ++i) {
+        const long long s = slotOf[i];
+        const int c = (int)(cnt[s] & 0xffffu);
+        if (counts) counts[i] = c;
+        if (list) {
+            for (int k = 0; k < c; ++k) {
+                if (acc + k < cap) list[acc + k] = orig[nbr[off[s >> 5] + 32ll * k + (s & 31)]];
+            }
+        }
+        acc += c;
+    }
+    if (total) *total = acc;
+    if (list && acc > cap) return fail(ctx, HIDEM_ERR_CAPACITY, "contact list has %lld entries, cap %lld", acc, (long long)cap);
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_break_events(hidem_ctx *ctx, int64_t *link_index, int64_t *step, int64_t cap,
+                                    int64_t *count) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    unsigned long long total = 0;
+    CK(cudaMemcpyAsync(&total, ctx->eventCount, sizeof total, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    long long avail = std::min<long long>((long long)total, ctx->eventCap) - ctx->eventsRead;
+    if (avail < 0) avail = 0;
+    long long take = std::min<long long>(avail, cap);
+    if (take > 0) {
+        std::vector<int2> ev((size_t)take);
+        CK(cudaMemcpy(ev.data(), ctx->events + ctx->eventsRead, sizeof(int2) * (size_t)take, cudaMemcpyDeviceToHost));
+        for (long long k = 0; k < take; ++k) {
+            if (link_index) link_index[k] = ev[k].x;
+            if (step) step[k] = ev[k].y;
+        }
+        ctx->eventsRead += take;
+    }
+    if (count) *count = take;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_stats(hidem_ctx *ctx, hidem_stats *o) {
+    if (!ctx || !o) return HIDEM_ERR_ARG;
+    std::memset(o, 0, sizeof *o);
+    o->step = ctx->step;
+    o->num_particles = ctx->n;
+    o->num_links = ctx->L;
+    o->num_neighbour_pairs = ctx->numPairs;
+    o->max_neighbours = ctx->maxNeigh;
+    o->max_links_per_particle = ctx->maxLinksPP;
+    o->grid_dims[0] = ctx->grid.X;
+    o->grid_dims[1] = ctx->grid.Y;
+    o->grid_dims[2] = ctx->grid.Z;
+    o->grid_min[0] = ctx->grid.xMin;
+    o->grid_min[1] = ctx->grid.yMin;
+    o->grid_min[2] = ctx->grid.zMin;
+    o->regen_count = ctx->regenCount;
+    o->last_regen_step = ctx->lastRegen;
+    o->accumulated_dist = ctx->accumulatedDist;
+    o->search_distance = ctx->searchDistance;
+    o->interact_distance = ctx->interactDist;
+    o->kernel_launches = ctx->launches;
+    if (ctx->haveLinks && ctx->L > 0) {
+        unsigned long long total = 0;
+        CK(cudaMemcpyAsync(&total, ctx->eventCount, sizeof total, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        o->broken_links = (int64_t)total;
+    }
+    return HIDEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,687 @@
+// CUDA kernels of the hot path (sm_100a). Built with -fmad=false and IEEE
+// division / square root: see physics.cuh.
+//
+//   binning      k_bounds, k_bounds_final, k_cells, scan_*, k_scatter, k_sort_cells,
+//                k_permute                         (NeighbourGrid::generate, NeighbourGrid.cpp:48-184)
+//   contacts     k_nbr_count, k_nbr_fill           (NeighAccel::generateNeighbours, NeighAccel.h:25-137)
+//   link ends    k_side_count, k_side_fill         (LinkAccelSide::generateLinks/sortSideData,
+//                                                   LinkAccelSide.h:92-143,160-417)
+//   timestep     k_step<FUSED>                     (CombinedAccel::iterateCombined + applyForce +
+//                                                   linkUpdate, CombinedAccel.h:122-235)
+//                k_integrate, k_link_break, k_max_diff
+#include <cstdio>
+
+#include "kernels.h"
+#include "physics.cuh"
+
+namespace hidem {
+
+// ------------------------------------------------------------------ helpers
+
+template <class LP>
+__device__ __forceinline__ PRec<LP> load_rec(const PRec<LP> *p) {
+    PRec<LP> r;
+    const int4 *src = reinterpret_cast<const int4 *>(p);
+    int4 *dst = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(PRec<LP>) / 16); ++k) dst[k] = __ldg(src + k);
+    return r;
+}
+
+template <class LP>
+__device__ __forceinline__ void store_rec(PRec<LP> *p, const PRec<LP> &r) {
+    int4 *dst = reinterpret_cast<int4 *>(p);
+    const int4 *src = reinterpret_cast<const int4 *>(&r);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(PRec<LP>) / 16); ++k) dst[k] = src[k];
+}
+
+__device__ __forceinline__ unsigned long long max_bits(float v) {
+    return (unsigned long long)__float_as_uint(v);
+}
+__device__ __forceinline__ unsigned long long max_bits(double v) {
+    return (unsigned long long)__double_as_longlong(v);
+}
+
+__device__ __forceinline__ void set_error(int *flag, int code) {
+    if (flag) atomicCAS(flag, 0, code);
+}
+
+// ------------------------------------------------------------------ binning
+
+// Per-block min / max of the three coordinates over all particles
+// (ParticleData::getLimits, PLiB/ParticleData.h:47-59).
+template <class LP>
+__global__ void k_bounds(const PRec<LP> *__restrict__ rec, int n, double *__restrict__ partial) {
+    double mn[3] = {INFINITY, INFINITY, INFINITY};
+    double mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double *p = reinterpret_cast<const double *>(rec + i);
+        double v[3] = {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fmin(mn[k], v[k]);
+            mx[k] = fmax(mx[k], v[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+        }
+    }
+    __shared__ double sm[32][6];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        for (int k = 0; k < 3; ++k) {
+            sm[w][k] = mn[k];
+            sm[w][3 + k] = mx[k];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int nw = blockDim.x >> 5;
+        for (int k = 0; k < 3; ++k) {
+            double a = sm[0][k], b = sm[0][3 + k];
+            for (int j = 1; j < nw; ++j) {
+                a = fmin(a, sm[j][k]);
+                b = fmax(b, sm[j][3 + k]);
+            }
+            partial[blockIdx.x * 6 + k] = a;
+            partial[blockIdx.x * 6 + 3 + k] = b;
+        }
+    }
+}
+
+__global__ void k_bounds_final(const double *__restrict__ partial, int nb, double *__restrict__ out) {
+    if (threadIdx.x < 6) {
+        int k = threadIdx.x;
+        double v = partial[k];
+        for (int b = 1; b < nb; ++b) {
+            double u = partial[b * 6 + k];
+            v = (k < 3) ? fmin(v, u) : fmax(v, u);
+        }
+        out[k] = v;
+    }
+}
+
+// Cell colour of every slot and the per-cell counts (NeighbourGrid::getGridId /
+// getGridColor / colourParticles, NeighbourGrid.cpp:25-33,116-161).
+template <class LP>
+__global__ void k_cells(const PRec<LP> *__restrict__ rec, int n, GridInfo g,
+                        int *__restrict__ cellOf, int *__restrict__ cellCount, int *errorFlag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PRec<LP> *p = rec + i;
+    int ix = (int)floor((p->x - g.xMin) / g.h);
+    int iy = (int)floor((p->y - g.yMin) / g.h);
+    int iz = (int)floor((p->z - g.zMin) / g.h);
+    long long c = (long long)ix + (long long)iy * g.X + (long long)iz * g.X * g.Y;
+    if (c < 0 || c >= g.total) {
+        set_error(errorFlag, 1);
+        c = 0;
+    }
+    cellOf[i] = (int)c;
+    atomicAdd(cellCount + c, 1);
+}
+
+// Exclusive prefix sum in three passes (block sums, scan of block sums, add).
+constexpr int kScanBlock = 1024;  // elements per block (256 threads x 4)
+
+template <class TI, class TO>
+__global__ void k_scan_blocks(const TI *__restrict__ in, long long n, TO scaleBy,
+                              TO *__restrict__ out, TO *__restrict__ blockSums) {
+    __shared__ TO sh[kScanBlock];
+    long long base = (long long)blockIdx.x * kScanBlock;
+    for (int k = threadIdx.x; k < kScanBlock; k += blockDim.x) {
+        long long i = base + k;
+        sh[k] = (i < n) ? (TO)in[i] * scaleBy : (TO)0;
+    }
+    __syncthreads();
+    // Hillis-Steele would cost log steps x 1024; a simple two-level scan instead:
+    // each thread scans 4 consecutive elements, then a warp-level scan of thread totals.
+    int t = threadIdx.x;
+    TO local[4];
+    TO run = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        local[k] = run;
+        run += sh[t * 4 + k];
+    }
+    // inclusive scan of `run` over 256 threads
+    TO v = run;
+    int lane = t & 31, w = t >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        TO u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    __shared__ TO wsum[8];
+    if (lane == 31) wsum[w] = v;
+    __syncthreads();
+    if (t == 0) {
+        TO acc = 0;
+        for (int j = 0; j < 8; ++j) {
+            TO s = wsum[j];
+            wsum[j] = acc;
+            acc += s;
+        }
+    }
+    __syncthreads();
+    TO excl = v - run + wsum[w];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        long long i = base + t * 4 + k;
+        if (i < n) out[i] = excl + local[k];
+    }
+    if (t == blockDim.x - 1) blockSums[blockIdx.x] = excl + run;
+}
+
+template <class TO>
+__global__ void k_scan_sums(TO *__restrict__ sums, long long nb, TO *__restrict__ total) {
+    // one block: sequential over chunks of 1024 with the same two-level scheme
+    __shared__ TO carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long long base = 0; base < nb; base += blockDim.x) {
+        long long i = base + threadIdx.x;
+        TO v = (i < nb) ? sums[i] : (TO)0;
+        TO orig = v;
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            TO u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        __shared__ TO wsum[32];
+        if (lane == 31) wsum[w] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            TO acc = 0;
+            int nw = blockDim.x >> 5;
+            for (int j = 0; j < nw; ++j) {
+                TO s = wsum[j];
+                wsum[j] = acc;
+                acc += s;
+            }
+        }
+        __syncthreads();
+        TO excl = v - orig + wsum[w] + carry;
+        if (i < nb) sums[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + orig;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
+template <class TO>
+__global__ void k_scan_add(TO *__restrict__ out, long long n, const TO *__restrict__ sums) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += sums[i / kScanBlock];
+}
+
+// Counting-sort placement, unstable inside a cell (fixed by k_sort_cells).
+__global__ void k_scatter(const int *__restrict__ cellOf, int n, const int *__restrict__ cellStart,
+                          int *__restrict__ cursor, int *__restrict__ perm) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = cellOf[i];
+    int pos = cellStart[c] + atomicAdd(cursor + c, 1);
+    perm[pos] = i;
+}
+
+// Orders each cell's members by input index: the (colour, index) order of
+// NeighbourGrid::generateIterationList (NeighbourGrid.cpp:163-184).
+__global__ void k_sort_cells(const int *__restrict__ cellStart, const int *__restrict__ cellCount,
+                             long long total, const int *__restrict__ origOld, int *__restrict__ perm) {
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= total) return;
+    int cnt = cellCount[c];
+    if (cnt < 2) return;
+    int s = cellStart[c];
+    for (int a = 1; a < cnt; ++a) {
+        int v = perm[s + a];
+        int key = origOld[v];
+        int b = a - 1;
+        while (b >= 0 && origOld[perm[s + b]] > key) {
+            perm[s + b + 1] = perm[s + b];
+            --b;
+        }
+        perm[s + b + 1] = v;
+    }
+}
+
+template <class LP>
+__global__ void k_permute(const int *__restrict__ perm, int n, const PRec<LP> *__restrict__ recOld,
+                          PRec<LP> *__restrict__ recNew, const uint8_t *__restrict__ typeOld,
+                          uint8_t *__restrict__ typeNew, const int *__restrict__ origOld,
+                          int *__restrict__ origNew, const int *__restrict__ cellOld,
+                          int *__restrict__ cellNew, int *__restrict__ slotOf) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int o = perm[k];
+    store_rec(recNew + k, load_rec(recOld + o));
+    typeNew[k] = typeOld[o];
+    int g = origOld[o];
+    origNew[k] = g;
+    cellNew[k] = cellOld[o];
+    slotOf[g] = k;
+}
+
+// ------------------------------------------------------------------ contacts
+
+// Walk of NeighbourGrid::iteratePossibleNeighbours (PLiB/NeighbourGrid.h:87-105) with
+// the filter of NeighAccel::iterateBlocks (PLiB/Accel/NeighAccel.h:98-137). FILL=false
+// counts, FILL=true writes the row.
+template <class LP, bool FILL>
+__device__ __forceinline__ int walk_cells(const PRec<LP> *__restrict__ rec, int i, int colour,
+                                          const GridInfo &g, const int *__restrict__ cellStart,
+                                          const int *__restrict__ cellCount, double interactDist,
+                                          int32_t *__restrict__ row, long long rowBase) {
+    const double xc = rec[i].x, yc = rec[i].y, zc = rec[i].z;
+    const LP ri = rec[i].r;
+    int count = 0;
+    for (int k = 0; k < 27; ++k) {
+        int target = (int)((long long)colour + g.off[k]);
+        if (target < 0 || (long long)target >= g.total) continue;
+        int cnt = cellCount[target];
+        if (cnt == 0) continue;
+        int start = cellStart[target];
+        for (int j = start; j < start + cnt; ++j) {
+            if (j == i) continue;
+            const PRec<LP> *q = rec + j;
+            LP xDist = (LP)(xc - q->x);
+            LP xDist2 = xDist * xDist;
+            LP yDist = (LP)(yc - q->y);
+            LP yDist2 = yDist * yDist;
+            LP zDist = (LP)(zc - q->z);
+            LP zDist2 = zDist * zDist;
+            LP particleDistance2 = xDist2 + yDist2 + zDist2;
+            LP particleDistance = lsqrt(particleDistance2);
+            LP radSum = ri + q->r;
+            LP dist = particleDistance - radSum;
+            if ((double)dist < interactDist) {
+                if (FILL) row[rowBase + (long long)count * kWarp] = j;
+                ++count;
+            }
+        }
+    }
+    return count;
+}
+
+template <class LP>
+__global__ void k_nbr_count(const PRec<LP> *__restrict__ rec, int n, const int *__restrict__ cellOf,
+                            GridInfo g, const int *__restrict__ cellStart,
+                            const int *__restrict__ cellCount, double interactDist,
+                            uint32_t *__restrict__ counts, int *__restrict__ blockWidth,
+                            int *errorFlag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int c = 0;
+    if (i < n) {
+        c = walk_cells<LP, false>(rec, i, cellOf[i], g, cellStart, cellCount, interactDist, nullptr, 0);
+        if (c > 0xffff) {
+            set_error(errorFlag, 2);
+            c = 0xffff;
+        }
+        counts[i] = (uint32_t)c;
+    }
+    int m = c;
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && (i >> 5) * kWarp < n) blockWidth[i >> 5] = m;
+}
+
+template <class LP>
+__global__ void k_nbr_fill(const PRec<LP> *__restrict__ rec, int n, const int *__restrict__ cellOf,
+                           GridInfo g, const int *__restrict__ cellStart,
+                           const int *__restrict__ cellCount, double interactDist,
+                           const long long *__restrict__ nOff, int32_t *__restrict__ nbr) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    walk_cells<LP, true>(rec, i, cellOf[i], g, cellStart, cellCount, interactDist, nbr,
+                         nOff[i >> 5] + (i & 31));
+}
+
+// ------------------------------------------------------------------ link ends
+
+__global__ void k_side_count(const int *__restrict__ orig, int n, const int *__restrict__ plStart,
+                             uint32_t *__restrict__ counts, int *__restrict__ blockWidth,
+                             int *errorFlag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int c = 0;
+    if (i < n) {
+        int o = orig[i];
+        c = plStart[o + 1] - plStart[o];
+        if (c > 0xffff) {
+            set_error(errorFlag, 3);
+            c = 0xffff;
+        }
+        counts[i] = (counts[i] & 0xffffu) | ((uint32_t)c << 16);
+    }
+    int m = c;
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && (i >> 5) * kWarp < n) blockWidth[i >> 5] = m;
+}
+
+template <class LP>
+__global__ void k_side_fill(const int *__restrict__ orig, int n, const int *__restrict__ slotOf,
+                            const int *__restrict__ plStart, const int *__restrict__ plLink,
+                            const uint8_t *__restrict__ plEnd, const int *__restrict__ linkA,
+                            const int *__restrict__ linkB, const LP *__restrict__ L0link,
+                            const int *__restrict__ sideSlotOld, SideView<LP> oldS,
+                            const long long *__restrict__ sOff, SideView<LP> newS,
+                            int *__restrict__ sideSlotNew) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int o = orig[i];
+    int ps = plStart[o], pe = plStart[o + 1];
+    long long base = sOff[i >> 5] + (i & 31);
+    for (int k = 0; k < pe - ps; ++k) {
+        int l = plLink[ps + k];
+        int e = plEnd[ps + k];
+        int other = e ? linkA[l] : linkB[l];
+        long long dst = base + (long long)k * kWarp;
+        int src = sideSlotOld[2 * l + e];
+        newS.partner[dst] = (uint32_t)slotOf[other] | (e ? kSideIsB : 0u);
+        newS.state[dst] = oldS.state[src];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) newS.ct[c][dst] = oldS.ct[c][src];
+        newS.L0[dst] = L0link[l];
+        newS.link[dst] = l;
+        sideSlotNew[2 * l + e] = (int)dst;
+    }
+}
+
+// ------------------------------------------------------------------ timestep
+
+// One particle per thread. FUSED: previous step's link update (if pending), contacts,
+// link ends, integrate, write the record to the other buffer. Split (FUSED=false):
+// contacts and link ends only, forces to a.force (HiDEMLib::computePartForce).
+template <class LP, bool FUSED>
+__global__ void __launch_bounds__(kStepThreads)
+    k_step(const Consts<LP> c, const StepArgs<LP> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < a.n;
+    LP dmax[3] = {LP(0), LP(0), LP(0)};
+    if (live) {
+        PRec<LP> me = load_rec(a.in + i);
+        const uint32_t cnt = __ldg(a.counts + i);
+        const int nn = (int)(cnt & 0xffffu), ns = (int)(cnt >> 16);
+        LP F[6] = {0, 0, 0, 0, 0, 0};
+
+        const long long nbase = __ldg(a.nOff + (i >> 5)) + (i & 31);
+        for (int k = 0; k < nn; ++k) {
+            const int j = __ldg(a.nbr + nbase + (long long)k * kWarp);
+            const PRec<LP> o = load_rec(a.in + j);
+            contact_pair<LP>(c, LP(1), (LP)(me.x - o.x), (LP)(me.y - o.y), (LP)(me.z - o.z), me.d,
+                             me.r, o.d, o.r, F);
+        }
+
+        const long long sbase = __ldg(a.sOff + (i >> 5)) + (i & 31);
+        for (int k = 0; k < ns; ++k) {
+            const long long si = sbase + (long long)k * kWarp;
+            const uint32_t pw = __ldg(a.sPartner + si);
+            const PRec<LP> o = load_rec(a.in + (pw & kSlotMask));
+            uint8_t st = a.sState[si];
+            if (FUSED && a.breakPending && st != 0) {
+                const LP L0 = __ldg(a.sL0 + si);
+                const uint8_t nst = (pw & kSideIsB) ? break_link<LP>(c, o, me, st, L0)
+                                                    : break_link<LP>(c, me, o, st, L0);
+                if (nst != st) {
+                    a.sState[si] = nst;
+                    if (nst == 0 && !(pw & kSideIsB)) {
+                        unsigned long long slot = atomicAdd(a.eventCount, 1ull);
+                        if ((long long)slot < a.eventCap)
+                            a.events[slot] = make_int2(__ldg(a.sLink + si), (int)a.breakStep);
+                    }
+                    st = nst;
+                }
+            }
+            const LP mask = (st == 0) ? LP(0) : LP(1);
+            LP CT[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) CT[q] = a.ct[q][si];
+            beam_side<LP>(c, mask, (LP)(me.x - o.x), (LP)(me.y - o.y), (LP)(me.z - o.z), me.d, o.d,
+                          CT, F);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) a.ct[q][si] = CT[q];
+        }
+
+        if (FUSED) {
+            integrate_particle<LP>(c, me, __ldg(a.type + i), F);
+            store_rec(a.out + i, me);
+            dmax[0] = me.d[0] > LP(0) ? me.d[0] : LP(0);
+            dmax[1] = me.d[1] > LP(0) ? me.d[1] : LP(0);
+            dmax[2] = me.d[2] > LP(0) ? me.d[2] : LP(0);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) a.force[(long long)q * a.n + i] = F[q];
+        }
+    }
+    if (FUSED && a.reduceDiff) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            LP v = dmax[q];
+            for (int o = 16; o > 0; o >>= 1) {
+                LP u = __shfl_xor_sync(0xffffffffu, v, o);
+                v = (u > v) ? u : v;
+            }
+            if ((threadIdx.x & 31) == 0 && v > LP(0)) atomicMax(a.diffMax + q, max_bits(v));
+        }
+    }
+}
+
+// HiDEMLib::applyForce with the integrate step, in place (split path).
+template <class LP>
+__global__ void k_integrate(const Consts<LP> c, PRec<LP> *__restrict__ rec,
+                            const uint8_t *__restrict__ type, const LP *__restrict__ force, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    PRec<LP> me = load_rec(rec + i);
+    LP F[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) F[q] = force[(long long)q * n + i];
+    integrate_particle<LP>(c, me, type[i], F);
+    store_rec(rec + i, me);
+}
+
+// HiDEMLib::linkUpdate: the break functor over every link
+// (CombinedAccel::iterateLinks, CombinedAccel.h:200-235), with a warp-compacted
+// flag-and-select append of the links that broke.
+template <class LP>
+__global__ void k_link_break(const Consts<LP> c, const PRec<LP> *__restrict__ rec,
+                             const int *__restrict__ slotOf, const int *__restrict__ linkA,
+                             const int *__restrict__ linkB, const int *__restrict__ sideSlot,
+                             uint8_t *__restrict__ sState, const LP *__restrict__ sL0, long long L,
+                             long long step, int2 *__restrict__ events,
+                             unsigned long long *__restrict__ eventCount, long long eventCap) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool broke = false;
+    if (l < L) {
+        int sA = sideSlot[2 * l];
+        uint8_t st = sState[sA];
+        if (st != 0) {
+            const PRec<LP> pa = load_rec(rec + slotOf[linkA[l]]);
+            const PRec<LP> pb = load_rec(rec + slotOf[linkB[l]]);
+            uint8_t nst = break_link<LP>(c, pa, pb, st, sL0[sA]);
+            if (nst != st) {
+                sState[sA] = nst;
+                sState[sideSlot[2 * l + 1]] = nst;
+                broke = (nst == 0);
+            }
+        }
+    }
+    const unsigned ballot = __ballot_sync(0xffffffffu, broke);
+    if (ballot) {
+        const int lane = threadIdx.x & 31;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(eventCount, (unsigned long long)__popc(ballot));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (broke) {
+            unsigned long long slot = base + __popc(ballot & ((1u << lane) - 1u));
+            if ((long long)slot < eventCap) events[slot] = make_int2((int)l, (int)step);
+        }
+    }
+}
+
+// max(0, xDiff), max(0, yDiff), max(0, zDiff) over all particles
+// (HiDEMLib::getMaxDistOwned, HiDEMLib.h:424-461).
+template <class LP>
+__global__ void k_max_diff(const PRec<LP> *__restrict__ rec, int n,
+                           unsigned long long *__restrict__ out) {
+    LP v[3] = {LP(0), LP(0), LP(0)};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const PRec<LP> &p = rec[i];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) v[q] = (p.d[q] > v[q]) ? p.d[q] : v[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        LP m = v[q];
+        for (int o = 16; o > 0; o >>= 1) {
+            LP u = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (u > m) ? u : m;
+        }
+        if ((threadIdx.x & 31) == 0 && m > LP(0)) atomicMax(out + q, max_bits(m));
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+static inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+template <class LP>
+void launch_bounds(const PRec<LP> *rec, int n, double *partial, int nb, double *out, cudaStream_t s) {
+    k_bounds<LP><<<nb, 256, 0, s>>>(rec, n, partial);
+    k_bounds_final<<<1, 32, 0, s>>>(partial, nb, out);
+}
+
+template <class LP>
+void launch_cells(const PRec<LP> *rec, int n, const GridInfo &g, int *cellOf, int *cellCount,
+                  int *errorFlag, cudaStream_t s) {
+    k_cells<LP><<<nblk(n, 256), 256, 0, s>>>(rec, n, g, cellOf, cellCount, errorFlag);
+}
+
+template <class TI, class TO>
+int launch_scan(const TI *in, long long n, TO scaleBy, TO *out, TO *sums, TO *total, cudaStream_t s) {
+    long long nb = (n + kScanBlock - 1) / kScanBlock;
+    if (nb == 0) nb = 1;
+    k_scan_blocks<TI, TO><<<(unsigned)nb, 256, 0, s>>>(in, n, scaleBy, out, sums);
+    k_scan_sums<TO><<<1, 1024, 0, s>>>(sums, nb, total);
+    k_scan_add<TO><<<nblk(n > 0 ? n : 1, 256), 256, 0, s>>>(out, n, sums);
+    return 3;
+}
+template int launch_scan<int, int>(const int *, long long, int, int *, int *, int *, cudaStream_t);
+template int launch_scan<int, long long>(const int *, long long, long long, long long *, long long *,
+                                         long long *, cudaStream_t);
+
+void launch_scatter(const int *cellOf, int n, const int *cellStart, int *cursor, int *perm,
+                    cudaStream_t s) {
+    k_scatter<<<nblk(n, 256), 256, 0, s>>>(cellOf, n, cellStart, cursor, perm);
+}
+
+void launch_sort_cells(const int *cellStart, const int *cellCount, long long total,
+                       const int *origOld, int *perm, cudaStream_t s) {
+    k_sort_cells<<<nblk(total, 256), 256, 0, s>>>(cellStart, cellCount, total, origOld, perm);
+}
+
+template <class LP>
+void launch_permute(const int *perm, int n, const PRec<LP> *recOld, PRec<LP> *recNew,
+                    const uint8_t *typeOld, uint8_t *typeNew, const int *origOld, int *origNew,
+                    const int *cellOld, int *cellNew, int *slotOf, cudaStream_t s) {
+    k_permute<LP><<<nblk(n, 256), 256, 0, s>>>(perm, n, recOld, recNew, typeOld, typeNew, origOld,
+                                               origNew, cellOld, cellNew, slotOf);
+}
+
+template <class LP>
+void launch_nbr_count(const PRec<LP> *rec, int n, const int *cellOf, const GridInfo &g,
+                      const int *cellStart, const int *cellCount, double interactDist,
+                      uint32_t *counts, int *blockWidth, int *errorFlag, cudaStream_t s) {
+    k_nbr_count<LP><<<nblk(n, 128), 128, 0, s>>>(rec, n, cellOf, g, cellStart, cellCount,
+                                                 interactDist, counts, blockWidth, errorFlag);
+}
+
+template <class LP>
+void launch_nbr_fill(const PRec<LP> *rec, int n, const int *cellOf, const GridInfo &g,
+                     const int *cellStart, const int *cellCount, double interactDist,
+                     const long long *nOff, int32_t *nbr, cudaStream_t s) {
+    k_nbr_fill<LP><<<nblk(n, 128), 128, 0, s>>>(rec, n, cellOf, g, cellStart, cellCount,
+                                                interactDist, nOff, nbr);
+}
+
+void launch_side_count(const int *orig, int n, const int *plStart, uint32_t *counts,
+                       int *blockWidth, int *errorFlag, cudaStream_t s) {
+    k_side_count<<<nblk(n, 256), 256, 0, s>>>(orig, n, plStart, counts, blockWidth, errorFlag);
+}
+
+template <class LP>
+void launch_side_fill(const int *orig, int n, const int *slotOf, const int *plStart,
+                      const int *plLink, const uint8_t *plEnd, const int *linkA, const int *linkB,
+                      const LP *L0link, const int *sideSlotOld, const SideView<LP> &oldS,
+                      const long long *sOff, const SideView<LP> &newS, int *sideSlotNew,
+                      cudaStream_t s) {
+    k_side_fill<LP><<<nblk(n, 256), 256, 0, s>>>(orig, n, slotOf, plStart, plLink, plEnd, linkA,
+                                                 linkB, L0link, sideSlotOld, oldS, sOff, newS,
+                                                 sideSlotNew);
+}
+
+template <class LP>
+void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, cudaStream_t s) {
+    int nb = nblk(a.n, kStepThreads);
+    if (fused)
+        k_step<LP, true><<<nb, kStepThreads, 0, s>>>(c, a);
+    else
+        k_step<LP, false><<<nb, kStepThreads, 0, s>>>(c, a);
+}
+
+template <class LP>
+void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,
+                      int n, cudaStream_t s) {
+    k_integrate<LP><<<nblk(n, 256), 256, 0, s>>>(c, rec, type, force, n);
+}
+
+template <class LP>
+void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slotOf,
+                       const int *linkA, const int *linkB, const int *sideSlot, uint8_t *sState,
+                       const LP *sL0, long long L, long long step, int2 *events,
+                       unsigned long long *eventCount, long long eventCap, cudaStream_t s) {
+    if (L <= 0) return;
+    k_link_break<LP><<<nblk(L, 256), 256, 0, s>>>(c, rec, slotOf, linkA, linkB, sideSlot, sState,
+                                                  sL0, L, step, events, eventCount, eventCap);
+}
+
+template <class LP>
+void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb, cudaStream_t s) {
+    k_max_diff<LP><<<nb, 256, 0, s>>>(rec, n, out);
+}
+
+#define HIDEM_INSTANTIATE(LP)                                                                      \
+    template void launch_bounds<LP>(const PRec<LP> *, int, double *, int, double *, cudaStream_t); \
+    template void launch_cells<LP>(const PRec<LP> *, int, const GridInfo &, int *, int *, int *,   \
+                                   cudaStream_t);                                                  \
+    template void launch_permute<LP>(const int *, int, const PRec<LP> *, PRec<LP> *,               \
+                                     const uint8_t *, uint8_t *, const int *, int *, const int *,  \
+                                     int *, int *, cudaStream_t);                                  \
+    template void launch_nbr_count<LP>(const PRec<LP> *, int, const int *, const GridInfo &,       \
+                                       const int *, const int *, double, uint32_t *, int *, int *, \
+                                       cudaStream_t);                                              \
+    template void launch_nbr_fill<LP>(const PRec<LP> *, int, const int *, const GridInfo &,        \
+                                      const int *, const int *, double, const long long *,         \
+                                      int32_t *, cudaStream_t);                                    \
+    template void launch_side_fill<LP>(const int *, int, const int *, const int *, const int *,    \
+                                       const uint8_t *, const int *, const int *, const LP *,      \
+                                       const int *, const SideView<LP> &, const long long *,       \
+                                       const SideView<LP> &, int *, cudaStream_t);                 \
+    template void launch_step<LP>(const Consts<LP> &, const StepArgs<LP> &, bool, cudaStream_t);   \
+    template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
+                                       const LP *, int, cudaStream_t);                             \
+    template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \
+                                        const int *, const int *, const int *, uint8_t *,          \
+                                        const LP *, long long, long long, int2 *,                  \
+                                        unsigned long long *, long long, cudaStream_t);            \
+    template void launch_max_diff<LP>(const PRec<LP> *, int, unsigned long long *, int,            \
+                                      cudaStream_t);
+
+HIDEM_INSTANTIATE(float)
+HIDEM_INSTANTIATE(double)
+
+}  // namespace hidem

@@ -1,0 +1,65 @@
+// Launch wrappers of the kernels in kernels.cu (all enqueue on the given stream).
+#pragma once
+#include "internal.h"
+
+namespace hidem {
+
+constexpr int kStepThreads = 128;
+
+// One set of link-end ("side") arrays in the warp-blocked ELL layout.
+template <class LP>
+struct SideView {
+    uint32_t *partner;  // partner slot | kSideIsB
+    LP *ct[6];          // CT0..CT5
+    uint8_t *state;     // per-side copy of the link state
+    LP *L0;             // initial length of the link
+    int32_t *link;      // link index (input order)
+};
+
+template <class LP>
+void launch_bounds(const PRec<LP> *rec, int n, double *partial, int nb, double *out, cudaStream_t s);
+template <class LP>
+void launch_cells(const PRec<LP> *rec, int n, const GridInfo &g, int *cellOf, int *cellCount,
+                  int *errorFlag, cudaStream_t s);
+// Exclusive scan of `in` (times scaleBy) into `out`; `sums` holds ceil(n/1024) elements;
+// `total` (may be null) receives the grand total. Returns the number of launches.
+template <class TI, class TO>
+int launch_scan(const TI *in, long long n, TO scaleBy, TO *out, TO *sums, TO *total, cudaStream_t s);
+void launch_scatter(const int *cellOf, int n, const int *cellStart, int *cursor, int *perm,
+                    cudaStream_t s);
+void launch_sort_cells(const int *cellStart, const int *cellCount, long long total,
+                       const int *origOld, int *perm, cudaStream_t s);
+template <class LP>
+void launch_permute(const int *perm, int n, const PRec<LP> *recOld, PRec<LP> *recNew,
+                    const uint8_t *typeOld, uint8_t *typeNew, const int *origOld, int *origNew,
+                    const int *cellOld, int *cellNew, int *slotOf, cudaStream_t s);
+template <class LP>
+void launch_nbr_count(const PRec<LP> *rec, int n, const int *cellOf, const GridInfo &g,
+                      const int *cellStart, const int *cellCount, double interactDist,
+                      uint32_t *counts, int *blockWidth, int *errorFlag, cudaStream_t s);
+template <class LP>
+void launch_nbr_fill(const PRec<LP> *rec, int n, const int *cellOf, const GridInfo &g,
+                     const int *cellStart, const int *cellCount, double interactDist,
+                     const long long *nOff, int32_t *nbr, cudaStream_t s);
+void launch_side_count(const int *orig, int n, const int *plStart, uint32_t *counts,
+                       int *blockWidth, int *errorFlag, cudaStream_t s);
+template <class LP>
+void launch_side_fill(const int *orig, int n, const int *slotOf, const int *plStart,
+                      const int *plLink, const uint8_t *plEnd, const int *linkA, const int *linkB,
+                      const LP *L0link, const int *sideSlotOld, const SideView<LP> &oldS,
+                      const long long *sOff, const SideView<LP> &newS, int *sideSlotNew,
+                      cudaStream_t s);
+template <class LP>
+void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, cudaStream_t s);
+template <class LP>
+void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,
+                      int n, cudaStream_t s);
+template <class LP>
+void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slotOf,
+                       const int *linkA, const int *linkB, const int *sideSlot, uint8_t *sState,
+                       const LP *sL0, long long L, long long step, int2 *events,
+                       unsigned long long *eventCount, long long eventCap, cudaStream_t s);
+template <class LP>
+void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb, cudaStream_t s);
+
+}  // namespace hidem

@@ -1,0 +1,248 @@
+// Per-pair, per-side, per-link and per-particle arithmetic of the default HiDEM
+// functors, written for the device. Every expression keeps the reference's operand
+// order and association (HiDEM/Common/HiDEMDefaultFunctions.h) and the translation
+// units are compiled with -fmad=false and IEEE division / square root, so results
+// are bit-identical to the reference's IEEE CPU build for the same inputs.
+#pragma once
+#include "internal.h"
+
+namespace hidem {
+
+__device__ __forceinline__ float lsqrt(float v) { return sqrtf(v); }
+__device__ __forceinline__ double lsqrt(double v) { return sqrt(v); }
+__device__ __forceinline__ float labs_(float v) { return fabsf(v); }
+__device__ __forceinline__ double labs_(double v) { return fabs(v); }
+
+// Contact / damping between two particles: HiDEMDefNeighForceFunc::operator()
+// (HiDEMDefaultFunctions.h:21-87). s = self (xDiff..wDiff, radius), o = other.
+template <class LP>
+__device__ __forceinline__ void contact_pair(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
+                                             LP zDist, const LP *s, LP sr, const LP *o, LP orr,
+                                             LP *F) {
+    LP xDist2 = xDist * xDist;
+    LP yDist2 = yDist * yDist;
+    LP zDist2 = zDist * zDist;
+    LP particleDistance2 = xDist2 + yDist2 + zDist2;
+    LP radSum = sr + orr;
+    LP activeDist2 = (radSum + c.attractDistance) * (radSum + c.attractDistance);
+    mask = (particleDistance2 >= activeDist2) ? LP(0) : mask;
+    LP particleDistance = lsqrt(particleDistance2);
+    LP invDist = LP(1) / particleDistance;
+    LP xComp = xDist * invDist;
+    LP yComp = yDist * invDist;
+    LP zComp = zDist * invDist;
+    LP Cnst = 0;
+    LP dimDist = radSum - particleDistance;
+    Cnst = (particleDistance < radSum) ? lsqrt(dimDist * dimDist * dimDist) : Cnst;
+    Cnst = (particleDistance >= radSum && particleDistance < radSum + c.attractDistance)
+               ? c.attractScaleForce * dimDist
+               : Cnst;
+    Cnst = Cnst * c.scaleE;
+    F[0] = F[0] + mask * ((-c.damping) * ((s[0] - o[0]) * c.invDt) + (Cnst * xComp));
+    F[1] = F[1] + mask * ((-c.damping) * ((s[1] - o[1]) * c.invDt) + (Cnst * yComp));
+    F[2] = F[2] + mask * ((-c.damping) * ((s[2] - o[2]) * c.invDt) + (Cnst * zComp));
+    F[3] = F[3] + mask * ((-c.dampingRotation) * ((s[3] - o[3]) * c.invDt));
+    F[4] = F[4] + mask * ((-c.dampingRotation) * ((s[4] - o[4]) * c.invDt));
+    F[5] = F[5] + mask * ((-c.dampingRotation) * ((s[5] - o[5]) * c.invDt));
+}
+
+// Bonded beam on one link end: HiDEMDefLinkForceFunc::operator()
+// (HiDEMDefaultFunctions.h:90-204). CT is this side's history state (in/out).
+template <class LP>
+__device__ __forceinline__ void beam_side(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
+                                          LP zDist, const LP *s, const LP *o, LP *CT, LP *F) {
+    F[0] = F[0] + (-c.damping * ((s[0] - o[0]) * c.invDt)) * mask;
+    F[1] = F[1] + (-c.damping * ((s[1] - o[1]) * c.invDt)) * mask;
+    F[2] = F[2] + (-c.damping * ((s[2] - o[2]) * c.invDt)) * mask;
+    F[3] = F[3] + (-c.dampingRotation * ((s[3] - o[3]) * c.invDt)) * mask;
+    F[4] = F[4] + (-c.dampingRotation * ((s[4] - o[4]) * c.invDt)) * mask;
+    F[5] = F[5] + (-c.dampingRotation * ((s[5] - o[5]) * c.invDt)) * mask;
+
+    LP xDist2 = xDist * xDist;
+    LP yDist2 = yDist * yDist;
+    if (xDist == LP(0) && yDist == LP(0)) {
+        xDist2 = LP(1e-10);
+        yDist2 = LP(1e-10);
+    }
+    LP zDist2 = zDist * zDist;
+    LP distSum = xDist2 + yDist2 + zDist2;
+    LP invLI = LP(1) / lsqrt(distSum);
+    LP invLP = LP(1) / lsqrt(xDist2 + yDist2);
+    LP invLILP = invLI * invLP;
+    LP LI = invLI * distSum;
+
+    LP T00 = xDist * invLI, T01 = yDist * invLI, T02 = zDist * invLI;
+    LP T10 = -yDist * invLP, T11 = xDist * invLP;
+    LP T20 = -(zDist * xDist) * invLILP;
+    LP T21 = -(zDist * yDist) * invLILP;
+    LP T22 = (xDist2 + yDist2) * invLILP;
+
+    LP B0 = T00 * s[0] + T01 * s[1] + T02 * s[2];
+    LP B1 = T10 * s[0] + T11 * s[1];
+    LP B2 = T20 * s[0] + T21 * s[1] + T22 * s[2];
+    LP B4 = T10 * s[3] + T11 * s[4];
+    LP B5 = T20 * s[3] + T21 * s[4] + T22 * s[5];
+    LP B6 = T00 * o[0] + T01 * o[1] + T02 * o[2];
+    LP B7 = T10 * o[0] + T11 * o[1];
+    LP B8 = T20 * o[0] + T21 * o[1] + T22 * o[2];
+    LP B10 = T10 * o[3] + T11 * o[4];
+    LP B11 = T20 * o[3] + T21 * o[4] + T22 * o[5];
+
+    LP L2 = LI * LI;
+    LP L3 = LI * LI * LI;
+    LP LIDiv6 = (LP(1) / LP(6)) * invLI;
+    LP K0 = c.E * c.W2 * invLI;
+    LP K1 = c.E * c.W4 / L3;
+    LP K5 = c.E * c.W4 / (LP(2) * L2);
+
+    CT[0] = CT[0] + (K0 * B0 + (-K0) * B6);
+    CT[1] = CT[1] + (K1 * B1 + K5 * B5 + (-K1) * B7 + K5 * B11);
+    CT[2] = CT[2] + (K1 * B2 + (-K5) * B4 + (-K1) * B8 + (-K5) * B10);
+
+    F[0] = F[0] + (-(T00 * CT[0] + T10 * CT[1] + T20 * CT[2])) * mask;
+    F[1] = F[1] + (-(T01 * CT[0] + T11 * CT[1] + T21 * CT[2])) * mask;
+    F[2] = F[2] + (-(T02 * CT[0] + T22 * CT[2])) * mask;
+
+    LP K2 = c.G * c.W4 * LIDiv6;
+    LP K3 = c.E * c.W4 * LIDiv6 * LP(2);
+    LP K4 = c.E * c.W4 * LIDiv6;
+    LP B3 = T00 * s[3] + T01 * s[4] + T02 * s[5];
+    LP B9 = T00 * o[3] + T01 * o[4] + T02 * o[5];
+
+    CT[3] = CT[3] + (K2 * B3 + (-K2) * B9);
+    CT[4] = CT[4] + ((-K5) * B2 + K3 * B4 + K5 * B8 + K4 * B10);
+    CT[5] = CT[5] + (K5 * B1 + K3 * B5 + (-K5) * B7 + K4 * B11);
+
+    F[3] = F[3] + (-(T00 * CT[3] + T10 * CT[4] + T20 * CT[5])) * mask;
+    F[4] = F[4] + (-(T01 * CT[3] + T11 * CT[4] + T21 * CT[5])) * mask;
+    F[5] = F[5] + (-(T02 * CT[3] + T22 * CT[5])) * mask;
+}
+
+// Link break test: HiDEMDefLinkBreakFunc::operator() (HiDEMDefaultFunctions.h:207-242)
+// with end A as particle 1 and end B as particle 2. Returns the new state.
+template <class LP>
+__device__ __forceinline__ uint8_t break_link(const Consts<LP> &c, const PRec<LP> &a,
+                                              const PRec<LP> &b, uint8_t state, LP initialLen) {
+    if (state == 0) return 0;
+    LP xDist = (LP)(a.x - b.x);
+    LP yDist = (LP)(a.y - b.y);
+    LP zDist = (LP)(a.z - b.z);
+    LP stretchLength = lsqrt((xDist * xDist) + (yDist * yDist) + (zDist * zDist));
+    LP ax = labs_(a.th[0] - b.th[0]);
+    LP ay = labs_(a.th[1] - b.th[1]);
+    LP az = labs_(a.th[2] - b.th[2]);
+    LP myz = (ay < az) ? az : ay;  // std::max(ay, az)
+    LP maxBend = (ax < myz) ? myz : ax;
+    LP load = (stretchLength - initialLen) / initialLen + c.bendBreak * maxBend;
+    return (load >= c.maxLoad) ? uint8_t(0) : state;
+}
+
+// The sample integrate step on one particle (HiDEM/MeshBlock/MainMeshBlock.cpp:182-261:
+// gravity / buoyancy, air / water drag, HiDEMDefTimeIntegration
+// HiDEMDefaultFunctions.h:318-370) plus the optional GlacierDem bed terms
+// (HiDEM/GlacierDem/MainDem.cpp:176-207), HiDEMDefVelocityLimit (245-290),
+// HiDEMDefBoundaryCondition (293-315) and the fixed-layer / front-pressure extensions.
+// `p` is updated in place; F is the particle's accumulated force.
+template <class LP>
+__device__ __forceinline__ void integrate_particle(const Consts<LP> &c, PRec<LP> &p, uint8_t type,
+                                                   LP *F) {
+    if (c.useFixed && (type & HIDEM_TYPE_FIXED)) {
+        for (int k = 0; k < 6; ++k) p.d[k] = LP(0);
+        return;
+    }
+    double xCord = p.x, yCord = p.y, zCord = p.z;
+    const LP xDiff = p.d[0], yDiff = p.d[1], zDiff = p.d[2];
+    const LP uDiff = p.d[3], vDiff = p.d[4], wDiff = p.d[5];
+    LP xTheta = p.th[0], yTheta = p.th[1], zTheta = p.th[2];
+    const LP radius = p.r;
+    const LP diameter = radius * LP(2);
+
+    LP dragCoeff;
+    if (c.useBed && ((zCord + (double)radius) - (double)c.bedHeight < (double)c.bedInteract)) {
+        LP a = c.bedDrag * c.bedFriction;
+        LP b = LP(1e+5) * c.scale * c.scale;
+        dragCoeff = (b < a) ? b : a;  // std::min(a, b)
+    } else if (zCord > (double)c.waterLevel) {
+        dragCoeff = c.airDrag;
+    } else {
+        dragCoeff = c.waterDrag;
+    }
+    LP xForce = F[0], yForce = F[1], zForce = F[2];
+    LP uForce = F[3], vForce = F[4], wForce = F[5];
+    const LP particleMass = c.rhoIce * diameter * diameter * diameter;
+    const LP particleMomentInertia = particleMass * diameter * diameter / LP(6);
+
+    if (zCord > (double)c.waterLevel) zForce = zForce + -c.g * particleMass;
+    if (zCord <= (double)c.waterLevel) zForce = zForce + c.lift * particleMass;
+    if (c.useBed && zCord + (double)radius < (double)c.bedHeight)
+        zForce = (LP)((double)zForce +
+                      (double)c.bedStiffness * ((double)c.bedHeight - (zCord + (double)radius)));
+    if (c.useFront && (type & HIDEM_TYPE_FRONT) && zCord < (double)c.waterLevel) {
+        LP depth = (LP)((double)c.waterLevel - zCord);
+        xForce = xForce - c.rhoWater * c.g * depth * diameter * diameter;
+    }
+
+    const LP dragInvDt2 = dragCoeff * c.invDt2;
+    const LP massDtSqr = particleMass * c.invDtSqr;
+    const LP pMassDtSqr = particleMass / c.dtSqr;
+    const LP pMemDtSqr = particleMomentInertia / c.dtSqr;
+    const LP invC1 = LP(1) / (pMassDtSqr + dragCoeff * c.invDt2);
+    const LP invC2 = LP(1) / (pMemDtSqr + dragCoeff * c.invDt2);
+    const LP interDtSqr = particleMomentInertia * c.invDtSqr;
+    const LP xDN = (xForce + massDtSqr * xDiff + dragInvDt2 * -xDiff) * invC1;
+    const LP yDN = (yForce + massDtSqr * yDiff + dragInvDt2 * -yDiff) * invC1;
+    const LP zDN = (zForce + massDtSqr * zDiff + dragInvDt2 * -zDiff) * invC1;
+    const LP uDN = (uForce + interDtSqr * uDiff + dragInvDt2 * -uDiff) * invC2;
+    const LP vDN = (vForce + interDtSqr * vDiff + dragInvDt2 * -vDiff) * invC2;
+    const LP wDN = (wForce + interDtSqr * wDiff + dragInvDt2 * -wDiff) * invC2;
+
+    const double xPrev = xCord, yPrev = yCord, zPrev = zCord;
+    const LP xThPrev = xTheta, yThPrev = yTheta, zThPrev = zTheta;
+    xCord = xCord + (double)xDN;
+    yCord = yCord + (double)yDN;
+    zCord = zCord + (double)zDN;
+    xTheta = xTheta + uDN;
+    yTheta = yTheta + vDN;
+    zTheta = zTheta + wDN;
+
+    if (c.useVel) {
+        const LP xVel = xDN * c.invDt, yVel = yDN * c.invDt, zVel = zDN * c.invDt;
+        const LP xTV = (xTheta - xThPrev) * c.invDt;
+        const LP yTV = (yTheta - yThPrev) * c.invDt;
+        const LP zTV = (zTheta - zThPrev) * c.invDt;
+        if (xVel > c.maxVel) xCord = (double)(c.dt * c.maxVel) + xPrev;
+        if (yVel > c.maxVel) yCord = (double)(c.dt * c.maxVel) + yPrev;
+        if (zVel > c.maxVel) zCord = (double)(c.dt * c.maxVel) + zPrev;
+        if (xTV > c.maxRot) xTheta = c.dt * c.maxRot + xThPrev;
+        if (yTV > c.maxRot) yTheta = c.dt * c.maxRot + yThPrev;
+        if (zTV > c.maxRot) zTheta = c.dt * c.maxRot + zThPrev;
+        if (xVel < -c.maxVel) xCord = (double)(c.dt * -c.maxVel) + xPrev;
+        if (yVel < -c.maxVel) yCord = (double)(c.dt * -c.maxVel) + yPrev;
+        if (zVel < -c.maxVel) zCord = (double)(c.dt * -c.maxVel) + zPrev;
+        if (xTV < -c.maxRot) xTheta = c.dt * -c.maxRot + xThPrev;
+        if (yTV < -c.maxRot) yTheta = c.dt * -c.maxRot + yThPrev;
+        if (zTV < -c.maxRot) zTheta = c.dt * -c.maxRot + zThPrev;
+    }
+    if (c.useBnd) {
+        if (xCord + (double)radius < c.lower[0] && c.bmin[0]) xCord = xPrev;
+        if (xCord - (double)radius > c.upper[0] && c.bmax[0]) xCord = xPrev;
+        if (yCord + (double)radius < c.lower[1] && c.bmin[1]) yCord = yPrev;
+        if (yCord - (double)radius > c.upper[1] && c.bmax[1]) yCord = yPrev;
+        if (zCord + (double)radius < c.lower[2] && c.bmin[2]) zCord = zPrev;
+        if (zCord - (double)radius > c.upper[2] && c.bmax[2]) zCord = zPrev;
+    }
+    p.x = xCord;
+    p.y = yCord;
+    p.z = zCord;
+    p.th[0] = xTheta;
+    p.th[1] = yTheta;
+    p.th[2] = zTheta;
+    p.d[0] = (LP)(xCord - xPrev);
+    p.d[1] = (LP)(yCord - yPrev);
+    p.d[2] = (LP)(zCord - zPrev);
+    p.d[3] = xTheta - xThPrev;
+    p.d[4] = yTheta - yThPrev;
+    p.d[5] = zTheta - zThPrev;
+}
+
+}  // namespace hidem

@@ -1,0 +1,181 @@
+"""Python host mirror of the reference's ``HiDEMLib`` operator surface over the C ABI.
+
+Method names follow ``HiDEMLib<PDataT, LDataT>`` (HiDEMLib/HiDEMLib.h): ``gridService``
+(533-628), ``computePartForce`` (316-382) with the default contact and beam functors,
+``applyForce`` (303-314) with the sample integrate step, ``linkUpdate`` (256-269) with the
+default break functor, ``finalizeTs`` (495-530), ``getCurrentTimestep`` (245-247), ``run``
+(234-240). ``step(n)`` runs n whole timesteps of the sample main loop
+(HiDEM/MeshBlock/MainMeshBlock.cpp:274-323) as one fused kernel per step.
+
+Errors follow the C ABI: every failing call raises ``HidemError`` carrying the status and
+``hidem_last_error`` text (the reference would print and ``exit(1)``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+class HiDEMLib:
+    def __init__(self, params: abi.HidemParams, device: int = 0, end_timestep: int | None = None):
+        self._lib = abi.load()
+        self.params = params
+        self.precision = int(params.precision)
+        self.lp = abi.lp_dtype(self.precision)
+        h = C.c_void_p()
+        st = self._lib.hidem_create(C.byref(params), int(device), C.byref(h))
+        if st != abi.HIDEM_OK:
+            raise abi.HidemError(st, self._lib.hidem_create_error().decode())
+        self._ctx = h
+        self.n = 0
+        self.L = 0
+        self.end_timestep = end_timestep
+
+    # ------------------------------------------------------------ plumbing
+    def _check(self, st: int) -> None:
+        if st != abi.HIDEM_OK:
+            raise abi.HidemError(st, self._lib.hidem_last_error(self._ctx).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            self._lib.hidem_destroy(self._ctx)
+            self._ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return int(self._lib.hidem_get_stream(self._ctx) or 0)
+
+    # ------------------------------------------------------------ data
+    def set_particles(self, arrays: dict) -> None:
+        n = int(arrays["xCord"].shape[0])
+        soa = abi.particle_soa(arrays, self.precision, n)
+        self._check(self._lib.hidem_set_particles(self._ctx, C.byref(soa), n))
+        self.n = n
+
+    def set_links(self, arrays: dict) -> None:
+        L = int(arrays["globalKeyEndA"].shape[0])
+        soa = abi.link_soa(arrays, self.precision, L)
+        self._check(self._lib.hidem_set_links(self._ctx, C.byref(soa), L))
+        self.L = L
+
+    def set_timestep(self, step: int) -> None:
+        self._check(self._lib.hidem_set_timestep(self._ctx, int(step)))
+
+    def set_params(self, params: abi.HidemParams) -> None:
+        self._check(self._lib.hidem_set_params(self._ctx, C.byref(params)))
+        self.params = params
+
+    # ------------------------------------------------------------ timestep surface
+    def gridService(self) -> None:
+        self._check(self._lib.hidem_grid_service(self._ctx))
+
+    def regenerate(self) -> None:
+        self._check(self._lib.hidem_regenerate(self._ctx))
+
+    def computePartForce(self) -> None:
+        self._check(self._lib.hidem_compute_forces(self._ctx))
+
+    def applyForce(self) -> None:
+        self._check(self._lib.hidem_integrate(self._ctx))
+
+    def linkUpdate(self) -> None:
+        self._check(self._lib.hidem_link_update(self._ctx))
+
+    def finalizeTs(self) -> None:
+        self._check(self._lib.hidem_finalize_ts(self._ctx))
+
+    def getCurrentTimestep(self) -> int:
+        return int(self.stats()["step"])
+
+    def run(self) -> bool:
+        return self.end_timestep is None or self.getCurrentTimestep() < self.end_timestep
+
+    def breakActive(self) -> bool:
+        """The sample main's gate ``getCurrentTimestep() * dt > breakTime`` in lp."""
+        lp = self.lp
+        t = lp(self.getCurrentTimestep())
+        return bool(lp(t * lp(self.params.dt)) > lp(self.params.breakTime))
+
+    def timestep_split(self) -> None:
+        """One sample-main timestep through the separate operator calls."""
+        self.gridService()
+        self.computePartForce()
+        self.applyForce()
+        if self.breakActive():
+            self.linkUpdate()
+        self.finalizeTs()
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self._lib.hidem_step(self._ctx, int(nsteps)))
+
+    def synchronize(self) -> None:
+        self._check(self._lib.hidem_synchronize(self._ctx))
+
+    # ------------------------------------------------------------ readback
+    def get_particles(self) -> dict:
+        out = abi.empty_particles(self.n, self.precision)
+        soa = abi.particle_soa(out, self.precision, self.n)
+        self._check(self._lib.hidem_get_particles(self._ctx, C.byref(soa)))
+        return out
+
+    def get_links(self) -> dict:
+        out = abi.empty_links(self.L, self.precision)
+        soa = abi.link_soa(out, self.precision, self.L)
+        self._check(self._lib.hidem_get_links(self._ctx, C.byref(soa)))
+        return out
+
+    def get_forces(self) -> np.ndarray:
+        f = np.zeros((6, self.n), self.lp)
+        ptrs = (C.c_void_p * 6)(*[f[k].ctypes.data for k in range(6)])
+        self._check(self._lib.hidem_get_forces(self._ctx, ptrs))
+        return f
+
+    def get_cells(self):
+        ix = np.zeros(self.n, np.int32)
+        iy = np.zeros(self.n, np.int32)
+        iz = np.zeros(self.n, np.int32)
+        dims = (C.c_int64 * 3)()
+        mins = (C.c_double * 3)()
+        self._check(self._lib.hidem_get_cells(self._ctx, ix.ctypes.data, iy.ctypes.data,
+                                              iz.ctypes.data, dims, mins))
+        return ix, iy, iz, tuple(dims), tuple(mins)
+
+    def get_neighbours(self):
+        counts = np.zeros(self.n, np.int32)
+        total = C.c_int64()
+        self._check(self._lib.hidem_get_neighbours(self._ctx, counts.ctypes.data, None, 0,
+                                                   C.byref(total)))
+        lst = np.zeros(max(total.value, 1), np.int32)
+        self._check(self._lib.hidem_get_neighbours(self._ctx, counts.ctypes.data, lst.ctypes.data,
+                                                   lst.shape[0], C.byref(total)))
+        return counts, lst[: total.value]
+
+    def get_break_events(self, cap: int | None = None):
+        cap = self.L if cap is None else cap
+        li = np.zeros(max(cap, 1), np.int64)
+        st = np.zeros(max(cap, 1), np.int64)
+        cnt = C.c_int64()
+        self._check(self._lib.hidem_get_break_events(self._ctx, li.ctypes.data, st.ctypes.data,
+                                                     cap, C.byref(cnt)))
+        return li[: cnt.value], st[: cnt.value]
+
+    def stats(self) -> dict:
+        s = abi.HidemStats()
+        self._check(self._lib.hidem_get_stats(self._ctx, C.byref(s)))
+        return s.as_dict()

@@ -1,0 +1,123 @@
+"""Synthetic workloads: FCC ice blocks and slabs with distance-rule links.
+
+The reference's MeshBlock benchmark reads HDF5 point files (HiDEM/Benchmark/*/particles.h5)
+that cannot be read here, so seeded FCC lattices with the same density, particle size
+and link rule stand in for them. Generation runs in the library's host code
+(``hidem_lattice_fcc``, ``hidem_links_by_distance``).
+
+Parameter mapping of the named configurations (the reference keys they set):
+  d = 1 m, a = sqrt(2) d            lattice.particleRadius = 0.5, fccSpacing = sqrt(2)
+  bonds within 1.01 d               lattice.linkGenScale = 1.01 (PLiB/Generators/LinkGenerator.h:83-89)
+  E 1e9, rho 910, g 9.81            general.E / rhoIce / g
+  strain threshold 5e-4             general.maxLoad = 5e-4, bendBreak = 0.01, breakTime = 0
+  repulsion below d                 general.attractDistance = 0, attractScaleForce = 0
+  velocity damping 1e-3             general.damping = dampingRotation = 1e-3 * m / dt = 9100
+  friction coefficient 0.3          bed friction 0.3 in the GlacierDem bed drag (slab only)
+  cell size 1.2 d                   grid.searchDistanceScale = 1.2
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import abi
+
+SQRT2 = math.sqrt(2.0)
+
+
+def fcc_particles(nx: int, ny: int, nz: int, precision: int, a: float = SQRT2, radius: float = 0.5,
+                  origin=(0.0, 0.0, 0.0), jitter: float = 0.01, seed: int = 1) -> dict:
+    lib = abi.load()
+    n = 4 * nx * ny * nz
+    p = abi.empty_particles(n, precision)
+    soa = abi.particle_soa(p, precision, n)
+    org = (C.c_double * 3)(*origin)
+    st = lib.hidem_lattice_fcc(nx, ny, nz, a, radius, org, jitter, seed, precision, C.byref(soa))
+    if st != abi.HIDEM_OK:
+        raise abi.HidemError(st, "hidem_lattice_fcc failed")
+    return p
+
+
+def distance_links(p: dict, precision: int, scale: float = 1.01) -> dict:
+    lib = abi.load()
+    n = p["xCord"].shape[0]
+    soa = abi.particle_soa(p, precision, n)
+    cnt = C.c_int64()
+    st = lib.hidem_links_by_distance(C.byref(soa), n, precision, scale, None, 0, C.byref(cnt))
+    if st != abi.HIDEM_OK:
+        raise abi.HidemError(st, "hidem_links_by_distance (count) failed")
+    L = cnt.value
+    links = abi.empty_links(L, precision)
+    lsoa = abi.link_soa(links, precision, L)
+    st = lib.hidem_links_by_distance(C.byref(soa), n, precision, scale, C.byref(lsoa), L,
+                                     C.byref(cnt))
+    if st != abi.HIDEM_OK:
+        raise abi.HidemError(st, "hidem_links_by_distance failed")
+    return links
+
+
+def block_params(precision: int, **over) -> abi.HidemParams:
+    """Material and contact parameters of the ice-block configurations."""
+    dt = 1e-4
+    mass = 910.0 * 1.0 ** 3
+    base = dict(dt=dt, scale=1.0, E=1e9, rhoIce=910.0, g=9.81, maxLoad=5e-4, bendBreak=0.01,
+                breakTime=0.0, attractDistance=0.0, attractScaleForce=0.0,
+                damping=1e-3 * mass / dt, dampingRotation=1e-3 * mass / dt,
+                searchDistanceScale=1.2, maxRadius=0.5, waterLevel=-1.0e3, precision=precision)
+    base.update(over)
+    return abi.default_params(**base)
+
+
+def ice_block(cells=(20, 20, 20), precision: int = abi.PREC_MIXED, seed: int = 1,
+              jitter: float = 0.01, fixed_bottom: bool = True, **param_over):
+    """FCC block of cells^3 unit cells (config: 20x20x20 = 32,000 spheres), bonded within
+    1.01 d, bottom layer fixed, in air. Returns (params, particles, links)."""
+    nx, ny, nz = cells
+    p = fcc_particles(nx, ny, nz, precision, jitter=jitter, seed=seed)
+    if fixed_bottom:
+        z0 = p["zCord"].min()
+        p["type"][p["zCord"] < z0 + 0.25 * SQRT2] |= abi.TYPE_FIXED
+    links = distance_links(p, precision, 1.01)
+    params = block_params(precision, useFixed=1 if fixed_bottom else 0, **param_over)
+    return params, p, links
+
+
+def calving_slab(size=(400.0, 100.0, 100.0), precision: int = abi.PREC_MIXED, seed: int = 7,
+                 jitter: float = 0.01, broken_fraction: float = 0.01, water_level: float = 90.0,
+                 **param_over):
+    """FCC slab on a flat bed with a calving front on the x-max face, water line at
+    `water_level`, a seeded fraction of links pre-broken (config: 400 x 100 x 100 m,
+    ~5.7M particles, ~34M links)."""
+    nx, ny, nz = (max(1, int(round(s / SQRT2))) for s in size)
+    p = fcc_particles(nx, ny, nz, precision, jitter=jitter, seed=seed)
+    xmax = p["xCord"].max()
+    p["type"][p["xCord"] > xmax - 0.25 * SQRT2] |= abi.TYPE_FRONT
+    links = distance_links(p, precision, 1.01)
+    rng = np.random.default_rng(seed)
+    L = links["state"].shape[0]
+    k = int(round(broken_fraction * L))
+    if k:
+        links["state"][rng.choice(L, size=k, replace=False)] = 0
+    zmin = float(p["zCord"].min())
+    params = block_params(precision, waterLevel=water_level, useBed=1, bedHeight=zmin + 0.5,
+                          bedFriction=0.3, useFrontPressure=1, **param_over)
+    return params, p, links
+
+
+def algorithmic_bytes(n: int, L: int, pairs: int, precision: int) -> dict:
+    """Bytes per timestep of the byte model of the hot path: each particle's own fields
+    once, partner reads as cache hits (sp = 8, lp = ct = 4 mixed / 8 fp64):
+        N*(3sp+6lp+lp+6lp) force + N*(3sp+3lp+6lp+6lp+lp + 3sp+3lp+6lp) integrate
+        + S*(12ct+8) link ends + L*(2+lp+8) link break + C*4 contact list."""
+    sp = 8
+    lp = 4 if precision == abi.PREC_MIXED else 8
+    S = 2 * L
+    force = n * (3 * sp + 6 * lp + lp + 6 * lp)
+    integ = n * (3 * sp + 3 * lp + 6 * lp + 6 * lp + lp + 3 * sp + 3 * lp + 6 * lp)
+    sides = S * (12 * lp + 8)
+    brk = L * (2 + lp + 8)
+    pair = pairs * 4
+    total = force + integ + sides + brk + pair
+    return dict(force=force, integrate=integ, sides=sides, link_break=brk, pairs=pair, total=total)

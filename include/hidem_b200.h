@@ -1,0 +1,227 @@
+/*
+ * hidem_b200.h — C ABI of the B200-native HiDEM per-timestep hot path.
+ *
+ * One context owns one particle set and one link set resident in device
+ * memory of one GPU, one CUDA stream, and the neighbour / link acceleration
+ * structures.  Host arrays passed in or out are caller-owned and copied.
+ * Every entry point returns a hidem_status; none exits or raises signals
+ * (the reference's getErrorDev/exit(1) convention, Iterators/DevCall.h:29-91,
+ * becomes a status code plus hidem_last_error()).
+ *
+ * Layout contract (reference field order, HiDEMLib/HiDEMParticleData.h:45-51,
+ * HiDEMLib/HiDEMLinkData.h:39-50):
+ *   particles: xCord yCord zCord (f64) xTheta yTheta zTheta xDiff yDiff zDiff
+ *              uDiff vDiff wDiff radius (lp) owners (i32) type (u8) globalKeys (i64)
+ *   links:     owners (i32) state (u8) globalKeys globalKeyEndA globalKeyEndB (i64)
+ *              initialLen (lp) particleLinkNum (i32)
+ *   link sides: CT0..CT5 (ct), 2 values per link: [sideA(l0), sideB(l0), sideA(l1), ...]
+ *              (the checkpoint order, PLiB/LinkDataHandler.h:373-380,443-446)
+ * lp = ct = float in HIDEM_PREC_MIXED (the reference default build, FP64
+ * positions, PLiB/Global.h.in:47-52 with SET_FP32/SET_CT_FP32) and double in
+ * HIDEM_PREC_FP64 (the reference built with both flags off).
+ */
+#ifndef HIDEM_B200_H
+#define HIDEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HIDEM_B200_ABI_VERSION 1
+
+typedef enum hidem_status {
+    HIDEM_OK = 0,
+    HIDEM_ERR_ARG = 1,       /* null pointer, negative size, unknown enum value */
+    HIDEM_ERR_CUDA = 2,      /* a CUDA runtime call failed; see hidem_last_error */
+    HIDEM_ERR_STATE = 3,     /* call out of order (e.g. forces before particles) */
+    HIDEM_ERR_CAPACITY = 4,  /* a size exceeds a fixed limit (int32 indices, per-particle width) */
+    HIDEM_ERR_IO = 5,        /* checkpoint or run-config file error */
+    HIDEM_ERR_DEVICE = 6,    /* a device-side check failed (index out of range) */
+    HIDEM_ERR_NOT_FOUND = 7  /* a link end names a globalKey that is not a particle */
+} hidem_status;
+
+typedef enum hidem_precision {
+    HIDEM_PREC_FP64 = 0,  /* lp = ct = double */
+    HIDEM_PREC_MIXED = 1  /* lp = ct = float, positions double (reference default) */
+} hidem_precision;
+
+/* Bits of the particle `type` byte read by the integrate step (extensions of
+ * the sample integrate lambdas; the low bits keep the reference's material
+ * type used for link generation). */
+#define HIDEM_TYPE_FIXED 0x40u /* held in place: position and rotation unchanged, diffs zero */
+#define HIDEM_TYPE_FRONT 0x80u /* calving-front face: hydrostatic pressure below waterLevel */
+
+/* Raw run-config values (TOML keys general.*, grid.*, distribution.*; defaults
+ * from HiDEM/MeshBlock/MainMeshBlock.cpp:69-102 and HiDEMLib/HiDEMLib.h:714-750).
+ * Derived constants (scaled drags, invDt, W2, W4, G, ...) are computed inside
+ * the library in lp precision exactly as the sample main does. */
+typedef struct hidem_params {
+    double dt, scale, E, beamWidth, damping, dampingRotation;
+    double attractDistance, attractScaleForce;
+    double maxLoad, bendBreak, breakTime;
+    double g, rhoIce, rhoWater, waterLevel;
+    double airDrag, waterDrag, bedDrag, bedStiffness, bedInteract;
+    double maxVel, maxRot;
+    double lowerLimit[3], upperLimit[3];    /* simulation box for the boundary conditions */
+    int32_t boundaryMin[3], boundaryMax[3]; /* general.{x,y,z}Boundary{Min,Max} */
+    double searchDistanceScale;             /* grid.searchDistanceScale */
+    int32_t gridRegenInterval;              /* grid.gridRegenInterval (-1: displacement rule) */
+    int32_t firstBalanceTimestep;           /* distribution.firstBalanceTimestep (forces a rebuild) */
+    double maxRadius;                       /* largest particle radius (geometry.maxRadius) */
+    /* integrate extensions (off in the MeshBlock sample) */
+    int32_t useBed;                         /* flat bed: GlacierDem bed drag + stiffness (HiDEM/GlacierDem/MainDem.cpp:176-207) */
+    double bedHeight, bedFriction;
+    int32_t useVelocityLimit;               /* HiDEMDefVelocityLimit */
+    int32_t useBoundary;                    /* HiDEMDefBoundaryCondition */
+    int32_t useFixed;                       /* honour HIDEM_TYPE_FIXED */
+    int32_t useFrontPressure;               /* honour HIDEM_TYPE_FRONT */
+    int32_t precision;                      /* hidem_precision */
+} hidem_params;
+
+/* Particle arrays, reference field order. lp fields point at float (mixed) or
+ * double (fp64) arrays of n elements. Any pointer may be NULL on output calls
+ * to skip that field. */
+typedef struct hidem_particle_soa {
+    double *xCord, *yCord, *zCord;
+    void *xTheta, *yTheta, *zTheta;
+    void *xDiff, *yDiff, *zDiff, *uDiff, *vDiff, *wDiff;
+    void *radius;
+    int32_t *owners;
+    uint8_t *type;
+    int64_t *globalKeys;
+} hidem_particle_soa;
+
+/* Link arrays (L elements) plus side data CT0..CT5 (2L elements each). */
+typedef struct hidem_link_soa {
+    int32_t *owners;
+    uint8_t *state;
+    int64_t *globalKeys, *globalKeyEndA, *globalKeyEndB;
+    void *initialLen;
+    int32_t *particleLinkNum;
+    void *CT[6];
+} hidem_link_soa;
+
+typedef struct hidem_ctx hidem_ctx;
+
+/* Counters of what the last calls did (for logs and tests). */
+typedef struct hidem_stats {
+    int64_t step;              /* current timestep (HiDEMLib::currentTimestep) */
+    int64_t num_particles, num_links;
+    int64_t num_neighbour_pairs;   /* directed pairs in the contact list */
+    int64_t max_neighbours, max_links_per_particle;
+    int64_t grid_dims[3];
+    double grid_min[3];
+    int64_t regen_count;       /* neighbour-structure rebuilds so far */
+    int64_t last_regen_step;
+    double accumulated_dist;   /* HiDEMLib::accumulatedDist */
+    double search_distance, interact_distance;
+    int64_t broken_links;      /* links with state == 0 */
+    int64_t kernel_launches;   /* kernels launched by this context so far */
+} hidem_stats;
+
+/* ---- defaults -------------------------------------------------------- */
+
+/* MeshBlock sample defaults (HiDEM/MeshBlock/MainMeshBlock.cpp:69-102,
+ * HiDEMLib/HiDEMLib.h:714-750); extensions off; precision mixed. */
+void hidem_params_default(hidem_params *p);
+
+/* ---- context --------------------------------------------------------- */
+
+/* Replaces HiDEMLib::setup (HiDEMLib/HiDEMLib.h:707-822) for the hot path:
+ * selects `device`, creates the stream and the derived constants. */
+hidem_status hidem_create(const hidem_params *params, int device, hidem_ctx **out);
+void hidem_destroy(hidem_ctx *ctx);
+const char *hidem_last_error(const hidem_ctx *ctx);
+/* Per-thread text of the last hidem_create failure (ctx not yet available). */
+const char *hidem_create_error(void);
+int hidem_abi_version(void);
+
+/* Replaces ParticleDataHandler::appendInitParticles / fromCheckpoint
+ * (PLiB/ParticleDataHandler.h:215-267): copies n particles to the device. */
+hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, int64_t n);
+/* Replaces LinkDataHandler::appendInitLinks + LinkData::makeLocalPartEnds
+ * (PLiB/LinkDataHandler.h:212-241, PLiB/LinkData.h:91-115): copies L links,
+ * resolves their ends by globalKey, zeroes CT when `links->CT[0]` is NULL. */
+hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L);
+/* Sets the timestep counter (restart: HiDEMLib::setFromRestart, HiDEMLib.h:840-846). */
+hidem_status hidem_set_timestep(hidem_ctx *ctx, int64_t step);
+/* Replaces the per-config params after creation (same precision). */
+hidem_status hidem_set_params(hidem_ctx *ctx, const hidem_params *params);
+
+/* ---- the per-timestep operator surface (HiDEMLib.h:256-530) ---------- */
+
+/* HiDEMLib::gridService (HiDEMLib.h:533-628): displacement-accumulation rule,
+ * then, when due, cell binning + reorder, contact list and link lists. */
+hidem_status hidem_grid_service(hidem_ctx *ctx);
+/* Forces a rebuild now (CombinedAccel::generateNeighbours + generateLinks). */
+hidem_status hidem_regenerate(hidem_ctx *ctx);
+/* HiDEMLib::computePartForce with HiDEMDefNeighForceFunc + HiDEMDefLinkForceFunc
+ * (HiDEMLib.h:316-382, PLiB/Accel/CombinedAccel.h:122-197): writes the six
+ * force arrays and advances CT. */
+hidem_status hidem_compute_forces(hidem_ctx *ctx);
+/* HiDEMLib::applyForce with the sample integrate lambda
+ * (HiDEMLib.h:303-314, HiDEM/MeshBlock/MainMeshBlock.cpp:182-261). */
+hidem_status hidem_integrate(hidem_ctx *ctx);
+/* HiDEMLib::linkUpdate with HiDEMDefLinkBreakFunc (HiDEMLib.h:256-269,
+ * PLiB/Accel/CombinedAccel.h:200-235). Always applies the functor; the
+ * t*dt > breakTime gate of the sample main is the caller's (hidem_step applies it). */
+hidem_status hidem_link_update(hidem_ctx *ctx);
+/* HiDEMLib::finalizeTs (HiDEMLib.h:495-530): ++timestep. */
+hidem_status hidem_finalize_ts(hidem_ctx *ctx);
+/* n whole timesteps of the sample main loop (MainMeshBlock.cpp:274-323):
+ * gridService, forces, integrate, gated link update, finalizeTs — as one fused
+ * kernel per step, graph-launched between rebuild checks. */
+hidem_status hidem_step(hidem_ctx *ctx, int32_t nsteps);
+/* Blocks until the context's stream is idle; reports device-side check failures. */
+hidem_status hidem_synchronize(hidem_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work
+ * on it (e.g. CUDA events recorded on the same stream). */
+void *hidem_get_stream(hidem_ctx *ctx);
+
+/* ---- readback (input order: index i is the i-th particle / link given) -- */
+
+hidem_status hidem_get_particles(hidem_ctx *ctx, hidem_particle_soa *out);
+hidem_status hidem_get_links(hidem_ctx *ctx, hidem_link_soa *out);
+/* Six lp arrays (x,y,z,u,v,w) of the last hidem_compute_forces. */
+hidem_status hidem_get_forces(hidem_ctx *ctx, void *force[6]);
+/* Cell (ix,iy,iz) of each particle at the last rebuild, grid dims and minimum
+ * corner (NeighbourGrid::getGridId / generateNeighbourGrid, PLiB/NeighbourGrid.cpp:31-114). */
+hidem_status hidem_get_cells(hidem_ctx *ctx, int32_t *ix, int32_t *iy, int32_t *iz,
+                             int64_t dims[3], double mins[3]);
+/* Contact list of the last rebuild, in the reference's per-particle order
+ * (NeighAccel::generateNeighbours, PLiB/Accel/NeighAccel.h:25-137):
+ * counts[n] and, when `list` is not NULL, the neighbour input indices packed
+ * row after row (sum(counts) entries, at most `cap`). */
+hidem_status hidem_get_neighbours(hidem_ctx *ctx, int32_t *counts, int32_t *list, int64_t cap,
+                                  int64_t *total);
+/* Links broken since the last call: input link indices and the timestep at
+ * which each broke (HiDEMDefLinkBreakFunc decisions), at most `cap`. */
+hidem_status hidem_get_break_events(hidem_ctx *ctx, int64_t *link_index, int64_t *step,
+                                    int64_t cap, int64_t *count);
+hidem_status hidem_get_stats(hidem_ctx *ctx, hidem_stats *out);
+
+/* ---- lattice generation (setup-side inputs for the workloads) --------- */
+
+/* FCC lattice of nx*ny*nz unit cells, lattice constant a, radius r, origin o,
+ * each coordinate jittered by U(-jitter, +jitter) from a seeded 64-bit
+ * Mersenne Twister (std::mt19937_64). Sites in z, y, x, site order; globalKeys
+ * 0..n-1; thetas, diffs zero. Arrays must hold 4*nx*ny*nz elements. `lp` fields
+ * follow `precision`. */
+hidem_status hidem_lattice_fcc(int32_t nx, int32_t ny, int32_t nz, double a, double radius,
+                               const double origin[3], double jitter, uint64_t seed,
+                               int32_t precision, hidem_particle_soa *out);
+/* Distance-rule link generation (PLiB/Generators/LinkGenerator.h:60-110):
+ * every pair i<j (by globalKey) with |x_i - x_j| <= scale*(r_i + r_j) gets a
+ * link, ordered by (endA input index, endB input index), initialLen = |x_i-x_j|.
+ * With out==NULL only *count is written. */
+hidem_status hidem_links_by_distance(const hidem_particle_soa *p, int64_t n, int32_t precision,
+                                     double scale, hidem_link_soa *out, int64_t cap,
+                                     int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HIDEM_B200_H */

@@ -1,0 +1,141 @@
+"""ctypes bindings of the oracle libraries. TEST INFRASTRUCTURE ONLY.
+
+* ``libhidem_oracle.so`` — the plain-C restatement (oracle/hidem_oracle.c), always built.
+* ``_ref/libhidem_ref_{mixed,fp64}.so`` — the reference's own CPU hot path compiled from
+  its sources by oracle/Makefile (IEEE flags), when the reference tree was available at
+  build time; ``_ref/libhidem_ref_fast_*.so`` — the same with the reference's own
+  optimisation flags, used only to time the CPU baseline.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from hidem_b200 import abi
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "libhidem_oracle.so"
+REF_DIR = HERE / "_ref"
+
+_i64 = C.c_int64
+_P = C.POINTER
+
+
+def _bind(lib, prefix: str):
+    getattr(lib, prefix + "_cells").argtypes = [_P(abi.HidemParams), _P(abi.HidemParticleSoA), _i64,
+                                                C.c_void_p, C.c_void_p, C.c_void_p, _P(_i64),
+                                                _P(C.c_double)]
+    getattr(lib, prefix + "_neighbours").argtypes = [_P(abi.HidemParams), _P(abi.HidemParticleSoA),
+                                                     _i64, C.c_void_p, C.c_void_p, _i64, _P(_i64)]
+    getattr(lib, prefix + "_run").argtypes = [
+        _P(abi.HidemParams), _P(abi.HidemParticleSoA), _i64, _P(abi.HidemLinkSoA), _i64, _i64,
+        C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, _i64, _P(_i64), C.c_void_p, _i64, _P(_i64),
+        _P(C.c_double)]
+    for name in ("_cells", "_neighbours", "_run"):
+        getattr(lib, prefix + name).restype = C.c_int
+    getattr(lib, prefix + "_threads").restype = C.c_int
+    return lib
+
+
+class CpuPath:
+    """One CPU implementation of the hot path: the C restatement ('port') or the
+    reference's own code ('reference')."""
+
+    def __init__(self, path: Path, prefix: str, kind: str, precision: int | None = None):
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle)")
+        self.lib = _bind(C.CDLL(str(path)), prefix)
+        self.prefix = prefix
+        self.kind = kind
+        self.path = path
+        self.fixed_precision = precision
+
+    def threads(self) -> int:
+        return int(getattr(self.lib, self.prefix + "_threads")())
+
+    def _prec(self, params) -> int:
+        p = int(params.precision)
+        if self.fixed_precision is not None and p != self.fixed_precision:
+            raise ValueError(f"{self.path.name} is built for precision {self.fixed_precision}")
+        return p
+
+    def cells(self, params, particles: dict):
+        prec = self._prec(params)
+        n = particles["xCord"].shape[0]
+        soa = abi.particle_soa(particles, prec, n)
+        ix, iy, iz = (np.zeros(n, np.int32) for _ in range(3))
+        dims = (_i64 * 3)()
+        mins = (C.c_double * 3)()
+        rc = getattr(self.lib, self.prefix + "_cells")(C.byref(params), C.byref(soa), n,
+                                                       ix.ctypes.data, iy.ctypes.data,
+                                                       iz.ctypes.data, dims, mins)
+        if rc:
+            raise RuntimeError(f"{self.prefix}_cells -> {rc}")
+        return ix, iy, iz, tuple(dims), tuple(mins)
+
+    def neighbours(self, params, particles: dict):
+        prec = self._prec(params)
+        n = particles["xCord"].shape[0]
+        soa = abi.particle_soa(particles, prec, n)
+        counts = np.zeros(n, np.int32)
+        total = _i64()
+        f = getattr(self.lib, self.prefix + "_neighbours")
+        rc = f(C.byref(params), C.byref(soa), n, counts.ctypes.data, None, 0, C.byref(total))
+        if rc:
+            raise RuntimeError(f"{self.prefix}_neighbours -> {rc}")
+        lst = np.zeros(max(total.value, 1), np.int32)
+        rc = f(C.byref(params), C.byref(soa), n, counts.ctypes.data, lst.ctypes.data, lst.shape[0],
+               C.byref(total))
+        if rc:
+            raise RuntimeError(f"{self.prefix}_neighbours -> {rc}")
+        return counts, lst[: total.value]
+
+    def run(self, params, particles: dict, links: dict, nsteps: int, start_step: int = 0):
+        """Runs the timestep loop on copies of the inputs. Returns (particles, links,
+        forces[6,n] of the last step, events (link, step), regen steps, seconds)."""
+        prec = self._prec(params)
+        p = {k: v.copy() for k, v in particles.items()}
+        l = {k: v.copy() for k, v in links.items()}
+        n = p["xCord"].shape[0]
+        L = l["globalKeyEndA"].shape[0]
+        psoa = abi.particle_soa(p, prec, n)
+        lsoa = abi.link_soa(l, prec, L)
+        lp = abi.lp_dtype(prec)
+        F = np.zeros((6, n), lp)
+        fptr = (C.c_void_p * 6)(*[F[k].ctypes.data for k in range(6)])
+        cap = max(L, 1)
+        ev_l = np.zeros(cap, np.int64)
+        ev_s = np.zeros(cap, np.int64)
+        nev = _i64()
+        rcap = nsteps + 1
+        rg = np.zeros(rcap, np.int64)
+        nrg = _i64()
+        secs = C.c_double()
+        rc = getattr(self.lib, self.prefix + "_run")(
+            C.byref(params), C.byref(psoa), n, C.byref(lsoa), L, start_step, nsteps, fptr,
+            ev_l.ctypes.data, ev_s.ctypes.data, cap, C.byref(nev), rg.ctypes.data, rcap,
+            C.byref(nrg), C.byref(secs))
+        if rc:
+            raise RuntimeError(f"{self.prefix}_run -> {rc}")
+        k = min(nev.value, cap)
+        order = np.lexsort((ev_l[:k], ev_s[:k]))
+        events = np.stack([ev_l[:k][order], ev_s[:k][order]], axis=1)
+        return p, l, F, events, rg[: min(nrg.value, rcap)], secs.value
+
+
+def port() -> CpuPath:
+    return CpuPath(ORACLE_LIB, "hidem_oracle", "port")
+
+
+def reference(precision: int, fast: bool = False) -> CpuPath:
+    tag = ("fast_" if fast else "") + ("mixed" if precision == abi.PREC_MIXED else "fp64")
+    return CpuPath(REF_DIR / f"libhidem_ref_{tag}.so", "hidem_ref", "reference", precision)
+
+
+def reference_available(precision: int, fast: bool = False) -> bool:
+    tag = ("fast_" if fast else "") + ("mixed" if precision == abi.PREC_MIXED else "fp64")
+    return (REF_DIR / f"libhidem_ref_{tag}.so").exists()

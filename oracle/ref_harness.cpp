@@ -1,0 +1,493 @@
+// Oracle harness around the reference's own CPU hot path — TEST INFRASTRUCTURE ONLY.
+//
+// This file is compiled against the unmodified reference headers where they lie
+// (NeighbourGrid, NeighAccel, LinkAccelSide, CombinedAccel, LinkGenerator,
+// HiDEMDefaultFunctions, the particle/link data handlers) by oracle/Makefile, with
+// the project-written shims in oracle/refshim/ standing in for MPI, HDF5 and the
+// CMake-generated Global.h. The outputs go to oracle/_ref/ and are used only by the
+// tests, by __graft_entry__.smoke() and by bench.py's CPU reference arm. Nothing in
+// the product links or loads it.
+//
+// What is project code here (because the reference has it only inside HiDEMLib.h,
+// which needs toml11, or inside a sample main):
+//   * the derived constants of the sample main (HiDEM/MeshBlock/MainMeshBlock.cpp:106-156),
+//   * the integrate functor of the sample mains (MainMeshBlock.cpp:182-261 plus the
+//     GlacierDem bed terms HiDEM/GlacierDem/MainDem.cpp:176-207 and the project's
+//     fixed-layer / front-pressure extensions, identical in the product),
+//   * the gridService rebuild policy (HiDEMLib/HiDEMLib.h:533-628, 424-474),
+//   * the timestep loop order (MainMeshBlock.cpp:274-323).
+// Redistribution (HiDEMLib/HiDEMDistribution.h:99-198) only permutes storage on one
+// rank; the harness keeps the caller's order and performs the rebuild it triggers.
+//
+// Overload note: HiDEMDefaultFunctions.h calls unqualified sqrt() and abs() on lpReal_t.
+// The harness is built with -include math.h -include stdlib.h so that these resolve to
+// the float overloads (as in the reference's CUDA build, where device code sees CUDA's
+// float overloads). Without them, a g++ translation unit that includes the functor
+// header first (as MainMeshBlock.cpp does) binds abs(float) to int abs(int).
+
+#include <cassert>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <chrono>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "Global.h"
+#include "HiDEM/Common/HiDEMDefaultFunctions.h"
+#include "NeighbourGrid.h"
+#include "Accel/CombinedAccel.h"
+#include "Geometry/Map.h"
+#include "Generators/LinkGenerator.h"
+#include "HiDEMParticleData.h"
+#include "HiDEMLinkData.h"
+#include "ParticleDataHandler.h"
+#include "LinkDataHandler.h"
+
+#include "hidem_b200.h"
+
+using PData = ParticleDataHandler<HiDEMParticleData>;
+using LData = LinkDataHandler<HiDEMLinkData>;
+
+namespace {
+
+struct Derived {
+    // the sample main's locals, in its types (MainMeshBlock.cpp:69-156)
+    lpReal_t breakTime, dt, scale, beamWidth, E, waterLevel, attractDistance, attractScaleForce;
+    lpReal_t maxVel, maxRot, rhoWater, rhoIce, bedStiffness, bedInteract, waterDrag, airDrag, bedDrag;
+    lpReal_t g, damping, dampingRotation, maxLoad, bendBreak;
+    lpReal_t lift, invDt, invDt2, dtSqr, invDtSqr, G, W2, W4, scaleE;
+    lpReal_t bedHeight, bedFriction;
+    double searchDistance, interactDist;
+};
+
+Derived derive(const hidem_params &P) {
+    Derived d;
+    d.breakTime = P.breakTime;
+    d.dt = P.dt;
+    d.scale = P.scale;
+    d.beamWidth = P.beamWidth;
+    d.E = P.E;
+    d.waterLevel = P.waterLevel;
+    d.attractDistance = P.attractDistance;
+    d.attractScaleForce = P.attractScaleForce;
+    d.maxVel = P.maxVel;
+    d.maxRot = P.maxRot;
+    d.rhoWater = P.rhoWater;
+    d.rhoIce = P.rhoIce;
+    d.bedStiffness = P.bedStiffness;
+    d.bedInteract = P.bedInteract;
+    d.waterDrag = P.waterDrag;
+    d.airDrag = P.airDrag;
+    d.bedDrag = P.bedDrag;
+    d.g = P.g;
+    d.damping = P.damping;
+    d.dampingRotation = P.dampingRotation;
+    d.maxLoad = P.maxLoad;
+    d.bendBreak = P.bendBreak;
+    d.bedHeight = P.bedHeight;
+    d.bedFriction = P.bedFriction;
+
+    d.beamWidth *= d.scale;
+    d.bedInteract *= d.scale;
+    d.bedStiffness *= d.scale * d.scale;
+    d.waterDrag *= d.scale * d.scale;
+    d.airDrag *= d.scale * d.scale;
+    d.bedDrag *= d.scale * d.scale;
+    d.damping *= d.scale * d.scale;
+    d.dampingRotation *= d.scale * d.scale;
+    d.attractDistance *= d.scale;
+    d.lift = (d.rhoWater - d.rhoIce) / d.rhoIce * d.g;
+    d.invDt = 1.0 / d.dt;
+    d.invDt2 = 1.0 / (2.0 * d.dt);
+    d.dtSqr = pow(d.dt, 2.0);
+    d.invDtSqr = 1.0 / pow(d.dt, 2.0);
+    d.G = d.E / 2.0;
+    d.W2 = d.beamWidth * d.beamWidth;
+    d.W4 = d.beamWidth * d.beamWidth * d.beamWidth * d.beamWidth;
+    d.scaleE = d.E * d.scale;
+
+    lpReal_t maxRadius = P.maxRadius;
+    lpReal_t maxParticleDist = maxRadius * 2.0;  // HiDEMLib.h:759
+    d.searchDistance = P.searchDistanceScale * maxParticleDist;
+    d.interactDist = d.searchDistance - maxParticleDist;
+    return d;
+}
+
+template <class T>
+void copy_in(ManVec<T> &dst, const void *src, int64_t n) {
+    const T *s = static_cast<const T *>(src);
+    for (int64_t i = 0; i < n; ++i) dst[i] = s[i];
+}
+template <class T>
+void copy_out(void *dst, ManVec<T> &src, int64_t n) {
+    if (!dst) return;
+    T *d = static_cast<T *>(dst);
+    for (int64_t i = 0; i < n; ++i) d[i] = src[i];
+}
+
+PData *make_particles(const hidem_particle_soa *p, int64_t n) {
+    PData *pd = new PData();
+    pd->resize(n);
+    copy_in<hpReal_t>(pd->xCord, p->xCord, n);
+    copy_in<hpReal_t>(pd->yCord, p->yCord, n);
+    copy_in<hpReal_t>(pd->zCord, p->zCord, n);
+    copy_in<lpReal_t>(pd->xTheta, p->xTheta, n);
+    copy_in<lpReal_t>(pd->yTheta, p->yTheta, n);
+    copy_in<lpReal_t>(pd->zTheta, p->zTheta, n);
+    copy_in<lpReal_t>(pd->xDiff, p->xDiff, n);
+    copy_in<lpReal_t>(pd->yDiff, p->yDiff, n);
+    copy_in<lpReal_t>(pd->zDiff, p->zDiff, n);
+    copy_in<lpReal_t>(pd->uDiff, p->uDiff, n);
+    copy_in<lpReal_t>(pd->vDiff, p->vDiff, n);
+    copy_in<lpReal_t>(pd->wDiff, p->wDiff, n);
+    copy_in<lpReal_t>(pd->radius, p->radius, n);
+    for (int64_t i = 0; i < n; ++i) {
+        pd->owners[i] = 0;  // one rank owns everything
+        pd->type[i] = p->type ? p->type[i] : 0;
+        pd->globalKeys[i] = p->globalKeys ? p->globalKeys[i] : i;
+        pd->xForce[i] = pd->yForce[i] = pd->zForce[i] = 0;
+        pd->uForce[i] = pd->vForce[i] = pd->wForce[i] = 0;
+    }
+    pd->generateOnwedList();
+    return pd;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hidem_ref_precision(void) { return sizeof(lpReal_t) == 4 ? HIDEM_PREC_MIXED : HIDEM_PREC_FP64; }
+
+int hidem_ref_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+// Cell (ix,iy,iz) of every particle: NeighbourGrid::generate with the run's search
+// distance (PLiB/NeighbourGrid.cpp:48-161).
+int hidem_ref_cells(const hidem_params *P, const hidem_particle_soa *p, int64_t n, int32_t *ix,
+                    int32_t *iy, int32_t *iz, int64_t dims[3], double mins[3]) {
+    Derived d = derive(*P);
+    PData *pd = make_particles(p, n);
+    NeighbourGrid *grid = new NeighbourGrid();
+    grid->generate(*pd, d.searchDistance);
+    for (int64_t i = 0; i < n; ++i) {
+        auto [x, y, z] = grid->getCord((int)grid->colours[i]);
+        ix[i] = x;
+        iy[i] = y;
+        iz[i] = z;
+    }
+    dims[0] = grid->xGridSize;
+    dims[1] = grid->yGridSize;
+    dims[2] = grid->zGridSize;
+    mins[0] = grid->xMin;
+    mins[1] = grid->yMin;
+    mins[2] = grid->zMin;
+    delete grid;
+    delete pd;
+    return 0;
+}
+
+// Contact list: NeighAccel::generateNeighbours (PLiB/Accel/NeighAccel.h:25-137), rows
+// packed in the reference's per-particle order.
+int hidem_ref_neighbours(const hidem_params *P, const hidem_particle_soa *p, int64_t n,
+                         int32_t *counts, int32_t *list, int64_t cap, int64_t *total) {
+    Derived d = derive(*P);
+    PData *pd = make_particles(p, n);
+    CombinedAccel *accel = new CombinedAccel();
+    accel->grid.generate(*pd, d.searchDistance);
+    accel->nList.generateNeighbours(accel->grid, *pd, d.searchDistance, d.interactDist);
+    int64_t off = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        int c = accel->nList.numNeighs[i];
+        counts[i] = c;
+        for (int k = 0; k < c; ++k) {
+            if (list && off < cap) list[off] = accel->nList.getPartNeighId(k, (pInd_t)i);
+            ++off;
+        }
+    }
+    *total = off;
+    delete accel;
+    delete pd;
+    return (list && off > cap) ? HIDEM_ERR_CAPACITY : 0;
+}
+
+// LinkGenerator::generateLinksDistance with the given distance scale
+// (PLiB/Generators/LinkGenerator.h:30-37,60-181). Output order is the generator's
+// (thread-dependent); compare as a set.
+int hidem_ref_links(const hidem_particle_soa *p, int64_t n, double maxRadius, double scale,
+                    int64_t *keyA, int64_t *keyB, void *initialLen, int64_t cap, int64_t *count) {
+    PData *pd = make_particles(p, n);
+    for (int64_t i = 0; i < n; ++i) pd->type[i] = 0;
+    OffloadHashMap<gKey_t, pInd_t> mapper;
+    pd->remap(mapper);
+    LinkGenerator *gen = new LinkGenerator();
+    gen->setDistScale(scale);
+    ManVec<ElementaryLink> links = gen->generateLinksDistance(maxRadius, *pd);
+    *count = links.size();
+    for (size_t i = 0; i < links.size() && (int64_t)i < cap; ++i) {
+        keyA[i] = links[i].globalKeyParticleA;
+        keyB[i] = links[i].globalKeyParticleB;
+        static_cast<lpReal_t *>(initialLen)[i] = links[i].initialLen;
+    }
+    delete gen;
+    delete pd;
+    return (int64_t)links.size() > cap ? HIDEM_ERR_CAPACITY : 0;
+}
+
+// The timestep loop of the sample main over [start_step, start_step + nsteps).
+// Particles and links are updated in place (links: state and CT). force_out receives
+// the six force arrays of the last computePartForce. Break events record (link index,
+// step) of every link whose state went to 0; regen_steps the steps that rebuilt.
+int hidem_ref_run(const hidem_params *P, hidem_particle_soa *p, int64_t n, hidem_link_soa *l,
+                  int64_t L, int64_t start_step, int32_t nsteps, void *force_out[6],
+                  int64_t *ev_link, int64_t *ev_step, int64_t ev_cap, int64_t *ev_count,
+                  int64_t *regen_steps, int64_t regen_cap, int64_t *regen_count,
+                  double *seconds) {
+    const Derived d = derive(*P);
+    PData *pdp = make_particles(p, n);
+    PData &pData = *pdp;
+    OffloadHashMap<gKey_t, pInd_t> pMapper;
+    pData.remap(pMapper);
+
+    LData *ldp = new LData();
+    LData &lData = *ldp;
+    {
+        ManVec<ElementaryLink> links;
+        links.resize(L);
+        const lpReal_t *L0 = static_cast<const lpReal_t *>(l->initialLen);
+        for (int64_t i = 0; i < L; ++i) {
+            ElementaryLink e;
+            e.globalKey = l->globalKeys ? l->globalKeys[i] : i;
+            e.globalKeyParticleA = l->globalKeyEndA[i];
+            e.globalKeyParticleB = l->globalKeyEndB[i];
+            e.particleLinkNum = l->particleLinkNum ? l->particleLinkNum[i] : 0;
+            e.owner = 0;
+            e.initialLen = L0[i];
+            e.state = l->state[i];
+            links[i] = e;
+        }
+        lData.appendInitLinks(links);
+    }
+    if (l->CT[0]) {
+        ManVec<ctReal_t> *ct[6] = {&lData.CT0_flat, &lData.CT1_flat, &lData.CT2_flat,
+                                   &lData.CT3_flat, &lData.CT4_flat, &lData.CT5_flat};
+        for (int k = 0; k < 6; ++k) copy_in<ctReal_t>(*ct[k], l->CT[k], 2 * L);
+    }
+    lData.makeLocalPartEnds(pMapper);
+
+    CombinedAccel *accelp = new CombinedAccel();
+    CombinedAccel &accel = *accelp;
+
+    // integrate functor: sample integrate lambda (MainMeshBlock.cpp:182-261) with the
+    // GlacierDem bed terms (MainDem.cpp:176-207) and the fixed / front extensions.
+    const Real3 lowerLimit(P->lowerLimit[0], P->lowerLimit[1], P->lowerLimit[2]);
+    const Real3 upperLimit(P->upperLimit[0], P->upperLimit[1], P->upperLimit[2]);
+    const bool useBed = P->useBed, useVel = P->useVelocityLimit, useBnd = P->useBoundary;
+    const bool useFixed = P->useFixed, useFront = P->useFrontPressure;
+    const bool bMinX = P->boundaryMin[0], bMinY = P->boundaryMin[1], bMinZ = P->boundaryMin[2];
+    const bool bMaxX = P->boundaryMax[0], bMaxY = P->boundaryMax[1], bMaxZ = P->boundaryMax[2];
+    auto integrate = [=](pInd_t pInd, PData &pd) {
+        const uint8_t type = pd.type[pInd];
+        if (useFixed && (type & HIDEM_TYPE_FIXED)) {
+            pd.xDiff[pInd] = 0;
+            pd.yDiff[pInd] = 0;
+            pd.zDiff[pInd] = 0;
+            pd.uDiff[pInd] = 0;
+            pd.vDiff[pInd] = 0;
+            pd.wDiff[pInd] = 0;
+            return;
+        }
+        hpReal_t xCord = pd.xCord[pInd], yCord = pd.yCord[pInd], zCord = pd.zCord[pInd];
+        hpReal_t xCordPrev = 0, yCordPrev = 0, zCordPrev = 0;
+        lpReal_t xDiff = pd.xDiff[pInd], yDiff = pd.yDiff[pInd], zDiff = pd.zDiff[pInd];
+        lpReal_t xTheta = pd.xTheta[pInd], yTheta = pd.yTheta[pInd], zTheta = pd.zTheta[pInd];
+        lpReal_t xThetaPrev = 0, yThetaPrev = 0, zThetaPrev = 0;
+        lpReal_t uDiff = pd.uDiff[pInd], vDiff = pd.vDiff[pInd], wDiff = pd.wDiff[pInd];
+        lpReal_t radius = pd.radius[pInd];
+        lpReal_t diameter = radius * lpReal_t(2.0);
+
+        lpReal_t dragCoeff;
+        if (useBed && (zCord + radius) - d.bedHeight < d.bedInteract) {
+            dragCoeff = std::min(d.bedDrag * d.bedFriction, lpReal_t(1e+5) * d.scale * d.scale);
+        } else if (zCord > d.waterLevel) {
+            dragCoeff = d.airDrag;
+        } else {
+            dragCoeff = d.waterDrag;
+        }
+        lpReal_t xForce = pd.xForce[pInd], yForce = pd.yForce[pInd], zForce = pd.zForce[pInd];
+        lpReal_t uForce = pd.uForce[pInd], vForce = pd.vForce[pInd], wForce = pd.wForce[pInd];
+
+        lpReal_t particleMass = d.rhoIce * diameter * diameter * diameter;
+        lpReal_t particleMomentInertia = particleMass * diameter * diameter / lpReal_t(6.0);
+
+        if (zCord > d.waterLevel) zForce += -d.g * particleMass;
+        if (zCord <= d.waterLevel) zForce += d.lift * particleMass;
+        if (useBed && zCord + radius < d.bedHeight)
+            zForce += d.bedStiffness * (d.bedHeight - (zCord + radius));
+        if (useFront && (type & HIDEM_TYPE_FRONT) && zCord < d.waterLevel) {
+            lpReal_t depth = (lpReal_t)(d.waterLevel - zCord);
+            xForce -= d.rhoWater * d.g * depth * diameter * diameter;
+        }
+
+        auto vel = HiDEMDefTimeIntegration(dragCoeff, d.invDt2, particleMass, d.invDtSqr, d.dtSqr,
+                                           particleMomentInertia, d.invDt,
+                                           xForce, xDiff, xCord, xCordPrev,
+                                           yForce, yDiff, yCord, yCordPrev,
+                                           zForce, zDiff, zCord, zCordPrev,
+                                           uForce, uDiff, xTheta, xThetaPrev,
+                                           vForce, vDiff, yTheta, yThetaPrev,
+                                           wForce, wDiff, zTheta, zThetaPrev);
+        if (useVel) {
+            auto [xVel, yVel, zVel, xThetaVel, yThetaVel, zThetaVel] = vel;
+            HiDEMDefVelocityLimit(d.maxVel, d.maxRot, d.dt,
+                                  xVel, xCord, xCordPrev, yVel, yCord, yCordPrev,
+                                  zVel, zCord, zCordPrev,
+                                  xThetaVel, xTheta, xThetaPrev, yThetaVel, yTheta, yThetaPrev,
+                                  zThetaVel, zTheta, zThetaPrev);
+        }
+        if (useBnd) {
+            HiDEMDefBoundaryCondition(radius, lowerLimit, upperLimit, bMinX, bMaxX, bMinY, bMaxY,
+                                      bMinZ, bMaxZ, xCord, xCordPrev, yCord, yCordPrev, zCord,
+                                      zCordPrev);
+        }
+        pd.xCord[pInd] = xCord;
+        pd.yCord[pInd] = yCord;
+        pd.zCord[pInd] = zCord;
+        pd.xTheta[pInd] = xTheta;
+        pd.yTheta[pInd] = yTheta;
+        pd.zTheta[pInd] = zTheta;
+        pd.xDiff[pInd] = static_cast<lpReal_t>(xCord - xCordPrev);
+        pd.yDiff[pInd] = static_cast<lpReal_t>(yCord - yCordPrev);
+        pd.zDiff[pInd] = static_cast<lpReal_t>(zCord - zCordPrev);
+        pd.uDiff[pInd] = xTheta - xThetaPrev;
+        pd.vDiff[pInd] = yTheta - yThetaPrev;
+        pd.wDiff[pInd] = zTheta - zThetaPrev;
+    };
+
+    HiDEMDefNeighForceFunc nFunc(d.invDt, d.attractDistance, d.attractScaleForce, d.damping,
+                                 d.dampingRotation, d.scaleE);
+    HiDEMDefLinkForceFunc lFunc(d.invDt, d.damping, d.dampingRotation, d.E, d.W2, d.W4, d.G);
+    HiDEMDefLinkBreakFunc bFunc(d.bendBreak, d.maxLoad);
+
+    double accumulatedDist = 0;
+    int64_t nev = 0, nregen = 0;
+    std::vector<uint8_t> before(L);
+    auto t0 = std::chrono::steady_clock::now();
+
+    for (int64_t t = start_step; t < start_step + nsteps; ++t) {
+        // gridService (HiDEMLib.h:533-628) on one rank
+        bool regen = (t == start_step);
+        if (P->gridRegenInterval != -1) {
+            regen = (t % P->gridRegenInterval) == 0;
+        } else if (t % 10 == 0) {
+            // accumulateDist / getMaxDistOwned (HiDEMLib.h:424-474)
+            double mx = 0.0, my = 0.0, mz = 0.0;
+            for (int64_t i = 0; i < n; ++i) {
+                double a = pData.xDiff[i], b = pData.yDiff[i], c = pData.zDiff[i];
+                if (a > mx) mx = a;
+                if (b > my) my = b;
+                if (c > mz) mz = c;
+            }
+            lpReal_t xM = mx, yM = my, zM = mz;
+            double currDist = 10 * std::sqrt((xM * xM) + (yM * yM) + (zM * zM));
+            accumulatedDist += currDist;
+            if (accumulatedDist >= d.interactDist / 2.0) regen = true;
+        }
+        if (t == P->firstBalanceTimestep) regen = true;
+        if (regen) {
+            accumulatedDist = 0;
+            accel.generateNeighbours(pData, lData, d.searchDistance, d.interactDist);
+            accel.generateLinks(pData, lData, d.searchDistance, d.interactDist);
+            accel.lAccel.sortSideData(pData, lData);
+            accel.generateIndexes(pData, lData, d.searchDistance, d.interactDist);
+            if (regen_steps && nregen < regen_cap) regen_steps[nregen] = t;
+            ++nregen;
+        }
+
+        // computePartForce (HiDEMLib.h:316-382) -> CombinedAccel::iterateCombined
+        auto fullArgs = make4Pack(
+            packVecPtrs(pData.xDiff, pData.yDiff, pData.zDiff, pData.uDiff, pData.vDiff,
+                        pData.wDiff, pData.radius),
+            packVecPtrs(),
+            packVecPtrs(lData.CT0_flat, lData.CT1_flat, lData.CT2_flat, lData.CT3_flat,
+                        lData.CT4_flat, lData.CT5_flat),
+            packVecPtrs(pData.xForce, pData.yForce, pData.zForce, pData.uForce, pData.vForce,
+                        pData.wForce));
+        accel.iterateCombinedPre(OffloadExec(), pData, lData, nFunc, lFunc, fullArgs);
+        Iterator::syncAll();
+
+        // applyForce (HiDEMLib.h:303-314)
+        pData.iterateAllParticles(OffloadExec(), integrate, pData);
+        Iterator::syncAll();
+
+        // linkUpdate, gated as in MainMeshBlock.cpp:312
+        if ((lpReal_t)(t * d.dt) > d.breakTime) {
+            for (int64_t i = 0; i < L; ++i) before[i] = lData.state[i];
+            accel.iterateLinks(OffloadExec(), pData, lData, bFunc,
+                               make3Pack(packVecPtrs(pData.xCord, pData.yCord, pData.zCord,
+                                                     pData.xTheta, pData.yTheta, pData.zTheta),
+                                         packVecPtrs(), packVecPtrs(lData.state, lData.initialLen)));
+            Iterator::syncAll();
+            for (int64_t i = 0; i < L; ++i) {
+                if (before[i] != 0 && lData.state[i] == 0) {
+                    if (nev < ev_cap) {
+                        ev_link[nev] = i;
+                        ev_step[nev] = t;
+                    }
+                    ++nev;
+                }
+            }
+        }
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (ev_count) *ev_count = nev;
+    if (regen_count) *regen_count = nregen;
+
+    // write back
+    copy_out<hpReal_t>(p->xCord, pData.xCord, n);
+    copy_out<hpReal_t>(p->yCord, pData.yCord, n);
+    copy_out<hpReal_t>(p->zCord, pData.zCord, n);
+    copy_out<lpReal_t>(p->xTheta, pData.xTheta, n);
+    copy_out<lpReal_t>(p->yTheta, pData.yTheta, n);
+    copy_out<lpReal_t>(p->zTheta, pData.zTheta, n);
+    copy_out<lpReal_t>(p->xDiff, pData.xDiff, n);
+    copy_out<lpReal_t>(p->yDiff, pData.yDiff, n);
+    copy_out<lpReal_t>(p->zDiff, pData.zDiff, n);
+    copy_out<lpReal_t>(p->uDiff, pData.uDiff, n);
+    copy_out<lpReal_t>(p->vDiff, pData.vDiff, n);
+    copy_out<lpReal_t>(p->wDiff, pData.wDiff, n);
+    if (force_out) {
+        copy_out<lpReal_t>(force_out[0], pData.xForce, n);
+        copy_out<lpReal_t>(force_out[1], pData.yForce, n);
+        copy_out<lpReal_t>(force_out[2], pData.zForce, n);
+        copy_out<lpReal_t>(force_out[3], pData.uForce, n);
+        copy_out<lpReal_t>(force_out[4], pData.vForce, n);
+        copy_out<lpReal_t>(force_out[5], pData.wForce, n);
+    }
+    for (int64_t i = 0; i < L; ++i) l->state[i] = lData.state[i];
+    if (l->CT[0]) {
+        ManVec<ctReal_t> *ct[6] = {&lData.CT0_flat, &lData.CT1_flat, &lData.CT2_flat,
+                                   &lData.CT3_flat, &lData.CT4_flat, &lData.CT5_flat};
+        for (int k = 0; k < 6; ++k) {
+            ctReal_t *dst = static_cast<ctReal_t *>(l->CT[k]);
+            for (int64_t i = 0; i < L; ++i) {
+                dst[2 * i] = (*ct[k])[lData.sideIndEndA[i]];
+                dst[2 * i + 1] = (*ct[k])[lData.sideIndEndB[i]];
+            }
+        }
+    }
+    delete accelp;
+    delete ldp;
+    delete pdp;
+    return 0;
+}
+
+}  // extern "C"
