@@ -1,0 +1,330 @@
+"""Benchmark of the HiDEM hot path: particle-steps/s on the 5.7M-particle calving slab.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+                    [--impl ours|reference] [--workload slab|block]
+
+A "step" is one timestep of the sample main loop (gridService, forces, integrate, link
+update) over the whole slab. `value` times K steps with the state resident in HBM (CUDA
+events on the library's stream, max over ranks). `e2e` times the same K steps through the
+C ABI from host arrays: upload of the particle and link state, the K steps, download of
+the particle state. `roofline` divides the byte model of the step by the fused step
+kernel's event-timed duration. `cpu_baseline` times the reference's own CPU path
+(oracle/_ref, built from its sources with its own flags) on the same slab.
+With --gpus N > 1 (torchrun) every rank advances its own replica of the slab (the path
+has no exchange on one node for this workload; weak scaling).
+--impl reference times the reference's CPU implementation on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+# best published single-device figure for this metric (mixed, 5.7M MeshBlock slab,
+# RTX 5090, HiDEM/Docs/Performance.md:68): 5,723,826 particles x 5000 steps / 25.83 s
+PUBLISHED_MIXED = 5723826 * 5000 / 25.83
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["slab", "block"], default="slab")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_workload(args):
+    from hidem_b200 import abi, workloads
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    if args.workload == "slab":
+        P, p, l = workloads.calving_slab(precision=prec, jitter=0.0)
+        name = "calving slab 400x100x100 m FCC d=1 m (283x71x71 cells), bed, water 90 m, 1% pre-broken"
+    else:
+        P, p, l = workloads.ice_block(cells=(20, 20, 20), precision=prec)
+        name = "ice block 20^3 FCC cells, jitter 0.01 d, bottom fixed"
+    return prec, P, p, l, name
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(precision: str):
+    """DRAM bytes per particle-step of the fused step kernel from the committed ncu
+    summary (profiles/fused_step_*.md, line `dram_bytes_per_particle_step: X`)."""
+    f = ROOT / "profiles" / f"fused_step_slab_{precision}.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.strip().startswith("dram_bytes_per_particle_step:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(P, p, l, n):
+    """The reference's CPU path (oracle/_ref fast build, all host threads) on a bounded
+    sample of the same workload: a few timesteps of the whole slab after one warm-up."""
+    from oracle import oracle
+    if oracle.reference_available(int(P.precision), fast=True):
+        sess = oracle.RefSession(P, p, l, fast=True)
+        kind = "reference"
+        cores = sess.threads()
+        t1 = sess.advance(1)  # warm-up (includes nothing of the setup)
+        k = int(max(1, min(10, 15.0 / max(t1, 1e-3))))
+        secs = sess.advance(k)
+        sess.close()
+        return {"value": n * k / secs, "unit": "particle-steps/s", "cores": cores, "kind": kind,
+                "sample": f"{k} timesteps of the full workload ({n} particles) after 1 warm-up step, "
+                          f"reference CPU path built with -O3 -ffast-math -march=x86-64-v3 -fopenmp"}
+    port = oracle.port()
+    _, _, _, _, _, secs = port.run(P, p, l, 3)
+    return {"value": n * 3 / secs, "unit": "particle-steps/s", "cores": port.threads(),
+            "kind": "port", "sample": f"3 timesteps of the full workload ({n} particles)"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation, K timed steps after W warm-up."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle
+    prec, P, p, l, name = make_workload(args)
+    n = p["xCord"].shape[0]
+    fast_ok = oracle.reference_available(prec, fast=True)
+    sess = oracle.RefSession(P, p, l, fast=True) if fast_ok else None
+    if sess is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+        return
+    sess.advance(max(args.warmup, 1))
+    secs = sess.advance(args.steps)
+    cores = sess.threads()
+    sess.close()
+    value = n * args.steps / secs
+    line = {
+        "metric": "particle-steps/s (5.7M slab)" if args.workload == "slab" else "particle-steps/s (32k block)",
+        "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64pos" if prec == 1 else "f64", "data": "synthetic",
+        "config": {"workload": name, "particles": n, "links": int(l["state"].shape[0]),
+                   "precision": args.precision},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{args.steps} timesteps of the full workload after {max(args.warmup, 1)} warm-up"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    from hidem_b200 import abi, workloads
+    from hidem_b200.hidemlib import HiDEMLib
+
+    prec, P, p, l, name = make_workload(args)
+    n = p["xCord"].shape[0]
+    L = l["state"].shape[0]
+
+    lib = HiDEMLib(P, device=local)
+    lib.set_particles(p)
+    lib.set_links(l)
+    stream = torch.cuda.ExternalStream(lib.stream_handle)
+    lib.step(args.warmup)
+    lib.synchronize()
+    st0 = lib.stats()
+    pairs = st0["num_neighbour_pairs"]
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    lib.profile(True)
+    e0.record(stream)
+    lib.step(args.steps)
+    e1.record(stream)
+    lib.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    kern_ms, kern_n = lib.profile_read()
+    lib.profile(False)
+    clk = clocks.stop()
+    st1 = lib.stats()
+    launches = int(st1["kernel_launches"] - st0["kernel_launches"])
+    if pg:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    lib.close()
+
+    value = world * n * args.steps / (ms / 1e3)
+    bytes_step = workloads.algorithmic_bytes(n, L, pairs, prec)["total"]
+    kern_avg_s = (kern_ms / max(kern_n, 1)) / 1e3
+    peak, peak_kind = measured_peak()
+    achieved = bytes_step / kern_avg_s / 1e9
+    dpps = profile_traffic(args.precision)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": (dpps * n) if dpps else None,
+                "peak_source": peak_kind, "kernel": "k_step<fused>",
+                "kernel_ms": kern_ms / max(kern_n, 1),
+                "algorithmic_bytes_per_launch": bytes_step}
+
+    e2e = None
+    if not args.no_e2e:
+        # the same K steps through the C ABI from host buffers (state upload, K steps,
+        # particle state download)
+        lib2 = HiDEMLib(P, device=local)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        lib2.set_particles(p)
+        lib2.set_links(l)
+        lib2.step(args.steps)
+        outp = lib2.get_particles()
+        lib2.synchronize()
+        t1 = time.perf_counter()
+        el = t1 - t0
+        if pg:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            el = float(t.item())
+        lib2.close()
+        h2d = sum(v.nbytes for v in p.values()) + sum(v.nbytes for v in l.values())
+        d2h = sum(v.nbytes for v in outp.values())
+        e2e = {"value": world * n * args.steps / el, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "step": f"one C-ABI job: upload state, {args.steps} timesteps, download particles"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(P, p, l, n)
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
+                   "sample": f"failed: {ex}"}
+
+    if pg:
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "particle-steps/s (5.7M slab)" if args.workload == "slab" else "particle-steps/s (32k block)",
+        "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": (value / PUBLISHED_MIXED) if (prec == abi.PREC_MIXED and args.workload == "slab") else None,
+        "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
+        "config": {"workload": name, "particles": n, "links": L, "contact_pairs": pairs,
+                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (records + link ends > 126 MB)",
+                   "baseline_number": "RTX 5090 1.108e9 particle-steps/s, HiDEM/Docs/Performance.md:68"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -190,6 +190,8 @@ _PROTOS = [
     ("hidem_step", C.c_int, [C.c_void_p, C.c_int32]),
     ("hidem_synchronize", C.c_int, [C.c_void_p]),
     ("hidem_get_stream", C.c_void_p, [C.c_void_p]),
+    ("hidem_profile", C.c_int, [C.c_void_p, C.c_int32]),
+    ("hidem_profile_read", C.c_int, [C.c_void_p, C.POINTER(_d), C.POINTER(_i64)]),
     ("hidem_get_particles", C.c_int, [C.c_void_p, C.POINTER(HidemParticleSoA)]),
     ("hidem_get_links", C.c_int, [C.c_void_p, C.POINTER(HidemLinkSoA)]),
     ("hidem_get_forces", C.c_int, [C.c_void_p, C.c_void_p * 6]),

@@ -93,6 +93,11 @@ struct hidem_ctx {
     unsigned long long *diffMax = nullptr;
     int *errorFlag = nullptr;
 
+    // optional CUDA-event timing of the fused step kernel (pairs recorded around launches)
+    bool profile = false;
+    std::vector<cudaEvent_t> evPool;
+    size_t evUsed = 0;
+
     double accumulatedDist = 0;
     long long regenCount = 0, lastRegen = -1;
     long long launches = 0;
@@ -554,6 +559,18 @@ hidem_status link_update_now(hidem_ctx *ctx, long long tagStep) {
     return HIDEM_OK;
 }
 
+hidem_status profile_pair(hidem_ctx *ctx, cudaEvent_t *e0, cudaEvent_t *e1) {
+    while (ctx->evPool.size() < ctx->evUsed + 2) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        ctx->evPool.push_back(e);
+    }
+    *e0 = ctx->evPool[ctx->evUsed];
+    *e1 = ctx->evPool[ctx->evUsed + 1];
+    ctx->evUsed += 2;
+    return HIDEM_OK;
+}
+
 // n whole timesteps, one fused kernel each (MainMeshBlock.cpp:274-323).
 template <class LP>
 hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
@@ -577,7 +594,11 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
             CK(cudaMemsetAsync(ctx->diffMax, 0, 3 * sizeof(unsigned long long), ctx->stream));
             diffReady = true;
         }
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (ctx->profile) TRY(profile_pair(ctx, &e0, &e1));
+        if (e0) CK(cudaEventRecord(e0, ctx->stream));
         launch_step<LP>(consts<LP>(ctx), a, true, ctx->stream);
+        if (e1) CK(cudaEventRecord(e1, ctx->stream));
         ctx->launches += 1;
         ctx->cur = 1 - ctx->cur;  // the slot order (type / orig / cellOf) is unchanged
         pending = break_active<LP>(ctx, t);
@@ -723,6 +744,7 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->eventCount);
     dfree(ctx->diffMax);
     dfree(ctx->errorFlag);
+    for (cudaEvent_t e : ctx->evPool) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -998,6 +1020,27 @@ hidem_status hidem_synchronize(hidem_ctx *ctx) {
 }
 
 void *hidem_get_stream(hidem_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+hidem_status hidem_profile(hidem_ctx *ctx, int32_t enable) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    ctx->profile = enable != 0;
+    ctx->evUsed = 0;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_profile_read(hidem_ctx *ctx, double *step_kernel_ms, int64_t *launches) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    double total = 0;
+    for (size_t k = 0; k + 1 < ctx->evUsed; k += 2) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->evPool[k], ctx->evPool[k + 1]));
+        total += ms;
+    }
+    if (step_kernel_ms) *step_kernel_ms = total;
+    if (launches) *launches = (int64_t)(ctx->evUsed / 2);
+    return HIDEM_OK;
+}
 
 hidem_status hidem_get_particles(hidem_ctx *ctx, hidem_particle_soa *out) {
     if (!ctx || !out) return HIDEM_ERR_ARG;

@@ -124,6 +124,16 @@ class HiDEMLib:
     def step(self, nsteps: int = 1) -> None:
         self._check(self._lib.hidem_step(self._ctx, int(nsteps)))
 
+    def profile(self, enable: bool = True) -> None:
+        """CUDA-event timing of the fused step kernel on the context's stream."""
+        self._check(self._lib.hidem_profile(self._ctx, 1 if enable else 0))
+
+    def profile_read(self) -> tuple[float, int]:
+        ms = C.c_double()
+        n = C.c_int64()
+        self._check(self._lib.hidem_profile_read(self._ctx, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
     def synchronize(self) -> None:
         self._check(self._lib.hidem_synchronize(self._ctx))
 

@@ -180,6 +180,10 @@ hidem_status hidem_synchronize(hidem_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work
  * on it (e.g. CUDA events recorded on the same stream). */
 void *hidem_get_stream(hidem_ctx *ctx);
+/* Turns CUDA-event timing of the fused step kernel on (1) or off (0) and clears the
+ * record; hidem_profile_read sums the kernel time of the launches since then. */
+hidem_status hidem_profile(hidem_ctx *ctx, int32_t enable);
+hidem_status hidem_profile_read(hidem_ctx *ctx, double *step_kernel_ms, int64_t *launches);
 
 /* ---- readback (input order: index i is the i-th particle / link given) -- */
 

@@ -516,6 +516,7 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
             if (regen_steps && nregen < regen_cap) regen_steps[nregen] = t;
             ++nregen;
         }
+        if (t == start_step) clock_gettime(CLOCK_MONOTONIC, &t0); /* time excludes the first rebuild */
 
         /* ---- computePartForce: CombinedAccel::iterateCombined
          *      (PLiB/Accel/CombinedAccel.h:122-197) ---- */

@@ -139,3 +139,51 @@ def reference(precision: int, fast: bool = False) -> CpuPath:
 def reference_available(precision: int, fast: bool = False) -> bool:
     tag = ("fast_" if fast else "") + ("mixed" if precision == abi.PREC_MIXED else "fp64")
     return (REF_DIR / f"libhidem_ref_{tag}.so").exists()
+
+
+class RefSession:
+    """A persistent run of the reference's CPU timestep loop (oracle/_ref), so steps can be
+    timed without its setup: ``advance(k)`` returns the seconds of k timesteps, excluding
+    the rebuild of the first one."""
+
+    def __init__(self, params, particles: dict, links: dict, fast: bool = True, start_step: int = 0):
+        prec = int(params.precision)
+        tag = ("fast_" if fast else "") + ("mixed" if prec == abi.PREC_MIXED else "fp64")
+        path = REF_DIR / f"libhidem_ref_{tag}.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle)")
+        lib = C.CDLL(str(path))
+        lib.hidem_ref_open.restype = C.c_void_p
+        lib.hidem_ref_open.argtypes = [_P(abi.HidemParams), _P(abi.HidemParticleSoA), _i64,
+                                       _P(abi.HidemLinkSoA), _i64, _i64]
+        lib.hidem_ref_advance.restype = C.c_int
+        lib.hidem_ref_advance.argtypes = [C.c_void_p, C.c_int32, _P(C.c_double)]
+        lib.hidem_ref_close.argtypes = [C.c_void_p]
+        lib.hidem_ref_threads.restype = C.c_int
+        self.lib = lib
+        self.path = path
+        self.params = params
+        n = particles["xCord"].shape[0]
+        L = links["globalKeyEndA"].shape[0]
+        psoa = abi.particle_soa(particles, prec, n)
+        lsoa = abi.link_soa(links, prec, L)
+        self.n = n
+        self.h = lib.hidem_ref_open(C.byref(params), C.byref(psoa), n, C.byref(lsoa), L, start_step)
+
+    def threads(self) -> int:
+        return int(self.lib.hidem_ref_threads())
+
+    def advance(self, nsteps: int) -> float:
+        secs = C.c_double()
+        rc = self.lib.hidem_ref_advance(self.h, nsteps, C.byref(secs))
+        if rc:
+            raise RuntimeError(f"hidem_ref_advance -> {rc}")
+        return secs.value
+
+    def close(self):
+        if self.h:
+            self.lib.hidem_ref_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

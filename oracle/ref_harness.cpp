@@ -241,151 +241,73 @@ int hidem_ref_links(const hidem_particle_soa *p, int64_t n, double maxRadius, do
     return (int64_t)links.size() > cap ? HIDEM_ERR_CAPACITY : 0;
 }
 
-// The timestep loop of the sample main over [start_step, start_step + nsteps).
-// Particles and links are updated in place (links: state and CT). force_out receives
-// the six force arrays of the last computePartForce. Break events record (link index,
-// step) of every link whose state went to 0; regen_steps the steps that rebuilt.
-int hidem_ref_run(const hidem_params *P, hidem_particle_soa *p, int64_t n, hidem_link_soa *l,
-                  int64_t L, int64_t start_step, int32_t nsteps, void *force_out[6],
-                  int64_t *ev_link, int64_t *ev_step, int64_t ev_cap, int64_t *ev_count,
-                  int64_t *regen_steps, int64_t regen_cap, int64_t *regen_count,
-                  double *seconds) {
-    const Derived d = derive(*P);
-    PData *pdp = make_particles(p, n);
-    PData &pData = *pdp;
-    OffloadHashMap<gKey_t, pInd_t> pMapper;
-    pData.remap(pMapper);
-
-    LData *ldp = new LData();
-    LData &lData = *ldp;
-    {
-        ManVec<ElementaryLink> links;
-        links.resize(L);
-        const lpReal_t *L0 = static_cast<const lpReal_t *>(l->initialLen);
-        for (int64_t i = 0; i < L; ++i) {
-            ElementaryLink e;
-            e.globalKey = l->globalKeys ? l->globalKeys[i] : i;
-            e.globalKeyParticleA = l->globalKeyEndA[i];
-            e.globalKeyParticleB = l->globalKeyEndB[i];
-            e.particleLinkNum = l->particleLinkNum ? l->particleLinkNum[i] : 0;
-            e.owner = 0;
-            e.initialLen = L0[i];
-            e.state = l->state[i];
-            links[i] = e;
-        }
-        lData.appendInitLinks(links);
-    }
-    if (l->CT[0]) {
-        ManVec<ctReal_t> *ct[6] = {&lData.CT0_flat, &lData.CT1_flat, &lData.CT2_flat,
-                                   &lData.CT3_flat, &lData.CT4_flat, &lData.CT5_flat};
-        for (int k = 0; k < 6; ++k) copy_in<ctReal_t>(*ct[k], l->CT[k], 2 * L);
-    }
-    lData.makeLocalPartEnds(pMapper);
-
-    CombinedAccel *accelp = new CombinedAccel();
-    CombinedAccel &accel = *accelp;
-
-    // integrate functor: sample integrate lambda (MainMeshBlock.cpp:182-261) with the
-    // GlacierDem bed terms (MainDem.cpp:176-207) and the fixed / front extensions.
-    const Real3 lowerLimit(P->lowerLimit[0], P->lowerLimit[1], P->lowerLimit[2]);
-    const Real3 upperLimit(P->upperLimit[0], P->upperLimit[1], P->upperLimit[2]);
-    const bool useBed = P->useBed, useVel = P->useVelocityLimit, useBnd = P->useBoundary;
-    const bool useFixed = P->useFixed, useFront = P->useFrontPressure;
-    const bool bMinX = P->boundaryMin[0], bMinY = P->boundaryMin[1], bMinZ = P->boundaryMin[2];
-    const bool bMaxX = P->boundaryMax[0], bMaxY = P->boundaryMax[1], bMaxZ = P->boundaryMax[2];
-    auto integrate = [=](pInd_t pInd, PData &pd) {
-        const uint8_t type = pd.type[pInd];
-        if (useFixed && (type & HIDEM_TYPE_FIXED)) {
-            pd.xDiff[pInd] = 0;
-            pd.yDiff[pInd] = 0;
-            pd.zDiff[pInd] = 0;
-            pd.uDiff[pInd] = 0;
-            pd.vDiff[pInd] = 0;
-            pd.wDiff[pInd] = 0;
-            return;
-        }
-        hpReal_t xCord = pd.xCord[pInd], yCord = pd.yCord[pInd], zCord = pd.zCord[pInd];
-        hpReal_t xCordPrev = 0, yCordPrev = 0, zCordPrev = 0;
-        lpReal_t xDiff = pd.xDiff[pInd], yDiff = pd.yDiff[pInd], zDiff = pd.zDiff[pInd];
-        lpReal_t xTheta = pd.xTheta[pInd], yTheta = pd.yTheta[pInd], zTheta = pd.zTheta[pInd];
-        lpReal_t xThetaPrev = 0, yThetaPrev = 0, zThetaPrev = 0;
-        lpReal_t uDiff = pd.uDiff[pInd], vDiff = pd.vDiff[pInd], wDiff = pd.wDiff[pInd];
-        lpReal_t radius = pd.radius[pInd];
-        lpReal_t diameter = radius * lpReal_t(2.0);
-
-        lpReal_t dragCoeff;
-        if (useBed && (zCord + radius) - d.bedHeight < d.bedInteract) {
-            dragCoeff = std::min(d.bedDrag * d.bedFriction, lpReal_t(1e+5) * d.scale * d.scale);
-        } else if (zCord > d.waterLevel) {
-            dragCoeff = d.airDrag;
-        } else {
-            dragCoeff = d.waterDrag;
-        }
-        lpReal_t xForce = pd.xForce[pInd], yForce = pd.yForce[pInd], zForce = pd.zForce[pInd];
-        lpReal_t uForce = pd.uForce[pInd], vForce = pd.vForce[pInd], wForce = pd.wForce[pInd];
-
-        lpReal_t particleMass = d.rhoIce * diameter * diameter * diameter;
-        lpReal_t particleMomentInertia = particleMass * diameter * diameter / lpReal_t(6.0);
-
-        if (zCord > d.waterLevel) zForce += -d.g * particleMass;
-        if (zCord <= d.waterLevel) zForce += d.lift * particleMass;
-        if (useBed && zCord + radius < d.bedHeight)
-            zForce += d.bedStiffness * (d.bedHeight - (zCord + radius));
-        if (useFront && (type & HIDEM_TYPE_FRONT) && zCord < d.waterLevel) {
-            lpReal_t depth = (lpReal_t)(d.waterLevel - zCord);
-            xForce -= d.rhoWater * d.g * depth * diameter * diameter;
-        }
-
-        auto vel = HiDEMDefTimeIntegration(dragCoeff, d.invDt2, particleMass, d.invDtSqr, d.dtSqr,
-                                           particleMomentInertia, d.invDt,
-                                           xForce, xDiff, xCord, xCordPrev,
-                                           yForce, yDiff, yCord, yCordPrev,
-                                           zForce, zDiff, zCord, zCordPrev,
-                                           uForce, uDiff, xTheta, xThetaPrev,
-                                           vForce, vDiff, yTheta, yThetaPrev,
-                                           wForce, wDiff, zTheta, zThetaPrev);
-        if (useVel) {
-            auto [xVel, yVel, zVel, xThetaVel, yThetaVel, zThetaVel] = vel;
-            HiDEMDefVelocityLimit(d.maxVel, d.maxRot, d.dt,
-                                  xVel, xCord, xCordPrev, yVel, yCord, yCordPrev,
-                                  zVel, zCord, zCordPrev,
-                                  xThetaVel, xTheta, xThetaPrev, yThetaVel, yTheta, yThetaPrev,
-                                  zThetaVel, zTheta, zThetaPrev);
-        }
-        if (useBnd) {
-            HiDEMDefBoundaryCondition(radius, lowerLimit, upperLimit, bMinX, bMaxX, bMinY, bMaxY,
-                                      bMinZ, bMaxZ, xCord, xCordPrev, yCord, yCordPrev, zCord,
-                                      zCordPrev);
-        }
-        pd.xCord[pInd] = xCord;
-        pd.yCord[pInd] = yCord;
-        pd.zCord[pInd] = zCord;
-        pd.xTheta[pInd] = xTheta;
-        pd.yTheta[pInd] = yTheta;
-        pd.zTheta[pInd] = zTheta;
-        pd.xDiff[pInd] = static_cast<lpReal_t>(xCord - xCordPrev);
-        pd.yDiff[pInd] = static_cast<lpReal_t>(yCord - yCordPrev);
-        pd.zDiff[pInd] = static_cast<lpReal_t>(zCord - zCordPrev);
-        pd.uDiff[pInd] = xTheta - xThetaPrev;
-        pd.vDiff[pInd] = yTheta - yThetaPrev;
-        pd.wDiff[pInd] = zTheta - zThetaPrev;
-    };
-
-    HiDEMDefNeighForceFunc nFunc(d.invDt, d.attractDistance, d.attractScaleForce, d.damping,
-                                 d.dampingRotation, d.scaleE);
-    HiDEMDefLinkForceFunc lFunc(d.invDt, d.damping, d.dampingRotation, d.E, d.W2, d.W4, d.G);
-    HiDEMDefLinkBreakFunc bFunc(d.bendBreak, d.maxLoad);
-
+// A persistent run of the sample-main timestep loop: the reference's particle and link
+// data, its CombinedAccel and the rebuild policy state, kept between calls so that
+// steps can be timed without the setup.
+struct RefSession {
+    Derived d;
+    hidem_params P;
+    PData *pd = nullptr;
+    LData *ld = nullptr;
+    CombinedAccel *accel = nullptr;
+    OffloadHashMap<gKey_t, pInd_t> *pMapper = nullptr;
+    int64_t n = 0, L = 0, step = 0, start = 0;
     double accumulatedDist = 0;
-    int64_t nev = 0, nregen = 0;
-    std::vector<uint8_t> before(L);
-    auto t0 = std::chrono::steady_clock::now();
+    std::vector<uint8_t> before;
+    std::vector<int64_t> evLink, evStep, regen;
 
-    for (int64_t t = start_step; t < start_step + nsteps; ++t) {
-        // gridService (HiDEMLib.h:533-628) on one rank
-        bool regen = (t == start_step);
-        if (P->gridRegenInterval != -1) {
-            regen = (t % P->gridRegenInterval) == 0;
+    ~RefSession() {
+        delete accel;
+        delete ld;
+        delete pd;
+        delete pMapper;
+    }
+
+    void setup(const hidem_params *Pin, const hidem_particle_soa *p, int64_t nIn,
+               const hidem_link_soa *l, int64_t LIn, int64_t startStep) {
+        P = *Pin;
+        d = derive(P);
+        n = nIn;
+        L = LIn;
+        step = start = startStep;
+        pd = make_particles(p, n);
+        pMapper = new OffloadHashMap<gKey_t, pInd_t>();
+        pd->remap(*pMapper);
+        ld = new LData();
+        {
+            ManVec<ElementaryLink> links;
+            links.resize(L);
+            const lpReal_t *L0 = static_cast<const lpReal_t *>(l->initialLen);
+            for (int64_t i = 0; i < L; ++i) {
+                ElementaryLink e;
+                e.globalKey = l->globalKeys ? l->globalKeys[i] : i;
+                e.globalKeyParticleA = l->globalKeyEndA[i];
+                e.globalKeyParticleB = l->globalKeyEndB[i];
+                e.particleLinkNum = l->particleLinkNum ? l->particleLinkNum[i] : 0;
+                e.owner = 0;
+                e.initialLen = L0[i];
+                e.state = l->state[i];
+                links[i] = e;
+            }
+            ld->appendInitLinks(links);
+        }
+        if (l->CT[0]) {
+            ManVec<ctReal_t> *ct[6] = {&ld->CT0_flat, &ld->CT1_flat, &ld->CT2_flat,
+                                       &ld->CT3_flat, &ld->CT4_flat, &ld->CT5_flat};
+            for (int k = 0; k < 6; ++k) copy_in<ctReal_t>(*ct[k], l->CT[k], 2 * L);
+        }
+        ld->makeLocalPartEnds(*pMapper);
+        accel = new CombinedAccel();
+        before.resize(L);
+    }
+
+    // gridService (HiDEMLib.h:533-628) on one rank; returns whether it rebuilt.
+    bool gridService() {
+        PData &pData = *pd;
+        const int64_t t = step;
+        bool rg = (t == start);
+        if (P.gridRegenInterval != -1) {
+            rg = (t % P.gridRegenInterval) == 0;
         } else if (t % 10 == 0) {
             // accumulateDist / getMaxDistOwned (HiDEMLib.h:424-474)
             double mx = 0.0, my = 0.0, mz = 0.0;
@@ -398,18 +320,115 @@ int hidem_ref_run(const hidem_params *P, hidem_particle_soa *p, int64_t n, hidem
             lpReal_t xM = mx, yM = my, zM = mz;
             double currDist = 10 * std::sqrt((xM * xM) + (yM * yM) + (zM * zM));
             accumulatedDist += currDist;
-            if (accumulatedDist >= d.interactDist / 2.0) regen = true;
+            if (accumulatedDist >= d.interactDist / 2.0) rg = true;
         }
-        if (t == P->firstBalanceTimestep) regen = true;
-        if (regen) {
+        if (t == P.firstBalanceTimestep) rg = true;
+        if (rg) {
             accumulatedDist = 0;
-            accel.generateNeighbours(pData, lData, d.searchDistance, d.interactDist);
-            accel.generateLinks(pData, lData, d.searchDistance, d.interactDist);
-            accel.lAccel.sortSideData(pData, lData);
-            accel.generateIndexes(pData, lData, d.searchDistance, d.interactDist);
-            if (regen_steps && nregen < regen_cap) regen_steps[nregen] = t;
-            ++nregen;
+            accel->generateNeighbours(pData, *ld, d.searchDistance, d.interactDist);
+            accel->generateLinks(pData, *ld, d.searchDistance, d.interactDist);
+            accel->lAccel.sortSideData(pData, *ld);
+            accel->generateIndexes(pData, *ld, d.searchDistance, d.interactDist);
+            regen.push_back(t);
         }
+        return rg;
+    }
+
+    // computePartForce + applyForce + gated linkUpdate + finalizeTs (MainMeshBlock.cpp:295-320).
+    void rest_of_step() {
+        PData &pData = *pd;
+        LData &lData = *ld;
+        const Derived &dd = d;
+        const Real3 lowerLimit(P.lowerLimit[0], P.lowerLimit[1], P.lowerLimit[2]);
+        const Real3 upperLimit(P.upperLimit[0], P.upperLimit[1], P.upperLimit[2]);
+        const bool useBed = P.useBed, useVel = P.useVelocityLimit, useBnd = P.useBoundary;
+        const bool useFixed = P.useFixed, useFront = P.useFrontPressure;
+        const bool bMinX = P.boundaryMin[0], bMinY = P.boundaryMin[1], bMinZ = P.boundaryMin[2];
+        const bool bMaxX = P.boundaryMax[0], bMaxY = P.boundaryMax[1], bMaxZ = P.boundaryMax[2];
+        // integrate functor: sample integrate lambda (MainMeshBlock.cpp:182-261) with the
+        // GlacierDem bed terms (MainDem.cpp:176-207) and the fixed / front extensions.
+        auto integrate = [=](pInd_t pInd, PData &p) {
+            const uint8_t type = p.type[pInd];
+            if (useFixed && (type & HIDEM_TYPE_FIXED)) {
+                p.xDiff[pInd] = 0;
+                p.yDiff[pInd] = 0;
+                p.zDiff[pInd] = 0;
+                p.uDiff[pInd] = 0;
+                p.vDiff[pInd] = 0;
+                p.wDiff[pInd] = 0;
+                return;
+            }
+            hpReal_t xCord = p.xCord[pInd], yCord = p.yCord[pInd], zCord = p.zCord[pInd];
+            hpReal_t xCordPrev = 0, yCordPrev = 0, zCordPrev = 0;
+            lpReal_t xDiff = p.xDiff[pInd], yDiff = p.yDiff[pInd], zDiff = p.zDiff[pInd];
+            lpReal_t xTheta = p.xTheta[pInd], yTheta = p.yTheta[pInd], zTheta = p.zTheta[pInd];
+            lpReal_t xThetaPrev = 0, yThetaPrev = 0, zThetaPrev = 0;
+            lpReal_t uDiff = p.uDiff[pInd], vDiff = p.vDiff[pInd], wDiff = p.wDiff[pInd];
+            lpReal_t radius = p.radius[pInd];
+            lpReal_t diameter = radius * lpReal_t(2.0);
+
+            lpReal_t dragCoeff;
+            if (useBed && (zCord + radius) - dd.bedHeight < dd.bedInteract) {
+                dragCoeff = std::min(dd.bedDrag * dd.bedFriction, lpReal_t(1e+5) * dd.scale * dd.scale);
+            } else if (zCord > dd.waterLevel) {
+                dragCoeff = dd.airDrag;
+            } else {
+                dragCoeff = dd.waterDrag;
+            }
+            lpReal_t xForce = p.xForce[pInd], yForce = p.yForce[pInd], zForce = p.zForce[pInd];
+            lpReal_t uForce = p.uForce[pInd], vForce = p.vForce[pInd], wForce = p.wForce[pInd];
+
+            lpReal_t particleMass = dd.rhoIce * diameter * diameter * diameter;
+            lpReal_t particleMomentInertia = particleMass * diameter * diameter / lpReal_t(6.0);
+
+            if (zCord > dd.waterLevel) zForce += -dd.g * particleMass;
+            if (zCord <= dd.waterLevel) zForce += dd.lift * particleMass;
+            if (useBed && zCord + radius < dd.bedHeight)
+                zForce += dd.bedStiffness * (dd.bedHeight - (zCord + radius));
+            if (useFront && (type & HIDEM_TYPE_FRONT) && zCord < dd.waterLevel) {
+                lpReal_t depth = (lpReal_t)(dd.waterLevel - zCord);
+                xForce -= dd.rhoWater * dd.g * depth * diameter * diameter;
+            }
+
+            auto vel = HiDEMDefTimeIntegration(dragCoeff, dd.invDt2, particleMass, dd.invDtSqr, dd.dtSqr,
+                                               particleMomentInertia, dd.invDt,
+                                               xForce, xDiff, xCord, xCordPrev,
+                                               yForce, yDiff, yCord, yCordPrev,
+                                               zForce, zDiff, zCord, zCordPrev,
+                                               uForce, uDiff, xTheta, xThetaPrev,
+                                               vForce, vDiff, yTheta, yThetaPrev,
+                                               wForce, wDiff, zTheta, zThetaPrev);
+            if (useVel) {
+                auto [xVel, yVel, zVel, xThetaVel, yThetaVel, zThetaVel] = vel;
+                HiDEMDefVelocityLimit(dd.maxVel, dd.maxRot, dd.dt,
+                                      xVel, xCord, xCordPrev, yVel, yCord, yCordPrev,
+                                      zVel, zCord, zCordPrev,
+                                      xThetaVel, xTheta, xThetaPrev, yThetaVel, yTheta, yThetaPrev,
+                                      zThetaVel, zTheta, zThetaPrev);
+            }
+            if (useBnd) {
+                HiDEMDefBoundaryCondition(radius, lowerLimit, upperLimit, bMinX, bMaxX, bMinY, bMaxY,
+                                          bMinZ, bMaxZ, xCord, xCordPrev, yCord, yCordPrev, zCord,
+                                          zCordPrev);
+            }
+            p.xCord[pInd] = xCord;
+            p.yCord[pInd] = yCord;
+            p.zCord[pInd] = zCord;
+            p.xTheta[pInd] = xTheta;
+            p.yTheta[pInd] = yTheta;
+            p.zTheta[pInd] = zTheta;
+            p.xDiff[pInd] = static_cast<lpReal_t>(xCord - xCordPrev);
+            p.yDiff[pInd] = static_cast<lpReal_t>(yCord - yCordPrev);
+            p.zDiff[pInd] = static_cast<lpReal_t>(zCord - zCordPrev);
+            p.uDiff[pInd] = xTheta - xThetaPrev;
+            p.vDiff[pInd] = yTheta - yThetaPrev;
+            p.wDiff[pInd] = zTheta - zThetaPrev;
+        };
+
+        HiDEMDefNeighForceFunc nFunc(dd.invDt, dd.attractDistance, dd.attractScaleForce, dd.damping,
+                                     dd.dampingRotation, dd.scaleE);
+        HiDEMDefLinkForceFunc lFunc(dd.invDt, dd.damping, dd.dampingRotation, dd.E, dd.W2, dd.W4, dd.G);
+        HiDEMDefLinkBreakFunc bFunc(dd.bendBreak, dd.maxLoad);
 
         // computePartForce (HiDEMLib.h:316-382) -> CombinedAccel::iterateCombined
         auto fullArgs = make4Pack(
@@ -420,7 +439,7 @@ int hidem_ref_run(const hidem_params *P, hidem_particle_soa *p, int64_t n, hidem
                         lData.CT4_flat, lData.CT5_flat),
             packVecPtrs(pData.xForce, pData.yForce, pData.zForce, pData.uForce, pData.vForce,
                         pData.wForce));
-        accel.iterateCombinedPre(OffloadExec(), pData, lData, nFunc, lFunc, fullArgs);
+        accel->iterateCombinedPre(OffloadExec(), pData, lData, nFunc, lFunc, fullArgs);
         Iterator::syncAll();
 
         // applyForce (HiDEMLib.h:303-314)
@@ -428,65 +447,110 @@ int hidem_ref_run(const hidem_params *P, hidem_particle_soa *p, int64_t n, hidem
         Iterator::syncAll();
 
         // linkUpdate, gated as in MainMeshBlock.cpp:312
-        if ((lpReal_t)(t * d.dt) > d.breakTime) {
+        const int64_t t = step;
+        if ((lpReal_t)(t * dd.dt) > dd.breakTime) {
             for (int64_t i = 0; i < L; ++i) before[i] = lData.state[i];
-            accel.iterateLinks(OffloadExec(), pData, lData, bFunc,
-                               make3Pack(packVecPtrs(pData.xCord, pData.yCord, pData.zCord,
-                                                     pData.xTheta, pData.yTheta, pData.zTheta),
-                                         packVecPtrs(), packVecPtrs(lData.state, lData.initialLen)));
+            accel->iterateLinks(OffloadExec(), pData, lData, bFunc,
+                                make3Pack(packVecPtrs(pData.xCord, pData.yCord, pData.zCord,
+                                                      pData.xTheta, pData.yTheta, pData.zTheta),
+                                          packVecPtrs(), packVecPtrs(lData.state, lData.initialLen)));
             Iterator::syncAll();
             for (int64_t i = 0; i < L; ++i) {
                 if (before[i] != 0 && lData.state[i] == 0) {
-                    if (nev < ev_cap) {
-                        ev_link[nev] = i;
-                        ev_step[nev] = t;
-                    }
-                    ++nev;
+                    evLink.push_back(i);
+                    evStep.push_back(t);
+                }
+            }
+        }
+        step = t + 1;  // finalizeTs
+    }
+
+    // Runs nsteps; `seconds` covers the loop except the rebuild of its first step.
+    void advance(int32_t nsteps, double *seconds) {
+        auto t0 = std::chrono::steady_clock::now();
+        for (int32_t s = 0; s < nsteps; ++s) {
+            gridService();
+            if (s == 0) t0 = std::chrono::steady_clock::now();
+            rest_of_step();
+        }
+        auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    }
+
+    void read(hidem_particle_soa *p, hidem_link_soa *l, void *force_out[6]) {
+        PData &pData = *pd;
+        LData &lData = *ld;
+        copy_out<hpReal_t>(p->xCord, pData.xCord, n);
+        copy_out<hpReal_t>(p->yCord, pData.yCord, n);
+        copy_out<hpReal_t>(p->zCord, pData.zCord, n);
+        copy_out<lpReal_t>(p->xTheta, pData.xTheta, n);
+        copy_out<lpReal_t>(p->yTheta, pData.yTheta, n);
+        copy_out<lpReal_t>(p->zTheta, pData.zTheta, n);
+        copy_out<lpReal_t>(p->xDiff, pData.xDiff, n);
+        copy_out<lpReal_t>(p->yDiff, pData.yDiff, n);
+        copy_out<lpReal_t>(p->zDiff, pData.zDiff, n);
+        copy_out<lpReal_t>(p->uDiff, pData.uDiff, n);
+        copy_out<lpReal_t>(p->vDiff, pData.vDiff, n);
+        copy_out<lpReal_t>(p->wDiff, pData.wDiff, n);
+        if (force_out) {
+            copy_out<lpReal_t>(force_out[0], pData.xForce, n);
+            copy_out<lpReal_t>(force_out[1], pData.yForce, n);
+            copy_out<lpReal_t>(force_out[2], pData.zForce, n);
+            copy_out<lpReal_t>(force_out[3], pData.uForce, n);
+            copy_out<lpReal_t>(force_out[4], pData.vForce, n);
+            copy_out<lpReal_t>(force_out[5], pData.wForce, n);
+        }
+        if (l->state)
+            for (int64_t i = 0; i < L; ++i) l->state[i] = lData.state[i];
+        if (l->CT[0]) {
+            ManVec<ctReal_t> *ct[6] = {&lData.CT0_flat, &lData.CT1_flat, &lData.CT2_flat,
+                                       &lData.CT3_flat, &lData.CT4_flat, &lData.CT5_flat};
+            for (int k = 0; k < 6; ++k) {
+                ctReal_t *dst = static_cast<ctReal_t *>(l->CT[k]);
+                for (int64_t i = 0; i < L; ++i) {
+                    dst[2 * i] = (*ct[k])[lData.sideIndEndA[i]];
+                    dst[2 * i + 1] = (*ct[k])[lData.sideIndEndB[i]];
                 }
             }
         }
     }
-    auto t1 = std::chrono::steady_clock::now();
-    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
-    if (ev_count) *ev_count = nev;
-    if (regen_count) *regen_count = nregen;
+};
 
-    // write back
-    copy_out<hpReal_t>(p->xCord, pData.xCord, n);
-    copy_out<hpReal_t>(p->yCord, pData.yCord, n);
-    copy_out<hpReal_t>(p->zCord, pData.zCord, n);
-    copy_out<lpReal_t>(p->xTheta, pData.xTheta, n);
-    copy_out<lpReal_t>(p->yTheta, pData.yTheta, n);
-    copy_out<lpReal_t>(p->zTheta, pData.zTheta, n);
-    copy_out<lpReal_t>(p->xDiff, pData.xDiff, n);
-    copy_out<lpReal_t>(p->yDiff, pData.yDiff, n);
-    copy_out<lpReal_t>(p->zDiff, pData.zDiff, n);
-    copy_out<lpReal_t>(p->uDiff, pData.uDiff, n);
-    copy_out<lpReal_t>(p->vDiff, pData.vDiff, n);
-    copy_out<lpReal_t>(p->wDiff, pData.wDiff, n);
-    if (force_out) {
-        copy_out<lpReal_t>(force_out[0], pData.xForce, n);
-        copy_out<lpReal_t>(force_out[1], pData.yForce, n);
-        copy_out<lpReal_t>(force_out[2], pData.zForce, n);
-        copy_out<lpReal_t>(force_out[3], pData.uForce, n);
-        copy_out<lpReal_t>(force_out[4], pData.vForce, n);
-        copy_out<lpReal_t>(force_out[5], pData.wForce, n);
+void *hidem_ref_open(const hidem_params *P, const hidem_particle_soa *p, int64_t n,
+                     const hidem_link_soa *l, int64_t L, int64_t start_step) {
+    RefSession *s = new RefSession();
+    s->setup(P, p, n, l, L, start_step);
+    return s;
+}
+
+int hidem_ref_advance(void *h, int32_t nsteps, double *seconds) {
+    if (!h || nsteps < 0) return HIDEM_ERR_ARG;
+    static_cast<RefSession *>(h)->advance(nsteps, seconds);
+    return 0;
+}
+
+void hidem_ref_close(void *h) { delete static_cast<RefSession *>(h); }
+
+// One-shot form: setup, nsteps of the loop, write-back (particles in place; links: state
+// and CT), forces of the last step, break events (link index, step), rebuild steps.
+int hidem_ref_run(const hidem_params *P, hidem_particle_soa *p, int64_t n, hidem_link_soa *l,
+                  int64_t L, int64_t start_step, int32_t nsteps, void *force_out[6],
+                  int64_t *ev_link, int64_t *ev_step, int64_t ev_cap, int64_t *ev_count,
+                  int64_t *regen_steps, int64_t regen_cap, int64_t *regen_count,
+                  double *seconds) {
+    RefSession s;
+    s.setup(P, p, n, l, L, start_step);
+    s.advance(nsteps, seconds);
+    s.read(p, l, force_out);
+    int64_t nev = (int64_t)s.evLink.size();
+    for (int64_t i = 0; i < nev && i < ev_cap; ++i) {
+        ev_link[i] = s.evLink[i];
+        ev_step[i] = s.evStep[i];
     }
-    for (int64_t i = 0; i < L; ++i) l->state[i] = lData.state[i];
-    if (l->CT[0]) {
-        ManVec<ctReal_t> *ct[6] = {&lData.CT0_flat, &lData.CT1_flat, &lData.CT2_flat,
-                                   &lData.CT3_flat, &lData.CT4_flat, &lData.CT5_flat};
-        for (int k = 0; k < 6; ++k) {
-            ctReal_t *dst = static_cast<ctReal_t *>(l->CT[k]);
-            for (int64_t i = 0; i < L; ++i) {
-                dst[2 * i] = (*ct[k])[lData.sideIndEndA[i]];
-                dst[2 * i + 1] = (*ct[k])[lData.sideIndEndB[i]];
-            }
-        }
-    }
-    delete accelp;
-    delete ldp;
-    delete pdp;
+    if (ev_count) *ev_count = nev;
+    int64_t nr = (int64_t)s.regen.size();
+    for (int64_t i = 0; i < nr && i < regen_cap; ++i) regen_steps[i] = s.regen[i];
+    if (regen_count) *regen_count = nr;
     return 0;
 }
 

@@ -1,0 +1,90 @@
+"""C-ABI surface on CPU: the library loads, exports every function include/hidem_b200.h
+declares, mirrors the sample defaults, and fails cleanly without a GPU."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from hidem_b200 import abi
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "hidem_b200.h"
+
+
+def declared_functions() -> list[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hidem_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = abi.load()
+    names = declared_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the ctypes prototypes cover the header
+    assert set(names) <= set(abi.EXPORTED)
+
+
+def test_abi_version_and_struct_sizes():
+    lib = abi.load()
+    assert lib.hidem_abi_version() == 1
+    # C layout of the params struct: 22 doubles + 2x3 doubles + 2x3 int32 + ...
+    assert C.sizeof(abi.HidemParticleSoA) == 16 * 8
+    assert C.sizeof(abi.HidemLinkSoA) == 13 * 8
+
+
+def test_defaults_are_the_meshblock_sample_defaults():
+    p = abi.default_params()
+    # HiDEM/MeshBlock/MainMeshBlock.cpp:69-102, HiDEMLib/HiDEMLib.h:744-745
+    assert p.dt == 0.0001 and p.scale == 1.0 and p.E == 1e9 and p.beamWidth == 0.6
+    assert p.damping == 1000.0 and p.dampingRotation == 1000.0
+    assert p.maxLoad == 0.35 and p.bendBreak == 0.35 and p.breakTime == 10.0
+    assert p.rhoIce == 910.0 and p.rhoWater == 1030.0 and p.g == 9.81
+    assert p.maxVel == 20 and p.maxRot == 5 and p.searchDistanceScale == 1.4
+    assert p.gridRegenInterval == -1 and p.firstBalanceTimestep == 2000
+    assert p.precision == abi.PREC_MIXED
+
+
+def test_create_rejects_bad_params_without_touching_cuda():
+    lib = abi.load()
+    p = abi.default_params(precision=7)
+    h = C.c_void_p()
+    assert lib.hidem_create(C.byref(p), 0, C.byref(h)) == 1  # HIDEM_ERR_ARG
+    assert b"precision" in lib.hidem_create_error()
+    p = abi.default_params(dt=-1.0)
+    assert lib.hidem_create(C.byref(p), 0, C.byref(h)) == 1
+    assert not h.value
+
+
+def test_create_without_device_is_a_status_not_a_crash():
+    from conftest import cuda_available
+    if cuda_available():
+        pytest.skip("a GPU is present")
+    lib = abi.load()
+    p = abi.default_params()
+    h = C.c_void_p()
+    st = lib.hidem_create(C.byref(p), 0, C.byref(h))
+    assert st == 2  # HIDEM_ERR_CUDA
+    assert not h.value
+    assert lib.hidem_create_error()
+
+
+def test_null_context_calls_return_arg_error():
+    lib = abi.load()
+    assert lib.hidem_step(None, 1) == 1
+    assert lib.hidem_grid_service(None) == 1
+    assert lib.hidem_compute_forces(None) == 1
+    assert lib.hidem_last_error(None) == b"null context"
+
+
+def test_soa_checks_dtypes_and_sizes():
+    p = abi.empty_particles(4, abi.PREC_MIXED)
+    abi.particle_soa(p, abi.PREC_MIXED, 4)
+    with pytest.raises(TypeError):
+        abi.particle_soa(p, abi.PREC_FP64, 4)
+    with pytest.raises(ValueError):
+        abi.particle_soa(p, abi.PREC_MIXED, 5)
