@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["slab", "block"], default="slab")
+    ap.add_argument("--slab", default="400,100,100",
+                    help="slab size in metres x,y,z (smaller slabs for profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -59,8 +61,11 @@ def make_workload(args):
     from hidem_b200 import abi, workloads
     prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
     if args.workload == "slab":
-        P, p, l = workloads.calving_slab(precision=prec, jitter=0.0)
-        name = "calving slab 400x100x100 m FCC d=1 m (283x71x71 cells), bed, water 90 m, 1% pre-broken"
+        size = tuple(float(v) for v in args.slab.split(","))
+        P, p, l = workloads.calving_slab(size=size, precision=prec, jitter=0.0)
+        cells = tuple(max(1, int(round(s / workloads.SQRT2))) for s in size)
+        name = (f"calving slab {size[0]:g}x{size[1]:g}x{size[2]:g} m FCC d=1 m "
+                f"({cells[0]}x{cells[1]}x{cells[2]} cells), bed, water 90 m, 1% pre-broken")
     else:
         P, p, l = workloads.ice_block(cells=(20, 20, 20), precision=prec)
         name = "ice block 20^3 FCC cells, jitter 0.01 d, bottom fixed"

@@ -21,7 +21,7 @@ LIB = PKG / "libhidem_b200.so"
 OBJ = PKG / "_build"
 
 CU_SOURCES = ["kernels.cu", "api.cu"]
-CPP_SOURCES = ["lattice.cpp"]
+CPP_SOURCES = ["lattice.cpp", "config.cpp"]
 HEADERS = ["internal.h", "kernels.h", "physics.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

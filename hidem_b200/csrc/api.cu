@@ -12,9 +12,14 @@
 
 using namespace hidem;
 
+namespace hidem {
+// per-thread text of the last failure of a call that has no context
+thread_local std::string g_nocontext_error;
+}  // namespace hidem
+
 namespace {
 
-thread_local std::string g_create_error;
+std::string &g_create_error = hidem::g_nocontext_error;
 
 struct SideSet {
     uint32_t *partner = nullptr;
@@ -79,7 +84,8 @@ struct hidem_ctx {
     int32_t *sideSlot[2] = {nullptr, nullptr};
     SideSet side[2];
     int curSide = 0;  // always 0: rebuild swaps the new layout into side[0]
-    std::vector<int64_t> linkOwners, linkKeys, linkKeyA, linkKeyB;
+    std::vector<int32_t> linkOwners;
+    std::vector<int64_t> linkKeys, linkKeyA, linkKeyB;
     std::vector<int32_t> linkNum;
 
     // particle metadata kept on the host (input order)
@@ -375,10 +381,11 @@ hidem_status rebuild(hidem_ctx *ctx) {
 
     // 4. contact list (NeighAccel::generateNeighbours: count pass, widths, fill pass)
     const long long nb32 = nblocks32(n);
+    CK(cudaMemsetAsync(ctx->blockWidth, 0, sizeof(int) * (size_t)(nb32 + 1), st));
     launch_nbr_count<LP>(recp<LP>(ctx, rc), n, ctx->cellOf[c], g, ctx->cellStart, ctx->cellCount,
                          ctx->interactDist, ctx->counts, ctx->blockWidth, ctx->errorFlag, st);
     ctx->launches += 1;
-    ctx->launches += launch_scan<int, long long>(ctx->blockWidth, nb32, 32ll, ctx->nOff,
+    ctx->launches += launch_scan<int, long long>(ctx->blockWidth, nb32 + 1, 32ll, ctx->nOff,
                                                  ctx->scanSums64, ctx->offTotal, st);
     long long nTotal = 0;
     CK(cudaMemcpyAsync(&nTotal, ctx->offTotal, sizeof nTotal, cudaMemcpyDeviceToHost, st));
@@ -394,9 +401,10 @@ hidem_status rebuild(hidem_ctx *ctx) {
     ctx->launches += 1;
 
     // 5. link ends in the new slot order (LinkAccelSide::generateLinks + sortSideData)
+    CK(cudaMemsetAsync(ctx->blockWidth, 0, sizeof(int) * (size_t)(nb32 + 1), st));
     launch_side_count(ctx->orig[c], n, ctx->plStart, ctx->counts, ctx->blockWidth, ctx->errorFlag, st);
     ctx->launches += 1;
-    ctx->launches += launch_scan<int, long long>(ctx->blockWidth, nb32, 32ll, ctx->sOff,
+    ctx->launches += launch_scan<int, long long>(ctx->blockWidth, nb32 + 1, 32ll, ctx->sOff,
                                                  ctx->scanSums64, ctx->offTotal, st);
     long long sTotal = 0;
     CK(cudaMemcpyAsync(&sTotal, ctx->offTotal, sizeof sTotal, cudaMemcpyDeviceToHost, st));
@@ -597,7 +605,7 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (ctx->profile) TRY(profile_pair(ctx, &e0, &e1));
         if (e0) CK(cudaEventRecord(e0, ctx->stream));
-        launch_step<LP>(consts<LP>(ctx), a, true, ctx->stream);
+        launch_step<LP>(consts<LP>(ctx), a, true, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, ctx->stream);
         if (e1) CK(cudaEventRecord(e1, ctx->stream));
         ctx->launches += 1;
         ctx->cur = 1 - ctx->cur;  // the slot order (type / orig / cellOf) is unchanged
@@ -607,6 +615,45 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
     }
     if (pending) TRY(link_update_now<LP>(ctx, pendingStep));
     CK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+template <class LP>
+SoaIn<LP> soa_layout(void *base, long long n) {
+    // caller-order particle fields as contiguous arrays inside one device buffer
+    SoaIn<LP> s;
+    char *b = static_cast<char *>(base);
+    s.x = reinterpret_cast<const double *>(b);
+    s.y = s.x + n;
+    s.z = s.y + n;
+    const LP *lp = reinterpret_cast<const LP *>(b + 24 * n);
+    for (int k = 0; k < 6; ++k) s.d[k] = lp + k * n;
+    s.r = lp + 6 * n;
+    for (int k = 0; k < 3; ++k) s.th[k] = lp + (7 + k) * n;
+    return s;
+}
+
+template <class LP>
+hidem_status upload_particles(hidem_ctx *ctx, const hidem_particle_soa *p, long long n) {
+    cudaStream_t st = ctx->stream;
+    // stage the caller's arrays in the second record buffer, pack into the first
+    SoaIn<LP> s = soa_layout<LP>(ctx->rec[1], n);
+    CK(cudaMemcpyAsync((void *)s.x, p->xCord, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)s.y, p->yCord, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)s.z, p->zCord, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
+    const void *d[6] = {p->xDiff, p->yDiff, p->zDiff, p->uDiff, p->vDiff, p->wDiff};
+    const void *th[3] = {p->xTheta, p->yTheta, p->zTheta};
+    for (int k = 0; k < 6; ++k) {
+        if (d[k]) CK(cudaMemcpyAsync((void *)s.d[k], d[k], sizeof(LP) * (size_t)n, cudaMemcpyHostToDevice, st));
+        else s.d[k] = nullptr;
+    }
+    CK(cudaMemcpyAsync((void *)s.r, p->radius, sizeof(LP) * (size_t)n, cudaMemcpyHostToDevice, st));
+    for (int k = 0; k < 3; ++k) {
+        if (th[k]) CK(cudaMemcpyAsync((void *)s.th[k], th[k], sizeof(LP) * (size_t)n, cudaMemcpyHostToDevice, st));
+        else s.th[k] = nullptr;
+    }
+    launch_pack_records<LP>(s, (int)n, static_cast<PRec<LP> *>(ctx->rec[0]), st);
+    ctx->launches += 1;
     return HIDEM_OK;
 }
 
@@ -776,33 +823,6 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     CK(cudaSetDevice(ctx->device));
     const size_t lp = ctx->lp;
     const size_t recBytes = ctx->mixed ? sizeof(PRec<float>) : sizeof(PRec<double>);
-    std::vector<unsigned char> host(recBytes * (size_t)n, 0);
-    auto lpval = [&](const void *arr, int64_t i) -> double {
-        if (!arr) return 0.0;
-        return lp == 4 ? (double)static_cast<const float *>(arr)[i] : static_cast<const double *>(arr)[i];
-    };
-    for (int64_t i = 0; i < n; ++i) {
-        unsigned char *r = host.data() + recBytes * (size_t)i;
-        double xyz[3] = {p->xCord[i], p->yCord[i], p->zCord[i]};
-        std::memcpy(r, xyz, 24);
-        const void *d[6] = {p->xDiff, p->yDiff, p->zDiff, p->uDiff, p->vDiff, p->wDiff};
-        const void *th[3] = {p->xTheta, p->yTheta, p->zTheta};
-        if (ctx->mixed) {
-            PRec<float> q;
-            std::memcpy(&q, r, 24);
-            for (int k = 0; k < 6; ++k) q.d[k] = d[k] ? static_cast<const float *>(d[k])[i] : 0.f;
-            q.r = static_cast<const float *>(p->radius)[i];
-            for (int k = 0; k < 3; ++k) q.th[k] = th[k] ? static_cast<const float *>(th[k])[i] : 0.f;
-            std::memcpy(r, &q, sizeof q);
-        } else {
-            PRec<double> q{};
-            std::memcpy(&q, r, 24);
-            for (int k = 0; k < 6; ++k) q.d[k] = lpval(d[k], i);
-            q.r = static_cast<const double *>(p->radius)[i];
-            for (int k = 0; k < 3; ++k) q.th[k] = lpval(th[k], i);
-            std::memcpy(r, &q, sizeof q);
-        }
-    }
     for (int b = 0; b < 2; ++b) {
         TRY(dalloc_bytes(ctx, &ctx->rec[b], recBytes * (size_t)n));
         TRY(dalloc(ctx, &ctx->type[b], n));
@@ -819,21 +839,24 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     TRY(dalloc(ctx, &ctx->sOff, nb32 + 1));
     ctx->cur = 0;
     ctx->ord = 0;
-    CK(cudaMemcpyAsync(ctx->rec[0], host.data(), host.size(), cudaMemcpyHostToDevice, ctx->stream));
-    std::vector<uint8_t> ty((size_t)n, 0);
-    if (p->type) std::memcpy(ty.data(), p->type, (size_t)n);
+    TRY(ctx->mixed ? upload_particles<float>(ctx, p, n) : upload_particles<double>(ctx, p, n));
+    if (p->type)
+        CK(cudaMemcpyAsync(ctx->type[0], p->type, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    else
+        CK(cudaMemsetAsync(ctx->type[0], 0, (size_t)n, ctx->stream));
     std::vector<int32_t> ident((size_t)n);
     for (int64_t i = 0; i < n; ++i) ident[i] = (int32_t)i;
-    CK(cudaMemcpyAsync(ctx->type[0], ty.data(), (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->orig[0], ident.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->slotOf, ident.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->slotOf, ctx->orig[0], 4 * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaMemsetAsync(ctx->counts, 0, 4 * (size_t)n, ctx->stream));
     CK(cudaMemsetAsync(ctx->force, 0, 6 * lp * (size_t)n, ctx->stream));
     ctx->owners.assign((size_t)n, 0);
     if (p->owners) std::memcpy(ctx->owners.data(), p->owners, 4 * (size_t)n);
     ctx->keys.resize((size_t)n);
-    for (int64_t i = 0; i < n; ++i) ctx->keys[i] = p->globalKeys ? p->globalKeys[i] : i;
+    if (p->globalKeys) std::memcpy(ctx->keys.data(), p->globalKeys, 8 * (size_t)n);
+    else for (int64_t i = 0; i < n; ++i) ctx->keys[i] = i;
     CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
     ctx->n = n;
     ctx->haveParticles = true;
     ctx->built = false;
@@ -853,46 +876,40 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     CK(cudaSetDevice(ctx->device));
     const long long n = ctx->n;
     const size_t lp = ctx->lp;
-    // globalKey -> input index (LinkData::makeLocalPartEnds, PLiB/LinkData.h:91-115)
-    std::vector<std::pair<int64_t, int32_t>> km((size_t)n);
-    for (long long i = 0; i < n; ++i) km[i] = {ctx->keys[i], (int32_t)i};
-    std::sort(km.begin(), km.end());
+    // globalKey -> input index (LinkData::makeLocalPartEnds, PLiB/LinkData.h:91-115):
+    // direct when the keys are 0..n-1 in order, else through a sorted key table
+    bool identity = true;
+    for (long long i = 0; i < n && identity; ++i) identity = ctx->keys[i] == i;
+    std::vector<std::pair<int64_t, int32_t>> km;
+    if (!identity) {
+        km.resize((size_t)n);
+        for (long long i = 0; i < n; ++i) km[i] = {ctx->keys[i], (int32_t)i};
+        std::sort(km.begin(), km.end());
+    }
     auto find = [&](int64_t key) -> int32_t {
+        if (identity) return (key >= 0 && key < n) ? (int32_t)key : -1;
         auto it = std::lower_bound(km.begin(), km.end(), std::make_pair(key, (int32_t)-1));
         if (it == km.end() || it->first != key) return -1;
         return it->second;
     };
     std::vector<int32_t> A((size_t)L), B((size_t)L);
+    long long bad = -1, self = -1;
+#pragma omp parallel for schedule(static)
     for (long long i = 0; i < L; ++i) {
         A[i] = find(l->globalKeyEndA[i]);
         B[i] = find(l->globalKeyEndB[i]);
-        if (A[i] < 0 || B[i] < 0)
-            return fail(ctx, HIDEM_ERR_NOT_FOUND, "link %lld: dangling end (keys %lld, %lld)", i,
-                        (long long)l->globalKeyEndA[i], (long long)l->globalKeyEndB[i]);
-        if (A[i] == B[i]) return fail(ctx, HIDEM_ERR_ARG, "link %lld joins a particle to itself", i);
+        if (A[i] < 0 || B[i] < 0) {
+#pragma omp critical
+            if (bad < 0 || i < bad) bad = i;
+        } else if (A[i] == B[i]) {
+#pragma omp critical
+            if (self < 0 || i < self) self = i;
+        }
     }
-    // per-particle link ends in ascending link index (LinkAccelSide::generateLinks)
-    std::vector<int32_t> start((size_t)n + 1, 0);
-    for (long long i = 0; i < L; ++i) {
-        start[A[i] + 1]++;
-        start[B[i] + 1]++;
-    }
-    for (long long i = 0; i < n; ++i) start[i + 1] += start[i];
-    std::vector<int32_t> plink((size_t)(2 * L + 1)), cursor(start.begin(), start.end() - 1);
-    std::vector<uint8_t> pend((size_t)(2 * L + 1));
-    for (long long i = 0; i < L; ++i) {
-        int32_t a = cursor[A[i]]++;
-        plink[a] = (int32_t)i;
-        pend[a] = 0;
-        int32_t b = cursor[B[i]]++;
-        plink[b] = (int32_t)i;
-        pend[b] = 1;
-    }
-    // flat initial side layout: side 2l+e
-    std::vector<int32_t> sslot((size_t)(2 * L + 1));
-    for (long long s = 0; s < 2 * L; ++s) sslot[s] = (int32_t)s;
-    std::vector<uint8_t> sstate((size_t)(2 * L + 1));
-    for (long long i = 0; i < L; ++i) sstate[2 * i] = sstate[2 * i + 1] = l->state[i];
+    if (bad >= 0)
+        return fail(ctx, HIDEM_ERR_NOT_FOUND, "link %lld: dangling end (keys %lld, %lld)", bad,
+                    (long long)l->globalKeyEndA[bad], (long long)l->globalKeyEndB[bad]);
+    if (self >= 0) return fail(ctx, HIDEM_ERR_ARG, "link %lld joins a particle to itself", self);
 
     TRY(dalloc(ctx, &ctx->linkA, L));
     TRY(dalloc(ctx, &ctx->linkB, L));
@@ -908,15 +925,20 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     TRY(dalloc(ctx, &ctx->events, std::max<long long>(L, 1)));
     ctx->eventCap = std::max<long long>(L, 1);
     ctx->eventsRead = 0;
+    TRY(ensure_scan(ctx, n + 2));
+    int *deg = nullptr, *cursor = nullptr;
+    uint8_t *lstate = nullptr;
+    TRY(dalloc(ctx, &deg, n + 1));
+    TRY(dalloc(ctx, &cursor, n + 1));
+    TRY(dalloc(ctx, &lstate, std::max<long long>(L, 1)));
     cudaStream_t st = ctx->stream;
+    CK(cudaMemsetAsync(deg, 0, 4 * (size_t)(n + 1), st));
+    CK(cudaMemsetAsync(cursor, 0, 4 * (size_t)(n + 1), st));
     if (L > 0) {
         CK(cudaMemcpyAsync(ctx->linkA, A.data(), 4 * (size_t)L, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->linkB, B.data(), 4 * (size_t)L, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->L0link, l->initialLen, lp * (size_t)L, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(ctx->plLink, plink.data(), 4 * (size_t)(2 * L), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(ctx->plEnd, pend.data(), (size_t)(2 * L), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(ctx->sideSlot[0], sslot.data(), 4 * (size_t)(2 * L), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(ctx->side[0].state, sstate.data(), (size_t)(2 * L), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(lstate, l->state, (size_t)L, cudaMemcpyHostToDevice, st));
         for (int k = 0; k < 6; ++k) {
             if (l->CT[k])
                 CK(cudaMemcpyAsync(ctx->side[0].ct[k], l->CT[k], lp * (size_t)(2 * L), cudaMemcpyHostToDevice, st));
@@ -924,19 +946,28 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
                 CK(cudaMemsetAsync(ctx->side[0].ct[k], 0, lp * (size_t)(2 * L), st));
         }
     }
-    CK(cudaMemcpyAsync(ctx->plStart, start.data(), 4 * (size_t)(n + 1), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(ctx->eventCount, 0, sizeof(unsigned long long), st));
+    // per-particle link ends in ascending link index (LinkAccelSide::generateLinks) and the
+    // flat initial side layout (side 2l+e)
+    launch_link_lists(ctx->linkA, ctx->linkB, L, (int)n, deg, ctx->plStart, cursor, ctx->scanSums32,
+                      ctx->plLink, ctx->plEnd, st);
+    launch_side_init(lstate, L, ctx->sideSlot[0], ctx->side[0].state, st);
+    ctx->launches += 6;
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    dfree(deg);
+    dfree(cursor);
+    dfree(lstate);
     ctx->linkOwners.assign((size_t)L, 0);
     ctx->linkKeys.resize((size_t)L);
     ctx->linkKeyA.assign(l ? l->globalKeyEndA : nullptr, l ? l->globalKeyEndA + L : nullptr);
     ctx->linkKeyB.assign(l ? l->globalKeyEndB : nullptr, l ? l->globalKeyEndB + L : nullptr);
     ctx->linkNum.assign((size_t)L, 0);
-    for (long long i = 0; i < L; ++i) {
-        if (l->owners) ctx->linkOwners[i] = l->owners[i];
-        ctx->linkKeys[i] = l->globalKeys ? l->globalKeys[i] : i;
-        if (l->particleLinkNum) ctx->linkNum[i] = l->particleLinkNum[i];
+    if (L > 0) {
+        if (l->owners) std::memcpy(ctx->linkOwners.data(), l->owners, 4 * (size_t)L);
+        if (l->globalKeys) std::memcpy(ctx->linkKeys.data(), l->globalKeys, 8 * (size_t)L);
+        else for (long long i = 0; i < L; ++i) ctx->linkKeys[i] = i;
+        if (l->particleLinkNum) std::memcpy(ctx->linkNum.data(), l->particleLinkNum, 4 * (size_t)L);
     }
-    CK(cudaStreamSynchronize(st));
     ctx->L = L;
     ctx->haveLinks = true;
     ctx->built = false;
@@ -965,10 +996,10 @@ hidem_status hidem_compute_forces(hidem_ctx *ctx) {
     if (!ctx->built) TRY(do_rebuild(ctx));
     if (ctx->mixed) {
         StepArgs<float> a = step_args<float>(ctx);
-        launch_step<float>(ctx->cf, a, false, ctx->stream);
+        launch_step<float>(ctx->cf, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, ctx->stream);
     } else {
         StepArgs<double> a = step_args<double>(ctx);
-        launch_step<double>(ctx->cd, a, false, ctx->stream);
+        launch_step<double>(ctx->cd, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, ctx->stream);
     }
     ctx->launches += 1;
     CK(cudaGetLastError());
@@ -1047,42 +1078,38 @@ hidem_status hidem_get_particles(hidem_ctx *ctx, hidem_particle_soa *out) {
     if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
     CK(cudaSetDevice(ctx->device));
     const long long n = ctx->n;
-    const size_t recBytes = ctx->mixed ? sizeof(PRec<float>) : sizeof(PRec<double>);
-    std::vector<unsigned char> host(recBytes * (size_t)n);
-    std::vector<int32_t> orig((size_t)n);
-    std::vector<uint8_t> ty((size_t)n);
-    CK(cudaMemcpyAsync(host.data(), ctx->rec[ctx->cur], host.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(orig.data(), ctx->orig[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(ty.data(), ctx->type[ctx->ord], (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    for (long long s = 0; s < n; ++s) {
-        const long long i = orig[s];
-        const unsigned char *r = host.data() + recBytes * (size_t)s;
-        if (ctx->mixed) {
-            PRec<float> q;
-            std::memcpy(&q, r, sizeof q);
-            if (out->xCord) out->xCord[i] = q.x;
-            if (out->yCord) out->yCord[i] = q.y;
-            if (out->zCord) out->zCord[i] = q.z;
-            void *d[6] = {out->xDiff, out->yDiff, out->zDiff, out->uDiff, out->vDiff, out->wDiff};
-            for (int k = 0; k < 6; ++k) if (d[k]) static_cast<float *>(d[k])[i] = q.d[k];
-            void *th[3] = {out->xTheta, out->yTheta, out->zTheta};
-            for (int k = 0; k < 3; ++k) if (th[k]) static_cast<float *>(th[k])[i] = q.th[k];
-            if (out->radius) static_cast<float *>(out->radius)[i] = q.r;
-        } else {
-            PRec<double> q;
-            std::memcpy(&q, r, sizeof q);
-            if (out->xCord) out->xCord[i] = q.x;
-            if (out->yCord) out->yCord[i] = q.y;
-            if (out->zCord) out->zCord[i] = q.z;
-            void *d[6] = {out->xDiff, out->yDiff, out->zDiff, out->uDiff, out->vDiff, out->wDiff};
-            for (int k = 0; k < 6; ++k) if (d[k]) static_cast<double *>(d[k])[i] = q.d[k];
-            void *th[3] = {out->xTheta, out->yTheta, out->zTheta};
-            for (int k = 0; k < 3; ++k) if (th[k]) static_cast<double *>(th[k])[i] = q.th[k];
-            if (out->radius) static_cast<double *>(out->radius)[i] = q.r;
-        }
-        if (out->type) out->type[i] = ty[s];
+    cudaStream_t st = ctx->stream;
+    // unpack the slot-ordered records into caller order in the idle record buffer
+    void *stage = ctx->rec[1 - ctx->cur];
+    const size_t lp = ctx->lp;
+    if (ctx->mixed) {
+        SoaIn<float> s = soa_layout<float>(stage, n);
+        launch_unpack_records<float>(recp<float>(ctx, ctx->cur), ctx->orig[ctx->ord], (int)n, s, st);
+    } else {
+        SoaIn<double> s = soa_layout<double>(stage, n);
+        launch_unpack_records<double>(recp<double>(ctx, ctx->cur), ctx->orig[ctx->ord], (int)n, s, st);
     }
+    ctx->launches += 1;
+    const char *b = static_cast<const char *>(stage);
+    double *xyz[3] = {out->xCord, out->yCord, out->zCord};
+    for (int k = 0; k < 3; ++k)
+        if (xyz[k]) CK(cudaMemcpyAsync(xyz[k], b + 8 * (size_t)n * k, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    const char *lpb = b + 24 * (size_t)n;
+    void *lpf[10] = {out->xDiff, out->yDiff, out->zDiff, out->uDiff, out->vDiff, out->wDiff,
+                     out->radius, out->xTheta, out->yTheta, out->zTheta};
+    for (int k = 0; k < 10; ++k)
+        if (lpf[k]) CK(cudaMemcpyAsync(lpf[k], lpb + lp * (size_t)n * k, lp * (size_t)n, cudaMemcpyDeviceToHost, st));
+    std::vector<int32_t> orig;
+    std::vector<uint8_t> ty;
+    if (out->type) {
+        orig.resize((size_t)n);
+        ty.resize((size_t)n);
+        CK(cudaMemcpyAsync(orig.data(), ctx->orig[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ty.data(), ctx->type[ctx->ord], (size_t)n, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    if (out->type)
+        for (long long s2 = 0; s2 < n; ++s2) out->type[orig[s2]] = ty[s2];
     if (out->owners) std::memcpy(out->owners, ctx->owners.data(), 4 * (size_t)n);
     if (out->globalKeys) std::memcpy(out->globalKeys, ctx->keys.data(), 8 * (size_t)n);
     return HIDEM_OK;
@@ -1094,25 +1121,37 @@ hidem_status hidem_get_links(hidem_ctx *ctx, hidem_link_soa *out) {
     CK(cudaSetDevice(ctx->device));
     const long long L = ctx->L;
     if (L == 0) return HIDEM_OK;
+    cudaStream_t st = ctx->stream;
     SideSet &s = ctx->side[ctx->curSide];
-    const long long cap = s.cap;
-    std::vector<int32_t> slot((size_t)(2 * L));
-    std::vector<uint8_t> st((size_t)cap);
-    CK(cudaMemcpyAsync(slot.data(), ctx->sideSlot[ctx->curSide], 4 * (size_t)(2 * L), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(st.data(), s.state, (size_t)cap, cudaMemcpyDeviceToHost, ctx->stream));
     const size_t lp = ctx->lp;
-    std::vector<unsigned char> ct((size_t)cap * lp);
+    void *stage = nullptr;
+    uint8_t *lstate = nullptr;
+    TRY(dalloc_bytes(ctx, &stage, lp * (size_t)(2 * L)));
+    TRY(dalloc(ctx, &lstate, L));
+    const int *slot = ctx->sideSlot[ctx->curSide];
+    // side data and link state back in caller order
     for (int k = 0; k < 6; ++k) {
         if (!out->CT[k]) continue;
-        CK(cudaMemcpyAsync(ct.data(), s.ct[k], ct.size(), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        unsigned char *dst = static_cast<unsigned char *>(out->CT[k]);
-        for (long long q = 0; q < 2 * L; ++q) std::memcpy(dst + lp * q, ct.data() + lp * (size_t)slot[q], lp);
+        if (ctx->mixed)
+            launch_gather_sides<float>(slot, L, static_cast<const float *>(s.ct[k]), static_cast<float *>(stage), nullptr, nullptr, st);
+        else
+            launch_gather_sides<double>(slot, L, static_cast<const double *>(s.ct[k]), static_cast<double *>(stage), nullptr, nullptr, st);
+        CK(cudaMemcpyAsync(out->CT[k], stage, lp * (size_t)(2 * L), cudaMemcpyDeviceToHost, st));
+        ctx->launches += 1;
     }
-    CK(cudaStreamSynchronize(ctx->stream));
-    if (out->state) for (long long i = 0; i < L; ++i) out->state[i] = st[slot[2 * i]];
-    if (out->initialLen) CK(cudaMemcpy(out->initialLen, ctx->L0link, lp * (size_t)L, cudaMemcpyDeviceToHost));
-    if (out->owners) for (long long i = 0; i < L; ++i) out->owners[i] = (int32_t)ctx->linkOwners[i];
+    if (out->state) {
+        if (ctx->mixed)
+            launch_gather_sides<float>(slot, L, nullptr, nullptr, s.state, lstate, st);
+        else
+            launch_gather_sides<double>(slot, L, nullptr, nullptr, s.state, lstate, st);
+        CK(cudaMemcpyAsync(out->state, lstate, (size_t)L, cudaMemcpyDeviceToHost, st));
+        ctx->launches += 1;
+    }
+    if (out->initialLen) CK(cudaMemcpyAsync(out->initialLen, ctx->L0link, lp * (size_t)L, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    dfree(stage);
+    dfree(lstate);
+    if (out->owners) std::memcpy(out->owners, ctx->linkOwners.data(), 4 * (size_t)L);
     if (out->globalKeys) std::memcpy(out->globalKeys, ctx->linkKeys.data(), 8 * (size_t)L);
     if (out->globalKeyEndA) std::memcpy(out->globalKeyEndA, ctx->linkKeyA.data(), 8 * (size_t)L);
     if (out->globalKeyEndB) std::memcpy(out->globalKeyEndB, ctx->linkKeyB.data(), 8 * (size_t)L);
@@ -1126,17 +1165,17 @@ hidem_status hidem_get_forces(hidem_ctx *ctx, void *force[6]) {
     CK(cudaSetDevice(ctx->device));
     const long long n = ctx->n;
     const size_t lp = ctx->lp;
-    std::vector<unsigned char> f(6 * lp * (size_t)n);
-    std::vector<int32_t> orig((size_t)n);
-    CK(cudaMemcpyAsync(f.data(), ctx->force, f.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(orig.data(), ctx->orig[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    for (int k = 0; k < 6; ++k) {
-        if (!force[k]) continue;
-        unsigned char *dst = static_cast<unsigned char *>(force[k]);
-        for (long long s = 0; s < n; ++s)
-            std::memcpy(dst + lp * (size_t)orig[s], f.data() + lp * (size_t)(k * n + s), lp);
-    }
+    cudaStream_t st = ctx->stream;
+    void *stage = ctx->rec[1 - ctx->cur];
+    if (ctx->mixed)
+        launch_unpack_force<float>(static_cast<const float *>(ctx->force), ctx->orig[ctx->ord], (int)n, static_cast<float *>(stage), st);
+    else
+        launch_unpack_force<double>(static_cast<const double *>(ctx->force), ctx->orig[ctx->ord], (int)n, static_cast<double *>(stage), st);
+    ctx->launches += 1;
+    for (int k = 0; k < 6; ++k)
+        if (force[k])
+            CK(cudaMemcpyAsync(force[k], static_cast<const char *>(stage) + lp * (size_t)n * k, lp * (size_t)n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     return HIDEM_OK;
 }
 

@@ -470,6 +470,172 @@ __global__ void __launch_bounds__(kStepThreads)
     }
 }
 
+// Item-parallel step: one CTA per 32-slot ELL block. Every (particle, contact) and
+// (particle, link end) item of the block is evaluated by its own thread — the ELL
+// entries are read coalesced and the partner gathers are independent — and writes the
+// values its functor adds to the forces into shared memory. One warp then adds them in
+// the reference's order (contacts in list order, then per link end the damping term
+// and the CT term) and integrates, so the result is bit-identical to k_step.
+template <class LP, bool FUSED>
+__global__ void __launch_bounds__(kItemThreads)
+    k_step_items(const Consts<LP> c, const StepArgs<LP> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double *ox = reinterpret_cast<double *>(smem);  // own x, y, z: [3][32]
+    LP *od = reinterpret_cast<LP *>(ox + 96);       // own d[6], r, th[3]: [10][32]
+    int *cn = reinterpret_cast<int *>(od + 320);    // contacts per lane
+    int *cs = cn + 32;                              // link ends per lane
+    LP *terms = reinterpret_cast<LP *>(cs + 32);
+
+    const int w = blockIdx.x;
+    const int base = w * 32;
+    const int t = threadIdx.x;
+    const long long nOff0 = __ldg(a.nOff + w), sOff0 = __ldg(a.sOff + w);
+    const int Wn = (int)((__ldg(a.nOff + w + 1) - nOff0) >> 5);
+    const int Ws = (int)((__ldg(a.sOff + w + 1) - sOff0) >> 5);
+    LP *tc = terms;                  // [Wn][6][32]
+    LP *ts = terms + Wn * 6 * 32;    // [Ws][12][32]
+
+    if (t < 32) {
+        const int i = base + t;
+        if (i < a.n) {
+            const PRec<LP> r = load_rec(a.in + i);
+            ox[t] = r.x;
+            ox[32 + t] = r.y;
+            ox[64 + t] = r.z;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) od[q * 32 + t] = r.d[q];
+            od[6 * 32 + t] = r.r;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) od[(7 + q) * 32 + t] = r.th[q];
+            const uint32_t cnt = __ldg(a.counts + i);
+            cn[t] = (int)(cnt & 0xffffu);
+            cs[t] = (int)(cnt >> 16);
+        } else {
+            cn[t] = 0;
+            cs[t] = 0;
+        }
+    }
+    __syncthreads();
+
+    for (int q = t; q < Wn * 32; q += blockDim.x) {
+        const int k = q >> 5, lane = q & 31;
+        if (k < cn[lane]) {
+            const int j = __ldg(a.nbr + nOff0 + q);
+            const PRec<LP> o = load_rec(a.in + j);
+            LP s[6];
+#pragma unroll
+            for (int u = 0; u < 6; ++u) s[u] = od[u * 32 + lane];
+            LP tt[6];
+            contact_terms<LP>(c, LP(1), (LP)(ox[lane] - o.x), (LP)(ox[32 + lane] - o.y),
+                              (LP)(ox[64 + lane] - o.z), s, od[6 * 32 + lane], o.d, o.r, tt);
+#pragma unroll
+            for (int u = 0; u < 6; ++u) tc[(k * 6 + u) * 32 + lane] = tt[u];
+        }
+    }
+
+    for (int q = t; q < Ws * 32; q += blockDim.x) {
+        const int k = q >> 5, lane = q & 31;
+        if (k < cs[lane]) {
+            const long long si = sOff0 + q;
+            const uint32_t pw = __ldg(a.sPartner + si);
+            const PRec<LP> o = load_rec(a.in + (pw & kSlotMask));
+            uint8_t st = a.sState[si];
+            if (FUSED && a.breakPending && st != 0) {
+                PRec<LP> me;
+                me.x = ox[lane];
+                me.y = ox[32 + lane];
+                me.z = ox[64 + lane];
+#pragma unroll
+                for (int u = 0; u < 3; ++u) me.th[u] = od[(7 + u) * 32 + lane];
+                const LP L0 = __ldg(a.sL0 + si);
+                const uint8_t nst = (pw & kSideIsB) ? break_link<LP>(c, o, me, st, L0)
+                                                    : break_link<LP>(c, me, o, st, L0);
+                if (nst != st) {
+                    a.sState[si] = nst;
+                    if (nst == 0 && !(pw & kSideIsB)) {
+                        unsigned long long slot = atomicAdd(a.eventCount, 1ull);
+                        if ((long long)slot < a.eventCap)
+                            a.events[slot] = make_int2(__ldg(a.sLink + si), (int)a.breakStep);
+                    }
+                    st = nst;
+                }
+            }
+            const LP mask = (st == 0) ? LP(0) : LP(1);
+            LP CT[6];
+#pragma unroll
+            for (int u = 0; u < 6; ++u) CT[u] = a.ct[u][si];
+            LP s[6];
+#pragma unroll
+            for (int u = 0; u < 6; ++u) s[u] = od[u * 32 + lane];
+            LP dp[6], ctt[6];
+            beam_terms<LP>(c, mask, (LP)(ox[lane] - o.x), (LP)(ox[32 + lane] - o.y),
+                           (LP)(ox[64 + lane] - o.z), s, o.d, CT, dp, ctt);
+#pragma unroll
+            for (int u = 0; u < 6; ++u) a.ct[u][si] = CT[u];
+#pragma unroll
+            for (int u = 0; u < 6; ++u) {
+                ts[(k * 12 + u) * 32 + lane] = dp[u];
+                ts[(k * 12 + 6 + u) * 32 + lane] = ctt[u];
+            }
+        }
+    }
+    __syncthreads();
+
+    if (t < 32) {
+        const int i = base + t;
+        LP dmax[3] = {LP(0), LP(0), LP(0)};
+        if (i < a.n) {
+            LP F[6] = {0, 0, 0, 0, 0, 0};
+            const int nn = cn[t], ns = cs[t];
+            for (int k = 0; k < nn; ++k) {
+#pragma unroll
+                for (int u = 0; u < 6; ++u) F[u] = F[u] + tc[(k * 6 + u) * 32 + t];
+            }
+            for (int k = 0; k < ns; ++k) {
+#pragma unroll
+                for (int u = 0; u < 6; ++u) {
+                    F[u] = F[u] + ts[(k * 12 + u) * 32 + t];
+                    F[u] = F[u] + ts[(k * 12 + 6 + u) * 32 + t];
+                }
+            }
+            if (FUSED) {
+                PRec<LP> me;
+                me.x = ox[t];
+                me.y = ox[32 + t];
+                me.z = ox[64 + t];
+#pragma unroll
+                for (int u = 0; u < 6; ++u) me.d[u] = od[u * 32 + t];
+                me.r = od[6 * 32 + t];
+#pragma unroll
+                for (int u = 0; u < 3; ++u) me.th[u] = od[(7 + u) * 32 + t];
+                if (sizeof(PRec<LP>) == 128) {
+                    double *pad = reinterpret_cast<double *>(&me) + 13;
+                    pad[0] = pad[1] = pad[2] = 0.0;
+                }
+                integrate_particle<LP>(c, me, __ldg(a.type + i), F);
+                store_rec(a.out + i, me);
+                dmax[0] = me.d[0] > LP(0) ? me.d[0] : LP(0);
+                dmax[1] = me.d[1] > LP(0) ? me.d[1] : LP(0);
+                dmax[2] = me.d[2] > LP(0) ? me.d[2] : LP(0);
+            } else {
+#pragma unroll
+                for (int u = 0; u < 6; ++u) a.force[(long long)u * a.n + i] = F[u];
+            }
+        }
+        if (FUSED && a.reduceDiff) {
+#pragma unroll
+            for (int u = 0; u < 3; ++u) {
+                LP v = dmax[u];
+                for (int o = 16; o > 0; o >>= 1) {
+                    LP x = __shfl_xor_sync(0xffffffffu, v, o);
+                    v = (x > v) ? x : v;
+                }
+                if (t == 0 && v > LP(0)) atomicMax(a.diffMax + u, max_bits(v));
+            }
+        }
+    }
+}
+
 // HiDEMLib::applyForce with the integrate step, in place (split path).
 template <class LP>
 __global__ void k_integrate(const Consts<LP> c, PRec<LP> *__restrict__ rec,
@@ -625,7 +791,32 @@ void launch_side_fill(const int *orig, int n, const int *slotOf, const int *plSt
 }
 
 template <class LP>
-void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, cudaStream_t s) {
+size_t item_smem_bytes(int maxContacts, int maxEnds) {
+    return 96 * sizeof(double) + 320 * sizeof(LP) + 64 * sizeof(int) +
+           (size_t)(maxContacts * 6 + maxEnds * 12) * 32 * sizeof(LP);
+}
+
+template <class LP>
+void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, int maxContacts,
+                 int maxEnds, cudaStream_t s) {
+    const size_t smem = item_smem_bytes<LP>(maxContacts, maxEnds);
+    if (smem <= kItemSmemLimit) {
+        static bool configured[2] = {false, false};
+        if (!configured[fused ? 1 : 0]) {
+            if (fused)
+                cudaFuncSetAttribute(k_step_items<LP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kItemSmemLimit);
+            else
+                cudaFuncSetAttribute(k_step_items<LP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kItemSmemLimit);
+            configured[fused ? 1 : 0] = true;
+        }
+        const int nb = nblk(a.n, 32);
+        if (fused)
+            k_step_items<LP, true><<<nb, kItemThreads, smem, s>>>(c, a);
+        else
+            k_step_items<LP, false><<<nb, kItemThreads, smem, s>>>(c, a);
+        return;
+    }
+    // rows too wide for the shared-memory term buffers: one thread per particle
     int nb = nblk(a.n, kStepThreads);
     if (fused)
         k_step<LP, true><<<nb, kStepThreads, 0, s>>>(c, a);
@@ -671,7 +862,8 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
                                        const uint8_t *, const int *, const int *, const LP *,      \
                                        const int *, const SideView<LP> &, const long long *,       \
                                        const SideView<LP> &, int *, cudaStream_t);                 \
-    template void launch_step<LP>(const Consts<LP> &, const StepArgs<LP> &, bool, cudaStream_t);   \
+    template void launch_step<LP>(const Consts<LP> &, const StepArgs<LP> &, bool, int, int,          \
+                                  cudaStream_t);   \
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \
@@ -683,5 +875,165 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
 
 HIDEM_INSTANTIATE(float)
 HIDEM_INSTANTIATE(double)
+
+}  // namespace hidem
+
+// ------------------------------------------------------------------ setup / readback
+// Packing between the caller's SoA arrays (input order) and the slot-ordered records,
+// and the per-particle link-end lists, done on the device so that setup and readback
+// cost one copy of each array.
+
+namespace hidem {
+
+template <class LP>
+__global__ void k_pack_records(SoaIn<LP> s, int n, PRec<LP> *__restrict__ rec) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    PRec<LP> r;
+    r.x = s.x[i];
+    r.y = s.y[i];
+    r.z = s.z[i];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) r.d[k] = s.d[k] ? s.d[k][i] : LP(0);
+    r.r = s.r[i];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r.th[k] = s.th[k] ? s.th[k][i] : LP(0);
+    if (sizeof(PRec<LP>) == 128) {
+        double *pad = reinterpret_cast<double *>(&r) + 13;
+        pad[0] = pad[1] = pad[2] = 0.0;
+    }
+    store_rec(rec + i, r);
+}
+
+template <class LP>
+__global__ void k_unpack_records(const PRec<LP> *__restrict__ rec, const int *__restrict__ orig,
+                                 int n, SoaIn<LP> s) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const PRec<LP> r = load_rec(rec + k);
+    const int i = orig[k];
+    const_cast<double *>(s.x)[i] = r.x;
+    const_cast<double *>(s.y)[i] = r.y;
+    const_cast<double *>(s.z)[i] = r.z;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) const_cast<LP *>(s.d[q])[i] = r.d[q];
+    const_cast<LP *>(s.r)[i] = r.r;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) const_cast<LP *>(s.th[q])[i] = r.th[q];
+}
+
+template <class LP>
+__global__ void k_unpack_force(const LP *__restrict__ force, const int *__restrict__ orig, int n,
+                               LP *__restrict__ out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = orig[k];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) out[(long long)q * n + i] = force[(long long)q * n + k];
+}
+
+// per-particle number of link ends
+__global__ void k_link_degree(const int *__restrict__ A, const int *__restrict__ B, long long L,
+                              int *__restrict__ deg) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= L) return;
+    atomicAdd(deg + A[l], 1);
+    atomicAdd(deg + B[l], 1);
+}
+
+__global__ void k_link_fill(const int *__restrict__ A, const int *__restrict__ B, long long L,
+                            const int *__restrict__ start, int *__restrict__ cursor,
+                            int *__restrict__ plLink, uint8_t *__restrict__ plEnd) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= L) return;
+    int a = start[A[l]] + atomicAdd(cursor + A[l], 1);
+    plLink[a] = (int)l;
+    plEnd[a] = 0;
+    int b = start[B[l]] + atomicAdd(cursor + B[l], 1);
+    plLink[b] = (int)l;
+    plEnd[b] = 1;
+}
+
+// a particle's ends in ascending link index (LinkAccelSide::generateLinks, LinkAccelSide.h:118-131)
+__global__ void k_link_sort_ends(const int *__restrict__ start, int n, int *__restrict__ plLink,
+                                 uint8_t *__restrict__ plEnd) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = start[i], e = start[i + 1];
+    for (int a = s + 1; a < e; ++a) {
+        const int v = plLink[a];
+        const uint8_t ve = plEnd[a];
+        int b = a - 1;
+        while (b >= s && plLink[b] > v) {
+            plLink[b + 1] = plLink[b];
+            plEnd[b + 1] = plEnd[b];
+            --b;
+        }
+        plLink[b + 1] = v;
+        plEnd[b + 1] = ve;
+    }
+}
+
+// flat initial side layout: side 2l+e, state copied from the link
+__global__ void k_side_init(const uint8_t *__restrict__ linkState, long long L,
+                            int *__restrict__ sideSlot, uint8_t *__restrict__ sideState) {
+    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= 2 * L) return;
+    sideSlot[s] = (int)s;
+    sideState[s] = linkState[s >> 1];
+}
+
+// side data back in the caller's order: CT[k][2l+e] and the link state
+template <class LP>
+__global__ void k_gather_sides(const int *__restrict__ sideSlot, long long L,
+                               const LP *__restrict__ ct, LP *__restrict__ out,
+                               const uint8_t *__restrict__ sState, uint8_t *__restrict__ linkState) {
+    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= 2 * L) return;
+    const int src = sideSlot[s];
+    if (ct) out[s] = ct[src];
+    if (linkState && (s & 1) == 0) linkState[s >> 1] = sState[src];
+}
+
+template <class LP>
+void launch_pack_records(const SoaIn<LP> &s, int n, PRec<LP> *rec, cudaStream_t st) {
+    k_pack_records<LP><<<nblk(n, 256), 256, 0, st>>>(s, n, rec);
+}
+template <class LP>
+void launch_unpack_records(const PRec<LP> *rec, const int *orig, int n, const SoaIn<LP> &s,
+                           cudaStream_t st) {
+    k_unpack_records<LP><<<nblk(n, 256), 256, 0, st>>>(rec, orig, n, s);
+}
+template <class LP>
+void launch_unpack_force(const LP *force, const int *orig, int n, LP *out, cudaStream_t st) {
+    k_unpack_force<LP><<<nblk(n, 256), 256, 0, st>>>(force, orig, n, out);
+}
+void launch_link_lists(const int *A, const int *B, long long L, int n, int *deg, int *start,
+                       int *cursor, int *sums, int *plLink, uint8_t *plEnd, cudaStream_t st) {
+    if (L > 0) k_link_degree<<<nblk(L, 256), 256, 0, st>>>(A, B, L, deg);
+    // start[0..n] = exclusive scan of deg[0..n] with deg[n] = 0
+    launch_scan<int, int>(deg, (long long)n + 1, 1, start, sums, nullptr, st);
+    if (L > 0) k_link_fill<<<nblk(L, 256), 256, 0, st>>>(A, B, L, start, cursor, plLink, plEnd);
+    k_link_sort_ends<<<nblk(n, 256), 256, 0, st>>>(start, n, plLink, plEnd);
+}
+void launch_side_init(const uint8_t *linkState, long long L, int *sideSlot, uint8_t *sideState,
+                      cudaStream_t st) {
+    if (L > 0) k_side_init<<<nblk(2 * L, 256), 256, 0, st>>>(linkState, L, sideSlot, sideState);
+}
+template <class LP>
+void launch_gather_sides(const int *sideSlot, long long L, const LP *ct, LP *out,
+                         const uint8_t *sState, uint8_t *linkState, cudaStream_t st) {
+    if (L > 0) k_gather_sides<LP><<<nblk(2 * L, 256), 256, 0, st>>>(sideSlot, L, ct, out, sState, linkState);
+}
+
+#define HIDEM_INSTANTIATE_IO(LP)                                                                   \
+    template void launch_pack_records<LP>(const SoaIn<LP> &, int, PRec<LP> *, cudaStream_t);       \
+    template void launch_unpack_records<LP>(const PRec<LP> *, const int *, int, const SoaIn<LP> &,  \
+                                            cudaStream_t);                                         \
+    template void launch_unpack_force<LP>(const LP *, const int *, int, LP *, cudaStream_t);       \
+    template void launch_gather_sides<LP>(const int *, long long, const LP *, LP *,                \
+                                          const uint8_t *, uint8_t *, cudaStream_t);
+HIDEM_INSTANTIATE_IO(float)
+HIDEM_INSTANTIATE_IO(double)
 
 }  // namespace hidem

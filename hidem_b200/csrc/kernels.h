@@ -5,6 +5,8 @@
 namespace hidem {
 
 constexpr int kStepThreads = 128;
+constexpr int kItemThreads = 128;
+constexpr size_t kItemSmemLimit = 160 * 1024;
 
 // One set of link-end ("side") arrays in the warp-blocked ELL layout.
 template <class LP>
@@ -15,6 +17,32 @@ struct SideView {
     LP *L0;             // initial length of the link
     int32_t *link;      // link index (input order)
 };
+
+// Device pointers to the caller-order particle fields (positions f64, the rest lp).
+template <class LP>
+struct SoaIn {
+    const double *x, *y, *z;
+    const LP *d[6];
+    const LP *r;
+    const LP *th[3];
+};
+
+template <class LP>
+void launch_pack_records(const SoaIn<LP> &s, int n, PRec<LP> *rec, cudaStream_t st);
+template <class LP>
+void launch_unpack_records(const PRec<LP> *rec, const int *orig, int n, const SoaIn<LP> &s,
+                           cudaStream_t st);
+template <class LP>
+void launch_unpack_force(const LP *force, const int *orig, int n, LP *out, cudaStream_t st);
+// per-particle link-end lists (ascending link index) from the link ends A, B;
+// deg and cursor hold n+1 zeros on entry; sums >= (n+1)/1024 + 1 elements
+void launch_link_lists(const int *A, const int *B, long long L, int n, int *deg, int *start,
+                       int *cursor, int *sums, int *plLink, uint8_t *plEnd, cudaStream_t st);
+void launch_side_init(const uint8_t *linkState, long long L, int *sideSlot, uint8_t *sideState,
+                      cudaStream_t st);
+template <class LP>
+void launch_gather_sides(const int *sideSlot, long long L, const LP *ct, LP *out,
+                         const uint8_t *sState, uint8_t *linkState, cudaStream_t st);
 
 template <class LP>
 void launch_bounds(const PRec<LP> *rec, int n, double *partial, int nb, double *out, cudaStream_t s);
@@ -49,8 +77,11 @@ void launch_side_fill(const int *orig, int n, const int *slotOf, const int *plSt
                       const LP *L0link, const int *sideSlotOld, const SideView<LP> &oldS,
                       const long long *sOff, const SideView<LP> &newS, int *sideSlotNew,
                       cudaStream_t s);
+// One timestep's forces (fused: + previous link update, integrate, record swap) for
+// rows of at most maxContacts contacts and maxEnds link ends.
 template <class LP>
-void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, cudaStream_t s);
+void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, int maxContacts,
+                 int maxEnds, cudaStream_t s);
 template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,
                       int n, cudaStream_t s);

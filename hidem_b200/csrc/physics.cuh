@@ -14,11 +14,13 @@ __device__ __forceinline__ float labs_(float v) { return fabsf(v); }
 __device__ __forceinline__ double labs_(double v) { return fabs(v); }
 
 // Contact / damping between two particles: HiDEMDefNeighForceFunc::operator()
-// (HiDEMDefaultFunctions.h:21-87). s = self (xDiff..wDiff, radius), o = other.
+// (HiDEMDefaultFunctions.h:21-87). s = self (xDiff..wDiff), sr its radius, o / orr the
+// other. contact_terms returns the six values the functor adds to the forces; adding
+// them to F in component order is exactly the functor's update.
 template <class LP>
-__device__ __forceinline__ void contact_pair(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
-                                             LP zDist, const LP *s, LP sr, const LP *o, LP orr,
-                                             LP *F) {
+__device__ __forceinline__ void contact_terms(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
+                                              LP zDist, const LP *s, LP sr, const LP *o, LP orr,
+                                              LP *t) {
     LP xDist2 = xDist * xDist;
     LP yDist2 = yDist * yDist;
     LP zDist2 = zDist * zDist;
@@ -38,25 +40,38 @@ __device__ __forceinline__ void contact_pair(const Consts<LP> &c, LP mask, LP xD
                ? c.attractScaleForce * dimDist
                : Cnst;
     Cnst = Cnst * c.scaleE;
-    F[0] = F[0] + mask * ((-c.damping) * ((s[0] - o[0]) * c.invDt) + (Cnst * xComp));
-    F[1] = F[1] + mask * ((-c.damping) * ((s[1] - o[1]) * c.invDt) + (Cnst * yComp));
-    F[2] = F[2] + mask * ((-c.damping) * ((s[2] - o[2]) * c.invDt) + (Cnst * zComp));
-    F[3] = F[3] + mask * ((-c.dampingRotation) * ((s[3] - o[3]) * c.invDt));
-    F[4] = F[4] + mask * ((-c.dampingRotation) * ((s[4] - o[4]) * c.invDt));
-    F[5] = F[5] + mask * ((-c.dampingRotation) * ((s[5] - o[5]) * c.invDt));
+    t[0] = mask * ((-c.damping) * ((s[0] - o[0]) * c.invDt) + (Cnst * xComp));
+    t[1] = mask * ((-c.damping) * ((s[1] - o[1]) * c.invDt) + (Cnst * yComp));
+    t[2] = mask * ((-c.damping) * ((s[2] - o[2]) * c.invDt) + (Cnst * zComp));
+    t[3] = mask * ((-c.dampingRotation) * ((s[3] - o[3]) * c.invDt));
+    t[4] = mask * ((-c.dampingRotation) * ((s[4] - o[4]) * c.invDt));
+    t[5] = mask * ((-c.dampingRotation) * ((s[5] - o[5]) * c.invDt));
+}
+
+template <class LP>
+__device__ __forceinline__ void contact_pair(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
+                                             LP zDist, const LP *s, LP sr, const LP *o, LP orr,
+                                             LP *F) {
+    LP t[6];
+    contact_terms<LP>(c, mask, xDist, yDist, zDist, s, sr, o, orr, t);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) F[k] = F[k] + t[k];
 }
 
 // Bonded beam on one link end: HiDEMDefLinkForceFunc::operator()
-// (HiDEMDefaultFunctions.h:90-204). CT is this side's history state (in/out).
+// (HiDEMDefaultFunctions.h:90-204). CT is this side's history state (in/out). The
+// functor adds two values to each force component, first the damping term (dp), later
+// the CT term (ct); beam_terms returns both, beam_side applies them in that order.
 template <class LP>
-__device__ __forceinline__ void beam_side(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
-                                          LP zDist, const LP *s, const LP *o, LP *CT, LP *F) {
-    F[0] = F[0] + (-c.damping * ((s[0] - o[0]) * c.invDt)) * mask;
-    F[1] = F[1] + (-c.damping * ((s[1] - o[1]) * c.invDt)) * mask;
-    F[2] = F[2] + (-c.damping * ((s[2] - o[2]) * c.invDt)) * mask;
-    F[3] = F[3] + (-c.dampingRotation * ((s[3] - o[3]) * c.invDt)) * mask;
-    F[4] = F[4] + (-c.dampingRotation * ((s[4] - o[4]) * c.invDt)) * mask;
-    F[5] = F[5] + (-c.dampingRotation * ((s[5] - o[5]) * c.invDt)) * mask;
+__device__ __forceinline__ void beam_terms(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
+                                           LP zDist, const LP *s, const LP *o, LP *CT, LP *dp,
+                                           LP *ct) {
+    dp[0] = (-c.damping * ((s[0] - o[0]) * c.invDt)) * mask;
+    dp[1] = (-c.damping * ((s[1] - o[1]) * c.invDt)) * mask;
+    dp[2] = (-c.damping * ((s[2] - o[2]) * c.invDt)) * mask;
+    dp[3] = (-c.dampingRotation * ((s[3] - o[3]) * c.invDt)) * mask;
+    dp[4] = (-c.dampingRotation * ((s[4] - o[4]) * c.invDt)) * mask;
+    dp[5] = (-c.dampingRotation * ((s[5] - o[5]) * c.invDt)) * mask;
 
     LP xDist2 = xDist * xDist;
     LP yDist2 = yDist * yDist;
@@ -99,9 +114,9 @@ __device__ __forceinline__ void beam_side(const Consts<LP> &c, LP mask, LP xDist
     CT[1] = CT[1] + (K1 * B1 + K5 * B5 + (-K1) * B7 + K5 * B11);
     CT[2] = CT[2] + (K1 * B2 + (-K5) * B4 + (-K1) * B8 + (-K5) * B10);
 
-    F[0] = F[0] + (-(T00 * CT[0] + T10 * CT[1] + T20 * CT[2])) * mask;
-    F[1] = F[1] + (-(T01 * CT[0] + T11 * CT[1] + T21 * CT[2])) * mask;
-    F[2] = F[2] + (-(T02 * CT[0] + T22 * CT[2])) * mask;
+    ct[0] = (-(T00 * CT[0] + T10 * CT[1] + T20 * CT[2])) * mask;
+    ct[1] = (-(T01 * CT[0] + T11 * CT[1] + T21 * CT[2])) * mask;
+    ct[2] = (-(T02 * CT[0] + T22 * CT[2])) * mask;
 
     LP K2 = c.G * c.W4 * LIDiv6;
     LP K3 = c.E * c.W4 * LIDiv6 * LP(2);
@@ -113,9 +128,18 @@ __device__ __forceinline__ void beam_side(const Consts<LP> &c, LP mask, LP xDist
     CT[4] = CT[4] + ((-K5) * B2 + K3 * B4 + K5 * B8 + K4 * B10);
     CT[5] = CT[5] + (K5 * B1 + K3 * B5 + (-K5) * B7 + K4 * B11);
 
-    F[3] = F[3] + (-(T00 * CT[3] + T10 * CT[4] + T20 * CT[5])) * mask;
-    F[4] = F[4] + (-(T01 * CT[3] + T11 * CT[4] + T21 * CT[5])) * mask;
-    F[5] = F[5] + (-(T02 * CT[3] + T22 * CT[5])) * mask;
+    ct[3] = (-(T00 * CT[3] + T10 * CT[4] + T20 * CT[5])) * mask;
+    ct[4] = (-(T01 * CT[3] + T11 * CT[4] + T21 * CT[5])) * mask;
+    ct[5] = (-(T02 * CT[3] + T22 * CT[5])) * mask;
+}
+
+template <class LP>
+__device__ __forceinline__ void beam_side(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
+                                          LP zDist, const LP *s, const LP *o, LP *CT, LP *F) {
+    LP dp[6], ct[6];
+    beam_terms<LP>(c, mask, xDist, yDist, zDist, s, o, CT, dp, ct);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) F[k] = (F[k] + dp[k]) + ct[k];
 }
 
 // Link break test: HiDEMDefLinkBreakFunc::operator() (HiDEMDefaultFunctions.h:207-242)

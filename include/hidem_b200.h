@@ -128,6 +128,18 @@ typedef struct hidem_stats {
  * HiDEMLib/HiDEMLib.h:714-750); extensions off; precision mixed. */
 void hidem_params_default(hidem_params *p);
 
+/* Run config from a TOML file plus command-line overrides — the keys the sample main
+ * and HiDEMLib::setup read (MainMeshBlock.cpp:69-102, HiDEMLib.h:714-750, maxRadius =
+ * lattice.particleRadius * general.scale as HiDEMGeometry.cpp:88-92) and ArgParser's
+ * `--section.key=value` overrides (PLiB/Util/ArgParser.h:170-270). Keys that are absent
+ * keep the hidem_params_default values; extension keys in [general]: useBed, bedHeight,
+ * bedFriction, useVelocityLimit, useBoundary, useFixed, useFrontPressure, lowerLimit,
+ * upperLimit, precision ("mixed" | "fp64"). path may be NULL (overrides only);
+ * time_steps (may be NULL) receives iteration.timeSteps. Errors: HIDEM_ERR_IO with the
+ * text in hidem_create_error(). */
+hidem_status hidem_params_from_toml(const char *path, int32_t argc, const char *const *argv,
+                                    hidem_params *out, int64_t *time_steps);
+
 /* ---- context --------------------------------------------------------- */
 
 /* Replaces HiDEMLib::setup (HiDEMLib/HiDEMLib.h:707-822) for the hot path:
@@ -135,7 +147,8 @@ void hidem_params_default(hidem_params *p);
 hidem_status hidem_create(const hidem_params *params, int device, hidem_ctx **out);
 void hidem_destroy(hidem_ctx *ctx);
 const char *hidem_last_error(const hidem_ctx *ctx);
-/* Per-thread text of the last hidem_create failure (ctx not yet available). */
+/* Per-thread text of the last failure of a call that has no context
+ * (hidem_create, hidem_params_from_toml). */
 const char *hidem_create_error(void);
 int hidem_abi_version(void);
 

@@ -1,0 +1,74 @@
+// hidem_b200.hpp — header-only C++ adapter with the shape of the reference's HiDEMLib
+// timestep surface (HiDEMLib/HiDEMLib.h:256-530) over the C ABI of hidem_b200.h.
+//
+// The default functors of the reference (HiDEMDefNeighForceFunc, HiDEMDefLinkForceFunc,
+// HiDEMDefLinkBreakFunc, HiDEM/Common/HiDEMDefaultFunctions.h) and the sample integrate
+// step are built into the library; their parameters come from the run config in
+// hidem_params. computePartForce / linkUpdate therefore take no functor objects: a
+// caller that needs a different functor keeps the reference's templated path.
+// Errors throw hidem::Error (status + hidem_last_error text) instead of exit(1).
+#pragma once
+
+#include <stdexcept>
+#include <string>
+
+#include "hidem_b200.h"
+
+namespace hidem {
+
+struct Error : std::runtime_error {
+    hidem_status status;
+    Error(hidem_status s, const std::string &what) : std::runtime_error(what), status(s) {}
+};
+
+class HiDEMLibB200 {
+public:
+    explicit HiDEMLibB200(const hidem_params &p, int device = 0) : params_(p) {
+        hidem_status s = hidem_create(&p, device, &ctx_);
+        if (s != HIDEM_OK) throw Error(s, hidem_create_error());
+    }
+    ~HiDEMLibB200() { hidem_destroy(ctx_); }
+    HiDEMLibB200(const HiDEMLibB200 &) = delete;
+    HiDEMLibB200 &operator=(const HiDEMLibB200 &) = delete;
+
+    // ParticleDataHandler::appendInitParticles / LinkDataHandler::appendInitLinks
+    void setParticles(const hidem_particle_soa &p, int64_t n) { check(hidem_set_particles(ctx_, &p, n)); }
+    void setLinks(const hidem_link_soa &l, int64_t L) { check(hidem_set_links(ctx_, &l, L)); }
+    void setTimestep(int64_t t) { check(hidem_set_timestep(ctx_, t)); }
+
+    // HiDEMLib::gridService / computePartForce / applyForce / linkUpdate / finalizeTs
+    void gridService() { check(hidem_grid_service(ctx_)); }
+    void computePartForce() { check(hidem_compute_forces(ctx_)); }
+    void applyForce() { check(hidem_integrate(ctx_)); }
+    void linkUpdate() { check(hidem_link_update(ctx_)); }
+    void finalizeTs() { check(hidem_finalize_ts(ctx_)); }
+    // n whole timesteps of the sample main loop, one fused kernel per step
+    void step(int32_t n) { check(hidem_step(ctx_, n)); }
+
+    int64_t getCurrentTimestep() {
+        hidem_stats s;
+        check(hidem_get_stats(ctx_, &s));
+        return s.step;
+    }
+    // the sample main's gate `getCurrentTimestep() * dt > breakTime` in lp precision
+    bool breakActive() {
+        const int64_t t = getCurrentTimestep();
+        if (params_.precision == HIDEM_PREC_MIXED)
+            return (float)((float)t * (float)params_.dt) > (float)params_.breakTime;
+        return (double)t * params_.dt > params_.breakTime;
+    }
+
+    void getParticles(hidem_particle_soa &out) { check(hidem_get_particles(ctx_, &out)); }
+    void getLinks(hidem_link_soa &out) { check(hidem_get_links(ctx_, &out)); }
+    void synchronize() { check(hidem_synchronize(ctx_)); }
+    hidem_ctx *handle() { return ctx_; }
+
+private:
+    void check(hidem_status s) {
+        if (s != HIDEM_OK) throw Error(s, hidem_last_error(ctx_));
+    }
+    hidem_params params_;
+    hidem_ctx *ctx_ = nullptr;
+};
+
+}  // namespace hidem

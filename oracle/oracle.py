@@ -25,6 +25,28 @@ _i64 = C.c_int64
 _P = C.POINTER
 
 
+class _quiet_stdout:
+    """Sends C-level stdout to /dev/null while the reference code runs: its Logger prints
+    progress lines (e.g. NeighbourGrid::generate, PLiB/NeighbourGrid.cpp:67) that would
+    mix into a caller's machine-readable output."""
+
+    def __enter__(self):
+        import os
+        import sys
+        sys.stdout.flush()
+        self._saved = os.dup(1)
+        self._null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self._null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        import os
+        C.CDLL(None).fflush(None)
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        os.close(self._null)
+
+
 def _bind(lib, prefix: str):
     getattr(lib, prefix + "_cells").argtypes = [_P(abi.HidemParams), _P(abi.HidemParticleSoA), _i64,
                                                 C.c_void_p, C.c_void_p, C.c_void_p, _P(_i64),
@@ -70,9 +92,10 @@ class CpuPath:
         ix, iy, iz = (np.zeros(n, np.int32) for _ in range(3))
         dims = (_i64 * 3)()
         mins = (C.c_double * 3)()
-        rc = getattr(self.lib, self.prefix + "_cells")(C.byref(params), C.byref(soa), n,
-                                                       ix.ctypes.data, iy.ctypes.data,
-                                                       iz.ctypes.data, dims, mins)
+        with _quiet_stdout():
+            rc = getattr(self.lib, self.prefix + "_cells")(C.byref(params), C.byref(soa), n,
+                                                           ix.ctypes.data, iy.ctypes.data,
+                                                           iz.ctypes.data, dims, mins)
         if rc:
             raise RuntimeError(f"{self.prefix}_cells -> {rc}")
         return ix, iy, iz, tuple(dims), tuple(mins)
@@ -84,12 +107,14 @@ class CpuPath:
         counts = np.zeros(n, np.int32)
         total = _i64()
         f = getattr(self.lib, self.prefix + "_neighbours")
-        rc = f(C.byref(params), C.byref(soa), n, counts.ctypes.data, None, 0, C.byref(total))
+        with _quiet_stdout():
+            rc = f(C.byref(params), C.byref(soa), n, counts.ctypes.data, None, 0, C.byref(total))
         if rc:
             raise RuntimeError(f"{self.prefix}_neighbours -> {rc}")
         lst = np.zeros(max(total.value, 1), np.int32)
-        rc = f(C.byref(params), C.byref(soa), n, counts.ctypes.data, lst.ctypes.data, lst.shape[0],
-               C.byref(total))
+        with _quiet_stdout():
+            rc = f(C.byref(params), C.byref(soa), n, counts.ctypes.data, lst.ctypes.data,
+                   lst.shape[0], C.byref(total))
         if rc:
             raise RuntimeError(f"{self.prefix}_neighbours -> {rc}")
         return counts, lst[: total.value]
@@ -115,10 +140,11 @@ class CpuPath:
         rg = np.zeros(rcap, np.int64)
         nrg = _i64()
         secs = C.c_double()
-        rc = getattr(self.lib, self.prefix + "_run")(
-            C.byref(params), C.byref(psoa), n, C.byref(lsoa), L, start_step, nsteps, fptr,
-            ev_l.ctypes.data, ev_s.ctypes.data, cap, C.byref(nev), rg.ctypes.data, rcap,
-            C.byref(nrg), C.byref(secs))
+        with _quiet_stdout():
+            rc = getattr(self.lib, self.prefix + "_run")(
+                C.byref(params), C.byref(psoa), n, C.byref(lsoa), L, start_step, nsteps, fptr,
+                ev_l.ctypes.data, ev_s.ctypes.data, cap, C.byref(nev), rg.ctypes.data, rcap,
+                C.byref(nrg), C.byref(secs))
         if rc:
             raise RuntimeError(f"{self.prefix}_run -> {rc}")
         k = min(nev.value, cap)
@@ -168,14 +194,17 @@ class RefSession:
         psoa = abi.particle_soa(particles, prec, n)
         lsoa = abi.link_soa(links, prec, L)
         self.n = n
-        self.h = lib.hidem_ref_open(C.byref(params), C.byref(psoa), n, C.byref(lsoa), L, start_step)
+        with _quiet_stdout():
+            self.h = lib.hidem_ref_open(C.byref(params), C.byref(psoa), n, C.byref(lsoa), L,
+                                        start_step)
 
     def threads(self) -> int:
         return int(self.lib.hidem_ref_threads())
 
     def advance(self, nsteps: int) -> float:
         secs = C.c_double()
-        rc = self.lib.hidem_ref_advance(self.h, nsteps, C.byref(secs))
+        with _quiet_stdout():
+            rc = self.lib.hidem_ref_advance(self.h, nsteps, C.byref(secs))
         if rc:
             raise RuntimeError(f"hidem_ref_advance -> {rc}")
         return secs.value

@@ -88,3 +88,40 @@ def test_soa_checks_dtypes_and_sizes():
         abi.particle_soa(p, abi.PREC_FP64, 4)
     with pytest.raises(ValueError):
         abi.particle_soa(p, abi.PREC_MIXED, 5)
+
+
+def test_cpp_adapter_compiles_and_links(tmp_path):
+    """include/hidem_b200.hpp (the HiDEMLib-shaped C++ binding) compiles against the
+    header and links against the library; without a GPU, construction throws a status."""
+    import shutil
+    import subprocess
+    from conftest import cuda_available
+    gxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else shutil.which("g++")
+    if not gxx:
+        pytest.skip("no C++ compiler")
+    root = Path(__file__).resolve().parents[1]
+    src = tmp_path / "adapter.cpp"
+    src.write_text(r'''
+#include "hidem_b200.hpp"
+#include <cstdio>
+int main() {
+    hidem_params p;
+    hidem_params_default(&p);
+    try {
+        hidem::HiDEMLibB200 lib(p, 0);
+        std::printf("created step=%lld\n", (long long)lib.getCurrentTimestep());
+    } catch (const hidem::Error &e) {
+        std::printf("status=%d\n", (int)e.status);
+    }
+    return 0;
+}
+''')
+    exe = tmp_path / "adapter"
+    r = subprocess.run([gxx, "-std=c++17", f"-I{root / 'include'}", str(src), "-o", str(exe),
+                        f"-L{root / 'hidem_b200'}", "-lhidem_b200",
+                        f"-Wl,-rpath,{root / 'hidem_b200'}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0
+    if not cuda_available():
+        assert "status=2" in out.stdout
