@@ -202,6 +202,9 @@ _PROTOS = [
     ("hidem_get_break_events", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64,
                                          C.POINTER(_i64)]),
     ("hidem_get_stats", C.c_int, [C.c_void_p, C.POINTER(HidemStats)]),
+    ("hidem_bin_cells_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64, _d,
+                                          C.c_void_p, C.c_void_p, C.POINTER(_i64), C.POINTER(_d),
+                                          C.c_void_p]),
     ("hidem_params_from_toml", C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p),
                                          C.POINTER(HidemParams), C.POINTER(_i64)]),
     ("hidem_lattice_fcc", C.c_int, [_i32, _i32, _i32, _d, _d, C.POINTER(_d), _d, C.c_uint64,

@@ -20,7 +20,7 @@ INCLUDE = PKG.parent / "include"
 LIB = PKG / "libhidem_b200.so"
 OBJ = PKG / "_build"
 
-CU_SOURCES = ["kernels.cu", "api.cu"]
+CU_SOURCES = ["kernels.cu", "api.cu", "noalloc.cu"]
 CPP_SOURCES = ["lattice.cpp", "config.cpp"]
 HEADERS = ["internal.h", "kernels.h", "physics.cuh"]
 

@@ -148,7 +148,7 @@ hidem_status hidem_create(const hidem_params *params, int device, hidem_ctx **ou
 void hidem_destroy(hidem_ctx *ctx);
 const char *hidem_last_error(const hidem_ctx *ctx);
 /* Per-thread text of the last failure of a call that has no context
- * (hidem_create, hidem_params_from_toml). */
+ * (hidem_create, hidem_params_from_toml, hidem_bin_cells_noalloc). */
 const char *hidem_create_error(void);
 int hidem_abi_version(void);
 
@@ -237,6 +237,29 @@ hidem_status hidem_lattice_fcc(int32_t nx, int32_t ny, int32_t nz, double a, dou
 hidem_status hidem_links_by_distance(const hidem_particle_soa *p, int64_t n, int32_t precision,
                                      double scale, hidem_link_soa *out, int64_t cap,
                                      int64_t *count);
+
+/* ---- allocation-free binning ------------------------------------------ */
+
+/* No counterpart in the reference. For callers that cannot let a library allocate
+ * device memory: applications that place every device buffer themselves (an arena or
+ * pool they size up front, or a host framework whose allocator must own all device
+ * memory) and loops that cannot afford the device-wide synchronisation cudaMalloc and
+ * cudaFree imply. Same binning as the rebuild (hidem_regenerate): bounds of x, y, z,
+ * cell colour ix + iy*X + iz*X*Y of each particle (cell_of), and `order` = particle
+ * indices sorted by (cell, index). x, y, z, cell_of, order are caller-owned device
+ * arrays of n elements; dims and mins are host arrays; work is queued on `stream`
+ * (a cudaStream_t, 0 for the default stream) and the call returns after the bounds
+ * are known on the host. Scratch is one fixed device array in the library (about
+ * 3.1 MB, held on every GPU that loads the library until exit), so grids of more than
+ * HIDEM_NOALLOC_MAX_CELLS cells are refused with HIDEM_ERR_CAPACITY. The first call on
+ * a device looks up that array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture. All calls share the array: calls that overlap on the GPU
+ * race. On failure the text is in hidem_create_error(). */
+#define HIDEM_NOALLOC_MAX_CELLS 262144
+hidem_status hidem_bin_cells_noalloc(const double *x, const double *y, const double *z,
+                                     int64_t n, double cell_size, int32_t *cell_of,
+                                     int32_t *order, int64_t dims[3], double mins[3],
+                                     void *stream);
 
 #ifdef __cplusplus
 }
