@@ -207,6 +207,8 @@ _PROTOS = [
                                           C.c_void_p]),
     ("hidem_params_from_toml", C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p),
                                          C.POINTER(HidemParams), C.POINTER(_i64)]),
+    ("hidem_checkpoint_write", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("hidem_checkpoint_read", C.c_int, [C.c_void_p, C.c_char_p]),
     ("hidem_lattice_fcc", C.c_int, [_i32, _i32, _i32, _d, _d, C.POINTER(_d), _d, C.c_uint64,
                                     _i32, C.POINTER(HidemParticleSoA)]),
     ("hidem_links_by_distance", C.c_int, [C.POINTER(HidemParticleSoA), _i64, _i32, _d,

@@ -21,8 +21,8 @@ LIB = PKG / "libhidem_b200.so"
 OBJ = PKG / "_build"
 
 CU_SOURCES = ["kernels.cu", "api.cu", "noalloc.cu"]
-CPP_SOURCES = ["lattice.cpp", "config.cpp"]
-HEADERS = ["internal.h", "kernels.h", "physics.cuh"]
+CPP_SOURCES = ["lattice.cpp", "config.cpp", "h5lite.cpp", "checkpoint.cpp"]
+HEADERS = ["internal.h", "kernels.h", "physics.cuh", "h5lite.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-prec-div=true",

@@ -255,6 +255,7 @@ hidem_status check_device_error(hidem_ctx *ctx) {
         const char *what = flag == 1   ? "particle outside the grid bounds"
                            : flag == 2 ? "more than 65535 contacts for one particle"
                            : flag == 3 ? "more than 65535 link ends for one particle"
+                           : flag == 4 ? "shared-memory staging copies did not complete in time"
                                        : "device check failed";
         return fail(ctx, HIDEM_ERR_DEVICE, "device check %d: %s", flag, what);
     }
@@ -615,7 +616,7 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
     }
     if (pending) TRY(link_update_now<LP>(ctx, pendingStep));
     CK(cudaGetLastError());
-    return HIDEM_OK;
+    return check_device_error(ctx);
 }
 
 template <class LP>
@@ -658,6 +659,13 @@ hidem_status upload_particles(hidem_ctx *ctx, const hidem_particle_soa *p, long 
 }
 
 }  // namespace
+
+namespace hidem {
+hidem_status ctx_fail(hidem_ctx *ctx, hidem_status s, const std::string &msg) {
+    return fail(ctx, s, "%s", msg.c_str());
+}
+int ctx_precision(const hidem_ctx *ctx) { return ctx->P.precision; }
+}  // namespace hidem
 
 // =================================================================== C ABI
 

@@ -114,6 +114,7 @@ struct StepArgs {
     unsigned long long *eventCount;
     long long eventCap;
     int *errorFlag;
+    int maxContacts, maxEnds; // widest rows of this layout
 };
 
 }  // namespace hidem

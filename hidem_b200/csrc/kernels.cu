@@ -470,58 +470,140 @@ __global__ void __launch_bounds__(kStepThreads)
     }
 }
 
-// Item-parallel step: one CTA per 32-slot ELL block. Every (particle, contact) and
-// (particle, link end) item of the block is evaluated by its own thread — the ELL
-// entries are read coalesced and the partner gathers are independent — and writes the
-// values its functor adds to the forces into shared memory. One warp then adds them in
-// the reference's order (contacts in list order, then per link end the damping term
-// and the CT term) and integrates, so the result is bit-identical to k_step.
-template <class LP, bool FUSED>
-__global__ void __launch_bounds__(kItemThreads)
-    k_step_items(const Consts<LP> c, const StepArgs<LP> a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    double *ox = reinterpret_cast<double *>(smem);  // own x, y, z: [3][32]
-    LP *od = reinterpret_cast<LP *>(ox + 96);       // own d[6], r, th[3]: [10][32]
-    int *cn = reinterpret_cast<int *>(od + 320);    // contacts per lane
-    int *cs = cn + 32;                              // link ends per lane
-    LP *terms = reinterpret_cast<LP *>(cs + 32);
+// ---- shared-memory staging with bulk copies (cp.async.bulk + mbarrier) ----
 
-    const int w = blockIdx.x;
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// 1-D bulk copy global -> shared; both addresses 16-byte aligned, size a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: gives up after kMbarSpins polls (each poll may suspend briefly)
+constexpr int kMbarSpins = 1 << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    for (int it = 0; it < kMbarSpins; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Item-parallel step: one CTA per 32-slot ELL block. The CTA first stages, with bulk
+// copies (cp.async.bulk + mbarrier), everything of its block that is contiguous in HBM:
+// its 32 own records, its contact indices, and its link ends' partner words, CT0..CT5,
+// states and initial lengths. Every (particle, contact) and (particle, link end) item is
+// then evaluated by its own thread — one dependent global load per item, the partner
+// record, served by L1 / L2 — and writes the values its functor adds to the forces into
+// shared memory; one warp adds them in the reference's order (contacts in list order, then
+// per link end the damping term and the CT term) and integrates, so the result is
+// bit-identical to k_step.
+template <class LP, bool FUSED>
+__device__ __forceinline__ void step_items_block(const Consts<LP> &c, const StepArgs<LP> &a,
+                                                 const int w, unsigned char *smem) {
+    const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), a.maxContacts, a.maxEnds);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    PRec<LP> *own = reinterpret_cast<PRec<LP> *>(smem + L.own);
+    double *ox = reinterpret_cast<double *>(smem + L.soa);  // own x, y, z: [3][32]
+    LP *od = reinterpret_cast<LP *>(ox + 96);               // own d[6], r, th[3]: [10][32]
+    int *cn = reinterpret_cast<int *>(od + 320);
+    int *cs = cn + 32;
+    const int *nb = reinterpret_cast<const int *>(smem + L.nbr);
+    const uint32_t *spw = reinterpret_cast<const uint32_t *>(smem + L.spw);
+    LP *sct = reinterpret_cast<LP *>(smem + L.sct);          // [6][maxEnds * 32]
+    const uint8_t *sst = smem + L.sst;
+    const LP *sl0 = reinterpret_cast<const LP *>(smem + L.sl0);
+    LP *terms = reinterpret_cast<LP *>(smem + L.terms);
+    const int ctStride = a.maxEnds * 32;
+
     const int base = w * 32;
     const int t = threadIdx.x;
+    const int nown = min(32, a.n - base);
     const long long nOff0 = __ldg(a.nOff + w), sOff0 = __ldg(a.sOff + w);
     const int Wn = (int)((__ldg(a.nOff + w + 1) - nOff0) >> 5);
     const int Ws = (int)((__ldg(a.sOff + w + 1) - sOff0) >> 5);
+    const bool wantL0 = FUSED && a.breakPending;
     LP *tc = terms;                  // [Wn][6][32]
     LP *ts = terms + Wn * 6 * 32;    // [Ws][12][32]
 
+    if (t == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (t == 0) {
+        const uint32_t ends = (uint32_t)(Ws * 32);
+        uint32_t bytes = (uint32_t)(nown * sizeof(PRec<LP>)) + (uint32_t)(Wn * 32 * 4);
+        if (ends)
+            bytes += ends * (4u + 6u * (uint32_t)sizeof(LP) + 1u) +
+                     (wantL0 ? ends * (uint32_t)sizeof(LP) : 0u);
+        mbar_expect_tx(bar, bytes);
+        bulk_g2s(own, a.in + base, (uint32_t)(nown * sizeof(PRec<LP>)), bar);
+        if (Wn) bulk_g2s((void *)nb, a.nbr + nOff0, (uint32_t)(Wn * 32 * 4), bar);
+        if (ends) {
+            bulk_g2s((void *)spw, a.sPartner + sOff0, ends * 4u, bar);
+            for (int u = 0; u < 6; ++u)
+                bulk_g2s(sct + u * ctStride, a.ct[u] + sOff0, ends * (uint32_t)sizeof(LP), bar);
+            bulk_g2s((void *)sst, a.sState + sOff0, ends, bar);
+            if (wantL0) bulk_g2s((void *)sl0, a.sL0 + sOff0, ends * (uint32_t)sizeof(LP), bar);
+        }
+    }
     if (t < 32) {
         const int i = base + t;
-        if (i < a.n) {
-            const PRec<LP> r = load_rec(a.in + i);
-            ox[t] = r.x;
-            ox[32 + t] = r.y;
-            ox[64 + t] = r.z;
+        const uint32_t cnt = (i < a.n) ? __ldg(a.counts + i) : 0u;
+        cn[t] = (int)(cnt & 0xffffu);
+        cs[t] = (int)(cnt >> 16);
+    }
+    const bool ok = mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        // the copies did not complete in time: flag it, give in-flight copies a bounded
+        // chance to land in this CTA's shared memory, and leave without computing
+        if (t == 0) set_error(a.errorFlag, 4);
+        if (!ok) mbar_wait_bounded(bar, 0);
+        __syncthreads();
+        return;
+    }
+    // own records to structure-of-arrays (conflict-free lane-indexed reads below)
+    if (t < nown) {
+        const PRec<LP> r = own[t];
+        ox[t] = r.x;
+        ox[32 + t] = r.y;
+        ox[64 + t] = r.z;
 #pragma unroll
-            for (int q = 0; q < 6; ++q) od[q * 32 + t] = r.d[q];
-            od[6 * 32 + t] = r.r;
+        for (int q = 0; q < 6; ++q) od[q * 32 + t] = r.d[q];
+        od[6 * 32 + t] = r.r;
 #pragma unroll
-            for (int q = 0; q < 3; ++q) od[(7 + q) * 32 + t] = r.th[q];
-            const uint32_t cnt = __ldg(a.counts + i);
-            cn[t] = (int)(cnt & 0xffffu);
-            cs[t] = (int)(cnt >> 16);
-        } else {
-            cn[t] = 0;
-            cs[t] = 0;
-        }
+        for (int q = 0; q < 3; ++q) od[(7 + q) * 32 + t] = r.th[q];
     }
     __syncthreads();
 
     for (int q = t; q < Wn * 32; q += blockDim.x) {
         const int k = q >> 5, lane = q & 31;
         if (k < cn[lane]) {
-            const int j = __ldg(a.nbr + nOff0 + q);
-            const PRec<LP> o = load_rec(a.in + j);
+            const PRec<LP> o = load_rec(a.in + nb[q]);
             LP s[6];
 #pragma unroll
             for (int u = 0; u < 6; ++u) s[u] = od[u * 32 + lane];
@@ -537,9 +619,9 @@ __global__ void __launch_bounds__(kItemThreads)
         const int k = q >> 5, lane = q & 31;
         if (k < cs[lane]) {
             const long long si = sOff0 + q;
-            const uint32_t pw = __ldg(a.sPartner + si);
+            const uint32_t pw = spw[q];
             const PRec<LP> o = load_rec(a.in + (pw & kSlotMask));
-            uint8_t st = a.sState[si];
+            uint8_t st = sst[q];
             if (FUSED && a.breakPending && st != 0) {
                 PRec<LP> me;
                 me.x = ox[lane];
@@ -547,7 +629,7 @@ __global__ void __launch_bounds__(kItemThreads)
                 me.z = ox[64 + lane];
 #pragma unroll
                 for (int u = 0; u < 3; ++u) me.th[u] = od[(7 + u) * 32 + lane];
-                const LP L0 = __ldg(a.sL0 + si);
+                const LP L0 = sl0[q];
                 const uint8_t nst = (pw & kSideIsB) ? break_link<LP>(c, o, me, st, L0)
                                                     : break_link<LP>(c, me, o, st, L0);
                 if (nst != st) {
@@ -563,7 +645,7 @@ __global__ void __launch_bounds__(kItemThreads)
             const LP mask = (st == 0) ? LP(0) : LP(1);
             LP CT[6];
 #pragma unroll
-            for (int u = 0; u < 6; ++u) CT[u] = a.ct[u][si];
+            for (int u = 0; u < 6; ++u) CT[u] = sct[u * ctStride + q];
             LP s[6];
 #pragma unroll
             for (int u = 0; u < 6; ++u) s[u] = od[u * 32 + lane];
@@ -599,19 +681,7 @@ __global__ void __launch_bounds__(kItemThreads)
                 }
             }
             if (FUSED) {
-                PRec<LP> me;
-                me.x = ox[t];
-                me.y = ox[32 + t];
-                me.z = ox[64 + t];
-#pragma unroll
-                for (int u = 0; u < 6; ++u) me.d[u] = od[u * 32 + t];
-                me.r = od[6 * 32 + t];
-#pragma unroll
-                for (int u = 0; u < 3; ++u) me.th[u] = od[(7 + u) * 32 + t];
-                if (sizeof(PRec<LP>) == 128) {
-                    double *pad = reinterpret_cast<double *>(&me) + 13;
-                    pad[0] = pad[1] = pad[2] = 0.0;
-                }
+                PRec<LP> me = own[t];
                 integrate_particle<LP>(c, me, __ldg(a.type + i), F);
                 store_rec(a.out + i, me);
                 dmax[0] = me.d[0] > LP(0) ? me.d[0] : LP(0);
@@ -634,6 +704,31 @@ __global__ void __launch_bounds__(kItemThreads)
             }
         }
     }
+}
+
+template <class LP, bool FUSED>
+__global__ void __launch_bounds__(kItemThreads)
+    k_step_items(const Consts<LP> c, const StepArgs<LP> a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    step_items_block<LP, FUSED>(c, a, blockIdx.x, smem);
+}
+
+// One fused step of many independent contexts in one launch: CTA b belongs to the entry
+// whose block range [firstBlock, next firstBlock) holds b; each entry carries its own
+// constants, buffers and layout (the dynamic shared memory is the largest entry's).
+template <class LP>
+__global__ void __launch_bounds__(kItemThreads)
+    k_step_batch(const BatchEntry<LP> *__restrict__ entries, int nentries) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int b = blockIdx.x;
+    int lo = 0, hi = nentries - 1;
+    while (lo < hi) {  // last entry with firstBlock <= b
+        const int mid = (lo + hi + 1) >> 1;
+        if (entries[mid].firstBlock <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchEntry<LP> &e = entries[lo];
+    step_items_block<LP, true>(e.c, e.a, b - e.firstBlock, smem);
 }
 
 // HiDEMLib::applyForce with the integrate step, in place (split path).
@@ -791,16 +886,13 @@ void launch_side_fill(const int *orig, int n, const int *slotOf, const int *plSt
 }
 
 template <class LP>
-size_t item_smem_bytes(int maxContacts, int maxEnds) {
-    return 96 * sizeof(double) + 320 * sizeof(LP) + 64 * sizeof(int) +
-           (size_t)(maxContacts * 6 + maxEnds * 12) * 32 * sizeof(LP);
-}
-
-template <class LP>
-void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, int maxContacts,
+void launch_step(const Consts<LP> &c, const StepArgs<LP> &a0, bool fused, int maxContacts,
                  int maxEnds, cudaStream_t s) {
-    const size_t smem = item_smem_bytes<LP>(maxContacts, maxEnds);
-    if (smem <= kItemSmemLimit) {
+    StepArgs<LP> a = a0;
+    a.maxContacts = maxContacts;
+    a.maxEnds = maxEnds;
+    const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds);
+    if (L.total <= kItemSmemLimit) {
         static bool configured[2] = {false, false};
         if (!configured[fused ? 1 : 0]) {
             if (fused)
@@ -811,17 +903,34 @@ void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, int max
         }
         const int nb = nblk(a.n, 32);
         if (fused)
-            k_step_items<LP, true><<<nb, kItemThreads, smem, s>>>(c, a);
+            k_step_items<LP, true><<<nb, kItemThreads, L.total, s>>>(c, a);
         else
-            k_step_items<LP, false><<<nb, kItemThreads, smem, s>>>(c, a);
+            k_step_items<LP, false><<<nb, kItemThreads, L.total, s>>>(c, a);
         return;
     }
-    // rows too wide for the shared-memory term buffers: one thread per particle
+    // rows too wide for the shared-memory buffers: one thread per particle
     int nb = nblk(a.n, kStepThreads);
     if (fused)
         k_step<LP, true><<<nb, kStepThreads, 0, s>>>(c, a);
     else
         k_step<LP, false><<<nb, kStepThreads, 0, s>>>(c, a);
+}
+
+template <class LP>
+bool batch_fits(int maxContacts, int maxEnds) {
+    return stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds).total <= kItemSmemLimit;
+}
+
+template <class LP>
+void launch_step_batch(const BatchEntry<LP> *entries, int nentries, int totalBlocks,
+                       int maxContacts, int maxEnds, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_step_batch<LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kItemSmemLimit);
+        configured = true;
+    }
+    const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds);
+    k_step_batch<LP><<<totalBlocks, kItemThreads, L.total, s>>>(entries, nentries);
 }
 
 template <class LP>
@@ -864,6 +973,8 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
                                        const SideView<LP> &, int *, cudaStream_t);                 \
     template void launch_step<LP>(const Consts<LP> &, const StepArgs<LP> &, bool, int, int,          \
                                   cudaStream_t);   \
+    template bool batch_fits<LP>(int, int);                                                        \
+    template void launch_step_batch<LP>(const BatchEntry<LP> *, int, int, int, int, cudaStream_t);  \
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \

@@ -5,8 +5,30 @@
 namespace hidem {
 
 constexpr int kStepThreads = 128;
-constexpr int kItemThreads = 128;
-constexpr size_t kItemSmemLimit = 160 * 1024;
+constexpr int kItemThreads = 256;
+constexpr size_t kItemSmemLimit = 200 * 1024;
+// Byte offsets of the item kernel's shared-memory regions (same for all CTAs of a launch):
+// mbarrier, own records (AoS as copied, then SoA), contact indices, the link-end streams
+// partner word / CT0..CT5 / state / initial length, then the force terms.
+struct StageLayout {
+    size_t own, soa, nbr, spw, sct, sst, sl0, terms, total;
+};
+inline __host__ __device__ size_t stage_align(size_t v) { return (v + 127) & ~size_t(127); }
+inline __host__ __device__ StageLayout stage_layout(size_t rec, size_t lp, int maxContacts,
+                                                    int maxEnds) {
+    StageLayout L;
+    const size_t ends = (size_t)maxEnds * 32;
+    L.own = 128;
+    L.soa = stage_align(L.own + 32 * rec);
+    L.nbr = stage_align(L.soa + 96 * 8 + 320 * lp + 64 * 4);
+    L.spw = stage_align(L.nbr + (size_t)maxContacts * 32 * 4);
+    L.sct = stage_align(L.spw + ends * 4);
+    L.sst = stage_align(L.sct + 6 * ends * lp);
+    L.sl0 = stage_align(L.sst + ends);
+    L.terms = stage_align(L.sl0 + ends * lp);
+    L.total = stage_align(L.terms + (size_t)(maxContacts * 6 + maxEnds * 12) * 32 * lp);
+    return L;
+}
 
 // One set of link-end ("side") arrays in the warp-blocked ELL layout.
 template <class LP>
@@ -82,6 +104,21 @@ void launch_side_fill(const int *orig, int n, const int *slotOf, const int *plSt
 template <class LP>
 void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, int maxContacts,
                  int maxEnds, cudaStream_t s);
+// One context's share of a batched step launch.
+template <class LP>
+struct BatchEntry {
+    Consts<LP> c;
+    StepArgs<LP> a;
+    int firstBlock;  // first CTA of this context in the launch
+};
+// whether rows of these widths run in the item kernel (else: per-context launches)
+template <class LP>
+bool batch_fits(int maxContacts, int maxEnds);
+// entries: device array; maxContacts / maxEnds: the widest over all entries (shared memory)
+template <class LP>
+void launch_step_batch(const BatchEntry<LP> *entries, int nentries, int totalBlocks,
+                       int maxContacts, int maxEnds, cudaStream_t s);
+
 template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,
                       int n, cudaStream_t s);

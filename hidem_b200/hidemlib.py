@@ -137,9 +137,23 @@ class HiDEMLib:
     def synchronize(self) -> None:
         self._check(self._lib.hidem_synchronize(self._ctx))
 
+    # ------------------------------------------------------------ checkpoint
+    def write_checkpoint(self, path: str) -> None:
+        """HiDEMH5Checkpoint::writeCheckpoint layout (one rank)."""
+        self._check(self._lib.hidem_checkpoint_write(self._ctx, str(path).encode()))
+
+    def read_checkpoint(self, path: str) -> None:
+        """HiDEMLib::setFromRestart + fromCheckpoint: timestep, particles, links, CT."""
+        self._check(self._lib.hidem_checkpoint_read(self._ctx, str(path).encode()))
+        s = self.stats()
+        self.n = int(s["num_particles"])
+        self.L = int(s["num_links"])
+
     # ------------------------------------------------------------ readback
-    def get_particles(self) -> dict:
-        out = abi.empty_particles(self.n, self.precision)
+    def get_particles(self, out: dict | None = None) -> dict:
+        """Particle state in input order, into `out` (e.g. pinned arrays) when given."""
+        if out is None:
+            out = abi.empty_particles(self.n, self.precision)
         soa = abi.particle_soa(out, self.precision, self.n)
         self._check(self._lib.hidem_get_particles(self._ctx, C.byref(soa)))
         return out

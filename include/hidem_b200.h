@@ -220,6 +220,21 @@ hidem_status hidem_get_break_events(hidem_ctx *ctx, int64_t *link_index, int64_t
                                     int64_t cap, int64_t *count);
 hidem_status hidem_get_stats(hidem_ctx *ctx, hidem_stats *out);
 
+/* ---- checkpoint (HDF5) ------------------------------------------------ */
+
+/* Writes the context's state in the reference's checkpoint layout for one rank
+ * (HiDEMLib/HiDEMH5Checkpoint.h:24-50, PLiB/H5IO/H5Checkpoint.h:42-111,
+ * PLiB/ParticleDataHandler.h:215-230, PLiB/LinkDataHandler.h:356-395): root attribute
+ * timeStep; groups Domains, Particles (field_0..15), Links (field_0..6), LinkSideData
+ * (side_field_7..12, CT in [sideA, sideB] order), spann_sizes / spann_offsets; contiguous
+ * datasets, lp fields float (mixed) or double (FP64). The file is written by the
+ * library's own HDF5 encoder (superblock v2, compact groups). */
+hidem_status hidem_checkpoint_write(hidem_ctx *ctx, const char *path);
+/* Restarts from such a file (ParticleDataHandler::fromCheckpoint, LinkDataHandler::
+ * fromCheckpoint, HiDEMLib::setFromRestart): timestep, particles, links, CT. The file's
+ * lp type must match the context's precision. */
+hidem_status hidem_checkpoint_read(hidem_ctx *ctx, const char *path);
+
 /* ---- lattice generation (setup-side inputs for the workloads) --------- */
 
 /* FCC lattice of nx*ny*nz unit cells, lattice constant a, radius r, origin o,

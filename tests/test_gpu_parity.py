@@ -297,3 +297,24 @@ def test_slab_fused_equals_split_and_lists_are_symmetric(gpu, slab_mixed):
     bwd = lst.astype(np.int64) * n + rows
     assert np.array_equal(np.sort(fwd), np.sort(bwd))  # the contact filter is symmetric
     assert counts.max() == 12  # FCC at 1.2 d: the 12 nearest neighbours
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_wide_rows_take_the_thread_per_particle_kernel(gpu, precision):
+    """Rows too long for the item kernel's shared-memory term buffers (here a search
+    distance spanning the whole lattice) run the thread-per-particle kernel; same results."""
+    g = np.arange(8) * 1.05
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    n = x.size
+    p = abi.empty_particles(n, precision)
+    p["xCord"][:], p["yCord"][:], p["zCord"][:] = x.ravel(), y.ravel(), z.ravel()
+    p["radius"][:] = 0.5
+    p["globalKeys"][:] = np.arange(n)
+    l = workloads.distance_links(p, precision, 1.06)
+    P = abi.default_params(precision=precision, waterLevel=-10.0, searchDistanceScale=9.0,
+                           breakTime=0.0, maxLoad=1e-6)
+    ref = oracle.port().run(P, p, l, 5)
+    for mode in ("fused", "split"):
+        res = gpu_run(P, p, l, 5, mode)
+        assert res[4]["max_neighbours"] > 300
+        assert_same(res, ref[0], ref[1], ref[3], ref[2] if mode == "split" else None)
