@@ -1,7 +1,8 @@
 """Benchmark of the HiDEM hot path: particle-steps/s on the 5.7M-particle calving slab.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
-                    [--impl ours|reference] [--workload slab|block]
+                    [--impl ours|reference] [--workload slab|block|ensemble]
+                    [--kernel auto|items|thread|thread-capped]
 
 A "step" is one timestep of the sample main loop (gridService, forces, integrate, link
 update) over the whole slab. `value` times K steps with the state resident in HBM (CUDA
@@ -13,6 +14,9 @@ kernel's event-timed duration. `cpu_baseline` times the reference's own CPU path
 With --gpus N > 1 (torchrun) every rank advances its own replica of the slab (the path
 has no exchange on one node for this workload; weak scaling).
 --impl reference times the reference's CPU implementation on this host's cores.
+--workload ensemble: 256 independent FCC blocks of 5k-80k particles advanced by one
+batched launch per timestep (runs of launches replayed from CUDA graphs); with --gpus N
+the blocks are split across the ranks by particle count (strong scaling, no exchange).
 """
 from __future__ import annotations
 
@@ -34,6 +38,10 @@ sys.path.insert(0, str(ROOT))
 # RTX 5090, HiDEM/Docs/Performance.md:68): 5,723,826 particles x 5000 steps / 25.83 s
 PUBLISHED_MIXED = 5723826 * 5000 / 25.83
 
+# step kernels of the library (hidem_set_step_kernel)
+KERNELS = {"auto": 0, "items": 1, "thread": 2, "thread-capped": 3}
+KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -42,7 +50,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["slab", "block"], default="slab")
+    ap.add_argument("--workload", choices=["slab", "block", "ensemble"], default="slab")
+    ap.add_argument("--blocks", type=int, default=256, help="ensemble: number of blocks")
+    ap.add_argument("--no-graphs", action="store_true", help="ensemble: plain launches")
+    ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped"],
+                    default="auto", help="step kernel (auto: timed on the first steps)")
     ap.add_argument("--slab", default="400,100,100",
                     help="slab size in metres x,y,z (smaller slabs for profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -207,8 +219,231 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_reference_ensemble(args):
+    """--impl reference --workload ensemble: the reference's CPU path block after block on
+    a bounded sample (the first blocks of the ensemble), particle-steps/s."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from hidem_b200 import abi, workloads
+    from oracle import oracle
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    if not oracle.reference_available(prec, fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+        return
+    blocks = workloads.ensemble(args.blocks, prec)
+    sample = blocks[:8]
+    tot_ps, tot_s, cores = 0, 0.0, 1
+    for P, p, l in sample:
+        sess = oracle.RefSession(P, p, l, fast=True)
+        sess.advance(max(args.warmup, 1))
+        secs = sess.advance(args.steps)
+        cores = sess.threads()
+        sess.close()
+        tot_ps += p["xCord"].shape[0] * args.steps
+        tot_s += secs
+    value = tot_ps / tot_s
+    n_all = sum(b[1]["xCord"].shape[0] for b in blocks)
+    line = {
+        "metric": "particle-steps/s (256-block ensemble)", "value": value,
+        "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * n_all / value, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32+f64pos" if prec == 1 else "f64", "data": "synthetic",
+        "config": {"workload": f"ensemble of {len(blocks)} FCC blocks, 5k-80k particles",
+                   "particles": n_all, "precision": args.precision},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{args.steps} timesteps of each of the first {len(sample)} blocks"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main_ensemble(args):
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    from hidem_b200 import abi, workloads
+    from hidem_b200.hidemlib import HiDEMBatch, HiDEMLib
+
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    all_blocks = workloads.ensemble(args.blocks, prec)
+    n_all = sum(b[1]["xCord"].shape[0] for b in all_blocks)
+    mine = workloads.ensemble_shard([b[1]["xCord"].shape[0] for b in all_blocks], world, rank)
+    blocks = [all_blocks[i] for i in mine]
+    n = sum(b[1]["xCord"].shape[0] for b in blocks)
+    L = sum(b[2]["state"].shape[0] for b in blocks)
+    kernel = KERNELS[args.kernel]
+
+    def open_all(src):
+        libs = []
+        for P, p, l in src:
+            lib = HiDEMLib(P, device=local)
+            lib.set_particles(p)
+            lib.set_links(l)
+            libs.append(lib)
+        if kernel != abi.STEP_KERNEL_AUTO:
+            libs[0].set_step_kernel(kernel)
+        return libs
+
+    libs = open_all(blocks)
+    batch = HiDEMBatch(libs, graphs=not args.no_graphs)
+    stream = torch.cuda.ExternalStream(batch.stream_handle)
+    batch.step(args.warmup)
+    st0 = [lib.stats() for lib in libs]
+    c0 = batch.counts()
+    pairs = sum(s["num_neighbour_pairs"] for s in st0)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    libs[0].profile(True)
+    e0.record(stream)
+    batch.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    kern_ms, kern_n = libs[0].profile_read()
+    libs[0].profile(False)
+    clk = clocks.stop()
+    c1 = batch.counts()
+    st1 = [lib.stats() for lib in libs]
+    launches = int(sum(b["kernel_launches"] for b in st1) - sum(a["kernel_launches"] for a in st0))
+    broken = [s["broken_links"] / max(1, s["num_links"]) for s in st1]
+    if pg:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    batch.close()
+    for lib in libs:
+        lib.close()
+
+    value = n_all * args.steps / (ms / 1e3)
+    bytes_step = workloads.algorithmic_bytes(n, L, pairs, prec)["total"]
+    # kernel time per step from the event pairs around each run of launches
+    kern_step_s = kern_ms / 1e3 / max(1, args.steps)
+    peak, peak_kind = measured_peak()
+    achieved = bytes_step / kern_step_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "kernel": "k_step_batch (" + KERNEL_NAMES[kernel if kernel else abi.STEP_KERNEL_THREAD_CAPPED] + ")",
+                "kernel_ms": kern_step_s * 1e3,
+                "algorithmic_bytes_per_launch": bytes_step}
+
+    e2e = None
+    if not args.no_e2e:
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.from_numpy(a[:1]).dtype, pin_memory=True)
+            out = t.numpy()
+            out[...] = a
+            return out, t
+        keep, host = [], []
+        for P, p, l in blocks:
+            pp, ll, oo = {}, {}, {}
+            for k, v in p.items():
+                pp[k], t = pinned(v)
+                keep.append(t)
+            for k, v in l.items():
+                ll[k], t = pinned(v)
+                keep.append(t)
+            for k, v in abi.empty_particles(p["xCord"].shape[0], prec).items():
+                oo[k], t = pinned(v)
+                keep.append(t)
+            host.append((P, pp, ll, oo))
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        libs2 = open_all([(P, pp, ll) for P, pp, ll, _ in host])
+        b2 = HiDEMBatch(libs2, graphs=not args.no_graphs)
+        b2.step(args.steps)
+        for lib, (_, _, _, oo) in zip(libs2, host):
+            lib.get_particles(oo)
+        for lib in libs2:
+            lib.synchronize()
+        el = time.perf_counter() - t0
+        b2.close()
+        for lib in libs2:
+            lib.close()
+        if pg:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            el = float(t.item())
+        h2d = sum(v.nbytes for _, pp, ll, _ in host for v in list(pp.values()) + list(ll.values()))
+        d2h = sum(v.nbytes for _, _, _, oo in host for v in oo.values())
+        e2e = {"value": n_all * args.steps / el, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "step": f"one C-ABI job per rank from pinned host arrays: create {len(blocks)} "
+                       f"contexts, upload, {args.steps} batched timesteps, download particles"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import oracle
+            P, p, l = blocks[0]
+            if oracle.reference_available(prec, fast=True):
+                sess = oracle.RefSession(P, p, l, fast=True)
+                sess.advance(1)
+                k = 20
+                secs = sess.advance(k)
+                cores = sess.threads()
+                sess.close()
+                nb = p["xCord"].shape[0]
+                cpu = {"value": nb * k / secs, "unit": "particle-steps/s", "cores": cores,
+                       "kind": "reference",
+                       "sample": f"{k} timesteps of block 0 ({nb} particles) after 1 warm-up"}
+        except Exception as ex:
+            cpu = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
+                   "sample": f"failed: {ex}"}
+
+    if pg:
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "particle-steps/s (256-block ensemble)", "value": value,
+        "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
+        "config": {"workload": f"ensemble of {len(all_blocks)} FCC blocks, 5k-80k particles "
+                               f"log-uniform, maxLoad lognormal(5e-4, 0.3)",
+                   "particles": n_all, "particles_rank0": n, "links_rank0": L,
+                   "precision": args.precision, "parallelism": f"blocks split over {world} ranks",
+                   "graphs": not args.no_graphs,
+                   "graph_replays": c1["graph_launches"] - c0["graph_launches"],
+                   "l2": "inputs larger than L2 (records + link ends > 126 MB)",
+                   "broken_fraction_rank0": {"min": float(np.min(broken)),
+                                             "median": float(np.median(broken)),
+                                             "max": float(np.max(broken))}},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.workload == "ensemble":
+        if args.impl == "reference":
+            run_reference_ensemble(args)
+        else:
+            main_ensemble(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -229,10 +464,13 @@ def main():
     L = l["state"].shape[0]
 
     lib = HiDEMLib(P, device=local)
+    lib.set_step_kernel(KERNELS[args.kernel])
     lib.set_particles(p)
     lib.set_links(l)
     stream = torch.cuda.ExternalStream(lib.stream_handle)
-    lib.step(args.warmup)
+    # warm-up: at least the autotuner's rounds, so the timed steps use its choice
+    warm = max(args.warmup, 12) if args.kernel == "auto" else args.warmup
+    lib.step(warm)
     lib.synchronize()
     st0 = lib.stats()
     pairs = st0["num_neighbour_pairs"]
@@ -255,6 +493,7 @@ def main():
     lib.profile(False)
     clk = clocks.stop()
     st1 = lib.stats()
+    step_kernel = lib.step_kernel()
     launches = int(st1["kernel_launches"] - st0["kernel_launches"])
     if pg:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -271,7 +510,8 @@ def main():
     dpps = profile_traffic(args.precision)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": (dpps * n) if dpps else None,
-                "peak_source": peak_kind, "kernel": "k_step<fused>",
+                "peak_source": peak_kind,
+                "kernel": "fused step, " + KERNEL_NAMES.get(step_kernel, "?") + " kernel",
                 "kernel_ms": kern_ms / max(kern_n, 1),
                 "algorithmic_bytes_per_launch": bytes_step}
 
@@ -298,6 +538,7 @@ def main():
         # the same K steps through the C ABI from host buffers (state upload, K steps,
         # particle state download)
         lib2 = HiDEMLib(P, device=local)
+        lib2.set_step_kernel(step_kernel)
         torch.cuda.synchronize()
         if pg:
             pg.barrier()
@@ -336,7 +577,7 @@ def main():
     line = {
         "metric": "particle-steps/s (5.7M slab)" if args.workload == "slab" else "particle-steps/s (32k block)",
         "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": (value / PUBLISHED_MIXED) if (prec == abi.PREC_MIXED and args.workload == "slab") else None,
         "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",

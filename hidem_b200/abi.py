@@ -20,6 +20,12 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 TYPE_FIXED = 0x40
 TYPE_FRONT = 0x80
+BATCH_GRAPHS = 1
+BATCH_PER_CONTEXT = 2
+STEP_KERNEL_AUTO = 0
+STEP_KERNEL_ITEMS = 1
+STEP_KERNEL_THREAD = 2
+STEP_KERNEL_THREAD_CAPPED = 3
 
 _d = C.c_double
 _i32 = C.c_int32
@@ -202,6 +208,15 @@ _PROTOS = [
     ("hidem_get_break_events", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64,
                                          C.POINTER(_i64)]),
     ("hidem_get_stats", C.c_int, [C.c_void_p, C.POINTER(HidemStats)]),
+    ("hidem_set_step_kernel", C.c_int, [C.c_void_p, _i32]),
+    ("hidem_get_step_kernel", _i32, [C.c_void_p]),
+    ("hidem_batch_create", C.c_int, [C.POINTER(C.c_void_p), _i32, _i32, C.POINTER(C.c_void_p)]),
+    ("hidem_batch_destroy", None, [C.c_void_p]),
+    ("hidem_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("hidem_batch_step", C.c_int, [C.c_void_p, _i32]),
+    ("hidem_batch_get_stream", C.c_void_p, [C.c_void_p]),
+    ("hidem_batch_counts", C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64),
+                                     C.POINTER(_i64)]),
     ("hidem_bin_cells_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64, _d,
                                           C.c_void_p, C.c_void_p, C.POINTER(_i64), C.POINTER(_d),
                                           C.c_void_p]),

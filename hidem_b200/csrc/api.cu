@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -108,6 +109,12 @@ struct hidem_ctx {
     long long regenCount = 0, lastRegen = -1;
     long long launches = 0;
     int smCount = 148;
+
+    // step kernel: fixed by the caller, or timed on the first fused steps (AUTO)
+    int stepKernel = HIDEM_STEP_KERNEL_AUTO;
+    int tunedKernel = HIDEM_STEP_KERNEL_AUTO;
+    int tuneStep = 0;
+    cudaEvent_t tuneEv[2 * 9] = {};
 };
 
 namespace {
@@ -492,18 +499,20 @@ hidem_status reduce_diff_now(hidem_ctx *ctx) {
     return HIDEM_OK;
 }
 
-// HiDEMLib::gridService (HiDEMLib.h:533-628) on one rank. `diffReady` says the
-// device words already hold this step's maxima (computed by the previous fused step).
-hidem_status grid_service(hidem_ctx *ctx, bool diffReady) {
+// Whether gridService at the current step reads the diff maxima (HiDEMLib.h:563-575).
+bool gs_wants_diff(const hidem_ctx *ctx) {
+    return ctx->P.gridRegenInterval == -1 && ctx->step % 10 == 0;
+}
+
+// The rest of HiDEMLib::gridService (HiDEMLib.h:533-628) on one rank, once the
+// accumulated-distance increment of this step (when gs_wants_diff) is known.
+hidem_status gs_finish(hidem_ctx *ctx, double currDist) {
     const long long t = ctx->step;
     bool regen = (t == ctx->startStep);
     if (ctx->P.gridRegenInterval != -1) {
         regen = ctx->P.gridRegenInterval > 0 && (t % ctx->P.gridRegenInterval) == 0;
     } else if (t % 10 == 0) {
-        if (!diffReady) TRY(reduce_diff_now(ctx));
-        double cd = 0;
-        TRY(read_diff_max(ctx, &cd));
-        ctx->accumulatedDist += cd;
+        ctx->accumulatedDist += currDist;
         if (ctx->accumulatedDist >= ctx->interactDist / 2.0) regen = true;
     }
     if (t == ctx->P.firstBalanceTimestep) regen = true;
@@ -514,6 +523,43 @@ hidem_status grid_service(hidem_ctx *ctx, bool diffReady) {
     }
     return HIDEM_OK;
 }
+
+// HiDEMLib::gridService on one rank. `diffReady` says the device words already hold this
+// step's maxima (computed by the previous fused step).
+hidem_status grid_service(hidem_ctx *ctx, bool diffReady) {
+    double cd = 0;
+    if (gs_wants_diff(ctx)) {
+        if (!diffReady) TRY(reduce_diff_now(ctx));
+        TRY(read_diff_max(ctx, &cd));
+    }
+    return gs_finish(ctx, cd);
+}
+
+// Whether gridService can do anything at the current step, and the number of steps
+// from the current one to the next step where it can.
+bool gs_due(const hidem_ctx *ctx) {
+    const long long t = ctx->step;
+    const long long iv = ctx->P.gridRegenInterval;
+    return !ctx->built || t == ctx->startStep || t == ctx->P.firstBalanceTimestep ||
+           (iv == -1 && t % 10 == 0) || (iv > 0 && t % iv == 0);
+}
+long long gs_next_due(const hidem_ctx *ctx) {
+    const long long t = ctx->step;
+    const long long iv = ctx->P.gridRegenInterval;
+    long long d = (long long)1 << 60;
+    if (iv == -1) d = 10 - ((t % 10) + 10) % 10;
+    else if (iv > 0) d = iv - ((t % iv) + iv) % iv;
+    if (ctx->P.firstBalanceTimestep > t) d = std::min<long long>(d, ctx->P.firstBalanceTimestep - t);
+    if (ctx->startStep > t) d = std::min<long long>(d, ctx->startStep - t);
+    return d;
+}
+
+template <class LP>
+const Consts<LP> &consts(hidem_ctx *ctx);
+template <>
+const Consts<float> &consts<float>(hidem_ctx *ctx) { return ctx->cf; }
+template <>
+const Consts<double> &consts<double>(hidem_ctx *ctx) { return ctx->cd; }
 
 template <class LP>
 StepArgs<LP> step_args(hidem_ctx *ctx) {
@@ -534,6 +580,8 @@ StepArgs<LP> step_args(hidem_ctx *ctx) {
     a.force = static_cast<LP *>(ctx->force);
     a.n = (int)ctx->n;
     a.step = ctx->step;
+    a.bendBreak = consts<LP>(ctx).bendBreak;
+    a.maxLoad = consts<LP>(ctx).maxLoad;
     a.diffMax = ctx->diffMax;
     a.events = ctx->events;
     a.eventCount = ctx->eventCount;
@@ -542,12 +590,6 @@ StepArgs<LP> step_args(hidem_ctx *ctx) {
     return a;
 }
 
-template <class LP>
-const Consts<LP> &consts(hidem_ctx *ctx);
-template <>
-const Consts<float> &consts<float>(hidem_ctx *ctx) { return ctx->cf; }
-template <>
-const Consts<double> &consts<double>(hidem_ctx *ctx) { return ctx->cd; }
 
 // HiDEMDefLinkBreakFunc gate of the sample main: t * dt > breakTime, in lp
 // (MainMeshBlock.cpp:312).
@@ -580,6 +622,58 @@ hidem_status profile_pair(hidem_ctx *ctx, cudaEvent_t *e0, cudaEvent_t *e1) {
     return HIDEM_OK;
 }
 
+// Step-kernel autotuner: the first kTuneRounds * 3 fused steps of a context cycle
+// through the candidate kernels with an event pair around each launch; after the rounds
+// have run, the fastest (summed over all but the first round) is kept.
+constexpr int kTuneCandidates[3] = {HIDEM_STEP_KERNEL_ITEMS, HIDEM_STEP_KERNEL_THREAD,
+                                    HIDEM_STEP_KERNEL_THREAD_CAPPED};
+constexpr int kTuneRounds = 3;
+
+int step_kernel_now(hidem_ctx *ctx, cudaEvent_t *e0, cudaEvent_t *e1) {
+    *e0 = *e1 = nullptr;
+    if (ctx->stepKernel != HIDEM_STEP_KERNEL_AUTO) return ctx->stepKernel;
+    if (ctx->tunedKernel != HIDEM_STEP_KERNEL_AUTO) return ctx->tunedKernel;
+    if (ctx->tuneStep < 3 * kTuneRounds) {
+        const int k = ctx->tuneStep++;
+        for (int q = 0; q < 2; ++q)
+            if (!ctx->tuneEv[2 * k + q] && cudaEventCreate(&ctx->tuneEv[2 * k + q]) != cudaSuccess)
+                ctx->tuneEv[2 * k + q] = nullptr;
+        *e0 = ctx->tuneEv[2 * k];
+        *e1 = ctx->tuneEv[2 * k + 1];
+        return kTuneCandidates[k % 3];
+    }
+    return HIDEM_STEP_KERNEL_THREAD;  // rounds done, choice made at the next sync
+}
+
+// the kernel of a launch outside the tuning rounds
+int step_kernel_settled(const hidem_ctx *ctx) {
+    if (ctx->stepKernel != HIDEM_STEP_KERNEL_AUTO) return ctx->stepKernel;
+    if (ctx->tunedKernel != HIDEM_STEP_KERNEL_AUTO) return ctx->tunedKernel;
+    return HIDEM_STEP_KERNEL_THREAD;
+}
+
+// called after the stream has been synchronised
+void step_kernel_resolve(hidem_ctx *ctx) {
+    if (ctx->stepKernel != HIDEM_STEP_KERNEL_AUTO || ctx->tunedKernel != HIDEM_STEP_KERNEL_AUTO ||
+        ctx->tuneStep < 3 * kTuneRounds)
+        return;
+    double t[3] = {0, 0, 0};
+    for (int k = 3; k < 3 * kTuneRounds; ++k) {
+        float ms = 0;
+        if (!ctx->tuneEv[2 * k] || !ctx->tuneEv[2 * k + 1] ||
+            cudaEventElapsedTime(&ms, ctx->tuneEv[2 * k], ctx->tuneEv[2 * k + 1]) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->tunedKernel = HIDEM_STEP_KERNEL_THREAD;
+            return;
+        }
+        t[k % 3] += ms;
+    }
+    int best = 0;
+    for (int q = 1; q < 3; ++q)
+        if (t[q] < t[best]) best = q;
+    ctx->tunedKernel = kTuneCandidates[best];
+}
+
 // n whole timesteps, one fused kernel each (MainMeshBlock.cpp:274-323).
 template <class LP>
 hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
@@ -603,10 +697,14 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
             CK(cudaMemsetAsync(ctx->diffMax, 0, 3 * sizeof(unsigned long long), ctx->stream));
             diffReady = true;
         }
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr, t0 = nullptr, t1 = nullptr;
+        const int kern = step_kernel_now(ctx, &t0, &t1);
         if (ctx->profile) TRY(profile_pair(ctx, &e0, &e1));
         if (e0) CK(cudaEventRecord(e0, ctx->stream));
-        launch_step<LP>(consts<LP>(ctx), a, true, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, ctx->stream);
+        if (t0) CK(cudaEventRecord(t0, ctx->stream));
+        launch_step<LP>(consts<LP>(ctx), a, true, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, kern,
+                        ctx->stream);
+        if (t1) CK(cudaEventRecord(t1, ctx->stream));
         if (e1) CK(cudaEventRecord(e1, ctx->stream));
         ctx->launches += 1;
         ctx->cur = 1 - ctx->cur;  // the slot order (type / orig / cellOf) is unchanged
@@ -616,7 +714,9 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
     }
     if (pending) TRY(link_update_now<LP>(ctx, pendingStep));
     CK(cudaGetLastError());
-    return check_device_error(ctx);
+    TRY(check_device_error(ctx));
+    step_kernel_resolve(ctx);
+    return HIDEM_OK;
 }
 
 template <class LP>
@@ -655,6 +755,372 @@ hidem_status upload_particles(hidem_ctx *ctx, const hidem_particle_soa *p, long 
     }
     launch_pack_records<LP>(s, (int)n, static_cast<PRec<LP> *>(ctx->rec[0]), st);
     ctx->launches += 1;
+    return HIDEM_OK;
+}
+
+}  // namespace
+
+// Many contexts advanced together (no counterpart in the reference): one launch per
+// timestep and group of contexts; runs of launches between two gridService points are
+// replayed from CUDA graphs.
+struct hidem_batch {
+    std::vector<hidem_ctx *> ctxs;
+    int mixed = 1;
+    int device = 0;
+    int flags = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    void *entries = nullptr;                 // device BatchEntry<LP>[nctx], then int[2 * nctx]
+    void *staging = nullptr;                 // pinned host copy of the entries
+    BatchCounter *ctr = nullptr;             // device launch counters, one per group
+    unsigned long long *diff = nullptr;      // device diff maxima, 3 words per context
+    unsigned long long *diffHost = nullptr;  // pinned
+    cudaEvent_t uploaded = nullptr;
+    bool uploadPending = false;
+    std::map<int, cudaGraphExec_t> graphs;   // by run length, for one launch shape
+    std::string shape;                       // the launch shape the graphs were captured for
+    // contexts that share every constant but the break thresholds form a group: one launch
+    // per group and step, the group's constants as kernel parameters
+    struct Group {
+        int first = 0, count = 0;             // entries [first, first + count)
+        int fbOffset = 0;                     // its CTA offsets in the offset array
+        long long blocks = 0;                 // CTAs of its launch
+        int maxC = 0, maxE = 0;
+        std::vector<unsigned char> consts;    // Consts<LP> of the group
+    };
+    std::vector<Group> groups;
+    std::vector<int> order;                  // context index of each entry
+    long long launches = 0, graphLaunches = 0, uploads = 0;
+};
+
+namespace {
+
+constexpr int kBatchMaxRun = 10;
+
+hidem_status bfail(hidem_batch *b, hidem_status s, const char *fmt, ...) {
+    char buf[640];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (b) b->err = buf;
+    return s;
+}
+
+#define BCK(call)                                                                            \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return bfail(b, HIDEM_ERR_CUDA, "%s failed: %s (%s:%d)", #call,                  \
+                         cudaGetErrorString(e_), __FILE__, __LINE__);                        \
+    } while (0)
+
+// a call on context `idx` failed: keep its text
+#define BTRY(expr)                                                                           \
+    do {                                                                                     \
+        hidem_status s_ = (expr);                                                            \
+        if (s_ != HIDEM_OK)                                                                  \
+            return bfail(b, s_, "context %d: %s", idx, b->ctxs[idx]->err.c_str());           \
+    } while (0)
+
+void batch_clear_graphs(hidem_batch *b) {
+    for (auto &g : b->graphs) cudaGraphExecDestroy(g.second);
+    b->graphs.clear();
+    b->shape.clear();
+}
+
+// For the length of one batch call every context queues its work on the batch's stream
+// and folds its diff maxima into the batch's array; both are given back on exit (after
+// the stream has drained, so the contexts' own streams see finished work).
+struct BatchBind {
+    hidem_batch *b;
+    std::vector<cudaStream_t> streams;
+    std::vector<unsigned long long *> diffs;
+    explicit BatchBind(hidem_batch *bb) : b(bb) {
+        for (size_t i = 0; i < b->ctxs.size(); ++i) {
+            hidem_ctx *c = b->ctxs[i];
+            streams.push_back(c->stream);
+            diffs.push_back(c->diffMax);
+            c->stream = b->stream;
+            c->diffMax = b->diff + 3 * i;
+        }
+    }
+    ~BatchBind() {
+        cudaStreamSynchronize(b->stream);
+        for (size_t i = 0; i < b->ctxs.size(); ++i) {
+            b->ctxs[i]->stream = streams[i];
+            b->ctxs[i]->diffMax = diffs[i];
+        }
+    }
+};
+
+// the kernel a batch run uses: the first context's fixed or tuned choice, else the
+// register-capped one-thread-per-particle kernel
+int batch_kernel(const hidem_batch *b) {
+    const hidem_ctx *c = b->ctxs[0];
+    if (c->stepKernel != HIDEM_STEP_KERNEL_AUTO) return c->stepKernel;
+    if (c->tunedKernel != HIDEM_STEP_KERNEL_AUTO) return c->tunedKernel;
+    return HIDEM_STEP_KERNEL_THREAD_CAPPED;
+}
+
+// Groups of contexts with equal constants apart from the break thresholds (compared
+// byte for byte; the constants are value-initialised and assigned field by field, so
+// their padding compares equal), with their CTA counts and row widths for `kernel`.
+template <class LP>
+void batch_group(hidem_batch *b, int kernel) {
+    const int nc = (int)b->ctxs.size();
+    const int per = batch_particles_per_cta(kernel);
+    std::vector<std::vector<unsigned char>> keys(nc);
+    for (int idx = 0; idx < nc; ++idx) {
+        Consts<LP> k;
+        std::memcpy(&k, &consts<LP>(b->ctxs[idx]), sizeof k);
+        k.bendBreak = LP(0);
+        k.maxLoad = LP(0);
+        const unsigned char *kb = reinterpret_cast<const unsigned char *>(&k);
+        keys[idx].assign(kb, kb + sizeof k);
+    }
+    b->groups.clear();
+    b->order.clear();
+    std::vector<char> done(nc, 0);
+    int fb = 0;
+    for (int idx = 0; idx < nc; ++idx) {
+        if (done[idx]) continue;
+        hidem_batch::Group g;
+        g.first = (int)b->order.size();
+        g.fbOffset = fb;
+        g.consts = keys[idx];
+        for (int j = idx; j < nc; ++j) {
+            if (done[j] || keys[j] != keys[idx]) continue;
+            done[j] = 1;
+            const hidem_ctx *c = b->ctxs[j];
+            b->order.push_back(j);
+            g.blocks += (c->n + per - 1) / per;
+            g.maxC = std::max(g.maxC, (int)c->maxNeigh);
+            g.maxE = std::max(g.maxE, (int)c->maxLinksPP);
+        }
+        g.count = (int)b->order.size() - g.first;
+        fb += g.count + 1;
+        b->groups.push_back(std::move(g));
+    }
+}
+
+// what identifies the launches of a run: graphs are re-captured when it changes
+std::string batch_shape(const hidem_batch *b, int kernel) {
+    std::string sh(reinterpret_cast<const char *>(&kernel), sizeof kernel);
+    for (const auto &g : b->groups) {
+        const long long v[6] = {g.first, g.count, g.fbOffset, g.blocks, g.maxC, g.maxE};
+        sh.append(reinterpret_cast<const char *>(v), sizeof v);
+        sh.append(g.consts.begin(), g.consts.end());
+    }
+    return sh;
+}
+
+template <class LP>
+hidem_status batch_upload(hidem_batch *b, const std::vector<char> &pending, int kernel) {
+    const int nc = (int)b->ctxs.size();
+    if (b->uploadPending) BCK(cudaEventSynchronize(b->uploaded));
+    BatchEntry<LP> *h = static_cast<BatchEntry<LP> *>(b->staging);
+    int *fb = reinterpret_cast<int *>(h + nc);
+    const int per = batch_particles_per_cta(kernel);
+    for (const auto &g : b->groups) {
+        int firstBlock = 0;
+        for (int q = 0; q < g.count; ++q) {
+            const int idx = b->order[g.first + q];
+            hidem_ctx *c = b->ctxs[idx];
+            BatchEntry<LP> e{};
+            e.a = step_args<LP>(c);
+            e.a.maxContacts = (int)c->maxNeigh;
+            e.a.maxEnds = (int)c->maxLinksPP;
+            e.rec[0] = recp<LP>(c, 0);
+            e.rec[1] = recp<LP>(c, 1);
+            e.step0 = c->step;
+            e.cur0 = c->cur;
+            e.pend0 = pending[idx] ? 1 : 0;
+            e.reduceEvery10 = c->P.gridRegenInterval == -1 ? 1 : 0;
+            h[g.first + q] = e;
+            fb[g.fbOffset + q] = firstBlock;
+            firstBlock += (int)((c->n + per - 1) / per);
+        }
+        fb[g.fbOffset + g.count] = firstBlock;
+    }
+    BCK(cudaMemcpyAsync(b->entries, h, sizeof(BatchEntry<LP>) * nc + sizeof(int) * 2 * nc,
+                        cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaEventRecord(b->uploaded, b->stream));
+    b->uploadPending = true;
+    BCK(cudaMemsetAsync(b->ctr, 0, sizeof(BatchCounter) * b->groups.size(), b->stream));
+    b->uploads += 1;
+    return HIDEM_OK;
+}
+
+template <class LP>
+void batch_enqueue_step(hidem_batch *b, int kernel) {
+    const int nc = (int)b->ctxs.size();
+    const BatchEntry<LP> *ent = static_cast<const BatchEntry<LP> *>(b->entries);
+    const int *fb = reinterpret_cast<const int *>(ent + nc);
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        const auto &g = b->groups[gi];
+        if (g.blocks == 0) continue;
+        Consts<LP> c;
+        std::memcpy(&c, g.consts.data(), sizeof c);
+        launch_step_batch<LP>(c, ent + g.first, fb + g.fbOffset, g.count, b->ctr + gi,
+                              (int)g.blocks, g.maxC, g.maxE, kernel, b->stream);
+    }
+}
+
+// `run` timesteps of the batch (one launch per group each), from a cached graph when
+// graphs are on
+template <class LP>
+hidem_status batch_launch_run(hidem_batch *b, int run, int kernel) {
+    const std::string sh = batch_shape(b, kernel);
+    if (sh != b->shape) {
+        batch_clear_graphs(b);
+        b->shape = sh;
+    }
+    if (!(b->flags & HIDEM_BATCH_GRAPHS)) {
+        for (int j = 0; j < run; ++j) batch_enqueue_step<LP>(b, kernel);
+        BCK(cudaGetLastError());
+        return HIDEM_OK;
+    }
+    auto it = b->graphs.find(run);
+    if (it == b->graphs.end()) {
+        cudaGraph_t g = nullptr;
+        BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        for (int j = 0; j < run; ++j) batch_enqueue_step<LP>(b, kernel);
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (le != cudaSuccess || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return bfail(b, HIDEM_ERR_CUDA, "capturing the batched step failed: %s",
+                         cudaGetErrorString(le != cudaSuccess ? le : ce));
+        }
+        cudaGraphExec_t x = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&x, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess)
+            return bfail(b, HIDEM_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ie));
+        it = b->graphs.emplace(run, x).first;
+    }
+    BCK(cudaGraphLaunch(it->second, b->stream));
+    b->graphLaunches += 1;
+    return HIDEM_OK;
+}
+
+// nsteps timesteps of every context: per step exactly the work hidem_step does for each
+// context alone (gridService, the fused step, the pending link update), in one launch
+// per group.
+template <class LP>
+hidem_status batch_run(hidem_batch *b, int nsteps) {
+    const int nc = (int)b->ctxs.size();
+    for (int idx = 0; idx < nc; ++idx) BCK(cudaStreamSynchronize(b->ctxs[idx]->stream));
+    BatchBind bind(b);
+    BCK(cudaMemsetAsync(b->diff, 0, 3 * sizeof(unsigned long long) * nc, b->stream));
+    std::vector<char> pending(nc, 0), diffReady(nc, 0);
+    std::vector<long long> pendStep(nc, 0);
+    bool dirty = true;
+    int s = 0;
+    while (s < nsteps) {
+        // gridService of every context due at its current step; one copy of the maxima
+        bool anyDue = false, anyRead = false;
+        for (int idx = 0; idx < nc; ++idx) {
+            hidem_ctx *c = b->ctxs[idx];
+            if (!gs_due(c)) continue;
+            anyDue = true;
+            if (gs_wants_diff(c)) {
+                anyRead = true;
+                if (!diffReady[idx]) BTRY(reduce_diff_now(c));
+            }
+        }
+        if (anyRead) {
+            BCK(cudaMemcpyAsync(b->diffHost, b->diff, 3 * sizeof(unsigned long long) * nc,
+                                cudaMemcpyDeviceToHost, b->stream));
+            BCK(cudaStreamSynchronize(b->stream));
+        }
+        if (anyDue) {
+            for (int idx = 0; idx < nc; ++idx) {
+                hidem_ctx *c = b->ctxs[idx];
+                if (!gs_due(c)) continue;
+                const double cd = gs_wants_diff(c) ? curr_dist<LP>(b->diffHost + 3 * idx) : 0.0;
+                BTRY(gs_finish(c, cd));
+            }
+            dirty = true;
+        }
+        long long run = nsteps - s;
+        for (int idx = 0; idx < nc; ++idx) run = std::min(run, gs_next_due(b->ctxs[idx]));
+        run = std::min<long long>(run, kBatchMaxRun);
+        const int kernel = batch_kernel(b);
+        bool oneLaunch = !(b->flags & HIDEM_BATCH_PER_CONTEXT);
+        if (oneLaunch) {
+            if (dirty || b->shape.compare(0, sizeof kernel, reinterpret_cast<const char *>(&kernel),
+                                          sizeof kernel) != 0) {
+                // layouts or the kernel changed: regroup and lay the entries out again
+                batch_group<LP>(b, kernel);
+                dirty = true;
+            }
+            for (const auto &g : b->groups) {
+                if (g.blocks > 0x7fffffffLL)
+                    return bfail(b, HIDEM_ERR_CAPACITY, "too many particles for one batched launch");
+                if (kernel == HIDEM_STEP_KERNEL_ITEMS && !batch_fits<LP>(g.maxC, g.maxE))
+                    oneLaunch = false;
+            }
+        }
+        hidem_ctx *c0 = b->ctxs[0];
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (c0->profile) {
+            const int idx = 0;
+            BTRY(profile_pair(c0, &e0, &e1));
+            BCK(cudaEventRecord(e0, b->stream));
+        }
+        if (oneLaunch) {
+            if (dirty) TRY(batch_upload<LP>(b, pending, kernel));
+            dirty = false;
+            TRY(batch_launch_run<LP>(b, (int)run, kernel));
+            b->launches += run * (long long)b->groups.size();
+            c0->launches += run * (long long)b->groups.size();
+        } else {
+            // per-context launches asked for, or rows too wide for the item kernel: the
+            // single-context launch sequence, context after context
+            dirty = true;
+            for (int j = 0; j < run; ++j) {
+                for (int idx = 0; idx < nc; ++idx) {
+                    hidem_ctx *c = b->ctxs[idx];
+                    const long long t = c->step + j;
+                    StepArgs<LP> a = step_args<LP>(c);
+                    const int par = (c->cur + j) & 1;
+                    a.in = recp<LP>(c, par);
+                    a.out = recp<LP>(c, par ^ 1);
+                    a.step = t;
+                    a.breakStep = t - 1;
+                    a.breakPending = j > 0 ? (break_active<LP>(c, t - 1) ? 1 : 0) : (pending[idx] ? 1 : 0);
+                    a.reduceDiff = (c->P.gridRegenInterval == -1 && (t + 1) % 10 == 0) ? 1 : 0;
+                    if (a.reduceDiff)
+                        BCK(cudaMemsetAsync(c->diffMax, 0, 3 * sizeof(unsigned long long), b->stream));
+                    launch_step<LP>(consts<LP>(c), a, true, (int)c->maxNeigh, (int)c->maxLinksPP,
+                                    step_kernel_settled(c), b->stream);
+                    c->launches += 1;
+                    b->launches += 1;
+                }
+            }
+            BCK(cudaGetLastError());
+        }
+        if (e1) BCK(cudaEventRecord(e1, b->stream));
+        // the host's copy of each context's step state (finalizeTs per step)
+        for (int idx = 0; idx < nc; ++idx) {
+            hidem_ctx *c = b->ctxs[idx];
+            for (long long j = 0; j < run; ++j) {
+                const long long t = c->step;
+                pending[idx] = break_active<LP>(c, t) ? 1 : 0;
+                pendStep[idx] = t;
+                diffReady[idx] = (c->P.gridRegenInterval == -1 && (t + 1) % 10 == 0) ? 1 : 0;
+                c->cur = 1 - c->cur;
+                c->step = t + 1;
+            }
+        }
+        s += (int)run;
+    }
+    for (int idx = 0; idx < nc; ++idx)
+        if (pending[idx]) BTRY(link_update_now<LP>(b->ctxs[idx], pendStep[idx]));
+    BCK(cudaGetLastError());
+    for (int idx = 0; idx < nc; ++idx) BTRY(check_device_error(b->ctxs[idx]));
     return HIDEM_OK;
 }
 
@@ -800,6 +1266,8 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->diffMax);
     dfree(ctx->errorFlag);
     for (cudaEvent_t e : ctx->evPool) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->tuneEv)
+        if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1002,12 +1470,15 @@ hidem_status hidem_compute_forces(hidem_ctx *ctx) {
     if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
     CK(cudaSetDevice(ctx->device));
     if (!ctx->built) TRY(do_rebuild(ctx));
+    const int kern = step_kernel_settled(ctx);
     if (ctx->mixed) {
         StepArgs<float> a = step_args<float>(ctx);
-        launch_step<float>(ctx->cf, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, ctx->stream);
+        launch_step<float>(ctx->cf, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, kern,
+                           ctx->stream);
     } else {
         StepArgs<double> a = step_args<double>(ctx);
-        launch_step<double>(ctx->cd, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, ctx->stream);
+        launch_step<double>(ctx->cd, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, kern,
+                            ctx->stream);
     }
     ctx->launches += 1;
     CK(cudaGetLastError());
@@ -1303,6 +1774,118 @@ hidem_status hidem_get_stats(hidem_ctx *ctx, hidem_stats *o) {
         CK(cudaStreamSynchronize(ctx->stream));
         o->broken_links = (int64_t)total;
     }
+    return HIDEM_OK;
+}
+
+hidem_status hidem_set_step_kernel(hidem_ctx *ctx, int32_t kernel) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (kernel < HIDEM_STEP_KERNEL_AUTO || kernel > HIDEM_STEP_KERNEL_THREAD_CAPPED)
+        return fail(ctx, HIDEM_ERR_ARG, "unknown step kernel %d", (int)kernel);
+    ctx->stepKernel = kernel;
+    return HIDEM_OK;
+}
+
+int32_t hidem_get_step_kernel(const hidem_ctx *ctx) {
+    if (!ctx) return -1;
+    return ctx->stepKernel != HIDEM_STEP_KERNEL_AUTO ? ctx->stepKernel : ctx->tunedKernel;
+}
+
+hidem_status hidem_batch_create(hidem_ctx *const *ctxs, int32_t nctx, int32_t flags,
+                                hidem_batch **out) {
+    g_create_error.clear();
+    if (!out) {
+        g_create_error = "out is NULL";
+        return HIDEM_ERR_ARG;
+    }
+    *out = nullptr;
+    if (!ctxs || nctx <= 0) {
+        g_create_error = "no contexts";
+        return HIDEM_ERR_ARG;
+    }
+    if (flags & ~(HIDEM_BATCH_GRAPHS | HIDEM_BATCH_PER_CONTEXT)) {
+        g_create_error = "unknown batch flags";
+        return HIDEM_ERR_ARG;
+    }
+    for (int i = 0; i < nctx; ++i) {
+        if (!ctxs[i]) {
+            g_create_error = "context " + std::to_string(i) + " is NULL";
+            return HIDEM_ERR_ARG;
+        }
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == ctxs[i]) {
+                g_create_error = "context " + std::to_string(i) + " appears twice";
+                return HIDEM_ERR_ARG;
+            }
+        if (ctxs[i]->device != ctxs[0]->device || ctxs[i]->mixed != ctxs[0]->mixed) {
+            g_create_error = "contexts of one batch must share the device and the precision";
+            return HIDEM_ERR_ARG;
+        }
+    }
+    hidem_batch *b = new hidem_batch();
+    b->ctxs.assign(ctxs, ctxs + nctx);
+    b->mixed = ctxs[0]->mixed;
+    b->device = ctxs[0]->device;
+    b->flags = flags;
+    const size_t eb = (b->mixed ? sizeof(BatchEntry<float>) : sizeof(BatchEntry<double>)) * (size_t)nctx +
+                      sizeof(int) * 2 * (size_t)nctx;
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&b->entries, eb);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->staging, eb);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->ctr, sizeof(BatchCounter) * (size_t)nctx);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->diff, 3 * sizeof(unsigned long long) * (size_t)nctx);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&b->diffHost, 3 * sizeof(unsigned long long) * (size_t)nctx);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->uploaded, cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+        if (b->mixed) prepare_step_batch<float>();
+        else prepare_step_batch<double>();
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        g_create_error = std::string("batch setup failed: ") + cudaGetErrorString(e);
+        hidem_batch_destroy(b);
+        return HIDEM_ERR_CUDA;
+    }
+    *out = b;
+    return HIDEM_OK;
+}
+
+void hidem_batch_destroy(hidem_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_clear_graphs(b);
+    if (b->uploaded) cudaEventDestroy(b->uploaded);
+    if (b->entries) cudaFree(b->entries);
+    if (b->staging) cudaFreeHost(b->staging);
+    if (b->ctr) cudaFree(b->ctr);
+    if (b->diff) cudaFree(b->diff);
+    if (b->diffHost) cudaFreeHost(b->diffHost);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char *hidem_batch_last_error(const hidem_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+void *hidem_batch_get_stream(hidem_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+hidem_status hidem_batch_step(hidem_batch *b, int32_t nsteps) {
+    if (!b) return HIDEM_ERR_ARG;
+    b->err.clear();
+    if (nsteps < 0) return bfail(b, HIDEM_ERR_ARG, "negative step count");
+    for (size_t i = 0; i < b->ctxs.size(); ++i)
+        if (!b->ctxs[i]->haveParticles || !b->ctxs[i]->haveLinks)
+            return bfail(b, HIDEM_ERR_STATE, "context %d: particles and links must be set", (int)i);
+    BCK(cudaSetDevice(b->device));
+    return b->mixed ? batch_run<float>(b, nsteps) : batch_run<double>(b, nsteps);
+}
+
+hidem_status hidem_batch_counts(const hidem_batch *b, int64_t *launches, int64_t *graph_launches,
+                                int64_t *uploads) {
+    if (!b) return HIDEM_ERR_ARG;
+    if (launches) *launches = b->launches;
+    if (graph_launches) *graph_launches = b->graphLaunches;
+    if (uploads) *uploads = b->uploads;
     return HIDEM_OK;
 }
 

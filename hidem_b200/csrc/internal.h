@@ -115,6 +115,7 @@ struct StepArgs {
     long long eventCap;
     int *errorFlag;
     int maxContacts, maxEnds; // widest rows of this layout
+    LP bendBreak, maxLoad;    // HiDEMDefLinkBreakFunc thresholds (per context in a batch)
 };
 
 }  // namespace hidem

@@ -393,39 +393,102 @@ __global__ void k_side_fill(const int *__restrict__ orig, int n, const int *__re
 
 // ------------------------------------------------------------------ timestep
 
+// The first CHUNKS 16-byte chunks of a record (the fields a functor reads); the rest of
+// the returned record is left unset and must not be read.
+template <class LP, int CHUNKS>
+__device__ __forceinline__ PRec<LP> load_rec_head(const PRec<LP> *p) {
+    PRec<LP> r;
+    const int4 *src = reinterpret_cast<const int4 *>(p);
+    int4 *dst = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+    for (int k = 0; k < CHUNKS; ++k) dst[k] = __ldg(src + k);
+    return r;
+}
+// chunks holding x, y, z, d[6], r
+template <class LP>
+constexpr int kContactChunks = (int)((3 * sizeof(double) + 7 * sizeof(LP) + 15) / 16);
+
 // One particle per thread. FUSED: previous step's link update (if pending), contacts,
 // link ends, integrate, write the record to the other buffer. Split (FUSED=false):
 // contacts and link ends only, forces to a.force (HiDEMLib::computePartForce).
+// Both item loops are software-pipelined: while item k is evaluated, the partner record
+// (and for link ends the CT state, link state and initial length) of item k + 1 and the
+// index of item k + 2 are already in flight, and the first link end's loads go out behind
+// the last contact, so each thread keeps its dependent loads outstanding behind its
+// arithmetic. The functors still run in the reference's order per particle.
 template <class LP, bool FUSED>
-__global__ void __launch_bounds__(kStepThreads)
-    k_step(const Consts<LP> c, const StepArgs<LP> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void step_thread_particle(const Consts<LP> &c, const StepArgs<LP> &a,
+                                                     const int i) {
     const bool live = i < a.n;
     LP dmax[3] = {LP(0), LP(0), LP(0)};
     if (live) {
         PRec<LP> me = load_rec(a.in + i);
         const uint32_t cnt = __ldg(a.counts + i);
+        const uint8_t ty = FUSED ? __ldg(a.type + i) : uint8_t(0);
         const int nn = (int)(cnt & 0xffffu), ns = (int)(cnt >> 16);
         LP F[6] = {0, 0, 0, 0, 0, 0};
+        constexpr int HC = kContactChunks<LP>;
 
-        const long long nbase = __ldg(a.nOff + (i >> 5)) + (i & 31);
+        const int32_t *nb = a.nbr + __ldg(a.nOff + (i >> 5)) + (i & 31);
+        const long long sbase = __ldg(a.sOff + (i >> 5)) + (i & 31);
+        PRec<LP> o;
+        int jn = 0;
+        if (nn > 0) o = load_rec_head<LP, HC>(a.in + __ldg(nb));
+        if (nn > 1) jn = __ldg(nb + kWarp);
+        // first link end's partner word while the contacts run
+        uint32_t pwn = (ns > 0) ? __ldg(a.sPartner + sbase) : 0u;
+        PRec<LP> o2;
+        uint8_t stn = 0;
+        LP ctn[6] = {0, 0, 0, 0, 0, 0};
+        LP l0n = LP(0);
+        uint32_t pwnn = 0;
+        const bool brk = FUSED && a.breakPending;
+        // the first link end's partner record, state and CT go out behind the last contact
+        auto first_side = [&]() {
+            if (ns > 0) {
+                o2 = load_rec(a.in + (pwn & kSlotMask));
+                stn = a.sState[sbase];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) ctn[q] = a.ct[q][sbase];
+                if (brk) l0n = __ldg(a.sL0 + sbase);
+                if (ns > 1) pwnn = __ldg(a.sPartner + sbase + kWarp);
+            }
+        };
+        if (nn == 0) first_side();
         for (int k = 0; k < nn; ++k) {
-            const int j = __ldg(a.nbr + nbase + (long long)k * kWarp);
-            const PRec<LP> o = load_rec(a.in + j);
-            contact_pair<LP>(c, LP(1), (LP)(me.x - o.x), (LP)(me.y - o.y), (LP)(me.z - o.z), me.d,
-                             me.r, o.d, o.r, F);
+            const PRec<LP> cur = o;
+            if (k + 1 < nn) {
+                o = load_rec_head<LP, HC>(a.in + jn);
+                if (k + 2 < nn) jn = __ldg(nb + (k + 2) * kWarp);
+            } else {
+                first_side();
+            }
+            contact_pair<LP>(c, LP(1), (LP)(me.x - cur.x), (LP)(me.y - cur.y), (LP)(me.z - cur.z),
+                             me.d, me.r, cur.d, cur.r, F);
         }
 
-        const long long sbase = __ldg(a.sOff + (i >> 5)) + (i & 31);
         for (int k = 0; k < ns; ++k) {
             const long long si = sbase + (long long)k * kWarp;
-            const uint32_t pw = __ldg(a.sPartner + si);
-            const PRec<LP> o = load_rec(a.in + (pw & kSlotMask));
-            uint8_t st = a.sState[si];
-            if (FUSED && a.breakPending && st != 0) {
-                const LP L0 = __ldg(a.sL0 + si);
-                const uint8_t nst = (pw & kSideIsB) ? break_link<LP>(c, o, me, st, L0)
-                                                    : break_link<LP>(c, me, o, st, L0);
+            const PRec<LP> cur = o2;
+            const uint32_t pw = pwn;
+            uint8_t st = stn;
+            const LP L0 = l0n;
+            LP CT[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) CT[q] = ctn[q];
+            if (k + 1 < ns) {
+                pwn = pwnn;
+                o2 = load_rec(a.in + (pwn & kSlotMask));
+                stn = a.sState[si + kWarp];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) ctn[q] = a.ct[q][si + kWarp];
+                if (brk) l0n = __ldg(a.sL0 + si + kWarp);
+                if (k + 2 < ns) pwnn = __ldg(a.sPartner + si + 2 * kWarp);
+            }
+            if (brk && st != 0) {
+                const uint8_t nst =
+                    (pw & kSideIsB) ? break_link<LP>(a.bendBreak, a.maxLoad, cur, me, st, L0)
+                                    : break_link<LP>(a.bendBreak, a.maxLoad, me, cur, st, L0);
                 if (nst != st) {
                     a.sState[si] = nst;
                     if (nst == 0 && !(pw & kSideIsB)) {
@@ -437,17 +500,14 @@ __global__ void __launch_bounds__(kStepThreads)
                 }
             }
             const LP mask = (st == 0) ? LP(0) : LP(1);
-            LP CT[6];
-#pragma unroll
-            for (int q = 0; q < 6; ++q) CT[q] = a.ct[q][si];
-            beam_side<LP>(c, mask, (LP)(me.x - o.x), (LP)(me.y - o.y), (LP)(me.z - o.z), me.d, o.d,
-                          CT, F);
+            beam_side<LP>(c, mask, (LP)(me.x - cur.x), (LP)(me.y - cur.y), (LP)(me.z - cur.z),
+                          me.d, cur.d, CT, F);
 #pragma unroll
             for (int q = 0; q < 6; ++q) a.ct[q][si] = CT[q];
         }
 
         if (FUSED) {
-            integrate_particle<LP>(c, me, __ldg(a.type + i), F);
+            integrate_particle<LP>(c, me, ty, F);
             store_rec(a.out + i, me);
             dmax[0] = me.d[0] > LP(0) ? me.d[0] : LP(0);
             dmax[1] = me.d[1] > LP(0) ? me.d[1] : LP(0);
@@ -468,6 +528,20 @@ __global__ void __launch_bounds__(kStepThreads)
             if ((threadIdx.x & 31) == 0 && v > LP(0)) atomicMax(a.diffMax + q, max_bits(v));
         }
     }
+}
+
+// CTAs per SM the register-capped variant asks the compiler for: 5 (96 registers) in the
+// mixed build, 3 (168 registers) in fp64 — each the tightest cap that spills little.
+template <class LP>
+constexpr int kCapBlocks = sizeof(LP) == 4 ? 5 : 3;
+// and the plain variant: 4 CTAs (128 registers) in the mixed build, no cap in fp64
+template <class LP>
+constexpr int kThreadBlocks = sizeof(LP) == 4 ? 4 : 1;
+
+template <class LP, bool FUSED, int MINB>
+__global__ void __launch_bounds__(kStepThreads, MINB)
+    k_step(const Consts<LP> c, const StepArgs<LP> a) {
+    step_thread_particle<LP, FUSED>(c, a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---- shared-memory staging with bulk copies (cp.async.bulk + mbarrier) ----
@@ -630,8 +704,9 @@ __device__ __forceinline__ void step_items_block(const Consts<LP> &c, const Step
 #pragma unroll
                 for (int u = 0; u < 3; ++u) me.th[u] = od[(7 + u) * 32 + lane];
                 const LP L0 = sl0[q];
-                const uint8_t nst = (pw & kSideIsB) ? break_link<LP>(c, o, me, st, L0)
-                                                    : break_link<LP>(c, me, o, st, L0);
+                const uint8_t nst =
+                    (pw & kSideIsB) ? break_link<LP>(a.bendBreak, a.maxLoad, o, me, st, L0)
+                                    : break_link<LP>(a.bendBreak, a.maxLoad, me, o, st, L0);
                 if (nst != st) {
                     a.sState[si] = nst;
                     if (nst == 0 && !(pw & kSideIsB)) {
@@ -713,22 +788,67 @@ __global__ void __launch_bounds__(kItemThreads)
     step_items_block<LP, FUSED>(c, a, blockIdx.x, smem);
 }
 
-// One fused step of many independent contexts in one launch: CTA b belongs to the entry
-// whose block range [firstBlock, next firstBlock) holds b; each entry carries its own
-// constants, buffers and layout (the dynamic shared memory is the largest entry's).
-template <class LP>
-__global__ void __launch_bounds__(kItemThreads)
-    k_step_batch(const BatchEntry<LP> *__restrict__ entries, int nentries) {
+// One fused step of many independent contexts in one launch. CTA b belongs to the entry
+// whose CTA range [firstBlocks[e], firstBlocks[e + 1]) holds b; all entries share the
+// launch's constants except the break thresholds (in each entry's arguments), and each
+// entry's per-step arguments are derived from the run counter the way the single-context
+// host loop sets them: records alternate between the two buffers, the link update of the
+// previous step is applied first once the break gate t * dt > breakTime was open at that
+// step (MainMeshBlock.cpp:312), the diff maxima are folded on steps t with
+// (t + 1) % 10 == 0 and cleared on steps with t % 10 == 0 (after the host has read them
+// at the start of that step). KIND selects the per-CTA body: the item kernel (32
+// particles per CTA, dynamic shared memory for the widest entry) or one thread per
+// particle (kStepThreads particles per CTA, registers capped or not).
+template <class LP, int KIND>
+__global__ void __launch_bounds__(KIND == HIDEM_STEP_KERNEL_ITEMS ? kItemThreads : kStepThreads,
+                                  KIND == HIDEM_STEP_KERNEL_THREAD_CAPPED ? kCapBlocks<LP>
+                                  : KIND == HIDEM_STEP_KERNEL_THREAD      ? kThreadBlocks<LP>
+                                                                          : 1)
+    k_step_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
+                 const int *__restrict__ firstBlocks, int nentries, BatchCounter *__restrict__ ctr,
+                 int totalBlocks) {
     extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int sRun, sEntry;
     const int b = blockIdx.x;
-    int lo = 0, hi = nentries - 1;
-    while (lo < hi) {  // last entry with firstBlock <= b
-        const int mid = (lo + hi + 1) >> 1;
-        if (entries[mid].firstBlock <= b) lo = mid;
-        else hi = mid - 1;
+    if (threadIdx.x == 0) {
+        sRun = *reinterpret_cast<volatile int *>(&ctr->s);
+        int lo = 0, hi = nentries - 1;
+        while (lo < hi) {  // last entry with firstBlocks[e] <= b
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(firstBlocks + mid) <= b) lo = mid;
+            else hi = mid - 1;
+        }
+        sEntry = lo;
     }
-    const BatchEntry<LP> &e = entries[lo];
-    step_items_block<LP, true>(e.c, e.a, b - e.firstBlock, smem);
+    __syncthreads();
+    const int s = sRun;
+    const BatchEntry<LP> &e = entries[sEntry];
+    StepArgs<LP> a = e.a;
+    const int par = (e.cur0 + s) & 1;
+    a.in = e.rec[par];
+    a.out = e.rec[par ^ 1];
+    a.step = e.step0 + s;
+    a.breakStep = a.step - 1;
+    a.breakPending = (s > 0) ? ((LP)((LP)a.breakStep * c.dt) > c.breakTime ? 1 : 0) : e.pend0;
+    a.reduceDiff = (e.reduceEvery10 && (a.step + 1) % 10 == 0) ? 1 : 0;
+    const int lb = b - __ldg(firstBlocks + sEntry);
+    if (e.reduceEvery10 && a.step % 10 == 0 && lb == 0 && threadIdx.x < 3)
+        a.diffMax[threadIdx.x] = 0ull;
+    if (KIND == HIDEM_STEP_KERNEL_ITEMS)
+        step_items_block<LP, true>(c, a, lb, smem);
+    else
+        step_thread_particle<LP, true>(c, a, lb * kStepThreads + threadIdx.x);
+    // the last CTA to finish advances the counter for the next launch of the run
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int prev = atomicAdd(&ctr->done, 1u);
+        if (prev == (unsigned int)totalBlocks - 1u) {
+            ctr->done = 0u;
+            ctr->s = s + 1;
+            __threadfence();
+        }
+    }
 }
 
 // HiDEMLib::applyForce with the integrate step, in place (split path).
@@ -887,12 +1007,12 @@ void launch_side_fill(const int *orig, int n, const int *slotOf, const int *plSt
 
 template <class LP>
 void launch_step(const Consts<LP> &c, const StepArgs<LP> &a0, bool fused, int maxContacts,
-                 int maxEnds, cudaStream_t s) {
+                 int maxEnds, int kernel, cudaStream_t s) {
     StepArgs<LP> a = a0;
     a.maxContacts = maxContacts;
     a.maxEnds = maxEnds;
     const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds);
-    if (L.total <= kItemSmemLimit) {
+    if (kernel == HIDEM_STEP_KERNEL_ITEMS && L.total <= kItemSmemLimit) {
         static bool configured[2] = {false, false};
         if (!configured[fused ? 1 : 0]) {
             if (fused)
@@ -908,12 +1028,19 @@ void launch_step(const Consts<LP> &c, const StepArgs<LP> &a0, bool fused, int ma
             k_step_items<LP, false><<<nb, kItemThreads, L.total, s>>>(c, a);
         return;
     }
-    // rows too wide for the shared-memory buffers: one thread per particle
-    int nb = nblk(a.n, kStepThreads);
-    if (fused)
-        k_step<LP, true><<<nb, kStepThreads, 0, s>>>(c, a);
-    else
-        k_step<LP, false><<<nb, kStepThreads, 0, s>>>(c, a);
+    // one thread per particle (also for rows too wide for the item kernel's buffers)
+    const int nb = nblk(a.n, kStepThreads);
+    if (kernel == HIDEM_STEP_KERNEL_THREAD_CAPPED) {
+        if (fused)
+            k_step<LP, true, kCapBlocks<LP>><<<nb, kStepThreads, 0, s>>>(c, a);
+        else
+            k_step<LP, false, kCapBlocks<LP>><<<nb, kStepThreads, 0, s>>>(c, a);
+    } else {
+        if (fused)
+            k_step<LP, true, kThreadBlocks<LP>><<<nb, kStepThreads, 0, s>>>(c, a);
+        else
+            k_step<LP, false, kThreadBlocks<LP>><<<nb, kStepThreads, 0, s>>>(c, a);
+    }
 }
 
 template <class LP>
@@ -922,15 +1049,30 @@ bool batch_fits(int maxContacts, int maxEnds) {
 }
 
 template <class LP>
-void launch_step_batch(const BatchEntry<LP> *entries, int nentries, int totalBlocks,
-                       int maxContacts, int maxEnds, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_step_batch<LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kItemSmemLimit);
-        configured = true;
+void prepare_step_batch() {
+    cudaFuncSetAttribute(k_step_batch<LP, HIDEM_STEP_KERNEL_ITEMS>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kItemSmemLimit);
+}
+
+int batch_particles_per_cta(int kernel) {
+    return kernel == HIDEM_STEP_KERNEL_ITEMS ? 32 : kStepThreads;
+}
+
+template <class LP>
+void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
+                       int nentries, BatchCounter *ctr, int totalBlocks, int maxContacts,
+                       int maxEnds, int kernel, cudaStream_t s) {
+    if (kernel == HIDEM_STEP_KERNEL_ITEMS) {
+        const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds);
+        k_step_batch<LP, HIDEM_STEP_KERNEL_ITEMS><<<totalBlocks, kItemThreads, L.total, s>>>(
+            c, entries, firstBlocks, nentries, ctr, totalBlocks);
+    } else if (kernel == HIDEM_STEP_KERNEL_THREAD_CAPPED) {
+        k_step_batch<LP, HIDEM_STEP_KERNEL_THREAD_CAPPED><<<totalBlocks, kStepThreads, 0, s>>>(
+            c, entries, firstBlocks, nentries, ctr, totalBlocks);
+    } else {
+        k_step_batch<LP, HIDEM_STEP_KERNEL_THREAD><<<totalBlocks, kStepThreads, 0, s>>>(
+            c, entries, firstBlocks, nentries, ctr, totalBlocks);
     }
-    const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds);
-    k_step_batch<LP><<<totalBlocks, kItemThreads, L.total, s>>>(entries, nentries);
 }
 
 template <class LP>
@@ -971,10 +1113,12 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
                                        const uint8_t *, const int *, const int *, const LP *,      \
                                        const int *, const SideView<LP> &, const long long *,       \
                                        const SideView<LP> &, int *, cudaStream_t);                 \
-    template void launch_step<LP>(const Consts<LP> &, const StepArgs<LP> &, bool, int, int,          \
-                                  cudaStream_t);   \
+    template void launch_step<LP>(const Consts<LP> &, const StepArgs<LP> &, bool, int, int, int,     \
+                                  cudaStream_t);                                                   \
     template bool batch_fits<LP>(int, int);                                                        \
-    template void launch_step_batch<LP>(const BatchEntry<LP> *, int, int, int, int, cudaStream_t);  \
+    template void prepare_step_batch<LP>();                                                        \
+    template void launch_step_batch<LP>(const Consts<LP> &, const BatchEntry<LP> *, const int *,     \
+                                        int, BatchCounter *, int, int, int, int, cudaStream_t);    \
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \

@@ -100,24 +100,47 @@ void launch_side_fill(const int *orig, int n, const int *slotOf, const int *plSt
                       const long long *sOff, const SideView<LP> &newS, int *sideSlotNew,
                       cudaStream_t s);
 // One timestep's forces (fused: + previous link update, integrate, record swap) for
-// rows of at most maxContacts contacts and maxEnds link ends.
+// rows of at most maxContacts contacts and maxEnds link ends, by the kernel `kernel`
+// (HIDEM_STEP_KERNEL_*, not AUTO; the item kernel falls back to one thread per particle
+// for rows too wide for its shared-memory buffers).
 template <class LP>
 void launch_step(const Consts<LP> &c, const StepArgs<LP> &a, bool fused, int maxContacts,
-                 int maxEnds, cudaStream_t s);
-// One context's share of a batched step launch.
+                 int maxEnds, int kernel, cudaStream_t s);
+// One context's share of a batched step launch (the constants other than the break
+// thresholds, which travel in `a`, are the launch's). The per-step fields of `a` (in, out,
+// step, breakPending, breakStep, reduceDiff) are not read: launch s of a run derives them
+// from the state at its start (rec, cur0, step0, pend0) and s, the way the host loop of a
+// single context sets them, so a run of launches needs no host work between steps and can
+// be captured as one CUDA graph.
 template <class LP>
 struct BatchEntry {
-    Consts<LP> c;
     StepArgs<LP> a;
-    int firstBlock;  // first CTA of this context in the launch
+    PRec<LP> *rec[2];   // the context's two record buffers
+    long long step0;    // timestep of launch 0
+    int cur0;           // record buffer holding the state at launch 0
+    int pend0;          // link update of step0 - 1 still to apply at launch 0
+    int reduceEvery10;  // gridService reads the diff maxima every 10 steps
+};
+// Launch counter shared by a run of batched launches: launch s reads s; the last CTA to
+// finish sets s + 1 for the next launch in the stream.
+struct BatchCounter {
+    int s;
+    unsigned int done;
 };
 // whether rows of these widths run in the item kernel (else: per-context launches)
 template <class LP>
 bool batch_fits(int maxContacts, int maxEnds);
-// entries: device array; maxContacts / maxEnds: the widest over all entries (shared memory)
+// sets the item kernel's shared-memory limit (call once before a launch is captured)
 template <class LP>
-void launch_step_batch(const BatchEntry<LP> *entries, int nentries, int totalBlocks,
-                       int maxContacts, int maxEnds, cudaStream_t s);
+void prepare_step_batch();
+// particles per CTA of the batch kernel `kernel` (HIDEM_STEP_KERNEL_*, not AUTO)
+int batch_particles_per_cta(int kernel);
+// entries, firstBlocks (nentries + 1 CTA offsets): device arrays; maxContacts / maxEnds:
+// the widest rows over all entries (shared memory of the item kernel)
+template <class LP>
+void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
+                       int nentries, BatchCounter *ctr, int totalBlocks, int maxContacts,
+                       int maxEnds, int kernel, cudaStream_t s);
 
 template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,

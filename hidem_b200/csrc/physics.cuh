@@ -143,10 +143,12 @@ __device__ __forceinline__ void beam_side(const Consts<LP> &c, LP mask, LP xDist
 }
 
 // Link break test: HiDEMDefLinkBreakFunc::operator() (HiDEMDefaultFunctions.h:207-242)
-// with end A as particle 1 and end B as particle 2. Returns the new state.
+// with end A as particle 1 and end B as particle 2 and the functor's two thresholds.
+// Returns the new state.
 template <class LP>
-__device__ __forceinline__ uint8_t break_link(const Consts<LP> &c, const PRec<LP> &a,
-                                              const PRec<LP> &b, uint8_t state, LP initialLen) {
+__device__ __forceinline__ uint8_t break_link(const LP bendBreak, const LP maxLoad,
+                                              const PRec<LP> &a, const PRec<LP> &b,
+                                              uint8_t state, LP initialLen) {
     if (state == 0) return 0;
     LP xDist = (LP)(a.x - b.x);
     LP yDist = (LP)(a.y - b.y);
@@ -157,8 +159,13 @@ __device__ __forceinline__ uint8_t break_link(const Consts<LP> &c, const PRec<LP
     LP az = labs_(a.th[2] - b.th[2]);
     LP myz = (ay < az) ? az : ay;  // std::max(ay, az)
     LP maxBend = (ax < myz) ? myz : ax;
-    LP load = (stretchLength - initialLen) / initialLen + c.bendBreak * maxBend;
-    return (load >= c.maxLoad) ? uint8_t(0) : state;
+    LP load = (stretchLength - initialLen) / initialLen + bendBreak * maxBend;
+    return (load >= maxLoad) ? uint8_t(0) : state;
+}
+template <class LP>
+__device__ __forceinline__ uint8_t break_link(const Consts<LP> &c, const PRec<LP> &a,
+                                              const PRec<LP> &b, uint8_t state, LP initialLen) {
+    return break_link<LP>(c.bendBreak, c.maxLoad, a, b, state, initialLen);
 }
 
 // The sample integrate step on one particle (HiDEM/MeshBlock/MainMeshBlock.cpp:182-261:

@@ -124,6 +124,13 @@ class HiDEMLib:
     def step(self, nsteps: int = 1) -> None:
         self._check(self._lib.hidem_step(self._ctx, int(nsteps)))
 
+    def set_step_kernel(self, kernel: int) -> None:
+        """abi.STEP_KERNEL_* (AUTO: timed on the first fused steps)."""
+        self._check(self._lib.hidem_set_step_kernel(self._ctx, int(kernel)))
+
+    def step_kernel(self) -> int:
+        return int(self._lib.hidem_get_step_kernel(self._ctx))
+
     def profile(self, enable: bool = True) -> None:
         """CUDA-event timing of the fused step kernel on the context's stream."""
         self._check(self._lib.hidem_profile(self._ctx, 1 if enable else 0))
@@ -203,3 +210,55 @@ class HiDEMLib:
         s = abi.HidemStats()
         self._check(self._lib.hidem_get_stats(self._ctx, C.byref(s)))
         return s.as_dict()
+
+
+class HiDEMBatch:
+    """Independent contexts advanced together, one kernel launch per timestep over all of
+    them (``hidem_batch_*``; no counterpart in the reference). Each context's results are
+    those of ``HiDEMLib.step`` on it alone. The contexts must stay open while the batch
+    exists; ``close`` the batch first."""
+
+    def __init__(self, libs: list[HiDEMLib], graphs: bool = True, per_context: bool = False):
+        self._lib = abi.load()
+        self.libs = list(libs)
+        arr = (C.c_void_p * len(self.libs))(*[l._ctx for l in self.libs])
+        flags = (abi.BATCH_GRAPHS if graphs else 0) | (abi.BATCH_PER_CONTEXT if per_context else 0)
+        h = C.c_void_p()
+        st = self._lib.hidem_batch_create(arr, len(self.libs), flags, C.byref(h))
+        if st != abi.HIDEM_OK:
+            raise abi.HidemError(st, self._lib.hidem_create_error().decode())
+        self._b = h
+
+    def _check(self, st: int) -> None:
+        if st != abi.HIDEM_OK:
+            raise abi.HidemError(st, self._lib.hidem_batch_last_error(self._b).decode())
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self._lib.hidem_batch_step(self._b, int(nsteps)))
+
+    @property
+    def stream_handle(self) -> int:
+        """The cudaStream_t the batch's work runs on."""
+        return int(self._lib.hidem_batch_get_stream(self._b) or 0)
+
+    def counts(self) -> dict:
+        v = [C.c_int64() for _ in range(3)]
+        self._check(self._lib.hidem_batch_counts(self._b, *[C.byref(x) for x in v]))
+        return dict(launches=v[0].value, graph_launches=v[1].value, uploads=v[2].value)
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            self._lib.hidem_batch_destroy(self._b)
+            self._b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -121,3 +121,39 @@ def algorithmic_bytes(n: int, L: int, pairs: int, precision: int) -> dict:
     pair = pairs * 4
     total = force + integ + sides + brk + pair
     return dict(force=force, integrate=integ, sides=sides, link_break=brk, pairs=pair, total=total)
+
+
+def ensemble_sizes(count: int = 256, n_min: int = 5000, n_max: int = 80000, seed: int = 11):
+    """Cube edges (unit cells) and per-block maxLoad of the batched ensemble: particle
+    counts drawn log-uniform from [n_min, n_max] and rounded to whole FCC unit cells
+    (4 particles each), fracture strain threshold lognormal with median 5e-4, sigma 0.3."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(math.log(n_min), math.log(n_max), size=count))
+    edges = np.maximum(1, np.rint(np.cbrt(n / 4.0))).astype(int)
+    max_load = 5e-4 * np.exp(0.3 * rng.standard_normal(count))
+    return edges, max_load
+
+
+def ensemble(count: int = 256, precision: int = abi.PREC_MIXED, seed: int = 11,
+             n_min: int = 5000, n_max: int = 80000):
+    """Independent FCC ice blocks of uneven sizes (config: 256 blocks, 5k-80k particles
+    log-uniform, per-block maxLoad lognormal(5e-4, 0.3), per-block jitter seed, other
+    parameters as the 20^3 ice block). Returns a list of (params, particles, links)."""
+    edges, max_load = ensemble_sizes(count, n_min, n_max, seed)
+    out = []
+    for i, (e, ml) in enumerate(zip(edges, max_load)):
+        out.append(ice_block((int(e),) * 3, precision, seed=seed * 100003 + i, maxLoad=float(ml)))
+    return out
+
+
+def ensemble_shard(sizes, world: int, rank: int) -> list[int]:
+    """Blocks of rank `rank` out of `world` (no data exchange between ranks): largest block
+    first, each to the rank with the fewest particles so far (ties to the lower rank)."""
+    load = [0] * world
+    mine = []
+    for i in sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += int(sizes[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)

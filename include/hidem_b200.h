@@ -253,6 +253,55 @@ hidem_status hidem_links_by_distance(const hidem_particle_soa *p, int64_t n, int
                                      double scale, hidem_link_soa *out, int64_t cap,
                                      int64_t *count);
 
+/* ---- step kernel choice ----------------------------------------------- */
+
+/* No counterpart in the reference. The fused step has several kernels that give
+ * bit-identical results and differ only in speed: one thread per (particle, contact) and
+ * (particle, link end) item with the block's streams staged in shared memory (ITEMS), one
+ * thread per particle with software-pipelined partner loads (THREAD), and the same with
+ * registers capped for more CTAs per SM (THREAD_CAPPED: five in the mixed build, three in
+ * FP64). AUTO (the default) times each on the context's own first fused steps (three
+ * rounds, the first discarded) and keeps the fastest; those steps are ordinary timesteps.
+ * hidem_get_step_kernel returns the kernel in use (AUTO while still timing). */
+#define HIDEM_STEP_KERNEL_AUTO 0
+#define HIDEM_STEP_KERNEL_ITEMS 1
+#define HIDEM_STEP_KERNEL_THREAD 2
+#define HIDEM_STEP_KERNEL_THREAD_CAPPED 3
+hidem_status hidem_set_step_kernel(hidem_ctx *ctx, int32_t kernel);
+int32_t hidem_get_step_kernel(const hidem_ctx *ctx);
+
+/* ---- batched contexts ------------------------------------------------- */
+
+/* No counterpart in the reference (one HiDEMLib instance runs one particle set per
+ * rank). Many independent contexts (ice blocks of uneven sizes) on one device and of one
+ * precision advance together: every timestep is one kernel launch over all contexts
+ * that share their constants apart from the break thresholds (maxLoad, bendBreak may
+ * differ per context; contexts that differ in anything else form further launches), and
+ * the launches between two gridService points (at most 10 steps) are replayed from a
+ * CUDA graph when HIDEM_BATCH_GRAPHS is set. Each context's results are bit-identical to
+ * hidem_step on that context alone: the batch runs the same gridService policy, the same
+ * fused step and the same deferred link update per context. The step kernel is the first
+ * context's (hidem_set_step_kernel; AUTO or untimed means THREAD_CAPPED).
+ * HIDEM_BATCH_PER_CONTEXT runs the single-context launch sequence context after context
+ * instead (the same results, for comparison); rows too wide for the ITEMS kernel's shared
+ * memory take that path too. During a batch call the contexts' work runs on the batch's
+ * stream; the call returns after it finished. The contexts must outlive the batch and
+ * must not be used from another thread during a batch call. On failure of
+ * hidem_batch_create the text is in hidem_create_error(). */
+typedef struct hidem_batch hidem_batch;
+#define HIDEM_BATCH_GRAPHS 1
+#define HIDEM_BATCH_PER_CONTEXT 2
+hidem_status hidem_batch_create(hidem_ctx *const *ctxs, int32_t nctx, int32_t flags,
+                                hidem_batch **out);
+void hidem_batch_destroy(hidem_batch *b);
+const char *hidem_batch_last_error(const hidem_batch *b);
+hidem_status hidem_batch_step(hidem_batch *b, int32_t nsteps);
+/* the cudaStream_t the batch's work runs on */
+void *hidem_batch_get_stream(hidem_batch *b);
+/* kernel launches of the batch so far, graph replays, entry uploads */
+hidem_status hidem_batch_counts(const hidem_batch *b, int64_t *launches, int64_t *graph_launches,
+                                int64_t *uploads);
+
 /* ---- allocation-free binning ------------------------------------------ */
 
 /* No counterpart in the reference. For callers that cannot let a library allocate

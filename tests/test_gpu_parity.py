@@ -20,8 +20,9 @@ L_OUT = ["state", "CT0", "CT1", "CT2", "CT3", "CT4", "CT5"]
 PRECS = [abi.PREC_MIXED, abi.PREC_FP64]
 
 
-def gpu_run(P, p, l, steps, mode="fused", start_step=0):
+def gpu_run(P, p, l, steps, mode="fused", start_step=0, kernel=abi.STEP_KERNEL_AUTO):
     lib = HiDEMLib(P)
+    lib.set_step_kernel(kernel)
     if start_step:
         lib.set_timestep(start_step)
     lib.set_particles(p)
@@ -65,6 +66,35 @@ def test_gpu_matches_reference_golden(gpu, name, mode):
     ref_l = {k: g["out_l_" + k] for k in L_OUT}
     assert_same(res, ref_p, ref_l, g["out_events"], g["out_force"] if mode == "split" else None)
     assert res[4]["regen_count"] == len(g["out_regen"])
+
+
+@pytest.mark.parametrize("name", ["block6_mixed", "block6_fp64", "slab533_mixed", "slab533_fp64"])
+@pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD,
+                                    abi.STEP_KERNEL_THREAD_CAPPED])
+def test_every_step_kernel_matches_golden(gpu, name, kernel):
+    """Each step kernel on its own (the autotuner only picks among them by speed)."""
+    g = load_golden(name)
+    P, p, l = golden_inputs(g)
+    for mode in ("fused", "split"):
+        res = gpu_run(P, p, l, int(g["steps"]), mode, kernel=kernel)
+        ref_p = {k: g["out_p_" + k] for k in P_OUT}
+        ref_l = {k: g["out_l_" + k] for k in L_OUT}
+        assert_same(res, ref_p, ref_l, g["out_events"], g["out_force"] if mode == "split" else None)
+
+
+def test_step_kernel_autotuner_settles(gpu):
+    P, p, l = workloads.ice_block(cells=(6, 6, 6), precision=abi.PREC_MIXED, seed=3)
+    lib = HiDEMLib(P)
+    lib.set_particles(p)
+    lib.set_links(l)
+    assert lib.step_kernel() == abi.STEP_KERNEL_AUTO
+    lib.step(4)
+    lib.step(8)
+    assert lib.step_kernel() in (abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD,
+                                 abi.STEP_KERNEL_THREAD_CAPPED)
+    with pytest.raises(abi.HidemError):
+        lib.set_step_kernel(9)
+    lib.close()
 
 
 @pytest.mark.parametrize("precision", PRECS)
