@@ -175,6 +175,11 @@ def empty_links(L: int, precision: int) -> dict:
 
 _lib = None
 
+class HidemSurrogateConfig(C.Structure):
+    _fields_ = [("hidden_layers", C.c_int32), ("width", C.c_int32), ("fourier_bands", C.c_int32),
+                ("batch", C.c_int32), ("learning_rate", C.c_double), ("seed", C.c_uint64)]
+
+
 # (name, restype, argtypes)
 _PROTOS = [
     ("hidem_abi_version", C.c_int, []),
@@ -217,6 +222,19 @@ _PROTOS = [
     ("hidem_batch_get_stream", C.c_void_p, [C.c_void_p]),
     ("hidem_batch_counts", C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64),
                                      C.POINTER(_i64)]),
+    ("hidem_surrogate_config_default", None, [C.POINTER(HidemSurrogateConfig)]),
+    ("hidem_surrogate_create", C.c_int, [C.POINTER(HidemSurrogateConfig), C.c_int,
+                                         C.POINTER(C.c_void_p)]),
+    ("hidem_surrogate_destroy", None, [C.c_void_p]),
+    ("hidem_surrogate_last_error", C.c_char_p, [C.c_void_p]),
+    ("hidem_surrogate_num_params", _i64, [C.c_void_p]),
+    ("hidem_surrogate_get_params", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("hidem_surrogate_set_params", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("hidem_surrogate_set_data", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64]),
+    ("hidem_surrogate_train", C.c_int, [C.c_void_p, _i32, C.POINTER(_d)]),
+    ("hidem_surrogate_predict", C.c_int, [C.c_void_p, C.c_void_p, _i64, C.c_void_p]),
+    ("hidem_surrogate_gradients", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64, C.c_void_p,
+                                            C.POINTER(_d)]),
     ("hidem_bin_cells_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64, _d,
                                           C.c_void_p, C.c_void_p, C.POINTER(_i64), C.POINTER(_d),
                                           C.c_void_p]),

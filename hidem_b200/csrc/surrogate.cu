@@ -1,0 +1,978 @@
+// Learned warm start: the coordinate MLP that predicts the gravity/buoyancy-settled
+// displacement of a particle from its position and the local ice geometry, trained and
+// evaluated by this library's own kernels. No counterpart in the reference (HiDEM settles
+// every geometry from rest). The hidden layers are BF16 GEMMs on the 5th-generation tensor
+// cores: tiles staged by TMA (cp.async.bulk.tensor, 128-byte swizzle) through a 4-stage
+// mbarrier ring, tcgen05.mma issued by one thread with the FP32 accumulator in tensor
+// memory, and an epilogue (bias + SiLU, or the SiLU derivative) that reads the
+// accumulator back with tcgen05.ld. The 3-wide output layer, the loss, the reductions
+// and Adam run on the CUDA cores.
+//
+// Network: features(u) -> [Linear(K_l -> W) + SiLU] x L -> Linear(W -> 3), with
+// u = 5 normalised inputs (x, y, z, local thickness, bed height) and Fourier features
+// u_i, sin(2^f pi u_i), cos(2^f pi u_i) for f < F, zero-padded to 128 inputs.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hidem_b200.h"
+
+namespace hidem {
+extern thread_local std::string g_nocontext_error;
+}
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+// ------------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t su32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mb_init(uint64_t *b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mb_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mb_expect_tx(uint64_t *b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mb_try(uint64_t *b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// every wait is bounded: after kSpins polls the caller records an error and gives up
+constexpr int kSpins = 1 << 22;
+__device__ __forceinline__ bool mb_wait(uint64_t *b, uint32_t parity) {
+    for (int i = 0; i < kSpins; ++i)
+        if (mb_try(b, parity)) return true;
+    return false;
+}
+// 2-D tiled TMA load of box {64 elements, rows} at (c0 = element column, c1 = row)
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(su32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(su32(bar)), "r"(c0), "r"(c1)
+        : "memory");
+}
+__device__ __forceinline__ void tm_alloc(uint32_t *slot, uint32_t cols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(slot)),
+                 "r"(cols)
+                 : "memory");
+}
+__device__ __forceinline__ void tm_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tm_dealloc(uint32_t taddr, uint32_t cols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// D[tmem] (+)= A[smem] * B[smem]^T, both K-major, kind::f16 (BF16 in, FP32 accumulate)
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+// arrive on `bar` once every MMA issued so far by this thread has completed
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     su32(bar))
+                 : "memory");
+}
+// 16 consecutive FP32 columns of this thread's tensor-memory lane
+__device__ __forceinline__ void tm_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// Shared-memory matrix descriptor of a K-major tile written by TMA with the 128-byte
+// swizzle: rows of 64 BF16 (128 B), 8-row atoms 1024 B apart (stride byte offset),
+// descriptor version 1, layout type 2 (128-byte swizzle). Moving 16 elements along K
+// inside the atom adds 32 B to the start address.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void set_err(int *flag, int code) {
+    if (flag) atomicCAS(flag, 0, code);
+}
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+    const float s = 1.0f / (1.0f + __expf(-z));
+    return s * (1.0f + z * (1.0f - s));
+}
+
+}  // namespace
+
+namespace {
+
+// ------------------------------------------------------------------ tensor-core GEMM
+
+enum Epi { EPI_F32 = 0, EPI_BIAS_SILU = 1, EPI_SILU_GRAD = 2 };
+
+struct GemmArgs {
+    int M, N, K;             // C[M][N] = A[M][K] * B[N][K]^T
+    int kTiles;              // 64-wide K tiles per CTA (split-K: gridDim.y splits)
+    float *outF;             // EPI_F32: [split][M][ldo] (+ bias when given)
+    long long splitStride;   // elements between split partials of outF
+    bf16 *outH;              // EPI_BIAS_SILU: SiLU(acc + bias); EPI_SILU_GRAD: acc * SiLU'(zIn)
+    float *zOut;             // EPI_BIAS_SILU: acc + bias (may be null)
+    const float *zIn;        // EPI_SILU_GRAD: pre-activation [M][ldo]
+    const float *bias;       // [N] or null
+    int ldo;
+    int *err;
+};
+
+constexpr int kGemmStages = 4;
+constexpr int kGemmThreads = 128;
+
+template <int BN>
+constexpr size_t gemm_smem_bytes() {
+    return (size_t)kGemmStages * (128 * 128 + BN * 128) + 1024 + 256;
+}
+
+// One CTA: rows [128 * blockIdx.x, +128) x all BN columns, K tiles
+// [kTiles * blockIdx.y, +kTiles). Thread 0 streams A / B tiles with TMA and issues the
+// MMAs (4 of K = 16 per 64-wide tile); the four warps then read the accumulator (warp w:
+// lanes / rows 32w..32w+31) and apply the epilogue.
+template <int BN, int EPI>
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    k_umma_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+                const GemmArgs g) {
+    constexpr int S = kGemmStages;
+    constexpr uint32_t ABYTES = 128 * 128, BBYTES = BN * 128, STAGE = ABYTES + BBYTES;
+    constexpr uint32_t COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+    extern __shared__ unsigned char dyn[];
+    unsigned char *sm =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + S * STAGE);
+    uint64_t *empty = full + S;
+    uint64_t *done = empty + S;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(done + 1);
+    __shared__ int sFail;
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mb_init(full + s, 1);
+            mb_init(empty + s, 1);
+        }
+        mb_init(done, 1);
+        sFail = 0;
+        mb_fence_init();
+    }
+    if (warp == 0) {
+        tm_alloc(slot, COLS);
+        tm_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    const int m0 = blockIdx.x * 128;
+    const int kt0 = blockIdx.y * g.kTiles;
+    const int nk = g.kTiles;
+
+    if (tid == 0) {
+        // kind::f16 descriptor: D FP32, A and B BF16, both K-major, N = BN, M = 128
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(128 >> 4) << 24);
+        int issued = 0;
+        auto load = [&](int i) {
+            const int s = i % S;
+            unsigned char *a = sm + s * STAGE;
+            mb_expect_tx(full + s, STAGE);
+            tma_load_2d(a, &ta, (kt0 + i) * 64, m0, full + s);
+            tma_load_2d(a + ABYTES, &tb, (kt0 + i) * 64, 0, full + s);
+        };
+        for (; issued < nk && issued < S; ++issued) load(issued);
+        bool ok = true;
+        int i = 0;
+        for (; i < nk; ++i) {
+            const int s = i % S;
+            const uint32_t par = (uint32_t)((i / S) & 1);
+            if (!mb_wait(full + s, par)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = su32(sm + s * STAGE), b0 = a0 + ABYTES;
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+                tc_mma(tmem, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), idesc,
+                       (i > 0 || kk > 0) ? 1u : 0u);
+            tc_commit(empty + s);
+            if (issued < nk) {
+                if (!mb_wait(empty + s, par)) {
+                    ok = false;
+                    ++i;
+                    break;
+                }
+                load(issued);
+                ++issued;
+            }
+        }
+        tc_commit(done);
+        if (!ok) {
+            sFail = 1;
+            set_err(g.err, 1);
+            // copies still in flight land in this CTA's shared memory: give them a
+            // bounded chance to complete before the CTA exits
+            for (int j = i; j < issued; ++j) mb_wait(full + (j % S), (uint32_t)((j / S) & 1));
+        }
+    }
+    const bool accReady = mb_wait(done, 0);
+    tc_fence_after();
+    __syncthreads();
+    if (accReady && !sFail) {
+        const int row = m0 + warp * 32 + (tid & 31);
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            float v[16];
+            tm_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            const long long o = (long long)row * g.ldo + c0;
+            if (EPI == EPI_F32) {
+                float *dst = g.outF + blockIdx.y * g.splitStride + o;
+#pragma unroll
+                for (int j = 0; j < 16; j += 4) {
+                    float4 q;
+                    q.x = v[j] + (g.bias ? g.bias[c0 + j] : 0.f);
+                    q.y = v[j + 1] + (g.bias ? g.bias[c0 + j + 1] : 0.f);
+                    q.z = v[j + 2] + (g.bias ? g.bias[c0 + j + 2] : 0.f);
+                    q.w = v[j + 3] + (g.bias ? g.bias[c0 + j + 3] : 0.f);
+                    *reinterpret_cast<float4 *>(dst + j) = q;
+                }
+            } else if (EPI == EPI_BIAS_SILU) {
+                __align__(16) bf16 h[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const float z = v[j] + g.bias[c0 + j];
+                    v[j] = z;
+                    h[j] = __float2bfloat16_rn(silu(z));
+                }
+                if (g.zOut) {
+#pragma unroll
+                    for (int j = 0; j < 16; j += 4)
+                        *reinterpret_cast<float4 *>(g.zOut + o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                }
+                *reinterpret_cast<uint4 *>(g.outH + o) = *reinterpret_cast<const uint4 *>(h);
+                *reinterpret_cast<uint4 *>(g.outH + o + 8) = *reinterpret_cast<const uint4 *>(h + 8);
+            } else {
+                __align__(16) bf16 h[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) h[j] = __float2bfloat16_rn(v[j] * silu_grad(g.zIn[o + j]));
+                *reinterpret_cast<uint4 *>(g.outH + o) = *reinterpret_cast<const uint4 *>(h);
+                *reinterpret_cast<uint4 *>(g.outH + o + 8) = *reinterpret_cast<const uint4 *>(h + 8);
+            }
+        }
+    } else if (tid == 0 && !accReady) {
+        set_err(g.err, 2);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tm_dealloc(tmem, COLS);
+}
+
+}  // namespace
+
+namespace {
+
+// ------------------------------------------------------------------ CUDA-core kernels
+
+constexpr int kIn = 5;      // normalised inputs per particle
+constexpr int kFeat = 128;  // padded feature width (first layer's K)
+constexpr int kOut = 3;     // displacement components
+
+// Fourier features of the rows idx[b] (or b when idx is null) of `in` [n][5]:
+// u_i, then sin(2^f pi u_i), cos(2^f pi u_i) for f < bands, zero padding to 128.
+__global__ void k_features(const float *__restrict__ in, const int *__restrict__ idx, int rows,
+                           int bands, bf16 *__restrict__ X) {
+    const int b = blockIdx.x * blockDim.y + threadIdx.y;
+    if (b >= rows) return;
+    const int src = idx ? idx[b] : b;
+    float u[kIn];
+#pragma unroll
+    for (int i = 0; i < kIn; ++i) u[i] = in ? in[(long long)src * kIn + i] : 0.f;
+    for (int c = threadIdx.x; c < kFeat; c += blockDim.x) {
+        float v = 0.f;
+        if (c < kIn) {
+            v = u[c];
+        } else {
+            const int q = c - kIn, f = q / (2 * kIn), r = q % (2 * kIn), i = r >> 1;
+            if (f < bands) {
+                const float a = (float)(1 << f) * 3.14159265358979f * u[i];
+                v = (r & 1) ? cosf(a) : sinf(a);
+            }
+        }
+        X[(long long)b * kFeat + c] = __float2bfloat16_rn(v);
+    }
+}
+
+// out[c][r] = in[r][c] for a [R][C] BF16 matrix (32 x 32 tiles through shared memory)
+__global__ void k_transpose(const bf16 *__restrict__ in, int R, int C, bf16 *__restrict__ out) {
+    __shared__ bf16 t[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = r0 + j, c = c0 + threadIdx.x;
+        if (r < R && c < C) t[j][threadIdx.x] = in[(long long)r * C + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int c = c0 + j, r = r0 + threadIdx.x;
+        if (r < R && c < C) out[(long long)c * R + r] = t[threadIdx.x][j];
+    }
+}
+
+// out[e] = sum over s (in order) of part[s * count + e]
+__global__ void k_sum_splits(const float *__restrict__ part, int splits, long long count,
+                             float *__restrict__ out) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    float acc = 0.f;
+    for (int s = 0; s < splits; ++s) acc += part[s * count + e];
+    out[e] = acc;
+}
+
+// Column sums of a BF16 [rows][N] matrix over row chunks of kChunk: part[chunk][N]
+constexpr int kChunk = 256;
+__global__ void k_colsum_bf16(const bf16 *__restrict__ A, int rows, int N, float *__restrict__ part) {
+    __shared__ float red[8][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    const int r0 = blockIdx.y * kChunk;
+    float acc = 0.f;
+    if (c < N)
+        for (int r = r0 + threadIdx.y; r < min(rows, r0 + kChunk); r += 8)
+            acc += __bfloat162float(A[(long long)r * N + c]);
+    red[threadIdx.y][threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < N) {
+        float s = 0.f;
+        for (int j = 0; j < 8; ++j) s += red[j][threadIdx.x];
+        part[(long long)blockIdx.y * N + c] = s;
+    }
+}
+
+// Output layer forward: Y[b][j] = sum_k H[b][k] Wo[j][k] + bo[j] (FP32 accumulate)
+__global__ void k_out_fwd(const bf16 *__restrict__ H, int rows, int W, const float *__restrict__ Wo,
+                          const float *__restrict__ bo, float *__restrict__ Y) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= rows) return;
+    float acc[kOut] = {0.f, 0.f, 0.f};
+    for (int k = 0; k < W; ++k) {
+        const float h = __bfloat162float(H[(long long)b * W + k]);
+#pragma unroll
+        for (int j = 0; j < kOut; ++j) acc[j] += h * Wo[j * W + k];
+    }
+#pragma unroll
+    for (int j = 0; j < kOut; ++j) Y[(long long)b * kOut + j] = acc[j] + bo[j];
+}
+
+// MSE over the batch: dY = 2 (Y - T) / (rows * 3); per-block partial losses
+__global__ void k_loss(const float *__restrict__ Y, const float *__restrict__ targets,
+                       const int *__restrict__ idx, int rows, float *__restrict__ dY,
+                       float *__restrict__ lossPart) {
+    __shared__ float red[256];
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (b < rows) {
+        const int src = idx ? idx[b] : b;
+        const float inv = 2.0f / (float)(rows * kOut);
+#pragma unroll
+        for (int j = 0; j < kOut; ++j) {
+            const float d = Y[(long long)b * kOut + j] - targets[(long long)src * kOut + j];
+            dY[(long long)b * kOut + j] = d * inv;
+            l += d * d;
+        }
+    }
+    red[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) lossPart[blockIdx.x] = red[0];
+}
+
+// Output layer backward into the last hidden layer:
+// dZ[b][k] = (sum_j dY[b][j] Wo[j][k]) * SiLU'(Z[b][k]), stored BF16
+__global__ void k_out_bwd(const float *__restrict__ dY, const float *__restrict__ Wo,
+                          const float *__restrict__ Z, int rows, int W, bf16 *__restrict__ dZ) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)rows * W) return;
+    const int b = (int)(e / W), k = (int)(e % W);
+    float g = 0.f;
+#pragma unroll
+    for (int j = 0; j < kOut; ++j) g += dY[(long long)b * kOut + j] * Wo[j * W + k];
+    dZ[e] = __float2bfloat16_rn(g * silu_grad(Z[e]));
+}
+
+// Output layer weight / bias gradients over row chunks of kChunk:
+// part[chunk][j][W + 1]: column k < W holds sum dY[b][j] H[b][k], column W sum dY[b][j]
+__global__ void k_out_grad(const float *__restrict__ dY, const bf16 *__restrict__ H, int rows, int W,
+                           float *__restrict__ part) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;  // 0..W (W = bias)
+    if (k > W) return;
+    const int r0 = blockIdx.y * kChunk;
+    float acc[kOut] = {0.f, 0.f, 0.f};
+    for (int b = r0; b < min(rows, r0 + kChunk); ++b) {
+        const float h = (k < W) ? __bfloat162float(H[(long long)b * W + k]) : 1.f;
+#pragma unroll
+        for (int j = 0; j < kOut; ++j) acc[j] += dY[(long long)b * kOut + j] * h;
+    }
+#pragma unroll
+    for (int j = 0; j < kOut; ++j) part[((long long)blockIdx.y * kOut + j) * (W + 1) + k] = acc[j];
+}
+
+// Adam on a flat FP32 parameter array (t = step count after this update)
+__global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, long long n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const float gr = g[e];
+    const float mm = b1 * m[e] + (1.f - b1) * gr;
+    const float vv = b2 * v[e] + (1.f - b2) * gr * gr;
+    m[e] = mm;
+    v[e] = vv;
+    p[e] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+}
+
+// BF16 copies of a [R][C] FP32 weight: as is and transposed
+__global__ void k_weight_bf16(const float *__restrict__ w, int R, int C, bf16 *__restrict__ wb,
+                              bf16 *__restrict__ wbT) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)R * C) return;
+    const int r = (int)(e / C), c = (int)(e % C);
+    const bf16 h = __float2bfloat16_rn(w[e]);
+    wb[e] = h;
+    wbT[(long long)c * R + r] = h;
+}
+
+// Batch rows drawn uniformly (with replacement) from n samples: a splitmix64 hash of
+// (seed, step, row)
+__global__ void k_sample(unsigned long long seed, unsigned long long step, int rows, long long n,
+                         int *__restrict__ idx) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= rows) return;
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (step * 0x100000001B3ull + (unsigned long long)b + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    idx[b] = (int)(z % (unsigned long long)n);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+
+struct hidem_surrogate {
+    hidem_surrogate_config cfg{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int *dErr = nullptr;
+    int L = 4, W = 256, B = 16384, splits = 64;
+    long long np = 0;                            // parameter count
+    std::vector<long long> offW, offB;           // hidden layer weight / bias offsets in P
+    long long offWo = 0, offBo = 0;
+    std::vector<int> Kl;                         // input width of hidden layer l
+    float *P = nullptr, *G = nullptr, *Mm = nullptr, *Vv = nullptr;
+    std::vector<bf16 *> Wb, WbT;                 // BF16 weights [W][K_l] and [K_l][W]
+    bf16 *X0 = nullptr;                          // [B][128]
+    std::vector<float *> Z;                      // [B][W] pre-activations
+    std::vector<bf16 *> H;                       // [B][W] activations
+    float *Y = nullptr, *dY = nullptr;           // [B][3]
+    bf16 *dZa = nullptr, *dZb = nullptr;         // [B][W]
+    bf16 *dZT = nullptr, *inT = nullptr;         // [W][B], [max K][B]
+    float *part = nullptr;                       // split / chunk partials
+    long long partCap = 0;
+    float *lossPart = nullptr, *lossHost = nullptr;
+    int *idx = nullptr;
+    float *dataIn = nullptr, *dataT = nullptr;   // training set [n][5], [n][3]
+    long long nData = 0;
+    float *scratchIn = nullptr, *scratchT = nullptr;  // caller rows for predict / gradients
+    long long steps = 0;
+};
+
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// BF16 [rows][cols] row-major, boxes of 64 columns x boxRows rows, 128-byte swizzle
+bool make_map(CUtensorMap *m, const void *base, long long rows, long long cols, int boxRows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * sizeof(bf16)};
+    cuuint32_t box[2] = {64u, (cuuint32_t)boxRows};
+    cuuint32_t es[2] = {1u, 1u};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+hidem_status sfail(hidem_surrogate *s, hidem_status st, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (s) s->err = buf;
+    return st;
+}
+
+#define SCK(call)                                                                            \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return sfail(s, HIDEM_ERR_CUDA, "%s failed: %s (%s:%d)", #call,                  \
+                         cudaGetErrorString(e_), __FILE__, __LINE__);                        \
+    } while (0)
+#define STRY(expr)                           \
+    do {                                     \
+        hidem_status s_ = (expr);            \
+        if (s_ != HIDEM_OK) return s_;       \
+    } while (0)
+
+template <int BN, int EPI>
+hidem_status gemm(hidem_surrogate *s, const bf16 *A, int M, int K, const bf16 *Bm, int splits,
+                  GemmArgs g) {
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_umma_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)gemm_smem_bytes<BN>());
+        configured = true;
+    }
+    if (M % 128 || K % 64 || (K / 64) % splits)
+        return sfail(s, HIDEM_ERR_ARG, "GEMM shape %d x %d x %d (splits %d) is not tile-aligned", M, BN, K, splits);
+    CUtensorMap ta, tb;
+    if (!make_map(&ta, A, M, K, 128) || !make_map(&tb, Bm, BN, K, BN))
+        return sfail(s, HIDEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    g.M = M;
+    g.N = BN;
+    g.K = K;
+    g.kTiles = K / 64 / splits;
+    g.err = s->dErr;
+    k_umma_gemm<BN, EPI><<<dim3(M / 128, splits), kGemmThreads, gemm_smem_bytes<BN>(), s->stream>>>(ta, tb, g);
+    SCK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+template <int EPI>
+hidem_status gemm_n(hidem_surrogate *s, int N, const bf16 *A, int M, int K, const bf16 *Bm,
+                    int splits, const GemmArgs &g) {
+    if (N == 256) return gemm<256, EPI>(s, A, M, K, Bm, splits, g);
+    if (N == 128) return gemm<128, EPI>(s, A, M, K, Bm, splits, g);
+    return sfail(s, HIDEM_ERR_ARG, "GEMM width %d (128 or 256)", N);
+}
+
+// the partial buffer is sized at creation for the largest batch; a call that would need
+// more is a bug, reported rather than reallocating under queued work
+hidem_status ensure_part(hidem_surrogate *s, long long count) {
+    if (s->partCap >= count) return HIDEM_OK;
+    return sfail(s, HIDEM_ERR_CAPACITY, "partial buffer too small (%lld < %lld)", s->partCap, count);
+}
+
+hidem_status refresh_bf16(hidem_surrogate *s) {
+    for (int l = 0; l < s->L; ++l) {
+        const long long n = (long long)s->W * s->Kl[l];
+        k_weight_bf16<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(s->P + s->offW[l], s->W, s->Kl[l], s->Wb[l], s->WbT[l]);
+    }
+    SCK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+// forward over `rows` rows whose features are in X0 (keepZ: store pre-activations)
+hidem_status forward(hidem_surrogate *s, int rows, bool keepZ) {
+    const bf16 *in = s->X0;
+    for (int l = 0; l < s->L; ++l) {
+        GemmArgs g{};
+        g.outH = s->H[l];
+        g.zOut = keepZ ? s->Z[l] : nullptr;
+        g.bias = s->P + s->offB[l];
+        g.ldo = s->W;
+        STRY(gemm_n<EPI_BIAS_SILU>(s, s->W, in, rows, s->Kl[l], s->Wb[l], 1, g));
+        in = s->H[l];
+    }
+    k_out_fwd<<<(rows + 127) / 128, 128, 0, s->stream>>>(s->H[s->L - 1], rows, s->W, s->P + s->offWo,
+                                                       s->P + s->offBo, s->Y);
+    SCK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+// loss and all gradients into G for the rows of X0 (targets[idx[b]] or targets[b])
+hidem_status backward(hidem_surrogate *s, int rows, const float *targets, const int *idx) {
+    const int W = s->W, L = s->L;
+    const int nb = (rows + 255) / 256;
+    k_loss<<<nb, 256, 0, s->stream>>>(s->Y, targets, idx, rows, s->dY, s->lossPart);
+    // output layer
+    const int chunks = (rows + kChunk - 1) / kChunk;
+    STRY(ensure_part(s, (long long)(chunks + 1) * kOut * (W + 1)));
+    k_out_grad<<<dim3((W + 1 + 127) / 128, chunks), 128, 0, s->stream>>>(s->dY, s->H[L - 1], rows, W, s->part);
+    // sum the chunk partials into a [3][W + 1] block, then split weights and biases
+    float *outBlock = s->part + (long long)chunks * kOut * (W + 1);
+    k_sum_splits<<<(unsigned)((kOut * (W + 1) + 255) / 256), 256, 0, s->stream>>>(s->part, chunks, (long long)kOut * (W + 1), outBlock);
+    for (int j = 0; j < kOut; ++j) {
+        SCK(cudaMemcpyAsync(s->G + s->offWo + (long long)j * W, outBlock + (long long)j * (W + 1),
+                            sizeof(float) * W, cudaMemcpyDeviceToDevice, s->stream));
+        SCK(cudaMemcpyAsync(s->G + s->offBo + j, outBlock + (long long)j * (W + 1) + W, sizeof(float),
+                            cudaMemcpyDeviceToDevice, s->stream));
+    }
+    const long long e = (long long)rows * W;
+    bf16 *dZ = s->dZa, *dZn = s->dZb;
+    k_out_bwd<<<(unsigned)((e + 255) / 256), 256, 0, s->stream>>>(s->dY, s->P + s->offWo, s->Z[L - 1], rows, W, dZ);
+    SCK(cudaGetLastError());
+    // hidden layers, last to first
+    for (int l = L - 1; l >= 0; --l) {
+        const int K = s->Kl[l];
+        const bf16 *in = l == 0 ? s->X0 : s->H[l - 1];
+        // dW_l = dZ^T * in: both operands transposed to K-major [.][rows], split over rows
+        k_transpose<<<dim3((W + 31) / 32, (rows + 31) / 32), dim3(32, 8), 0, s->stream>>>(dZ, rows, W, s->dZT);
+        k_transpose<<<dim3((K + 31) / 32, (rows + 31) / 32), dim3(32, 8), 0, s->stream>>>(in, rows, K, s->inT);
+        int splits = s->splits;
+        while (splits > 1 && ((rows / 64) % splits)) splits >>= 1;
+        STRY(ensure_part(s, (long long)splits * W * K));
+        GemmArgs g{};
+        g.outF = s->part;
+        g.splitStride = (long long)W * K;
+        g.ldo = K;
+        STRY(gemm_n<EPI_F32>(s, K, s->dZT, W, rows, s->inT, splits, g));
+        k_sum_splits<<<(unsigned)(((long long)W * K + 255) / 256), 256, 0, s->stream>>>(s->part, splits, (long long)W * K, s->G + s->offW[l]);
+        // db_l = column sums of dZ
+        STRY(ensure_part(s, (long long)chunks * W + W));
+        k_colsum_bf16<<<dim3((W + 31) / 32, chunks), dim3(32, 8), 0, s->stream>>>(dZ, rows, W, s->part);
+        k_sum_splits<<<(W + 255) / 256, 256, 0, s->stream>>>(s->part, chunks, W, s->G + s->offB[l]);
+        if (l > 0) {
+            // dZ_{l-1} = (dZ_l * W_l) . SiLU'(Z_{l-1}); B operand W_l^T is [K_l][W]
+            GemmArgs gd{};
+            gd.outH = dZn;
+            gd.zIn = s->Z[l - 1];
+            gd.ldo = K;
+            STRY(gemm_n<EPI_SILU_GRAD>(s, K, dZ, rows, W, s->WbT[l], 1, gd));
+            std::swap(dZ, dZn);
+        }
+    }
+    SCK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+hidem_status read_loss(hidem_surrogate *s, int rows, double *loss) {
+    const int nb = (rows + 255) / 256;
+    SCK(cudaMemcpyAsync(s->lossHost, s->lossPart, sizeof(float) * nb, cudaMemcpyDeviceToHost, s->stream));
+    SCK(cudaStreamSynchronize(s->stream));
+    double t = 0;
+    for (int i = 0; i < nb; ++i) t += s->lossHost[i];
+    if (loss) *loss = t / ((double)rows * kOut);
+    return HIDEM_OK;
+}
+
+hidem_status check_err(hidem_surrogate *s) {
+    int flag = 0;
+    SCK(cudaMemcpyAsync(&flag, s->dErr, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    SCK(cudaStreamSynchronize(s->stream));
+    if (flag) {
+        SCK(cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream));
+        return sfail(s, HIDEM_ERR_DEVICE, "tensor-core GEMM: %s",
+                     flag == 1 ? "tile copies did not complete in time"
+                               : "accumulator did not complete in time");
+    }
+    return HIDEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void hidem_surrogate_config_default(hidem_surrogate_config *c) {
+    if (!c) return;
+    c->hidden_layers = 4;
+    c->width = 256;
+    c->fourier_bands = 8;
+    c->batch = 16384;
+    c->learning_rate = 1e-3;
+    c->seed = 1;
+}
+
+void hidem_surrogate_destroy(hidem_surrogate *s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    void *bufs[] = {s->P, s->G, s->Mm, s->Vv, s->X0, s->Y, s->dY, s->dZa, s->dZb, s->dZT, s->inT,
+                    s->part, s->lossPart, s->idx, s->dataIn, s->dataT, s->scratchIn, s->scratchT, s->dErr};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    for (auto *p : s->Wb) if (p) cudaFree(p);
+    for (auto *p : s->WbT) if (p) cudaFree(p);
+    for (auto *p : s->Z) if (p) cudaFree(p);
+    for (auto *p : s->H) if (p) cudaFree(p);
+    if (s->lossHost) cudaFreeHost(s->lossHost);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device, hidem_surrogate **out) {
+    std::string &err = hidem::g_nocontext_error;
+    err.clear();
+    if (!c || !out) {
+        err = "config or out is NULL";
+        return HIDEM_ERR_ARG;
+    }
+    *out = nullptr;
+    if (c->hidden_layers < 1 || c->hidden_layers > 16 || (c->width != 128 && c->width != 256) ||
+        c->fourier_bands < 1 || c->fourier_bands > 12 || c->batch < 128 || c->batch % 128 ||
+        c->batch > (1 << 20) || !(c->learning_rate > 0)) {
+        err = "surrogate config out of range (layers 1..16, width 128 | 256, bands 1..12, batch a multiple of 128)";
+        return HIDEM_ERR_ARG;
+    }
+    if (!encode_fn()) {
+        err = "cuTensorMapEncodeTiled is not available from the driver";
+        return HIDEM_ERR_CUDA;
+    }
+    hidem_surrogate *s = new hidem_surrogate();
+    s->cfg = *c;
+    s->device = device;
+    s->L = c->hidden_layers;
+    s->W = c->width;
+    s->B = c->batch;
+    const int L = s->L, W = s->W, B = s->B;
+    long long off = 0;
+    for (int l = 0; l < L; ++l) {
+        const int K = l == 0 ? kFeat : W;
+        s->Kl.push_back(K);
+        s->offW.push_back(off);
+        off += (long long)W * K;
+        s->offB.push_back(off);
+        off += W;
+    }
+    s->offWo = off;
+    off += (long long)kOut * W;
+    s->offBo = off;
+    off += kOut;
+    s->np = off;
+    const int chunks = (B + kChunk - 1) / kChunk;
+    long long partNeed = std::max<long long>((long long)(chunks + 1) * kOut * (W + 1), (long long)chunks * W + W);
+    partNeed = std::max<long long>(partNeed, (long long)s->splits * W * std::max(W, kFeat));
+    auto fail = [&](cudaError_t e) {
+        err = std::string("surrogate setup failed: ") + cudaGetErrorString(e);
+        hidem_surrogate_destroy(s);
+        return HIDEM_ERR_CUDA;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    auto dm = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    dm((void **)&s->dErr, sizeof(int));
+    dm((void **)&s->P, sizeof(float) * s->np);
+    dm((void **)&s->G, sizeof(float) * s->np);
+    dm((void **)&s->Mm, sizeof(float) * s->np);
+    dm((void **)&s->Vv, sizeof(float) * s->np);
+    s->Wb.assign(L, nullptr);
+    s->WbT.assign(L, nullptr);
+    s->Z.assign(L, nullptr);
+    s->H.assign(L, nullptr);
+    for (int l = 0; l < L; ++l) {
+        dm((void **)&s->Wb[l], sizeof(bf16) * W * s->Kl[l]);
+        dm((void **)&s->WbT[l], sizeof(bf16) * W * s->Kl[l]);
+        dm((void **)&s->Z[l], sizeof(float) * (size_t)B * W);
+        dm((void **)&s->H[l], sizeof(bf16) * (size_t)B * W);
+    }
+    dm((void **)&s->X0, sizeof(bf16) * (size_t)B * kFeat);
+    dm((void **)&s->Y, sizeof(float) * (size_t)B * kOut);
+    dm((void **)&s->dY, sizeof(float) * (size_t)B * kOut);
+    dm((void **)&s->dZa, sizeof(bf16) * (size_t)B * W);
+    dm((void **)&s->dZb, sizeof(bf16) * (size_t)B * W);
+    dm((void **)&s->dZT, sizeof(bf16) * (size_t)B * W);
+    dm((void **)&s->inT, sizeof(bf16) * (size_t)B * std::max(W, kFeat));
+    dm((void **)&s->part, sizeof(float) * partNeed);
+    s->partCap = partNeed;
+    dm((void **)&s->lossPart, sizeof(float) * ((B + 255) / 256));
+    dm((void **)&s->idx, sizeof(int) * B);
+    dm((void **)&s->scratchIn, sizeof(float) * (size_t)B * kIn);
+    dm((void **)&s->scratchT, sizeof(float) * (size_t)B * kOut);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&s->lossHost, sizeof(float) * ((B + 255) / 256));
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->Mm, 0, sizeof(float) * s->np, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->Vv, 0, sizeof(float) * s->np, s->stream);
+    if (e != cudaSuccess) return fail(e);
+    // initial weights: uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) from a seeded 64-bit
+    // generator (splitmix64), biases zero
+    std::vector<float> p(s->np, 0.f);
+    unsigned long long st = c->seed * 0x9E3779B97F4A7C15ull + 12345;
+    auto next = [&]() {
+        unsigned long long z = (st += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    for (int l = 0; l < L; ++l) {
+        const double a = 1.0 / std::sqrt((double)s->Kl[l]);
+        for (long long q = 0; q < (long long)W * s->Kl[l]; ++q) p[s->offW[l] + q] = (float)((2 * next() - 1) * a);
+    }
+    const double ao = 1.0 / std::sqrt((double)W);
+    for (long long q = 0; q < (long long)kOut * W; ++q) p[s->offWo + q] = (float)((2 * next() - 1) * ao);
+    e = cudaMemcpy(s->P, p.data(), sizeof(float) * s->np, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(e);
+    if (refresh_bf16(s) != HIDEM_OK || cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        err = s->err;
+        hidem_surrogate_destroy(s);
+        return HIDEM_ERR_CUDA;
+    }
+    *out = s;
+    return HIDEM_OK;
+}
+
+const char *hidem_surrogate_last_error(const hidem_surrogate *s) { return s ? s->err.c_str() : "null surrogate"; }
+
+int64_t hidem_surrogate_num_params(const hidem_surrogate *s) { return s ? s->np : 0; }
+
+hidem_status hidem_surrogate_get_params(hidem_surrogate *s, float *out) {
+    if (!s || !out) return HIDEM_ERR_ARG;
+    SCK(cudaSetDevice(s->device));
+    SCK(cudaMemcpyAsync(out, s->P, sizeof(float) * s->np, cudaMemcpyDeviceToHost, s->stream));
+    SCK(cudaStreamSynchronize(s->stream));
+    return HIDEM_OK;
+}
+
+hidem_status hidem_surrogate_set_params(hidem_surrogate *s, const float *in) {
+    if (!s || !in) return HIDEM_ERR_ARG;
+    SCK(cudaSetDevice(s->device));
+    SCK(cudaMemcpyAsync(s->P, in, sizeof(float) * s->np, cudaMemcpyHostToDevice, s->stream));
+    STRY(refresh_bf16(s));
+    SCK(cudaStreamSynchronize(s->stream));
+    return HIDEM_OK;
+}
+
+hidem_status hidem_surrogate_set_data(hidem_surrogate *s, const float *inputs, const float *targets,
+                                      int64_t n) {
+    if (!s) return HIDEM_ERR_ARG;
+    if (!inputs || !targets || n <= 0 || n > 0x7fffffff) return sfail(s, HIDEM_ERR_ARG, "bad training set");
+    SCK(cudaSetDevice(s->device));
+    if (s->dataIn) cudaFree(s->dataIn);
+    if (s->dataT) cudaFree(s->dataT);
+    s->dataIn = s->dataT = nullptr;
+    s->nData = 0;
+    SCK(cudaMalloc((void **)&s->dataIn, sizeof(float) * kIn * (size_t)n));
+    SCK(cudaMalloc((void **)&s->dataT, sizeof(float) * kOut * (size_t)n));
+    SCK(cudaMemcpyAsync(s->dataIn, inputs, sizeof(float) * kIn * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    SCK(cudaMemcpyAsync(s->dataT, targets, sizeof(float) * kOut * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    SCK(cudaStreamSynchronize(s->stream));
+    s->nData = n;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_surrogate_train(hidem_surrogate *s, int32_t steps, double *loss) {
+    if (!s) return HIDEM_ERR_ARG;
+    if (steps < 0) return sfail(s, HIDEM_ERR_ARG, "negative step count");
+    if (!s->nData) return sfail(s, HIDEM_ERR_STATE, "no training set");
+    SCK(cudaSetDevice(s->device));
+    const int B = s->B;
+    for (int it = 0; it < steps; ++it) {
+        k_sample<<<(B + 255) / 256, 256, 0, s->stream>>>(s->cfg.seed, (unsigned long long)s->steps, B, s->nData, s->idx);
+        k_features<<<(B + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->dataIn, s->idx, B, s->cfg.fourier_bands, s->X0);
+        STRY(forward(s, B, true));
+        STRY(backward(s, B, s->dataT, s->idx));
+        s->steps += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - std::pow(b1, (float)s->steps), c2 = 1.f - std::pow(b2, (float)s->steps);
+        k_adam<<<(unsigned)((s->np + 255) / 256), 256, 0, s->stream>>>(s->P, s->G, s->Mm, s->Vv, s->np,
+                                                                      (float)s->cfg.learning_rate, b1, b2, 1e-8f, c1, c2);
+        STRY(refresh_bf16(s));
+    }
+    if (steps > 0 && loss) STRY(read_loss(s, B, loss));
+    return check_err(s);
+}
+
+hidem_status hidem_surrogate_predict(hidem_surrogate *s, const float *inputs, int64_t n, float *out) {
+    if (!s) return HIDEM_ERR_ARG;
+    if (!inputs || !out || n < 0) return sfail(s, HIDEM_ERR_ARG, "bad arguments");
+    SCK(cudaSetDevice(s->device));
+    const int B = s->B;
+    for (int64_t r0 = 0; r0 < n; r0 += B) {
+        const int rows = (int)std::min<int64_t>(B, n - r0);
+        const int padded = (rows + 127) / 128 * 128;
+        if (padded > rows) SCK(cudaMemsetAsync(s->scratchIn, 0, sizeof(float) * kIn * padded, s->stream));
+        SCK(cudaMemcpyAsync(s->scratchIn, inputs + r0 * kIn, sizeof(float) * kIn * rows, cudaMemcpyHostToDevice, s->stream));
+        k_features<<<(padded + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->scratchIn, nullptr, padded, s->cfg.fourier_bands, s->X0);
+        STRY(forward(s, padded, false));
+        SCK(cudaMemcpyAsync(out + r0 * kOut, s->Y, sizeof(float) * kOut * rows, cudaMemcpyDeviceToHost, s->stream));
+    }
+    SCK(cudaStreamSynchronize(s->stream));
+    return check_err(s);
+}
+
+hidem_status hidem_surrogate_gradients(hidem_surrogate *s, const float *inputs, const float *targets,
+                                       int64_t n, float *grads, double *loss) {
+    if (!s) return HIDEM_ERR_ARG;
+    if (!inputs || !targets || !grads || n <= 0 || n % 128 || n > s->B)
+        return sfail(s, HIDEM_ERR_ARG, "n must be a positive multiple of 128 up to the batch size");
+    SCK(cudaSetDevice(s->device));
+    const int rows = (int)n;
+    SCK(cudaMemcpyAsync(s->scratchIn, inputs, sizeof(float) * kIn * rows, cudaMemcpyHostToDevice, s->stream));
+    SCK(cudaMemcpyAsync(s->scratchT, targets, sizeof(float) * kOut * rows, cudaMemcpyHostToDevice, s->stream));
+    k_features<<<(rows + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->scratchIn, nullptr, rows, s->cfg.fourier_bands, s->X0);
+    STRY(forward(s, rows, true));
+    STRY(backward(s, rows, s->scratchT, nullptr));
+    STRY(read_loss(s, rows, loss));
+    SCK(cudaMemcpyAsync(grads, s->G, sizeof(float) * s->np, cudaMemcpyDeviceToHost, s->stream));
+    SCK(cudaStreamSynchronize(s->stream));
+    return check_err(s);
+}
+
+}  // extern "C"

@@ -1,0 +1,127 @@
+"""Learned warm start: the settling surrogate (``hidem_surrogate_*``).
+
+A coordinate MLP maps 5 normalised inputs per particle — x, y, z, local ice thickness and
+bed height under the particle — to its settled displacement (3 components, normalised).
+Training and inference run in the library's own kernels: BF16 tensor-core GEMMs for the
+hidden layers, CUDA-core kernels for the output layer, loss, reductions and Adam. No
+counterpart in the reference, which settles every geometry from rest; the plain settling
+run stays the judge of every prediction (see ``hidem_b200.settle``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+N_IN = 5
+N_OUT = 3
+N_FEAT = 128
+
+
+def default_config(**over) -> abi.HidemSurrogateConfig:
+    lib = abi.load()
+    c = abi.HidemSurrogateConfig()
+    lib.hidem_surrogate_config_default(C.byref(c))
+    for k, v in over.items():
+        setattr(c, k, v)
+    return c
+
+
+def param_shapes(cfg: abi.HidemSurrogateConfig) -> list[tuple[str, tuple[int, ...]]]:
+    """Names and shapes of the parameters in the library's flat order."""
+    out = []
+    k = N_FEAT
+    for l in range(cfg.hidden_layers):
+        out.append((f"W{l}", (cfg.width, k)))
+        out.append((f"b{l}", (cfg.width,)))
+        k = cfg.width
+    out.append(("Wo", (N_OUT, cfg.width)))
+    out.append(("bo", (N_OUT,)))
+    return out
+
+
+def unflatten(flat: np.ndarray, cfg) -> dict:
+    out, o = {}, 0
+    for name, shp in param_shapes(cfg):
+        n = int(np.prod(shp))
+        out[name] = flat[o:o + n].reshape(shp)
+        o += n
+    return out
+
+
+def flatten(params: dict, cfg) -> np.ndarray:
+    return np.concatenate([np.asarray(params[n], np.float32).ravel() for n, _ in param_shapes(cfg)])
+
+
+class Surrogate:
+    def __init__(self, cfg: abi.HidemSurrogateConfig | None = None, device: int = 0):
+        self._lib = abi.load()
+        self.cfg = cfg if cfg is not None else default_config()
+        h = C.c_void_p()
+        st = self._lib.hidem_surrogate_create(C.byref(self.cfg), int(device), C.byref(h))
+        if st != abi.HIDEM_OK:
+            raise abi.HidemError(st, self._lib.hidem_create_error().decode())
+        self._s = h
+        self.num_params = int(self._lib.hidem_surrogate_num_params(h))
+
+    def _check(self, st: int) -> None:
+        if st != abi.HIDEM_OK:
+            raise abi.HidemError(st, self._lib.hidem_surrogate_last_error(self._s).decode())
+
+    @staticmethod
+    def _f32(a, cols):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        assert a.ndim == 2 and a.shape[1] == cols
+        return a
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.num_params, np.float32)
+        self._check(self._lib.hidem_surrogate_get_params(self._s, out.ctypes.data))
+        return out
+
+    def set_params(self, flat: np.ndarray) -> None:
+        flat = np.ascontiguousarray(flat, dtype=np.float32)
+        assert flat.shape == (self.num_params,)
+        self._check(self._lib.hidem_surrogate_set_params(self._s, flat.ctypes.data))
+
+    def set_data(self, inputs, targets) -> None:
+        x, t = self._f32(inputs, N_IN), self._f32(targets, N_OUT)
+        self._check(self._lib.hidem_surrogate_set_data(self._s, x.ctypes.data, t.ctypes.data, x.shape[0]))
+
+    def train(self, steps: int) -> float:
+        loss = C.c_double()
+        self._check(self._lib.hidem_surrogate_train(self._s, int(steps), C.byref(loss)))
+        return loss.value
+
+    def predict(self, inputs) -> np.ndarray:
+        x = self._f32(inputs, N_IN)
+        out = np.empty((x.shape[0], N_OUT), np.float32)
+        self._check(self._lib.hidem_surrogate_predict(self._s, x.ctypes.data, x.shape[0], out.ctypes.data))
+        return out
+
+    def gradients(self, inputs, targets) -> tuple[np.ndarray, float]:
+        x, t = self._f32(inputs, N_IN), self._f32(targets, N_OUT)
+        g = np.empty(self.num_params, np.float32)
+        loss = C.c_double()
+        self._check(self._lib.hidem_surrogate_gradients(self._s, x.ctypes.data, t.ctypes.data, x.shape[0],
+                                                        g.ctypes.data, C.byref(loss)))
+        return g, loss.value
+
+    def close(self) -> None:
+        if getattr(self, "_s", None):
+            self._lib.hidem_surrogate_destroy(self._s)
+            self._s = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

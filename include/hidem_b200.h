@@ -302,6 +302,47 @@ void *hidem_batch_get_stream(hidem_batch *b);
 hidem_status hidem_batch_counts(const hidem_batch *b, int64_t *launches, int64_t *graph_launches,
                                 int64_t *uploads);
 
+/* ---- learned warm start (settling surrogate) -------------------------- */
+
+/* No counterpart in the reference, which settles every geometry from rest. A coordinate
+ * MLP predicts the gravity/buoyancy-settled displacement of each particle from 5
+ * normalised inputs (x, y, z, local ice thickness, bed height under the particle):
+ * Fourier features (u_i, sin(2^f pi u_i), cos(2^f pi u_i), f < fourier_bands, zero-padded
+ * to 128), hidden_layers x [Linear(width) + SiLU], Linear(3). Hidden layers are BF16
+ * tensor-core GEMMs (tcgen05, FP32 accumulation) written for this library; training is
+ * MSE with Adam on FP32 master weights, `batch` rows per step drawn uniformly from the
+ * training set. Parameters, flat, in this order: for each hidden layer l the weight
+ * [width][K_l] (K_0 = 128, else width) then the bias [width]; the output weight
+ * [3][width], the output bias [3]. Inputs are [n][5] and targets / outputs [n][3] FP32
+ * host arrays, row-major. On failure of hidem_surrogate_create the text is in
+ * hidem_create_error(). */
+typedef struct hidem_surrogate hidem_surrogate;
+typedef struct hidem_surrogate_config {
+    int32_t hidden_layers;   /* 4 */
+    int32_t width;           /* 128 or 256 */
+    int32_t fourier_bands;   /* 1..12 */
+    int32_t batch;           /* rows per training step, a multiple of 128 (16384) */
+    double learning_rate;    /* Adam step size (1e-3) */
+    uint64_t seed;           /* weight initialisation and batch sampling */
+} hidem_surrogate_config;
+void hidem_surrogate_config_default(hidem_surrogate_config *c);
+hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device, hidem_surrogate **out);
+void hidem_surrogate_destroy(hidem_surrogate *s);
+const char *hidem_surrogate_last_error(const hidem_surrogate *s);
+int64_t hidem_surrogate_num_params(const hidem_surrogate *s);
+hidem_status hidem_surrogate_get_params(hidem_surrogate *s, float *out);
+hidem_status hidem_surrogate_set_params(hidem_surrogate *s, const float *in);
+/* the training set (copied to the device) */
+hidem_status hidem_surrogate_set_data(hidem_surrogate *s, const float *inputs, const float *targets,
+                                      int64_t n);
+/* `steps` Adam steps; *loss (may be NULL) receives the last step's batch loss */
+hidem_status hidem_surrogate_train(hidem_surrogate *s, int32_t steps, double *loss);
+hidem_status hidem_surrogate_predict(hidem_surrogate *s, const float *inputs, int64_t n, float *out);
+/* loss and gradient of all parameters (flat order above) on exactly these n rows, no
+ * update; n a multiple of 128 and at most `batch` */
+hidem_status hidem_surrogate_gradients(hidem_surrogate *s, const float *inputs, const float *targets,
+                                       int64_t n, float *grads, double *loss);
+
 /* ---- allocation-free binning ------------------------------------------ */
 
 /* No counterpart in the reference. For callers that cannot let a library allocate

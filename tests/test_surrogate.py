@@ -1,0 +1,112 @@
+"""The settling surrogate's MLP: the oracle's backward pass against finite differences
+(CPU), and the library's tensor-core forward / backward / training against the oracle
+(GPU): predictions and every parameter gradient within the stated tolerance, and a
+training run that lowers the loss."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import surrogate_oracle as so
+
+
+def small_params(rng, layers, width):
+    p, k = {}, so.N_FEAT
+    for l in range(layers):
+        p[f"W{l}"] = (rng.uniform(-1, 1, (width, k)) / np.sqrt(k)).astype(np.float32)
+        p[f"b{l}"] = (0.1 * rng.standard_normal(width)).astype(np.float32)
+        k = width
+    p["Wo"] = (rng.uniform(-1, 1, (so.N_OUT, width)) / np.sqrt(width)).astype(np.float32)
+    p["bo"] = (0.1 * rng.standard_normal(so.N_OUT)).astype(np.float32)
+    return p
+
+
+def test_bf16_rounding_known_answers():
+    vals = np.array([1.0, 1.00390625, 1.005859375, 1.001953125, 1.01171875, -3.14159265],
+                    np.float32)
+    got = so.bf16_round(vals)
+    # BF16 spacing at 1 is 2^-7: 1 + 2^-8 is a tie and goes to the even neighbour 1.0,
+    # 1 + 3*2^-9 lies above the midpoint, 1 + 3*2^-8 is a tie that goes to 1 + 2^-6,
+    # pi rounds to 3.140625
+    want = np.array([1.0, 1.0, 1.0078125, 1.0, 1.015625, -3.140625], np.float32)
+    assert np.array_equal(got, want)
+    import torch
+    rng = np.random.default_rng(4)
+    x = (rng.standard_normal(4096) * 10.0 ** rng.uniform(-6, 6, 4096)).astype(np.float32)
+    assert np.array_equal(so.bf16_round(x), torch.from_numpy(x).to(torch.bfloat16).float().numpy())
+
+
+def test_oracle_backward_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    layers, width, bands = 2, 16, 3
+    p = {k: v.astype(np.float64) for k, v in small_params(rng, layers, width).items()}
+    u = rng.uniform(-1, 1, (12, so.N_IN))
+    t = rng.standard_normal((12, so.N_OUT))
+    loss, g, _ = so.forward_backward(p, layers, u, t, bands, bf16=False)
+    eps = 1e-6
+    for name in ["W0", "b0", "W1", "b1", "Wo", "bo"]:
+        flat = p[name].ravel()
+        for j in rng.choice(flat.size, size=min(6, flat.size), replace=False):
+            old = flat[j]
+            flat[j] = old + eps
+            lp, _, _ = so.forward_backward(p, layers, u, t, bands, bf16=False)
+            flat[j] = old - eps
+            lm, _, _ = so.forward_backward(p, layers, u, t, bands, bf16=False)
+            flat[j] = old
+            fd = (lp - lm) / (2 * eps)
+            assert abs(fd - g[name].ravel()[j]) <= 1e-6 + 1e-5 * abs(fd), (name, j)
+
+
+def _rows(rng, n):
+    u = rng.uniform(-1, 1, (n, so.N_IN)).astype(np.float32)
+    t = np.stack([np.sin(2 * u[:, 0]) * u[:, 3], 0.5 * u[:, 1] * u[:, 2], np.cos(u[:, 4]) - u[:, 2] ** 2],
+                 axis=1).astype(np.float32)
+    return u, t
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("width", [256, 128])
+def test_gpu_forward_and_gradients_match_oracle(gpu, width):
+    from hidem_b200 import surrogate as sg
+    cfg = sg.default_config(width=width, hidden_layers=4, fourier_bands=8, batch=1024, seed=3)
+    rng = np.random.default_rng(1)
+    with sg.Surrogate(cfg) as s:
+        p = small_params(rng, 4, width)
+        s.set_params(sg.flatten(p, cfg))
+        assert np.array_equal(s.get_params(), sg.flatten(p, cfg))
+        u, t = _rows(rng, 512)
+        y = s.predict(u)
+        _, _, y_ref = so.forward_backward(p, 4, u, t, 8)
+        # BF16 activations: a relative error of a few 1e-3 of the output scale
+        assert np.max(np.abs(y - y_ref)) <= 2e-2 * (np.max(np.abs(y_ref)) + 1e-3)
+        g, loss = s.gradients(u, t)
+        loss_ref, g_ref, _ = so.forward_backward(p, 4, u, t, 8)
+        assert abs(loss - loss_ref) <= 1e-2 * loss_ref
+        gg = sg.unflatten(g, cfg)
+        for name, _ in sg.param_shapes(cfg):
+            a, b = gg[name].astype(np.float64), g_ref[name]
+            rel = np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30)
+            assert rel < 2e-2, (name, rel)
+        # predictions of rows that are not a multiple of 128, split over batches
+        u2, _ = _rows(rng, 1500)
+        y2 = s.predict(u2)
+        _, _, y2_ref = so.forward_backward(p, 4, u2, np.zeros((1500, 3), np.float32), 8)
+        assert np.max(np.abs(y2 - y2_ref)) <= 2e-2 * (np.max(np.abs(y2_ref)) + 1e-3)
+
+
+@pytest.mark.gpu
+def test_gpu_training_lowers_the_loss(gpu):
+    from hidem_b200 import surrogate as sg
+    cfg = sg.default_config(width=256, hidden_layers=4, fourier_bands=6, batch=4096, seed=5,
+                            learning_rate=2e-3)
+    rng = np.random.default_rng(2)
+    u, t = _rows(rng, 50000)
+    with sg.Surrogate(cfg) as s:
+        s.set_data(u, t)
+        first = s.train(1)
+        s.train(300)
+        last = s.train(1)
+        uv, tv = _rows(rng, 4096)
+        mse = float(np.mean((s.predict(uv) - tv) ** 2))
+    assert last < 0.1 * first
+    assert mse < 0.1 * float(np.mean(tv ** 2))
