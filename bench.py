@@ -50,7 +50,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["slab", "block", "ensemble"], default="slab")
+    ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle"], default="slab")
+    ap.add_argument("--train-tongues", type=int, default=64, help="settle: training geometries")
+    ap.add_argument("--test-tongues", type=int, default=16, help="settle: held-out geometries")
+    ap.add_argument("--train-steps", type=int, default=20000, help="settle: surrogate Adam steps")
     ap.add_argument("--blocks", type=int, default=256, help="ensemble: number of blocks")
     ap.add_argument("--no-graphs", action="store_true", help="ensemble: plain launches")
     ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped"],
@@ -436,8 +439,66 @@ def main_ensemble(args):
     print(json.dumps(line))
 
 
+def main_settle(args):
+    """Learned warm start: settling steps of held-out glacier tongues, cold vs surrogate-
+    seeded, both judged by the plain method's convergence test (kinetic energy per particle
+    below 1e-6 J over the last 200 steps); plus the surrogate's tensor-core throughput."""
+    import dataclasses
+    import torch
+    from hidem_b200 import settle
+    from hidem_b200 import surrogate as sg
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    size, thick, amp = (40.0, 12.0), 6.0, 2.0
+    rep = settle.warm_start_experiment(n_train=args.train_tongues, n_test=args.test_tongues, size=size,
+                                       base_thickness=thick, amplitude=amp, train_steps=args.train_steps)
+    # tensor-core forward throughput of the trained network's shape on 2M rows
+    cfg = sg.default_config()
+    rows = 1 << 21
+    u = np.random.default_rng(0).uniform(-1, 1, (rows, 5)).astype(np.float32)
+    with sg.Surrogate(cfg) as net:
+        net.predict(u[:16384])
+        t0 = time.perf_counter()
+        net.predict(u)
+        el = time.perf_counter() - t0
+    flops = 2.0 * rows * (128 * cfg.width + (cfg.hidden_layers - 1) * cfg.width * cfg.width + 3 * cfg.width)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    d = dataclasses.asdict(rep)
+    line = {
+        "metric": "settle steps, cold / surrogate-warm (KE < 1e-6 J per particle)",
+        "value": d["step_ratio"], "unit": "x fewer steps", "n_gpus": 1, "steps": None,
+        "warmup": None, "higher_is_better": True, "scaling": "none", "vs_baseline": None,
+        "dtype": "f32+f64pos (settling), bf16/f32-accumulate (surrogate)", "data": "synthetic",
+        "config": {"workload": f"glacier tongues {size[0]:g} x {size[1]:g} m plan, base thickness {thick:g} m, "
+                               f"bed and surface 8 Fourier modes each (total amplitude {amp:g} m), "
+                               f"FCC d = 1 m; {args.train_tongues} training, {args.test_tongues} held out",
+                   "particles_per_tongue": d["particles_per_tongue"], "train_samples": d["train_samples"],
+                   "surrogate": "4 x 256 SiLU MLP, Fourier features, BF16 tcgen05 GEMMs",
+                   "train_steps": args.train_steps},
+        "cold_steps": d["cold_steps"], "warm_steps": d["warm_steps"],
+        "prediction_rel_error": d["prediction_rel_error"],
+        "settled_error_over_d": d["settled_error_over_d"],
+        "converged": {"cold": d["cold_converged"], "warm": d["warm_converged"]},
+        "final_train_loss": d["final_loss"], "seconds": d["seconds"],
+        "surrogate_forward": {"rows": rows, "seconds": el, "tflops": flops / el / 1e12,
+                              "frac_of_bf16_peak": flops / el / 1e12 / peak,
+                              "includes": "host-device copies of inputs and outputs, features, 4 GEMMs, output layer"},
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.workload == "settle":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no learned warm start; its settling is the cold start"}))
+        else:
+            main_settle(args)
+        return
     if args.workload == "ensemble":
         if args.impl == "reference":
             run_reference_ensemble(args)

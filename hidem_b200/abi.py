@@ -213,6 +213,7 @@ _PROTOS = [
     ("hidem_get_break_events", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64,
                                          C.POINTER(_i64)]),
     ("hidem_get_stats", C.c_int, [C.c_void_p, C.POINTER(HidemStats)]),
+    ("hidem_kinetic_energy", C.c_int, [C.c_void_p, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)]),
     ("hidem_set_step_kernel", C.c_int, [C.c_void_p, _i32]),
     ("hidem_get_step_kernel", _i32, [C.c_void_p]),
     ("hidem_batch_create", C.c_int, [C.POINTER(C.c_void_p), _i32, _i32, C.POINTER(C.c_void_p)]),

@@ -115,6 +115,9 @@ struct hidem_ctx {
     int tunedKernel = HIDEM_STEP_KERNEL_AUTO;
     int tuneStep = 0;
     cudaEvent_t tuneEv[2 * 9] = {};
+
+    double *energyBuf = nullptr;  // kinetic-energy partials + result
+    int energyBlocks = 0;
 };
 
 namespace {
@@ -1266,6 +1269,7 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->diffMax);
     dfree(ctx->errorFlag);
     for (cudaEvent_t e : ctx->evPool) cudaEventDestroy(e);
+    dfree(ctx->energyBuf);
     for (cudaEvent_t e : ctx->tuneEv)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1774,6 +1778,31 @@ hidem_status hidem_get_stats(hidem_ctx *ctx, hidem_stats *o) {
         CK(cudaStreamSynchronize(ctx->stream));
         o->broken_links = (int64_t)total;
     }
+    return HIDEM_OK;
+}
+
+hidem_status hidem_kinetic_energy(hidem_ctx *ctx, double *translational, double *rotational,
+                                  double *max_speed) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    CK(cudaSetDevice(ctx->device));
+    const int nb = (int)std::max<long long>(1, std::min<long long>((ctx->n + 255) / 256, 4LL * ctx->smCount));
+    if (ctx->energyBlocks < nb) {
+        TRY(dalloc(ctx, &ctx->energyBuf, 3LL * nb + 3));
+        ctx->energyBlocks = nb;
+    }
+    double *out = ctx->energyBuf + 3 * ctx->energyBlocks;
+    if (ctx->mixed)
+        launch_energy<float>(ctx->cf, recp<float>(ctx, ctx->cur), (int)ctx->n, ctx->energyBuf, nb, out, ctx->stream);
+    else
+        launch_energy<double>(ctx->cd, recp<double>(ctx, ctx->cur), (int)ctx->n, ctx->energyBuf, nb, out, ctx->stream);
+    ctx->launches += 2;
+    double h[3];
+    CK(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (translational) *translational = h[0];
+    if (rotational) *rotational = h[1];
+    if (max_speed) *max_speed = std::sqrt(h[2]);
     return HIDEM_OK;
 }
 

@@ -1091,6 +1091,73 @@ void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slot
                                                   sL0, L, step, events, eventCount, eventCap);
 }
 
+// Kinetic energy with the integrate step's mass and moment of inertia (m = rho d^3,
+// I = m d^2 / 6, MainMeshBlock.cpp:228-229) and velocities diff / dt; per-block sums in
+// a fixed tree order, then one block over the partials, so the result is deterministic.
+template <class LP>
+__global__ void k_energy(const Consts<LP> c, const PRec<LP> *__restrict__ rec, int n,
+                         double *__restrict__ partial) {
+    __shared__ double red[3][256];
+    double kt = 0, kr = 0, vmax = 0;
+    const double dt = (double)c.dt, rho = (double)c.rhoIce;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const PRec<LP> p = load_rec(rec + i);
+        const double d = 2.0 * (double)p.r;
+        const double m = rho * d * d * d, I = m * d * d / 6.0;
+        const double vx = p.d[0] / dt, vy = p.d[1] / dt, vz = p.d[2] / dt;
+        const double wx = p.d[3] / dt, wy = p.d[4] / dt, wz = p.d[5] / dt;
+        const double v2 = vx * vx + vy * vy + vz * vz;
+        kt += 0.5 * m * v2;
+        kr += 0.5 * I * (wx * wx + wy * wy + wz * wz);
+        vmax = v2 > vmax ? v2 : vmax;
+    }
+    red[0][threadIdx.x] = kt;
+    red[1][threadIdx.x] = kr;
+    red[2][threadIdx.x] = vmax;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+            red[2][threadIdx.x] = fmax(red[2][threadIdx.x], red[2][threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; ++q) partial[q * gridDim.x + blockIdx.x] = red[q][0];
+}
+
+__global__ void k_energy_final(const double *__restrict__ partial, int nb, double *__restrict__ out) {
+    __shared__ double red[3][256];
+    double a = 0, b = 0, m = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        a += partial[i];
+        b += partial[nb + i];
+        m = fmax(m, partial[2 * nb + i]);
+    }
+    red[0][threadIdx.x] = a;
+    red[1][threadIdx.x] = b;
+    red[2][threadIdx.x] = m;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+            red[2][threadIdx.x] = fmax(red[2][threadIdx.x], red[2][threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; ++q) out[q] = red[q][0];
+}
+
+template <class LP>
+void launch_energy(const Consts<LP> &c, const PRec<LP> *rec, int n, double *partial, int nb,
+                   double *out, cudaStream_t s) {
+    k_energy<LP><<<nb, 256, 0, s>>>(c, rec, n, partial);
+    k_energy_final<<<1, 256, 0, s>>>(partial, nb, out);
+}
+
 template <class LP>
 void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb, cudaStream_t s) {
     k_max_diff<LP><<<nb, 256, 0, s>>>(rec, n, out);
@@ -1126,7 +1193,9 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
                                         const LP *, long long, long long, int2 *,                  \
                                         unsigned long long *, long long, cudaStream_t);            \
     template void launch_max_diff<LP>(const PRec<LP> *, int, unsigned long long *, int,            \
-                                      cudaStream_t);
+                                      cudaStream_t);                                               \
+    template void launch_energy<LP>(const Consts<LP> &, const PRec<LP> *, int, double *, int,       \
+                                    double *, cudaStream_t);
 
 HIDEM_INSTANTIATE(float)
 HIDEM_INSTANTIATE(double)

@@ -150,6 +150,11 @@ void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slot
                        const int *linkA, const int *linkB, const int *sideSlot, uint8_t *sState,
                        const LP *sL0, long long L, long long step, int2 *events,
                        unsigned long long *eventCount, long long eventCap, cudaStream_t s);
+// Kinetic energy of the particles (double precision): out[0] translational, out[1]
+// rotational, out[2] largest squared speed; `partial` holds 3 * nb doubles
+template <class LP>
+void launch_energy(const Consts<LP> &c, const PRec<LP> *rec, int n, double *partial, int nb,
+                   double *out, cudaStream_t s);
 template <class LP>
 void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb, cudaStream_t s);
 

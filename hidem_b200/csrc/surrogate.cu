@@ -136,9 +136,11 @@ __device__ __forceinline__ void set_err(int *flag, int code) {
     if (flag) atomicCAS(flag, 0, code);
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU and its derivative with the fast exponential and division (the network trains in
+// BF16; these need no IEEE rounding)
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
+    const float s = __fdividef(1.0f, 1.0f + __expf(-z));
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -164,7 +166,7 @@ struct GemmArgs {
 };
 
 constexpr int kGemmStages = 4;
-constexpr int kGemmThreads = 128;
+constexpr int kGemmThreads = 256;
 
 template <int BN>
 constexpr size_t gemm_smem_bytes() {
@@ -173,8 +175,8 @@ constexpr size_t gemm_smem_bytes() {
 
 // One CTA: rows [128 * blockIdx.x, +128) x all BN columns, K tiles
 // [kTiles * blockIdx.y, +kTiles). Thread 0 streams A / B tiles with TMA and issues the
-// MMAs (4 of K = 16 per 64-wide tile); the four warps then read the accumulator (warp w:
-// lanes / rows 32w..32w+31) and apply the epilogue.
+// MMAs (4 of K = 16 per 64-wide tile); the eight warps then read the accumulator (warp w:
+// lanes / rows 32 (w % 4) .. +31, column half w / 4) and apply the epilogue.
 template <int BN, int EPI>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
@@ -265,45 +267,39 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     tc_fence_after();
     __syncthreads();
     if (accReady && !sFail) {
-        const int row = m0 + warp * 32 + (tid & 31);
+        // The accumulator lane of a thread is one row; stores are made coalesced by
+        // passing each 32 x 32 block through shared memory (the pipeline stages are free
+        // now): lane j then writes column c0 + j of 32 consecutive rows.
+        float *stage = reinterpret_cast<float *>(sm) + warp * 32 * 33;
+        const int lane = tid & 31;
+        const int quarter = warp & 3;
+        const int rowBase = m0 + quarter * 32;
+        const uint32_t tlane = (uint32_t)(quarter * 32) << 16;
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            float v[16];
-            tm_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            const long long o = (long long)row * g.ldo + c0;
-            if (EPI == EPI_F32) {
-                float *dst = g.outF + blockIdx.y * g.splitStride + o;
+        for (int c0 = (warp >> 2) * (BN / 2); c0 < ((warp >> 2) + 1) * (BN / 2); c0 += 32) {
+            float v[32];
+            tm_ld16(tmem + tlane + (uint32_t)c0, v);
+            tm_ld16(tmem + tlane + (uint32_t)(c0 + 16), v + 16);
 #pragma unroll
-                for (int j = 0; j < 16; j += 4) {
-                    float4 q;
-                    q.x = v[j] + (g.bias ? g.bias[c0 + j] : 0.f);
-                    q.y = v[j + 1] + (g.bias ? g.bias[c0 + j + 1] : 0.f);
-                    q.z = v[j + 2] + (g.bias ? g.bias[c0 + j + 2] : 0.f);
-                    q.w = v[j + 3] + (g.bias ? g.bias[c0 + j + 3] : 0.f);
-                    *reinterpret_cast<float4 *>(dst + j) = q;
+            for (int j = 0; j < 32; ++j) stage[lane * 33 + j] = v[j];
+            __syncwarp();
+            const int col = c0 + lane;
+            const float bias = g.bias ? g.bias[col] : 0.f;
+#pragma unroll 4
+            for (int r = 0; r < 32; ++r) {
+                const float acc = stage[r * 33 + lane];
+                const long long o = (long long)(rowBase + r) * g.ldo + col;
+                if (EPI == EPI_F32) {
+                    g.outF[blockIdx.y * g.splitStride + o] = acc + bias;
+                } else if (EPI == EPI_BIAS_SILU) {
+                    const float z = acc + bias;
+                    if (g.zOut) g.zOut[o] = z;
+                    g.outH[o] = __float2bfloat16_rn(silu(z));
+                } else {
+                    g.outH[o] = __float2bfloat16_rn(acc * silu_grad(g.zIn[o]));
                 }
-            } else if (EPI == EPI_BIAS_SILU) {
-                __align__(16) bf16 h[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const float z = v[j] + g.bias[c0 + j];
-                    v[j] = z;
-                    h[j] = __float2bfloat16_rn(silu(z));
-                }
-                if (g.zOut) {
-#pragma unroll
-                    for (int j = 0; j < 16; j += 4)
-                        *reinterpret_cast<float4 *>(g.zOut + o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-                }
-                *reinterpret_cast<uint4 *>(g.outH + o) = *reinterpret_cast<const uint4 *>(h);
-                *reinterpret_cast<uint4 *>(g.outH + o + 8) = *reinterpret_cast<const uint4 *>(h + 8);
-            } else {
-                __align__(16) bf16 h[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) h[j] = __float2bfloat16_rn(v[j] * silu_grad(g.zIn[o + j]));
-                *reinterpret_cast<uint4 *>(g.outH + o) = *reinterpret_cast<const uint4 *>(h);
-                *reinterpret_cast<uint4 *>(g.outH + o + 8) = *reinterpret_cast<const uint4 *>(h + 8);
             }
+            __syncwarp();
         }
     } else if (tid == 0 && !accReady) {
         set_err(g.err, 2);

@@ -124,6 +124,12 @@ class HiDEMLib:
     def step(self, nsteps: int = 1) -> None:
         self._check(self._lib.hidem_step(self._ctx, int(nsteps)))
 
+    def kinetic_energy(self) -> tuple[float, float, float]:
+        """(translational, rotational, max speed) of the current state."""
+        t, r, v = C.c_double(), C.c_double(), C.c_double()
+        self._check(self._lib.hidem_kinetic_energy(self._ctx, C.byref(t), C.byref(r), C.byref(v)))
+        return t.value, r.value, v.value
+
     def set_step_kernel(self, kernel: int) -> None:
         """abi.STEP_KERNEL_* (AUTO: timed on the first fused steps)."""
         self._check(self._lib.hidem_set_step_kernel(self._ctx, int(kernel)))

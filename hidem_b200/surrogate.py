@@ -125,3 +125,30 @@ class Surrogate:
             self.close()
         except Exception:
             pass
+
+
+def _main(argv=None) -> None:
+    """python -m hidem_b200.surrogate [--rows N] [--repeat R]: forward throughput of the
+    default network on N random rows (the tensor-core GEMMs and their epilogues)."""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rows", type=int, default=1 << 20)
+    ap.add_argument("--repeat", type=int, default=3)
+    a = ap.parse_args(argv)
+    cfg = default_config()
+    u = np.random.default_rng(0).uniform(-1, 1, (a.rows, N_IN)).astype(np.float32)
+    with Surrogate(cfg) as net:
+        net.predict(u[: min(a.rows, 16384)])
+        best = float("inf")
+        for _ in range(a.repeat):
+            t0 = time.perf_counter()
+            net.predict(u)
+            best = min(best, time.perf_counter() - t0)
+    flops = 2.0 * a.rows * (N_FEAT * cfg.width + (cfg.hidden_layers - 1) * cfg.width ** 2 + N_OUT * cfg.width)
+    print(json.dumps({"rows": a.rows, "seconds": best, "tflops": flops / best / 1e12}))
+
+
+if __name__ == "__main__":
+    _main()

@@ -253,6 +253,16 @@ hidem_status hidem_links_by_distance(const hidem_particle_soa *p, int64_t n, int
                                      double scale, hidem_link_soa *out, int64_t cap,
                                      int64_t *count);
 
+/* ---- diagnostics ------------------------------------------------------ */
+
+/* Kinetic energy of the current state, the convergence measure of settling runs (no
+ * counterpart in the reference's step loop): translational and rotational energy summed
+ * over the particles, with velocities diff / dt and the integrate step's mass rho d^3 and
+ * moment of inertia m d^2 / 6 (MainMeshBlock.cpp:228-229); max_speed the largest particle
+ * speed. Any output pointer may be NULL. Synchronises the context's stream. */
+hidem_status hidem_kinetic_energy(hidem_ctx *ctx, double *translational, double *rotational,
+                                  double *max_speed);
+
 /* ---- step kernel choice ----------------------------------------------- */
 
 /* No counterpart in the reference. The fused step has several kernels that give
