@@ -404,6 +404,11 @@ __device__ __forceinline__ PRec<LP> load_rec_head(const PRec<LP> *p) {
     for (int k = 0; k < CHUNKS; ++k) dst[k] = __ldg(src + k);
     return r;
 }
+// Hint the L2 to fetch a line that a later iteration will load (no register, no wait).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // chunks holding x, y, z, d[6], r
 template <class LP>
 constexpr int kContactChunks = (int)((3 * sizeof(double) + 7 * sizeof(LP) + 15) / 16);
@@ -459,7 +464,10 @@ __device__ __forceinline__ void step_thread_particle(const Consts<LP> &c, const 
             const PRec<LP> cur = o;
             if (k + 1 < nn) {
                 o = load_rec_head<LP, HC>(a.in + jn);
-                if (k + 2 < nn) jn = __ldg(nb + (k + 2) * kWarp);
+                if (k + 2 < nn) {
+                    jn = __ldg(nb + (k + 2) * kWarp);
+                    if (k + 3 < nn) prefetch_l2(nb + (k + 3) * kWarp);
+                }
             } else {
                 first_side();
             }
@@ -483,7 +491,13 @@ __device__ __forceinline__ void step_thread_particle(const Consts<LP> &c, const 
 #pragma unroll
                 for (int q = 0; q < 6; ++q) ctn[q] = a.ct[q][si + kWarp];
                 if (brk) l0n = __ldg(a.sL0 + si + kWarp);
-                if (k + 2 < ns) pwnn = __ldg(a.sPartner + si + 2 * kWarp);
+                if (k + 2 < ns) {
+                    pwnn = __ldg(a.sPartner + si + 2 * kWarp);
+                    // the CT and state lines of item k + 2 start their way to L2
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) prefetch_l2(a.ct[q] + si + 2 * kWarp);
+                    prefetch_l2(a.sState + si + 2 * kWarp);
+                }
             }
             if (brk && st != 0) {
                 const uint8_t nst =
