@@ -175,6 +175,19 @@ def empty_links(L: int, precision: int) -> dict:
 
 _lib = None
 
+class HidemMap2d(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("x_points", C.c_int32), ("y_points", C.c_int32),
+                ("x_min", C.c_float), ("y_min", C.c_float), ("x_max", C.c_float), ("y_max", C.c_float)]
+
+
+def map2d(values, x_min: float, y_min: float, x_max: float, y_max: float, precision: int):
+    """A hidem_map2d over `values` [y_points][x_points] (x fastest) in the lp type of
+    `precision`; returns (struct, array) — keep the array alive while the struct is used."""
+    arr = np.ascontiguousarray(values, dtype=lp_dtype(precision))
+    m = HidemMap2d(arr.ctypes.data, arr.shape[1], arr.shape[0], x_min, y_min, x_max, y_max)
+    return m, arr
+
+
 class HidemSurrogateConfig(C.Structure):
     _fields_ = [("hidden_layers", C.c_int32), ("width", C.c_int32), ("fourier_bands", C.c_int32),
                 ("batch", C.c_int32), ("learning_rate", C.c_double), ("seed", C.c_uint64)]
@@ -213,6 +226,8 @@ _PROTOS = [
     ("hidem_get_break_events", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _i64,
                                          C.POINTER(_i64)]),
     ("hidem_get_stats", C.c_int, [C.c_void_p, C.POINTER(HidemStats)]),
+    ("hidem_set_bed_maps", C.c_int, [C.c_void_p, C.POINTER(HidemMap2d), C.POINTER(HidemMap2d)]),
+    ("hidem_set_external_force_maps", C.c_int, [C.c_void_p, C.POINTER(HidemMap2d)]),
     ("hidem_kinetic_energy", C.c_int, [C.c_void_p, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)]),
     ("hidem_set_step_kernel", C.c_int, [C.c_void_p, _i32]),
     ("hidem_get_step_kernel", _i32, [C.c_void_p]),

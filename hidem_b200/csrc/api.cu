@@ -118,6 +118,11 @@ struct hidem_ctx {
 
     double *energyBuf = nullptr;  // kinetic-energy partials + result
     int energyBlocks = 0;
+
+    // GlacierDem maps on the device: 0 bed height, 1 bed friction, 2..7 external forces
+    void *mapData[8] = {};
+    Map2dView mapView[8] = {};
+    bool mapSet[8] = {};
 };
 
 namespace {
@@ -241,6 +246,21 @@ hidem_status check_params(hidem_ctx *ctx, const hidem_params *p) {
     return HIDEM_OK;
 }
 
+// The maps set on the context, in both precisions' constants.
+template <class LP>
+void attach_maps_to(const hidem_ctx *ctx, Consts<LP> &c) {
+    c.bedMap = ctx->mapView[0];
+    c.fricMap = ctx->mapView[1];
+    for (int k = 0; k < 6; ++k) c.extMap[k] = ctx->mapView[2 + k];
+    c.useBedMap = ctx->mapSet[0] ? 1 : 0;
+    c.useFricMap = ctx->mapSet[1] ? 1 : 0;
+    c.useExtMaps = ctx->mapSet[2] ? 1 : 0;
+}
+void attach_maps(hidem_ctx *ctx) {
+    attach_maps_to<float>(ctx, ctx->cf);
+    attach_maps_to<double>(ctx, ctx->cd);
+}
+
 hidem_status apply_params(hidem_ctx *ctx, const hidem_params *p) {
     TRY(check_params(ctx, p));
     ctx->P = *p;
@@ -249,6 +269,7 @@ hidem_status apply_params(hidem_ctx *ctx, const hidem_params *p) {
     double sd, id;
     derive<float>(*p, ctx->cf, sd, id);
     derive<double>(*p, ctx->cd, ctx->searchDistance, ctx->interactDist);
+    attach_maps(ctx);
     if (ctx->mixed) {
         ctx->searchDistance = sd;
         ctx->interactDist = id;
@@ -1269,6 +1290,8 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->diffMax);
     dfree(ctx->errorFlag);
     for (cudaEvent_t e : ctx->evPool) cudaEventDestroy(e);
+    for (void *m : ctx->mapData)
+        if (m) cudaFree(m);
     dfree(ctx->energyBuf);
     for (cudaEvent_t e : ctx->tuneEv)
         if (e) cudaEventDestroy(e);
@@ -1803,6 +1826,58 @@ hidem_status hidem_kinetic_energy(hidem_ctx *ctx, double *translational, double 
     if (translational) *translational = h[0];
     if (rotational) *rotational = h[1];
     if (max_speed) *max_speed = std::sqrt(h[2]);
+    return HIDEM_OK;
+}
+
+// one map to the device (slot), or the slot cleared (m == NULL)
+static hidem_status set_map(hidem_ctx *ctx, int slot, const hidem_map2d *m) {
+    if (ctx->mapData[slot]) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->mapData[slot]);
+        ctx->mapData[slot] = nullptr;
+    }
+    ctx->mapSet[slot] = false;
+    ctx->mapView[slot] = Map2dView{};
+    if (!m) return HIDEM_OK;
+    if (!m->data || m->x_points < 2 || m->y_points < 2 || !(m->x_max > m->x_min) || !(m->y_max > m->y_min))
+        return fail(ctx, HIDEM_ERR_ARG, "map %d: needs data, at least 2 x 2 points and max > min", slot);
+    const size_t bytes = ctx->lp * (size_t)m->x_points * (size_t)m->y_points;
+    CK(cudaMalloc(&ctx->mapData[slot], bytes));
+    CK(cudaMemcpyAsync(ctx->mapData[slot], m->data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    Map2dView v{};
+    v.data = ctx->mapData[slot];
+    v.xPoints = m->x_points;
+    v.yPoints = m->y_points;
+    v.xMin = m->x_min;
+    v.yMin = m->y_min;
+    v.xMax = m->x_max;
+    v.yMax = m->y_max;
+    // grid metrics as the Map2d constructor computes them, in float (Map2d.h:43-58)
+    v.xRes = (v.xMax - v.xMin) / (float)(v.xPoints - 1);
+    v.yRes = (v.yMax - v.yMin) / (float)(v.yPoints - 1);
+    v.invXMaxMin = 1.0f / (v.xMax - v.xMin);
+    v.invYMaxMin = 1.0f / (v.yMax - v.yMin);
+    ctx->mapView[slot] = v;
+    ctx->mapSet[slot] = true;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_set_bed_maps(hidem_ctx *ctx, const hidem_map2d *bed, const hidem_map2d *friction) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    TRY(set_map(ctx, 0, bed));
+    TRY(set_map(ctx, 1, friction));
+    attach_maps(ctx);
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HIDEM_OK;
+}
+
+hidem_status hidem_set_external_force_maps(hidem_ctx *ctx, const hidem_map2d *maps) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    for (int k = 0; k < 6; ++k) TRY(set_map(ctx, 2 + k, maps ? &maps[k] : nullptr));
+    attach_maps(ctx);
+    CK(cudaStreamSynchronize(ctx->stream));
     return HIDEM_OK;
 }
 

@@ -52,6 +52,14 @@ struct alignas(16) PRec<double> {
 static_assert(sizeof(PRec<float>) == 64, "mixed particle record must be 64 bytes");
 static_assert(sizeof(PRec<double>) == 128, "fp64 particle record must be 128 bytes");
 
+// A regular 2-D map in the reference's Map2d form (PLiB/Geometry/Map2d.h:23-60): lp
+// values, x fastest; the grid metrics in float as the Map2d constructor computes them.
+struct Map2dView {
+    const void *data;
+    float xMin, yMin, xMax, yMax, xRes, yRes, invXMaxMin, invYMaxMin;
+    int xPoints, yPoints;
+};
+
 // Constants of the default functors and of the sample integrate step, in lp
 // precision, computed on the host exactly as the sample main computes them
 // (HiDEM/MeshBlock/MainMeshBlock.cpp:106-156).
@@ -70,6 +78,9 @@ struct Consts {
     double lower[3], upper[3];
     int bmin[3], bmax[3];
     int useBed, useVel, useBnd, useFixed, useFront;
+    // GlacierDem bed / friction maps and external force maps (x, y, z, u, v, w)
+    Map2dView bedMap, fricMap, extMap[6];
+    int useBedMap, useFricMap, useExtMaps;
 };
 
 // Grid of the last rebuild (NeighbourGrid members, PLiB/NeighbourGrid.h:25-52).

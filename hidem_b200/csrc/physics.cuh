@@ -168,6 +168,44 @@ __device__ __forceinline__ uint8_t break_link(const Consts<LP> &c, const PRec<LP
     return break_link<LP>(c.bendBreak, c.maxLoad, a, b, state, initialLen);
 }
 
+// Map2d::interp (PLiB/Geometry/Map2d.h:93-152, indices from getIndexes 93-111):
+// bilinear interpolation on the map's grid in float arithmetic, the cell corner found by
+// floor and clamped to the grid, the edge cases of a degenerate cell handled as there.
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+template <class LP>
+__device__ __forceinline__ LP map_interp(const Map2dView &m, float x, float y) {
+    const LP *d = static_cast<const LP *>(m.data);
+    // (the float value is clamped before the integer conversion, which leaves every
+    // in-range index as it is)
+    float fx = floorf(((x - m.xMin) * m.invXMaxMin) * (float)(m.xPoints - 1));
+    float fy = floorf(((y - m.yMin) * m.invYMaxMin) * (float)(m.yPoints - 1));
+    fx = fminf(fmaxf(fx, -1.0f), (float)m.xPoints);
+    fy = fminf(fmaxf(fy, -1.0f), (float)m.yPoints);
+    const int xp = (int)fx, yp = (int)fy;
+    const int xl = clampi(xp, 0, m.xPoints - 1), yl = clampi(yp, 0, m.yPoints - 1);
+    const int xh = clampi(xp + 1, 0, m.xPoints - 1), yh = clampi(yp + 1, 0, m.yPoints - 1);
+    if (xl == xh && yl == yh) return d[xl + yl * m.xPoints];
+    const float v00 = (float)d[xl + yl * m.xPoints];
+    const float v01 = (float)d[xl + yh * m.xPoints];
+    const float v10 = (float)d[xh + yl * m.xPoints];
+    const float v11 = (float)d[xh + yh * m.xPoints];
+    const float x0 = x - m.xMin, y0 = y - m.yMin;
+    const float x1 = (float)xl * m.xRes, x2 = (float)xh * m.xRes;
+    const float y1 = (float)yl * m.yRes, y2 = (float)yh * m.yRes;
+    const float invX21 = 1.0f / (x2 - x1);
+    const float c1 = (x2 - x0) * invX21, c2 = (x0 - x1) * invX21;
+    float fxy1 = (c1 * v00) + (c2 * v10);
+    float fxy2 = (c1 * v01) + (c2 * v11);
+    if (xl == xh) {
+        fxy1 = v00;
+        fxy2 = v01;
+    } else if (yl == yh) {
+        return (LP)fxy1;
+    }
+    const float invY21 = 1.0f / (y2 - y1);
+    return (LP)((((y2 - y0) * invY21) * fxy1) + (((y0 - y1) * invY21) * fxy2));
+}
+
 // The sample integrate step on one particle (HiDEM/MeshBlock/MainMeshBlock.cpp:182-261:
 // gravity / buoyancy, air / water drag, HiDEMDefTimeIntegration
 // HiDEMDefaultFunctions.h:318-370) plus the optional GlacierDem bed terms
@@ -188,9 +226,14 @@ __device__ __forceinline__ void integrate_particle(const Consts<LP> &c, PRec<LP>
     const LP radius = p.r;
     const LP diameter = radius * LP(2);
 
+    // bed height and friction under the particle: the GlacierDem maps
+    // (InputBed::getHeight / getFric, PLiB/Geometry/InputGeometry.h:58-68) or constants
+    LP bedHeight = c.bedHeight, bedFriction = c.bedFriction;
+    if (c.useBed && c.useBedMap) bedHeight = map_interp<LP>(c.bedMap, (float)xCord, (float)yCord);
     LP dragCoeff;
-    if (c.useBed && ((zCord + (double)radius) - (double)c.bedHeight < (double)c.bedInteract)) {
-        LP a = c.bedDrag * c.bedFriction;
+    if (c.useBed && ((zCord + (double)radius) - (double)bedHeight < (double)c.bedInteract)) {
+        if (c.useFricMap) bedFriction = map_interp<LP>(c.fricMap, (float)xCord, (float)yCord);
+        LP a = c.bedDrag * bedFriction;
         LP b = LP(1e+5) * c.scale * c.scale;
         dragCoeff = (b < a) ? b : a;  // std::min(a, b)
     } else if (zCord > (double)c.waterLevel) {
@@ -205,9 +248,19 @@ __device__ __forceinline__ void integrate_particle(const Consts<LP> &c, PRec<LP>
 
     if (zCord > (double)c.waterLevel) zForce = zForce + -c.g * particleMass;
     if (zCord <= (double)c.waterLevel) zForce = zForce + c.lift * particleMass;
-    if (c.useBed && zCord + (double)radius < (double)c.bedHeight)
+    if (c.useBed && zCord + (double)radius < (double)bedHeight)
         zForce = (LP)((double)zForce +
-                      (double)c.bedStiffness * ((double)c.bedHeight - (zCord + (double)radius)));
+                      (double)c.bedStiffness * ((double)bedHeight - (zCord + (double)radius)));
+    // external force maps (ExternalForces, PLiB/ExternalForces.h; MainDem.cpp:211-216)
+    if (c.useExtMaps) {
+        const float fx = (float)xCord, fy = (float)yCord;
+        xForce = xForce + map_interp<LP>(c.extMap[0], fx, fy);
+        yForce = yForce + map_interp<LP>(c.extMap[1], fx, fy);
+        zForce = zForce + map_interp<LP>(c.extMap[2], fx, fy);
+        uForce = uForce + map_interp<LP>(c.extMap[3], fx, fy);
+        vForce = vForce + map_interp<LP>(c.extMap[4], fx, fy);
+        wForce = wForce + map_interp<LP>(c.extMap[5], fx, fy);
+    }
     if (c.useFront && (type & HIDEM_TYPE_FRONT) && zCord < (double)c.waterLevel) {
         LP depth = (LP)((double)c.waterLevel - zCord);
         xForce = xForce - c.rhoWater * c.g * depth * diameter * diameter;

@@ -124,6 +124,16 @@ class HiDEMLib:
     def step(self, nsteps: int = 1) -> None:
         self._check(self._lib.hidem_step(self._ctx, int(nsteps)))
 
+    def set_bed_maps(self, bed=None, friction=None) -> None:
+        """GlacierDem bed height / friction maps (abi.map2d structs, or None)."""
+        self._check(self._lib.hidem_set_bed_maps(self._ctx, C.byref(bed) if bed is not None else None,
+                                                 C.byref(friction) if friction is not None else None))
+
+    def set_external_force_maps(self, maps=None) -> None:
+        """Six external force maps (x, y, z, u, v, w; abi.map2d structs), or None."""
+        arr = (abi.HidemMap2d * 6)(*maps) if maps is not None else None
+        self._check(self._lib.hidem_set_external_force_maps(self._ctx, arr))
+
     def kinetic_energy(self) -> tuple[float, float, float]:
         """(translational, rotational, max speed) of the current state."""
         t, r, v = C.c_double(), C.c_double(), C.c_double()

@@ -40,7 +40,9 @@ def fcc_particles(nx: int, ny: int, nz: int, precision: int, a: float = SQRT2, r
     return p
 
 
-def distance_links(p: dict, precision: int, scale: float = 1.01) -> dict:
+def distance_links(p: dict, precision: int, scale: float = 1.01, lean: bool = False) -> dict:
+    """Links of all pairs within scale * (r_i + r_j). lean: only the fields hidem_set_links
+    needs (ends, state, initial length; the CT history starts at zero), for large sets."""
     lib = abi.load()
     n = p["xCord"].shape[0]
     soa = abi.particle_soa(p, precision, n)
@@ -49,7 +51,11 @@ def distance_links(p: dict, precision: int, scale: float = 1.01) -> dict:
     if st != abi.HIDEM_OK:
         raise abi.HidemError(st, "hidem_links_by_distance (count) failed")
     L = cnt.value
-    links = abi.empty_links(L, precision)
+    if lean:
+        dts = abi.link_dtypes(precision)
+        links = {k: np.zeros(L, dts[k]) for k in ("globalKeyEndA", "globalKeyEndB", "state", "initialLen")}
+    else:
+        links = abi.empty_links(L, precision)
     lsoa = abi.link_soa(links, precision, L)
     st = lib.hidem_links_by_distance(C.byref(soa), n, precision, scale, C.byref(lsoa), L,
                                      C.byref(cnt))
@@ -157,3 +163,55 @@ def ensemble_shard(sizes, world: int, rank: int) -> list[int]:
         if r == rank:
             mine.append(i)
     return sorted(mine)
+
+
+def bed_modes(seed: int, size, amplitude: float, count: int = 8):
+    """Bed heightfield of `count` seeded Fourier modes over a plan of `size` (x, y), total
+    amplitude at most `amplitude`: a function of (x, y)."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.0, 1.0, count)
+    amp *= amplitude / max(amp.sum(), 1e-12)
+    kx = rng.integers(0, 5, count)
+    ky = rng.integers(0, 3, count)
+    kx[(kx == 0) & (ky == 0)] = 1
+    ph = rng.uniform(0, 2 * math.pi, count)
+
+    def height(x, y):
+        out = np.zeros(np.broadcast(x, y).shape)
+        for a, i, j, p in zip(amp, kx, ky, ph):
+            out += a * np.cos(2 * math.pi * (i * x / size[0] + j * y / size[1]) + p)
+        return out
+    return height
+
+
+def slab_on_bed(size=(1200.0, 200.0, 150.0), precision: int = abi.PREC_MIXED, seed: int = 13,
+                amplitude: float = 15.0, water_level: float = 135.0, broken_fraction: float = 0.01,
+                map_resolution: float = 5.0):
+    """FCC slab of `size` whose base follows a bed of 8 seeded Fourier modes (config: 1200 x
+    200 x 150 m, ~50M particles, bed amplitude <= 15 m, water line 135 m), calving front
+    on the x-max face, a seeded fraction of links pre-broken; the bed enters the integrate
+    step as a GlacierDem bed map. Returns (params, particles, links, bed map values
+    [ny][nx], map extents (x_min, y_min, x_max, y_max))."""
+    bed = bed_modes(seed, size[:2], amplitude)
+    nx, ny = (max(1, int(round(s / SQRT2))) for s in size[:2])
+    nz = max(1, int(math.ceil((size[2] + 2 * amplitude) / SQRT2)))
+    p = fcc_particles(nx, ny, nz, precision, origin=(0.0, 0.0, -amplitude), jitter=0.0, seed=seed)
+    b = bed(p["xCord"], p["yCord"])
+    keep = (p["zCord"] >= b + 0.5) & (p["zCord"] <= b + size[2])
+    p = {k: np.ascontiguousarray(v[keep]) for k, v in p.items()}
+    p["globalKeys"][:] = np.arange(p["xCord"].shape[0])
+    xmax = p["xCord"].max()
+    p["type"][p["xCord"] > xmax - 0.25 * SQRT2] |= abi.TYPE_FRONT
+    links = distance_links(p, precision, 1.01, lean=True)
+    rng = np.random.default_rng(seed)
+    L = links["state"].shape[0]
+    k = int(round(broken_fraction * L))
+    if k:
+        links["state"][rng.choice(L, size=k, replace=False)] = 0
+    ext = (-5.0, -5.0, size[0] + 5.0, size[1] + 5.0)
+    mx = int(round((ext[2] - ext[0]) / map_resolution)) + 1
+    my = int(round((ext[3] - ext[1]) / map_resolution)) + 1
+    X, Y = np.meshgrid(np.linspace(ext[0], ext[2], mx), np.linspace(ext[1], ext[3], my))
+    params = block_params(precision, waterLevel=water_level, useBed=1, bedHeight=0.0,
+                          bedFriction=0.3, useFrontPressure=1)
+    return params, p, links, bed(X, Y), ext

@@ -253,6 +253,30 @@ hidem_status hidem_links_by_distance(const hidem_particle_soa *p, int64_t n, int
                                      double scale, hidem_link_soa *out, int64_t cap,
                                      int64_t *count);
 
+/* ---- bed and external force maps ------------------------------------- */
+
+/* A regular 2-D map in the reference's Map2d form (PLiB/Geometry/Map2d.h:23-60): values
+ * (lp: float in HIDEM_PREC_MIXED, double in HIDEM_PREC_FP64) at x_points x y_points grid
+ * points spanning [x_min, x_max] x [y_min, y_max], x fastest (data[ix + iy * x_points]).
+ * Values between points are Map2d::interp's bilinear interpolation in float arithmetic
+ * (Map2d.h:93-152), clamped to the grid outside it. */
+typedef struct hidem_map2d {
+    const void *data;
+    int32_t x_points, y_points;
+    float x_min, y_min, x_max, y_max;
+} hidem_map2d;
+/* The GlacierDem bed (InputBed, PLiB/Geometry/InputGeometry.h:54-78, used by
+ * HiDEM/GlacierDem/MainDem.cpp:176-207): with params.useBed set, the bed height under a
+ * particle is bed(x, y) instead of params.bedHeight, and the bed friction is
+ * friction(x, y) instead of params.bedFriction. Either may be NULL (the constant). The
+ * data is copied. */
+hidem_status hidem_set_bed_maps(hidem_ctx *ctx, const hidem_map2d *bed, const hidem_map2d *friction);
+/* External force maps (ExternalForces, PLiB/ExternalForces.h; MainDem.cpp:211-216): six
+ * maps added to the x, y, z forces and u, v, w moments of every particle at its (x, y)
+ * in the integrate step, after gravity, buoyancy and the bed force. maps: 6 maps, or NULL
+ * to remove them. The data is copied. */
+hidem_status hidem_set_external_force_maps(hidem_ctx *ctx, const hidem_map2d *maps);
+
 /* ---- diagnostics ------------------------------------------------------ */
 
 /* Kinetic energy of the current state, the convergence measure of settling runs (no

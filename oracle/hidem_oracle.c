@@ -15,6 +15,23 @@
 #endif
 #include "hidem_oracle.h"
 
+/* GlacierDem maps of the next runs (slot 0 bed height, 1 bed friction, 2..7 external
+ * forces x y z u v w); the caller keeps the data alive. */
+static hidem_map2d g_maps[8];
+static int g_map_set[8];
+
+void hidem_oracle_set_maps(const hidem_map2d *bed, const hidem_map2d *friction,
+                           const hidem_map2d *ext) {
+    memset(g_maps, 0, sizeof g_maps);
+    memset(g_map_set, 0, sizeof g_map_set);
+    if (bed) { g_maps[0] = *bed; g_map_set[0] = 1; }
+    if (friction) { g_maps[1] = *friction; g_map_set[1] = 1; }
+    if (ext)
+        for (int k = 0; k < 6; ++k) { g_maps[2 + k] = ext[k]; g_map_set[2 + k] = 1; }
+}
+
+static int clampi_(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
 #define LP float
 #define LSQRT sqrtf
 #define LABS fabsf

@@ -36,6 +36,11 @@ int hidem_oracle_run(const hidem_params *P, hidem_particle_soa *p, int64_t n, hi
 
 int hidem_oracle_threads(void);
 
+/* Bed / friction / external force maps used by the integrate step of the next runs
+ * (NULL: none); the data must stay alive while they run. */
+void hidem_oracle_set_maps(const hidem_map2d *bed, const hidem_map2d *friction,
+                           const hidem_map2d *ext);
+
 #ifdef __cplusplus
 }
 #endif

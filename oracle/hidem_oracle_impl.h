@@ -312,6 +312,39 @@ static inline uint8_t SFX(break_test)(const SFX(derived) *d, double x1, double y
 
 /* --------------------------------------------------------- public entries */
 
+/* Map2d::interp (PLiB/Geometry/Map2d.h:113-152) with getIndexes (93-111) and the
+ * constructor's float grid metrics (43-58): bilinear, float arithmetic, clamped. */
+static LP SFX(map_interp)(const hidem_map2d *m, float x, float y) {
+    const LP *d = (const LP *)m->data;
+    const float xRes = (m->x_max - m->x_min) / (float)(m->x_points - 1);
+    const float yRes = (m->y_max - m->y_min) / (float)(m->y_points - 1);
+    const float invX = 1.0f / (m->x_max - m->x_min);
+    const float invY = 1.0f / (m->y_max - m->y_min);
+    float fx = floorf(((x - m->x_min) * invX) * (float)(m->x_points - 1));
+    float fy = floorf(((y - m->y_min) * invY) * (float)(m->y_points - 1));
+    fx = fminf(fmaxf(fx, -1.0f), (float)m->x_points);
+    fy = fminf(fmaxf(fy, -1.0f), (float)m->y_points);
+    int xp = (int)fx, yp = (int)fy;
+    int xl = clampi_(xp, 0, m->x_points - 1), yl = clampi_(yp, 0, m->y_points - 1);
+    int xh = clampi_(xp + 1, 0, m->x_points - 1), yh = clampi_(yp + 1, 0, m->y_points - 1);
+    if (xl == xh && yl == yh) return d[xl + yl * m->x_points];
+    float v00 = (float)d[xl + yl * m->x_points], v01 = (float)d[xl + yh * m->x_points];
+    float v10 = (float)d[xh + yl * m->x_points], v11 = (float)d[xh + yh * m->x_points];
+    float x0 = x - m->x_min, y0 = y - m->y_min;
+    float x1 = (float)xl * xRes, x2 = (float)xh * xRes, y1 = (float)yl * yRes, y2 = (float)yh * yRes;
+    float invX21 = 1.0f / (x2 - x1);
+    float c1 = (x2 - x0) * invX21, c2 = (x0 - x1) * invX21;
+    float fxy1 = (c1 * v00) + (c2 * v10), fxy2 = (c1 * v01) + (c2 * v11);
+    if (xl == xh) {
+        fxy1 = v00;
+        fxy2 = v01;
+    } else if (yl == yh) {
+        return (LP)fxy1;
+    }
+    float invY21 = 1.0f / (y2 - y1);
+    return (LP)((((y2 - y0) * invY21) * fxy1) + (((y0 - y1) * invY21) * fxy2));
+}
+
 static void SFX(get_particle_arrays)(const hidem_particle_soa *p, const LP **th, const LP **df,
                                      const LP **rad) {
     th[0] = (const LP *)p->xTheta;
@@ -560,9 +593,12 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
             LP xTheta = th[0][i], yTheta = th[1][i], zTheta = th[2][i];
             LP radius = rad[i];
             LP diameter = radius * (LP)2;
+            LP bedHeight = d.bedHeight, bedFriction = d.bedFriction;
+            if (useBed && g_map_set[0]) bedHeight = SFX(map_interp)(&g_maps[0], (float)xCord, (float)yCord);
             LP dragCoeff;
-            if (useBed && ((zCord + (double)radius) - (double)d.bedHeight < (double)d.bedInteract)) {
-                LP a = d.bedDrag * d.bedFriction;
+            if (useBed && ((zCord + (double)radius) - (double)bedHeight < (double)d.bedInteract)) {
+                if (g_map_set[1]) bedFriction = SFX(map_interp)(&g_maps[1], (float)xCord, (float)yCord);
+                LP a = d.bedDrag * bedFriction;
                 LP b = (LP)1e+5 * d.scale * d.scale;
                 dragCoeff = (b < a) ? b : a; /* std::min(a, b) */
             } else if (zCord > (double)d.waterLevel) {
@@ -576,9 +612,19 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
             LP particleMomentInertia = particleMass * diameter * diameter / (LP)6;
             if (zCord > (double)d.waterLevel) zForce = zForce + -d.g * particleMass;
             if (zCord <= (double)d.waterLevel) zForce = zForce + d.lift * particleMass;
-            if (useBed && zCord + (double)radius < (double)d.bedHeight)
+            if (useBed && zCord + (double)radius < (double)bedHeight)
                 zForce = (LP)((double)zForce +
-                              (double)d.bedStiffness * ((double)d.bedHeight - (zCord + (double)radius)));
+                              (double)d.bedStiffness * ((double)bedHeight - (zCord + (double)radius)));
+            /* external force maps (MainDem.cpp:211-216) */
+            if (g_map_set[2]) {
+                float fx = (float)xCord, fy = (float)yCord;
+                xForce = xForce + SFX(map_interp)(&g_maps[2], fx, fy);
+                yForce = yForce + SFX(map_interp)(&g_maps[3], fx, fy);
+                zForce = zForce + SFX(map_interp)(&g_maps[4], fx, fy);
+                uForce = uForce + SFX(map_interp)(&g_maps[5], fx, fy);
+                vForce = vForce + SFX(map_interp)(&g_maps[6], fx, fy);
+                wForce = wForce + SFX(map_interp)(&g_maps[7], fx, fy);
+            }
             if (useFront && (ty & HIDEM_TYPE_FRONT) && zCord < (double)d.waterLevel) {
                 LP depth = (LP)((double)d.waterLevel - zCord);
                 xForce = xForce - d.rhoWater * d.g * depth * diameter * diameter;

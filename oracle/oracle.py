@@ -79,6 +79,16 @@ class CpuPath:
     def threads(self) -> int:
         return int(getattr(self.lib, self.prefix + "_threads")())
 
+    def set_maps(self, bed=None, friction=None, ext=None) -> None:
+        """Bed / friction / external force maps (abi.map2d structs) of the next runs; the
+        caller keeps the data arrays alive."""
+        f = getattr(self.lib, self.prefix + "_set_maps")
+        f.argtypes = [_P(abi.HidemMap2d), _P(abi.HidemMap2d), _P(abi.HidemMap2d)]
+        f.restype = None
+        extarr = (abi.HidemMap2d * 6)(*ext) if ext is not None else None
+        f(C.byref(bed) if bed is not None else None, C.byref(friction) if friction is not None else None,
+          extarr)
+
     def _prec(self, params) -> int:
         p = int(params.precision)
         if self.fixed_precision is not None and p != self.fixed_precision:

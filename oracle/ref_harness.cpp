@@ -40,6 +40,7 @@
 #include "NeighbourGrid.h"
 #include "Accel/CombinedAccel.h"
 #include "Geometry/Map.h"
+#include "Geometry/Map2d.h"
 #include "Generators/LinkGenerator.h"
 #include "HiDEMParticleData.h"
 #include "HiDEMLinkData.h"
@@ -47,6 +48,9 @@
 #include "LinkDataHandler.h"
 
 #include "hidem_b200.h"
+
+// maps of the next sessions (slot 0 bed height, 1 bed friction, 2..7 external forces)
+static Map2d<lpReal_t> *g_maps[8] = {};
 
 using PData = ParticleDataHandler<HiDEMParticleData>;
 using LData = LinkDataHandler<HiDEMLinkData>;
@@ -335,6 +339,8 @@ struct RefSession {
     }
 
     // computePartForce + applyForce + gated linkUpdate + finalizeTs (MainMeshBlock.cpp:295-320).
+    // The bed / friction / external force maps, when set, are the reference's own Map2d
+    // (PLiB/Geometry/Map2d.h), used as GlacierDem uses them (MainDem.cpp:176-216).
     void rest_of_step() {
         PData &pData = *pd;
         LData &lData = *ld;
@@ -367,9 +373,11 @@ struct RefSession {
             lpReal_t radius = p.radius[pInd];
             lpReal_t diameter = radius * lpReal_t(2.0);
 
+            lpReal_t bedzCord = (useBed && g_maps[0]) ? g_maps[0]->interp(xCord, yCord) : dd.bedHeight;
             lpReal_t dragCoeff;
-            if (useBed && (zCord + radius) - dd.bedHeight < dd.bedInteract) {
-                dragCoeff = std::min(dd.bedDrag * dd.bedFriction, lpReal_t(1e+5) * dd.scale * dd.scale);
+            if (useBed && (zCord + radius) - bedzCord < dd.bedInteract) {
+                lpReal_t fric = g_maps[1] ? g_maps[1]->interp(xCord, yCord) : dd.bedFriction;
+                dragCoeff = std::min(dd.bedDrag * fric, lpReal_t(1e+5) * dd.scale * dd.scale);
             } else if (zCord > dd.waterLevel) {
                 dragCoeff = dd.airDrag;
             } else {
@@ -383,8 +391,16 @@ struct RefSession {
 
             if (zCord > dd.waterLevel) zForce += -dd.g * particleMass;
             if (zCord <= dd.waterLevel) zForce += dd.lift * particleMass;
-            if (useBed && zCord + radius < dd.bedHeight)
-                zForce += dd.bedStiffness * (dd.bedHeight - (zCord + radius));
+            if (useBed && zCord + radius < bedzCord)
+                zForce += dd.bedStiffness * (bedzCord - (zCord + radius));
+            if (g_maps[2]) {
+                xForce += g_maps[2]->interp(xCord, yCord);
+                yForce += g_maps[3]->interp(xCord, yCord);
+                zForce += g_maps[4]->interp(xCord, yCord);
+                uForce += g_maps[5]->interp(xCord, yCord);
+                vForce += g_maps[6]->interp(xCord, yCord);
+                wForce += g_maps[7]->interp(xCord, yCord);
+            }
             if (useFront && (type & HIDEM_TYPE_FRONT) && zCord < dd.waterLevel) {
                 lpReal_t depth = (lpReal_t)(dd.waterLevel - zCord);
                 xForce -= dd.rhoWater * dd.g * depth * diameter * diameter;
@@ -530,6 +546,27 @@ int hidem_ref_advance(void *h, int32_t nsteps, double *seconds) {
 }
 
 void hidem_ref_close(void *h) { delete static_cast<RefSession *>(h); }
+
+// Bed / friction / external force maps of the next sessions (NULL: none), built as the
+// reference's Map2d objects (grid points, then the values point by point).
+void hidem_ref_set_maps(const hidem_map2d *bed, const hidem_map2d *friction, const hidem_map2d *ext) {
+    for (auto &m : g_maps) {
+        delete m;
+        m = nullptr;
+    }
+    auto make = [](const hidem_map2d *src) {
+        auto *m = new Map2d<lpReal_t>(src->x_points, src->y_points, src->x_min, src->y_min, src->x_max,
+                                      src->y_max);
+        const lpReal_t *v = static_cast<const lpReal_t *>(src->data);
+        for (int y = 0; y < src->y_points; ++y)
+            for (int x = 0; x < src->x_points; ++x) m->setPointInd(x, y, v[x + y * src->x_points]);
+        return m;
+    };
+    if (bed) g_maps[0] = make(bed);
+    if (friction) g_maps[1] = make(friction);
+    if (ext)
+        for (int k = 0; k < 6; ++k) g_maps[2 + k] = make(&ext[k]);
+}
 
 // One-shot form: setup, nsteps of the loop, write-back (particles in place; links: state
 // and CT), forces of the last step, break events (link index, step), rebuild steps.

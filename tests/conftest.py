@@ -49,3 +49,31 @@ def golden_inputs(g: dict):
     p = {k[len("in_p_"):]: v.copy() for k, v in g.items() if k.startswith("in_p_")}
     l = {k[len("in_l_"):]: v.copy() for k, v in g.items() if k.startswith("in_l_")}
     return P, p, l
+
+
+def maps_case(precision):
+    """A 4^3-cell block resting on a GlacierDem bed map (some particles below the bed,
+    most within bedInteract), with a friction map and six external force maps; returns
+    (params, particles, links, (bed, friction, ext), arrays to keep alive)."""
+    from hidem_b200 import abi, workloads
+    P, p, l = workloads.ice_block(cells=(4, 4, 4), precision=precision, seed=21, fixed_bottom=False,
+                                  useBed=1, bedInteract=2.0, bedFriction=0.3, waterLevel=2.0)
+    nx, ny = 13, 9
+    xs = np.linspace(-1.0, 7.0, nx)
+    ys = np.linspace(-1.0, 7.0, ny)
+    X, Y = np.meshgrid(xs, ys)  # [ny][nx], x fastest
+    zmin = float(p["zCord"].min())
+    bed_v = zmin + 0.3 * np.sin(0.9 * X) + 0.2 * np.cos(1.3 * Y) + 0.1
+    fric_v = 0.3 + 0.1 * np.sin(X + Y)
+    keep = []
+    bed, a = abi.map2d(bed_v, -1.0, -1.0, 7.0, 7.0, precision)
+    keep.append(a)
+    fric, a = abi.map2d(fric_v, -1.0, -1.0, 7.0, 7.0, precision)
+    keep.append(a)
+    ext = []
+    for k in range(6):
+        v = (2000.0 if k < 3 else 50.0) * np.cos(0.7 * X + 0.4 * k) * np.sin(0.5 * Y - 0.3 * k)
+        m, a = abi.map2d(v, -1.5, -0.5, 6.5, 7.5, precision)
+        ext.append(m)
+        keep.append(a)
+    return P, p, l, (bed, fric, ext), keep

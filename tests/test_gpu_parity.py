@@ -166,6 +166,39 @@ def test_gpu_matches_oracle_live(gpu, precision, variant):
 
 
 @pytest.mark.parametrize("precision", PRECS)
+@pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD_CAPPED])
+def test_gpu_bed_and_force_maps_match_oracle(gpu, precision, kernel):
+    from conftest import maps_case
+    P, p, l, (bed, fric, ext), keep = maps_case(precision)
+    port = oracle.port()
+    port.set_maps(bed, fric, ext)
+    try:
+        ref = port.run(P, p, l, 40)
+    finally:
+        port.set_maps()
+    for mode in ("fused", "split"):
+        lib = HiDEMLib(P)
+        lib.set_step_kernel(kernel)
+        lib.set_bed_maps(bed, fric)
+        lib.set_external_force_maps(ext)
+        lib.set_particles(p)
+        lib.set_links(l)
+        if mode == "fused":
+            lib.step(40)
+        else:
+            for _ in range(40):
+                lib.timestep_split()
+        out_p, out_l = lib.get_particles(), lib.get_links()
+        lib.set_bed_maps(None, None)
+        lib.set_external_force_maps(None)
+        lib.close()
+        for k in P_OUT:
+            assert np.array_equal(out_p[k], ref[0][k]), (mode, k)
+        for k in L_OUT:
+            assert np.array_equal(out_l[k], ref[1][k]), (mode, k)
+
+
+@pytest.mark.parametrize("precision", PRECS)
 def test_gpu_config0_1000_steps_bit_exact(gpu, precision):
     """The CPU-runnable configuration: 20^3 FCC cells (32,000 spheres), 1000 steps."""
     P, p, l = workloads.ice_block(cells=(20, 20, 20), precision=precision, seed=1)

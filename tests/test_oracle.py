@@ -84,6 +84,33 @@ def test_oracle_matches_reference_live(precision, variant):
 
 
 @needs_ref
+@needs_ref
+@pytest.mark.parametrize("precision", [abi.PREC_MIXED, abi.PREC_FP64])
+def test_oracle_bed_and_force_maps_match_reference(precision):
+    """GlacierDem bed height / friction maps and external force maps: the restatement's
+    interpolation and integrate terms against the reference's own Map2d."""
+    from conftest import maps_case
+    P, p, l, (bed, fric, ext), keep = maps_case(precision)
+    port = oracle.port()
+    ref = oracle.reference(precision)
+    port.set_maps(bed, fric, ext)
+    ref.set_maps(bed, fric, ext)
+    try:
+        a = port.run(P, p, l, 40)
+        b = ref.run(P, p, l, 40)
+    finally:
+        port.set_maps()
+        ref.set_maps()
+    for k in P_OUT:
+        assert np.array_equal(a[0][k], b[0][k]), k
+    for k in L_OUT:
+        assert np.array_equal(a[1][k], b[1][k]), k
+    assert np.array_equal(a[3], b[3])
+    # the maps mattered: the same run without them differs
+    c = port.run(P, p, l, 40)
+    assert not np.array_equal(a[0]["zCord"], c[0]["zCord"])
+
+
 @pytest.mark.parametrize("precision", [abi.PREC_MIXED, abi.PREC_FP64])
 def test_oracle_contact_list_matches_reference_on_irregular_input(precision):
     rng = np.random.default_rng(5)
