@@ -39,7 +39,7 @@ sys.path.insert(0, str(ROOT))
 PUBLISHED_MIXED = 5723826 * 5000 / 25.83
 
 # step kernels of the library (hidem_set_step_kernel)
-KERNELS = {"auto": 0, "items": 1, "thread": 2, "thread-capped": 3}
+KERNELS = {"auto": 0, "items": 1, "thread": 2, "thread-capped": 3, "thread-async": 4}
 KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
 
 
@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--train-steps", type=int, default=20000, help="settle: surrogate Adam steps")
     ap.add_argument("--blocks", type=int, default=256, help="ensemble: number of blocks")
     ap.add_argument("--no-graphs", action="store_true", help="ensemble: plain launches")
-    ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped"],
+    ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped", "thread-async"],
                     default="auto", help="step kernel (auto: timed on the first steps)")
     ap.add_argument("--slab", default="400,100,100",
                     help="slab size in metres x,y,z (smaller slabs for profiling captures)")
@@ -513,7 +513,7 @@ def main_topo(args):
     lib.set_particles(p)
     lib.set_links(l)
     del p, l
-    warm = max(args.warmup, 12)
+    warm = max(args.warmup, 15)
     lib.step(warm)
     lib.synchronize()
     setup_s = time.perf_counter() - t0
@@ -632,7 +632,7 @@ def main():
     lib.set_links(l)
     stream = torch.cuda.ExternalStream(lib.stream_handle)
     # warm-up: at least the autotuner's rounds, so the timed steps use its choice
-    warm = max(args.warmup, 12) if args.kernel == "auto" else args.warmup
+    warm = max(args.warmup, 15) if args.kernel == "auto" else args.warmup
     lib.step(warm)
     lib.synchronize()
     st0 = lib.stats()
@@ -707,12 +707,17 @@ def main():
             pg.barrier()
         t0 = time.perf_counter()
         lib2.set_particles(pp)
+        ta = time.perf_counter()
         lib2.set_links(ll)
+        tb = time.perf_counter()
         lib2.step(args.steps)
+        tc = time.perf_counter()
         lib2.get_particles(outp)
         lib2.synchronize()
         t1 = time.perf_counter()
         el = t1 - t0
+        parts = {"set_particles_s": ta - t0, "set_links_s": tb - ta, "steps_s": tc - tb,
+                 "get_particles_s": t1 - tc}
         if pg:
             t = torch.tensor([el], device="cuda", dtype=torch.float64)
             pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -723,7 +728,7 @@ def main():
         e2e = {"value": world * n * args.steps / el, "unit": "particle-steps/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "step": f"one C-ABI job from pinned host arrays: upload state, {args.steps} "
-                       f"timesteps, download particles"}
+                       f"timesteps, download particles", "breakdown": parts}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

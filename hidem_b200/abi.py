@@ -26,6 +26,7 @@ STEP_KERNEL_AUTO = 0
 STEP_KERNEL_ITEMS = 1
 STEP_KERNEL_THREAD = 2
 STEP_KERNEL_THREAD_CAPPED = 3
+STEP_KERNEL_THREAD_ASYNC = 4
 
 _d = C.c_double
 _i32 = C.c_int32

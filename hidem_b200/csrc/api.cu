@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -85,9 +86,9 @@ struct hidem_ctx {
     int32_t *sideSlot[2] = {nullptr, nullptr};
     SideSet side[2];
     int curSide = 0;  // always 0: rebuild swaps the new layout into side[0]
-    std::vector<int32_t> linkOwners;
-    std::vector<int64_t> linkKeys, linkKeyA, linkKeyB;
-    std::vector<int32_t> linkNum;
+    // the caller's link fields the step never reads, kept on the device for get_links
+    int32_t *dLinkOwners = nullptr, *dLinkNum = nullptr;
+    long long *dLinkKeys = nullptr, *dLinkKeyA = nullptr, *dLinkKeyB = nullptr;
 
     // particle metadata kept on the host (input order)
     std::vector<int32_t> owners;
@@ -114,7 +115,7 @@ struct hidem_ctx {
     int stepKernel = HIDEM_STEP_KERNEL_AUTO;
     int tunedKernel = HIDEM_STEP_KERNEL_AUTO;
     int tuneStep = 0;
-    cudaEvent_t tuneEv[2 * 9] = {};
+    cudaEvent_t tuneEv[2 * 12] = {};
 
     double *energyBuf = nullptr;  // kinetic-energy partials + result
     int energyBlocks = 0;
@@ -649,22 +650,23 @@ hidem_status profile_pair(hidem_ctx *ctx, cudaEvent_t *e0, cudaEvent_t *e1) {
 // Step-kernel autotuner: the first kTuneRounds * 3 fused steps of a context cycle
 // through the candidate kernels with an event pair around each launch; after the rounds
 // have run, the fastest (summed over all but the first round) is kept.
-constexpr int kTuneCandidates[3] = {HIDEM_STEP_KERNEL_ITEMS, HIDEM_STEP_KERNEL_THREAD,
-                                    HIDEM_STEP_KERNEL_THREAD_CAPPED};
+constexpr int kTuneCandidates[] = {HIDEM_STEP_KERNEL_ITEMS, HIDEM_STEP_KERNEL_THREAD,
+                                   HIDEM_STEP_KERNEL_THREAD_CAPPED, HIDEM_STEP_KERNEL_THREAD_ASYNC};
+constexpr int kNumCandidates = (int)(sizeof(kTuneCandidates) / sizeof(int));
 constexpr int kTuneRounds = 3;
 
 int step_kernel_now(hidem_ctx *ctx, cudaEvent_t *e0, cudaEvent_t *e1) {
     *e0 = *e1 = nullptr;
     if (ctx->stepKernel != HIDEM_STEP_KERNEL_AUTO) return ctx->stepKernel;
     if (ctx->tunedKernel != HIDEM_STEP_KERNEL_AUTO) return ctx->tunedKernel;
-    if (ctx->tuneStep < 3 * kTuneRounds) {
+    if (ctx->tuneStep < kNumCandidates * kTuneRounds) {
         const int k = ctx->tuneStep++;
         for (int q = 0; q < 2; ++q)
             if (!ctx->tuneEv[2 * k + q] && cudaEventCreate(&ctx->tuneEv[2 * k + q]) != cudaSuccess)
                 ctx->tuneEv[2 * k + q] = nullptr;
         *e0 = ctx->tuneEv[2 * k];
         *e1 = ctx->tuneEv[2 * k + 1];
-        return kTuneCandidates[k % 3];
+        return kTuneCandidates[k % kNumCandidates];
     }
     return HIDEM_STEP_KERNEL_THREAD;  // rounds done, choice made at the next sync
 }
@@ -679,10 +681,10 @@ int step_kernel_settled(const hidem_ctx *ctx) {
 // called after the stream has been synchronised
 void step_kernel_resolve(hidem_ctx *ctx) {
     if (ctx->stepKernel != HIDEM_STEP_KERNEL_AUTO || ctx->tunedKernel != HIDEM_STEP_KERNEL_AUTO ||
-        ctx->tuneStep < 3 * kTuneRounds)
+        ctx->tuneStep < kNumCandidates * kTuneRounds)
         return;
-    double t[3] = {0, 0, 0};
-    for (int k = 3; k < 3 * kTuneRounds; ++k) {
+    double t[kNumCandidates] = {};
+    for (int k = kNumCandidates; k < kNumCandidates * kTuneRounds; ++k) {
         float ms = 0;
         if (!ctx->tuneEv[2 * k] || !ctx->tuneEv[2 * k + 1] ||
             cudaEventElapsedTime(&ms, ctx->tuneEv[2 * k], ctx->tuneEv[2 * k + 1]) != cudaSuccess) {
@@ -690,10 +692,10 @@ void step_kernel_resolve(hidem_ctx *ctx) {
             ctx->tunedKernel = HIDEM_STEP_KERNEL_THREAD;
             return;
         }
-        t[k % 3] += ms;
+        t[k % kNumCandidates] += ms;
     }
     int best = 0;
-    for (int q = 1; q < 3; ++q)
+    for (int q = 1; q < kNumCandidates; ++q)
         if (t[q] < t[best]) best = q;
     ctx->tunedKernel = kTuneCandidates[best];
 }
@@ -878,13 +880,15 @@ struct BatchBind {
     }
 };
 
-// the kernel a batch run uses: the first context's fixed or tuned choice, else the
-// register-capped one-thread-per-particle kernel
+// the kernel a batch run uses: the first context's fixed or tuned choice (the
+// asynchronous-copy kernel has no batched form: its register-capped sibling stands in),
+// else the register-capped one-thread-per-particle kernel
 int batch_kernel(const hidem_batch *b) {
     const hidem_ctx *c = b->ctxs[0];
-    if (c->stepKernel != HIDEM_STEP_KERNEL_AUTO) return c->stepKernel;
-    if (c->tunedKernel != HIDEM_STEP_KERNEL_AUTO) return c->tunedKernel;
-    return HIDEM_STEP_KERNEL_THREAD_CAPPED;
+    int k = HIDEM_STEP_KERNEL_THREAD_CAPPED;
+    if (c->stepKernel != HIDEM_STEP_KERNEL_AUTO) k = c->stepKernel;
+    else if (c->tunedKernel != HIDEM_STEP_KERNEL_AUTO) k = c->tunedKernel;
+    return k == HIDEM_STEP_KERNEL_THREAD_ASYNC ? HIDEM_STEP_KERNEL_THREAD_CAPPED : k;
 }
 
 // Groups of contexts with equal constants apart from the break thresholds (compared
@@ -1290,6 +1294,11 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->diffMax);
     dfree(ctx->errorFlag);
     for (cudaEvent_t e : ctx->evPool) cudaEventDestroy(e);
+    dfree(ctx->dLinkOwners);
+    dfree(ctx->dLinkNum);
+    dfree(ctx->dLinkKeys);
+    dfree(ctx->dLinkKeyA);
+    dfree(ctx->dLinkKeyB);
     for (void *m : ctx->mapData)
         if (m) cudaFree(m);
     dfree(ctx->energyBuf);
@@ -1380,33 +1389,59 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     const long long n = ctx->n;
     const size_t lp = ctx->lp;
     // globalKey -> input index (LinkData::makeLocalPartEnds, PLiB/LinkData.h:91-115):
-    // direct when the keys are 0..n-1 in order, else through a sorted key table
+    // on the device when the keys are 0..n-1 in order, else through a sorted key table on
+    // the host
     bool identity = true;
     for (long long i = 0; i < n && identity; ++i) identity = ctx->keys[i] == i;
-    std::vector<std::pair<int64_t, int32_t>> km;
-    if (!identity) {
-        km.resize((size_t)n);
+    cudaStream_t st = ctx->stream;
+    TRY(dalloc(ctx, &ctx->linkA, L));
+    TRY(dalloc(ctx, &ctx->linkB, L));
+    TRY(dalloc(ctx, &ctx->dLinkKeyA, L));
+    TRY(dalloc(ctx, &ctx->dLinkKeyB, L));
+    if (L > 0) {
+        CK(cudaMemcpyAsync(ctx->dLinkKeyA, l->globalKeyEndA, 8 * (size_t)L, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->dLinkKeyB, l->globalKeyEndB, 8 * (size_t)L, cudaMemcpyHostToDevice, st));
+    }
+    long long bad = -1, self = -1;
+    if (identity) {
+        unsigned long long *mins = nullptr;
+        TRY(dalloc(ctx, &mins, 2));
+        CK(cudaMemsetAsync(mins, 0xff, 2 * sizeof(unsigned long long), st));
+        launch_link_keys_identity(ctx->dLinkKeyA, ctx->dLinkKeyB, L, n, ctx->linkA, ctx->linkB, mins,
+                                  mins + 1, st);
+        unsigned long long h[2];
+        CK(cudaMemcpyAsync(h, mins, sizeof h, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        dfree(mins);
+        if (h[0] != ~0ull) bad = (long long)h[0];
+        if (h[1] != ~0ull) self = (long long)h[1];
+    } else {
+        std::vector<std::pair<int64_t, int32_t>> km((size_t)n);
         for (long long i = 0; i < n; ++i) km[i] = {ctx->keys[i], (int32_t)i};
         std::sort(km.begin(), km.end());
-    }
-    auto find = [&](int64_t key) -> int32_t {
-        if (identity) return (key >= 0 && key < n) ? (int32_t)key : -1;
-        auto it = std::lower_bound(km.begin(), km.end(), std::make_pair(key, (int32_t)-1));
-        if (it == km.end() || it->first != key) return -1;
-        return it->second;
-    };
-    std::vector<int32_t> A((size_t)L), B((size_t)L);
-    long long bad = -1, self = -1;
+        auto find = [&](int64_t key) -> int32_t {
+            auto it = std::lower_bound(km.begin(), km.end(), std::make_pair(key, (int32_t)-1));
+            if (it == km.end() || it->first != key) return -1;
+            return it->second;
+        };
+        std::unique_ptr<int32_t[]> A(new int32_t[(size_t)std::max<long long>(L, 1)]);
+        std::unique_ptr<int32_t[]> B(new int32_t[(size_t)std::max<long long>(L, 1)]);
 #pragma omp parallel for schedule(static)
-    for (long long i = 0; i < L; ++i) {
-        A[i] = find(l->globalKeyEndA[i]);
-        B[i] = find(l->globalKeyEndB[i]);
-        if (A[i] < 0 || B[i] < 0) {
+        for (long long i = 0; i < L; ++i) {
+            A[i] = find(l->globalKeyEndA[i]);
+            B[i] = find(l->globalKeyEndB[i]);
+            if (A[i] < 0 || B[i] < 0) {
 #pragma omp critical
-            if (bad < 0 || i < bad) bad = i;
-        } else if (A[i] == B[i]) {
+                if (bad < 0 || i < bad) bad = i;
+            } else if (A[i] == B[i]) {
 #pragma omp critical
-            if (self < 0 || i < self) self = i;
+                if (self < 0 || i < self) self = i;
+            }
+        }
+        if (bad < 0 && self < 0 && L > 0) {
+            CK(cudaMemcpyAsync(ctx->linkA, A.get(), 4 * (size_t)L, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(ctx->linkB, B.get(), 4 * (size_t)L, cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
         }
     }
     if (bad >= 0)
@@ -1414,8 +1449,6 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
                     (long long)l->globalKeyEndA[bad], (long long)l->globalKeyEndB[bad]);
     if (self >= 0) return fail(ctx, HIDEM_ERR_ARG, "link %lld joins a particle to itself", self);
 
-    TRY(dalloc(ctx, &ctx->linkA, L));
-    TRY(dalloc(ctx, &ctx->linkB, L));
     TRY(dalloc_bytes(ctx, &ctx->L0link, lp * (size_t)std::max<long long>(L, 1)));
     TRY(dalloc(ctx, &ctx->plStart, n + 1));
     TRY(dalloc(ctx, &ctx->plLink, 2 * L));
@@ -1434,12 +1467,9 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     TRY(dalloc(ctx, &deg, n + 1));
     TRY(dalloc(ctx, &cursor, n + 1));
     TRY(dalloc(ctx, &lstate, std::max<long long>(L, 1)));
-    cudaStream_t st = ctx->stream;
     CK(cudaMemsetAsync(deg, 0, 4 * (size_t)(n + 1), st));
     CK(cudaMemsetAsync(cursor, 0, 4 * (size_t)(n + 1), st));
     if (L > 0) {
-        CK(cudaMemcpyAsync(ctx->linkA, A.data(), 4 * (size_t)L, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(ctx->linkB, B.data(), 4 * (size_t)L, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->L0link, l->initialLen, lp * (size_t)L, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(lstate, l->state, (size_t)L, cudaMemcpyHostToDevice, st));
         for (int k = 0; k < 6; ++k) {
@@ -1454,23 +1484,24 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     launch_link_lists(ctx->linkA, ctx->linkB, L, (int)n, deg, ctx->plStart, cursor, ctx->scanSums32,
                       ctx->plLink, ctx->plEnd, st);
     launch_side_init(lstate, L, ctx->sideSlot[0], ctx->side[0].state, st);
-    ctx->launches += 6;
+    ctx->launches += 7;
+    // the fields only get_links returns: copied as given, or their defaults
+    TRY(dalloc(ctx, &ctx->dLinkOwners, L));
+    TRY(dalloc(ctx, &ctx->dLinkNum, L));
+    TRY(dalloc(ctx, &ctx->dLinkKeys, L));
+    if (L > 0) {
+        if (l->owners) CK(cudaMemcpyAsync(ctx->dLinkOwners, l->owners, 4 * (size_t)L, cudaMemcpyHostToDevice, st));
+        else CK(cudaMemsetAsync(ctx->dLinkOwners, 0, 4 * (size_t)L, st));
+        if (l->particleLinkNum) CK(cudaMemcpyAsync(ctx->dLinkNum, l->particleLinkNum, 4 * (size_t)L, cudaMemcpyHostToDevice, st));
+        else CK(cudaMemsetAsync(ctx->dLinkNum, 0, 4 * (size_t)L, st));
+        if (l->globalKeys) CK(cudaMemcpyAsync(ctx->dLinkKeys, l->globalKeys, 8 * (size_t)L, cudaMemcpyHostToDevice, st));
+        else launch_iota64(ctx->dLinkKeys, L, st);
+    }
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
     dfree(deg);
     dfree(cursor);
     dfree(lstate);
-    ctx->linkOwners.assign((size_t)L, 0);
-    ctx->linkKeys.resize((size_t)L);
-    ctx->linkKeyA.assign(l ? l->globalKeyEndA : nullptr, l ? l->globalKeyEndA + L : nullptr);
-    ctx->linkKeyB.assign(l ? l->globalKeyEndB : nullptr, l ? l->globalKeyEndB + L : nullptr);
-    ctx->linkNum.assign((size_t)L, 0);
-    if (L > 0) {
-        if (l->owners) std::memcpy(ctx->linkOwners.data(), l->owners, 4 * (size_t)L);
-        if (l->globalKeys) std::memcpy(ctx->linkKeys.data(), l->globalKeys, 8 * (size_t)L);
-        else for (long long i = 0; i < L; ++i) ctx->linkKeys[i] = i;
-        if (l->particleLinkNum) std::memcpy(ctx->linkNum.data(), l->particleLinkNum, 4 * (size_t)L);
-    }
     ctx->L = L;
     ctx->haveLinks = true;
     ctx->built = false;
@@ -1654,14 +1685,14 @@ hidem_status hidem_get_links(hidem_ctx *ctx, hidem_link_soa *out) {
         ctx->launches += 1;
     }
     if (out->initialLen) CK(cudaMemcpyAsync(out->initialLen, ctx->L0link, lp * (size_t)L, cudaMemcpyDeviceToHost, st));
+    if (out->owners) CK(cudaMemcpyAsync(out->owners, ctx->dLinkOwners, 4 * (size_t)L, cudaMemcpyDeviceToHost, st));
+    if (out->globalKeys) CK(cudaMemcpyAsync(out->globalKeys, ctx->dLinkKeys, 8 * (size_t)L, cudaMemcpyDeviceToHost, st));
+    if (out->globalKeyEndA) CK(cudaMemcpyAsync(out->globalKeyEndA, ctx->dLinkKeyA, 8 * (size_t)L, cudaMemcpyDeviceToHost, st));
+    if (out->globalKeyEndB) CK(cudaMemcpyAsync(out->globalKeyEndB, ctx->dLinkKeyB, 8 * (size_t)L, cudaMemcpyDeviceToHost, st));
+    if (out->particleLinkNum) CK(cudaMemcpyAsync(out->particleLinkNum, ctx->dLinkNum, 4 * (size_t)L, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     dfree(stage);
     dfree(lstate);
-    if (out->owners) std::memcpy(out->owners, ctx->linkOwners.data(), 4 * (size_t)L);
-    if (out->globalKeys) std::memcpy(out->globalKeys, ctx->linkKeys.data(), 8 * (size_t)L);
-    if (out->globalKeyEndA) std::memcpy(out->globalKeyEndA, ctx->linkKeyA.data(), 8 * (size_t)L);
-    if (out->globalKeyEndB) std::memcpy(out->globalKeyEndB, ctx->linkKeyB.data(), 8 * (size_t)L);
-    if (out->particleLinkNum) std::memcpy(out->particleLinkNum, ctx->linkNum.data(), 4 * (size_t)L);
     return HIDEM_OK;
 }
 
@@ -1883,7 +1914,7 @@ hidem_status hidem_set_external_force_maps(hidem_ctx *ctx, const hidem_map2d *ma
 
 hidem_status hidem_set_step_kernel(hidem_ctx *ctx, int32_t kernel) {
     if (!ctx) return HIDEM_ERR_ARG;
-    if (kernel < HIDEM_STEP_KERNEL_AUTO || kernel > HIDEM_STEP_KERNEL_THREAD_CAPPED)
+    if (kernel < HIDEM_STEP_KERNEL_AUTO || kernel > HIDEM_STEP_KERNEL_THREAD_ASYNC)
         return fail(ctx, HIDEM_ERR_ARG, "unknown step kernel %d", (int)kernel);
     ctx->stepKernel = kernel;
     return HIDEM_OK;

@@ -9,6 +9,7 @@
 //   timestep     k_step<FUSED>                     (CombinedAccel::iterateCombined + applyForce +
 //                                                   linkUpdate, CombinedAccel.h:122-235)
 //                k_integrate, k_link_break, k_max_diff
+#include <algorithm>
 #include <cstdio>
 
 #include "kernels.h"
@@ -551,6 +552,9 @@ constexpr int kCapBlocks = sizeof(LP) == 4 ? 5 : 3;
 // and the plain variant: 4 CTAs (128 registers) in the mixed build, no cap in fp64
 template <class LP>
 constexpr int kThreadBlocks = sizeof(LP) == 4 ? 4 : 1;
+// and the asynchronous-copy variant (its partner data lives in shared memory)
+template <class LP>
+constexpr int kAsyncBlocks = sizeof(LP) == 4 ? 5 : 3;
 
 template <class LP, bool FUSED, int MINB>
 __global__ void __launch_bounds__(kStepThreads, MINB)
@@ -563,6 +567,190 @@ __global__ void __launch_bounds__(kStepThreads, MINB)
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
+
+// ---- one thread per particle, partner data staged by asynchronous copies ----
+//
+// The same per-particle evaluation as step_thread_particle, but the next items' partner
+// records (and, for link ends, CT0..CT5) travel with cp.async into this thread's own
+// shared-memory slots instead of registers: two items are in flight behind the one being
+// evaluated, and the registers that held the prefetched record are free (more CTAs per
+// SM). Slot layout per CTA, chunk-major so that a warp's 16-byte reads are conflict-free:
+// rec[slot][chunk][thread] (16 B), ct[slot][q][thread] (lp).
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem, int bytes16_4_8) {
+    if (bytes16_4_8 == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+    else if (bytes16_4_8 == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most one group of this thread is still in flight
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <class LP>
+constexpr int kRecChunks = (int)(sizeof(PRec<LP>) / 16);
+template <class LP>
+constexpr size_t async_smem_bytes() {
+    return (size_t)2 * kStepThreads * (sizeof(PRec<LP>) + 6 * sizeof(LP));
+}
+
+template <class LP, bool FUSED>
+__device__ __forceinline__ void step_thread_async(const Consts<LP> &c, const StepArgs<LP> &a,
+                                                  const int i, unsigned char *smem) {
+    constexpr int NC = kRecChunks<LP>;
+    constexpr int HC = kContactChunks<LP>;
+    const int t = threadIdx.x;
+    int4 *srec = reinterpret_cast<int4 *>(smem);                                  // [2][NC][128]
+    LP *sct = reinterpret_cast<LP *>(smem + (size_t)2 * NC * kStepThreads * 16);   // [2][6][128]
+    auto rec_slot = [&](int s, int ch) { return srec + (s * NC + ch) * kStepThreads + t; };
+    auto ct_slot = [&](int s, int q) { return sct + (s * 6 + q) * kStepThreads + t; };
+    auto read_rec = [&](int s, int chunks) {
+        PRec<LP> r;
+        int4 *dst = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+        for (int ch = 0; ch < NC; ++ch)
+            if (ch < chunks) dst[ch] = *rec_slot(s, ch);
+        return r;
+    };
+
+    const bool live = i < a.n;
+    LP dmax[3] = {LP(0), LP(0), LP(0)};
+    if (live) {
+        PRec<LP> me = load_rec(a.in + i);
+        const uint32_t cnt = __ldg(a.counts + i);
+        const uint8_t ty = FUSED ? __ldg(a.type + i) : uint8_t(0);
+        const int nn = (int)(cnt & 0xffffu), ns = (int)(cnt >> 16);
+        LP F[6] = {0, 0, 0, 0, 0, 0};
+        const int32_t *nb = a.nbr + __ldg(a.nOff + (i >> 5)) + (i & 31);
+        const long long sbase = __ldg(a.sOff + (i >> 5)) + (i & 31);
+
+        // contacts: item k's record in slot k & 1; items k + 1 and k + 2 in flight
+        auto issue_contact = [&](int s, int j) {
+            const int4 *src = reinterpret_cast<const int4 *>(a.in + j);
+#pragma unroll
+            for (int ch = 0; ch < HC; ++ch) cp_async(rec_slot(s, ch), src + ch, 16);
+        };
+        int j2 = 0;
+        if (nn > 0) issue_contact(0, __ldg(nb));
+        cp_async_commit();
+        if (nn > 1) issue_contact(1, __ldg(nb + kWarp));
+        cp_async_commit();
+        if (nn > 2) j2 = __ldg(nb + 2 * kWarp);
+        for (int k = 0; k < nn; ++k) {
+            cp_async_wait1();
+            const PRec<LP> cur = read_rec(k & 1, HC);
+            if (k + 2 < nn) {
+                issue_contact(k & 1, j2);
+                if (k + 3 < nn) j2 = __ldg(nb + (k + 3) * kWarp);
+            }
+            cp_async_commit();
+            contact_pair<LP>(c, LP(1), (LP)(me.x - cur.x), (LP)(me.y - cur.y), (LP)(me.z - cur.z),
+                             me.d, me.r, cur.d, cur.r, F);
+        }
+        cp_async_wait0();
+
+        // link ends: record and CT of item k in slot k & 1; state and initial length one
+        // item ahead in registers
+        const bool brk = FUSED && a.breakPending;
+        auto issue_side = [&](int s, long long si, uint32_t pw) {
+            const int4 *src = reinterpret_cast<const int4 *>(a.in + (pw & kSlotMask));
+#pragma unroll
+            for (int ch = 0; ch < NC; ++ch) cp_async(rec_slot(s, ch), src + ch, 16);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) cp_async(ct_slot(s, q), a.ct[q] + si, (int)sizeof(LP));
+        };
+        uint32_t pw0 = 0, pw1 = 0, pw2 = 0;
+        uint8_t stn = 0;
+        LP l0n = LP(0);
+        if (ns > 0) {
+            pw0 = __ldg(a.sPartner + sbase);
+            issue_side(0, sbase, pw0);
+            stn = a.sState[sbase];
+            if (brk) l0n = __ldg(a.sL0 + sbase);
+        }
+        cp_async_commit();
+        if (ns > 1) {
+            pw1 = __ldg(a.sPartner + sbase + kWarp);
+            issue_side(1, sbase + kWarp, pw1);
+        }
+        cp_async_commit();
+        if (ns > 2) pw2 = __ldg(a.sPartner + sbase + 2 * kWarp);
+        for (int k = 0; k < ns; ++k) {
+            const long long si = sbase + (long long)k * kWarp;
+            const uint32_t pw = pw0;
+            uint8_t st = stn;
+            const LP L0 = l0n;
+            cp_async_wait1();
+            const PRec<LP> cur = read_rec(k & 1, NC);
+            LP CT[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) CT[q] = *ct_slot(k & 1, q);
+            pw0 = pw1;
+            pw1 = pw2;
+            if (k + 1 < ns) {
+                stn = a.sState[si + kWarp];
+                if (brk) l0n = __ldg(a.sL0 + si + kWarp);
+            }
+            if (k + 2 < ns) {
+                issue_side(k & 1, si + 2 * kWarp, pw1);
+                if (k + 3 < ns) pw2 = __ldg(a.sPartner + si + 3 * kWarp);
+            }
+            cp_async_commit();
+            if (brk && st != 0) {
+                const uint8_t nst =
+                    (pw & kSideIsB) ? break_link<LP>(a.bendBreak, a.maxLoad, cur, me, st, L0)
+                                    : break_link<LP>(a.bendBreak, a.maxLoad, me, cur, st, L0);
+                if (nst != st) {
+                    a.sState[si] = nst;
+                    if (nst == 0 && !(pw & kSideIsB)) {
+                        unsigned long long slot = atomicAdd(a.eventCount, 1ull);
+                        if ((long long)slot < a.eventCap)
+                            a.events[slot] = make_int2(__ldg(a.sLink + si), (int)a.breakStep);
+                    }
+                    st = nst;
+                }
+            }
+            const LP mask = (st == 0) ? LP(0) : LP(1);
+            beam_side<LP>(c, mask, (LP)(me.x - cur.x), (LP)(me.y - cur.y), (LP)(me.z - cur.z),
+                          me.d, cur.d, CT, F);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) a.ct[q][si] = CT[q];
+        }
+        cp_async_wait0();
+
+        if (FUSED) {
+            integrate_particle<LP>(c, me, ty, F);
+            store_rec(a.out + i, me);
+            dmax[0] = me.d[0] > LP(0) ? me.d[0] : LP(0);
+            dmax[1] = me.d[1] > LP(0) ? me.d[1] : LP(0);
+            dmax[2] = me.d[2] > LP(0) ? me.d[2] : LP(0);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) a.force[(long long)q * a.n + i] = F[q];
+        }
+    }
+    if (FUSED && a.reduceDiff) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            LP v = dmax[q];
+            for (int o = 16; o > 0; o >>= 1) {
+                LP u = __shfl_xor_sync(0xffffffffu, v, o);
+                v = (u > v) ? u : v;
+            }
+            if ((threadIdx.x & 31) == 0 && v > LP(0)) atomicMax(a.diffMax + q, max_bits(v));
+        }
+    }
+}
+
+template <class LP, bool FUSED, int MINB>
+__global__ void __launch_bounds__(kStepThreads, MINB)
+    k_step_async(const Consts<LP> c, const StepArgs<LP> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    step_thread_async<LP, FUSED>(c, a, blockIdx.x * blockDim.x + threadIdx.x, smem);
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -1044,7 +1232,13 @@ void launch_step(const Consts<LP> &c, const StepArgs<LP> &a0, bool fused, int ma
     }
     // one thread per particle (also for rows too wide for the item kernel's buffers)
     const int nb = nblk(a.n, kStepThreads);
-    if (kernel == HIDEM_STEP_KERNEL_THREAD_CAPPED) {
+    if (kernel == HIDEM_STEP_KERNEL_THREAD_ASYNC) {
+        const size_t sm = async_smem_bytes<LP>();
+        if (fused)
+            k_step_async<LP, true, kAsyncBlocks<LP>><<<nb, kStepThreads, sm, s>>>(c, a);
+        else
+            k_step_async<LP, false, kAsyncBlocks<LP>><<<nb, kStepThreads, sm, s>>>(c, a);
+    } else if (kernel == HIDEM_STEP_KERNEL_THREAD_CAPPED) {
         if (fused)
             k_step<LP, true, kCapBlocks<LP>><<<nb, kStepThreads, 0, s>>>(c, a);
         else
@@ -1331,6 +1525,44 @@ __global__ void k_gather_sides(const int *__restrict__ sideSlot, long long L,
     const int src = sideSlot[s];
     if (ct) out[s] = ct[src];
     if (linkState && (s & 1) == 0) linkState[s >> 1] = sState[src];
+}
+
+__global__ void k_link_keys_identity(const long long *__restrict__ ka, const long long *__restrict__ kb,
+                                     long long L, long long n, int *__restrict__ A, int *__restrict__ B,
+                                     unsigned long long *badMin, unsigned long long *selfMin) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long a = ka[i], b = kb[i];
+        if (a < 0 || a >= n || b < 0 || b >= n) {
+            atomicMin(badMin, (unsigned long long)i);
+            A[i] = 0;
+            B[i] = 0;
+            continue;
+        }
+        A[i] = (int)a;
+        B[i] = (int)b;
+        if (a == b) atomicMin(selfMin, (unsigned long long)i);
+    }
+}
+
+__global__ void k_iota64(long long *out, long long count) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = i;
+}
+
+void launch_link_keys_identity(const long long *keyA, const long long *keyB, long long L,
+                               long long n, int *A, int *B, unsigned long long *badMin,
+                               unsigned long long *selfMin, cudaStream_t st) {
+    if (L <= 0) return;
+    const int nb = (int)std::min<long long>((L + 255) / 256, 148LL * 32);
+    k_link_keys_identity<<<nb, 256, 0, st>>>(keyA, keyB, L, n, A, B, badMin, selfMin);
+}
+
+void launch_iota64(long long *out, long long count, cudaStream_t st) {
+    if (count <= 0) return;
+    const int nb = (int)std::min<long long>((count + 255) / 256, 148LL * 32);
+    k_iota64<<<nb, 256, 0, st>>>(out, count);
 }
 
 template <class LP>

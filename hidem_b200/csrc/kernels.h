@@ -62,6 +62,14 @@ void launch_link_lists(const int *A, const int *B, long long L, int n, int *deg,
                        int *cursor, int *sums, int *plLink, uint8_t *plEnd, cudaStream_t st);
 void launch_side_init(const uint8_t *linkState, long long L, int *sideSlot, uint8_t *sideState,
                       cudaStream_t st);
+// link ends from particle keys that are the input indices 0..n-1: A, B; the lowest link
+// index with an end outside [0, n) into *badMin, with A == B into *selfMin (both start at
+// the largest value)
+void launch_link_keys_identity(const long long *keyA, const long long *keyB, long long L,
+                               long long n, int *A, int *B, unsigned long long *badMin,
+                               unsigned long long *selfMin, cudaStream_t st);
+// out[i] = i (int64)
+void launch_iota64(long long *out, long long count, cudaStream_t st);
 template <class LP>
 void launch_gather_sides(const int *sideSlot, long long L, const LP *ct, LP *out,
                          const uint8_t *sState, uint8_t *linkState, cudaStream_t st);

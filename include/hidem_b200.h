@@ -294,13 +294,15 @@ hidem_status hidem_kinetic_energy(hidem_ctx *ctx, double *translational, double 
  * (particle, link end) item with the block's streams staged in shared memory (ITEMS), one
  * thread per particle with software-pipelined partner loads (THREAD), and the same with
  * registers capped for more CTAs per SM (THREAD_CAPPED: five in the mixed build, three in
- * FP64). AUTO (the default) times each on the context's own first fused steps (three
+ * FP64), and one thread per particle whose next two items' partner data travel by
+ * asynchronous copies into shared memory (THREAD_ASYNC). AUTO (the default) times each on the context's own first fused steps (three
  * rounds, the first discarded) and keeps the fastest; those steps are ordinary timesteps.
  * hidem_get_step_kernel returns the kernel in use (AUTO while still timing). */
 #define HIDEM_STEP_KERNEL_AUTO 0
 #define HIDEM_STEP_KERNEL_ITEMS 1
 #define HIDEM_STEP_KERNEL_THREAD 2
 #define HIDEM_STEP_KERNEL_THREAD_CAPPED 3
+#define HIDEM_STEP_KERNEL_THREAD_ASYNC 4
 hidem_status hidem_set_step_kernel(hidem_ctx *ctx, int32_t kernel);
 int32_t hidem_get_step_kernel(const hidem_ctx *ctx);
 

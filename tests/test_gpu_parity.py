@@ -70,7 +70,7 @@ def test_gpu_matches_reference_golden(gpu, name, mode):
 
 @pytest.mark.parametrize("name", ["block6_mixed", "block6_fp64", "slab533_mixed", "slab533_fp64"])
 @pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD,
-                                    abi.STEP_KERNEL_THREAD_CAPPED])
+                                    abi.STEP_KERNEL_THREAD_CAPPED, abi.STEP_KERNEL_THREAD_ASYNC])
 def test_every_step_kernel_matches_golden(gpu, name, kernel):
     """Each step kernel on its own (the autotuner only picks among them by speed)."""
     g = load_golden(name)
@@ -89,9 +89,10 @@ def test_step_kernel_autotuner_settles(gpu):
     lib.set_links(l)
     assert lib.step_kernel() == abi.STEP_KERNEL_AUTO
     lib.step(4)
+    assert lib.step_kernel() == abi.STEP_KERNEL_AUTO  # still timing (4 kernels x 3 rounds)
     lib.step(8)
     assert lib.step_kernel() in (abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD,
-                                 abi.STEP_KERNEL_THREAD_CAPPED)
+                                 abi.STEP_KERNEL_THREAD_CAPPED, abi.STEP_KERNEL_THREAD_ASYNC)
     with pytest.raises(abi.HidemError):
         lib.set_step_kernel(9)
     lib.close()
@@ -326,6 +327,42 @@ def test_errors_are_status_codes(gpu):
     with pytest.raises(abi.HidemError) as e:
         lib.regenerate()
     assert e.value.status == 4
+    lib.close()
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_arbitrary_particle_keys_give_the_same_run(gpu, precision):
+    """Particle globalKeys that are not the input indices (link ends mapped through the
+    key table) give the run of the index-keyed input, and get_links returns the caller's
+    link fields unchanged; dangling and self links are refused on that path too."""
+    P, p, l = workloads.ice_block(cells=(3, 3, 3), precision=precision, seed=5)
+    ref = gpu_run(P, p, l, 15)
+    q = {k: v.copy() for k, v in p.items()}
+    q["globalKeys"][:] = 1000 + 7 * np.arange(q["globalKeys"].shape[0])[::-1]
+    m = {k: v.copy() for k, v in l.items()}
+    m["globalKeyEndA"][:] = q["globalKeys"][l["globalKeyEndA"]]
+    m["globalKeyEndB"][:] = q["globalKeys"][l["globalKeyEndB"]]
+    m["owners"][:] = 3
+    m["globalKeys"][:] = 5 + np.arange(m["globalKeys"].shape[0])
+    got = gpu_run(P, q, m, 15)
+    for k in P_OUT:
+        assert np.array_equal(got[0][k], ref[0][k]), k
+    for k in L_OUT:
+        assert np.array_equal(got[1][k], ref[1][k]), k
+    for k in ("globalKeyEndA", "globalKeyEndB", "owners", "globalKeys"):
+        assert np.array_equal(got[1][k], m[k]), k
+    lib = HiDEMLib(P)
+    lib.set_particles(q)
+    bad = {k: v.copy() for k, v in m.items()}
+    bad["globalKeyEndA"][3] = 999
+    with pytest.raises(abi.HidemError) as e:
+        lib.set_links(bad)
+    assert e.value.status == 7
+    bad = {k: v.copy() for k, v in m.items()}
+    bad["globalKeyEndA"][2] = bad["globalKeyEndB"][2]
+    with pytest.raises(abi.HidemError) as e:
+        lib.set_links(bad)
+    assert e.value.status == 1
     lib.close()
 
 
