@@ -431,6 +431,8 @@ def main_ensemble(args):
                    "precision": args.precision, "parallelism": f"blocks split over {world} ranks",
                    "graphs": not args.no_graphs,
                    "graph_replays": c1["graph_launches"] - c0["graph_launches"],
+                   "entry_uploads": c1["uploads"] - c0["uploads"],
+                   "rebuilds_in_timed_steps": int(sum(b["regen_count"] for b in st1) - sum(a["regen_count"] for a in st0)),
                    "l2": "inputs larger than L2 (records + link ends > 126 MB)",
                    "broken_fraction_rank0": {"min": float(np.min(broken)),
                                              "median": float(np.median(broken)),

@@ -310,9 +310,12 @@ SideView<LP> side_view(SideSet &s) {
     return v;
 }
 
+// grows a side set to at least `cap` link ends, with a quarter of headroom so that the
+// two sets a rebuild alternates between stop reallocating (cudaFree synchronises the device)
 hidem_status side_alloc(hidem_ctx *ctx, SideSet &s, long long cap) {
     if (s.cap >= cap && s.partner) return HIDEM_OK;
     if (cap <= 0) cap = 1;
+    cap += cap / 4;
     TRY(dalloc(ctx, &s.partner, cap));
     for (int k = 0; k < 6; ++k) TRY(dalloc_bytes(ctx, &s.ct[k], ctx->lp * (size_t)cap));
     TRY(dalloc(ctx, &s.state, cap));
