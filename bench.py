@@ -167,6 +167,17 @@ def profile_traffic(precision: str):
     return None
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (for the CPU baseline's record)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(P, p, l, n):
     """The reference's CPU path (oracle/_ref fast build, all host threads) on a bounded
     sample of the same workload: a few timesteps of the whole slab after one warm-up."""
@@ -180,6 +191,7 @@ def cpu_baseline(P, p, l, n):
         secs = sess.advance(k)
         sess.close()
         return {"value": n * k / secs, "unit": "particle-steps/s", "cores": cores, "kind": kind,
+                "cpu": cpu_model(), "host_threads": os.cpu_count(),
                 "sample": f"{k} timesteps of the full workload ({n} particles) after 1 warm-up step, "
                           f"reference CPU path built with -O3 -ffast-math -march=x86-64-v3 -fopenmp"}
     port = oracle.port()
@@ -216,7 +228,7 @@ def run_reference(args):
                    "precision": args.precision},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
-                         "kind": "reference",
+                         "kind": "reference", "cpu": cpu_model(), "host_threads": os.cpu_count(),
                          "sample": f"{args.steps} timesteps of the full workload after {max(args.warmup, 1)} warm-up"},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},

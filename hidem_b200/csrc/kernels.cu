@@ -10,6 +10,7 @@
 //                                                   linkUpdate, CombinedAccel.h:122-235)
 //                k_integrate, k_link_break, k_max_diff
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "kernels.h"
@@ -1215,13 +1216,18 @@ void launch_step(const Consts<LP> &c, const StepArgs<LP> &a0, bool fused, int ma
     a.maxEnds = maxEnds;
     const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds);
     if (kernel == HIDEM_STEP_KERNEL_ITEMS && L.total <= kItemSmemLimit) {
-        static bool configured[2] = {false, false};
-        if (!configured[fused ? 1 : 0]) {
+        // the shared-memory limit is a per-device attribute: set it once on each device
+        // (setting it twice, as racing threads may, is harmless)
+        static std::atomic<unsigned long long> configured[2];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const unsigned long long bit = 1ull << (dev & 63);
+        if (!(configured[fused ? 1 : 0].load() & bit)) {
             if (fused)
                 cudaFuncSetAttribute(k_step_items<LP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kItemSmemLimit);
             else
                 cudaFuncSetAttribute(k_step_items<LP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kItemSmemLimit);
-            configured[fused ? 1 : 0] = true;
+            configured[fused ? 1 : 0].fetch_or(bit);
         }
         const int nb = nblk(a.n, 32);
         if (fused)

@@ -15,6 +15,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
@@ -588,11 +589,15 @@ hidem_status sfail(hidem_surrogate *s, hidem_status st, const char *fmt, ...) {
 template <int BN, int EPI>
 hidem_status gemm(hidem_surrogate *s, const bf16 *A, int M, int K, const bf16 *Bm, int splits,
                   GemmArgs g) {
-    static bool configured = false;
-    if (!configured) {
+    // per-device attribute, set once on each device (a repeated set is harmless)
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured.load() & bit)) {
         cudaFuncSetAttribute(k_umma_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)gemm_smem_bytes<BN>());
-        configured = true;
+        configured.fetch_or(bit);
     }
     if (M % 128 || K % 64 || (K / 64) % splits)
         return sfail(s, HIDEM_ERR_ARG, "GEMM shape %d x %d x %d (splits %d) is not tile-aligned", M, BN, K, splits);
