@@ -53,7 +53,9 @@ def parse():
     ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle", "topo"], default="slab")
     ap.add_argument("--topo", default="1200,200,150",
                     help="topo: slab size in metres on the Fourier-mode bed (the 50M configuration)")
-    ap.add_argument("--train-tongues", type=int, default=64, help="settle: training geometries")
+    ap.add_argument("--train-tongues", type=int, default=256, help="settle: training geometries")
+    ap.add_argument("--surrogate-inputs", choices=["lattice", "coords"], default="lattice",
+                    help="settle: the surrogate's inputs (lattice neighbourhood, or 5 coordinates)")
     ap.add_argument("--test-tongues", type=int, default=16, help="settle: held-out geometries")
     ap.add_argument("--train-steps", type=int, default=20000, help="settle: surrogate Adam steps")
     ap.add_argument("--blocks", type=int, default=256, help="ensemble: number of blocks")
@@ -469,17 +471,21 @@ def main_settle(args):
     torch.cuda.set_device(local)
     size, thick, amp = (40.0, 12.0), 6.0, 2.0
     rep = settle.warm_start_experiment(n_train=args.train_tongues, n_test=args.test_tongues, size=size,
-                                       base_thickness=thick, amplitude=amp, train_steps=args.train_steps)
+                                       base_thickness=thick, amplitude=amp, train_steps=args.train_steps,
+                                       inputs=args.surrogate_inputs)
     # tensor-core forward throughput of the trained network's shape on 2M rows
-    cfg = sg.default_config()
+    lattice = args.surrogate_inputs == "lattice"
+    nin = settle.N_LATTICE_INPUTS if lattice else 5
+    cfg = sg.default_config(inputs=nin, fourier_bands=4 if lattice else 6)
+    k0 = sg.feature_width(nin, cfg.fourier_bands)
     rows = 1 << 21
-    u = np.random.default_rng(0).uniform(-1, 1, (rows, 5)).astype(np.float32)
+    u = np.random.default_rng(0).uniform(-1, 1, (rows, nin)).astype(np.float32)
     with sg.Surrogate(cfg) as net:
         net.predict(u[:16384])
         t0 = time.perf_counter()
         net.predict(u)
         el = time.perf_counter() - t0
-    flops = 2.0 * rows * (128 * cfg.width + (cfg.hidden_layers - 1) * cfg.width * cfg.width + 3 * cfg.width)
+    flops = 2.0 * rows * (k0 * cfg.width + (cfg.hidden_layers - 1) * cfg.width * cfg.width + 3 * cfg.width)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("bf16_tflops", 1590.0))
     d = dataclasses.asdict(rep)
@@ -492,7 +498,8 @@ def main_settle(args):
                                f"bed and surface 8 Fourier modes each (total amplitude {amp:g} m), "
                                f"FCC d = 1 m; {args.train_tongues} training, {args.test_tongues} held out",
                    "particles_per_tongue": d["particles_per_tongue"], "train_samples": d["train_samples"],
-                   "surrogate": "4 x 256 SiLU MLP, Fourier features, BF16 tcgen05 GEMMs",
+                   "surrogate": f"{nin} inputs ({args.surrogate_inputs}), {k0} Fourier features, "
+                                f"4 x 256 SiLU MLP, BF16 tcgen05 GEMMs",
                    "train_steps": args.train_steps},
         "cold_steps": d["cold_steps"], "warm_steps": d["warm_steps"],
         "prediction_rel_error": d["prediction_rel_error"],

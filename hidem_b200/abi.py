@@ -191,7 +191,8 @@ def map2d(values, x_min: float, y_min: float, x_max: float, y_max: float, precis
 
 class HidemSurrogateConfig(C.Structure):
     _fields_ = [("hidden_layers", C.c_int32), ("width", C.c_int32), ("fourier_bands", C.c_int32),
-                ("batch", C.c_int32), ("learning_rate", C.c_double), ("seed", C.c_uint64)]
+                ("batch", C.c_int32), ("learning_rate", C.c_double), ("seed", C.c_uint64),
+                ("inputs", C.c_int32), ("cosine_decay", C.c_int32)]
 
 
 # (name, restype, argtypes)

@@ -9,12 +9,14 @@
 // and Adam run on the CUDA cores.
 //
 // Network: features(u) -> [Linear(K_l -> W) + SiLU] x L -> Linear(W -> 3), with
-// u = 5 normalised inputs (x, y, z, local thickness, bed height) and Fourier features
-// u_i, sin(2^f pi u_i), cos(2^f pi u_i) for f < F, zero-padded to 128 inputs.
+// u = the row's normalised inputs (the caller's: coordinates, local geometry, lattice
+// neighbourhood) and Fourier features u_i, sin(2^f pi u_i), cos(2^f pi u_i) for f < F,
+// zero-padded to K_0, a multiple of 128.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -316,32 +318,39 @@ namespace {
 
 // ------------------------------------------------------------------ CUDA-core kernels
 
-constexpr int kIn = 5;      // normalised inputs per particle
-constexpr int kFeat = 128;  // padded feature width (first layer's K)
-constexpr int kOut = 3;     // displacement components
+constexpr int kMaxIn = 128;  // normalised inputs per row, at most
+constexpr int kOut = 3;      // displacement components
 
-// Fourier features of the rows idx[b] (or b when idx is null) of `in` [n][5]:
-// u_i, then sin(2^f pi u_i), cos(2^f pi u_i) for f < bands, zero padding to 128.
+// first layer's input width: inputs * (1 + 2 bands) rounded up to a multiple of 128
+int feature_width(int nin, int bands) {
+    const int f = nin * (1 + 2 * bands);
+    return std::max(128, (f + 127) / 128 * 128);
+}
+
+// Fourier features of the rows idx[b] (or b when idx is null) of `in` [n][nin]:
+// u_i, then sin(2^f pi u_i), cos(2^f pi u_i) for f < bands (f-major), zero padding to K0.
+// One warp per row; the row's inputs are staged in shared memory.
 __global__ void k_features(const float *__restrict__ in, const int *__restrict__ idx, int rows,
-                           int bands, bf16 *__restrict__ X) {
+                           int nin, int bands, int K0, bf16 *__restrict__ X) {
+    __shared__ float su[8][kMaxIn];
     const int b = blockIdx.x * blockDim.y + threadIdx.y;
     if (b >= rows) return;
     const int src = idx ? idx[b] : b;
-    float u[kIn];
-#pragma unroll
-    for (int i = 0; i < kIn; ++i) u[i] = in ? in[(long long)src * kIn + i] : 0.f;
-    for (int c = threadIdx.x; c < kFeat; c += blockDim.x) {
+    float *u = su[threadIdx.y];
+    for (int i = threadIdx.x; i < nin; i += blockDim.x) u[i] = in[(long long)src * nin + i];
+    __syncwarp();
+    for (int c = threadIdx.x; c < K0; c += blockDim.x) {
         float v = 0.f;
-        if (c < kIn) {
+        if (c < nin) {
             v = u[c];
         } else {
-            const int q = c - kIn, f = q / (2 * kIn), r = q % (2 * kIn), i = r >> 1;
+            const int q = c - nin, f = q / (2 * nin), r = q % (2 * nin), i = r >> 1;
             if (f < bands) {
                 const float a = (float)(1 << f) * 3.14159265358979f * u[i];
                 v = (r & 1) ? cosf(a) : sinf(a);
             }
         }
-        X[(long long)b * kFeat + c] = __float2bfloat16_rn(v);
+        X[(long long)b * K0 + c] = __float2bfloat16_rn(v);
     }
 }
 
@@ -509,13 +518,14 @@ struct hidem_surrogate {
     std::string err;
     int *dErr = nullptr;
     int L = 4, W = 256, B = 16384, splits = 64;
+    int nin = 5, K0 = 128;                       // inputs per row, first layer's K
     long long np = 0;                            // parameter count
     std::vector<long long> offW, offB;           // hidden layer weight / bias offsets in P
     long long offWo = 0, offBo = 0;
     std::vector<int> Kl;                         // input width of hidden layer l
     float *P = nullptr, *G = nullptr, *Mm = nullptr, *Vv = nullptr;
     std::vector<bf16 *> Wb, WbT;                 // BF16 weights [W][K_l] and [K_l][W]
-    bf16 *X0 = nullptr;                          // [B][128]
+    bf16 *X0 = nullptr;                          // [B][K0]
     std::vector<float *> Z;                      // [B][W] pre-activations
     std::vector<bf16 *> H;                       // [B][W] activations
     float *Y = nullptr, *dY = nullptr;           // [B][3]
@@ -525,7 +535,7 @@ struct hidem_surrogate {
     long long partCap = 0;
     float *lossPart = nullptr, *lossHost = nullptr;
     int *idx = nullptr;
-    float *dataIn = nullptr, *dataT = nullptr;   // training set [n][5], [n][3]
+    float *dataIn = nullptr, *dataT = nullptr;   // training set [n][nin], [n][3]
     long long nData = 0;
     float *scratchIn = nullptr, *scratchT = nullptr;  // caller rows for predict / gradients
     long long steps = 0;
@@ -688,11 +698,16 @@ hidem_status backward(hidem_surrogate *s, int rows, const float *targets, const 
         int splits = s->splits;
         while (splits > 1 && ((rows / 64) % splits)) splits >>= 1;
         STRY(ensure_part(s, (long long)splits * W * K));
-        GemmArgs g{};
-        g.outF = s->part;
-        g.splitStride = (long long)W * K;
-        g.ldo = K;
-        STRY(gemm_n<EPI_F32>(s, K, s->dZT, W, rows, s->inT, splits, g));
+        // columns of dW in tiles of 256 (then 128): rows n0.. of the K-major input
+        for (int n0 = 0; n0 < K;) {
+            const int bn = K - n0 >= 256 ? 256 : 128;
+            GemmArgs g{};
+            g.outF = s->part + n0;
+            g.splitStride = (long long)W * K;
+            g.ldo = K;
+            STRY(gemm_n<EPI_F32>(s, bn, s->dZT, W, rows, s->inT + (long long)n0 * rows, splits, g));
+            n0 += bn;
+        }
         k_sum_splits<<<(unsigned)(((long long)W * K + 255) / 256), 256, 0, s->stream>>>(s->part, splits, (long long)W * K, s->G + s->offW[l]);
         // db_l = column sums of dZ
         STRY(ensure_part(s, (long long)chunks * W + W));
@@ -747,6 +762,8 @@ void hidem_surrogate_config_default(hidem_surrogate_config *c) {
     c->batch = 16384;
     c->learning_rate = 1e-3;
     c->seed = 1;
+    c->inputs = 5;
+    c->cosine_decay = 0;
 }
 
 void hidem_surrogate_destroy(hidem_surrogate *s) {
@@ -776,8 +793,10 @@ hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device,
     *out = nullptr;
     if (c->hidden_layers < 1 || c->hidden_layers > 16 || (c->width != 128 && c->width != 256) ||
         c->fourier_bands < 1 || c->fourier_bands > 12 || c->batch < 128 || c->batch % 128 ||
-        c->batch > (1 << 20) || !(c->learning_rate > 0)) {
-        err = "surrogate config out of range (layers 1..16, width 128 | 256, bands 1..12, batch a multiple of 128)";
+        c->batch > (1 << 20) || !(c->learning_rate > 0) || c->inputs < 1 || c->inputs > kMaxIn ||
+        (c->cosine_decay != 0 && c->cosine_decay != 1)) {
+        err = "surrogate config out of range (layers 1..16, width 128 | 256, bands 1..12, batch a "
+              "multiple of 128, inputs 1..128, cosine_decay 0 | 1)";
         return HIDEM_ERR_ARG;
     }
     if (!encode_fn()) {
@@ -790,10 +809,12 @@ hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device,
     s->L = c->hidden_layers;
     s->W = c->width;
     s->B = c->batch;
-    const int L = s->L, W = s->W, B = s->B;
+    s->nin = c->inputs;
+    s->K0 = feature_width(c->inputs, c->fourier_bands);
+    const int L = s->L, W = s->W, B = s->B, K0 = s->K0;
     long long off = 0;
     for (int l = 0; l < L; ++l) {
-        const int K = l == 0 ? kFeat : W;
+        const int K = l == 0 ? K0 : W;
         s->Kl.push_back(K);
         s->offW.push_back(off);
         off += (long long)W * K;
@@ -807,7 +828,7 @@ hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device,
     s->np = off;
     const int chunks = (B + kChunk - 1) / kChunk;
     long long partNeed = std::max<long long>((long long)(chunks + 1) * kOut * (W + 1), (long long)chunks * W + W);
-    partNeed = std::max<long long>(partNeed, (long long)s->splits * W * std::max(W, kFeat));
+    partNeed = std::max<long long>(partNeed, (long long)s->splits * W * std::max(W, K0));
     auto fail = [&](cudaError_t e) {
         err = std::string("surrogate setup failed: ") + cudaGetErrorString(e);
         hidem_surrogate_destroy(s);
@@ -833,18 +854,18 @@ hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device,
         dm((void **)&s->Z[l], sizeof(float) * (size_t)B * W);
         dm((void **)&s->H[l], sizeof(bf16) * (size_t)B * W);
     }
-    dm((void **)&s->X0, sizeof(bf16) * (size_t)B * kFeat);
+    dm((void **)&s->X0, sizeof(bf16) * (size_t)B * K0);
     dm((void **)&s->Y, sizeof(float) * (size_t)B * kOut);
     dm((void **)&s->dY, sizeof(float) * (size_t)B * kOut);
     dm((void **)&s->dZa, sizeof(bf16) * (size_t)B * W);
     dm((void **)&s->dZb, sizeof(bf16) * (size_t)B * W);
     dm((void **)&s->dZT, sizeof(bf16) * (size_t)B * W);
-    dm((void **)&s->inT, sizeof(bf16) * (size_t)B * std::max(W, kFeat));
+    dm((void **)&s->inT, sizeof(bf16) * (size_t)B * std::max(W, K0));
     dm((void **)&s->part, sizeof(float) * partNeed);
     s->partCap = partNeed;
     dm((void **)&s->lossPart, sizeof(float) * ((B + 255) / 256));
     dm((void **)&s->idx, sizeof(int) * B);
-    dm((void **)&s->scratchIn, sizeof(float) * (size_t)B * kIn);
+    dm((void **)&s->scratchIn, sizeof(float) * (size_t)B * s->nin);
     dm((void **)&s->scratchT, sizeof(float) * (size_t)B * kOut);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&s->lossHost, sizeof(float) * ((B + 255) / 256));
     if (e == cudaSuccess) e = cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream);
@@ -909,9 +930,9 @@ hidem_status hidem_surrogate_set_data(hidem_surrogate *s, const float *inputs, c
     if (s->dataT) cudaFree(s->dataT);
     s->dataIn = s->dataT = nullptr;
     s->nData = 0;
-    SCK(cudaMalloc((void **)&s->dataIn, sizeof(float) * kIn * (size_t)n));
+    SCK(cudaMalloc((void **)&s->dataIn, sizeof(float) * s->nin * (size_t)n));
     SCK(cudaMalloc((void **)&s->dataT, sizeof(float) * kOut * (size_t)n));
-    SCK(cudaMemcpyAsync(s->dataIn, inputs, sizeof(float) * kIn * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    SCK(cudaMemcpyAsync(s->dataIn, inputs, sizeof(float) * s->nin * (size_t)n, cudaMemcpyHostToDevice, s->stream));
     SCK(cudaMemcpyAsync(s->dataT, targets, sizeof(float) * kOut * (size_t)n, cudaMemcpyHostToDevice, s->stream));
     SCK(cudaStreamSynchronize(s->stream));
     s->nData = n;
@@ -926,14 +947,16 @@ hidem_status hidem_surrogate_train(hidem_surrogate *s, int32_t steps, double *lo
     const int B = s->B;
     for (int it = 0; it < steps; ++it) {
         k_sample<<<(B + 255) / 256, 256, 0, s->stream>>>(s->cfg.seed, (unsigned long long)s->steps, B, s->nData, s->idx);
-        k_features<<<(B + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->dataIn, s->idx, B, s->cfg.fourier_bands, s->X0);
+        k_features<<<(B + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->dataIn, s->idx, B, s->nin, s->cfg.fourier_bands, s->K0, s->X0);
         STRY(forward(s, B, true));
         STRY(backward(s, B, s->dataT, s->idx));
         s->steps += 1;
         const float b1 = 0.9f, b2 = 0.999f;
         const float c1 = 1.f - std::pow(b1, (float)s->steps), c2 = 1.f - std::pow(b2, (float)s->steps);
+        double lr = s->cfg.learning_rate;
+        if (s->cfg.cosine_decay) lr *= 0.5 * (1.0 + std::cos(3.14159265358979 * it / (double)steps));
         k_adam<<<(unsigned)((s->np + 255) / 256), 256, 0, s->stream>>>(s->P, s->G, s->Mm, s->Vv, s->np,
-                                                                      (float)s->cfg.learning_rate, b1, b2, 1e-8f, c1, c2);
+                                                                      (float)lr, b1, b2, 1e-8f, c1, c2);
         STRY(refresh_bf16(s));
     }
     if (steps > 0 && loss) STRY(read_loss(s, B, loss));
@@ -948,9 +971,9 @@ hidem_status hidem_surrogate_predict(hidem_surrogate *s, const float *inputs, in
     for (int64_t r0 = 0; r0 < n; r0 += B) {
         const int rows = (int)std::min<int64_t>(B, n - r0);
         const int padded = (rows + 127) / 128 * 128;
-        if (padded > rows) SCK(cudaMemsetAsync(s->scratchIn, 0, sizeof(float) * kIn * padded, s->stream));
-        SCK(cudaMemcpyAsync(s->scratchIn, inputs + r0 * kIn, sizeof(float) * kIn * rows, cudaMemcpyHostToDevice, s->stream));
-        k_features<<<(padded + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->scratchIn, nullptr, padded, s->cfg.fourier_bands, s->X0);
+        if (padded > rows) SCK(cudaMemsetAsync(s->scratchIn, 0, sizeof(float) * s->nin * padded, s->stream));
+        SCK(cudaMemcpyAsync(s->scratchIn, inputs + r0 * s->nin, sizeof(float) * s->nin * rows, cudaMemcpyHostToDevice, s->stream));
+        k_features<<<(padded + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->scratchIn, nullptr, padded, s->nin, s->cfg.fourier_bands, s->K0, s->X0);
         STRY(forward(s, padded, false));
         SCK(cudaMemcpyAsync(out + r0 * kOut, s->Y, sizeof(float) * kOut * rows, cudaMemcpyDeviceToHost, s->stream));
     }
@@ -965,9 +988,9 @@ hidem_status hidem_surrogate_gradients(hidem_surrogate *s, const float *inputs, 
         return sfail(s, HIDEM_ERR_ARG, "n must be a positive multiple of 128 up to the batch size");
     SCK(cudaSetDevice(s->device));
     const int rows = (int)n;
-    SCK(cudaMemcpyAsync(s->scratchIn, inputs, sizeof(float) * kIn * rows, cudaMemcpyHostToDevice, s->stream));
+    SCK(cudaMemcpyAsync(s->scratchIn, inputs, sizeof(float) * s->nin * rows, cudaMemcpyHostToDevice, s->stream));
     SCK(cudaMemcpyAsync(s->scratchT, targets, sizeof(float) * kOut * rows, cudaMemcpyHostToDevice, s->stream));
-    k_features<<<(rows + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->scratchIn, nullptr, rows, s->cfg.fourier_bands, s->X0);
+    k_features<<<(rows + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->scratchIn, nullptr, rows, s->nin, s->cfg.fourier_bands, s->K0, s->X0);
     STRY(forward(s, rows, true));
     STRY(backward(s, rows, s->scratchT, nullptr));
     STRY(read_loss(s, rows, loss));

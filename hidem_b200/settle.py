@@ -42,6 +42,19 @@ class Tongue:
     bed: np.ndarray        # bed height under each particle
     thick: np.ndarray      # ice thickness under each particle
     seed: int
+    bed_modes: tuple = ()   # the heightfields as Fourier modes (amplitude, kx, ky, phase)
+    surf_modes: tuple = ()
+    base_thickness: float = 0.0
+
+    def bed_at(self, x, y):
+        return _field(np.asarray(x, np.float64), np.asarray(y, np.float64), self.size, self.bed_modes)
+
+    def thickness_at(self, x, y):
+        """ice thickness of the heightfields at (x, y); 0 outside the tongue's plan"""
+        x, y = np.asarray(x, np.float64), np.asarray(y, np.float64)
+        th = np.maximum(3.0, self.base_thickness + 0.5 * _field(x, y, self.size, self.surf_modes))
+        inside = (x >= 0) & (x <= self.size[0]) & (y >= 0) & (y <= self.size[1])
+        return np.where(inside, th, 0.0)
 
 
 def _modes(rng, count: int, total_amp: float):
@@ -87,7 +100,7 @@ def glacier_tongue(seed: int, size=(200.0, 60.0), base_thickness: float = 12.0,
     links = workloads.distance_links(p, precision, 1.01)
     wl = 0.5 * base_thickness if water_level is None else water_level
     params = workloads.block_params(precision, useFixed=1, waterLevel=wl, breakTime=1e30)
-    return Tongue(params, p, links, size, bed, thick, seed)
+    return Tongue(params, p, links, size, bed, thick, seed, bed_m, surf_m, base_thickness)
 
 
 def surrogate_inputs(t: Tongue) -> np.ndarray:
@@ -99,6 +112,91 @@ def surrogate_inputs(t: Tongue) -> np.ndarray:
     return np.stack([2 * p["xCord"] / t.size[0] - 1, 2 * p["yCord"] / t.size[1] - 1,
                      2 * zrel - 1, t.thick / THICK_SCALE - 1, t.bed / BED_SCALE],
                     axis=1).astype(np.float32)
+
+
+# geometry sampled around each particle: thickness and bed at x +- d, y +- d
+LATTICE_OFFSETS = (1.5, 3.0, 6.0)
+# surrounding lattice columns (column spacing: half the FCC cell), rings 1 and 2
+LATTICE_COLUMNS = tuple((i, j) for i in range(-2, 3) for j in range(-2, 3) if (i, j) != (0, 0))
+N_LATTICE_INPUTS = 5 + 8 * len(LATTICE_OFFSETS) + 5 + 2 * len(LATTICE_COLUMNS)
+
+
+def lattice_inputs(t: Tongue, mirror: tuple[int, int] = (1, 1)) -> np.ndarray:
+    """The surrogate's lattice-neighbourhood inputs of every particle (N_LATTICE_INPUTS
+    columns), optionally of the tongue's mirror image (x -> Lx - x for mirror[0] = -1,
+    y -> Ly - y for mirror[1] = -1, the particles keeping their order):
+
+    * the 5 coordinate inputs of surrogate_inputs;
+    * ice thickness (0 outside the plan) and bed height at x +- d and y +- d for each d of
+      LATTICE_OFFSETS (d-major, then the axis, then +d before -d);
+    * the particle's lattice column (particles sharing x and y): its bond count, the
+      particles above it, the free particles below it, and its height below the column's
+      top and above the column's lowest free particle;
+    * for each surrounding column of LATTICE_COLUMNS: the height of that column's top and
+      of its lowest free particle relative to the particle (-2 where there is no column).
+
+    The settled displacement of these coarse lattices depends on the discrete layering
+    of the ice around a particle, which the smooth heightfields alone do not describe."""
+    p = t.particles
+    n = p["xCord"].shape[0]
+    sx, sy = mirror
+    x = p["xCord"] if sx > 0 else t.size[0] - p["xCord"]
+    y = p["yCord"] if sy > 0 else t.size[1] - p["yCord"]
+    z = p["zCord"]
+
+    def geo(xx, yy):  # heightfields at mirror-frame points
+        ox = xx if sx > 0 else t.size[0] - xx
+        oy = yy if sy > 0 else t.size[1] - yy
+        return t.thickness_at(ox, oy), t.bed_at(ox, oy)
+
+    cols = [2 * x / t.size[0] - 1, 2 * y / t.size[1] - 1, 2 * (z - t.bed) / t.thick - 1,
+            t.thick / THICK_SCALE - 1, t.bed / BED_SCALE]
+    for d in LATTICE_OFFSETS:
+        for ax in (0, 1):
+            for sgn in (1, -1):
+                th, bd = geo(x + sgn * d, y) if ax == 0 else geo(x, y + sgn * d)
+                cols += [th / THICK_SCALE - 1, bd / BED_SCALE]
+    # bonds per particle
+    keys = np.asarray(p["globalKeys"])
+    korder = np.argsort(keys, kind="stable")
+    ends = [korder[np.searchsorted(keys, np.asarray(t.links[k]), sorter=korder)]
+            for k in ("globalKeyEndA", "globalKeyEndB")]
+    deg = np.bincount(ends[0], minlength=n) + np.bincount(ends[1], minlength=n)
+    # lattice columns
+    h = workloads.SQRT2 / 2
+    ci = np.rint(x / h).astype(np.int64) + 16
+    cj = np.rint(y / h).astype(np.int64) + 16
+    key = ci * 4096 + cj
+    free = (p["type"] & abi.TYPE_FIXED) == 0
+    order = np.lexsort((z, key))
+    ks, zs, fs = key[order], z[order], free[order].astype(np.int64)
+    start = np.r_[0, np.flatnonzero(np.diff(ks)) + 1]
+    size = np.diff(np.r_[start, n])
+    g = np.repeat(np.arange(start.shape[0]), size)
+    rank = np.arange(n) - start[g]
+    above, below, gid = np.empty(n), np.empty(n), np.empty(n, np.int64)
+    above[order] = size[g] - 1 - rank
+    cum = np.cumsum(fs) - fs
+    below[order] = cum - cum[start[g]]
+    gid[order] = g
+    top = zs[start + size - 1]
+    zf = np.where(fs > 0, zs, np.inf)
+    low_free = np.minimum.reduceat(zf, start)
+    has_free = np.isfinite(low_free)
+    lowest = np.where(has_free, low_free, zs[start])
+    cols += [deg / 6.0 - 1, above / 5.0 - 1, below / 5.0 - 1, (top[gid] - z) / 5.0 - 1,
+             (z - lowest[gid]) / 5.0 - 1]
+    ukeys = ks[start]
+    low_or_top = np.where(has_free, low_free, top)
+    for di, dj in LATTICE_COLUMNS:
+        nk = key + di * 4096 + dj
+        q = np.minimum(np.searchsorted(ukeys, nk), ukeys.shape[0] - 1)
+        ex = ukeys[q] == nk
+        cols.append(np.where(ex, (top[q] - z) / 5.0, -2.0))
+        cols.append(np.where(ex, (low_or_top[q] - z) / 5.0, -2.0))
+    out = np.stack(cols, axis=1).astype(np.float32)
+    assert out.shape[1] == N_LATTICE_INPUTS
+    return out
 
 
 def rotation_from_displacement(t: Tongue, disp: np.ndarray) -> np.ndarray:
@@ -276,14 +374,16 @@ class WarmStartReport:
     seconds: dict
 
 
-def warm_start_experiment(n_train: int = 64, n_test: int = 16, size=(40.0, 12.0),
+def warm_start_experiment(n_train: int = 256, n_test: int = 16, size=(40.0, 12.0),
                           base_thickness: float = 6.0, amplitude: float = 2.0,
                           train_steps: int = 20000, batch: int = 8192, seed: int = 1000,
                           tol: float = 1e-6, max_steps: int = 40000, surrogate_cfg: dict | None = None,
-                          with_rotation: bool = True, mirror: bool = True):
+                          with_rotation: bool = True, mirror: bool = True, inputs: str = "lattice"):
     """Cold settles of the training tongues, surrogate training on their settled
     displacements, then cold and warm settles of held-out tongues, compared by the plain
-    method's convergence test."""
+    method's convergence test. inputs: "lattice" (lattice_inputs, 4 Fourier bands, the
+    learning rate decayed along a half cosine) or "coords" (the 5 coordinate inputs of
+    surrogate_inputs, 6 bands, constant rate)."""
     import time
     from . import surrogate as sg
     sec = {}
@@ -294,23 +394,30 @@ def warm_start_experiment(n_train: int = 64, n_test: int = 16, size=(40.0, 12.0)
     t0 = time.time()
     cold_train = settle_many(train, tol=tol, max_steps=max_steps)
     sec["cold_train_settles"] = time.time() - t0
-    xs = np.concatenate([surrogate_inputs(t) for t in train])
-    ys = np.concatenate([displacement_of(t, r.final) for t, r in zip(train, cold_train)]) / DISP_SCALE
-    if mirror:
-        # the settling problem is symmetric under x -> Lx - x and y -> Ly - y (vertical
-        # gravity and buoyancy, a fixed base): each mirror image is a valid sample, with
-        # the mirrored displacement component negated
-        xa, ya = [xs], [ys]
-        for sx, sy in ((-1, 1), (1, -1), (-1, -1)):
-            xa.append(xs * np.array([sx, sy, 1, 1, 1], np.float32))
-            ya.append(ys * np.array([sx, sy, 1]))
-        xs, ys = np.concatenate(xa), np.concatenate(ya)
+    if inputs not in ("lattice", "coords"):
+        raise ValueError(f"inputs {inputs!r}: 'lattice' or 'coords'")
+
+    def feats(t, m=(1, 1)):
+        if inputs == "lattice":
+            return lattice_inputs(t, m)
+        return surrogate_inputs(t) * np.array([m[0], m[1], 1, 1, 1], np.float32)
+
     t0 = time.time()
-    cfg = sg.default_config(batch=batch, **({"fourier_bands": 6} | (surrogate_cfg or {})))
+    ys = np.concatenate([displacement_of(t, r.final) for t, r in zip(train, cold_train)]) / DISP_SCALE
+    # the settling problem is symmetric under x -> Lx - x and y -> Ly - y (vertical
+    # gravity and buoyancy, a fixed base): each mirror image is a valid sample, with the
+    # mirrored displacement component negated
+    mirrors = ((1, 1), (-1, 1), (1, -1), (-1, -1)) if mirror else ((1, 1),)
+    xs = np.concatenate([feats(t, m) for m in mirrors for t in train])
+    ys = np.concatenate([ys * np.array([m[0], m[1], 1]) for m in mirrors])
+    sec["features"] = time.time() - t0
+    t0 = time.time()
+    base = {"fourier_bands": 4, "cosine_decay": 1} if inputs == "lattice" else {"fourier_bands": 6}
+    cfg = sg.default_config(batch=batch, inputs=xs.shape[1], **(base | (surrogate_cfg or {})))
     with sg.Surrogate(cfg) as net:
         net.set_data(xs, ys.astype(np.float32))
         loss = net.train(train_steps)
-        preds = [net.predict(surrogate_inputs(t)).astype(np.float64) * DISP_SCALE for t in test]
+        preds = [net.predict(feats(t)).astype(np.float64) * DISP_SCALE for t in test]
     sec["training"] = time.time() - t0
     t0 = time.time()
     cold = settle_many(test, tol=tol, max_steps=max_steps)

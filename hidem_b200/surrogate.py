@@ -1,7 +1,9 @@
 """Learned warm start: the settling surrogate (``hidem_surrogate_*``).
 
-A coordinate MLP maps 5 normalised inputs per particle — x, y, z, local ice thickness and
-bed height under the particle — to its settled displacement (3 components, normalised).
+A coordinate MLP maps normalised inputs per particle (by default 5: x, y, z, local ice
+thickness and bed height under the particle; ``config.inputs`` of them in general, e.g.
+the lattice-neighbourhood inputs of ``hidem_b200.settle.lattice_inputs``) to its settled
+displacement (3 components, normalised).
 Training and inference run in the library's own kernels: BF16 tensor-core GEMMs for the
 hidden layers, CUDA-core kernels for the output layer, loss, reductions and Adam. No
 counterpart in the reference, which settles every geometry from rest; the plain settling
@@ -15,9 +17,14 @@ import numpy as np
 
 from . import abi
 
-N_IN = 5
+N_IN = 5      # default inputs per row
 N_OUT = 3
-N_FEAT = 128
+N_FEAT = 128  # first-layer width of the default inputs
+
+
+def feature_width(nin: int, bands: int) -> int:
+    """First layer's input width: nin * (1 + 2 bands) rounded up to a multiple of 128."""
+    return max(128, -(-nin * (1 + 2 * bands) // 128) * 128)
 
 
 def default_config(**over) -> abi.HidemSurrogateConfig:
@@ -32,7 +39,7 @@ def default_config(**over) -> abi.HidemSurrogateConfig:
 def param_shapes(cfg: abi.HidemSurrogateConfig) -> list[tuple[str, tuple[int, ...]]]:
     """Names and shapes of the parameters in the library's flat order."""
     out = []
-    k = N_FEAT
+    k = feature_width(cfg.inputs, cfg.fourier_bands)
     for l in range(cfg.hidden_layers):
         out.append((f"W{l}", (cfg.width, k)))
         out.append((f"b{l}", (cfg.width,)))
@@ -87,7 +94,7 @@ class Surrogate:
         self._check(self._lib.hidem_surrogate_set_params(self._s, flat.ctypes.data))
 
     def set_data(self, inputs, targets) -> None:
-        x, t = self._f32(inputs, N_IN), self._f32(targets, N_OUT)
+        x, t = self._f32(inputs, self.cfg.inputs), self._f32(targets, N_OUT)
         self._check(self._lib.hidem_surrogate_set_data(self._s, x.ctypes.data, t.ctypes.data, x.shape[0]))
 
     def train(self, steps: int) -> float:
@@ -96,13 +103,13 @@ class Surrogate:
         return loss.value
 
     def predict(self, inputs) -> np.ndarray:
-        x = self._f32(inputs, N_IN)
+        x = self._f32(inputs, self.cfg.inputs)
         out = np.empty((x.shape[0], N_OUT), np.float32)
         self._check(self._lib.hidem_surrogate_predict(self._s, x.ctypes.data, x.shape[0], out.ctypes.data))
         return out
 
     def gradients(self, inputs, targets) -> tuple[np.ndarray, float]:
-        x, t = self._f32(inputs, N_IN), self._f32(targets, N_OUT)
+        x, t = self._f32(inputs, self.cfg.inputs), self._f32(targets, N_OUT)
         g = np.empty(self.num_params, np.float32)
         loss = C.c_double()
         self._check(self._lib.hidem_surrogate_gradients(self._s, x.ctypes.data, t.ctypes.data, x.shape[0],
@@ -136,9 +143,11 @@ def _main(argv=None) -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--rows", type=int, default=1 << 20)
     ap.add_argument("--repeat", type=int, default=3)
+    ap.add_argument("--inputs", type=int, default=N_IN)
+    ap.add_argument("--bands", type=int, default=8)
     a = ap.parse_args(argv)
-    cfg = default_config()
-    u = np.random.default_rng(0).uniform(-1, 1, (a.rows, N_IN)).astype(np.float32)
+    cfg = default_config(inputs=a.inputs, fourier_bands=a.bands)
+    u = np.random.default_rng(0).uniform(-1, 1, (a.rows, a.inputs)).astype(np.float32)
     with Surrogate(cfg) as net:
         net.predict(u[: min(a.rows, 16384)])
         best = float("inf")
@@ -146,7 +155,8 @@ def _main(argv=None) -> None:
             t0 = time.perf_counter()
             net.predict(u)
             best = min(best, time.perf_counter() - t0)
-    flops = 2.0 * a.rows * (N_FEAT * cfg.width + (cfg.hidden_layers - 1) * cfg.width ** 2 + N_OUT * cfg.width)
+    k0 = feature_width(cfg.inputs, cfg.fourier_bands)
+    flops = 2.0 * a.rows * (k0 * cfg.width + (cfg.hidden_layers - 1) * cfg.width ** 2 + N_OUT * cfg.width)
     print(json.dumps({"rows": a.rows, "seconds": best, "tflops": flops / best / 1e12}))
 
 

@@ -341,17 +341,18 @@ hidem_status hidem_batch_counts(const hidem_batch *b, int64_t *launches, int64_t
 /* ---- learned warm start (settling surrogate) -------------------------- */
 
 /* No counterpart in the reference, which settles every geometry from rest. A coordinate
- * MLP predicts the gravity/buoyancy-settled displacement of each particle from 5
- * normalised inputs (x, y, z, local ice thickness, bed height under the particle):
- * Fourier features (u_i, sin(2^f pi u_i), cos(2^f pi u_i), f < fourier_bands, zero-padded
- * to 128), hidden_layers x [Linear(width) + SiLU], Linear(3). Hidden layers are BF16
- * tensor-core GEMMs (tcgen05, FP32 accumulation) written for this library; training is
- * MSE with Adam on FP32 master weights, `batch` rows per step drawn uniformly from the
- * training set. Parameters, flat, in this order: for each hidden layer l the weight
- * [width][K_l] (K_0 = 128, else width) then the bias [width]; the output weight
- * [3][width], the output bias [3]. Inputs are [n][5] and targets / outputs [n][3] FP32
- * host arrays, row-major. On failure of hidem_surrogate_create the text is in
- * hidem_create_error(). */
+ * MLP predicts the gravity/buoyancy-settled displacement of each particle from
+ * `inputs` normalised inputs per particle (the caller's choice: coordinates, the
+ * geometry around the particle, its lattice neighbourhood): Fourier features (u_i for
+ * all i, then sin(2^f pi u_i), cos(2^f pi u_i) for f < fourier_bands, f-major, zero-padded
+ * to K_0 = the next multiple of 128 of inputs * (1 + 2 fourier_bands), at least 128),
+ * hidden_layers x [Linear(width) + SiLU], Linear(3). Hidden layers are BF16 tensor-core
+ * GEMMs (tcgen05, FP32 accumulation) written for this library; training is MSE with Adam
+ * on FP32 master weights, `batch` rows per step drawn uniformly from the training set.
+ * Parameters, flat, in this order: for each hidden layer l the weight [width][K_l]
+ * (K_l = width for l > 0) then the bias [width]; the output weight [3][width], the output
+ * bias [3]. Inputs are [n][inputs] and targets / outputs [n][3] FP32 host arrays,
+ * row-major. On failure of hidem_surrogate_create the text is in hidem_create_error(). */
 typedef struct hidem_surrogate hidem_surrogate;
 typedef struct hidem_surrogate_config {
     int32_t hidden_layers;   /* 4 */
@@ -360,6 +361,9 @@ typedef struct hidem_surrogate_config {
     int32_t batch;           /* rows per training step, a multiple of 128 (16384) */
     double learning_rate;    /* Adam step size (1e-3) */
     uint64_t seed;           /* weight initialisation and batch sampling */
+    int32_t inputs;          /* normalised inputs per row, 1..128 (5) */
+    int32_t cosine_decay;    /* 0: constant rate; 1: each hidem_surrogate_train call
+                                decays it from learning_rate to 0 along a half cosine */
 } hidem_surrogate_config;
 void hidem_surrogate_config_default(hidem_surrogate_config *c);
 hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device, hidem_surrogate **out);

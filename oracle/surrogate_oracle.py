@@ -10,7 +10,12 @@ from __future__ import annotations
 
 import numpy as np
 
-N_IN, N_OUT, N_FEAT = 5, 3, 128
+N_IN, N_OUT, N_FEAT = 5, 3, 128   # default inputs, outputs, first-layer width of 5 inputs
+
+
+def feature_width(nin: int, bands: int) -> int:
+    """First layer's input width: nin * (1 + 2 bands) rounded up to a multiple of 128."""
+    return max(128, -(-nin * (1 + 2 * bands) // 128) * 128)
 
 
 def bf16_round(a: np.ndarray) -> np.ndarray:
@@ -22,15 +27,17 @@ def bf16_round(a: np.ndarray) -> np.ndarray:
 
 
 def features(u: np.ndarray, bands: int, bf16: bool = True) -> np.ndarray:
+    """u_i, then sin(2^f pi u_i), cos(2^f pi u_i) for f < bands (f-major, i, sin before
+    cos), zero padding to feature_width."""
     u = np.asarray(u, np.float32)
-    n = u.shape[0]
-    x = np.zeros((n, N_FEAT), np.float32)
-    x[:, :N_IN] = u
+    n, nin = u.shape
+    x = np.zeros((n, feature_width(nin, bands)), np.float32)
+    x[:, :nin] = u
     for f in range(bands):
         a = np.float32(2.0 ** f * 3.14159265358979) * u
-        for i in range(N_IN):
-            x[:, N_IN + 10 * f + 2 * i] = np.sin(a[:, i])
-            x[:, N_IN + 10 * f + 2 * i + 1] = np.cos(a[:, i])
+        for i in range(nin):
+            x[:, nin + 2 * nin * f + 2 * i] = np.sin(a[:, i])
+            x[:, nin + 2 * nin * f + 2 * i + 1] = np.cos(a[:, i])
     return bf16_round(x) if bf16 else x.astype(np.float64)
 
 

@@ -30,6 +30,46 @@ def test_tongue_geometry():
     assert 150_000 <= big.particles["xCord"].shape[0] <= 250_000
 
 
+def test_lattice_inputs_and_their_mirror_images():
+    t = small(9)
+    p = t.particles
+    n = p["xCord"].shape[0]
+    f = settle.lattice_inputs(t)
+    assert f.shape == (n, settle.N_LATTICE_INPUTS) and np.all(np.isfinite(f))
+    assert np.array_equal(f[:, :5], settle.surrogate_inputs(t))
+    no = len(settle.LATTICE_OFFSETS)
+    disc = 5 + 8 * no
+    # bonds, particles above, free particles below, against a direct count per column
+    x, y, z = p["xCord"], p["yCord"], p["zCord"]
+    free = (p["type"] & abi.TYPE_FIXED) == 0
+    deg = np.zeros(n, int)
+    np.add.at(deg, t.links["globalKeyEndA"], 1)
+    np.add.at(deg, t.links["globalKeyEndB"], 1)
+    for i in np.random.default_rng(0).choice(n, 40, replace=False):
+        col = (np.abs(x - x[i]) < 1e-6) & (np.abs(y - y[i]) < 1e-6)
+        assert f[i, disc] == pytest.approx(deg[i] / 6.0 - 1)
+        assert f[i, disc + 1] == pytest.approx((col & (z > z[i])).sum() / 5.0 - 1)
+        assert f[i, disc + 2] == pytest.approx((col & free & (z < z[i])).sum() / 5.0 - 1)
+        assert f[i, disc + 3] == pytest.approx((z[col].max() - z[i]) / 5.0 - 1, abs=1e-6)
+    # the x mirror image: x and the x offsets flip, the columns swap with their mirror
+    fm = settle.lattice_inputs(t, (-1, 1))
+    assert np.allclose(fm[:, 0], -f[:, 0], atol=1e-6) and np.array_equal(fm[:, 1:5], f[:, 1:5])
+    for k in range(no):
+        o = 5 + 8 * k
+        assert np.allclose(fm[:, o:o + 2], f[:, o + 2:o + 4], atol=1e-6)   # +d x <-> -d x
+        assert np.allclose(fm[:, o + 4:o + 8], f[:, o + 4:o + 8], atol=1e-6)  # y unchanged
+    assert np.array_equal(fm[:, disc:disc + 5], f[:, disc:disc + 5])
+    cols = settle.LATTICE_COLUMNS
+    for q, (di, dj) in enumerate(cols):
+        r = cols.index((-di, dj))
+        a, b = disc + 5 + 2 * q, disc + 5 + 2 * r
+        assert np.allclose(fm[:, a:a + 2], f[:, b:b + 2], atol=1e-6)
+    # outside the plan the thickness input is that of zero ice: column 7 is the thickness
+    # at x - 1.5 m, outside for x < 1 m
+    edge = x < 1.0
+    assert edge.any() and np.all(f[edge, 7] == -1.0)
+
+
 def test_rotation_estimate_of_a_rigid_rotation():
     """For u = w x x (a small rigid rotation) the estimate returns -w: the model's rotation
     sign convention."""

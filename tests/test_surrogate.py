@@ -10,8 +10,8 @@ import pytest
 from oracle import surrogate_oracle as so
 
 
-def small_params(rng, layers, width):
-    p, k = {}, so.N_FEAT
+def small_params(rng, layers, width, k0=so.N_FEAT):
+    p, k = {}, k0
     for l in range(layers):
         p[f"W{l}"] = (rng.uniform(-1, 1, (width, k)) / np.sqrt(k)).astype(np.float32)
         p[f"b{l}"] = (0.1 * rng.standard_normal(width)).astype(np.float32)
@@ -57,30 +57,47 @@ def test_oracle_backward_matches_finite_differences():
             assert abs(fd - g[name].ravel()[j]) <= 1e-6 + 1e-5 * abs(fd), (name, j)
 
 
-def _rows(rng, n):
-    u = rng.uniform(-1, 1, (n, so.N_IN)).astype(np.float32)
-    t = np.stack([np.sin(2 * u[:, 0]) * u[:, 3], 0.5 * u[:, 1] * u[:, 2], np.cos(u[:, 4]) - u[:, 2] ** 2],
-                 axis=1).astype(np.float32)
+def _rows(rng, n, nin=so.N_IN):
+    u = rng.uniform(-1, 1, (n, nin)).astype(np.float32)
+    t = np.stack([np.sin(2 * u[:, 0]) * u[:, 3], 0.5 * u[:, 1] * u[:, 2],
+                  np.cos(u[:, 4]) - u[:, 2] ** 2 + 0.3 * u[:, nin - 1]], axis=1).astype(np.float32)
     return u, t
 
 
+def test_feature_layout_and_width():
+    assert so.feature_width(5, 8) == 128 and so.feature_width(5, 12) == 128
+    assert so.feature_width(40, 4) == 384 and so.feature_width(82, 4) == 768
+    u = np.array([[0.25, -0.5, 0.125]], np.float32)
+    x = so.features(u, 2, bf16=False)
+    assert x.shape == (1, 128)
+    want = [0.25, -0.5, 0.125]
+    for f in range(2):
+        for i in range(3):
+            a = np.float32(2.0 ** f * 3.14159265358979) * u[0, i]
+            want += [np.sin(a), np.cos(a)]
+    assert np.allclose(x[0, :15], want) and not x[0, 15:].any()
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("width", [256, 128])
-def test_gpu_forward_and_gradients_match_oracle(gpu, width):
+@pytest.mark.parametrize("width,nin,bands", [(256, 5, 8), (128, 5, 8), (256, 40, 4)])
+def test_gpu_forward_and_gradients_match_oracle(gpu, width, nin, bands):
+    """nin 40, bands 4: a 384-wide first layer, whose weight gradient takes one 256-wide
+    and one 128-wide tile of columns."""
     from hidem_b200 import surrogate as sg
-    cfg = sg.default_config(width=width, hidden_layers=4, fourier_bands=8, batch=1024, seed=3)
+    cfg = sg.default_config(width=width, hidden_layers=4, fourier_bands=bands, batch=1024, seed=3,
+                            inputs=nin)
     rng = np.random.default_rng(1)
     with sg.Surrogate(cfg) as s:
-        p = small_params(rng, 4, width)
+        p = small_params(rng, 4, width, so.feature_width(nin, bands))
         s.set_params(sg.flatten(p, cfg))
         assert np.array_equal(s.get_params(), sg.flatten(p, cfg))
-        u, t = _rows(rng, 512)
+        u, t = _rows(rng, 512, nin)
         y = s.predict(u)
-        _, _, y_ref = so.forward_backward(p, 4, u, t, 8)
+        _, _, y_ref = so.forward_backward(p, 4, u, t, bands)
         # BF16 activations: a relative error of a few 1e-3 of the output scale
         assert np.max(np.abs(y - y_ref)) <= 2e-2 * (np.max(np.abs(y_ref)) + 1e-3)
         g, loss = s.gradients(u, t)
-        loss_ref, g_ref, _ = so.forward_backward(p, 4, u, t, 8)
+        loss_ref, g_ref, _ = so.forward_backward(p, 4, u, t, bands)
         assert abs(loss - loss_ref) <= 1e-2 * loss_ref
         gg = sg.unflatten(g, cfg)
         for name, _ in sg.param_shapes(cfg):
@@ -88,9 +105,9 @@ def test_gpu_forward_and_gradients_match_oracle(gpu, width):
             rel = np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30)
             assert rel < 2e-2, (name, rel)
         # predictions of rows that are not a multiple of 128, split over batches
-        u2, _ = _rows(rng, 1500)
+        u2, _ = _rows(rng, 1500, nin)
         y2 = s.predict(u2)
-        _, _, y2_ref = so.forward_backward(p, 4, u2, np.zeros((1500, 3), np.float32), 8)
+        _, _, y2_ref = so.forward_backward(p, 4, u2, np.zeros((1500, 3), np.float32), bands)
         assert np.max(np.abs(y2 - y2_ref)) <= 2e-2 * (np.max(np.abs(y2_ref)) + 1e-3)
 
 
@@ -110,3 +127,19 @@ def test_gpu_training_lowers_the_loss(gpu):
         mse = float(np.mean((s.predict(uv) - tv) ** 2))
     assert last < 0.1 * first
     assert mse < 0.1 * float(np.mean(tv ** 2))
+
+
+@pytest.mark.gpu
+def test_gpu_training_with_cosine_decay_and_wide_inputs(gpu):
+    from hidem_b200 import surrogate as sg
+    cfg = sg.default_config(width=256, hidden_layers=4, fourier_bands=4, batch=4096, seed=6,
+                            learning_rate=2e-3, inputs=40, cosine_decay=1)
+    rng = np.random.default_rng(3)
+    u, t = _rows(rng, 50000, 40)
+    with sg.Surrogate(cfg) as s:
+        s.set_data(u, t)
+        first = s.train(1)
+        s.train(300)
+        uv, tv = _rows(rng, 4096, 40)
+        mse = float(np.mean((s.predict(uv) - tv) ** 2))
+    assert mse < 0.2 * float(np.mean(tv ** 2)) and mse < first
