@@ -189,6 +189,27 @@ def map2d(values, x_min: float, y_min: float, x_max: float, y_max: float, precis
     return m, arr
 
 
+class HidemMesh(C.Structure):
+    _fields_ = [("x_vertex", C.c_void_p), ("y_vertex", C.c_void_p), ("z_vertex", C.c_void_p),
+                ("x_normal", C.c_void_p), ("y_normal", C.c_void_p), ("z_normal", C.c_void_p),
+                ("triangles", C.c_int32), ("cell_size", C.c_double), ("mesh_force", C.c_double),
+                ("mesh_drag", C.c_double)]
+
+
+def mesh(vertices, normals, cell_size: float, precision: int, mesh_force: float = 1e7,
+         mesh_drag: float = 1000.0):
+    """A hidem_mesh over `vertices` [triangles][3][3] (triangle, vertex, xyz) and `normals`
+    [triangles][3] in the lp type of `precision`; returns (struct, arrays) — keep the
+    arrays alive while the struct is used."""
+    lp = lp_dtype(precision)
+    v = np.asarray(vertices, np.float64).reshape(-1, 3, 3)
+    nrm = np.asarray(normals, np.float64).reshape(-1, 3)
+    arrs = [np.ascontiguousarray(v[:, :, k].ravel(), dtype=lp) for k in range(3)]
+    arrs += [np.ascontiguousarray(nrm[:, k], dtype=lp) for k in range(3)]
+    m = HidemMesh(*[a.ctypes.data for a in arrs], v.shape[0], cell_size, mesh_force, mesh_drag)
+    return m, arrs
+
+
 class HidemSurrogateConfig(C.Structure):
     _fields_ = [("hidden_layers", C.c_int32), ("width", C.c_int32), ("fourier_bands", C.c_int32),
                 ("batch", C.c_int32), ("learning_rate", C.c_double), ("seed", C.c_uint64),
@@ -231,6 +252,11 @@ _PROTOS = [
     ("hidem_set_bed_maps", C.c_int, [C.c_void_p, C.POINTER(HidemMap2d), C.POINTER(HidemMap2d)]),
     ("hidem_set_external_force_maps", C.c_int, [C.c_void_p, C.POINTER(HidemMap2d)]),
     ("hidem_kinetic_energy", C.c_int, [C.c_void_p, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)]),
+    ("hidem_set_collision_mesh", C.c_int, [C.c_void_p, C.POINTER(HidemMesh)]),
+    ("hidem_get_mesh_face_forces", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("hidem_zero_mesh_face_forces", C.c_int, [C.c_void_p]),
+    ("hidem_get_mesh_accel", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, _i64, C.POINTER(_i64)]),
     ("hidem_set_step_kernel", C.c_int, [C.c_void_p, _i32]),
     ("hidem_get_step_kernel", _i32, [C.c_void_p]),
     ("hidem_batch_create", C.c_int, [C.POINTER(C.c_void_p), _i32, _i32, C.POINTER(C.c_void_p)]),

@@ -20,7 +20,7 @@ INCLUDE = PKG.parent / "include"
 LIB = PKG / "libhidem_b200.so"
 OBJ = PKG / "_build"
 
-CU_SOURCES = ["kernels.cu", "api.cu", "noalloc.cu", "surrogate.cu"]
+CU_SOURCES = ["kernels.cu", "api.cu", "noalloc.cu", "surrogate.cu", "mesh.cu"]
 CPP_SOURCES = ["lattice.cpp", "config.cpp", "h5lite.cpp", "checkpoint.cpp"]
 HEADERS = ["internal.h", "kernels.h", "physics.cuh", "h5lite.h"]
 

@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <string>
@@ -124,6 +125,15 @@ struct hidem_ctx {
     void *mapData[8] = {};
     Map2dView mapView[8] = {};
     bool mapSet[8] = {};
+
+    // collision mesh: vertices (x, y, z), normals, face forces, MeshAccel cell lists
+    void *meshVtx[3] = {}, *meshNrm[3] = {}, *meshFace[3] = {};
+    int *meshSizes = nullptr, *meshStarts = nullptr, *meshValues = nullptr;
+    long long meshCells = 0, meshValueCount = 0;
+    int meshTris = 0;
+    bool meshSet = false;
+    MeshView<float> meshF{};
+    MeshView<double> meshD{};
 };
 
 namespace {
@@ -247,7 +257,7 @@ hidem_status check_params(hidem_ctx *ctx, const hidem_params *p) {
     return HIDEM_OK;
 }
 
-// The maps set on the context, in both precisions' constants.
+// The maps and the collision mesh set on the context, in both precisions' constants.
 template <class LP>
 void attach_maps_to(const hidem_ctx *ctx, Consts<LP> &c) {
     c.bedMap = ctx->mapView[0];
@@ -256,6 +266,11 @@ void attach_maps_to(const hidem_ctx *ctx, Consts<LP> &c) {
     c.useBedMap = ctx->mapSet[0] ? 1 : 0;
     c.useFricMap = ctx->mapSet[1] ? 1 : 0;
     c.useExtMaps = ctx->mapSet[2] ? 1 : 0;
+    if constexpr (sizeof(LP) == 4)
+        c.mesh = ctx->meshF;
+    else
+        c.mesh = ctx->meshD;
+    c.useMesh = ctx->meshSet ? 1 : 0;
 }
 void attach_maps(hidem_ctx *ctx) {
     attach_maps_to<float>(ctx, ctx->cf);
@@ -1304,6 +1319,14 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->dLinkKeyB);
     for (void *m : ctx->mapData)
         if (m) cudaFree(m);
+    for (int k = 0; k < 3; ++k) {
+        dfree(ctx->meshVtx[k]);
+        dfree(ctx->meshNrm[k]);
+        dfree(ctx->meshFace[k]);
+    }
+    dfree(ctx->meshSizes);
+    dfree(ctx->meshStarts);
+    dfree(ctx->meshValues);
     dfree(ctx->energyBuf);
     for (cudaEvent_t e : ctx->tuneEv)
         if (e) cudaEventDestroy(e);
@@ -1911,6 +1934,209 @@ hidem_status hidem_set_external_force_maps(hidem_ctx *ctx, const hidem_map2d *ma
     CK(cudaSetDevice(ctx->device));
     for (int k = 0; k < 6; ++k) TRY(set_map(ctx, 2 + k, maps ? &maps[k] : nullptr));
     attach_maps(ctx);
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HIDEM_OK;
+}
+
+// ------------------------------------------------------------------ collision mesh
+
+}  // extern "C"
+
+namespace {
+
+void free_mesh(hidem_ctx *ctx) {
+    for (int k = 0; k < 3; ++k) {
+        dfree(ctx->meshVtx[k]);
+        dfree(ctx->meshNrm[k]);
+        dfree(ctx->meshFace[k]);
+        ctx->meshVtx[k] = ctx->meshNrm[k] = ctx->meshFace[k] = nullptr;
+    }
+    dfree(ctx->meshSizes);
+    dfree(ctx->meshStarts);
+    dfree(ctx->meshValues);
+    ctx->meshSizes = ctx->meshStarts = ctx->meshValues = nullptr;
+    ctx->meshCells = ctx->meshValueCount = 0;
+    ctx->meshTris = 0;
+    ctx->meshSet = false;
+    ctx->meshF = MeshView<float>{};
+    ctx->meshD = MeshView<double>{};
+}
+
+// MeshAccel::generateAccel (PLiB/Geometry/MeshAccel.h:57-165): bounding box of the
+// vertices in lp (std::max / std::min folds), grown by one cell; counts
+// 1 + size / cellSize; the per-cell triangle lists built on the device.
+template <class LP>
+hidem_status build_mesh(hidem_ctx *ctx, const hidem_mesh *mesh, MeshView<LP> &m) {
+    const int T = mesh->triangles;
+    const LP *vx = static_cast<const LP *>(mesh->x_vertex);
+    const LP *vy = static_cast<const LP *>(mesh->y_vertex);
+    const LP *vz = static_cast<const LP *>(mesh->z_vertex);
+    const LP lowest = std::numeric_limits<LP>::lowest(), highest = std::numeric_limits<LP>::max();
+    LP xU = lowest, yU = lowest, zU = lowest, xL = highest, yL = highest, zL = highest;
+    for (long long i = 0; i < 3LL * T; ++i) {
+        xU = (vx[i] < xU) ? xU : vx[i];  // std::max(x, xUpper)
+        xL = (xL < vx[i]) ? xL : vx[i];  // std::min(x, xLower)
+        yU = (vy[i] < yU) ? yU : vy[i];
+        yL = (yL < vy[i]) ? yL : vy[i];
+        zU = (vz[i] < zU) ? zU : vz[i];
+        zL = (zL < vz[i]) ? zL : vz[i];
+    }
+    const LP cs = (LP)mesh->cell_size;
+    xU = xU + cs;
+    yU = yU + cs;
+    zU = zU + cs;
+    xL = xL - cs;
+    yL = yL - cs;
+    zL = zL - cs;
+    const LP xSize = xU - xL, ySize = yU - yL, zSize = zU - zL;
+    const double counts[3] = {(double)(LP(1) + xSize / cs), (double)(LP(1) + ySize / cs),
+                              (double)(LP(1) + zSize / cs)};
+    if (!(counts[0] * counts[1] * counts[2] < 2.0e9))
+        return fail(ctx, HIDEM_ERR_CAPACITY, "collision mesh grid of %.0f x %.0f x %.0f cells is too large",
+                    counts[0], counts[1], counts[2]);
+    m.xLower = xL;
+    m.yLower = yL;
+    m.zLower = zL;
+    m.xUpper = xU;
+    m.yUpper = yU;
+    m.zUpper = zU;
+    m.xInv = 1.f / cs;
+    m.yInv = 1.f / cs;
+    m.zInv = 1.f / cs;
+    m.xCount = (int)(LP(1) + xSize / cs);
+    m.yCount = (int)(LP(1) + ySize / cs);
+    m.zCount = (int)(LP(1) + zSize / cs);
+    m.force = (LP)mesh->mesh_force;
+    m.drag = (LP)mesh->mesh_drag;
+    const LP maxDist = (cs * cs) + (cs * cs) + (cs * cs) + cs;
+    const long long cells = (long long)m.xCount * m.yCount * m.zCount;
+    ctx->meshCells = cells;
+    ctx->meshTris = T;
+    const size_t vb = sizeof(LP) * 3 * (size_t)T, nb = sizeof(LP) * (size_t)T;
+    const void *vsrc[3] = {mesh->x_vertex, mesh->y_vertex, mesh->z_vertex};
+    const void *nsrc[3] = {mesh->x_normal, mesh->y_normal, mesh->z_normal};
+    for (int k = 0; k < 3; ++k) {
+        CK(cudaMalloc(&ctx->meshVtx[k], vb));
+        CK(cudaMalloc(&ctx->meshNrm[k], nb));
+        CK(cudaMalloc(&ctx->meshFace[k], nb));
+        CK(cudaMemcpyAsync(ctx->meshVtx[k], vsrc[k], vb, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->meshNrm[k], nsrc[k], nb, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(ctx->meshFace[k], 0, nb, ctx->stream));
+    }
+    m.vx = static_cast<const LP *>(ctx->meshVtx[0]);
+    m.vy = static_cast<const LP *>(ctx->meshVtx[1]);
+    m.vz = static_cast<const LP *>(ctx->meshVtx[2]);
+    m.nx = static_cast<const LP *>(ctx->meshNrm[0]);
+    m.ny = static_cast<const LP *>(ctx->meshNrm[1]);
+    m.nz = static_cast<const LP *>(ctx->meshNrm[2]);
+    m.fx = static_cast<LP *>(ctx->meshFace[0]);
+    m.fy = static_cast<LP *>(ctx->meshFace[1]);
+    m.fz = static_cast<LP *>(ctx->meshFace[2]);
+    // count pass, exclusive scan (the total into the last element of the scratch), fill
+    const long long sumsLen = cells / 1024 + 2;
+    int *scratch = nullptr;
+    CK(cudaMalloc(&ctx->meshSizes, sizeof(int) * cells));
+    CK(cudaMalloc(&ctx->meshStarts, sizeof(int) * cells));
+    CK(cudaMalloc(&scratch, sizeof(int) * (sumsLen + 1)));
+    CK(cudaMemsetAsync(ctx->meshSizes, 0, sizeof(int) * cells, ctx->stream));
+    launch_mesh_cells<LP>(m, T, cs, maxDist, ctx->meshSizes, nullptr, nullptr, false, ctx->stream);
+    launch_scan<int, int>(ctx->meshSizes, cells, 1, ctx->meshStarts, scratch, scratch + sumsLen, ctx->stream);
+    int total = 0;
+    cudaError_t e = cudaMemcpyAsync(&total, scratch + sumsLen, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(scratch);
+    CK(e);
+    ctx->meshValueCount = total;
+    CK(cudaMalloc(&ctx->meshValues, sizeof(int) * (size_t)std::max(total, 1)));
+    m.starts = ctx->meshStarts;
+    m.sizes = ctx->meshSizes;
+    m.values = ctx->meshValues;
+    launch_mesh_cells<LP>(m, T, cs, maxDist, ctx->meshSizes, ctx->meshStarts, ctx->meshValues, true,
+                          ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HIDEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+hidem_status hidem_set_collision_mesh(hidem_ctx *ctx, const hidem_mesh *mesh) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    free_mesh(ctx);
+    attach_maps(ctx);
+    if (!mesh) return HIDEM_OK;
+    if (mesh->triangles < 1 || !mesh->x_vertex || !mesh->y_vertex || !mesh->z_vertex || !mesh->x_normal ||
+        !mesh->y_normal || !mesh->z_normal)
+        return fail(ctx, HIDEM_ERR_ARG, "collision mesh: needs at least one triangle, vertices and normals");
+    if (!(mesh->cell_size > 0) || !std::isfinite(mesh->cell_size))
+        return fail(ctx, HIDEM_ERR_ARG, "collision mesh: cell_size must be positive");
+    hidem_status st = ctx->mixed ? build_mesh<float>(ctx, mesh, ctx->meshF) : build_mesh<double>(ctx, mesh, ctx->meshD);
+    if (st != HIDEM_OK) {
+        free_mesh(ctx);
+        attach_maps(ctx);
+        return st;
+    }
+    ctx->meshSet = true;
+    attach_maps(ctx);
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_mesh_face_forces(hidem_ctx *ctx, void *x, void *y, void *z) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->meshSet) return fail(ctx, HIDEM_ERR_STATE, "no collision mesh");
+    CK(cudaSetDevice(ctx->device));
+    void *out[3] = {x, y, z};
+    for (int k = 0; k < 3; ++k)
+        if (out[k])
+            CK(cudaMemcpyAsync(out[k], ctx->meshFace[k], ctx->lp * (size_t)ctx->meshTris, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HIDEM_OK;
+}
+
+hidem_status hidem_zero_mesh_face_forces(hidem_ctx *ctx) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->meshSet) return fail(ctx, HIDEM_ERR_STATE, "no collision mesh");
+    CK(cudaSetDevice(ctx->device));
+    for (int k = 0; k < 3; ++k)
+        CK(cudaMemsetAsync(ctx->meshFace[k], 0, ctx->lp * (size_t)ctx->meshTris, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_mesh_accel(hidem_ctx *ctx, int32_t counts[3], double lower[3], double upper[3],
+                                  int32_t *sizes, int32_t *starts, int32_t *values, int64_t values_cap,
+                                  int64_t *values_count) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->meshSet) return fail(ctx, HIDEM_ERR_STATE, "no collision mesh");
+    CK(cudaSetDevice(ctx->device));
+    const int c[3] = {ctx->mixed ? ctx->meshF.xCount : ctx->meshD.xCount,
+                      ctx->mixed ? ctx->meshF.yCount : ctx->meshD.yCount,
+                      ctx->mixed ? ctx->meshF.zCount : ctx->meshD.zCount};
+    const double lo[3] = {ctx->mixed ? (double)ctx->meshF.xLower : ctx->meshD.xLower,
+                          ctx->mixed ? (double)ctx->meshF.yLower : ctx->meshD.yLower,
+                          ctx->mixed ? (double)ctx->meshF.zLower : ctx->meshD.zLower};
+    const double hi[3] = {ctx->mixed ? (double)ctx->meshF.xUpper : ctx->meshD.xUpper,
+                          ctx->mixed ? (double)ctx->meshF.yUpper : ctx->meshD.yUpper,
+                          ctx->mixed ? (double)ctx->meshF.zUpper : ctx->meshD.zUpper};
+    for (int k = 0; k < 3; ++k) {
+        if (counts) counts[k] = c[k];
+        if (lower) lower[k] = lo[k];
+        if (upper) upper[k] = hi[k];
+    }
+    if (sizes)
+        CK(cudaMemcpyAsync(sizes, ctx->meshSizes, sizeof(int) * ctx->meshCells, cudaMemcpyDeviceToHost, ctx->stream));
+    if (starts)
+        CK(cudaMemcpyAsync(starts, ctx->meshStarts, sizeof(int) * ctx->meshCells, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    if (values && values_cap > 0)
+        CK(cudaMemcpyAsync(values, ctx->meshValues, sizeof(int) * std::min<long long>(values_cap, ctx->meshValueCount),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+    if (values_count) *values_count = ctx->meshValueCount;
     CK(cudaStreamSynchronize(ctx->stream));
     return HIDEM_OK;
 }

@@ -60,6 +60,20 @@ struct Map2dView {
     int xPoints, yPoints;
 };
 
+// A collision mesh with its MeshAccel grid (PLiB/Geometry/MeshAccel.h:15-47,
+// PLiB/MeshData.h:21-35): vertices and normals in lp, cell lists, face force sums.
+template <class LP>
+struct MeshView {
+    const LP *vx, *vy, *vz;        // vertex j of triangle t at 3t + j
+    const LP *nx, *ny, *nz;        // per triangle
+    const int *starts, *sizes, *values;
+    LP *fx, *fy, *fz;              // face forces, accumulated
+    LP xLower, yLower, zLower, xUpper, yUpper, zUpper;
+    LP xInv, yInv, zInv;           // 1 / cell size, as MeshAccel stores them
+    LP force, drag;                // meshForce, meshDrag of the sample main
+    int xCount, yCount, zCount;
+};
+
 // Constants of the default functors and of the sample integrate step, in lp
 // precision, computed on the host exactly as the sample main computes them
 // (HiDEM/MeshBlock/MainMeshBlock.cpp:106-156).
@@ -81,6 +95,9 @@ struct Consts {
     // GlacierDem bed / friction maps and external force maps (x, y, z, u, v, w)
     Map2dView bedMap, fricMap, extMap[6];
     int useBedMap, useFricMap, useExtMaps;
+    // collision mesh of the MeshConstrainedDem sample
+    MeshView<LP> mesh;
+    int useMesh;
 };
 
 // Grid of the last rebuild (NeighbourGrid members, PLiB/NeighbourGrid.h:25-52).

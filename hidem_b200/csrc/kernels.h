@@ -163,6 +163,11 @@ void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slot
 template <class LP>
 void launch_energy(const Consts<LP> &c, const PRec<LP> *rec, int n, double *partial, int nb,
                    double *out, cudaStream_t s);
+// MeshAccel grid of a collision mesh (m's grid fields set, sizes zeroed first): the count
+// pass (fill false) writes sizes; the fill pass writes values at starts
+template <class LP>
+void launch_mesh_cells(const MeshView<LP> &m, int ntri, LP cellSize, LP maxDist, int *sizes,
+                       const int *starts, int *values, bool fill, cudaStream_t s);
 template <class LP>
 void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb, cudaStream_t s);
 

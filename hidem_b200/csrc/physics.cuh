@@ -206,6 +206,98 @@ __device__ __forceinline__ LP map_interp(const Map2dView &m, float x, float y) {
     return (LP)((((y2 - y0) * invY21) * fxy1) + (((y0 - y1) * invY21) * fxy2));
 }
 
+// ------------------------------------------------------------------ collision mesh
+// Real3f of the reference (PLiB/Util/Real3.h:142-258): float components; dot sums
+// left to right, cross by components, no fused multiply-adds.
+struct V3f {
+    float x, y, z;
+};
+__device__ __forceinline__ V3f v3_sub(V3f a, V3f b) { return V3f{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3f v3_mul(V3f a, V3f b) { return V3f{a.x * b.x, a.y * b.y, a.z * b.z}; }
+__device__ __forceinline__ float v3_dot(V3f a, V3f b) { return (a.x * b.x) + (a.y * b.y) + (a.z * b.z); }
+__device__ __forceinline__ V3f v3_cross(V3f a, V3f b) {
+    return V3f{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float sign_f(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+
+// squared distance of point p from an edge e = b - a with q = p - a: the edge term of
+// MeshAccel::triSDF2, the projection parameter clamped to [0, 1] in lp (clamp3)
+template <class LP>
+__device__ __forceinline__ float tri_edge2(V3f e, V3f q) {
+    const float t = v3_dot(e, q) / v3_dot(e, e);
+    LP tl = (LP)t;
+    tl = tl < LP(0) ? LP(0) : (tl > LP(1) ? LP(1) : tl);
+    const float tc = (float)tl;
+    const V3f d = v3_sub(v3_mul(e, V3f{tc, tc, tc}), q);
+    return v3_dot(d, d);
+}
+
+// MeshAccel::triSDF2 (PLiB/Geometry/MeshAccel.h:329-372): squared distance of p from the
+// triangle abc — the nearest edge when p projects outside it, else the plane distance.
+template <class LP>
+__device__ __forceinline__ LP tri_sdf2(V3f p, V3f a, V3f b, V3f c) {
+    const V3f ba = v3_sub(b, a), pa = v3_sub(p, a);
+    const V3f cb = v3_sub(c, b), pb = v3_sub(p, b);
+    const V3f ac = v3_sub(a, c), pc = v3_sub(p, c);
+    const V3f nor = v3_cross(ba, ac);
+    const float s = sign_f(v3_dot(v3_cross(ba, nor), pa)) + sign_f(v3_dot(v3_cross(cb, nor), pb)) +
+                    sign_f(v3_dot(v3_cross(ac, nor), pc));
+    if (s < 2.0f) {
+        const float e1 = tri_edge2<LP>(ba, pa), e2 = tri_edge2<LP>(cb, pb), e3 = tri_edge2<LP>(ac, pc);
+        const float m12 = (e2 < e1) ? e2 : e1;  // std::min(e1, e2)
+        return (LP)((e3 < m12) ? e3 : m12);
+    }
+    const float dn = v3_dot(nor, pa);
+    return (LP)(dn * dn / v3_dot(nor, nor));
+}
+
+template <class LP>
+__device__ __forceinline__ V3f mesh_vertex(const MeshView<LP> &m, int i) {
+    return V3f{(float)m.vx[i], (float)m.vy[i], (float)m.vz[i]};
+}
+
+// MeshAccel::getCell of a point given as lp (getCellCord, MeshAccel.h:295-316): the
+// point as Real3f, minus the lower corner, times the inverse cell size, truncated.
+// -1 where the cell lies outside the grid (which the reference's bounding-box test
+// admits only through rounding at the upper faces, and then reads past its arrays).
+template <class LP>
+__device__ __forceinline__ int mesh_cell(const MeshView<LP> &m, LP x, LP y, LP z) {
+    const float cx = (float)((LP)(float)x - m.xLower);
+    const float cy = (float)((LP)(float)y - m.yLower);
+    const float cz = (float)((LP)(float)z - m.zLower);
+    const int xc = (int)((LP)cx * m.xInv), yc = (int)((LP)cy * m.yInv), zc = (int)((LP)cz * m.zInv);
+    if (xc < 0 || yc < 0 || zc < 0 || xc >= m.xCount || yc >= m.yCount || zc >= m.zCount) return -1;
+    return (xc * m.yCount * m.zCount) + (yc * m.zCount) + zc;
+}
+
+// MeshAccel::getClosestTriAccel (MeshAccel.h:375-412): the closest triangle of the
+// point's cell within interactDist (the first of equals), or -1; *dist2 its squared
+// distance.
+template <class LP>
+__device__ __forceinline__ int mesh_closest(const MeshView<LP> &m, LP x, LP y, LP z, LP interactDist,
+                                            LP *dist2) {
+    if (x > m.xUpper || y > m.yUpper || z > m.zUpper || x < m.xLower || y < m.yLower || z < m.zLower)
+        return -1;
+    const int cell = mesh_cell(m, x, y, z);
+    if (cell < 0) return -1;
+    const int start = m.starts[cell], size = m.sizes[cell];
+    const V3f p{(float)x, (float)y, (float)z};
+    const LP id2 = interactDist * interactDist;
+    LP minDist = sizeof(LP) == 4 ? (LP)3.40282347e+38f : (LP)1.7976931348623157e+308;
+    int closest = -1;
+    for (int i = start; i < start + size; ++i) {
+        const int tri = m.values[i];
+        const LP cur = tri_sdf2<LP>(p, mesh_vertex(m, 3 * tri), mesh_vertex(m, 3 * tri + 1),
+                                    mesh_vertex(m, 3 * tri + 2));
+        if (id2 > cur && cur < minDist) {
+            minDist = cur;
+            closest = tri;
+        }
+    }
+    *dist2 = minDist;
+    return closest;
+}
+
 // The sample integrate step on one particle (HiDEM/MeshBlock/MainMeshBlock.cpp:182-261:
 // gravity / buoyancy, air / water drag, HiDEMDefTimeIntegration
 // HiDEMDefaultFunctions.h:318-370) plus the optional GlacierDem bed terms
@@ -251,6 +343,25 @@ __device__ __forceinline__ void integrate_particle(const Consts<LP> &c, PRec<LP>
     if (c.useBed && zCord + (double)radius < (double)bedHeight)
         zForce = (LP)((double)zForce +
                       (double)c.bedStiffness * ((double)bedHeight - (zCord + (double)radius)));
+    // collision mesh (HiDEM/MeshConstrainedDem/MainMeshDem.cpp:220-235)
+    if (c.useMesh) {
+        LP dist2;
+        const int tri = mesh_closest(c.mesh, (LP)xCord, (LP)yCord, (LP)zCord, c.bedInteract + radius, &dist2);
+        if (tri >= 0) {
+            const float maxDist = (float)(c.bedInteract + radius);
+            const LP dist = lsqrt(dist2);
+            dragCoeff = c.mesh.drag * ((LP)maxDist - dist);
+            const LP fx = -c.mesh.nx[tri] * ((LP)maxDist - dist) * c.mesh.force;
+            const LP fy = -c.mesh.ny[tri] * ((LP)maxDist - dist) * c.mesh.force;
+            const LP fz = -c.mesh.nz[tri] * ((LP)maxDist - dist) * c.mesh.force;
+            atomicAdd(&c.mesh.fx[tri], fx);
+            atomicAdd(&c.mesh.fy[tri], fy);
+            atomicAdd(&c.mesh.fz[tri], fz);
+            xForce = xForce + fx;
+            yForce = yForce + fy;
+            zForce = zForce + fz;
+        }
+    }
     // external force maps (ExternalForces, PLiB/ExternalForces.h; MainDem.cpp:211-216)
     if (c.useExtMaps) {
         const float fx = (float)xCord, fy = (float)yCord;

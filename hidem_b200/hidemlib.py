@@ -23,6 +23,7 @@ class HiDEMLib:
     def __init__(self, params: abi.HidemParams, device: int = 0, end_timestep: int | None = None):
         self._lib = abi.load()
         self.params = params
+        self._mesh_tris = 0
         self.precision = int(params.precision)
         self.lp = abi.lp_dtype(self.precision)
         h = C.c_void_p()
@@ -133,6 +134,25 @@ class HiDEMLib:
         """Six external force maps (x, y, z, u, v, w; abi.map2d structs), or None."""
         arr = (abi.HidemMap2d * 6)(*maps) if maps is not None else None
         self._check(self._lib.hidem_set_external_force_maps(self._ctx, arr))
+
+    def set_collision_mesh(self, mesh=None) -> None:
+        """Collision mesh (an abi.mesh struct; the data is copied), or None to remove it."""
+        self._check(self._lib.hidem_set_collision_mesh(self._ctx, C.byref(mesh) if mesh is not None else None))
+        self._mesh_tris = int(mesh.triangles) if mesh is not None else 0
+
+    def mesh_face_forces(self) -> np.ndarray:
+        """[triangles][3] face forces accumulated since the mesh was set or zeroed."""
+        lp = abi.lp_dtype(int(self.params.precision))
+        out = [np.zeros(self._mesh_tris, lp) for _ in range(3)]
+        self._check(self._lib.hidem_get_mesh_face_forces(self._ctx, *[a.ctypes.data for a in out]))
+        return np.stack(out, axis=1)
+
+    def zero_mesh_face_forces(self) -> None:
+        self._check(self._lib.hidem_zero_mesh_face_forces(self._ctx))
+
+    def mesh_accel(self) -> dict:
+        """The MeshAccel grid: counts, lower, upper, sizes, starts, values."""
+        return _mesh_accel(lambda *a: self._check(self._lib.hidem_get_mesh_accel(self._ctx, *a)))
 
     def kinetic_energy(self) -> tuple[float, float, float]:
         """(translational, rotational, max speed) of the current state."""
@@ -278,3 +298,19 @@ class HiDEMBatch:
             self.close()
         except Exception:
             pass
+
+
+def _mesh_accel(call) -> dict:
+    """Reads a MeshAccel grid through `call(counts, lower, upper, sizes, starts, values, cap,
+    count)` (the contract of hidem_get_mesh_accel), sizing the arrays from a first call."""
+    counts = np.zeros(3, np.int32)
+    lower, upper = np.zeros(3), np.zeros(3)
+    nv = C.c_int64()
+    call(counts.ctypes.data, lower.ctypes.data, upper.ctypes.data, None, None, None, 0, C.byref(nv))
+    cells = int(np.prod(counts.astype(np.int64)))
+    sizes, starts = np.zeros(cells, np.int32), np.zeros(cells, np.int32)
+    values = np.zeros(max(nv.value, 1), np.int32)
+    call(counts.ctypes.data, lower.ctypes.data, upper.ctypes.data, sizes.ctypes.data, starts.ctypes.data,
+         values.ctypes.data, values.shape[0], C.byref(nv))
+    return {"counts": counts, "lower": lower, "upper": upper, "sizes": sizes, "starts": starts,
+            "values": values[:nv.value]}

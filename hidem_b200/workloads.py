@@ -90,6 +90,41 @@ def ice_block(cells=(20, 20, 20), precision: int = abi.PREC_MIXED, seed: int = 1
     return params, p, links
 
 
+def container_mesh(lo, hi, bed, nx: int = 8, ny: int = 8, walls: bool = True):
+    """A collision mesh shaped as an open container, the form the MeshConstrainedDem
+    sample's mesh takes: the bed z = bed(x, y) over [lo[0], hi[0]] x [lo[1], hi[1]] as a
+    triangulated grid of nx x ny quads (two triangles each), and with `walls` four vertical
+    walls up to hi[2]. Normals point out of the container (down through the bed, out
+    through the walls), so the mesh force, along minus the normal, pushes the particles
+    inside back in. Returns (vertices [T][3][3], normals [T][3])."""
+    xs = np.linspace(lo[0], hi[0], nx + 1)
+    ys = np.linspace(lo[1], hi[1], ny + 1)
+    tris = []
+    for i in range(nx):
+        for j in range(ny):
+            p00 = (xs[i], ys[j], bed(xs[i], ys[j]))
+            p10 = (xs[i + 1], ys[j], bed(xs[i + 1], ys[j]))
+            p11 = (xs[i + 1], ys[j + 1], bed(xs[i + 1], ys[j + 1]))
+            p01 = (xs[i], ys[j + 1], bed(xs[i], ys[j + 1]))
+            tris += [(p00, p10, p11), (p00, p11, p01)]
+    v = np.array(tris, np.float64)
+    nrm = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0])  # upward for these windings
+    nrm = -nrm / np.linalg.norm(nrm, axis=1, keepdims=True)
+    if walls:
+        zb = min(bed(x, y) for x in (lo[0], hi[0]) for y in (lo[1], hi[1])) - 1.0
+        zt = hi[2]
+        wall = []
+        for x, nx_ in ((lo[0], -1.0), (hi[0], 1.0)):
+            a, b, c, d = (x, lo[1], zb), (x, hi[1], zb), (x, hi[1], zt), (x, lo[1], zt)
+            wall += [((a, b, c), (nx_, 0.0, 0.0)), ((a, c, d), (nx_, 0.0, 0.0))]
+        for y, ny_ in ((lo[1], -1.0), (hi[1], 1.0)):
+            a, b, c, d = (lo[0], y, zb), (hi[0], y, zb), (hi[0], y, zt), (lo[0], y, zt)
+            wall += [((a, b, c), (0.0, ny_, 0.0)), ((a, c, d), (0.0, ny_, 0.0))]
+        v = np.concatenate([v, np.array([w[0] for w in wall])])
+        nrm = np.concatenate([nrm, np.array([w[1] for w in wall])])
+    return v, nrm
+
+
 def calving_slab(size=(400.0, 100.0, 100.0), precision: int = abi.PREC_MIXED, seed: int = 7,
                  jitter: float = 0.01, broken_fraction: float = 0.01, water_level: float = 90.0,
                  **param_over):

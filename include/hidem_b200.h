@@ -277,6 +277,51 @@ hidem_status hidem_set_bed_maps(hidem_ctx *ctx, const hidem_map2d *bed, const hi
  * to remove them. The data is copied. */
 hidem_status hidem_set_external_force_maps(hidem_ctx *ctx, const hidem_map2d *maps);
 
+/* ---- collision mesh ---------------------------------------------------- */
+
+/* A triangle mesh the particles collide with, as the MeshConstrainedDem sample uses it
+ * (HiDEM/MeshConstrainedDem/MainMeshDem.cpp:111-113, 220-235): the reference's
+ * CollisionMesh (PLiB/Geometry/CollisionMesh.h, Mesh.h) with its MeshAccel grid
+ * (PLiB/Geometry/MeshAccel.h). Vertex j of triangle t is (x_vertex[3t + j],
+ * y_vertex[3t + j], z_vertex[3t + j]) and its normal (x_normal[t], ...), the MeshData
+ * layout (PLiB/MeshData.h:21-27); all lp (float in HIDEM_PREC_MIXED, double in
+ * HIDEM_PREC_FP64). */
+typedef struct hidem_mesh {
+    const void *x_vertex, *y_vertex, *z_vertex;  /* [3 * triangles] */
+    const void *x_normal, *y_normal, *z_normal;  /* [triangles] */
+    int32_t triangles;
+    double cell_size;   /* MeshAccel cell size and search distance (the sample: 16 maxRadius) */
+    double mesh_force;  /* general.meshForce (the sample's default 1e7) */
+    double mesh_drag;   /* general.meshDrag (1000) */
+} hidem_mesh;
+/* Sets the collision mesh (NULL removes it) and builds its MeshAccel grid on the device
+ * (MeshAccel::generateAccel, MeshAccel.h:57-165: cells of cell_size over the vertices'
+ * bounding box grown by one cell, z fastest; each cell lists, in ascending order, the
+ * triangles whose squared distance from the cell centre (MeshAccel::triSDF2, 329-372) is
+ * below 3 cell_size^2 + cell_size). From then on the integrate step finds, for each
+ * particle inside the grid, the closest triangle of its cell within bedInteract + radius
+ * (Mesh::closestTriFun / MeshAccel::getClosestTriAccel, Mesh.h:69-83, MeshAccel.h:375-412)
+ * and, when there is one, pushes the particle along minus the triangle's normal by
+ * mesh_force * (bedInteract + radius - distance), sets the drag coefficient to
+ * mesh_drag * (bedInteract + radius - distance) and adds the push to the triangle's face
+ * force (MainMeshDem.cpp:220-235), after the bed force and before the external force maps.
+ * Face forces start at zero. The data is copied. */
+hidem_status hidem_set_collision_mesh(hidem_ctx *ctx, const hidem_mesh *mesh);
+/* The face forces accumulated since the mesh was set or last zeroed (CollisionMesh
+ * xFaceForce..zFaceForce, CollisionMesh.h:46-52): lp [triangles] each. The sum over a
+ * face is formed with atomic additions, as in the reference, so its rounding depends on
+ * the order the particles add in. */
+hidem_status hidem_get_mesh_face_forces(hidem_ctx *ctx, void *x, void *y, void *z);
+/* CollisionMesh::zeroForce (CollisionMesh.h:54-62) */
+hidem_status hidem_zero_mesh_face_forces(hidem_ctx *ctx);
+/* The MeshAccel grid: counts (x, y, z cells), lower and upper corners (lp values as
+ * doubles), per cell (index (x * Y + y) * Z + z) the triangle count and start, and the
+ * triangle lists (values_cap entries at most; *values_count receives the total). Any
+ * array pointer may be NULL. */
+hidem_status hidem_get_mesh_accel(hidem_ctx *ctx, int32_t counts[3], double lower[3], double upper[3],
+                                  int32_t *sizes, int32_t *starts, int32_t *values,
+                                  int64_t values_cap, int64_t *values_count);
+
 /* ---- diagnostics ------------------------------------------------------ */
 
 /* Kinetic energy of the current state, the convergence measure of settling runs (no

@@ -6,6 +6,7 @@
  * the mixed (float lp/ct) and the plain FP64 builds of the reference.
  */
 #define _POSIX_C_SOURCE 199309L
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -32,6 +33,35 @@ void hidem_oracle_set_maps(const hidem_map2d *bed, const hidem_map2d *friction,
 
 static int clampi_(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+/* Collision mesh of the next runs (the caller keeps its arrays alive) and the face forces
+ * of the last run with a mesh ([triangle][x y z], lp of that run). */
+static hidem_mesh g_mesh;
+static int g_mesh_set;
+static void *g_mesh_face;
+static int g_mesh_face_lp;
+
+void hidem_oracle_set_mesh(const hidem_mesh *mesh) {
+    memset(&g_mesh, 0, sizeof g_mesh);
+    g_mesh_set = 0;
+    if (mesh && mesh->triangles > 0) {
+        g_mesh = *mesh;
+        g_mesh_set = 1;
+    }
+}
+
+/* Real3f arithmetic of the reference (PLiB/Util/Real3.h:142-258) */
+typedef struct v3f {
+    float x, y, z;
+} v3f;
+static v3f v3f_sub(v3f a, v3f b) { v3f r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static v3f v3f_mul(v3f a, v3f b) { v3f r = {a.x * b.x, a.y * b.y, a.z * b.z}; return r; }
+static float v3f_dot(v3f a, v3f b) { return (a.x * b.x) + (a.y * b.y) + (a.z * b.z); }
+static v3f v3f_cross(v3f a, v3f b) {
+    v3f r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return r;
+}
+static float sign_f(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+
 #define LP float
 #define LSQRT sqrtf
 #define LABS fabsf
@@ -51,6 +81,59 @@ static int clampi_(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : 
 #undef LSQRT
 #undef LABS
 #undef SFX
+
+int hidem_oracle_mesh_face_forces(void *x, void *y, void *z) {
+    if (!g_mesh_face) return HIDEM_ERR_STATE;
+    void *out[3] = {x, y, z};
+    for (int k = 0; k < 3; ++k) {
+        if (!out[k]) continue;
+        for (int64_t t = 0; t < g_mesh.triangles; ++t) {
+            if (g_mesh_face_lp == 4)
+                ((float *)out[k])[t] = ((const float *)g_mesh_face)[3 * t + k];
+            else
+                ((double *)out[k])[t] = ((const double *)g_mesh_face)[3 * t + k];
+        }
+    }
+    return 0;
+}
+
+int hidem_oracle_mesh_accel(int32_t precision, int32_t counts[3], double lower[3], double upper[3],
+                            int32_t *sizes, int32_t *starts, int32_t *values, int64_t values_cap,
+                            int64_t *values_count) {
+    if (!g_mesh_set) return HIDEM_ERR_STATE;
+    int64_t cells, nv;
+    int c[3];
+    double lo[3], hi[3];
+    int32_t *sz, *st, *va;
+    if (precision == HIDEM_PREC_MIXED) {
+        mesh_accel_mixed A;
+        mesh_build_mixed(&g_mesh, &A);
+        c[0] = A.xCount; c[1] = A.yCount; c[2] = A.zCount;
+        lo[0] = A.xLower; lo[1] = A.yLower; lo[2] = A.zLower;
+        hi[0] = A.xUpper; hi[1] = A.yUpper; hi[2] = A.zUpper;
+        cells = A.cells; nv = A.nvalues; sz = A.sizes; st = A.starts; va = A.values;
+    } else {
+        mesh_accel_fp64 A;
+        mesh_build_fp64(&g_mesh, &A);
+        c[0] = A.xCount; c[1] = A.yCount; c[2] = A.zCount;
+        lo[0] = A.xLower; lo[1] = A.yLower; lo[2] = A.zLower;
+        hi[0] = A.xUpper; hi[1] = A.yUpper; hi[2] = A.zUpper;
+        cells = A.cells; nv = A.nvalues; sz = A.sizes; st = A.starts; va = A.values;
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (counts) counts[k] = c[k];
+        if (lower) lower[k] = lo[k];
+        if (upper) upper[k] = hi[k];
+    }
+    if (sizes) memcpy(sizes, sz, sizeof(int32_t) * (size_t)cells);
+    if (starts) memcpy(starts, st, sizeof(int32_t) * (size_t)cells);
+    if (values) memcpy(values, va, sizeof(int32_t) * (size_t)(nv < values_cap ? nv : values_cap));
+    if (values_count) *values_count = nv;
+    free(sz);
+    free(st);
+    free(va);
+    return 0;
+}
 
 int hidem_oracle_threads(void) {
 #ifdef _OPENMP

@@ -41,6 +41,19 @@ int hidem_oracle_threads(void);
 void hidem_oracle_set_maps(const hidem_map2d *bed, const hidem_map2d *friction,
                            const hidem_map2d *ext);
 
+/* Collision mesh used by the integrate step of the next runs (NULL: none), as
+ * HiDEM/MeshConstrainedDem/MainMeshDem.cpp:111-113, 220-235 uses it; the arrays must
+ * stay alive while they run. */
+void hidem_oracle_set_mesh(const hidem_mesh *mesh);
+/* Face forces accumulated over the last run with a mesh (summed in particle order),
+ * lp [triangles] each. */
+int hidem_oracle_mesh_face_forces(void *x, void *y, void *z);
+/* The MeshAccel grid of the set mesh in the given precision (the contract of
+ * hidem_get_mesh_accel). */
+int hidem_oracle_mesh_accel(int32_t precision, int32_t counts[3], double lower[3], double upper[3],
+                            int32_t *sizes, int32_t *starts, int32_t *values, int64_t values_cap,
+                            int64_t *values_count);
+
 #ifdef __cplusplus
 }
 #endif

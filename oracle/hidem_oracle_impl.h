@@ -449,6 +449,160 @@ static void SFX(adj_free)(SFX(adj) *a) {
     free(a->side);
 }
 
+/* ------------------------------------------------------------ collision mesh */
+
+/* MeshAccel grid of a collision mesh (PLiB/Geometry/MeshAccel.h:15-47) */
+typedef struct SFX(mesh_accel) {
+    LP xLower, yLower, zLower, xUpper, yUpper, zUpper, xInv, yInv, zInv, cellSize, maxDist;
+    int xCount, yCount, zCount;
+    int64_t cells, nvalues;
+    int32_t *sizes, *starts, *values;
+} SFX(mesh_accel);
+
+/* MeshAccel::triSDF2 (MeshAccel.h:329-372) in Real3f arithmetic (PLiB/Util/Real3.h:
+ * 142-258): float components, dot summed left to right; the edge parameter clamped in
+ * lp (clamp3 / clamp, PLiB/Util/Util.h:245-253); std::min(a, b) == (b < a) ? b : a. */
+static float SFX(tri_edge2)(v3f e, v3f q) {
+    float t = v3f_dot(e, q) / v3f_dot(e, e);
+    LP tl = (LP)t;
+    tl = tl < (LP)0 ? (LP)0 : (tl > (LP)1 ? (LP)1 : tl);
+    float tc = (float)tl;
+    v3f dd = v3f_sub(v3f_mul(e, (v3f){tc, tc, tc}), q);
+    return v3f_dot(dd, dd);
+}
+
+static LP SFX(tri_sdf2)(v3f pt, v3f a, v3f b, v3f c) {
+    v3f ba = v3f_sub(b, a), pa = v3f_sub(pt, a), cb = v3f_sub(c, b), pb = v3f_sub(pt, b);
+    v3f ac = v3f_sub(a, c), pc = v3f_sub(pt, c);
+    v3f nor = v3f_cross(ba, ac);
+    float sg = sign_f(v3f_dot(v3f_cross(ba, nor), pa)) + sign_f(v3f_dot(v3f_cross(cb, nor), pb)) +
+               sign_f(v3f_dot(v3f_cross(ac, nor), pc));
+    if (sg < 2.0f) {
+        float e1 = SFX(tri_edge2)(ba, pa), e2 = SFX(tri_edge2)(cb, pb), e3 = SFX(tri_edge2)(ac, pc);
+        float m12 = (e2 < e1) ? e2 : e1;
+        return (LP)((e3 < m12) ? e3 : m12);
+    }
+    float dn = v3f_dot(nor, pa);
+    return (LP)(dn * dn / v3f_dot(nor, nor));
+}
+
+static v3f SFX(mesh_vtx)(const hidem_mesh *m, int64_t i) {
+    const LP *vx = (const LP *)m->x_vertex, *vy = (const LP *)m->y_vertex, *vz = (const LP *)m->z_vertex;
+    v3f r = {(float)vx[i], (float)vy[i], (float)vz[i]};
+    return r;
+}
+
+/* MeshAccel::getCell / getCellCord (MeshAccel.h:295-316): the point as Real3f, the
+ * lower corner subtracted in lp and stored back to float, times the inverse cell size in
+ * lp, truncated; -1 outside the grid. */
+static int SFX(mesh_cell)(const SFX(mesh_accel) *A, LP x, LP y, LP z) {
+    float cx = (float)((LP)(float)x - A->xLower);
+    float cy = (float)((LP)(float)y - A->yLower);
+    float cz = (float)((LP)(float)z - A->zLower);
+    int xc = (int)((LP)cx * A->xInv), yc = (int)((LP)cy * A->yInv), zc = (int)((LP)cz * A->zInv);
+    if (xc < 0 || yc < 0 || zc < 0 || xc >= A->xCount || yc >= A->yCount || zc >= A->zCount) return -1;
+    return (xc * A->yCount * A->zCount) + (yc * A->zCount) + zc;
+}
+
+/* MeshAccel::generateAccel (MeshAccel.h:57-165): bounding box of the vertices grown by one
+ * cell, 1 + size / cellSize cells per axis (z fastest), and per cell the triangles whose
+ * triSDF2 from the cell centre is below 3 cellSize^2 + cellSize, ascending. */
+static void SFX(mesh_build)(const hidem_mesh *m, SFX(mesh_accel) *A) {
+    const LP *vx = (const LP *)m->x_vertex, *vy = (const LP *)m->y_vertex, *vz = (const LP *)m->z_vertex;
+    LP hi = sizeof(LP) == 4 ? (LP)FLT_MAX : (LP)DBL_MAX;
+    LP xU = -hi, yU = -hi, zU = -hi, xL = hi, yL = hi, zL = hi;
+    for (int64_t i = 0; i < 3 * (int64_t)m->triangles; ++i) {
+        xU = (vx[i] < xU) ? xU : vx[i];
+        xL = (xL < vx[i]) ? xL : vx[i];
+        yU = (vy[i] < yU) ? yU : vy[i];
+        yL = (yL < vy[i]) ? yL : vy[i];
+        zU = (vz[i] < zU) ? zU : vz[i];
+        zL = (zL < vz[i]) ? zL : vz[i];
+    }
+    LP cs = (LP)m->cell_size;
+    A->xUpper = xU + cs;
+    A->yUpper = yU + cs;
+    A->zUpper = zU + cs;
+    A->xLower = xL - cs;
+    A->yLower = yL - cs;
+    A->zLower = zL - cs;
+    LP xSize = A->xUpper - A->xLower, ySize = A->yUpper - A->yLower, zSize = A->zUpper - A->zLower;
+    A->cellSize = cs;
+    A->xInv = (LP)1.0f / cs;
+    A->yInv = (LP)1.0f / cs;
+    A->zInv = (LP)1.0f / cs;
+    A->xCount = (int)((LP)1 + xSize / cs);
+    A->yCount = (int)((LP)1 + ySize / cs);
+    A->zCount = (int)((LP)1 + zSize / cs);
+    A->maxDist = (cs * cs) + (cs * cs) + (cs * cs) + cs;
+    A->cells = (int64_t)A->xCount * A->yCount * A->zCount;
+    A->sizes = (int32_t *)calloc((size_t)A->cells, sizeof(int32_t));
+    A->starts = (int32_t *)calloc((size_t)A->cells, sizeof(int32_t));
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int x = 0; x < A->xCount; ++x)
+            for (int y = 0; y < A->yCount; ++y)
+                for (int zz = 0; zz < A->zCount; ++zz) {
+                    LP half = (LP)0.5f * cs;
+                    LP xPos = ((LP)x * cs + half) + A->xLower;
+                    LP yPos = ((LP)y * cs + half) + A->yLower;
+                    LP zPos = ((LP)zz * cs + half) + A->zLower;
+                    int cell = SFX(mesh_cell)(A, xPos, yPos, zPos);
+                    if (cell < 0) continue;
+                    v3f pt = {(float)xPos, (float)yPos, (float)zPos};
+                    int found = 0;
+                    for (int i = 0; i < m->triangles; ++i) {
+                        LP dd = SFX(tri_sdf2)(pt, SFX(mesh_vtx)(m, 3 * (int64_t)i), SFX(mesh_vtx)(m, 3 * (int64_t)i + 1),
+                                              SFX(mesh_vtx)(m, 3 * (int64_t)i + 2));
+                        if (dd < A->maxDist) {
+                            if (pass == 1) A->values[A->starts[cell] + found] = i;
+                            ++found;
+                        }
+                    }
+                    if (pass == 0) A->sizes[cell] = found;
+                }
+        if (pass == 0) {
+            int64_t acc = 0;
+            for (int64_t c = 0; c < A->cells; ++c) {
+                A->starts[c] = (int32_t)acc;
+                acc += A->sizes[c];
+            }
+            A->nvalues = acc;
+            A->values = (int32_t *)malloc(sizeof(int32_t) * (size_t)(acc + 1));
+        }
+    }
+}
+
+static void SFX(mesh_free)(SFX(mesh_accel) *A) {
+    free(A->sizes);
+    free(A->starts);
+    free(A->values);
+}
+
+/* MeshAccel::getClosestTriAccel (MeshAccel.h:375-412) as Mesh::closestTriFun calls it
+ * (Mesh.h:69-83): the closest triangle of the point's cell within interactDist, or -1. */
+static int SFX(mesh_closest)(const hidem_mesh *m, const SFX(mesh_accel) *A, LP x, LP y, LP z,
+                             LP interactDist, LP *dist2) {
+    if (x > A->xUpper || y > A->yUpper || z > A->zUpper || x < A->xLower || y < A->yLower || z < A->zLower)
+        return -1;
+    int cell = SFX(mesh_cell)(A, x, y, z);
+    if (cell < 0) return -1;
+    v3f pt = {(float)x, (float)y, (float)z};
+    LP id2 = interactDist * interactDist;
+    LP minDist = sizeof(LP) == 4 ? (LP)FLT_MAX : (LP)DBL_MAX;
+    int closest = -1;
+    for (int32_t i = A->starts[cell]; i < A->starts[cell] + A->sizes[cell]; ++i) {
+        int tri = A->values[i];
+        LP cur = SFX(tri_sdf2)(pt, SFX(mesh_vtx)(m, 3 * (int64_t)tri), SFX(mesh_vtx)(m, 3 * (int64_t)tri + 1),
+                               SFX(mesh_vtx)(m, 3 * (int64_t)tri + 2));
+        if (id2 > cur && cur < minDist) {
+            minDist = cur;
+            closest = tri;
+        }
+    }
+    *dist2 = minDist;
+    return closest;
+}
+
 static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hidem_link_soa *l,
                     int64_t L, int64_t start_step, int32_t nsteps, void *force_out[6],
                     int64_t *ev_link, int64_t *ev_step, int64_t ev_cap, int64_t *ev_count,
@@ -508,6 +662,18 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
     int64_t nev = 0, nregen = 0;
     const int useFixed = P->useFixed, useFront = P->useFrontPressure, useBed = P->useBed;
     const int useVel = P->useVelocityLimit, useBnd = P->useBoundary;
+    /* collision mesh: MeshAccel grid, face force sums (of this run, in particle order) and
+     * the per-particle contribution of the current step */
+    SFX(mesh_accel) macc;
+    memset(&macc, 0, sizeof macc);
+    int32_t *mtri = NULL;
+    LP *mcol = NULL, *mface = NULL;
+    if (g_mesh_set) {
+        SFX(mesh_build)(&g_mesh, &macc);
+        mtri = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+        mcol = (LP *)malloc(sizeof(LP) * 3 * (size_t)n);
+        mface = (LP *)calloc(3 * (size_t)g_mesh.triangles, sizeof(LP));
+    }
     struct timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
 
@@ -583,6 +749,7 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; ++i) {
             uint8_t ty = type ? type[i] : 0;
+            if (mtri) mtri[i] = -1;
             if (useFixed && (ty & HIDEM_TYPE_FIXED)) {
                 for (int c = 0; c < 6; ++c) df[c][i] = 0;
                 continue;
@@ -615,6 +782,30 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
             if (useBed && zCord + (double)radius < (double)bedHeight)
                 zForce = (LP)((double)zForce +
                               (double)d.bedStiffness * ((double)bedHeight - (zCord + (double)radius)));
+            /* collision mesh (HiDEM/MeshConstrainedDem/MainMeshDem.cpp:220-235) */
+            if (g_mesh_set) {
+                LP dist2 = 0;
+                int tri = SFX(mesh_closest)(&g_mesh, &macc, (LP)xCord, (LP)yCord, (LP)zCord,
+                                            d.bedInteract + radius, &dist2);
+                mtri[i] = tri;
+                if (tri >= 0) {
+                    const LP *nx = (const LP *)g_mesh.x_normal, *ny = (const LP *)g_mesh.y_normal;
+                    const LP *nz = (const LP *)g_mesh.z_normal;
+                    float maxDist = (float)(d.bedInteract + radius);
+                    LP dist = LSQRT(dist2);
+                    LP mForce = (LP)g_mesh.mesh_force, mDrag = (LP)g_mesh.mesh_drag;
+                    dragCoeff = mDrag * ((LP)maxDist - dist);
+                    LP fx = -nx[tri] * ((LP)maxDist - dist) * mForce;
+                    LP fy = -ny[tri] * ((LP)maxDist - dist) * mForce;
+                    LP fz = -nz[tri] * ((LP)maxDist - dist) * mForce;
+                    mcol[3 * i] = fx;
+                    mcol[3 * i + 1] = fy;
+                    mcol[3 * i + 2] = fz;
+                    xForce = xForce + fx;
+                    yForce = yForce + fy;
+                    zForce = zForce + fz;
+                }
+            }
             /* external force maps (MainDem.cpp:211-216) */
             if (g_map_set[2]) {
                 float fx = (float)xCord, fy = (float)yCord;
@@ -692,6 +883,16 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
             df[5][i] = zTheta - zThPrev;
         }
 
+        /* face forces (CollisionMesh::addForceToFace, CollisionMesh.h:46-52), summed here in
+         * particle order */
+        if (mtri) {
+            for (int64_t i = 0; i < n; ++i) {
+                int tri = mtri[i];
+                if (tri < 0) continue;
+                for (int k = 0; k < 3; ++k) mface[3 * (int64_t)tri + k] = mface[3 * (int64_t)tri + k] + mcol[3 * i + k];
+            }
+        }
+
         /* ---- linkUpdate gated as MainMeshBlock.cpp:312; per link
          *      CombinedAccel::iterateLinks (CombinedAccel.h:200-235) ---- */
         if ((LP)((LP)t * d.dt) > d.breakTime) {
@@ -726,6 +927,14 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
             LP *dst = (LP *)l->CT[k];
             for (int64_t s = 0; s < 2 * L; ++s) dst[s] = CT[s * 6 + k];
         }
+    }
+    if (g_mesh_set) {
+        free(g_mesh_face);
+        g_mesh_face = mface;
+        g_mesh_face_lp = (int)sizeof(LP);
+        SFX(mesh_free)(&macc);
+        free(mtri);
+        free(mcol);
     }
     SFX(adj_free)(&adj);
     free(ncount);

@@ -89,6 +89,42 @@ class CpuPath:
         f(C.byref(bed) if bed is not None else None, C.byref(friction) if friction is not None else None,
           extarr)
 
+    def set_mesh(self, mesh=None) -> None:
+        """Collision mesh (an abi.mesh struct) of the next runs; the caller keeps its arrays
+        alive."""
+        f = getattr(self.lib, self.prefix + "_set_mesh")
+        f.argtypes = [_P(abi.HidemMesh)]
+        f.restype = None
+        with _quiet_stdout():
+            f(C.byref(mesh) if mesh is not None else None)
+        self._mesh_tris = int(mesh.triangles) if mesh is not None else 0
+
+    def mesh_face_forces(self, precision: int) -> np.ndarray:
+        """[triangles][3] face forces of the last run with a mesh."""
+        lp = abi.lp_dtype(precision)
+        out = [np.zeros(self._mesh_tris, lp) for _ in range(3)]
+        f = getattr(self.lib, self.prefix + "_mesh_face_forces")
+        f.argtypes = [C.c_void_p] * 3
+        f.restype = C.c_int
+        rc = f(*[a.ctypes.data for a in out])
+        if rc != 0:
+            raise RuntimeError(f"{self.prefix}_mesh_face_forces failed ({rc})")
+        return np.stack(out, axis=1)
+
+    def mesh_accel(self, precision: int) -> dict:
+        """The MeshAccel grid of the set mesh (the contract of hidem_get_mesh_accel)."""
+        from hidem_b200.hidemlib import _mesh_accel
+        f = getattr(self.lib, self.prefix + "_mesh_accel")
+        port = self.prefix == "hidem_oracle"  # the port builds the grid in either precision
+        f.argtypes = ([C.c_int32] if port else []) + [C.c_void_p] * 6 + [_i64, _P(_i64)]
+        f.restype = C.c_int
+
+        def call(*a):
+            rc = f(precision, *a) if port else f(*a)
+            if rc != 0:
+                raise RuntimeError(f"{self.prefix}_mesh_accel failed ({rc})")
+        return _mesh_accel(call)
+
     def _prec(self, params) -> int:
         p = int(params.precision)
         if self.fixed_precision is not None and p != self.fixed_precision:

@@ -41,6 +41,8 @@
 #include "Accel/CombinedAccel.h"
 #include "Geometry/Map.h"
 #include "Geometry/Map2d.h"
+#include "Geometry/MeshAccel.h"
+#include <AtomicOps.h>
 #include "Generators/LinkGenerator.h"
 #include "HiDEMParticleData.h"
 #include "HiDEMLinkData.h"
@@ -51,6 +53,13 @@
 
 // maps of the next sessions (slot 0 bed height, 1 bed friction, 2..7 external forces)
 static Map2d<lpReal_t> *g_maps[8] = {};
+
+// collision mesh of the next sessions: the reference's MeshAccel over copies of the
+// vertex / normal arrays (the MeshData layout, PLiB/MeshData.h:21-35), the sample main's
+// meshForce / meshDrag, and the face force sums (CollisionMesh xFaceForce..zFaceForce)
+static MeshAccel *g_accel = nullptr;
+static std::vector<lpReal_t> g_mv[3], g_mn[3], g_face[3];
+static lpReal_t g_meshForce = 0, g_meshDrag = 0;
 
 using PData = ParticleDataHandler<HiDEMParticleData>;
 using LData = LinkDataHandler<HiDEMLinkData>;
@@ -393,6 +402,26 @@ struct RefSession {
             if (zCord <= dd.waterLevel) zForce += dd.lift * particleMass;
             if (useBed && zCord + radius < bedzCord)
                 zForce += dd.bedStiffness * (bedzCord - (zCord + radius));
+            // collision mesh: Mesh::closestTriFun (PLiB/Geometry/Mesh.h:69-83) with the
+            // sample's lambda (HiDEM/MeshConstrainedDem/MainMeshDem.cpp:220-235)
+            if (g_accel) {
+                auto [tri, dist, searched] = g_accel->getClosestTriAccel(
+                    xCord, yCord, zCord, dd.bedInteract + radius, g_mv[0].data(), g_mv[1].data(), g_mv[2].data());
+                if (tri >= 0) {
+                    float maxDist = dd.bedInteract + radius;
+                    dist = sqrt(dist);
+                    dragCoeff = g_meshDrag * ((maxDist - dist));
+                    lpReal_t xForceCol = -g_mn[0][tri] * (maxDist - dist) * g_meshForce;
+                    lpReal_t yForceCol = -g_mn[1][tri] * (maxDist - dist) * g_meshForce;
+                    lpReal_t zForceCol = -g_mn[2][tri] * (maxDist - dist) * g_meshForce;
+                    Atomic::atomicAddVal(g_face[0][tri], xForceCol);
+                    Atomic::atomicAddVal(g_face[1][tri], yForceCol);
+                    Atomic::atomicAddVal(g_face[2][tri], zForceCol);
+                    xForce += xForceCol;
+                    yForce += yForceCol;
+                    zForce += zForceCol;
+                }
+            }
             if (g_maps[2]) {
                 xForce += g_maps[2]->interp(xCord, yCord);
                 yForce += g_maps[3]->interp(xCord, yCord);
@@ -566,6 +595,66 @@ void hidem_ref_set_maps(const hidem_map2d *bed, const hidem_map2d *friction, con
     if (friction) g_maps[1] = make(friction);
     if (ext)
         for (int k = 0; k < 6; ++k) g_maps[2 + k] = make(&ext[k]);
+}
+
+// Collision mesh of the next sessions (NULL: none): the reference's MeshAccel built by
+// its own generateAccel as CollisionMesh::generateAccel calls it (CollisionMesh.h:31-38:
+// cell size and search distance both the given size). Face forces start at zero.
+void hidem_ref_set_mesh(const hidem_mesh *m) {
+    delete g_accel;
+    g_accel = nullptr;
+    for (int k = 0; k < 3; ++k) {
+        g_mv[k].clear();
+        g_mn[k].clear();
+        g_face[k].clear();
+    }
+    if (!m || m->triangles < 1) return;
+    const void *v[3] = {m->x_vertex, m->y_vertex, m->z_vertex};
+    const void *nrm[3] = {m->x_normal, m->y_normal, m->z_normal};
+    for (int k = 0; k < 3; ++k) {
+        const lpReal_t *src = static_cast<const lpReal_t *>(v[k]);
+        g_mv[k].assign(src, src + 3 * (size_t)m->triangles);
+        const lpReal_t *ns = static_cast<const lpReal_t *>(nrm[k]);
+        g_mn[k].assign(ns, ns + (size_t)m->triangles);
+        g_face[k].assign((size_t)m->triangles, lpReal_t(0));
+    }
+    g_meshForce = (lpReal_t)m->mesh_force;
+    g_meshDrag = (lpReal_t)m->mesh_drag;
+    g_accel = new MeshAccel();
+    const lpReal_t cs = (lpReal_t)m->cell_size;
+    g_accel->generateAccel(std::max(cs, cs), std::max(cs, cs), g_mv[0].data(), g_mv[1].data(), g_mv[2].data(),
+                           m->triangles);
+}
+
+int hidem_ref_mesh_face_forces(void *x, void *y, void *z) {
+    if (!g_accel) return HIDEM_ERR_STATE;
+    void *out[3] = {x, y, z};
+    for (int k = 0; k < 3; ++k)
+        if (out[k]) std::memcpy(out[k], g_face[k].data(), sizeof(lpReal_t) * g_face[k].size());
+    return 0;
+}
+
+int hidem_ref_mesh_accel(int32_t counts[3], double lower[3], double upper[3], int32_t *sizes,
+                         int32_t *starts, int32_t *values, int64_t values_cap, int64_t *values_count) {
+    if (!g_accel) return HIDEM_ERR_STATE;
+    MeshAccel &a = *g_accel;
+    const int c[3] = {a.xCount, a.yCount, a.zCount};
+    const double lo[3] = {a.xLower, a.yLower, a.zLower}, hi[3] = {a.xUpper, a.yUpper, a.zUpper};
+    for (int k = 0; k < 3; ++k) {
+        if (counts) counts[k] = c[k];
+        if (lower) lower[k] = lo[k];
+        if (upper) upper[k] = hi[k];
+    }
+    const size_t cells = (size_t)a.xCount * a.yCount * a.zCount;
+    for (size_t i = 0; i < cells; ++i) {
+        if (sizes) sizes[i] = a.sizes[i];
+        if (starts) starts[i] = a.starts[i];
+    }
+    const int64_t nv = (int64_t)a.values.size();
+    if (values)
+        for (int64_t i = 0; i < nv && i < values_cap; ++i) values[i] = a.values[i];
+    if (values_count) *values_count = nv;
+    return 0;
 }
 
 // One-shot form: setup, nsteps of the loop, write-back (particles in place; links: state

@@ -77,3 +77,25 @@ def maps_case(precision):
         ext.append(m)
         keep.append(a)
     return P, p, l, (bed, fric, ext), keep
+
+
+def mesh_case(precision, cell_size=2.0):
+    """A 4^3-cell block in a container mesh (bed with a slope and a bump just under the
+    lowest particles, walls 0.3 m from the block's x and y faces), plus one degenerate
+    triangle (its three vertices equal); returns (params, particles, links, mesh struct,
+    arrays to keep alive)."""
+    from hidem_b200 import abi, workloads
+    P, p, l = workloads.ice_block(cells=(4, 4, 4), precision=precision, seed=23, fixed_bottom=False,
+                                  bedInteract=0.4, waterLevel=2.0)
+    lo = (float(p["xCord"].min()) - 0.8, float(p["yCord"].min()) - 0.8)
+    hi = (float(p["xCord"].max()) + 0.8, float(p["yCord"].max()) + 0.8, float(p["zCord"].max()) + 2.0)
+    z0 = float(p["zCord"].min()) - 0.7
+
+    def bed(x, y):
+        return z0 + 0.05 * (x - lo[0]) + 0.2 * np.exp(-((x - 3.0) ** 2 + (y - 2.5) ** 2))
+
+    v, nrm = workloads.container_mesh(lo, hi, bed, nx=6, ny=5)
+    v = np.concatenate([v, np.full((1, 3, 3), 2.0)])
+    nrm = np.concatenate([nrm, [[0.0, 0.0, -1.0]]])
+    m, keep = abi.mesh(v, nrm, cell_size, precision, mesh_force=2e6, mesh_drag=500.0)
+    return P, p, l, m, keep

@@ -200,6 +200,52 @@ def test_gpu_bed_and_force_maps_match_oracle(gpu, precision, kernel):
 
 
 @pytest.mark.parametrize("precision", PRECS)
+@pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD_CAPPED,
+                                    abi.STEP_KERNEL_THREAD_ASYNC])
+def test_gpu_collision_mesh_matches_oracle(gpu, precision, kernel):
+    """The device MeshAccel grid equals the oracle's (itself pinned to the reference's
+    generateAccel); 40 steps with the closest-triangle force are bit-exact through the
+    fused and the split call paths; face forces (atomic sums) agree to rounding, and
+    zeroing them works."""
+    from conftest import mesh_case
+    P, p, l, m, keep = mesh_case(precision)
+    port = oracle.port()
+    port.set_mesh(m)
+    try:
+        grid = port.mesh_accel(precision)
+        ref = port.run(P, p, l, 40)
+        ref_face = port.mesh_face_forces(precision).astype(np.float64)
+    finally:
+        port.set_mesh()
+    tol = (1e-5 if precision == abi.PREC_MIXED else 1e-12) * float(np.abs(ref_face).max())
+    for mode in ("fused", "split"):
+        lib = HiDEMLib(P)
+        lib.set_step_kernel(kernel)
+        lib.set_collision_mesh(m)
+        g = lib.mesh_accel()
+        for k in ("counts", "lower", "upper", "sizes", "starts", "values"):
+            assert np.array_equal(g[k], grid[k]), (mode, k)
+        lib.set_particles(p)
+        lib.set_links(l)
+        if mode == "fused":
+            lib.step(40)
+        else:
+            for _ in range(40):
+                lib.timestep_split()
+        out_p, out_l = lib.get_particles(), lib.get_links()
+        face = lib.mesh_face_forces().astype(np.float64)
+        lib.zero_mesh_face_forces()
+        assert not lib.mesh_face_forces().any()
+        lib.set_collision_mesh(None)
+        lib.close()
+        for k in P_OUT:
+            assert np.array_equal(out_p[k], ref[0][k]), (mode, k)
+        for k in L_OUT:
+            assert np.array_equal(out_l[k], ref[1][k]), (mode, k)
+        assert np.abs(face - ref_face).max() <= tol, mode
+
+
+@pytest.mark.parametrize("precision", PRECS)
 def test_gpu_config0_1000_steps_bit_exact(gpu, precision):
     """The CPU-runnable configuration: 20^3 FCC cells (32,000 spheres), 1000 steps."""
     P, p, l = workloads.ice_block(cells=(20, 20, 20), precision=precision, seed=1)

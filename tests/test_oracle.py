@@ -112,6 +112,42 @@ def test_oracle_bed_and_force_maps_match_reference(precision):
 
 
 @pytest.mark.parametrize("precision", [abi.PREC_MIXED, abi.PREC_FP64])
+def test_oracle_collision_mesh_matches_reference(precision):
+    """Collision mesh of the MeshConstrainedDem sample: the restatement's MeshAccel grid
+    (bounds, counts, per-cell triangle lists) equals the reference's own generateAccel;
+    trajectories with the closest-triangle force are bit-exact; face forces (atomic sums in
+    the reference) agree to rounding."""
+    from conftest import mesh_case
+    P, p, l, m, keep = mesh_case(precision)
+    port = oracle.port()
+    ref = oracle.reference(precision)
+    port.set_mesh(m)
+    ref.set_mesh(m)
+    try:
+        ga, gb = port.mesh_accel(precision), ref.mesh_accel(precision)
+        for k in ("counts", "lower", "upper", "sizes", "starts", "values"):
+            assert np.array_equal(ga[k], gb[k]), k
+        assert ga["values"].shape[0] > 100 and np.all(np.diff(ga["values"][: ga["sizes"][0]]) > 0)
+        a = port.run(P, p, l, 40)
+        b = ref.run(P, p, l, 40)
+        fa, fb = port.mesh_face_forces(precision), ref.mesh_face_forces(precision)
+    finally:
+        port.set_mesh()
+        ref.set_mesh()
+    for k in P_OUT:
+        assert np.array_equal(a[0][k], b[0][k]), k
+    for k in L_OUT:
+        assert np.array_equal(a[1][k], b[1][k]), k
+    assert np.array_equal(a[2], b[2])
+    tol = (1e-5 if precision == abi.PREC_MIXED else 1e-12) * float(np.abs(fb).max())
+    assert (np.abs(fb).sum(axis=1) > 0).sum() >= 10
+    assert np.abs(fa.astype(np.float64) - fb).max() <= tol
+    # the mesh mattered: the same run without it differs
+    c = port.run(P, p, l, 40)
+    assert not np.array_equal(a[0]["zCord"], c[0]["zCord"])
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_MIXED, abi.PREC_FP64])
 def test_oracle_contact_list_matches_reference_on_irregular_input(precision):
     rng = np.random.default_rng(5)
     n = 3000
