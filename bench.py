@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle", "topo"], default="slab")
+    ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle", "topo", "mesh"],
+                    default="slab")
     ap.add_argument("--topo", default="1200,200,150",
                     help="topo: slab size in metres on the Fourier-mode bed (the 50M configuration)")
     ap.add_argument("--train-tongues", type=int, default=256, help="settle: training geometries")
@@ -606,8 +607,117 @@ def main_topo(args):
     print(json.dumps(line))
 
 
+def main_mesh(args):
+    """The calving slab in a fjord-shaped collision mesh (the MeshConstrainedDem setting):
+    particle-steps/s of the fused step with the closest-triangle query in its integrate,
+    the same slab without the mesh beside it, and the reference's CPU path with the same
+    mesh on a bounded sample."""
+    import torch
+    from hidem_b200 import abi, workloads
+    from hidem_b200.hidemlib import HiDEMLib
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    size = tuple(float(v) for v in args.slab.split(","))
+    P, p, l, md = workloads.slab_in_fjord(size=size, precision=prec)
+    mesh, keep = abi.mesh(md["vertices"], md["normals"], md["cell_size"], prec, md["mesh_force"], md["mesh_drag"])
+    n, L = p["xCord"].shape[0], l["state"].shape[0]
+
+    def timed(with_mesh: bool):
+        lib = HiDEMLib(P, device=local)
+        lib.set_step_kernel(KERNELS[args.kernel])
+        if with_mesh:
+            lib.set_collision_mesh(mesh)
+        lib.set_particles(p)
+        lib.set_links(l)
+        warm = max(args.warmup, 15) if args.kernel == "auto" else args.warmup
+        lib.step(warm)
+        lib.synchronize()
+        st0 = lib.stats()
+        stream = torch.cuda.ExternalStream(lib.stream_handle)
+        clocks = ClockSampler(local)
+        clocks.start()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        lib.profile(True)
+        e0.record(stream)
+        lib.step(args.steps)
+        e1.record(stream)
+        lib.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        kern_ms, kern_n = lib.profile_read()
+        lib.profile(False)
+        clk = clocks.stop()
+        st1 = lib.stats()
+        out = {"ms": ms, "kernel_ms": kern_ms / max(kern_n, 1), "kernel": lib.step_kernel(),
+               "launches": int(st1["kernel_launches"] - st0["kernel_launches"]),
+               "rebuilds": int(st1["regen_count"] - st0["regen_count"]) if "regen_count" in st1 else None,
+               "pairs": st1["num_neighbour_pairs"], "clocks": clk, "warm": warm}
+        if with_mesh:
+            g = lib.mesh_accel()
+            face = lib.mesh_face_forces()
+            nonempty = g["sizes"][g["sizes"] > 0]
+            out["grid"] = {"cells": int(g["sizes"].shape[0]), "counts": g["counts"].tolist(),
+                           "nonempty_cells": int(nonempty.shape[0]),
+                           "mean_triangles_per_nonempty_cell": float(nonempty.mean()) if nonempty.size else 0.0,
+                           "faces_pushed": int((np.abs(face).sum(axis=1) > 0).sum())}
+        lib.close()
+        return out
+
+    with_mesh = timed(True)
+    plain = timed(False)
+    value = n * args.steps / (with_mesh["ms"] / 1e3)
+    bytes_step = workloads.algorithmic_bytes(n, L, with_mesh["pairs"], prec)["total"]
+    peak, peak_kind = measured_peak()
+    achieved = bytes_step / (with_mesh["kernel_ms"] / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import oracle
+            if not oracle.reference_available(prec, fast=True):
+                raise RuntimeError("oracle/_ref not built")
+            ref = oracle.reference(prec, fast=True)
+            ref.set_mesh(mesh)
+            cpu = cpu_baseline(P, p, l, n)
+            ref.set_mesh(None)
+            cpu["sample"] += ", with the same collision mesh (the reference's MeshAccel)"
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
+                   "sample": f"failed: {ex}"}
+    line = {
+        "metric": "particle-steps/s (slab in a collision mesh)", "value": value, "unit": "particle-steps/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": with_mesh["warm"],
+        "ms_per_step": with_mesh["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
+        "config": {"workload": f"calving slab {size[0]:g}x{size[1]:g}x{size[2]:g} m in a fjord mesh "
+                               f"(bed of {md['vertices'].shape[0] - 6} triangles, 3 walls, open front), "
+                               f"MeshAccel cells {md['cell_size']:g} m",
+                   "particles": n, "links": L, "triangles": int(md["vertices"].shape[0]),
+                   "precision": args.precision, "parallelism": "replicas x1",
+                   "l2": "inputs larger than L2 (records + link ends > 126 MB)"},
+        "mesh_grid": with_mesh["grid"],
+        "without_mesh": {"value": n * args.steps / (plain["ms"] / 1e3), "ms_per_step": plain["ms"] / args.steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "kernel": "fused step with the mesh query, " + KERNEL_NAMES.get(with_mesh["kernel"], "?") + " kernel",
+                     "kernel_ms": with_mesh["kernel_ms"], "algorithmic_bytes_per_launch": bytes_step},
+        "cpu_baseline": cpu, "gpu_launches": with_mesh["launches"], "rebuilds_in_timed_steps": with_mesh["rebuilds"],
+        "clocks": with_mesh["clocks"],
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.workload == "mesh":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the mesh workload reports the reference CPU path in its own line (cpu_baseline)"}))
+        else:
+            main_mesh(args)
+        return
     if args.workload == "topo":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable":

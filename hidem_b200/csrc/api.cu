@@ -129,7 +129,11 @@ struct hidem_ctx {
     // collision mesh: vertices (x, y, z), normals, face forces, MeshAccel cell lists
     void *meshVtx[3] = {}, *meshNrm[3] = {}, *meshFace[3] = {};
     int *meshSizes = nullptr, *meshStarts = nullptr, *meshValues = nullptr;
-    long long meshCells = 0, meshValueCount = 0;
+    int *meshQSizes = nullptr, *meshQStarts = nullptr, *meshQValues = nullptr;  // query lists
+    uint8_t *meshKeep = nullptr;  // triangles the query lists always keep
+    long long meshCells = 0, meshValueCount = 0, meshQValueCount = 0;
+    double meshCellSize = 0;
+    double maxParticleRadius = 0;  // over the particles last set
     int meshTris = 0;
     bool meshSet = false;
     MeshView<float> meshF{};
@@ -1181,6 +1185,11 @@ int ctx_precision(const hidem_ctx *ctx) { return ctx->P.precision; }
 
 // =================================================================== C ABI
 
+namespace {
+// the collision mesh's query lists for the current particles and parameters
+hidem_status prune_mesh(hidem_ctx *ctx);
+}  // namespace
+
 extern "C" {
 
 int hidem_abi_version(void) { return HIDEM_B200_ABI_VERSION; }
@@ -1327,6 +1336,10 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->meshSizes);
     dfree(ctx->meshStarts);
     dfree(ctx->meshValues);
+    dfree(ctx->meshQSizes);
+    dfree(ctx->meshQStarts);
+    dfree(ctx->meshQValues);
+    dfree(ctx->meshKeep);
     dfree(ctx->energyBuf);
     for (cudaEvent_t e : ctx->tuneEv)
         if (e) cudaEventDestroy(e);
@@ -1340,7 +1353,8 @@ hidem_status hidem_set_params(hidem_ctx *ctx, const hidem_params *params) {
     if (!ctx) return HIDEM_ERR_ARG;
     if (params && params->precision != ctx->P.precision)
         return fail(ctx, HIDEM_ERR_ARG, "precision cannot change after creation");
-    return apply_params(ctx, params);
+    TRY(apply_params(ctx, params));
+    return prune_mesh(ctx);
 }
 
 hidem_status hidem_set_timestep(hidem_ctx *ctx, int64_t step) {
@@ -1398,6 +1412,15 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     ctx->n = n;
     ctx->haveParticles = true;
     ctx->built = false;
+    {
+        double r = 0;
+        if (ctx->mixed)
+            for (int64_t i = 0; i < n; ++i) r = std::max(r, (double)static_cast<const float *>(p->radius)[i]);
+        else
+            for (int64_t i = 0; i < n; ++i) r = std::max(r, static_cast<const double *>(p->radius)[i]);
+        ctx->maxParticleRadius = r;
+    }
+    TRY(prune_mesh(ctx));
     ctx->startStep = ctx->step;
     // a link set refers to particle indices of the previous particle set
     ctx->haveLinks = false;
@@ -1954,8 +1977,14 @@ void free_mesh(hidem_ctx *ctx) {
     dfree(ctx->meshSizes);
     dfree(ctx->meshStarts);
     dfree(ctx->meshValues);
+    dfree(ctx->meshQSizes);
+    dfree(ctx->meshQStarts);
+    dfree(ctx->meshQValues);
+    dfree(ctx->meshKeep);
     ctx->meshSizes = ctx->meshStarts = ctx->meshValues = nullptr;
-    ctx->meshCells = ctx->meshValueCount = 0;
+    ctx->meshQSizes = ctx->meshQStarts = ctx->meshQValues = nullptr;
+    ctx->meshKeep = nullptr;
+    ctx->meshCells = ctx->meshValueCount = ctx->meshQValueCount = 0;
     ctx->meshTris = 0;
     ctx->meshSet = false;
     ctx->meshF = MeshView<float>{};
@@ -2011,6 +2040,28 @@ hidem_status build_mesh(hidem_ctx *ctx, const hidem_mesh *mesh, MeshView<LP> &m)
     const LP maxDist = (cs * cs) + (cs * cs) + (cs * cs) + cs;
     const long long cells = (long long)m.xCount * m.yCount * m.zCount;
     ctx->meshCells = cells;
+    ctx->meshCellSize = (double)cs;
+    // triangles whose float normal is ill-conditioned (area small against the edges, or
+    // not finite): their float distances need not follow the geometry, so the query lists
+    // keep them in every cell that lists them
+    {
+        std::vector<uint8_t> keep((size_t)T);
+        for (int t = 0; t < T; ++t) {
+            const float ax = (float)vx[3 * t], ay = (float)vy[3 * t], az = (float)vz[3 * t];
+            const float bx = (float)vx[3 * t + 1], by = (float)vy[3 * t + 1], bz = (float)vz[3 * t + 1];
+            const float cx = (float)vx[3 * t + 2], cy = (float)vy[3 * t + 2], cz = (float)vz[3 * t + 2];
+            const float bax = bx - ax, bay = by - ay, baz = bz - az;
+            const float acx = ax - cx, acy = ay - cy, acz = az - cz;
+            const float cbx = cx - bx, cby = cy - by, cbz = cz - bz;
+            const float nx = bay * acz - baz * acy, ny = baz * acx - bax * acz, nz = bax * acy - bay * acx;
+            const float n2 = nx * nx + ny * ny + nz * nz;
+            const float e = std::max(std::max(bax * bax + bay * bay + baz * baz, acx * acx + acy * acy + acz * acz),
+                                     cbx * cbx + cby * cby + cbz * cbz);
+            keep[t] = (n2 > 1e-6f * e * e && std::isfinite(n2)) ? 0 : 1;
+        }
+        CK(cudaMalloc(&ctx->meshKeep, (size_t)T));
+        CK(cudaMemcpy(ctx->meshKeep, keep.data(), (size_t)T, cudaMemcpyHostToDevice));
+    }
     ctx->meshTris = T;
     const size_t vb = sizeof(LP) * 3 * (size_t)T, nb = sizeof(LP) * (size_t)T;
     const void *vsrc[3] = {mesh->x_vertex, mesh->y_vertex, mesh->z_vertex};
@@ -2058,6 +2109,52 @@ hidem_status build_mesh(hidem_ctx *ctx, const hidem_mesh *mesh, MeshView<LP> &m)
     return HIDEM_OK;
 }
 
+// The query lists for the current particles and parameters: the reach of the largest
+// interaction distance bedInteract + radius (lp, as the integrate step forms it), with a
+// relative and an absolute allowance for the float rounding of the distance tests.
+template <class LP>
+hidem_status prune_mesh_t(hidem_ctx *ctx, MeshView<LP> &m, const Consts<LP> &c) {
+    dfree(ctx->meshQSizes);
+    dfree(ctx->meshQStarts);
+    dfree(ctx->meshQValues);
+    ctx->meshQSizes = ctx->meshQStarts = ctx->meshQValues = nullptr;
+    const LP rmax = (LP)std::max(ctx->maxParticleRadius, ctx->P.maxRadius);
+    const LP id = c.bedInteract + rmax;
+    const double reach = (double)id * (1.0 + 1e-4) + 1e-3;
+    const double cs = ctx->meshCellSize;
+    const double margin = 1e-4 * cs + 1e-3;
+    const long long cells = ctx->meshCells;
+    const long long sumsLen = cells / 1024 + 2;
+    int *scratch = nullptr;
+    CK(cudaMalloc(&ctx->meshQSizes, sizeof(int) * cells));
+    CK(cudaMalloc(&ctx->meshQStarts, sizeof(int) * cells));
+    CK(cudaMalloc(&scratch, sizeof(int) * (sumsLen + 1)));
+    launch_mesh_prune<LP>(m, cs, margin, reach, ctx->meshKeep, ctx->meshQSizes, nullptr, nullptr, false, ctx->stream);
+    launch_scan<int, int>(ctx->meshQSizes, cells, 1, ctx->meshQStarts, scratch, scratch + sumsLen, ctx->stream);
+    int total = 0;
+    cudaError_t e = cudaMemcpyAsync(&total, scratch + sumsLen, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(scratch);
+    CK(e);
+    ctx->meshQValueCount = total;
+    CK(cudaMalloc(&ctx->meshQValues, sizeof(int) * (size_t)std::max(total, 1)));
+    launch_mesh_prune<LP>(m, cs, margin, reach, ctx->meshKeep, ctx->meshQSizes, ctx->meshQStarts, ctx->meshQValues,
+                          true, ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    m.qStarts = ctx->meshQStarts;
+    m.qSizes = ctx->meshQSizes;
+    m.qValues = ctx->meshQValues;
+    return HIDEM_OK;
+}
+
+hidem_status prune_mesh(hidem_ctx *ctx) {
+    if (!ctx->meshSet) return HIDEM_OK;
+    TRY(ctx->mixed ? prune_mesh_t<float>(ctx, ctx->meshF, ctx->cf) : prune_mesh_t<double>(ctx, ctx->meshD, ctx->cd));
+    attach_maps(ctx);
+    return HIDEM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2081,7 +2178,12 @@ hidem_status hidem_set_collision_mesh(hidem_ctx *ctx, const hidem_mesh *mesh) {
         return st;
     }
     ctx->meshSet = true;
-    attach_maps(ctx);
+    st = prune_mesh(ctx);
+    if (st != HIDEM_OK) {
+        free_mesh(ctx);
+        attach_maps(ctx);
+        return st;
+    }
     return HIDEM_OK;
 }
 

@@ -66,7 +66,9 @@ template <class LP>
 struct MeshView {
     const LP *vx, *vy, *vz;        // vertex j of triangle t at 3t + j
     const LP *nx, *ny, *nz;        // per triangle
-    const int *starts, *sizes, *values;
+    const int *starts, *sizes, *values;  // the reference's per-cell lists
+    const int *qStarts, *qSizes, *qValues;  // the same lists without the triangles that
+                                            // no particle of the cell can reach
     LP *fx, *fy, *fz;              // face forces, accumulated
     LP xLower, yLower, zLower, xUpper, yUpper, zUpper;
     LP xInv, yInv, zInv;           // 1 / cell size, as MeshAccel stores them

@@ -168,6 +168,13 @@ void launch_energy(const Consts<LP> &c, const PRec<LP> *rec, int n, double *part
 template <class LP>
 void launch_mesh_cells(const MeshView<LP> &m, int ntri, LP cellSize, LP maxDist, int *sizes,
                        const int *starts, int *values, bool fill, cudaStream_t s);
+// The query lists of a collision mesh (m's reference lists set): per cell, the
+// triangles that may lie within `reach` of the cell's box grown by `margin`, plus those
+// flagged in keep; count pass (fill false) into qSizes, fill pass into qValues at qStarts
+template <class LP>
+void launch_mesh_prune(const MeshView<LP> &m, double cellSize, double margin, double reach,
+                       const uint8_t *keep, int *qSizes, const int *qStarts, int *qValues, bool fill,
+                       cudaStream_t s);
 template <class LP>
 void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb, cudaStream_t s);
 

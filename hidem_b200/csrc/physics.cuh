@@ -272,7 +272,10 @@ __device__ __forceinline__ int mesh_cell(const MeshView<LP> &m, LP x, LP y, LP z
 
 // MeshAccel::getClosestTriAccel (MeshAccel.h:375-412): the closest triangle of the
 // point's cell within interactDist (the first of equals), or -1; *dist2 its squared
-// distance.
+// distance. The cell's list is the reference's with the triangles removed that lie
+// farther from every point of the cell than any particle's interaction distance
+// (k_mesh_prune): those never pass the distance test, so the closest triangle and its
+// distance are the same, found with fewer distance evaluations.
 template <class LP>
 __device__ __forceinline__ int mesh_closest(const MeshView<LP> &m, LP x, LP y, LP z, LP interactDist,
                                             LP *dist2) {
@@ -280,13 +283,14 @@ __device__ __forceinline__ int mesh_closest(const MeshView<LP> &m, LP x, LP y, L
         return -1;
     const int cell = mesh_cell(m, x, y, z);
     if (cell < 0) return -1;
-    const int start = m.starts[cell], size = m.sizes[cell];
+    const int start = m.qStarts[cell], size = m.qSizes[cell];
+    if (size == 0) return -1;
     const V3f p{(float)x, (float)y, (float)z};
     const LP id2 = interactDist * interactDist;
     LP minDist = sizeof(LP) == 4 ? (LP)3.40282347e+38f : (LP)1.7976931348623157e+308;
     int closest = -1;
     for (int i = start; i < start + size; ++i) {
-        const int tri = m.values[i];
+        const int tri = m.qValues[i];
         const LP cur = tri_sdf2<LP>(p, mesh_vertex(m, 3 * tri), mesh_vertex(m, 3 * tri + 1),
                                     mesh_vertex(m, 3 * tri + 2));
         if (id2 > cur && cur < minDist) {

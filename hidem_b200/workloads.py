@@ -90,13 +90,14 @@ def ice_block(cells=(20, 20, 20), precision: int = abi.PREC_MIXED, seed: int = 1
     return params, p, links
 
 
-def container_mesh(lo, hi, bed, nx: int = 8, ny: int = 8, walls: bool = True):
+def container_mesh(lo, hi, bed, nx: int = 8, ny: int = 8, walls=True):
     """A collision mesh shaped as an open container, the form the MeshConstrainedDem
     sample's mesh takes: the bed z = bed(x, y) over [lo[0], hi[0]] x [lo[1], hi[1]] as a
     triangulated grid of nx x ny quads (two triangles each), and with `walls` four vertical
     walls up to hi[2]. Normals point out of the container (down through the bed, out
     through the walls), so the mesh force, along minus the normal, pushes the particles
-    inside back in. Returns (vertices [T][3][3], normals [T][3])."""
+    inside back in. `walls`: True (all four), False, or the sides to build out of
+    "x-", "x+", "y-", "y+". Returns (vertices [T][3][3], normals [T][3])."""
     xs = np.linspace(lo[0], hi[0], nx + 1)
     ys = np.linspace(lo[1], hi[1], ny + 1)
     tris = []
@@ -113,11 +114,16 @@ def container_mesh(lo, hi, bed, nx: int = 8, ny: int = 8, walls: bool = True):
     if walls:
         zb = min(bed(x, y) for x in (lo[0], hi[0]) for y in (lo[1], hi[1])) - 1.0
         zt = hi[2]
+        sides = {"x-", "x+", "y-", "y+"} if walls is True else set(walls)
         wall = []
-        for x, nx_ in ((lo[0], -1.0), (hi[0], 1.0)):
+        for x, nx_, side in ((lo[0], -1.0, "x-"), (hi[0], 1.0, "x+")):
+            if side not in sides:
+                continue
             a, b, c, d = (x, lo[1], zb), (x, hi[1], zb), (x, hi[1], zt), (x, lo[1], zt)
             wall += [((a, b, c), (nx_, 0.0, 0.0)), ((a, c, d), (nx_, 0.0, 0.0))]
-        for y, ny_ in ((lo[1], -1.0), (hi[1], 1.0)):
+        for y, ny_, side in ((lo[1], -1.0, "y-"), (hi[1], 1.0, "y+")):
+            if side not in sides:
+                continue
             a, b, c, d = (lo[0], y, zb), (hi[0], y, zb), (hi[0], y, zt), (lo[0], y, zt)
             wall += [((a, b, c), (0.0, ny_, 0.0)), ((a, c, d), (0.0, ny_, 0.0))]
         v = np.concatenate([v, np.array([w[0] for w in wall])])
@@ -145,6 +151,30 @@ def calving_slab(size=(400.0, 100.0, 100.0), precision: int = abi.PREC_MIXED, se
     params = block_params(precision, waterLevel=water_level, useBed=1, bedHeight=zmin + 0.5,
                           bedFriction=0.3, useFrontPressure=1, **param_over)
     return params, p, links
+
+
+def slab_in_fjord(size=(400.0, 100.0, 100.0), precision: int = abi.PREC_MIXED, quad: float = 4.0,
+                  mesh_force: float = 1e5, mesh_drag: float = 1000.0, **param_over):
+    """The calving slab in a fjord-shaped collision mesh, the MeshConstrainedDem setting: a
+    bed surface (gently sloping, quads of `quad` m, two triangles each) 0.55 m below the
+    bottom layer's centres and side walls 0.55 m from the x-min, y-min and y-max faces,
+    open at the calving front (x-max); bed interaction distance 0.25 m, MeshAccel cells of
+    16 maxRadius (the sample's choice). Returns (params, particles, links, mesh dict with
+    vertices, normals, cell_size, mesh_force, mesh_drag)."""
+    P, p, l = calving_slab(size=size, precision=precision, bedInteract=0.25, **param_over)
+    x, y, z = p["xCord"], p["yCord"], p["zCord"]
+    lo = (float(x.min()) - 0.55, float(y.min()) - 0.55)
+    hi = (float(x.max()) + 0.55, float(y.max()) + 0.55, float(z.max()) + 5.0)
+    z0 = float(z.min()) - 0.55
+
+    def bed(xx, yy):
+        return z0 - 0.002 * (xx - lo[0])
+
+    nx = max(1, int(round((hi[0] - lo[0]) / quad)))
+    ny = max(1, int(round((hi[1] - lo[1]) / quad)))
+    v, nrm = container_mesh(lo, hi, bed, nx, ny, walls=("x-", "y-", "y+"))
+    return P, p, l, {"vertices": v, "normals": nrm, "cell_size": 16.0 * float(P.maxRadius),
+                     "mesh_force": mesh_force, "mesh_drag": mesh_drag}
 
 
 def algorithmic_bytes(n: int, L: int, pairs: int, precision: int) -> dict:

@@ -99,3 +99,30 @@ def mesh_case(precision, cell_size=2.0):
     nrm = np.concatenate([nrm, [[0.0, 0.0, -1.0]]])
     m, keep = abi.mesh(v, nrm, cell_size, precision, mesh_force=2e6, mesh_drag=500.0)
     return P, p, l, m, keep
+
+
+def mesh_cloud_case(precision, seed=5):
+    """Unbonded particles on a jittered 1.1 m grid filling the lower part of a container
+    mesh with a bumpy bed, many of them near the interaction distance of the bed or a wall
+    and near the MeshAccel cell faces (cells of 1.7 m); returns (params, particles, empty
+    links, mesh struct, arrays to keep alive)."""
+    from hidem_b200 import abi, workloads
+    rng = np.random.default_rng(seed)
+    lo, hi = (0.0, 0.0), (14.0, 9.0, 8.0)
+
+    def bed(x, y):
+        return 0.4 * np.sin(0.7 * x) * np.cos(0.5 * y) + 0.05 * x
+
+    g = np.mgrid[0.6:13.5:1.1, 0.6:8.5:1.1, 0.0:3.3:1.1].reshape(3, -1).T
+    g = g + rng.uniform(-0.2, 0.2, g.shape)
+    g[:, 2] += bed(g[:, 0], g[:, 1]) + 0.35
+    n = g.shape[0]
+    p = abi.empty_particles(n, precision)
+    p["xCord"][:], p["yCord"][:], p["zCord"][:] = g[:, 0], g[:, 1], g[:, 2]
+    p["radius"][:] = 0.5
+    p["globalKeys"][:] = np.arange(n)
+    P = workloads.block_params(precision, bedInteract=0.15, waterLevel=1.0)
+    l = abi.empty_links(0, precision)
+    v, nrm = workloads.container_mesh(lo, hi, bed, nx=10, ny=7)
+    m, keep = abi.mesh(v, nrm, 1.7, precision, mesh_force=2e5, mesh_drag=300.0)
+    return P, p, l, m, keep

@@ -246,6 +246,33 @@ def test_gpu_collision_mesh_matches_oracle(gpu, precision, kernel):
 
 
 @pytest.mark.parametrize("precision", PRECS)
+@pytest.mark.parametrize("seed", [5, 6, 7])
+def test_gpu_collision_mesh_cloud_matches_oracle(gpu, precision, seed):
+    """Unbonded particles around a bumpy container mesh, many near the interaction
+    distance and near cell faces: the device's pruned per-cell query lists find the same
+    closest triangles as the oracle's full lists (bit-exact states after 3 steps)."""
+    from conftest import mesh_cloud_case
+    P, p, l, m, keep = mesh_cloud_case(precision, seed)
+    port = oracle.port()
+    port.set_mesh(m)
+    try:
+        ref = port.run(P, p, l, 3)
+    finally:
+        port.set_mesh()
+    lib = HiDEMLib(P)
+    lib.set_collision_mesh(m)
+    lib.set_particles(p)
+    lib.set_links(l)
+    lib.step(3)
+    out = lib.get_particles()
+    face = lib.mesh_face_forces()
+    lib.close()
+    assert (np.abs(face).sum(axis=1) > 0).sum() >= 20
+    for k in P_OUT:
+        assert np.array_equal(out[k], ref[0][k]), k
+
+
+@pytest.mark.parametrize("precision", PRECS)
 def test_gpu_config0_1000_steps_bit_exact(gpu, precision):
     """The CPU-runnable configuration: 20^3 FCC cells (32,000 spheres), 1000 steps."""
     P, p, l = workloads.ice_block(cells=(20, 20, 20), precision=precision, seed=1)

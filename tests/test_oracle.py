@@ -148,6 +148,24 @@ def test_oracle_collision_mesh_matches_reference(precision):
 
 
 @pytest.mark.parametrize("precision", [abi.PREC_MIXED, abi.PREC_FP64])
+def test_oracle_collision_mesh_cloud_matches_reference(precision):
+    from conftest import mesh_cloud_case
+    P, p, l, m, keep = mesh_cloud_case(precision)
+    port = oracle.port()
+    ref = oracle.reference(precision)
+    port.set_mesh(m)
+    ref.set_mesh(m)
+    try:
+        a = port.run(P, p, l, 3)
+        b = ref.run(P, p, l, 3)
+    finally:
+        port.set_mesh()
+        ref.set_mesh()
+    for k in P_OUT:
+        assert np.array_equal(a[0][k], b[0][k]), k
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_MIXED, abi.PREC_FP64])
 def test_oracle_contact_list_matches_reference_on_irregular_input(precision):
     rng = np.random.default_rng(5)
     n = 3000
