@@ -9,6 +9,7 @@
 // Errors throw hidem::Error (status + hidem_last_error text) instead of exit(1).
 #pragma once
 
+#include <cstdint>
 #include <stdexcept>
 #include <string>
 
@@ -60,8 +61,37 @@ public:
 
     void getParticles(hidem_particle_soa &out) { check(hidem_get_particles(ctx_, &out)); }
     void getLinks(hidem_link_soa &out) { check(hidem_get_links(ctx_, &out)); }
+    void getForces(void *force[6]) { check(hidem_get_forces(ctx_, force)); }
+    hidem_stats getStats() {
+        hidem_stats s;
+        check(hidem_get_stats(ctx_, &s));
+        return s;
+    }
     void synchronize() { check(hidem_synchronize(ctx_)); }
     hidem_ctx *handle() { return ctx_; }
+
+    // HiDEMH5Checkpoint write / restart (HiDEMLib/HiDEMH5Checkpoint.h:24-50)
+    void writeCheckpoint(const std::string &path) { check(hidem_checkpoint_write(ctx_, path.c_str())); }
+    void readCheckpoint(const std::string &path) { check(hidem_checkpoint_read(ctx_, path.c_str())); }
+
+    // GlacierDem bed / friction maps (InputBed) and ExternalForces maps; nullptr removes them
+    void setBedMaps(const hidem_map2d *bed, const hidem_map2d *friction) {
+        check(hidem_set_bed_maps(ctx_, bed, friction));
+    }
+    void setExternalForceMaps(const hidem_map2d maps[6]) { check(hidem_set_external_force_maps(ctx_, maps)); }
+
+    // CollisionMesh of the MeshConstrainedDem sample: generateAccel, face forces, zeroForce
+    void setCollisionMesh(const hidem_mesh *mesh) { check(hidem_set_collision_mesh(ctx_, mesh)); }
+    void getMeshFaceForces(void *x, void *y, void *z) { check(hidem_get_mesh_face_forces(ctx_, x, y, z)); }
+    void zeroMeshForces() { check(hidem_zero_mesh_face_forces(ctx_)); }
+
+    // kinetic energy of the current state (translational, rotational, largest speed)
+    void kineticEnergy(double &translational, double &rotational, double &maxSpeed) {
+        check(hidem_kinetic_energy(ctx_, &translational, &rotational, &maxSpeed));
+    }
+    // step kernel (HIDEM_STEP_KERNEL_*; AUTO times the candidates on the first steps)
+    void setStepKernel(int32_t kernel) { check(hidem_set_step_kernel(ctx_, kernel)); }
+    int32_t stepKernel() { return hidem_get_step_kernel(ctx_); }
 
 private:
     void check(hidem_status s) {

@@ -110,6 +110,11 @@ int main() {
     try {
         hidem::HiDEMLibB200 lib(p, 0);
         std::printf("created step=%lld\n", (long long)lib.getCurrentTimestep());
+        lib.setBedMaps(nullptr, nullptr);
+        lib.setCollisionMesh(nullptr);
+        lib.setStepKernel(HIDEM_STEP_KERNEL_AUTO);
+        double kt = 0, kr = 0, vm = 0;
+        if (lib.getStats().num_particles > 0) lib.kineticEnergy(kt, kr, vm);
     } catch (const hidem::Error &e) {
         std::printf("status=%d\n", (int)e.status);
     }
