@@ -267,6 +267,8 @@ _PROTOS = [
     ("hidem_batch_counts", C.c_int, [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64),
                                      C.POINTER(_i64)]),
     ("hidem_surrogate_config_default", None, [C.POINTER(HidemSurrogateConfig)]),
+    ("hidem_surrogate_predict_device", C.c_int, [C.c_void_p, C.c_void_p, _i64, C.c_void_p]),
+    ("hidem_surrogate_get_stream", C.c_void_p, [C.c_void_p]),
     ("hidem_surrogate_create", C.c_int, [C.POINTER(HidemSurrogateConfig), C.c_int,
                                          C.POINTER(C.c_void_p)]),
     ("hidem_surrogate_destroy", None, [C.c_void_p]),

@@ -312,6 +312,230 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     if (warp == 0) tm_dealloc(tmem, COLS);
 }
 
+// ------------------------------------------------------------------ fused forward pass
+
+constexpr int kMlpMaxLayers = 8;
+constexpr int kMlpStages = 3;
+constexpr int kOutCols = 3;
+constexpr int kMlpThreads = 512;  // 16 warps: 4 lane quarters x 4 column quarters
+
+// SiLU for the forward pass from the hardware tanh: z * (1 + tanh(z / 2)) / 2 (the result is
+// rounded to BF16, far coarser than the approximation)
+__device__ __forceinline__ float silu_fast(float z) {
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
+    return 0.5f * z * (1.0f + t);
+}
+
+struct MlpMaps {
+    CUtensorMap x;                  // features [rows][K0], boxes of 64 x 128
+    CUtensorMap w[kMlpMaxLayers];   // hidden weights [W][K_l], boxes of 64 x W
+};
+
+struct MlpArgs {
+    int layers, k0;                 // hidden layers, first layer's K
+    const float *bias[kMlpMaxLayers];
+    const float *wo, *bo;           // output layer [3][W], [3]
+    float *y;                       // [rows][3]
+    float *z[kMlpMaxLayers];        // pre-activations [rows][W] (null: not kept)
+    bf16 *h[kMlpMaxLayers];         // activations [rows][W] (null: not kept)
+    int *err;
+};
+
+template <int BN>
+constexpr size_t mlp_smem_bytes() {
+    return (size_t)kMlpStages * (128 * 128 + BN * 128) + (size_t)128 * BN * 2 + 1024 + 256;
+}
+
+// One CTA per 128-row block runs the whole network: features and weights stream through a
+// 3-stage TMA ring; each hidden layer's accumulator (128 x BN FP32) sits in tensor memory;
+// its epilogue (bias + SiLU, BF16) writes the activations back into shared memory in the
+// 128-byte-swizzled K-major layout TMA would have written, so they are the next layer's A
+// operand without a round trip through global memory (the pre-activations and activations
+// go to global memory only when the training pass keeps them). The 3-wide output layer
+// runs on the CUDA cores from the last activations: per row, a sequential FP32 sum over k.
+// Thread 0 issues the copies and the MMAs (and prefetches the next layer's weights while
+// the epilogue runs); the sixteen warps share the epilogues (warp w: accumulator lanes
+// 32 (w % 4) .. +31, i.e. those rows, and the column quarter w / 4).
+template <int BN>
+__global__ void __launch_bounds__(kMlpThreads, 1)
+    k_mlp_fwd(const __grid_constant__ MlpMaps maps, const MlpArgs g) {
+    constexpr int S = kMlpStages;
+    constexpr uint32_t ABYTES = 128 * 128, BBYTES = BN * 128, STAGE = ABYTES + BBYTES;
+    constexpr uint32_t ACT_BLOCK = 128 * 128;   // 128 rows x 64 BF16 columns
+    constexpr uint32_t COLS = BN;
+    extern __shared__ unsigned char dyn[];
+    unsigned char *sm =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
+    unsigned char *act = sm + S * STAGE;
+    uint64_t *full = reinterpret_cast<uint64_t *>(act + (size_t)128 * BN * 2);
+    uint64_t *empty = full + S;
+    uint64_t *done = empty + S;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(done + 1);
+    __shared__ int sFail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int L = g.layers;
+    const int nk0 = g.k0 / 64, nkw = BN / 64;
+    const int nload = nk0 + (L - 1) * nkw;
+
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mb_init(full + s, 1);
+            mb_init(empty + s, 1);
+        }
+        mb_init(done, 1);
+        sFail = 0;
+        mb_fence_init();
+    }
+    if (warp == 0) {
+        tm_alloc(slot, COLS);
+        tm_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    const int m0 = blockIdx.x * 128;
+
+    // load i of the stream: k-tile kt of layer l (layer 0: features and weights)
+    auto load = [&](int i) {
+        const int s = i % S;
+        unsigned char *a = sm + s * STAGE;
+        if (i < nk0) {
+            mb_expect_tx(full + s, STAGE);
+            tma_load_2d(a, &maps.x, i * 64, m0, full + s);
+            tma_load_2d(a + ABYTES, &maps.w[0], i * 64, 0, full + s);
+        } else {
+            const int l = 1 + (i - nk0) / nkw, kt = (i - nk0) % nkw;
+            mb_expect_tx(full + s, BBYTES);
+            tma_load_2d(a + ABYTES, &maps.w[l], kt * 64, 0, full + s);
+        }
+    };
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(128 >> 4) << 24);
+    // i: next k-tile to consume; issued: k-tiles loaded; freed: k-tiles whose ring slot
+    // has been handed to a later load (issued == freed + S until the stream is exhausted)
+    int issued = 0, i = 0, freed = 0;
+    if (tid == 0)
+        for (; issued < nload && issued < S; ++issued) load(issued);
+    // reload the slots of k-tiles up to j once their MMAs have completed
+    auto refill_upto = [&](int j) -> bool {
+        while (freed <= j && issued < nload) {
+            if (!mb_wait(empty + (freed % S), (uint32_t)((freed / S) & 1))) return false;
+            load(issued++);
+            ++freed;
+        }
+        return true;
+    };
+
+    const int quarter = warp & 3, row = quarter * 32 + lane;
+    const uint32_t tlane = (uint32_t)(quarter * 32) << 16;
+    for (int l = 0; l < L; ++l) {
+        const int nk = l == 0 ? nk0 : nkw;
+        if (tid == 0 && !sFail) {
+            for (int kt = 0; kt < nk; ++kt, ++i) {
+                const int s = i % S;
+                if (!mb_wait(full + s, (uint32_t)((i / S) & 1))) {
+                    sFail = 1;
+                    set_err(g.err, 1);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a0 = l == 0 ? su32(sm + s * STAGE) : su32(act + kt * ACT_BLOCK);
+                const uint32_t b0 = su32(sm + s * STAGE) + ABYTES;
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
+                    tc_mma(tmem, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), idesc,
+                           (kt > 0 || kk > 0) ? 1u : 0u);
+                tc_commit(empty + s);
+                // refill the slot of the previous k-tile (its MMAs are the oldest in flight)
+                if (!refill_upto(i - 1)) {
+                    sFail = 1;
+                    set_err(g.err, 1);
+                    ++i;
+                    break;
+                }
+            }
+            tc_commit(done);
+        }
+        __syncthreads();
+        const bool ok = !sFail && mb_wait(done, (uint32_t)(l & 1));
+        tc_fence_after();
+        if (!ok && tid == 0) set_err(g.err, 2);
+        if (ok) {
+            // the ring slot of the last k-tile of this layer is free now: refill it
+            if (tid == 0 && !refill_upto(i - 1)) {
+                sFail = 1;
+                set_err(g.err, 1);
+            }
+            const float *bias = g.bias[l];
+            float *zo = g.z[l];
+            bf16 *ho = g.h[l];
+            const long long grow = (long long)(m0 + row) * BN;
+#pragma unroll 1
+            for (int c0 = (warp >> 2) * (BN / 4); c0 < ((warp >> 2) + 1) * (BN / 4); c0 += 32) {
+                float v[32];
+                tm_ld16(tmem + tlane + (uint32_t)c0, v);
+                tm_ld16(tmem + tlane + (uint32_t)(c0 + 16), v + 16);
+                uint32_t hp[16];
+#pragma unroll
+                for (int j = 0; j < 32; j += 2) {
+                    const float z0 = v[j] + bias[c0 + j], z1 = v[j + 1] + bias[c0 + j + 1];
+                    v[j] = z0;
+                    v[j + 1] = z1;
+                    const __nv_bfloat162 h2 = __floats2bfloat162_rn(silu_fast(z0), silu_fast(z1));
+                    hp[j >> 1] = *reinterpret_cast<const uint32_t *>(&h2);
+                }
+                if (zo) {
+                    float4 *zp = reinterpret_cast<float4 *>(zo + grow + c0);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) zp[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                }
+                if (ho) {
+                    uint4 *hq = reinterpret_cast<uint4 *>(ho + grow + c0);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) hq[q] = make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
+                }
+                // 16-byte chunks of 8 columns into the swizzled K-major activation tile
+                const int kb = c0 >> 6;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int ch = ((c0 & 63) >> 3) + q;
+                    uint4 *dst = reinterpret_cast<uint4 *>(act + kb * ACT_BLOCK + row * 128 + ((ch ^ (row & 7)) << 4));
+                    *dst = make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
+                }
+            }
+        }
+        // the activations are the tensor cores' next operand: generic-proxy writes made
+        // visible to the async proxy, and the accumulator reads ordered before the next MMAs
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    // output layer: one thread per row, a sequential FP32 sum over k
+    if (tid < 128 && !sFail) {
+        float acc[kOutCols] = {0.f, 0.f, 0.f};
+        const unsigned char *rowp = act + tid * 128;
+        for (int k = 0; k < BN; ++k) {
+            const int kb = k >> 6, ch = (k & 63) >> 3;
+            const bf16 hv = *reinterpret_cast<const bf16 *>(rowp + kb * ACT_BLOCK + ((ch ^ (tid & 7)) << 4) + ((k & 7) << 1));
+            const float h = __bfloat162float(hv);
+#pragma unroll
+            for (int j = 0; j < kOutCols; ++j) acc[j] += h * g.wo[j * BN + k];
+        }
+#pragma unroll
+        for (int j = 0; j < kOutCols; ++j) g.y[(long long)(m0 + tid) * kOutCols + j] = acc[j] + g.bo[j];
+    }
+    if (tid == 0 && sFail) {
+        // copies still in flight land in this CTA's shared memory: a bounded wait for them
+        for (int j = i; j < issued; ++j) mb_wait(full + (j % S), (uint32_t)((j / S) & 1));
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tm_dealloc(tmem, COLS);
+}
+
 }  // namespace
 
 namespace {
@@ -329,7 +553,9 @@ int feature_width(int nin, int bands) {
 
 // Fourier features of the rows idx[b] (or b when idx is null) of `in` [n][nin]:
 // u_i, then sin(2^f pi u_i), cos(2^f pi u_i) for f < bands (f-major), zero padding to K0.
-// One warp per row; the row's inputs are staged in shared memory.
+// One warp per row: the lanes take the row's inputs, then its (input, band) pairs, each
+// with one hardware sine / cosine pair (the features are rounded to BF16, far coarser than
+// the approximation), then the padding.
 __global__ void k_features(const float *__restrict__ in, const int *__restrict__ idx, int rows,
                            int nin, int bands, int K0, bf16 *__restrict__ X) {
     __shared__ float su[8][kMaxIn];
@@ -337,21 +563,22 @@ __global__ void k_features(const float *__restrict__ in, const int *__restrict__
     if (b >= rows) return;
     const int src = idx ? idx[b] : b;
     float *u = su[threadIdx.y];
-    for (int i = threadIdx.x; i < nin; i += blockDim.x) u[i] = in[(long long)src * nin + i];
-    __syncwarp();
-    for (int c = threadIdx.x; c < K0; c += blockDim.x) {
-        float v = 0.f;
-        if (c < nin) {
-            v = u[c];
-        } else {
-            const int q = c - nin, f = q / (2 * nin), r = q % (2 * nin), i = r >> 1;
-            if (f < bands) {
-                const float a = (float)(1 << f) * 3.14159265358979f * u[i];
-                v = (r & 1) ? cosf(a) : sinf(a);
-            }
-        }
-        X[(long long)b * K0 + c] = __float2bfloat16_rn(v);
+    bf16 *x = X + (long long)b * K0;
+    for (int i = threadIdx.x; i < nin; i += blockDim.x) {
+        const float v = in[(long long)src * nin + i];
+        u[i] = v;
+        x[i] = __float2bfloat16_rn(v);
     }
+    __syncwarp();
+    for (int p = threadIdx.x; p < nin * bands; p += blockDim.x) {
+        const int f = p / nin, i = p - f * nin;
+        float sv, cv;
+        __sincosf((float)(1 << f) * 3.14159265358979f * u[i], &sv, &cv);
+        const int c = nin + 2 * p;  // nin + 2 (nin f + i)
+        x[c] = __float2bfloat16_rn(sv);
+        x[c + 1] = __float2bfloat16_rn(cv);
+    }
+    for (int c = nin * (1 + 2 * bands) + threadIdx.x; c < K0; c += blockDim.x) x[c] = __float2bfloat16_rn(0.f);
 }
 
 // out[c][r] = in[r][c] for a [R][C] BF16 matrix (32 x 32 tiles through shared memory)
@@ -396,21 +623,6 @@ __global__ void k_colsum_bf16(const bf16 *__restrict__ A, int rows, int N, float
         for (int j = 0; j < 8; ++j) s += red[j][threadIdx.x];
         part[(long long)blockIdx.y * N + c] = s;
     }
-}
-
-// Output layer forward: Y[b][j] = sum_k H[b][k] Wo[j][k] + bo[j] (FP32 accumulate)
-__global__ void k_out_fwd(const bf16 *__restrict__ H, int rows, int W, const float *__restrict__ Wo,
-                          const float *__restrict__ bo, float *__restrict__ Y) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= rows) return;
-    float acc[kOut] = {0.f, 0.f, 0.f};
-    for (int k = 0; k < W; ++k) {
-        const float h = __bfloat162float(H[(long long)b * W + k]);
-#pragma unroll
-        for (int j = 0; j < kOut; ++j) acc[j] += h * Wo[j * W + k];
-    }
-#pragma unroll
-    for (int j = 0; j < kOut; ++j) Y[(long long)b * kOut + j] = acc[j] + bo[j];
 }
 
 // MSE over the batch: dY = 2 (Y - T) / (rows * 3); per-block partial losses
@@ -538,6 +750,9 @@ struct hidem_surrogate {
     float *dataIn = nullptr, *dataT = nullptr;   // training set [n][nin], [n][3]
     long long nData = 0;
     float *scratchIn = nullptr, *scratchT = nullptr;  // caller rows for predict / gradients
+    int PB = 0;                                   // rows per predict chunk
+    float *predIn = nullptr, *predY = nullptr;    // predict chunk: inputs [PB][nin], outputs [PB][3]
+    bf16 *predX = nullptr;                        // predict chunk features [PB][K0]
     long long steps = 0;
 };
 
@@ -649,21 +864,48 @@ hidem_status refresh_bf16(hidem_surrogate *s) {
 }
 
 // forward over `rows` rows whose features are in X0 (keepZ: store pre-activations)
-hidem_status forward(hidem_surrogate *s, int rows, bool keepZ) {
-    const bf16 *in = s->X0;
-    for (int l = 0; l < s->L; ++l) {
-        GemmArgs g{};
-        g.outH = s->H[l];
-        g.zOut = keepZ ? s->Z[l] : nullptr;
-        g.bias = s->P + s->offB[l];
-        g.ldo = s->W;
-        STRY(gemm_n<EPI_BIAS_SILU>(s, s->W, in, rows, s->Kl[l], s->Wb[l], 1, g));
-        in = s->H[l];
+// The whole forward pass over `rows` rows of features X (a multiple of 128) in one fused
+// launch (k_mlp_fwd); keepZ: the training pass, which keeps every layer's pre-activations
+// and activations for the backward pass.
+template <int BN>
+hidem_status mlp_forward_t(hidem_surrogate *s, const bf16 *X, int rows, float *Y, bool keepZ) {
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured.load() & bit)) {
+        cudaFuncSetAttribute(k_mlp_fwd<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem_bytes<BN>());
+        configured.fetch_or(bit);
     }
-    k_out_fwd<<<(rows + 127) / 128, 128, 0, s->stream>>>(s->H[s->L - 1], rows, s->W, s->P + s->offWo,
-                                                       s->P + s->offBo, s->Y);
+    if (rows % 128) return sfail(s, HIDEM_ERR_ARG, "forward rows %d not a multiple of 128", rows);
+    MlpMaps maps;
+    std::memset(&maps, 0, sizeof maps);
+    if (!make_map(&maps.x, X, rows, s->K0, 128)) return sfail(s, HIDEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    MlpArgs a{};
+    a.layers = s->L;
+    a.k0 = s->K0;
+    for (int l = 0; l < s->L; ++l) {
+        if (!make_map(&maps.w[l], s->Wb[l], BN, s->Kl[l], BN))
+            return sfail(s, HIDEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+        a.bias[l] = s->P + s->offB[l];
+        a.z[l] = keepZ ? s->Z[l] : nullptr;
+        a.h[l] = keepZ ? s->H[l] : nullptr;
+    }
+    a.wo = s->P + s->offWo;
+    a.bo = s->P + s->offBo;
+    a.y = Y;
+    a.err = s->dErr;
+    k_mlp_fwd<BN><<<rows / 128, kMlpThreads, mlp_smem_bytes<BN>(), s->stream>>>(maps, a);
     SCK(cudaGetLastError());
     return HIDEM_OK;
+}
+
+hidem_status mlp_forward(hidem_surrogate *s, const bf16 *X, int rows, float *Y, bool keepZ) {
+    return s->W == 256 ? mlp_forward_t<256>(s, X, rows, Y, keepZ) : mlp_forward_t<128>(s, X, rows, Y, keepZ);
+}
+
+hidem_status forward(hidem_surrogate *s, int rows, bool keepZ) {
+    return mlp_forward(s, s->X0, rows, s->Y, keepZ);
 }
 
 // loss and all gradients into G for the rows of X0 (targets[idx[b]] or targets[b])
@@ -771,7 +1013,8 @@ void hidem_surrogate_destroy(hidem_surrogate *s) {
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     void *bufs[] = {s->P, s->G, s->Mm, s->Vv, s->X0, s->Y, s->dY, s->dZa, s->dZb, s->dZT, s->inT,
-                    s->part, s->lossPart, s->idx, s->dataIn, s->dataT, s->scratchIn, s->scratchT, s->dErr};
+                    s->part, s->lossPart, s->idx, s->dataIn, s->dataT, s->scratchIn, s->scratchT, s->dErr,
+                    s->predIn, s->predY, s->predX};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (auto *p : s->Wb) if (p) cudaFree(p);
@@ -791,11 +1034,11 @@ hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device,
         return HIDEM_ERR_ARG;
     }
     *out = nullptr;
-    if (c->hidden_layers < 1 || c->hidden_layers > 16 || (c->width != 128 && c->width != 256) ||
+    if (c->hidden_layers < 1 || c->hidden_layers > kMlpMaxLayers || (c->width != 128 && c->width != 256) ||
         c->fourier_bands < 1 || c->fourier_bands > 12 || c->batch < 128 || c->batch % 128 ||
         c->batch > (1 << 20) || !(c->learning_rate > 0) || c->inputs < 1 || c->inputs > kMaxIn ||
         (c->cosine_decay != 0 && c->cosine_decay != 1)) {
-        err = "surrogate config out of range (layers 1..16, width 128 | 256, bands 1..12, batch a "
+        err = "surrogate config out of range (layers 1..8, width 128 | 256, bands 1..12, batch a "
               "multiple of 128, inputs 1..128, cosine_decay 0 | 1)";
         return HIDEM_ERR_ARG;
     }
@@ -867,6 +1110,10 @@ hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device,
     dm((void **)&s->idx, sizeof(int) * B);
     dm((void **)&s->scratchIn, sizeof(float) * (size_t)B * s->nin);
     dm((void **)&s->scratchT, sizeof(float) * (size_t)B * kOut);
+    s->PB = std::max(B, 65536);
+    dm((void **)&s->predIn, sizeof(float) * (size_t)s->PB * s->nin);
+    dm((void **)&s->predY, sizeof(float) * (size_t)s->PB * kOut);
+    dm((void **)&s->predX, sizeof(bf16) * (size_t)s->PB * K0);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&s->lossHost, sizeof(float) * ((B + 255) / 256));
     if (e == cudaSuccess) e = cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->Mm, 0, sizeof(float) * s->np, s->stream);
@@ -967,19 +1214,48 @@ hidem_status hidem_surrogate_predict(hidem_surrogate *s, const float *inputs, in
     if (!s) return HIDEM_ERR_ARG;
     if (!inputs || !out || n < 0) return sfail(s, HIDEM_ERR_ARG, "bad arguments");
     SCK(cudaSetDevice(s->device));
-    const int B = s->B;
-    for (int64_t r0 = 0; r0 < n; r0 += B) {
-        const int rows = (int)std::min<int64_t>(B, n - r0);
+    const int PB = s->PB;
+    for (int64_t r0 = 0; r0 < n; r0 += PB) {
+        const int rows = (int)std::min<int64_t>(PB, n - r0);
         const int padded = (rows + 127) / 128 * 128;
-        if (padded > rows) SCK(cudaMemsetAsync(s->scratchIn, 0, sizeof(float) * s->nin * padded, s->stream));
-        SCK(cudaMemcpyAsync(s->scratchIn, inputs + r0 * s->nin, sizeof(float) * s->nin * rows, cudaMemcpyHostToDevice, s->stream));
-        k_features<<<(padded + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->scratchIn, nullptr, padded, s->nin, s->cfg.fourier_bands, s->K0, s->X0);
-        STRY(forward(s, padded, false));
-        SCK(cudaMemcpyAsync(out + r0 * kOut, s->Y, sizeof(float) * kOut * rows, cudaMemcpyDeviceToHost, s->stream));
+        if (padded > rows) SCK(cudaMemsetAsync(s->predIn, 0, sizeof(float) * s->nin * padded, s->stream));
+        SCK(cudaMemcpyAsync(s->predIn, inputs + r0 * s->nin, sizeof(float) * s->nin * rows, cudaMemcpyHostToDevice, s->stream));
+        k_features<<<(padded + 7) / 8, dim3(32, 8), 0, s->stream>>>(s->predIn, nullptr, padded, s->nin, s->cfg.fourier_bands, s->K0, s->predX);
+        STRY(mlp_forward(s, s->predX, padded, s->predY, false));
+        SCK(cudaMemcpyAsync(out + r0 * kOut, s->predY, sizeof(float) * kOut * rows, cudaMemcpyDeviceToHost, s->stream));
     }
     SCK(cudaStreamSynchronize(s->stream));
     return check_err(s);
 }
+
+hidem_status hidem_surrogate_predict_device(hidem_surrogate *s, const float *inputs, int64_t n, float *out) {
+    if (!s) return HIDEM_ERR_ARG;
+    if (!inputs || !out || n < 0) return sfail(s, HIDEM_ERR_ARG, "bad arguments");
+    SCK(cudaSetDevice(s->device));
+    const int PB = s->PB;
+    for (int64_t r0 = 0; r0 < n; r0 += PB) {
+        const int rows = (int)std::min<int64_t>(PB, n - r0);
+        const int padded = (rows + 127) / 128 * 128;
+        const float *in = inputs + r0 * s->nin;
+        if (padded > rows) {
+            // the ragged last chunk: zero rows up to the next multiple of 128
+            SCK(cudaMemsetAsync(s->predIn, 0, sizeof(float) * s->nin * padded, s->stream));
+            SCK(cudaMemcpyAsync(s->predIn, in, sizeof(float) * s->nin * rows, cudaMemcpyDeviceToDevice, s->stream));
+            in = s->predIn;
+        }
+        k_features<<<(padded + 7) / 8, dim3(32, 8), 0, s->stream>>>(in, nullptr, padded, s->nin, s->cfg.fourier_bands,
+                                                                  s->K0, s->predX);
+        float *y = padded > rows ? s->predY : out + r0 * kOut;
+        STRY(mlp_forward(s, s->predX, padded, y, false));
+        if (padded > rows)
+            SCK(cudaMemcpyAsync(out + r0 * kOut, s->predY, sizeof(float) * kOut * rows, cudaMemcpyDeviceToDevice,
+                                s->stream));
+    }
+    SCK(cudaStreamSynchronize(s->stream));
+    return check_err(s);
+}
+
+void *hidem_surrogate_get_stream(hidem_surrogate *s) { return s ? (void *)s->stream : nullptr; }
 
 hidem_status hidem_surrogate_gradients(hidem_surrogate *s, const float *inputs, const float *targets,
                                        int64_t n, float *grads, double *loss) {

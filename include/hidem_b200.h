@@ -400,7 +400,7 @@ hidem_status hidem_batch_counts(const hidem_batch *b, int64_t *launches, int64_t
  * row-major. On failure of hidem_surrogate_create the text is in hidem_create_error(). */
 typedef struct hidem_surrogate hidem_surrogate;
 typedef struct hidem_surrogate_config {
-    int32_t hidden_layers;   /* 4 */
+    int32_t hidden_layers;   /* 1..8 (4) */
     int32_t width;           /* 128 or 256 */
     int32_t fourier_bands;   /* 1..12 */
     int32_t batch;           /* rows per training step, a multiple of 128 (16384) */
@@ -423,6 +423,11 @@ hidem_status hidem_surrogate_set_data(hidem_surrogate *s, const float *inputs, c
 /* `steps` Adam steps; *loss (may be NULL) receives the last step's batch loss */
 hidem_status hidem_surrogate_train(hidem_surrogate *s, int32_t steps, double *loss);
 hidem_status hidem_surrogate_predict(hidem_surrogate *s, const float *inputs, int64_t n, float *out);
+/* hidem_surrogate_predict for inputs and outputs already in device memory of the
+ * surrogate's GPU; the work runs on the surrogate's stream (hidem_surrogate_get_stream)
+ * and the call returns when it has completed. */
+hidem_status hidem_surrogate_predict_device(hidem_surrogate *s, const float *inputs, int64_t n, float *out);
+void *hidem_surrogate_get_stream(hidem_surrogate *s);
 /* loss and gradient of all parameters (flat order above) on exactly these n rows, no
  * update; n a multiple of 128 and at most `batch` */
 hidem_status hidem_surrogate_gradients(hidem_surrogate *s, const float *inputs, const float *targets,

@@ -112,6 +112,22 @@ def test_gpu_forward_and_gradients_match_oracle(gpu, width, nin, bands):
 
 
 @pytest.mark.gpu
+def test_gpu_predict_from_device_memory_equals_host_predict(gpu):
+    import torch
+    from hidem_b200 import surrogate as sg
+    cfg = sg.default_config(width=256, hidden_layers=4, fourier_bands=4, batch=1024, seed=7, inputs=40)
+    rng = np.random.default_rng(8)
+    u, _ = _rows(rng, 70000, 40)  # one full 65,536-row chunk and a ragged one
+    with sg.Surrogate(cfg) as s:
+        y = s.predict(u)
+        du = torch.from_numpy(u).cuda()
+        dy = torch.empty((u.shape[0], 3), dtype=torch.float32, device="cuda")
+        s.predict_device(du.data_ptr(), u.shape[0], dy.data_ptr())
+        assert s.stream_handle != 0
+    assert np.array_equal(dy.cpu().numpy(), y)
+
+
+@pytest.mark.gpu
 def test_gpu_training_lowers_the_loss(gpu):
     from hidem_b200 import surrogate as sg
     cfg = sg.default_config(width=256, hidden_layers=4, fourier_bands=6, batch=4096, seed=5,
