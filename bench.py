@@ -900,6 +900,7 @@ def main():
                    "l2": "inputs larger than L2 (records + link ends > 126 MB)",
                    "baseline_number": "RTX 5090 1.108e9 particle-steps/s, HiDEM/Docs/Performance.md:68"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "rebuilds_in_timed_steps": int(st1["regen_count"] - st0["regen_count"]),
         "clocks": clk,
     }
     print(json.dumps(line))

@@ -96,16 +96,32 @@ __global__ void k_bounds(const PRec<LP> *__restrict__ rec, int n, double *__rest
     }
 }
 
+// min / max are exact and idempotent, so the block's fold order (each thread starts from
+// one partial, repeated ones counting twice) gives the serial fold's result
+constexpr int kBoundsFinalThreads = 256;
 __global__ void k_bounds_final(const double *__restrict__ partial, int nb, double *__restrict__ out) {
-    if (threadIdx.x < 6) {
-        int k = threadIdx.x;
-        double v = partial[k];
-        for (int b = 1; b < nb; ++b) {
-            double u = partial[b * 6 + k];
-            v = (k < 3) ? fmin(v, u) : fmax(v, u);
+    __shared__ double red[6][kBoundsFinalThreads];
+    const int t = threadIdx.x;
+    double v[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v[k] = partial[(t % nb) * 6 + k];
+    for (int b = t + kBoundsFinalThreads; b < nb; b += kBoundsFinalThreads)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const double u = partial[b * 6 + k];
+            v[k] = (k < 3) ? fmin(v[k], u) : fmax(v[k], u);
         }
-        out[k] = v;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) red[k][t] = v[k];
+    __syncthreads();
+    for (int w = kBoundsFinalThreads / 2; w > 0; w >>= 1) {
+        if (t < w)
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+                red[k][t] = (k < 3) ? fmin(red[k][t], red[k][t + w]) : fmax(red[k][t], red[k][t + w]);
+        __syncthreads();
     }
+    if (t < 6) out[t] = red[t][0];
 }
 
 // Cell colour of every slot and the per-cell counts (NeighbourGrid::getGridId /
@@ -299,8 +315,13 @@ __device__ __forceinline__ int walk_cells(const PRec<LP> *__restrict__ rec, int 
             LP zDist = (LP)(zc - q->z);
             LP zDist2 = zDist * zDist;
             LP particleDistance2 = xDist2 + yDist2 + zDist2;
-            LP particleDistance = lsqrt(particleDistance2);
             LP radSum = ri + q->r;
+            // candidates farther than the interaction distance by a relative 1e-5 (far above
+            // the rounding of the square root and the subtraction below) fail the test
+            // whatever the rounding: skip the IEEE square root for them
+            const double reach = interactDist + (double)radSum;
+            if ((double)particleDistance2 > reach * reach * (1.0 + 1e-5) && reach > 0.0) continue;
+            LP particleDistance = lsqrt(particleDistance2);
             LP dist = particleDistance - radSum;
             if ((double)dist < interactDist) {
                 if (FILL) row[rowBase + (long long)count * kWarp] = j;
@@ -1136,7 +1157,7 @@ static inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 template <class LP>
 void launch_bounds(const PRec<LP> *rec, int n, double *partial, int nb, double *out, cudaStream_t s) {
     k_bounds<LP><<<nb, 256, 0, s>>>(rec, n, partial);
-    k_bounds_final<<<1, 32, 0, s>>>(partial, nb, out);
+    k_bounds_final<<<1, kBoundsFinalThreads, 0, s>>>(partial, nb, out);
 }
 
 template <class LP>
