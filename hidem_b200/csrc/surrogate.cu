@@ -139,9 +139,8 @@ __device__ __forceinline__ void set_err(int *flag, int code) {
     if (flag) atomicCAS(flag, 0, code);
 }
 
-// SiLU and its derivative with the fast exponential and division (the network trains in
+// The derivative of SiLU with the fast exponential and division (the network trains in
 // BF16; these need no IEEE rounding)
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
     const float s = __fdividef(1.0f, 1.0f + __expf(-z));
     return s * (1.0f + z * (1.0f - s));
@@ -153,15 +152,15 @@ namespace {
 
 // ------------------------------------------------------------------ tensor-core GEMM
 
-enum Epi { EPI_F32 = 0, EPI_BIAS_SILU = 1, EPI_SILU_GRAD = 2 };
+// the backward pass's epilogues (the forward pass is k_mlp_fwd)
+enum Epi { EPI_F32 = 0, EPI_SILU_GRAD = 2 };
 
 struct GemmArgs {
     int M, N, K;             // C[M][N] = A[M][K] * B[N][K]^T
     int kTiles;              // 64-wide K tiles per CTA (split-K: gridDim.y splits)
     float *outF;             // EPI_F32: [split][M][ldo] (+ bias when given)
     long long splitStride;   // elements between split partials of outF
-    bf16 *outH;              // EPI_BIAS_SILU: SiLU(acc + bias); EPI_SILU_GRAD: acc * SiLU'(zIn)
-    float *zOut;             // EPI_BIAS_SILU: acc + bias (may be null)
+    bf16 *outH;              // EPI_SILU_GRAD: acc * SiLU'(zIn)
     const float *zIn;        // EPI_SILU_GRAD: pre-activation [M][ldo]
     const float *bias;       // [N] or null
     int ldo;
@@ -294,10 +293,6 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 const long long o = (long long)(rowBase + r) * g.ldo + col;
                 if (EPI == EPI_F32) {
                     g.outF[blockIdx.y * g.splitStride + o] = acc + bias;
-                } else if (EPI == EPI_BIAS_SILU) {
-                    const float z = acc + bias;
-                    if (g.zOut) g.zOut[o] = z;
-                    g.outH[o] = __float2bfloat16_rn(silu(z));
                 } else {
                     g.outH[o] = __float2bfloat16_rn(acc * silu_grad(g.zIn[o]));
                 }
