@@ -461,10 +461,14 @@ hidem_status rebuild(hidem_ctx *ctx) {
     ctx->launches += 1;
     ctx->launches += launch_scan<int, long long>(ctx->blockWidth, nb32 + 1, 32ll, ctx->sOff,
                                                  ctx->scanSums64, ctx->offTotal, st);
-    long long sTotal = 0;
-    CK(cudaMemcpyAsync(&sTotal, ctx->offTotal, sizeof sTotal, cudaMemcpyDeviceToHost, st));
+    // the contact-list statistics travel with the link-end total
+    launch_count_stats(ctx->counts, n, ctx->offTotal + 1, ctx->smCount, st);
+    ctx->launches += 1;
+    long long tot[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(tot, ctx->offTotal, sizeof tot, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     TRY(check_device_error(ctx));
+    const long long sTotal = tot[0];
     if (sTotal >= (1ll << 31))
         return fail(ctx, HIDEM_ERR_CAPACITY, "%lld link-end slots (limit 2^31)", sTotal);
     // side[0] / sideSlot[0] hold the current layout; the new one is built in [1], then swapped
@@ -479,21 +483,9 @@ hidem_status rebuild(hidem_ctx *ctx) {
     std::swap(ctx->sideSlot[0], ctx->sideSlot[1]);
     std::swap(ctx->side[0], ctx->side[1]);
 
-    // statistics (host copies of the counts)
-    std::vector<uint32_t> cnt((size_t)n);
-    CK(cudaMemcpyAsync(cnt.data(), ctx->counts, sizeof(uint32_t) * (size_t)n,
-                       cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    long long pairs = 0, mn = 0, ml = 0;
-    for (int i = 0; i < n; ++i) {
-        long long a = cnt[i] & 0xffffu, s = cnt[i] >> 16;
-        pairs += a;
-        mn = std::max(mn, a);
-        ml = std::max(ml, s);
-    }
-    ctx->numPairs = pairs;
-    ctx->maxNeigh = mn;
-    ctx->maxLinksPP = ml;
+    ctx->numPairs = tot[1];
+    ctx->maxNeigh = tot[2];
+    ctx->maxLinksPP = tot[3];
     ctx->built = true;
     ctx->regenCount += 1;
     ctx->lastRegen = ctx->step;
@@ -1266,7 +1258,7 @@ hidem_status hidem_create(const hidem_params *params, int device, hidem_ctx **ou
     if (s == HIDEM_OK) s = dalloc(ctx, &ctx->eventCount, 1);
     if (s == HIDEM_OK) s = dalloc(ctx, &ctx->boundsPartial, 6 * 4 * ctx->smCount + 6);
     if (s == HIDEM_OK) s = dalloc(ctx, &ctx->boundsOut, 6);
-    if (s == HIDEM_OK) s = dalloc(ctx, &ctx->offTotal, 1);
+    if (s == HIDEM_OK) s = dalloc(ctx, &ctx->offTotal, 4);  // a scan total + the count statistics
     if (s == HIDEM_OK) {
         cudaMemsetAsync(ctx->errorFlag, 0, sizeof(int), ctx->stream);
         cudaMemsetAsync(ctx->eventCount, 0, sizeof(unsigned long long), ctx->stream);

@@ -364,6 +364,31 @@ __global__ void k_nbr_fill(const PRec<LP> *__restrict__ rec, int n, const int *_
                          nOff[i >> 5] + (i & 31));
 }
 
+// Contact-list statistics of a rebuild from the per-slot counts (low 16 bits: contacts,
+// high 16 bits: link ends): out[0] total contacts, out[1] the largest contact count,
+// out[2] the largest link-end count (integer sums and maxima: order-independent).
+__global__ void k_count_stats(const uint32_t *__restrict__ counts, int n, long long *__restrict__ out) {
+    long long pairs = 0, mn = 0, ml = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = counts[i];
+        const long long a = c & 0xffffu, e = c >> 16;
+        pairs += a;
+        mn = a > mn ? a : mn;
+        ml = e > ml ? e : ml;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+        const long long a = __shfl_xor_sync(0xffffffffu, mn, o), e = __shfl_xor_sync(0xffffffffu, ml, o);
+        mn = a > mn ? a : mn;
+        ml = e > ml ? e : ml;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long *>(out), (unsigned long long)pairs);
+        atomicMax(out + 1, mn);
+        atomicMax(out + 2, ml);
+    }
+}
+
 // ------------------------------------------------------------------ link ends
 
 __global__ void k_side_count(const int *__restrict__ orig, int n, const int *__restrict__ plStart,
@@ -1211,6 +1236,12 @@ void launch_nbr_fill(const PRec<LP> *rec, int n, const int *cellOf, const GridIn
                      const long long *nOff, int32_t *nbr, cudaStream_t s) {
     k_nbr_fill<LP><<<nblk(n, 128), 128, 0, s>>>(rec, n, cellOf, g, cellStart, cellCount,
                                                 interactDist, nOff, nbr);
+}
+
+void launch_count_stats(const uint32_t *counts, int n, long long *out, int smCount, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, 3 * sizeof(long long), s);
+    const int blocks = std::max(1, std::min(nblk(n, 256), 4 * smCount));
+    k_count_stats<<<blocks, 256, 0, s>>>(counts, n, out);
 }
 
 void launch_side_count(const int *orig, int n, const int *plStart, uint32_t *counts,

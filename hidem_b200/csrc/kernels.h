@@ -99,6 +99,9 @@ template <class LP>
 void launch_nbr_fill(const PRec<LP> *rec, int n, const int *cellOf, const GridInfo &g,
                      const int *cellStart, const int *cellCount, double interactDist,
                      const long long *nOff, int32_t *nbr, cudaStream_t s);
+// out[0..2] = total contacts, largest contact count, largest link-end count of the
+// per-slot counts (out zeroed first)
+void launch_count_stats(const uint32_t *counts, int n, long long *out, int smCount, cudaStream_t st);
 void launch_side_count(const int *orig, int n, const int *plStart, uint32_t *counts,
                        int *blockWidth, int *errorFlag, cudaStream_t s);
 template <class LP>
