@@ -48,10 +48,21 @@ __device__ __forceinline__ void contact_terms(const Consts<LP> &c, LP mask, LP x
     t[5] = mask * ((-c.dampingRotation) * ((s[5] - o[5]) * c.invDt));
 }
 
+// A pair beyond the active distance gets mask 0, and every term the functor adds is then
+// 0 times a finite value (the distance is positive there): adding those signed zeros
+// leaves each force component's value unchanged (a zero component at most changes its
+// sign, which no later operation can observe), so such pairs skip the arithmetic. A NaN
+// distance fails the comparison and takes the full path, as in the functor.
 template <class LP>
 __device__ __forceinline__ void contact_pair(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
                                              LP zDist, const LP *s, LP sr, const LP *o, LP orr,
                                              LP *F) {
+    {
+        const LP particleDistance2 = xDist * xDist + yDist * yDist + zDist * zDist;
+        const LP radSum = sr + orr;
+        const LP activeDist2 = (radSum + c.attractDistance) * (radSum + c.attractDistance);
+        if (particleDistance2 >= activeDist2) return;
+    }
     LP t[6];
     contact_terms<LP>(c, mask, xDist, yDist, zDist, s, sr, o, orr, t);
 #pragma unroll
