@@ -95,6 +95,10 @@ def test_step_kernel_autotuner_settles(gpu):
                                  abi.STEP_KERNEL_THREAD_CAPPED, abi.STEP_KERNEL_THREAD_ASYNC)
     with pytest.raises(abi.HidemError):
         lib.set_step_kernel(9)
+    # the rebuild's device-side statistics: link ends per particle
+    deg = np.bincount(l["globalKeyEndA"], minlength=p["xCord"].shape[0]) + \
+        np.bincount(l["globalKeyEndB"], minlength=p["xCord"].shape[0])
+    assert lib.stats()["max_links_per_particle"] == int(deg.max())
     lib.close()
 
 
@@ -107,6 +111,7 @@ def test_gpu_cells_and_contact_list_bit_exact(gpu, precision):
     lib.regenerate()
     ix, iy, iz, dims, mins = lib.get_cells()
     counts, lst = lib.get_neighbours()
+    st = lib.stats()
     lib.close()
     ox, oy, oz, odims, omins = oracle.port().cells(P, p)
     assert np.array_equal(ix, ox) and np.array_equal(iy, oy) and np.array_equal(iz, oz)
@@ -114,6 +119,8 @@ def test_gpu_cells_and_contact_list_bit_exact(gpu, precision):
     oc, ol = oracle.port().neighbours(P, p)
     assert np.array_equal(counts, oc)
     assert np.array_equal(lst, ol)  # same pairs in the same per-particle order
+    # the rebuild's device-side statistics
+    assert st["num_neighbour_pairs"] == int(oc.sum()) and st["max_neighbours"] == int(oc.max())
 
 
 @pytest.mark.parametrize("precision", PRECS)
