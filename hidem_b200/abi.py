@@ -252,6 +252,7 @@ _PROTOS = [
     ("hidem_set_bed_maps", C.c_int, [C.c_void_p, C.POINTER(HidemMap2d), C.POINTER(HidemMap2d)]),
     ("hidem_set_external_force_maps", C.c_int, [C.c_void_p, C.POINTER(HidemMap2d)]),
     ("hidem_kinetic_energy", C.c_int, [C.c_void_p, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)]),
+    ("hidem_momentum", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("hidem_set_collision_mesh", C.c_int, [C.c_void_p, C.POINTER(HidemMesh)]),
     ("hidem_get_mesh_face_forces", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("hidem_zero_mesh_face_forces", C.c_int, [C.c_void_p]),

@@ -1883,10 +1883,10 @@ hidem_status hidem_kinetic_energy(hidem_ctx *ctx, double *translational, double 
     CK(cudaSetDevice(ctx->device));
     const int nb = (int)std::max<long long>(1, std::min<long long>((ctx->n + 255) / 256, 4LL * ctx->smCount));
     if (ctx->energyBlocks < nb) {
-        TRY(dalloc(ctx, &ctx->energyBuf, 3LL * nb + 3));
+        TRY(dalloc(ctx, &ctx->energyBuf, 6LL * nb + 6));
         ctx->energyBlocks = nb;
     }
-    double *out = ctx->energyBuf + 3 * ctx->energyBlocks;
+    double *out = ctx->energyBuf + 6 * ctx->energyBlocks;
     if (ctx->mixed)
         launch_energy<float>(ctx->cf, recp<float>(ctx, ctx->cur), (int)ctx->n, ctx->energyBuf, nb, out, ctx->stream);
     else
@@ -1898,6 +1898,32 @@ hidem_status hidem_kinetic_energy(hidem_ctx *ctx, double *translational, double 
     if (translational) *translational = h[0];
     if (rotational) *rotational = h[1];
     if (max_speed) *max_speed = std::sqrt(h[2]);
+    return HIDEM_OK;
+}
+
+hidem_status hidem_momentum(hidem_ctx *ctx, double linear[3], double angular[3]) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    CK(cudaSetDevice(ctx->device));
+    const int nb = (int)std::max<long long>(1, std::min<long long>((ctx->n + 255) / 256, 4LL * ctx->smCount));
+    if (ctx->energyBlocks < nb) {
+        TRY(dalloc(ctx, &ctx->energyBuf, 6LL * nb + 6));
+        ctx->energyBlocks = nb;
+    }
+    double *out = ctx->energyBuf + 6 * ctx->energyBlocks;
+    if (ctx->mixed)
+        launch_momentum<float>(ctx->cf, recp<float>(ctx, ctx->cur), (int)ctx->n, ctx->energyBuf, nb, out, ctx->stream);
+    else
+        launch_momentum<double>(ctx->cd, recp<double>(ctx, ctx->cur), (int)ctx->n, ctx->energyBuf, nb, out,
+                                ctx->stream);
+    ctx->launches += 2;
+    double h[6];
+    CK(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 3; ++k) {
+        if (linear) linear[k] = h[k];
+        if (angular) angular[k] = h[3 + k];
+    }
     return HIDEM_OK;
 }
 

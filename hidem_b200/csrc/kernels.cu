@@ -1424,6 +1424,65 @@ void launch_energy(const Consts<LP> &c, const PRec<LP> *rec, int n, double *part
     k_energy_final<<<1, 256, 0, s>>>(partial, nb, out);
 }
 
+// Linear momentum sum m v and angular momentum about the origin sum x (x) m v + I w, in
+// double precision: per-block partials [6][gridDim.x] (tree sums in a fixed order), then
+// one block folding them, so the result does not depend on scheduling.
+template <class LP>
+__global__ void k_momentum(const Consts<LP> c, const PRec<LP> *__restrict__ rec, int n,
+                           double *__restrict__ partial) {
+    __shared__ double red[6][256];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const double dt = (double)c.dt, rho = (double)c.rhoIce;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const PRec<LP> p = load_rec(rec + i);
+        const double d = 2.0 * (double)p.r;
+        const double m = rho * d * d * d, I = m * d * d / 6.0;
+        const double px = m * (p.d[0] / dt), py = m * (p.d[1] / dt), pz = m * (p.d[2] / dt);
+        acc[0] += px;
+        acc[1] += py;
+        acc[2] += pz;
+        acc[3] += (p.y * pz - p.z * py) + I * (p.d[3] / dt);
+        acc[4] += (p.z * px - p.x * pz) + I * (p.d[4] / dt);
+        acc[5] += (p.x * py - p.y * px) + I * (p.d[5] / dt);
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) red[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 6; ++q) partial[q * gridDim.x + blockIdx.x] = red[q][0];
+}
+
+__global__ void k_momentum_final(const double *__restrict__ partial, int nb, double *__restrict__ out) {
+    __shared__ double red[6][256];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) acc[q] += partial[q * nb + i];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) red[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) out[threadIdx.x] = red[threadIdx.x][0];
+}
+
+template <class LP>
+void launch_momentum(const Consts<LP> &c, const PRec<LP> *rec, int n, double *partial, int nb,
+                     double *out, cudaStream_t s) {
+    k_momentum<LP><<<nb, 256, 0, s>>>(c, rec, n, partial);
+    k_momentum_final<<<1, 256, 0, s>>>(partial, nb, out);
+}
+
 template <class LP>
 void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb, cudaStream_t s) {
     k_max_diff<LP><<<nb, 256, 0, s>>>(rec, n, out);
@@ -1460,6 +1519,8 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
                                         unsigned long long *, long long, cudaStream_t);            \
     template void launch_max_diff<LP>(const PRec<LP> *, int, unsigned long long *, int,            \
                                       cudaStream_t);                                               \
+    template void launch_momentum<LP>(const Consts<LP> &, const PRec<LP> *, int, double *, int,     \
+                                      double *, cudaStream_t);                                     \
     template void launch_energy<LP>(const Consts<LP> &, const PRec<LP> *, int, double *, int,       \
                                     double *, cudaStream_t);
 

@@ -178,6 +178,11 @@ template <class LP>
 void launch_mesh_prune(const MeshView<LP> &m, double cellSize, double margin, double reach,
                        const uint8_t *keep, int *qSizes, const int *qStarts, int *qValues, bool fill,
                        cudaStream_t s);
+// Linear and angular momentum (about the origin) of the particles in double precision:
+// out[0..2] sum m v, out[3..5] sum x (x) m v + I w; `partial` holds 6 * nb doubles
+template <class LP>
+void launch_momentum(const Consts<LP> &c, const PRec<LP> *rec, int n, double *partial, int nb,
+                     double *out, cudaStream_t s);
 template <class LP>
 void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb, cudaStream_t s);
 

@@ -154,6 +154,12 @@ class HiDEMLib:
         """The MeshAccel grid: counts, lower, upper, sizes, starts, values."""
         return _mesh_accel(lambda *a: self._check(self._lib.hidem_get_mesh_accel(self._ctx, *a)))
 
+    def momentum(self) -> tuple[np.ndarray, np.ndarray]:
+        """(linear [3], angular about the origin [3]) momentum of the current state."""
+        lin, ang = np.zeros(3), np.zeros(3)
+        self._check(self._lib.hidem_momentum(self._ctx, lin.ctypes.data, ang.ctypes.data))
+        return lin, ang
+
     def kinetic_energy(self) -> tuple[float, float, float]:
         """(translational, rotational, max speed) of the current state."""
         t, r, v = C.c_double(), C.c_double(), C.c_double()

@@ -331,6 +331,10 @@ hidem_status hidem_get_mesh_accel(hidem_ctx *ctx, int32_t counts[3], double lowe
  * speed. Any output pointer may be NULL. Synchronises the context's stream. */
 hidem_status hidem_kinetic_energy(hidem_ctx *ctx, double *translational, double *rotational,
                                   double *max_speed);
+/* Momentum of the current state, with the velocities and masses of hidem_kinetic_energy:
+ * linear sum m v and angular about the origin sum x (x) m v + I w, reduced in double
+ * precision in a fixed order. Either pointer may be NULL. Synchronises the stream. */
+hidem_status hidem_momentum(hidem_ctx *ctx, double linear[3], double angular[3]);
 
 /* ---- step kernel choice ----------------------------------------------- */
 

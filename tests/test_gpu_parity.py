@@ -498,3 +498,37 @@ def test_wide_rows_take_the_thread_per_particle_kernel(gpu, precision):
         res = gpu_run(P, p, l, 5, mode)
         assert res[4]["max_neighbours"] > 300
         assert_same(res, ref[0], ref[1], ref[3], ref[2] if mode == "split" else None)
+
+
+def test_mixed_against_fp64_every_output(gpu):
+    """The mixed build against the plain FP64 build on the 32,000-particle block, breaking
+    off, 1000 steps: every output within its stated bound — positions within 1e-4 of the
+    largest displacement (and 2e-6 d), rotations, increments and CT within 5e-4 relative
+    L2, kinetic energy and momentum within 1e-3, the same link states."""
+    res = {}
+    for prec in PRECS:
+        P, p, l = workloads.ice_block(cells=(20, 20, 20), precision=prec, seed=1, breakTime=1e30)
+        lib = HiDEMLib(P)
+        lib.set_particles(p)
+        lib.set_links(l)
+        lib.step(1000)
+        q, ll = lib.get_particles(), lib.get_links()
+        kt, kr, _ = lib.kinetic_energy()
+        lin, ang = lib.momentum()
+        lib.close()
+        res[prec] = (p, q, ll, np.array([kt, kr]), lin, ang)
+    (p0, a, la, ea, lina, anga) = res[abi.PREC_MIXED]
+    (_, b, lb, eb, linb, angb) = res[abi.PREC_FP64]
+    disp = np.sqrt(sum((b[k] - p0[k].astype(np.float64)) ** 2 for k in ("xCord", "yCord", "zCord")))
+    for k in ("xCord", "yCord", "zCord"):
+        err = np.abs(a[k] - b[k]).max()
+        assert err <= 1e-4 * disp.max() and err <= 2e-6, k
+    rel = lambda x, y: np.linalg.norm(x.astype(np.float64) - y.astype(np.float64)) / np.linalg.norm(y.astype(np.float64))
+    for k in ("xTheta", "yTheta", "zTheta", "xDiff", "yDiff", "zDiff", "uDiff", "vDiff", "wDiff"):
+        assert rel(a[k], b[k]) <= 5e-4, k
+    for k in ("CT0", "CT1", "CT2", "CT3", "CT4", "CT5"):
+        assert rel(la[k], lb[k]) <= 5e-4, k
+    assert np.array_equal(la["state"], lb["state"])
+    assert np.all(np.abs(ea - eb) <= 1e-3 * eb)
+    assert np.linalg.norm(lina - linb) <= 1e-3 * np.linalg.norm(linb)
+    assert np.linalg.norm(anga - angb) <= 1e-3 * np.linalg.norm(angb)

@@ -103,6 +103,22 @@ def test_kinetic_energy_matches_the_host_formula(gpu):
     assert kr == pytest.approx(float(np.sum(0.5 * inertia * w2)), rel=1e-9)
     assert vmax == pytest.approx(float(np.sqrt(v2.max())), rel=1e-9)
     assert kt > 0
+    # momentum: linear and angular about the origin, the same velocities and masses
+    lib = HiDEMLib(t.params)
+    lib.set_particles(t.particles)
+    lib.set_links(t.links)
+    lib.step(30)
+    lin, ang = lib.momentum()
+    q = lib.get_particles()
+    lib.close()
+    v = np.stack([q[k].astype(np.float64) / dt for k in ("xDiff", "yDiff", "zDiff")], axis=1)
+    w = np.stack([q[k].astype(np.float64) / dt for k in ("uDiff", "vDiff", "wDiff")], axis=1)
+    x = np.stack([q[k] for k in ("xCord", "yCord", "zCord")], axis=1)
+    pm = m[:, None] * v
+    scale = float(np.abs(pm).sum())
+    assert np.allclose(lin, pm.sum(axis=0), rtol=1e-9, atol=1e-12 * scale)
+    want = np.cross(x, pm).sum(axis=0) + (inertia[:, None] * w).sum(axis=0)
+    assert np.allclose(ang, want, rtol=1e-9, atol=1e-12 * float(np.abs(np.cross(x, pm)).sum()))
 
 
 @pytest.mark.gpu
