@@ -1,6 +1,7 @@
 // C ABI of libhidem_b200: the context, the HiDEMLib-shaped step operations and the
 // host side of the rebuild (HiDEMLib::gridService) policy.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -9,6 +10,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.h"
@@ -169,20 +171,20 @@ hidem_status fail(hidem_ctx *c, hidem_status s, const char *fmt, ...) {
 template <class T>
 hidem_status dalloc(hidem_ctx *ctx, T **p, long long count) {
     if (*p) {
-        cudaFree(*p);
+        CK(cudaFreeAsync(*p, ctx->stream));
         *p = nullptr;
     }
     if (count <= 0) count = 1;
-    CK(cudaMalloc((void **)p, sizeof(T) * (size_t)count));
+    CK(cudaMallocAsync((void **)p, sizeof(T) * (size_t)count, ctx->stream));
     return HIDEM_OK;
 }
 hidem_status dalloc_bytes(hidem_ctx *ctx, void **p, size_t bytes) {
     if (*p) {
-        cudaFree(*p);
+        CK(cudaFreeAsync(*p, ctx->stream));
         *p = nullptr;
     }
     if (bytes == 0) bytes = 16;
-    CK(cudaMalloc(p, bytes));
+    CK(cudaMallocAsync(p, bytes, ctx->stream));
     return HIDEM_OK;
 }
 template <class T>
@@ -545,7 +547,8 @@ bool gs_wants_diff(const hidem_ctx *ctx) {
 
 // The rest of HiDEMLib::gridService (HiDEMLib.h:533-628) on one rank, once the
 // accumulated-distance increment of this step (when gs_wants_diff) is known.
-hidem_status gs_finish(hidem_ctx *ctx, double currDist) {
+// gridService's decision (accumulated distance updated; reset when it rebuilds)
+bool gs_decide(hidem_ctx *ctx, double currDist) {
     const long long t = ctx->step;
     bool regen = (t == ctx->startStep);
     if (ctx->P.gridRegenInterval != -1) {
@@ -556,10 +559,12 @@ hidem_status gs_finish(hidem_ctx *ctx, double currDist) {
     }
     if (t == ctx->P.firstBalanceTimestep) regen = true;
     if (!ctx->built) regen = true;
-    if (regen) {
-        ctx->accumulatedDist = 0;
-        TRY(do_rebuild(ctx));
-    }
+    if (regen) ctx->accumulatedDist = 0;
+    return regen;
+}
+
+hidem_status gs_finish(hidem_ctx *ctx, double currDist) {
+    if (gs_decide(ctx, currDist)) TRY(do_rebuild(ctx));
     return HIDEM_OK;
 }
 
@@ -1050,6 +1055,49 @@ hidem_status batch_launch_run(hidem_batch *b, int run, int kernel) {
 // nsteps timesteps of every context: per step exactly the work hidem_step does for each
 // context alone (gridService, the fused step, the pending link update), in one launch
 // per group.
+// The rebuilds of the contexts in `list`, each on its own stream (`own`, the streams the
+// contexts had before the batch bound them to its stream), several at a time from a few
+// host threads, so that their host round trips and small kernels overlap (buffers grow
+// with stream-ordered allocations, which do not wait for the rest of the device). The
+// batch's stream is drained first (the records come from its launches) and every
+// rebuild has completed on return.
+hidem_status batch_rebuild_set(hidem_batch *b, const std::vector<int> &list,
+                               const std::vector<cudaStream_t> &own, int maxThreads) {
+    const int nthreads = (int)std::min<size_t>(list.size(), (size_t)maxThreads);
+    std::atomic<int> next{0};
+    std::vector<hidem_status> st(list.size(), HIDEM_OK);
+    int device = 0;
+    BCK(cudaGetDevice(&device));
+    auto work = [&]() {
+        cudaSetDevice(device);
+        for (int k; (k = next.fetch_add(1)) < (int)list.size();) {
+            hidem_ctx *c = b->ctxs[list[k]];
+            c->stream = own[list[k]];
+            st[k] = do_rebuild(c);
+            if (cudaStreamSynchronize(c->stream) != cudaSuccess && st[k] == HIDEM_OK)
+                st[k] = fail(c, HIDEM_ERR_CUDA, "rebuild stream synchronisation failed");
+            c->stream = b->stream;
+        }
+    };
+    if (nthreads <= 1) {
+        work();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t) pool.emplace_back(work);
+        for (auto &t : pool) t.join();
+    }
+    for (size_t k = 0; k < list.size(); ++k)
+        if (st[k] != HIDEM_OK)
+            return bfail(b, st[k], "context %d: %s", list[k], b->ctxs[list[k]]->err.c_str());
+    return HIDEM_OK;
+}
+
+hidem_status batch_rebuild(hidem_batch *b, const std::vector<int> &list,
+                           const std::vector<cudaStream_t> &own) {
+    BCK(cudaStreamSynchronize(b->stream));
+    return batch_rebuild_set(b, list, own, 8);
+}
+
 template <class LP>
 hidem_status batch_run(hidem_batch *b, int nsteps) {
     const int nc = (int)b->ctxs.size();
@@ -1078,12 +1126,14 @@ hidem_status batch_run(hidem_batch *b, int nsteps) {
             BCK(cudaStreamSynchronize(b->stream));
         }
         if (anyDue) {
+            std::vector<int> regen;
             for (int idx = 0; idx < nc; ++idx) {
                 hidem_ctx *c = b->ctxs[idx];
                 if (!gs_due(c)) continue;
                 const double cd = gs_wants_diff(c) ? curr_dist<LP>(b->diffHost + 3 * idx) : 0.0;
-                BTRY(gs_finish(c, cd));
+                if (gs_decide(c, cd)) regen.push_back(idx);
             }
+            if (!regen.empty()) TRY(batch_rebuild(b, regen, bind.streams));
             dirty = true;
         }
         long long run = nsteps - s;
@@ -1248,6 +1298,16 @@ hidem_status hidem_create(const hidem_params *params, int device, hidem_ctx **ou
     e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smCount, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) {
+        // the contexts' buffers come from the device's default stream-ordered pool: keep
+        // freed blocks for reuse (later contexts, regrown buffers) instead of returning them
+        // to the driver at every synchronisation
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (e != cudaSuccess) {
         g_create_error = std::string("CUDA setup failed: ") + cudaGetErrorString(e);
         delete ctx;
