@@ -1448,10 +1448,9 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
         CK(cudaMemcpyAsync(ctx->type[0], p->type, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
     else
         CK(cudaMemsetAsync(ctx->type[0], 0, (size_t)n, ctx->stream));
-    std::vector<int32_t> ident((size_t)n);
-    for (int64_t i = 0; i < n; ++i) ident[i] = (int32_t)i;
-    CK(cudaMemcpyAsync(ctx->orig[0], ident.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->slotOf, ctx->orig[0], 4 * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
+    launch_iota32(ctx->orig[0], (int)n, ctx->stream);
+    launch_iota32(ctx->slotOf, (int)n, ctx->stream);
+    ctx->launches += 2;
     CK(cudaMemsetAsync(ctx->counts, 0, 4 * (size_t)n, ctx->stream));
     CK(cudaMemsetAsync(ctx->force, 0, 6 * lp * (size_t)n, ctx->stream));
     ctx->owners.assign((size_t)n, 0);
@@ -1464,14 +1463,7 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     ctx->n = n;
     ctx->haveParticles = true;
     ctx->built = false;
-    {
-        double r = 0;
-        if (ctx->mixed)
-            for (int64_t i = 0; i < n; ++i) r = std::max(r, (double)static_cast<const float *>(p->radius)[i]);
-        else
-            for (int64_t i = 0; i < n; ++i) r = std::max(r, static_cast<const double *>(p->radius)[i]);
-        ctx->maxParticleRadius = r;
-    }
+    ctx->maxParticleRadius = -1.0;  // found on the device when a collision mesh needs it
     TRY(prune_mesh(ctx));
     ctx->startStep = ctx->step;
     // a link set refers to particle indices of the previous particle set
@@ -2196,6 +2188,18 @@ hidem_status prune_mesh_t(hidem_ctx *ctx, MeshView<LP> &m, const Consts<LP> &c) 
     dfree(ctx->meshQStarts);
     dfree(ctx->meshQValues);
     ctx->meshQSizes = ctx->meshQStarts = ctx->meshQValues = nullptr;
+    if (ctx->haveParticles && ctx->maxParticleRadius < 0) {
+        // the largest radius of the particles last set (their records hold it)
+        launch_max_radius<LP>(recp<LP>(ctx, ctx->cur), (int)ctx->n, reinterpret_cast<unsigned long long *>(ctx->offTotal),
+                              ctx->stream);
+        ctx->launches += 1;
+        unsigned long long bits = 0;
+        CK(cudaMemcpyAsync(&bits, ctx->offTotal, sizeof bits, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        double r;
+        std::memcpy(&r, &bits, sizeof r);
+        ctx->maxParticleRadius = r;
+    }
     const LP rmax = (LP)std::max(ctx->maxParticleRadius, ctx->P.maxRadius);
     const LP id = c.bedInteract + rmax;
     const double reach = (double)id * (1.0 + 1e-4) + 1e-3;

@@ -1678,6 +1678,35 @@ void launch_link_keys_identity(const long long *keyA, const long long *keyB, lon
     k_link_keys_identity<<<nb, 256, 0, st>>>(keyA, keyB, L, n, A, B, badMin, selfMin);
 }
 
+__global__ void k_iota32(int *out, int count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) out[i] = i;
+}
+
+void launch_iota32(int *out, int count, cudaStream_t st) {
+    if (count <= 0) return;
+    const int nb = (int)std::min<long long>((count + 255LL) / 256, 148LL * 32);
+    k_iota32<<<nb, 256, 0, st>>>(out, count);
+}
+
+// largest particle radius (radii are positive, so their IEEE bits order like the values)
+template <class LP>
+__global__ void k_max_radius(const PRec<LP> *__restrict__ rec, int n, unsigned long long *__restrict__ out) {
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = fmax(m, (double)rec[i].r);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+template <class LP>
+void launch_max_radius(const PRec<LP> *rec, int n, unsigned long long *out, cudaStream_t st) {
+    cudaMemsetAsync(out, 0, sizeof(unsigned long long), st);
+    const int nb = (int)std::max<long long>(1, std::min<long long>((n + 255LL) / 256, 148LL * 4));
+    k_max_radius<LP><<<nb, 256, 0, st>>>(rec, n, out);
+}
+template void launch_max_radius<float>(const PRec<float> *, int, unsigned long long *, cudaStream_t);
+template void launch_max_radius<double>(const PRec<double> *, int, unsigned long long *, cudaStream_t);
+
 void launch_iota64(long long *out, long long count, cudaStream_t st) {
     if (count <= 0) return;
     const int nb = (int)std::min<long long>((count + 255) / 256, 148LL * 32);

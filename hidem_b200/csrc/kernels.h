@@ -68,8 +68,12 @@ void launch_side_init(const uint8_t *linkState, long long L, int *sideSlot, uint
 void launch_link_keys_identity(const long long *keyA, const long long *keyB, long long L,
                                long long n, int *A, int *B, unsigned long long *badMin,
                                unsigned long long *selfMin, cudaStream_t st);
-// out[i] = i (int64)
+// out[i] = i (int64 / int32)
 void launch_iota64(long long *out, long long count, cudaStream_t st);
+void launch_iota32(int *out, int count, cudaStream_t st);
+// *out = the IEEE bits of the largest particle radius, as a double (out zeroed first)
+template <class LP>
+void launch_max_radius(const PRec<LP> *rec, int n, unsigned long long *out, cudaStream_t st);
 template <class LP>
 void launch_gather_sides(const int *sideSlot, long long L, const LP *ct, LP *out,
                          const uint8_t *sState, uint8_t *linkState, cudaStream_t st);
