@@ -210,6 +210,13 @@ def mesh(vertices, normals, cell_size: float, precision: int, mesh_force: float 
     return m, arrs
 
 
+class HidemFunctorParams(C.Structure):
+    _fields_ = [(k, C.c_double) for k in (
+        "neigh_invDt", "neigh_attractDistance", "neigh_attractScaleForce", "neigh_damping",
+        "neigh_dampingRotation", "neigh_scaleE", "link_invDt", "link_damping", "link_dampingRotation",
+        "link_E", "link_W2", "link_W4", "link_G", "break_bendBreak", "break_maxLoad")]
+
+
 class HidemSurrogateConfig(C.Structure):
     _fields_ = [("hidden_layers", C.c_int32), ("width", C.c_int32), ("fourier_bands", C.c_int32),
                 ("batch", C.c_int32), ("learning_rate", C.c_double), ("seed", C.c_uint64),
@@ -253,6 +260,8 @@ _PROTOS = [
     ("hidem_set_external_force_maps", C.c_int, [C.c_void_p, C.POINTER(HidemMap2d)]),
     ("hidem_kinetic_energy", C.c_int, [C.c_void_p, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)]),
     ("hidem_momentum", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("hidem_set_functor_params", C.c_int, [C.c_void_p, C.POINTER(HidemFunctorParams)]),
+    ("hidem_get_functor_params", C.c_int, [C.c_void_p, C.POINTER(HidemFunctorParams)]),
     ("hidem_set_collision_mesh", C.c_int, [C.c_void_p, C.POINTER(HidemMesh)]),
     ("hidem_get_mesh_face_forces", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("hidem_zero_mesh_face_forces", C.c_int, [C.c_void_p]),

@@ -11,6 +11,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "kernels.h"
@@ -215,6 +216,10 @@ void derive(const hidem_params &P, Consts<LP> &c, double &searchDistance, double
     c.G = (LP)((double)E / 2.0);
     c.bendBreak = (LP)P.bendBreak;
     c.maxLoad = (LP)P.maxLoad;
+    c.linkInvDt = c.invDt;
+    c.linkDamping = c.damping;
+    c.linkDampingRotation = c.dampingRotation;
+    c.mainInvDt = c.invDt;
     c.dt = dt;
     c.invDt2 = (LP)(1.0 / (2.0 * (double)dt));
     c.dtSqr = (LP)std::pow((double)dt, 2.0);
@@ -1950,6 +1955,58 @@ hidem_status hidem_kinetic_energy(hidem_ctx *ctx, double *translational, double 
     if (translational) *translational = h[0];
     if (rotational) *rotational = h[1];
     if (max_speed) *max_speed = std::sqrt(h[2]);
+    return HIDEM_OK;
+}
+
+hidem_status hidem_set_functor_params(hidem_ctx *ctx, const hidem_functor_params *f) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!f) return fail(ctx, HIDEM_ERR_ARG, "functor parameters are NULL");
+    auto set = [&](auto &c) {
+        using LP = std::decay_t<decltype(c.invDt)>;
+        c.invDt = (LP)f->neigh_invDt;
+        c.attractDistance = (LP)f->neigh_attractDistance;
+        c.attractScaleForce = (LP)f->neigh_attractScaleForce;
+        c.damping = (LP)f->neigh_damping;
+        c.dampingRotation = (LP)f->neigh_dampingRotation;
+        c.scaleE = (LP)f->neigh_scaleE;
+        c.linkInvDt = (LP)f->link_invDt;
+        c.linkDamping = (LP)f->link_damping;
+        c.linkDampingRotation = (LP)f->link_dampingRotation;
+        c.E = (LP)f->link_E;
+        c.W2 = (LP)f->link_W2;
+        c.W4 = (LP)f->link_W4;
+        c.G = (LP)f->link_G;
+        c.bendBreak = (LP)f->break_bendBreak;
+        c.maxLoad = (LP)f->break_maxLoad;
+    };
+    set(ctx->cf);
+    set(ctx->cd);
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_functor_params(hidem_ctx *ctx, hidem_functor_params *out) {
+    if (!ctx || !out) return HIDEM_ERR_ARG;
+    auto get = [&](const auto &c) {
+        out->neigh_invDt = (double)c.invDt;
+        out->neigh_attractDistance = (double)c.attractDistance;
+        out->neigh_attractScaleForce = (double)c.attractScaleForce;
+        out->neigh_damping = (double)c.damping;
+        out->neigh_dampingRotation = (double)c.dampingRotation;
+        out->neigh_scaleE = (double)c.scaleE;
+        out->link_invDt = (double)c.linkInvDt;
+        out->link_damping = (double)c.linkDamping;
+        out->link_dampingRotation = (double)c.linkDampingRotation;
+        out->link_E = (double)c.E;
+        out->link_W2 = (double)c.W2;
+        out->link_W4 = (double)c.W4;
+        out->link_G = (double)c.G;
+        out->break_bendBreak = (double)c.bendBreak;
+        out->break_maxLoad = (double)c.maxLoad;
+    };
+    if (ctx->mixed)
+        get(ctx->cf);
+    else
+        get(ctx->cd);
     return HIDEM_OK;
 }
 

@@ -83,12 +83,13 @@ template <class LP>
 struct Consts {
     // HiDEMDefNeighForceFunc
     LP invDt, attractDistance, attractScaleForce, damping, dampingRotation, scaleE;
-    // HiDEMDefLinkForceFunc
-    LP E, W2, W4, G;
+    // HiDEMDefLinkForceFunc (its own invDt / damping / dampingRotation: a caller's main
+    // may construct the two functors with different values)
+    LP linkInvDt, linkDamping, linkDampingRotation, E, W2, W4, G;
     // HiDEMDefLinkBreakFunc
     LP bendBreak, maxLoad;
-    // integrate
-    LP dt, invDt2, dtSqr, invDtSqr, g, lift, rhoIce, rhoWater, waterLevel;
+    // integrate (mainInvDt: the sample main's invDt, used by the velocity limit)
+    LP mainInvDt, dt, invDt2, dtSqr, invDtSqr, g, lift, rhoIce, rhoWater, waterLevel;
     LP airDrag, waterDrag, bedDrag, bedFriction, bedHeight, bedInteract, bedStiffness, scale;
     LP maxVel, maxRot, breakTime;
     double lower[3], upper[3];

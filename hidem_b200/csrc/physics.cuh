@@ -77,12 +77,12 @@ template <class LP>
 __device__ __forceinline__ void beam_terms(const Consts<LP> &c, LP mask, LP xDist, LP yDist,
                                            LP zDist, const LP *s, const LP *o, LP *CT, LP *dp,
                                            LP *ct) {
-    dp[0] = (-c.damping * ((s[0] - o[0]) * c.invDt)) * mask;
-    dp[1] = (-c.damping * ((s[1] - o[1]) * c.invDt)) * mask;
-    dp[2] = (-c.damping * ((s[2] - o[2]) * c.invDt)) * mask;
-    dp[3] = (-c.dampingRotation * ((s[3] - o[3]) * c.invDt)) * mask;
-    dp[4] = (-c.dampingRotation * ((s[4] - o[4]) * c.invDt)) * mask;
-    dp[5] = (-c.dampingRotation * ((s[5] - o[5]) * c.invDt)) * mask;
+    dp[0] = (-c.linkDamping * ((s[0] - o[0]) * c.linkInvDt)) * mask;
+    dp[1] = (-c.linkDamping * ((s[1] - o[1]) * c.linkInvDt)) * mask;
+    dp[2] = (-c.linkDamping * ((s[2] - o[2]) * c.linkInvDt)) * mask;
+    dp[3] = (-c.linkDampingRotation * ((s[3] - o[3]) * c.linkInvDt)) * mask;
+    dp[4] = (-c.linkDampingRotation * ((s[4] - o[4]) * c.linkInvDt)) * mask;
+    dp[5] = (-c.linkDampingRotation * ((s[5] - o[5]) * c.linkInvDt)) * mask;
 
     LP xDist2 = xDist * xDist;
     LP yDist2 = yDist * yDist;
@@ -416,10 +416,10 @@ __device__ __forceinline__ void integrate_particle(const Consts<LP> &c, PRec<LP>
     zTheta = zTheta + wDN;
 
     if (c.useVel) {
-        const LP xVel = xDN * c.invDt, yVel = yDN * c.invDt, zVel = zDN * c.invDt;
-        const LP xTV = (xTheta - xThPrev) * c.invDt;
-        const LP yTV = (yTheta - yThPrev) * c.invDt;
-        const LP zTV = (zTheta - zThPrev) * c.invDt;
+        const LP xVel = xDN * c.mainInvDt, yVel = yDN * c.mainInvDt, zVel = zDN * c.mainInvDt;
+        const LP xTV = (xTheta - xThPrev) * c.mainInvDt;
+        const LP yTV = (yTheta - yThPrev) * c.mainInvDt;
+        const LP zTV = (zTheta - zThPrev) * c.mainInvDt;
         if (xVel > c.maxVel) xCord = (double)(c.dt * c.maxVel) + xPrev;
         if (yVel > c.maxVel) yCord = (double)(c.dt * c.maxVel) + yPrev;
         if (zVel > c.maxVel) zCord = (double)(c.dt * c.maxVel) + zPrev;

@@ -154,6 +154,16 @@ class HiDEMLib:
         """The MeshAccel grid: counts, lower, upper, sizes, starts, values."""
         return _mesh_accel(lambda *a: self._check(self._lib.hidem_get_mesh_accel(self._ctx, *a)))
 
+    def functor_params(self) -> abi.HidemFunctorParams:
+        """The default functors' parameters in use (derived from the run config unless set)."""
+        f = abi.HidemFunctorParams()
+        self._check(self._lib.hidem_get_functor_params(self._ctx, C.byref(f)))
+        return f
+
+    def set_functor_params(self, f: abi.HidemFunctorParams) -> None:
+        """Replaces the default functors' parameters (as a caller's main constructs them)."""
+        self._check(self._lib.hidem_set_functor_params(self._ctx, C.byref(f)))
+
     def momentum(self) -> tuple[np.ndarray, np.ndarray]:
         """(linear [3], angular about the origin [3]) momentum of the current state."""
         lin, ang = np.zeros(3), np.zeros(3)

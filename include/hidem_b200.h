@@ -188,6 +188,23 @@ hidem_status hidem_finalize_ts(hidem_ctx *ctx);
  * gridService, forces, integrate, gated link update, finalizeTs — as one fused
  * kernel per step, graph-launched between rebuild checks. */
 hidem_status hidem_step(hidem_ctx *ctx, int32_t nsteps);
+/* The default functors as a caller's main constructs them (HiDEM/Common/
+ * HiDEMDefaultFunctions.h): HiDEMDefNeighForceFunc(invDt, attractDistance,
+ * attractScaleForce, damping, dampingRotation, scaleE) (21-87), HiDEMDefLinkForceFunc(invDt,
+ * damping, dampingRotation, E, W2, W4, G) (90-204), HiDEMDefLinkBreakFunc(bendBreak,
+ * maxLoad) (207-242). Values are lp (each double is rounded once to float in
+ * HIDEM_PREC_MIXED). hidem_create / hidem_set_params derive them from the run config as the
+ * MeshBlock sample does (MainMeshBlock.cpp:106-156); hidem_set_functor_params replaces them
+ * (until the next hidem_set_params), hidem_get_functor_params reads the ones in use. The
+ * integrate step keeps the run config's constants. */
+typedef struct hidem_functor_params {
+    double neigh_invDt, neigh_attractDistance, neigh_attractScaleForce;
+    double neigh_damping, neigh_dampingRotation, neigh_scaleE;
+    double link_invDt, link_damping, link_dampingRotation, link_E, link_W2, link_W4, link_G;
+    double break_bendBreak, break_maxLoad;
+} hidem_functor_params;
+hidem_status hidem_set_functor_params(hidem_ctx *ctx, const hidem_functor_params *f);
+hidem_status hidem_get_functor_params(hidem_ctx *ctx, hidem_functor_params *out);
 /* Blocks until the context's stream is idle; reports device-side check failures. */
 hidem_status hidem_synchronize(hidem_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work

@@ -22,6 +22,19 @@ struct Error : std::runtime_error {
     Error(hidem_status s, const std::string &what) : std::runtime_error(what), status(s) {}
 };
 
+// The default functors' parameters, constructed as a caller's main constructs the
+// reference's functors (HiDEM/Common/HiDEMDefaultFunctions.h); passing them to
+// computePartForce / linkUpdate makes the library use them (hidem_set_functor_params).
+struct NeighForceFunc {  // HiDEMDefNeighForceFunc
+    double invDt, attractDistance, attractScaleForce, damping, dampingRotation, scaleE;
+};
+struct LinkForceFunc {  // HiDEMDefLinkForceFunc
+    double invDt, damping, dampingRotation, E, W2, W4, G;
+};
+struct LinkBreakFunc {  // HiDEMDefLinkBreakFunc
+    double bendBreak, maxLoad;
+};
+
 class HiDEMLibB200 {
 public:
     explicit HiDEMLibB200(const hidem_params &p, int device = 0) : params_(p) {
@@ -40,8 +53,35 @@ public:
     // HiDEMLib::gridService / computePartForce / applyForce / linkUpdate / finalizeTs
     void gridService() { check(hidem_grid_service(ctx_)); }
     void computePartForce() { check(hidem_compute_forces(ctx_)); }
+    void computePartForce(const NeighForceFunc &n, const LinkForceFunc &l) {
+        hidem_functor_params f;
+        check(hidem_get_functor_params(ctx_, &f));
+        f.neigh_invDt = n.invDt;
+        f.neigh_attractDistance = n.attractDistance;
+        f.neigh_attractScaleForce = n.attractScaleForce;
+        f.neigh_damping = n.damping;
+        f.neigh_dampingRotation = n.dampingRotation;
+        f.neigh_scaleE = n.scaleE;
+        f.link_invDt = l.invDt;
+        f.link_damping = l.damping;
+        f.link_dampingRotation = l.dampingRotation;
+        f.link_E = l.E;
+        f.link_W2 = l.W2;
+        f.link_W4 = l.W4;
+        f.link_G = l.G;
+        check(hidem_set_functor_params(ctx_, &f));
+        check(hidem_compute_forces(ctx_));
+    }
     void applyForce() { check(hidem_integrate(ctx_)); }
     void linkUpdate() { check(hidem_link_update(ctx_)); }
+    void linkUpdate(const LinkBreakFunc &b) {
+        hidem_functor_params f;
+        check(hidem_get_functor_params(ctx_, &f));
+        f.break_bendBreak = b.bendBreak;
+        f.break_maxLoad = b.maxLoad;
+        check(hidem_set_functor_params(ctx_, &f));
+        check(hidem_link_update(ctx_));
+    }
     void finalizeTs() { check(hidem_finalize_ts(ctx_)); }
     // n whole timesteps of the sample main loop, one fused kernel per step
     void step(int32_t n) { check(hidem_step(ctx_, n)); }

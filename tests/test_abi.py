@@ -113,6 +113,11 @@ int main() {
         lib.setBedMaps(nullptr, nullptr);
         lib.setCollisionMesh(nullptr);
         lib.setStepKernel(HIDEM_STEP_KERNEL_AUTO);
+        if (lib.getStats().num_particles > 0) {
+            lib.computePartForce(hidem::NeighForceFunc{1e4, 0, 0, 1, 1, 1e9},
+                                 hidem::LinkForceFunc{1e4, 1, 1, 1e9, 1, 1, 5e8});
+            lib.linkUpdate(hidem::LinkBreakFunc{0.01, 5e-4});
+        }
         double kt = 0, kr = 0, vm = 0;
         if (lib.getStats().num_particles > 0) lib.kineticEnergy(kt, kr, vm);
     } catch (const hidem::Error &e) {

@@ -532,3 +532,44 @@ def test_mixed_against_fp64_every_output(gpu):
     assert np.all(np.abs(ea - eb) <= 1e-3 * eb)
     assert np.linalg.norm(lina - linb) <= 1e-3 * np.linalg.norm(linb)
     assert np.linalg.norm(anga - angb) <= 1e-3 * np.linalg.norm(angb)
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_functor_params_set_by_the_caller(gpu, precision):
+    """A context whose run config differs in the functors' inputs (damping, E, beam width,
+    attraction, break thresholds) but is given the first context's functor parameters
+    (as a caller's main constructs the functors) steps bit-identically to it, fused and
+    split; the getter returns what was set."""
+    over = dict(seed=5, breakTime=0.0, attractDistance=0.02, attractScaleForce=0.2)
+    P1, p, l = workloads.ice_block(cells=(5, 4, 4), precision=precision, **over)
+    P2, _, _ = workloads.ice_block(cells=(5, 4, 4), precision=precision, **over)
+    P2.damping *= 2.0
+    P2.dampingRotation *= 3.0
+    P2.E *= 1.5
+    P2.beamWidth *= 1.1
+    P2.attractScaleForce *= 2.0
+    P2.maxLoad *= 2.0
+    P2.bendBreak *= 0.5
+    for mode in ("fused", "split"):
+        a = HiDEMLib(P1)
+        f = a.functor_params()
+        b = HiDEMLib(P2)
+        assert b.functor_params().neigh_damping != f.neigh_damping
+        b.set_functor_params(f)
+        g = b.functor_params()
+        assert all(getattr(g, k) == getattr(f, k) for k, _ in abi.HidemFunctorParams._fields_)
+        outs = []
+        for lib in (a, b):
+            lib.set_particles(p)
+            lib.set_links(l)
+            if mode == "fused":
+                lib.step(30)
+            else:
+                for _ in range(30):
+                    lib.timestep_split()
+            outs.append((lib.get_particles(), lib.get_links()))
+            lib.close()
+        for k in P_OUT:
+            assert np.array_equal(outs[0][0][k], outs[1][0][k]), (mode, k)
+        for k in L_OUT:
+            assert np.array_equal(outs[0][1][k], outs[1][1][k]), (mode, k)
