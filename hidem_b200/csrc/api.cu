@@ -1304,12 +1304,12 @@ hidem_status hidem_create(const hidem_params *params, int device, hidem_ctx **ou
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smCount, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) {
-        // the contexts' buffers come from the device's default stream-ordered pool: keep
-        // freed blocks for reuse (later contexts, regrown buffers) instead of returning them
-        // to the driver at every synchronisation
+        // the contexts' buffers come from the device's default stream-ordered pool: keep up
+        // to 8 GiB of freed blocks for reuse (later contexts, regrown buffers) instead of
+        // returning them to the driver at every synchronisation
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-            uint64_t keep = UINT64_MAX;
+            uint64_t keep = 8ull << 30;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
