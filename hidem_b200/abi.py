@@ -13,6 +13,8 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "libhidem_b200.so"
 
 HIDEM_OK = 0
+HIDEM_ERR_ARG, HIDEM_ERR_CUDA, HIDEM_ERR_STATE, HIDEM_ERR_CAPACITY = 1, 2, 3, 4
+HIDEM_ERR_IO, HIDEM_ERR_DEVICE, HIDEM_ERR_NOT_FOUND = 5, 6, 7
 STATUS_NAMES = {0: "HIDEM_OK", 1: "HIDEM_ERR_ARG", 2: "HIDEM_ERR_CUDA", 3: "HIDEM_ERR_STATE",
                 4: "HIDEM_ERR_CAPACITY", 5: "HIDEM_ERR_IO", 6: "HIDEM_ERR_DEVICE",
                 7: "HIDEM_ERR_NOT_FOUND"}

@@ -4,6 +4,8 @@ precisions, in the fused step and in the split operator calls; edge cases; and
 size-independent properties at the full slab size."""
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -573,3 +575,34 @@ def test_functor_params_set_by_the_caller(gpu, precision):
             assert np.array_equal(outs[0][0][k], outs[1][0][k]), (mode, k)
         for k in L_OUT:
             assert np.array_equal(outs[0][1][k], outs[1][1][k]), (mode, k)
+
+
+def test_new_entry_points_report_errors(gpu):
+    """Status codes of the collision-mesh, functor-parameter and diagnostic entry points on
+    bad input or out of order (no exits, the context stays usable)."""
+    from hidem_b200.abi import load
+    lib_ = load()
+    P, p, l = workloads.ice_block(cells=(3, 3, 3), precision=abi.PREC_MIXED, seed=2)
+    lib = HiDEMLib(P)
+    h = lib._ctx
+    assert lib_.hidem_get_mesh_face_forces(h, None, None, None) == abi.HIDEM_ERR_STATE
+    assert lib_.hidem_zero_mesh_face_forces(h) == abi.HIDEM_ERR_STATE
+    assert lib_.hidem_momentum(h, None, None) == abi.HIDEM_ERR_STATE  # no particles yet
+    assert lib_.hidem_set_functor_params(h, None) == abi.HIDEM_ERR_ARG
+    bad = abi.HidemMesh()
+    bad.triangles = 0
+    assert lib_.hidem_set_collision_mesh(h, C.byref(bad)) == abi.HIDEM_ERR_ARG
+    v = np.zeros((1, 3, 3))
+    v[0, 1, 0] = 1.0
+    v[0, 2, 1] = 1.0
+    m, keep = abi.mesh(v, [[0.0, 0.0, -1.0]], 0.0, abi.PREC_MIXED)
+    assert lib_.hidem_set_collision_mesh(h, C.byref(m)) == abi.HIDEM_ERR_ARG  # cell size 0
+    m, keep = abi.mesh(v, [[0.0, 0.0, -1.0]], 1.0, abi.PREC_MIXED)
+    assert lib_.hidem_set_collision_mesh(h, C.byref(m)) == abi.HIDEM_OK
+    lib.set_collision_mesh(None)
+    # the context still steps after the refused calls
+    lib.set_particles(p)
+    lib.set_links(l)
+    lib.step(5)
+    assert lib.stats()["step"] == 5
+    lib.close()
