@@ -59,6 +59,7 @@ def parse():
                     help="settle: the surrogate's inputs (lattice neighbourhood, or 5 coordinates)")
     ap.add_argument("--test-tongues", type=int, default=16, help="settle: held-out geometries")
     ap.add_argument("--train-steps", type=int, default=20000, help="settle: surrogate Adam steps")
+    ap.add_argument("--tongue", default="40,12", help="settle: tongue plan size in metres x,y")
     ap.add_argument("--blocks", type=int, default=256, help="ensemble: number of blocks")
     ap.add_argument("--no-graphs", action="store_true", help="ensemble: plain launches")
     ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped", "thread-async"],
@@ -470,7 +471,8 @@ def main_settle(args):
     if rank != 0:
         return
     torch.cuda.set_device(local)
-    size, thick, amp = (40.0, 12.0), 6.0, 2.0
+    size = tuple(float(v) for v in args.tongue.split(","))
+    thick, amp = 6.0, 2.0
     rep = settle.warm_start_experiment(n_train=args.train_tongues, n_test=args.test_tongues, size=size,
                                        base_thickness=thick, amplitude=amp, train_steps=args.train_steps,
                                        inputs=args.surrogate_inputs)
