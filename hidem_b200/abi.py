@@ -244,6 +244,13 @@ _PROTOS = [
     ("hidem_link_update", C.c_int, [C.c_void_p]),
     ("hidem_finalize_ts", C.c_int, [C.c_void_p]),
     ("hidem_step", C.c_int, [C.c_void_p, C.c_int32]),
+    ("hidem_grid_service_local", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_i32)]),
+    ("hidem_grid_service_decide", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_i32)]),
+    ("hidem_local_bounds", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("hidem_regenerate_frame", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("hidem_set_halo_exchange", C.c_int, [C.c_void_p, C.c_void_p, _i64, C.c_void_p, _i64]),
+    ("hidem_pack_halo_forces", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("hidem_unpack_halo_forces", C.c_int, [C.c_void_p, C.c_void_p]),
     ("hidem_synchronize", C.c_int, [C.c_void_p]),
     ("hidem_get_stream", C.c_void_p, [C.c_void_p]),
     ("hidem_profile", C.c_int, [C.c_void_p, C.c_int32]),

@@ -141,6 +141,13 @@ struct hidem_ctx {
     bool meshSet = false;
     MeshView<float> meshF{};
     MeshView<double> meshD{};
+
+    // slab decomposition: a grid box given for the next rebuild, and the halo force lists
+    // (particle indices in input order)
+    bool frameOnce = false;
+    double frame[6] = {};
+    int32_t *haloSend = nullptr, *haloRecv = nullptr;
+    long long nHaloSend = 0, nHaloRecv = 0;
 };
 
 namespace {
@@ -391,6 +398,13 @@ hidem_status rebuild(hidem_ctx *ctx) {
     CK(cudaStreamSynchronize(st));
     if (!(b[0] <= b[3] && b[1] <= b[4] && b[2] <= b[5]))
         return fail(ctx, HIDEM_ERR_DEVICE, "non-finite particle coordinates");
+    if (ctx->frameOnce) {
+        // the box spanning every rank's particles (hidem_regenerate_frame)
+        const double *f = ctx->frame;
+        if (!(f[0] <= b[0] && f[1] <= b[1] && f[2] <= b[2] && b[3] <= f[3] && b[4] <= f[4] && b[5] <= f[5]))
+            return fail(ctx, HIDEM_ERR_ARG, "particles outside the given grid box");
+        std::memcpy(b, f, sizeof b);
+    }
 
     // 2. grid (NeighbourGrid::generateNeighbourGrid, NeighbourGrid.cpp:72-114)
     GridInfo &g = ctx->grid;
@@ -508,29 +522,46 @@ hidem_status do_rebuild(hidem_ctx *ctx) {
 // max over particles of max(0, x/y/zDiff) -> accumulated displacement
 // (HiDEMLib::accumulateDist, HiDEMLib.h:463-474), from three device words.
 template <class LP>
-double curr_dist(const unsigned long long w[3]) {
-    LP m[3];
+void diff_words(const unsigned long long w[3], double out[3]) {
     for (int k = 0; k < 3; ++k) {
         if (sizeof(LP) == 4) {
             uint32_t u = (uint32_t)w[k];
             float f;
             std::memcpy(&f, &u, 4);
-            m[k] = (LP)f;
+            out[k] = (double)f;
         } else {
-            double d;
-            std::memcpy(&d, &w[k], 8);
-            m[k] = (LP)d;
+            std::memcpy(&out[k], &w[k], 8);
         }
     }
+}
+
+// the maxima are lp values held in doubles (exactly)
+template <class LP>
+double curr_dist(const double mx[3]) {
+    const LP m[3] = {(LP)mx[0], (LP)mx[1], (LP)mx[2]};
     LP root = std::sqrt((m[0] * m[0]) + (m[1] * m[1]) + (m[2] * m[2]));
     return (double)((LP)10 * root);
 }
 
-hidem_status read_diff_max(hidem_ctx *ctx, double *currDist) {
+double curr_dist_of(const hidem_ctx *ctx, const double mx[3]) {
+    return ctx->mixed ? curr_dist<float>(mx) : curr_dist<double>(mx);
+}
+
+hidem_status read_diff_words(hidem_ctx *ctx, double mx[3]) {
     unsigned long long w[3];
     CK(cudaMemcpyAsync(w, ctx->diffMax, sizeof w, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    *currDist = ctx->mixed ? curr_dist<float>(w) : curr_dist<double>(w);
+    if (ctx->mixed)
+        diff_words<float>(w, mx);
+    else
+        diff_words<double>(w, mx);
+    return HIDEM_OK;
+}
+
+hidem_status read_diff_max(hidem_ctx *ctx, double *currDist) {
+    double mx[3];
+    TRY(read_diff_words(ctx, mx));
+    *currDist = curr_dist_of(ctx, mx);
     return HIDEM_OK;
 }
 
@@ -1135,7 +1166,9 @@ hidem_status batch_run(hidem_batch *b, int nsteps) {
             for (int idx = 0; idx < nc; ++idx) {
                 hidem_ctx *c = b->ctxs[idx];
                 if (!gs_due(c)) continue;
-                const double cd = gs_wants_diff(c) ? curr_dist<LP>(b->diffHost + 3 * idx) : 0.0;
+                double mx[3] = {0.0, 0.0, 0.0};
+                if (gs_wants_diff(c)) diff_words<LP>(b->diffHost + 3 * idx, mx);
+                const double cd = gs_wants_diff(c) ? curr_dist<LP>(mx) : 0.0;
                 if (gs_decide(c, cd)) regen.push_back(idx);
             }
             if (!regen.empty()) TRY(batch_rebuild(b, regen, bind.streams));
@@ -1398,6 +1431,8 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->meshQValues);
     dfree(ctx->meshKeep);
     dfree(ctx->energyBuf);
+    dfree(ctx->haloSend);
+    dfree(ctx->haloRecv);
     for (cudaEvent_t e : ctx->tuneEv)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1471,6 +1506,8 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     ctx->maxParticleRadius = -1.0;  // found on the device when a collision mesh needs it
     TRY(prune_mesh(ctx));
     ctx->startStep = ctx->step;
+    // halo lists refer to particle indices of the previous particle set
+    ctx->nHaloSend = ctx->nHaloRecv = 0;
     // a link set refers to particle indices of the previous particle set
     ctx->haveLinks = false;
     ctx->L = 0;
@@ -1669,6 +1706,122 @@ hidem_status hidem_finalize_ts(hidem_ctx *ctx) {
     if (!ctx) return HIDEM_ERR_ARG;
     ctx->step += 1;
     return HIDEM_OK;
+}
+
+hidem_status hidem_grid_service_local(hidem_ctx *ctx, double diff_max[3], int32_t *needs_reduce) {
+    if (!ctx || !diff_max || !needs_reduce) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    CK(cudaSetDevice(ctx->device));
+    diff_max[0] = diff_max[1] = diff_max[2] = 0.0;
+    *needs_reduce = gs_wants_diff(ctx) ? 1 : 0;
+    if (*needs_reduce) {
+        TRY(reduce_diff_now(ctx));
+        TRY(read_diff_words(ctx, diff_max));
+    }
+    return HIDEM_OK;
+}
+
+hidem_status hidem_grid_service_decide(hidem_ctx *ctx, const double diff_max[3], int32_t *regen) {
+    if (!ctx || !diff_max || !regen) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    for (int k = 0; k < 3; ++k)
+        if (!(diff_max[k] >= 0.0) || std::isinf(diff_max[k]))
+            return fail(ctx, HIDEM_ERR_ARG, "diff_max[%d] = %g is not a finite maximum of max(0, diff)", k, diff_max[k]);
+    const double cd = gs_wants_diff(ctx) ? curr_dist_of(ctx, diff_max) : 0.0;
+    *regen = gs_decide(ctx, cd) ? 1 : 0;
+    return HIDEM_OK;
+}
+
+hidem_status hidem_local_bounds(hidem_ctx *ctx, double lower[3], double upper[3]) {
+    if (!ctx || !lower || !upper) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    CK(cudaSetDevice(ctx->device));
+    const long long n = ctx->n;
+    const int nbB = (int)std::min<long long>(std::max<long long>(1, (n + 255) / 256), 4 * ctx->smCount);
+    if (ctx->mixed)
+        launch_bounds<float>(recp<float>(ctx, ctx->cur), (int)n, ctx->boundsPartial, nbB, ctx->boundsOut, ctx->stream);
+    else
+        launch_bounds<double>(recp<double>(ctx, ctx->cur), (int)n, ctx->boundsPartial, nbB, ctx->boundsOut, ctx->stream);
+    ctx->launches += 2;
+    double b[6];
+    CK(cudaMemcpyAsync(b, ctx->boundsOut, sizeof b, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 3; ++k) {
+        lower[k] = b[k];
+        upper[k] = b[3 + k];
+    }
+    return HIDEM_OK;
+}
+
+hidem_status hidem_regenerate_frame(hidem_ctx *ctx, const double lower[3], const double upper[3]) {
+    if (!ctx || !lower || !upper) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    for (int k = 0; k < 3; ++k)
+        if (!(lower[k] <= upper[k]) || std::isinf(lower[k]) || std::isinf(upper[k]))
+            return fail(ctx, HIDEM_ERR_ARG, "grid box axis %d is [%g, %g]", k, lower[k], upper[k]);
+    CK(cudaSetDevice(ctx->device));
+    for (int k = 0; k < 3; ++k) {
+        ctx->frame[k] = lower[k];
+        ctx->frame[3 + k] = upper[k];
+    }
+    ctx->accumulatedDist = 0;
+    ctx->frameOnce = true;
+    const hidem_status st = do_rebuild(ctx);
+    ctx->frameOnce = false;
+    return st;
+}
+
+hidem_status hidem_set_halo_exchange(hidem_ctx *ctx, const int32_t *send_index, int64_t n_send,
+                                     const int32_t *recv_index, int64_t n_recv) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    if (n_send < 0 || n_recv < 0 || (n_send > 0 && !send_index) || (n_recv > 0 && !recv_index))
+        return fail(ctx, HIDEM_ERR_ARG, "halo lists need non-negative counts and arrays");
+    const int32_t *lists[2] = {send_index, recv_index};
+    const int64_t counts[2] = {n_send, n_recv};
+    for (int w = 0; w < 2; ++w)
+        for (int64_t k = 0; k < counts[w]; ++k)
+            if (lists[w][k] < 0 || lists[w][k] >= ctx->n)
+                return fail(ctx, HIDEM_ERR_ARG, "%s_index[%lld] = %d is not a particle index (n = %lld)",
+                            w ? "recv" : "send", (long long)k, lists[w][k], ctx->n);
+    CK(cudaSetDevice(ctx->device));
+    ctx->nHaloSend = ctx->nHaloRecv = 0;
+    if (n_send > 0) {
+        TRY(dalloc(ctx, &ctx->haloSend, n_send));
+        CK(cudaMemcpyAsync(ctx->haloSend, send_index, 4 * (size_t)n_send, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (n_recv > 0) {
+        TRY(dalloc(ctx, &ctx->haloRecv, n_recv));
+        CK(cudaMemcpyAsync(ctx->haloRecv, recv_index, 4 * (size_t)n_recv, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->nHaloSend = n_send;
+    ctx->nHaloRecv = n_recv;
+    return HIDEM_OK;
+}
+
+static hidem_status halo_forces(hidem_ctx *ctx, void *buf, bool pack) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
+    const long long m = pack ? ctx->nHaloSend : ctx->nHaloRecv;
+    if (m > 0 && !buf) return fail(ctx, HIDEM_ERR_ARG, "null halo buffer");
+    CK(cudaSetDevice(ctx->device));
+    const int *index = pack ? ctx->haloSend : ctx->haloRecv;
+    if (ctx->mixed)
+        launch_halo_forces<float>(static_cast<float *>(ctx->force), ctx->slotOf, index, m, (int)ctx->n,
+                                  static_cast<float *>(buf), pack, ctx->stream);
+    else
+        launch_halo_forces<double>(static_cast<double *>(ctx->force), ctx->slotOf, index, m, (int)ctx->n,
+                                   static_cast<double *>(buf), pack, ctx->stream);
+    if (m > 0) ctx->launches += 1;
+    CK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
+hidem_status hidem_pack_halo_forces(hidem_ctx *ctx, void *device_out) { return halo_forces(ctx, device_out, true); }
+
+hidem_status hidem_unpack_halo_forces(hidem_ctx *ctx, const void *device_in) {
+    return halo_forces(ctx, const_cast<void *>(device_in), false);
 }
 
 hidem_status hidem_step(hidem_ctx *ctx, int32_t nsteps) {

@@ -1583,6 +1583,29 @@ __global__ void k_unpack_force(const LP *__restrict__ force, const int *__restri
     for (int q = 0; q < 6; ++q) out[(long long)q * n + i] = force[(long long)q * n + k];
 }
 
+// Halo force exchange of a slab decomposition (CommunicatorPacked::packAllCommData /
+// unpackAllCommData, HiDEMLib.h:337-372): one thread per (listed particle, component); the
+// buffer holds 6 values per particle so that each peer's records are one contiguous run.
+template <class LP>
+__global__ void k_pack_halo(const LP *__restrict__ force, const int *__restrict__ slotOf,
+                            const int *__restrict__ index, long long m, int n, LP *__restrict__ out) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6 * m) return;
+    const long long k = t / 6;
+    const int q = (int)(t - 6 * k);
+    out[t] = force[(long long)q * n + slotOf[index[k]]];
+}
+
+template <class LP>
+__global__ void k_unpack_halo(const LP *__restrict__ in, const int *__restrict__ slotOf,
+                              const int *__restrict__ index, long long m, int n, LP *__restrict__ force) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6 * m) return;
+    const long long k = t / 6;
+    const int q = (int)(t - 6 * k);
+    force[(long long)q * n + slotOf[index[k]]] = in[t];
+}
+
 // per-particle number of link ends
 __global__ void k_link_degree(const int *__restrict__ A, const int *__restrict__ B, long long L,
                               int *__restrict__ deg) {
@@ -1726,6 +1749,15 @@ template <class LP>
 void launch_unpack_force(const LP *force, const int *orig, int n, LP *out, cudaStream_t st) {
     k_unpack_force<LP><<<nblk(n, 256), 256, 0, st>>>(force, orig, n, out);
 }
+template <class LP>
+void launch_halo_forces(LP *force, const int *slotOf, const int *index, long long m, int n, LP *buf,
+                        bool pack, cudaStream_t st) {
+    if (m <= 0) return;
+    if (pack)
+        k_pack_halo<LP><<<nblk(6 * m, 256), 256, 0, st>>>(force, slotOf, index, m, n, buf);
+    else
+        k_unpack_halo<LP><<<nblk(6 * m, 256), 256, 0, st>>>(buf, slotOf, index, m, n, force);
+}
 void launch_link_lists(const int *A, const int *B, long long L, int n, int *deg, int *start,
                        int *cursor, int *sums, int *plLink, uint8_t *plEnd, cudaStream_t st) {
     if (L > 0) k_link_degree<<<nblk(L, 256), 256, 0, st>>>(A, B, L, deg);
@@ -1749,6 +1781,8 @@ void launch_gather_sides(const int *sideSlot, long long L, const LP *ct, LP *out
     template void launch_unpack_records<LP>(const PRec<LP> *, const int *, int, const SoaIn<LP> &,  \
                                             cudaStream_t);                                         \
     template void launch_unpack_force<LP>(const LP *, const int *, int, LP *, cudaStream_t);       \
+    template void launch_halo_forces<LP>(LP *, const int *, const int *, long long, int, LP *, bool, \
+                                         cudaStream_t);                                            \
     template void launch_gather_sides<LP>(const int *, long long, const LP *, LP *,                \
                                           const uint8_t *, uint8_t *, cudaStream_t);
 HIDEM_INSTANTIATE_IO(float)

@@ -56,6 +56,11 @@ void launch_unpack_records(const PRec<LP> *rec, const int *orig, int n, const So
                            cudaStream_t st);
 template <class LP>
 void launch_unpack_force(const LP *force, const int *orig, int n, LP *out, cudaStream_t st);
+// pack: buf[6k + q] = force of particle index[k] (input order), component q;
+// unpack: the reverse, overwriting those forces
+template <class LP>
+void launch_halo_forces(LP *force, const int *slotOf, const int *index, long long m, int n, LP *buf,
+                        bool pack, cudaStream_t st);
 // per-particle link-end lists (ascending link index) from the link ends A, B;
 // deg and cursor hold n+1 zeros on entry; sums >= (n+1)/1024 + 1 elements
 void launch_link_lists(const int *A, const int *B, long long L, int n, int *deg, int *start,

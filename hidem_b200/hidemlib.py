@@ -24,6 +24,7 @@ class HiDEMLib:
         self._lib = abi.load()
         self.params = params
         self._mesh_tris = 0
+        self.device = int(device)
         self.precision = int(params.precision)
         self.lp = abi.lp_dtype(self.precision)
         h = C.c_void_p()
@@ -124,6 +125,45 @@ class HiDEMLib:
 
     def step(self, nsteps: int = 1) -> None:
         self._check(self._lib.hidem_step(self._ctx, int(nsteps)))
+
+    # ------------------------------------------------------------ slab decomposition hooks
+    def grid_service_local(self) -> tuple[np.ndarray, bool]:
+        """This rank's maxima of max(0, x/y/zDiff) and whether gridService reads them now."""
+        mx = np.zeros(3)
+        wants = C.c_int32()
+        self._check(self._lib.hidem_grid_service_local(self._ctx, mx.ctypes.data, C.byref(wants)))
+        return mx, bool(wants.value)
+
+    def grid_service_decide(self, diff_max) -> bool:
+        """gridService's decision from the maxima over all ranks; True: rebuild now."""
+        mx = np.ascontiguousarray(diff_max, np.float64)
+        regen = C.c_int32()
+        self._check(self._lib.hidem_grid_service_decide(self._ctx, mx.ctypes.data, C.byref(regen)))
+        return bool(regen.value)
+
+    def local_bounds(self) -> tuple[np.ndarray, np.ndarray]:
+        lo, hi = np.zeros(3), np.zeros(3)
+        self._check(self._lib.hidem_local_bounds(self._ctx, lo.ctypes.data, hi.ctypes.data))
+        return lo, hi
+
+    def regenerate_frame(self, lower, upper) -> None:
+        """Rebuild with the grid spanning [lower, upper] (every rank's particles)."""
+        lo = np.ascontiguousarray(lower, np.float64)
+        hi = np.ascontiguousarray(upper, np.float64)
+        self._check(self._lib.hidem_regenerate_frame(self._ctx, lo.ctypes.data, hi.ctypes.data))
+
+    def set_halo_exchange(self, send_index, recv_index) -> None:
+        """Particle indices (input order) whose forces are sent / received each step."""
+        snd = np.ascontiguousarray(send_index, np.int32)
+        rcv = np.ascontiguousarray(recv_index, np.int32)
+        self._check(self._lib.hidem_set_halo_exchange(self._ctx, snd.ctypes.data, snd.shape[0],
+                                                      rcv.ctypes.data, rcv.shape[0]))
+
+    def pack_halo_forces(self, device_ptr: int) -> None:
+        self._check(self._lib.hidem_pack_halo_forces(self._ctx, C.c_void_p(device_ptr)))
+
+    def unpack_halo_forces(self, device_ptr: int) -> None:
+        self._check(self._lib.hidem_unpack_halo_forces(self._ctx, C.c_void_p(device_ptr)))
 
     def set_bed_maps(self, bed=None, friction=None) -> None:
         """GlacierDem bed height / friction maps (abi.map2d structs, or None)."""

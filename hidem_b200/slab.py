@@ -1,0 +1,385 @@
+"""Slab decomposition of one particle set over ranks, one context per rank.
+
+What the reference does with MPI (HiDEMLib/HiDEMDistribution.h:99-234): each rank owns
+the particles inside its domain, holds halo copies of the other ranks' particles within a
+halo distance of it (ParticleTransporter.h:114-130, ``Domain::withinHalo``) and of the
+links that touch its own particles (LinkTransporter.h), computes the forces of its own
+particles, receives the forces of its halo particles from their owners and integrates
+both (``computePartForce``, HiDEMLib.h:316-382, the ``pForceComm`` exchange of 6 force
+components), so that halo copies stay identical to their originals; gridService reduces
+the displacement over ranks (``accumulateDist``, HiDEMLib.h:463-474) and, when the
+domains are rebalanced, particles move to their new owners with their link-side state
+(``syncLinkSideData`` + ``reDistribute``, HiDEMDistribution.h:59-98, 188-234).
+
+Here the domains are slabs along x with count-balanced cuts (the reference's
+``DomainBuilder::generateBalancedDomains`` in one dimension with unit weights), recut at
+every rebuild of the neighbour structures. Two choices differ from the reference so that
+a decomposed run is bit-identical to one context holding every particle:
+
+* every rank bins its particles in the grid of the whole set (``hidem_regenerate_frame``
+  with the box over all ranks), so cell colours, and with them the order of every contact
+  list, are those of one rank; particles and links keep the relative order of the whole
+  set, so the (colour, index) order and the link-id order of every link-end list are too;
+* gridService reduces the three displacement maxima over ranks, not each rank's norm of
+  its own.
+
+The per-step exchange is one packed buffer per rank (``hidem_pack_halo_forces``), one
+contiguous run per peer, moved by the ``comm`` object: ``LocalComm`` for several contexts
+in one process (device-to-device copies), ``DistComm`` for one rank per process over
+``torch.distributed`` (NCCL point-to-point on GPUs; gloo on the host for tests).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+
+# ---------------------------------------------------------------------------------------
+# partition (numpy only)
+
+
+def slab_cuts(x: np.ndarray, nranks: int) -> np.ndarray:
+    """nranks + 1 cut positions along x: -inf, the count quantiles, +inf. Particle i
+    belongs to rank r when cuts[r] <= x_i < cuts[r + 1]."""
+    if nranks < 1:
+        raise ValueError("need at least one rank")
+    xs = np.sort(np.asarray(x, np.float64))
+    n = xs.shape[0]
+    inner = [xs[min(n - 1, (k * n) // nranks)] for k in range(1, nranks)] if n else [0.0] * (nranks - 1)
+    return np.array([-np.inf, *inner, np.inf])
+
+
+def slab_owner(x: np.ndarray, cuts: np.ndarray) -> np.ndarray:
+    return np.searchsorted(cuts[1:-1], np.asarray(x, np.float64), side="right").astype(np.int32)
+
+
+@dataclass
+class SlabLayout:
+    """Which particles and links each rank holds (indices into the whole set, ascending)."""
+    cuts: np.ndarray
+    owner: np.ndarray            # int32[N] owning rank of every particle
+    local: list                  # local[r]: particles rank r holds (own + halo)
+    links: list                  # links[r]: links with an end rank r owns
+    send: list                   # send[r][s]: particles r owns whose force s integrates
+
+    @property
+    def nranks(self) -> int:
+        return len(self.local)
+
+    def local_index(self, r: int, glob: np.ndarray) -> np.ndarray:
+        """Positions of the whole-set particle indices `glob` in rank r's particle order."""
+        idx = np.searchsorted(self.local[r], glob)
+        if glob.size and not np.array_equal(self.local[r][np.minimum(idx, self.local[r].size - 1)], glob):
+            raise ValueError(f"particles not held by rank {r}")
+        return idx.astype(np.int32)
+
+    def send_list(self, r: int) -> np.ndarray:
+        """Rank r's send list in its own indices: the runs for peers 0, 1, ... in order."""
+        runs = [self.send[r][s] for s in range(self.nranks) if s != r]
+        glob = np.concatenate(runs) if runs else np.zeros(0, np.int64)
+        return self.local_index(r, glob)
+
+    def recv_list(self, r: int) -> np.ndarray:
+        runs = [self.send[s][r] for s in range(self.nranks) if s != r]
+        glob = np.concatenate(runs) if runs else np.zeros(0, np.int64)
+        return self.local_index(r, glob)
+
+    def send_counts(self, r: int) -> list:
+        return [0 if s == r else int(self.send[r][s].size) for s in range(self.nranks)]
+
+    def recv_counts(self, r: int) -> list:
+        return [0 if s == r else int(self.send[s][r].size) for s in range(self.nranks)]
+
+
+def slab_layout(x: np.ndarray, link_a: np.ndarray, link_b: np.ndarray, nranks: int,
+                halo: float, cuts: np.ndarray | None = None) -> SlabLayout:
+    """Owners by x slab, halos of width `halo` on either side of each slab plus the far
+    ends of every link that touches a rank's own particles (so that every link of an owned
+    particle is complete), and the force lists between ranks."""
+    x = np.asarray(x, np.float64)
+    link_a = np.asarray(link_a, np.int64)
+    link_b = np.asarray(link_b, np.int64)
+    if cuts is None:
+        cuts = slab_cuts(x, nranks)
+    owner = slab_owner(x, cuts)
+    oa, ob = owner[link_a], owner[link_b]
+    local, links = [], []
+    for r in range(nranks):
+        near = (x >= cuts[r] - halo) & (x < cuts[r + 1] + halo)
+        mine = (oa == r) | (ob == r)
+        held = near | (owner == r)
+        held[link_a[mine]] = True
+        held[link_b[mine]] = True
+        local.append(np.flatnonzero(held).astype(np.int64))
+        links.append(np.flatnonzero(mine).astype(np.int64))
+    send = [[np.zeros(0, np.int64) for _ in range(nranks)] for _ in range(nranks)]
+    for s in range(nranks):
+        held = local[s]
+        for r in range(nranks):
+            if r != s:
+                send[r][s] = held[owner[held] == r]
+    return SlabLayout(cuts=cuts, owner=owner, local=local, links=links, send=send)
+
+
+def key_index(keys: np.ndarray, wanted: np.ndarray) -> np.ndarray:
+    """Positions of the particle keys `wanted` in `keys` (globalKey -> index)."""
+    keys = np.asarray(keys, np.int64)
+    order = np.argsort(keys, kind="stable")
+    pos = np.searchsorted(keys[order], wanted)
+    pos = np.minimum(pos, keys.size - 1)
+    if not np.array_equal(keys[order][pos], wanted):
+        raise ValueError("link end key without a particle")
+    return order[pos]
+
+
+def link_ends(particles: dict, links: dict) -> tuple[np.ndarray, np.ndarray]:
+    keys = particles["globalKeys"]
+    return key_index(keys, links["globalKeyEndA"]), key_index(keys, links["globalKeyEndB"])
+
+
+def split_state(particles: dict, links: dict, layout: SlabLayout, r: int) -> tuple[dict, dict]:
+    """Rank r's particle and link arrays (whole-set order kept; owners = owning rank)."""
+    sel = layout.local[r]
+    p = {k: np.ascontiguousarray(v[sel]) for k, v in particles.items()}
+    p["owners"] = np.ascontiguousarray(layout.owner[sel].astype(np.int32))
+    ls = layout.links[r]
+    side = np.stack([2 * ls, 2 * ls + 1], axis=1).reshape(-1)
+    l = {}
+    for k, v in links.items():
+        l[k] = np.ascontiguousarray(v[side] if k in abi.SIDE_FIELDS else v[ls])
+    return p, l
+
+
+def merge_state(parts: list, layout: SlabLayout, n: int, L: int) -> tuple[dict, dict]:
+    """The whole set from every rank's arrays (as split_state laid them out): each
+    particle from its owner, each link side's state (CT0..5) from the owner of that side's
+    particle, the rest of a link from the owner of its end A."""
+    p0, l0 = parts[0]
+    particles = {k: np.zeros(n, v.dtype) for k, v in p0.items()}
+    links = {k: np.zeros(2 * L if k in abi.SIDE_FIELDS else L, v.dtype) for k, v in l0.items()}
+    have = np.zeros(n, bool)
+    for r, (p, l) in enumerate(parts):
+        sel = layout.local[r]
+        own = layout.owner[sel] == r
+        for k, v in p.items():
+            particles[k][sel[own]] = v[own]
+        have[sel[own]] = True
+    if not have.all():
+        raise ValueError("a particle has no owner")
+    a, b = link_ends(particles, links_keys(parts, layout, L))
+    for r, (p, l) in enumerate(parts):
+        ls = layout.links[r]
+        ownA = layout.owner[a[ls]] == r
+        ownB = layout.owner[b[ls]] == r
+        for k, v in l.items():
+            if k in abi.SIDE_FIELDS:
+                v2 = v.reshape(-1, 2)
+                links[k][2 * ls[ownA]] = v2[ownA, 0]
+                links[k][2 * ls[ownB] + 1] = v2[ownB, 1]
+            else:
+                links[k][ls[ownA]] = v[ownA]
+    return particles, links
+
+
+def links_keys(parts: list, layout: SlabLayout, L: int) -> dict:
+    """The link end keys of the whole set (every link is held by the owner of an end)."""
+    ka = np.zeros(L, np.int64)
+    kb = np.zeros(L, np.int64)
+    for r, (_, l) in enumerate(parts):
+        ls = layout.links[r]
+        ka[ls] = l["globalKeyEndA"]
+        kb[ls] = l["globalKeyEndB"]
+    return {"globalKeyEndA": ka, "globalKeyEndB": kb}
+
+
+def halo_width(search_distance: float, interact_distance: float, max_radius: float) -> float:
+    """Reach of a contact-list pair at a rebuild (NeighAccel.h:104-114:
+    d - (r_i + r_j) < interactDist), with 1 % to spare for the rounding of d."""
+    return 1.01 * max(search_distance, 2.0 * max_radius + interact_distance)
+
+
+# ---------------------------------------------------------------------------------------
+# transports
+
+
+class LocalComm:
+    """Every rank in this process (several contexts, on one GPU or several)."""
+
+    def __init__(self, nranks: int):
+        self.size = nranks
+        self.ranks = list(range(nranks))
+
+    def allmax(self, vals: list) -> np.ndarray:
+        return np.max(np.stack([np.asarray(v, np.float64) for v in vals]), axis=0)
+
+    def allgather(self, objs: list) -> list:
+        return list(objs)
+
+    def exchange(self, layout: SlabLayout, send_bufs: list, recv_bufs: list) -> None:
+        """recv_bufs[s]'s run from r <- send_bufs[r]'s run for s (torch tensors)."""
+        import torch
+        R = self.size
+        soff = [np.concatenate([[0], np.cumsum(layout.send_counts(r))]) for r in range(R)]
+        roff = [np.concatenate([[0], np.cumsum(layout.recv_counts(s))]) for s in range(R)]
+        for r in range(R):
+            for s in range(R):
+                cnt = 0 if r == s else int(layout.send[r][s].size)
+                if cnt:
+                    src = send_bufs[r][6 * soff[r][s]: 6 * (soff[r][s] + cnt)]
+                    dst = recv_bufs[s][6 * roff[s][r]: 6 * (roff[s][r] + cnt)]
+                    dst.copy_(src, non_blocking=False)
+        for t in recv_bufs:
+            if t.is_cuda:
+                torch.cuda.synchronize(t.device)
+
+
+class DistComm:
+    """One rank per process over torch.distributed (NCCL with CUDA buffers, gloo with host
+    buffers); the process group is initialised by the caller."""
+
+    def __init__(self):
+        import torch.distributed as dist
+        self.dist = dist
+        self.size = dist.get_world_size()
+        self.ranks = [dist.get_rank()]
+        self.backend = dist.get_backend()
+
+    def _dev(self):
+        import torch
+        return torch.device("cuda", torch.cuda.current_device()) if self.backend == "nccl" else torch.device("cpu")
+
+    def allmax(self, vals: list) -> np.ndarray:
+        import torch
+        t = torch.tensor(np.asarray(vals[0], np.float64), device=self._dev())
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return t.cpu().numpy()
+
+    def allgather(self, objs: list) -> list:
+        out = [None] * self.size
+        self.dist.all_gather_object(out, objs[0])
+        return out
+
+    def exchange(self, layout: SlabLayout, send_bufs: list, recv_bufs: list) -> None:
+        import torch
+        r = self.ranks[0]
+        sc, rc = layout.send_counts(r), layout.recv_counts(r)
+        soff, roff = np.concatenate([[0], np.cumsum(sc)]), np.concatenate([[0], np.cumsum(rc)])
+        ops = []
+        for s in range(self.size):
+            if sc[s]:
+                ops.append(self.dist.P2POp(self.dist.isend, send_bufs[0][6 * soff[s]: 6 * soff[s + 1]], s))
+            if rc[s]:
+                ops.append(self.dist.P2POp(self.dist.irecv, recv_bufs[0][6 * roff[s]: 6 * roff[s + 1]], s))
+        if ops:
+            for w in self.dist.batch_isend_irecv(ops):
+                w.wait()
+        if recv_bufs[0].is_cuda:
+            torch.cuda.current_stream(recv_bufs[0].device).synchronize()
+
+
+# ---------------------------------------------------------------------------------------
+# driver
+
+
+class SlabRun:
+    """The ranks of one particle set that live in this process, stepped together.
+
+    ``libs`` are this process's contexts (``HiDEMLib``, or any object with the same
+    methods), one per rank in ``comm.ranks``; ``particles`` / ``links`` the whole set
+    (numpy arrays as ``HiDEMLib.set_particles`` / ``set_links`` take them), the same on
+    every process. Steps follow the sample main: gridService, computePartForce (with the
+    halo force exchange), applyForce, linkUpdate when t*dt > breakTime, finalizeTs."""
+
+    def __init__(self, comm, libs: list, particles: dict, links: dict, halo: float | None = None):
+        import torch
+        if len(libs) != len(comm.ranks):
+            raise ValueError("one context per rank of this process")
+        self.comm, self.libs = comm, list(libs)
+        self.n = int(particles["xCord"].shape[0])
+        self.L = int(links["globalKeyEndA"].shape[0])
+        self.precision = int(self.libs[0].precision)
+        self.lp = abi.lp_dtype(self.precision)
+        self._tdtype = torch.float32 if self.lp == np.float32 else torch.float64
+        self._halo = halo
+        self.redistributions = 0
+        self.exchanged = 0      # halo force records moved so far (all ranks of this process)
+        self._distribute(particles, links)
+
+    # -- state movement
+    def _halo_width(self, particles: dict) -> float:
+        if self._halo is not None:
+            return float(self._halo)
+        s = self.libs[0].stats()
+        rmax = float(np.max(particles["radius"])) if self.n else 0.0
+        rmax = float(self.comm.allmax([np.array([rmax])])[0])
+        return halo_width(s["search_distance"], s["interact_distance"], rmax)
+
+    def _distribute(self, particles: dict, links: dict) -> None:
+        import torch
+        a, b = link_ends(particles, links)
+        self.layout = slab_layout(particles["xCord"], a, b, self.comm.size, self._halo_width(particles))
+        self.send_bufs, self.recv_bufs = [], []
+        for lib, r in zip(self.libs, self.comm.ranks):
+            p, l = split_state(particles, links, self.layout, r)
+            lib.set_particles(p)
+            lib.set_links(l)
+            snd, rcv = self.layout.send_list(r), self.layout.recv_list(r)
+            lib.set_halo_exchange(snd, rcv)
+            dev = _lib_device(lib)
+            self.send_bufs.append(torch.zeros(6 * max(1, snd.size), dtype=self._tdtype, device=dev))
+            self.recv_bufs.append(torch.zeros(6 * max(1, rcv.size), dtype=self._tdtype, device=dev))
+        self.redistributions += 1
+
+    def gather(self) -> tuple[dict, dict]:
+        """The whole set's particles and links (every process gets them)."""
+        mine = [(lib.get_particles(), lib.get_links()) for lib in self.libs]
+        parts = self.comm.allgather(mine)
+        return merge_state(parts, self.layout, self.n, self.L)
+
+    # -- one timestep
+    def _grid_service(self) -> None:
+        loc = [lib.grid_service_local() for lib in self.libs]
+        mx = self.comm.allmax([m for m, _ in loc])
+        regen = [np.array([1.0 if lib.grid_service_decide(mx) else 0.0]) for lib in self.libs]
+        if not self.comm.allmax(regen)[0]:
+            return
+        # rebalance: every particle to the owner of its slab, recut, halos rebuilt
+        particles, links = self.gather()
+        self._distribute(particles, links)
+        bounds = [lib.local_bounds() for lib in self.libs]
+        lo = -self.comm.allmax([-b[0] for b in bounds])
+        hi = self.comm.allmax([b[1] for b in bounds])
+        for lib in self.libs:
+            lib.regenerate_frame(lo, hi)
+
+    def _forces(self) -> None:
+        for lib, buf in zip(self.libs, self.send_bufs):
+            lib.computePartForce()
+            lib.pack_halo_forces(buf.data_ptr())
+        for lib in self.libs:
+            lib.synchronize()
+        self.comm.exchange(self.layout, self.send_bufs, self.recv_bufs)
+        for lib, r, buf in zip(self.libs, self.comm.ranks, self.recv_bufs):
+            lib.unpack_halo_forces(buf.data_ptr())
+            self.exchanged += sum(self.layout.recv_counts(r))
+
+    def step(self, nsteps: int = 1) -> None:
+        for _ in range(nsteps):
+            self._grid_service()
+            self._forces()
+            brk = self.libs[0].breakActive()
+            for lib in self.libs:
+                lib.applyForce()
+                if brk:
+                    lib.linkUpdate()
+                lib.finalizeTs()
+        for lib in self.libs:
+            lib.synchronize()
+
+
+def _lib_device(lib):
+    import torch
+    dev = getattr(lib, "device", 0)
+    return torch.device("cuda", int(dev)) if torch.cuda.is_available() else torch.device("cpu")

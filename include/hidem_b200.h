@@ -184,6 +184,62 @@ hidem_status hidem_integrate(hidem_ctx *ctx);
 hidem_status hidem_link_update(hidem_ctx *ctx);
 /* HiDEMLib::finalizeTs (HiDEMLib.h:495-530): ++timestep. */
 hidem_status hidem_finalize_ts(hidem_ctx *ctx);
+
+/* ---- slab decomposition hooks (one context per rank) ------------------ */
+
+/* The reference spreads one particle set over MPI ranks (HiDEMLib/HiDEMDistribution.h:
+ * 99-234): each rank holds the particles it owns plus halo copies of its neighbours'
+ * particles, computes the forces of its own, receives the forces of its halo particles
+ * from their owners and integrates both (computePartForce, HiDEMLib.h:316-382, the
+ * pForceComm exchange), and gridService reduces the displacement over ranks
+ * (accumulateDist, HiDEMLib.h:463-474, MPI_Allreduce). These calls split the
+ * rank-spanning steps so that the caller's transport (NCCL, or copies between
+ * contexts of one process) does the exchange and the reductions:
+ *
+ *   gridService:  hidem_grid_service_local -> max over ranks -> hidem_grid_service_decide;
+ *                 on regen: hidem_local_bounds -> min/max over ranks -> hidem_regenerate_frame
+ *   forces:       hidem_compute_forces -> hidem_pack_halo_forces -> exchange ->
+ *                 hidem_unpack_halo_forces -> hidem_integrate -> hidem_link_update ->
+ *                 hidem_finalize_ts
+ *
+ * Indices are particle indices in the order of the last hidem_set_particles call. */
+
+/* This rank's part of gridService's displacement rule at the current step: the maxima
+ * over its particles of max(0, xDiff / yDiff / zDiff), as doubles (HiDEMLib.h:424-460).
+ * *needs_reduce = 1 when the step reads them (the rule runs every 10 steps), else 0 and
+ * diff_max is zeros. */
+hidem_status hidem_grid_service_local(hidem_ctx *ctx, double diff_max[3], int32_t *needs_reduce);
+/* The rest of gridService's decision from the maxima over all ranks (element-wise max of
+ * every rank's hidem_grid_service_local): accumulated distance updated as
+ * HiDEMLib.h:463-474 and 563-575 do, *regen = 1 when the neighbour structures must be
+ * rebuilt now. Rebuilds nothing: the caller redistributes if it wants to, then calls
+ * hidem_regenerate_frame. The reference reduces each rank's distance (the norm of its
+ * own maxima); reducing the maxima makes every rank's decision that of one rank holding
+ * all particles. */
+hidem_status hidem_grid_service_decide(hidem_ctx *ctx, const double diff_max[3], int32_t *regen);
+/* Bounding box of this rank's particles (ParticleData::getLimits, PLiB/ParticleData.h:
+ * 47-59). Synchronises the context's stream. */
+hidem_status hidem_local_bounds(hidem_ctx *ctx, double lower[3], double upper[3]);
+/* hidem_regenerate with the grid spanning [lower, upper] (the element-wise min / max of
+ * every rank's hidem_local_bounds) instead of this rank's own bounding box, so that cell
+ * colours, and with them every contact list's order, are those of one rank holding all
+ * particles. HIDEM_ERR_ARG if a particle of this rank lies outside the box. */
+hidem_status hidem_regenerate_frame(hidem_ctx *ctx, const double lower[3], const double upper[3]);
+/* The halo force lists: send_index[k] is a particle this rank owns whose force another
+ * rank integrates (the k-th 6-value record of the packed buffer); recv_index[k] is a halo
+ * particle whose force arrives as the k-th record. The caller orders the lists by
+ * destination / source rank so that each peer's records are contiguous. Copied; the
+ * indices stay valid across rebuilds. Either count may be 0. */
+hidem_status hidem_set_halo_exchange(hidem_ctx *ctx, const int32_t *send_index, int64_t n_send,
+                                     const int32_t *recv_index, int64_t n_recv);
+/* Writes the forces of the send list, n_send x 6 lp values (x, y, z, u, v, w per
+ * particle), from the last hidem_compute_forces to `device_out` (device memory), on the
+ * context's stream (CommunicatorPacked::packAllCommData). */
+hidem_status hidem_pack_halo_forces(hidem_ctx *ctx, void *device_out);
+/* Overwrites the forces of the receive list with n_recv x 6 lp values read from
+ * `device_in` (device memory), on the context's stream; the caller has made the stream
+ * wait for the data (CommunicatorPacked::unpackAllCommData). */
+hidem_status hidem_unpack_halo_forces(hidem_ctx *ctx, const void *device_in);
 /* n whole timesteps of the sample main loop (MainMeshBlock.cpp:274-323):
  * gridService, forces, integrate, gated link update, finalizeTs — as one fused
  * kernel per step, graph-launched between rebuild checks. */
