@@ -8,8 +8,9 @@ A "step" is one timestep of the sample main loop (gridService, forces, integrate
 update) over the whole slab. `value` times K steps with the state resident in HBM (CUDA
 events on the library's stream, max over ranks). `e2e` times the same K steps through the
 C ABI from host arrays: upload of the particle and link state, the K steps, download of
-the particle state. `roofline` divides the byte model of the step by the fused step
-kernel's event-timed duration. `cpu_baseline` times the reference's own CPU path
+the particle state. `roofline` divides the byte model of the step by the event-timed
+duration of the step's kernels (the force, integrate and break passes of the two-pass
+step, or the one kernel of a fused step). `cpu_baseline` times the reference's own CPU path
 (oracle/_ref, built from its sources with its own flags) on the same slab.
 With --gpus N > 1 (torchrun) every rank advances its own replica of the slab (the path
 has no exchange on one node for this workload; weak scaling).
@@ -39,7 +40,7 @@ sys.path.insert(0, str(ROOT))
 PUBLISHED_MIXED = 5723826 * 5000 / 25.83
 
 # step kernels of the library (hidem_set_step_kernel)
-KERNELS = {"auto": 0, "items": 1, "thread": 2, "thread-capped": 3, "thread-async": 4}
+KERNELS = {"auto": 0, "items": 1, "thread": 2, "thread-capped": 3, "thread-async": 4, "two-pass": 5}
 KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
 
 
@@ -50,8 +51,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle", "topo", "mesh"],
+    ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle", "topo", "mesh", "ranks"],
                     default="slab")
+    ap.add_argument("--ranks", type=int, default=2,
+                    help="ranks: slab ranks held as contexts of this process (one GPU)")
     ap.add_argument("--topo", default="1200,200,150",
                     help="topo: slab size in metres on the Fourier-mode bed (the 50M configuration)")
     ap.add_argument("--train-tongues", type=int, default=256, help="settle: training geometries")
@@ -62,7 +65,7 @@ def parse():
     ap.add_argument("--tongue", default="40,12", help="settle: tongue plan size in metres x,y")
     ap.add_argument("--blocks", type=int, default=256, help="ensemble: number of blocks")
     ap.add_argument("--no-graphs", action="store_true", help="ensemble: plain launches")
-    ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped", "thread-async"],
+    ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped", "thread-async", "two-pass"],
                     default="auto", help="step kernel (auto: timed on the first steps)")
     ap.add_argument("--slab", default="400,100,100",
                     help="slab size in metres x,y,z (smaller slabs for profiling captures)")
@@ -156,10 +159,12 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profile_traffic(precision: str):
-    """DRAM bytes per particle-step of the fused step kernel from the committed ncu
-    summary (profiles/fused_step_*.md, line `dram_bytes_per_particle_step: X`)."""
-    f = ROOT / "profiles" / f"fused_step_slab_{precision}.md"
+def profile_traffic(precision: str, two_pass: bool = True):
+    """DRAM bytes per particle-step of the step's kernels from the committed ncu summary
+    (profiles/step_passes_slab_*.md for the two-pass step, profiles/fused_step_slab_*.md
+    for the fused one; line `dram_bytes_per_particle_step: X`)."""
+    stem = "step_passes_slab" if two_pass else "fused_step_slab"
+    f = ROOT / "profiles" / f"{stem}_{precision}.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -726,8 +731,119 @@ def main_mesh(args):
     print(json.dumps(line))
 
 
+def main_ranks(args):
+    """The slab decomposed over ranks (hidem_b200.slab): with one process, --ranks contexts
+    on its GPU exchange halo forces by device copies; under torchrun, one rank per GPU over
+    NCCL. Times K decomposed timesteps (gridService, forces, halo exchange, integrate, link
+    update) and, on one GPU, the same K steps of one context through the same separate
+    calls and through the fused step, so the cost of the decomposition shows."""
+    import torch
+    from hidem_b200 import abi, slab, workloads
+    from hidem_b200.hidemlib import HiDEMLib
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    size = tuple(float(v) for v in args.slab.split(","))
+    P, p, l = workloads.calving_slab(size=size, precision=prec)
+    n, L = p["xCord"].shape[0], l["state"].shape[0]
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        comm = slab.DistComm()
+        nranks = world
+    else:
+        comm = slab.LocalComm(args.ranks)
+        nranks = args.ranks
+
+    def region(body, steps):
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        body(steps)
+        torch.cuda.synchronize()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    single = {}
+    if world == 1:
+        for mode in ("split", "fused"):
+            lib = HiDEMLib(P, device=local)
+            lib.set_step_kernel(KERNELS["thread-capped" if prec == abi.PREC_MIXED else "thread-async"])
+            lib.set_particles(p)
+            lib.set_links(l)
+
+            def body(k, lib=lib, mode=mode):
+                for _ in range(k):
+                    if mode == "fused":
+                        lib.step(1)
+                    else:
+                        lib.timestep_split()
+                lib.synchronize()
+            body(args.warmup)
+            single[mode] = region(body, args.steps) / args.steps
+            lib.close()
+            torch.cuda.empty_cache()
+    libs = [HiDEMLib(P, device=local) for _ in comm.ranks]
+    for lib in libs:
+        lib.set_step_kernel(KERNELS["thread-capped" if prec == abi.PREC_MIXED else "thread-async"])
+    run = slab.SlabRun(comm, libs, p, l)
+    run.step(args.warmup)
+    st0 = [lib.stats() for lib in libs]
+    red0, ex0 = run.redistributions, run.exchanged
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = region(run.step, args.steps) / args.steps
+    clk = clocks.stop()
+    st1 = [lib.stats() for lib in libs]
+    held = [int(s["num_particles"]) for s in st1]
+    launches = sum(int(b["kernel_launches"] - a["kernel_launches"]) for a, b in zip(st0, st1))
+    if rank == 0:
+        lay = run.layout
+        halo = int(sum(len(lay.local[r]) for r in range(nranks)) - n)
+        line = {
+            "metric": "particle-steps/s (slab decomposed over ranks)", "value": n / (ms / 1e3),
+            "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
+            "config": {"workload": f"calving slab {size[0]:g}x{size[1]:g}x{size[2]:g} m in {nranks} x-slabs",
+                       "particles": n, "links": L, "ranks": nranks,
+                       "transport": "NCCL point-to-point" if world > 1 else "device copies between contexts of one process",
+                       "parallelism": f"slabs{nranks}", "precision": args.precision,
+                       "l2": "inputs larger than L2 (records + link ends > 126 MB)"},
+            "halo": {"halo_particles": halo, "halo_fraction": halo / n,
+                     "force_records_per_step": (run.exchanged - ex0) / max(args.steps, 1),
+                     "exchange_bytes_per_step": (run.exchanged - ex0) / max(args.steps, 1) * 6 * (4 if prec == abi.PREC_MIXED else 8),
+                     "particles_held_per_rank": held if world == 1 else None},
+            "redistributions_in_timed_steps": run.redistributions - red0,
+            "one_context_ms_per_step": single or None,
+            "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line))
+    for lib in libs:
+        lib.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = parse()
+    if args.workload == "ranks":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference's ranks are MPI processes; its CPU path is timed by the slab workload"}))
+        else:
+            main_ranks(args)
+        return
     if args.workload == "mesh":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable":
@@ -818,11 +934,13 @@ def main():
     kern_avg_s = (kern_ms / max(kern_n, 1)) / 1e3
     peak, peak_kind = measured_peak()
     achieved = bytes_step / kern_avg_s / 1e9
-    dpps = profile_traffic(args.precision)
+    two_pass = step_kernel == KERNELS["two-pass"]
+    dpps = profile_traffic(args.precision, two_pass)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": (dpps * n) if dpps else None,
                 "peak_source": peak_kind,
-                "kernel": "fused step, " + KERNEL_NAMES.get(step_kernel, "?") + " kernel",
+                "kernel": ("step passes (k_step force pass, k_integrate, k_link_break), two-pass kernel"
+                           if two_pass else "fused step, " + KERNEL_NAMES.get(step_kernel, "?") + " kernel"),
                 "kernel_ms": kern_ms / max(kern_n, 1),
                 "algorithmic_bytes_per_launch": bytes_step}
 

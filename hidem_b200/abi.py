@@ -29,6 +29,7 @@ STEP_KERNEL_ITEMS = 1
 STEP_KERNEL_THREAD = 2
 STEP_KERNEL_THREAD_CAPPED = 3
 STEP_KERNEL_THREAD_ASYNC = 4
+STEP_KERNEL_TWO_PASS = 5
 
 _d = C.c_double
 _i32 = C.c_int32

@@ -119,7 +119,7 @@ struct hidem_ctx {
     int stepKernel = HIDEM_STEP_KERNEL_AUTO;
     int tunedKernel = HIDEM_STEP_KERNEL_AUTO;
     int tuneStep = 0;
-    cudaEvent_t tuneEv[2 * 12] = {};
+    cudaEvent_t tuneEv[2 * 16] = {};
 
     double *energyBuf = nullptr;  // kinetic-energy partials + result
     int energyBlocks = 0;
@@ -706,9 +706,15 @@ hidem_status profile_pair(hidem_ctx *ctx, cudaEvent_t *e0, cudaEvent_t *e1) {
 // through the candidate kernels with an event pair around each launch; after the rounds
 // have run, the fastest (summed over all but the first round) is kept.
 constexpr int kTuneCandidates[] = {HIDEM_STEP_KERNEL_ITEMS, HIDEM_STEP_KERNEL_THREAD,
-                                   HIDEM_STEP_KERNEL_THREAD_CAPPED, HIDEM_STEP_KERNEL_THREAD_ASYNC};
+                                   HIDEM_STEP_KERNEL_THREAD_CAPPED, HIDEM_STEP_KERNEL_THREAD_ASYNC,
+                                   HIDEM_STEP_KERNEL_TWO_PASS};
 constexpr int kNumCandidates = (int)(sizeof(kTuneCandidates) / sizeof(int));
 constexpr int kTuneRounds = 3;
+static_assert(2 * kNumCandidates * kTuneRounds <= (int)(sizeof(hidem_ctx::tuneEv) / sizeof(cudaEvent_t)),
+              "one event pair per tuning step");
+
+// the force kernel of a step kernel choice (TWO_PASS: the register-capped one, unfused)
+int force_kernel(int k) { return k == HIDEM_STEP_KERNEL_TWO_PASS ? HIDEM_STEP_KERNEL_THREAD_CAPPED : k; }
 
 int step_kernel_now(hidem_ctx *ctx, cudaEvent_t *e0, cudaEvent_t *e1) {
     *e0 = *e1 = nullptr;
@@ -763,6 +769,13 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
     bool diffReady = false;
     for (int s = 0; s < nsteps; ++s) {
         const long long t = ctx->step;
+        cudaEvent_t e0 = nullptr, e1 = nullptr, t0 = nullptr, t1 = nullptr;
+        const int kern = step_kernel_now(ctx, &t0, &t1);
+        if (kern == HIDEM_STEP_KERNEL_TWO_PASS && pending) {
+            // the previous (fused) step's link update, where the reference runs it
+            TRY(link_update_now<LP>(ctx, pendingStep));
+            pending = false;
+        }
         if (ctx->P.gridRegenInterval == -1 && t % 10 == 0) {
             // gridService reads the maxima of the diffs at the start of step t
             TRY(grid_service(ctx, diffReady));
@@ -770,6 +783,22 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
             TRY(grid_service(ctx, false));
         }
         diffReady = false;
+        if (kern == HIDEM_STEP_KERNEL_TWO_PASS) {
+            // force pass, integrate pass (in place), break pass (MainMeshBlock.cpp:295-320)
+            if (ctx->profile) TRY(profile_pair(ctx, &e0, &e1));
+            if (e0) CK(cudaEventRecord(e0, ctx->stream));
+            if (t0) CK(cudaEventRecord(t0, ctx->stream));
+            launch_step<LP>(consts<LP>(ctx), step_args<LP>(ctx), false, (int)ctx->maxNeigh,
+                            (int)ctx->maxLinksPP, HIDEM_STEP_KERNEL_THREAD_CAPPED, ctx->stream);
+            launch_integrate<LP>(consts<LP>(ctx), recp<LP>(ctx, ctx->cur), ctx->type[ctx->ord],
+                                 static_cast<const LP *>(ctx->force), (int)ctx->n, ctx->stream);
+            ctx->launches += 2;
+            if (break_active<LP>(ctx, t)) TRY(link_update_now<LP>(ctx, t));
+            if (t1) CK(cudaEventRecord(t1, ctx->stream));
+            if (e1) CK(cudaEventRecord(e1, ctx->stream));
+            ctx->step = t + 1;
+            continue;
+        }
         StepArgs<LP> a = step_args<LP>(ctx);
         a.breakPending = pending ? 1 : 0;
         a.breakStep = pendingStep;
@@ -778,8 +807,6 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
             CK(cudaMemsetAsync(ctx->diffMax, 0, 3 * sizeof(unsigned long long), ctx->stream));
             diffReady = true;
         }
-        cudaEvent_t e0 = nullptr, e1 = nullptr, t0 = nullptr, t1 = nullptr;
-        const int kern = step_kernel_now(ctx, &t0, &t1);
         if (ctx->profile) TRY(profile_pair(ctx, &e0, &e1));
         if (e0) CK(cudaEventRecord(e0, ctx->stream));
         if (t0) CK(cudaEventRecord(t0, ctx->stream));
@@ -943,7 +970,7 @@ int batch_kernel(const hidem_batch *b) {
     int k = HIDEM_STEP_KERNEL_THREAD_CAPPED;
     if (c->stepKernel != HIDEM_STEP_KERNEL_AUTO) k = c->stepKernel;
     else if (c->tunedKernel != HIDEM_STEP_KERNEL_AUTO) k = c->tunedKernel;
-    return k == HIDEM_STEP_KERNEL_THREAD_ASYNC ? HIDEM_STEP_KERNEL_THREAD_CAPPED : k;
+    return (k == HIDEM_STEP_KERNEL_THREAD_ASYNC || k == HIDEM_STEP_KERNEL_TWO_PASS) ? HIDEM_STEP_KERNEL_THREAD_CAPPED : k;
 }
 
 // Groups of contexts with equal constants apart from the break thresholds (compared
@@ -1225,7 +1252,7 @@ hidem_status batch_run(hidem_batch *b, int nsteps) {
                     if (a.reduceDiff)
                         BCK(cudaMemsetAsync(c->diffMax, 0, 3 * sizeof(unsigned long long), b->stream));
                     launch_step<LP>(consts<LP>(c), a, true, (int)c->maxNeigh, (int)c->maxLinksPP,
-                                    step_kernel_settled(c), b->stream);
+                                    force_kernel(step_kernel_settled(c)), b->stream);
                     c->launches += 1;
                     b->launches += 1;
                 }
@@ -1663,7 +1690,7 @@ hidem_status hidem_compute_forces(hidem_ctx *ctx) {
     if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
     CK(cudaSetDevice(ctx->device));
     if (!ctx->built) TRY(do_rebuild(ctx));
-    const int kern = step_kernel_settled(ctx);
+    const int kern = force_kernel(step_kernel_settled(ctx));
     if (ctx->mixed) {
         StepArgs<float> a = step_args<float>(ctx);
         launch_step<float>(ctx->cf, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, kern,
@@ -2537,7 +2564,7 @@ hidem_status hidem_get_mesh_accel(hidem_ctx *ctx, int32_t counts[3], double lowe
 
 hidem_status hidem_set_step_kernel(hidem_ctx *ctx, int32_t kernel) {
     if (!ctx) return HIDEM_ERR_ARG;
-    if (kernel < HIDEM_STEP_KERNEL_AUTO || kernel > HIDEM_STEP_KERNEL_THREAD_ASYNC)
+    if (kernel < HIDEM_STEP_KERNEL_AUTO || kernel > HIDEM_STEP_KERNEL_TWO_PASS)
         return fail(ctx, HIDEM_ERR_ARG, "unknown step kernel %d", (int)kernel);
     ctx->stepKernel = kernel;
     return HIDEM_OK;

@@ -602,6 +602,9 @@ constexpr int kThreadBlocks = sizeof(LP) == 4 ? 4 : 1;
 // and the asynchronous-copy variant (its partner data lives in shared memory)
 template <class LP>
 constexpr int kAsyncBlocks = sizeof(LP) == 4 ? 5 : 3;
+// the register-capped force pass without the integrate tail (two-pass steps)
+template <class LP>
+constexpr int kCapBlocksForces = sizeof(LP) == 4 ? 5 : 3;
 
 template <class LP, bool FUSED, int MINB>
 __global__ void __launch_bounds__(kStepThreads, MINB)
@@ -1300,7 +1303,7 @@ void launch_step(const Consts<LP> &c, const StepArgs<LP> &a0, bool fused, int ma
         if (fused)
             k_step<LP, true, kCapBlocks<LP>><<<nb, kStepThreads, 0, s>>>(c, a);
         else
-            k_step<LP, false, kCapBlocks<LP>><<<nb, kStepThreads, 0, s>>>(c, a);
+            k_step<LP, false, kCapBlocksForces<LP>><<<nb, kStepThreads, 0, s>>>(c, a);
     } else {
         if (fused)
             k_step<LP, true, kThreadBlocks<LP>><<<nb, kStepThreads, 0, s>>>(c, a);

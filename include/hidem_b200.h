@@ -417,14 +417,19 @@ hidem_status hidem_momentum(hidem_ctx *ctx, double linear[3], double angular[3])
  * thread per particle with software-pipelined partner loads (THREAD), and the same with
  * registers capped for more CTAs per SM (THREAD_CAPPED: five in the mixed build, three in
  * FP64), and one thread per particle whose next two items' partner data travel by
- * asynchronous copies into shared memory (THREAD_ASYNC). AUTO (the default) times each on the context's own first fused steps (three
- * rounds, the first discarded) and keeps the fastest; those steps are ordinary timesteps.
- * hidem_get_step_kernel returns the kernel in use (AUTO while still timing). */
+ * asynchronous copies into shared memory (THREAD_ASYNC). TWO_PASS runs each timestep as
+ * the THREAD_CAPPED force pass without the integrate tail, then the integrate pass over
+ * the particles and the break pass over the links, as hidem_compute_forces /
+ * hidem_integrate / hidem_link_update do. AUTO (the default) times each on the context's
+ * own first steps (three rounds, the first discarded) and keeps the fastest; those steps
+ * are ordinary timesteps. hidem_get_step_kernel returns the kernel in use (AUTO while
+ * still timing). */
 #define HIDEM_STEP_KERNEL_AUTO 0
 #define HIDEM_STEP_KERNEL_ITEMS 1
 #define HIDEM_STEP_KERNEL_THREAD 2
 #define HIDEM_STEP_KERNEL_THREAD_CAPPED 3
 #define HIDEM_STEP_KERNEL_THREAD_ASYNC 4
+#define HIDEM_STEP_KERNEL_TWO_PASS 5
 hidem_status hidem_set_step_kernel(hidem_ctx *ctx, int32_t kernel);
 int32_t hidem_get_step_kernel(const hidem_ctx *ctx);
 

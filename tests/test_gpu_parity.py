@@ -72,7 +72,8 @@ def test_gpu_matches_reference_golden(gpu, name, mode):
 
 @pytest.mark.parametrize("name", ["block6_mixed", "block6_fp64", "slab533_mixed", "slab533_fp64"])
 @pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD,
-                                    abi.STEP_KERNEL_THREAD_CAPPED, abi.STEP_KERNEL_THREAD_ASYNC])
+                                    abi.STEP_KERNEL_THREAD_CAPPED, abi.STEP_KERNEL_THREAD_ASYNC,
+                                    abi.STEP_KERNEL_TWO_PASS])
 def test_every_step_kernel_matches_golden(gpu, name, kernel):
     """Each step kernel on its own (the autotuner only picks among them by speed)."""
     g = load_golden(name)
@@ -91,10 +92,11 @@ def test_step_kernel_autotuner_settles(gpu):
     lib.set_links(l)
     assert lib.step_kernel() == abi.STEP_KERNEL_AUTO
     lib.step(4)
-    assert lib.step_kernel() == abi.STEP_KERNEL_AUTO  # still timing (4 kernels x 3 rounds)
-    lib.step(8)
+    assert lib.step_kernel() == abi.STEP_KERNEL_AUTO  # still timing (5 kernels x 3 rounds)
+    lib.step(11)
     assert lib.step_kernel() in (abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD,
-                                 abi.STEP_KERNEL_THREAD_CAPPED, abi.STEP_KERNEL_THREAD_ASYNC)
+                                 abi.STEP_KERNEL_THREAD_CAPPED, abi.STEP_KERNEL_THREAD_ASYNC,
+                                 abi.STEP_KERNEL_TWO_PASS)
     with pytest.raises(abi.HidemError):
         lib.set_step_kernel(9)
     # the rebuild's device-side statistics: link ends per particle
@@ -176,7 +178,8 @@ def test_gpu_matches_oracle_live(gpu, precision, variant):
 
 
 @pytest.mark.parametrize("precision", PRECS)
-@pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD_CAPPED])
+@pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD_CAPPED,
+                                    abi.STEP_KERNEL_TWO_PASS])
 def test_gpu_bed_and_force_maps_match_oracle(gpu, precision, kernel):
     from conftest import maps_case
     P, p, l, (bed, fric, ext), keep = maps_case(precision)
@@ -210,7 +213,7 @@ def test_gpu_bed_and_force_maps_match_oracle(gpu, precision, kernel):
 
 @pytest.mark.parametrize("precision", PRECS)
 @pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_ITEMS, abi.STEP_KERNEL_THREAD_CAPPED,
-                                    abi.STEP_KERNEL_THREAD_ASYNC])
+                                    abi.STEP_KERNEL_THREAD_ASYNC, abi.STEP_KERNEL_TWO_PASS])
 def test_gpu_collision_mesh_matches_oracle(gpu, precision, kernel):
     """The device MeshAccel grid equals the oracle's (itself pinned to the reference's
     generateAccel); 40 steps with the closest-triangle force are bit-exact through the
