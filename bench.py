@@ -159,6 +159,13 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+def step_label(kernel: int, extra: str = "") -> str:
+    """What one step launches, for roofline.kernel."""
+    if kernel == KERNELS["two-pass"]:
+        return f"step passes (k_step force pass, k_integrate{extra}, k_link_break), two-pass kernel"
+    return f"fused step{extra}, " + KERNEL_NAMES.get(kernel, "?") + " kernel"
+
+
 def profile_traffic(precision: str, two_pass: bool = True):
     """DRAM bytes per particle-step of the step's kernels from the committed ncu summary
     (profiles/step_passes_slab_*.md for the two-pass step, profiles/fused_step_slab_*.md
@@ -617,7 +624,7 @@ def main_topo(args):
                    "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                     "kernel": "fused step, " + KERNEL_NAMES.get(kernel, "?") + " kernel",
+                     "kernel": step_label(kernel),
                      "kernel_ms": kern_ms / max(kern_n, 1), "algorithmic_bytes_per_launch": bytes_step},
         "mixed_vs_fp64_1M_subslab_1000_steps": {
             "particles": int(dx.shape[0]), "max_err_over_d": float(dx.max()),
@@ -723,7 +730,7 @@ def main_mesh(args):
         "without_mesh": {"value": n * args.steps / (plain["ms"] / 1e3), "ms_per_step": plain["ms"] / args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_source": peak_kind,
-                     "kernel": "fused step with the mesh query, " + KERNEL_NAMES.get(with_mesh["kernel"], "?") + " kernel",
+                     "kernel": step_label(with_mesh["kernel"], " with the mesh query"),
                      "kernel_ms": with_mesh["kernel_ms"], "algorithmic_bytes_per_launch": bytes_step},
         "cpu_baseline": cpu, "gpu_launches": with_mesh["launches"], "rebuilds_in_timed_steps": with_mesh["rebuilds"],
         "clocks": with_mesh["clocks"],
@@ -939,8 +946,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": (dpps * n) if dpps else None,
                 "peak_source": peak_kind,
-                "kernel": ("step passes (k_step force pass, k_integrate, k_link_break), two-pass kernel"
-                           if two_pass else "fused step, " + KERNEL_NAMES.get(step_kernel, "?") + " kernel"),
+                "kernel": step_label(step_kernel),
                 "kernel_ms": kern_ms / max(kern_n, 1),
                 "algorithmic_bytes_per_launch": bytes_step}
 
