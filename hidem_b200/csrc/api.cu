@@ -85,6 +85,7 @@ struct hidem_ctx {
     // links (input order)
     int32_t *linkA = nullptr, *linkB = nullptr;
     void *L0link = nullptr;
+    uint8_t *linkState = nullptr;  // per-link state, kept equal to the sides' states
     int32_t *plStart = nullptr, *plLink = nullptr;
     uint8_t *plEnd = nullptr;
     int32_t *sideSlot[2] = {nullptr, nullptr};
@@ -655,6 +656,7 @@ StepArgs<LP> step_args(hidem_ctx *ctx) {
     a.sPartner = s.partner;
     for (int k = 0; k < 6; ++k) a.ct[k] = static_cast<LP *>(s.ct[k]);
     a.sState = s.state;
+    a.linkState = ctx->linkState;
     a.sL0 = static_cast<const LP *>(s.L0);
     a.sLink = s.link;
     a.force = static_cast<LP *>(ctx->force);
@@ -683,8 +685,8 @@ template <class LP>
 hidem_status link_update_now(hidem_ctx *ctx, long long tagStep) {
     SideSet &s = ctx->side[ctx->curSide];
     launch_link_break<LP>(consts<LP>(ctx), recp<LP>(ctx, ctx->cur), ctx->slotOf, ctx->linkA,
-                          ctx->linkB, ctx->sideSlot[ctx->curSide], s.state,
-                          static_cast<const LP *>(s.L0), ctx->L, tagStep, ctx->events,
+                          ctx->linkB, ctx->sideSlot[ctx->curSide], s.state, ctx->linkState,
+                          static_cast<const LP *>(ctx->L0link), ctx->L, tagStep, ctx->events,
                           ctx->eventCount, ctx->eventCap, ctx->stream);
     if (ctx->L > 0) ctx->launches += 1;
     return HIDEM_OK;
@@ -1430,6 +1432,7 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->linkA);
     dfree(ctx->linkB);
     dfree(ctx->L0link);
+    dfree(ctx->linkState);
     dfree(ctx->plStart);
     dfree(ctx->plLink);
     dfree(ctx->plEnd);
@@ -1625,10 +1628,10 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     ctx->eventsRead = 0;
     TRY(ensure_scan(ctx, n + 2));
     int *deg = nullptr, *cursor = nullptr;
-    uint8_t *lstate = nullptr;
     TRY(dalloc(ctx, &deg, n + 1));
     TRY(dalloc(ctx, &cursor, n + 1));
-    TRY(dalloc(ctx, &lstate, std::max<long long>(L, 1)));
+    TRY(dalloc(ctx, &ctx->linkState, std::max<long long>(L, 1)));
+    uint8_t *lstate = ctx->linkState;
     CK(cudaMemsetAsync(deg, 0, 4 * (size_t)(n + 1), st));
     CK(cudaMemsetAsync(cursor, 0, 4 * (size_t)(n + 1), st));
     if (L > 0) {
@@ -1663,7 +1666,6 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     CK(cudaGetLastError());
     dfree(deg);
     dfree(cursor);
-    dfree(lstate);
     ctx->L = L;
     ctx->haveLinks = true;
     ctx->built = false;

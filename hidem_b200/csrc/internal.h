@@ -132,6 +132,7 @@ struct StepArgs {
     const uint32_t *sPartner; // partner slot | kSideIsB
     LP *ct[6];                // CT0..CT5 per side
     uint8_t *sState;          // per-side state mirror
+    uint8_t *linkState;       // per-link state mirror (input order), kept equal to sState
     const LP *sL0;            // initial length per side
     const int32_t *sLink;     // link index per side
     LP *force;                // [6][n] (split path only)

@@ -553,6 +553,7 @@ __device__ __forceinline__ void step_thread_particle(const Consts<LP> &c, const 
                                     : break_link<LP>(a.bendBreak, a.maxLoad, me, cur, st, L0);
                 if (nst != st) {
                     a.sState[si] = nst;
+                    a.linkState[__ldg(a.sLink + si)] = nst;  // both sides write the same value
                     if (nst == 0 && !(pw & kSideIsB)) {
                         unsigned long long slot = atomicAdd(a.eventCount, 1ull);
                         if ((long long)slot < a.eventCap)
@@ -754,6 +755,7 @@ __device__ __forceinline__ void step_thread_async(const Consts<LP> &c, const Ste
                                     : break_link<LP>(a.bendBreak, a.maxLoad, me, cur, st, L0);
                 if (nst != st) {
                     a.sState[si] = nst;
+                    a.linkState[__ldg(a.sLink + si)] = nst;  // both sides write the same value
                     if (nst == 0 && !(pw & kSideIsB)) {
                         unsigned long long slot = atomicAdd(a.eventCount, 1ull);
                         if ((long long)slot < a.eventCap)
@@ -961,6 +963,7 @@ __device__ __forceinline__ void step_items_block(const Consts<LP> &c, const Step
                                     : break_link<LP>(a.bendBreak, a.maxLoad, me, o, st, L0);
                 if (nst != st) {
                     a.sState[si] = nst;
+                    a.linkState[__ldg(a.sLink + si)] = nst;  // both sides write the same value
                     if (nst == 0 && !(pw & kSideIsB)) {
                         unsigned long long slot = atomicAdd(a.eventCount, 1ull);
                         if ((long long)slot < a.eventCap)
@@ -1124,20 +1127,22 @@ template <class LP>
 __global__ void k_link_break(const Consts<LP> c, const PRec<LP> *__restrict__ rec,
                              const int *__restrict__ slotOf, const int *__restrict__ linkA,
                              const int *__restrict__ linkB, const int *__restrict__ sideSlot,
-                             uint8_t *__restrict__ sState, const LP *__restrict__ sL0, long long L,
-                             long long step, int2 *__restrict__ events,
-                             unsigned long long *__restrict__ eventCount, long long eventCap) {
+                             uint8_t *__restrict__ sState, uint8_t *__restrict__ linkState,
+                             const LP *__restrict__ L0link, long long L, long long step,
+                             int2 *__restrict__ events, unsigned long long *__restrict__ eventCount,
+                             long long eventCap) {
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     bool broke = false;
     if (l < L) {
-        int sA = sideSlot[2 * l];
-        uint8_t st = sState[sA];
+        // state and initial length in link order (coalesced); the side copies only on a change
+        uint8_t st = linkState[l];
         if (st != 0) {
-            const PRec<LP> pa = load_rec(rec + slotOf[linkA[l]]);
-            const PRec<LP> pb = load_rec(rec + slotOf[linkB[l]]);
-            uint8_t nst = break_link<LP>(c, pa, pb, st, sL0[sA]);
+            const PRec<LP> pa = load_rec(rec + slotOf[__ldg(linkA + l)]);
+            const PRec<LP> pb = load_rec(rec + slotOf[__ldg(linkB + l)]);
+            uint8_t nst = break_link<LP>(c, pa, pb, st, __ldg(L0link + l));
             if (nst != st) {
-                sState[sA] = nst;
+                linkState[l] = nst;
+                sState[sideSlot[2 * l]] = nst;
                 sState[sideSlot[2 * l + 1]] = nst;
                 broke = (nst == 0);
             }
@@ -1353,11 +1358,13 @@ void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, c
 template <class LP>
 void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slotOf,
                        const int *linkA, const int *linkB, const int *sideSlot, uint8_t *sState,
-                       const LP *sL0, long long L, long long step, int2 *events,
-                       unsigned long long *eventCount, long long eventCap, cudaStream_t s) {
+                       uint8_t *linkState, const LP *L0link, long long L, long long step,
+                       int2 *events, unsigned long long *eventCount, long long eventCap,
+                       cudaStream_t s) {
     if (L <= 0) return;
     k_link_break<LP><<<nblk(L, 256), 256, 0, s>>>(c, rec, slotOf, linkA, linkB, sideSlot, sState,
-                                                  sL0, L, step, events, eventCount, eventCap);
+                                                  linkState, L0link, L, step, events, eventCount,
+                                                  eventCap);
 }
 
 // Kinetic energy with the integrate step's mass and moment of inertia (m = rho d^3,
@@ -1517,7 +1524,7 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \
-                                        const int *, const int *, const int *, uint8_t *,          \
+                                        const int *, const int *, const int *, uint8_t *, uint8_t *, \
                                         const LP *, long long, long long, int2 *,                  \
                                         unsigned long long *, long long, cudaStream_t);            \
     template void launch_max_diff<LP>(const PRec<LP> *, int, unsigned long long *, int,            \

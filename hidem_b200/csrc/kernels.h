@@ -168,8 +168,9 @@ void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, c
 template <class LP>
 void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slotOf,
                        const int *linkA, const int *linkB, const int *sideSlot, uint8_t *sState,
-                       const LP *sL0, long long L, long long step, int2 *events,
-                       unsigned long long *eventCount, long long eventCap, cudaStream_t s);
+                       uint8_t *linkState, const LP *L0link, long long L, long long step,
+                       int2 *events, unsigned long long *eventCount, long long eventCap,
+                       cudaStream_t s);
 // Kinetic energy of the particles (double precision): out[0] translational, out[1]
 // rotational, out[2] largest squared speed; `partial` holds 3 * nb doubles
 template <class LP>
