@@ -86,6 +86,7 @@ struct hidem_ctx {
     int32_t *linkA = nullptr, *linkB = nullptr;
     void *L0link = nullptr;
     uint8_t *linkState = nullptr;  // per-link state, kept equal to the sides' states
+    int32_t *linkSlotA = nullptr, *linkSlotB = nullptr;  // both ends' slots since the last rebuild
     int32_t *plStart = nullptr, *plLink = nullptr;
     uint8_t *plEnd = nullptr;
     int32_t *sideSlot[2] = {nullptr, nullptr};
@@ -451,6 +452,10 @@ hidem_status rebuild(hidem_ctx *ctx) {
                        ctx->type[nd], ctx->orig[od], ctx->orig[nd], ctx->cellOf[od],
                        ctx->cellOf[nd], ctx->slotOf, st);
     ctx->launches += 3;
+    if (ctx->L > 0) {
+        launch_link_slots(ctx->linkA, ctx->linkB, ctx->slotOf, ctx->L, ctx->linkSlotA, ctx->linkSlotB, st);
+        ctx->launches += 1;
+    }
     ctx->cur = nxt;
     ctx->ord = nd;
     const int c = nd;   // slot-order arrays
@@ -684,8 +689,13 @@ bool break_active(hidem_ctx *ctx, long long t) {
 template <class LP>
 hidem_status link_update_now(hidem_ctx *ctx, long long tagStep) {
     SideSet &s = ctx->side[ctx->curSide];
-    launch_link_break<LP>(consts<LP>(ctx), recp<LP>(ctx, ctx->cur), ctx->slotOf, ctx->linkA,
-                          ctx->linkB, ctx->sideSlot[ctx->curSide], s.state, ctx->linkState,
+    // the ends' slots are refreshed at every rebuild; before one, from the current slotOf
+    if (!ctx->built && ctx->L > 0) {
+        launch_link_slots(ctx->linkA, ctx->linkB, ctx->slotOf, ctx->L, ctx->linkSlotA, ctx->linkSlotB, ctx->stream);
+        ctx->launches += 1;
+    }
+    launch_link_break<LP>(consts<LP>(ctx), recp<LP>(ctx, ctx->cur), ctx->linkSlotA, ctx->linkSlotB,
+                          ctx->sideSlot[ctx->curSide], s.state, ctx->linkState,
                           static_cast<const LP *>(ctx->L0link), ctx->L, tagStep, ctx->events,
                           ctx->eventCount, ctx->eventCap, ctx->stream);
     if (ctx->L > 0) ctx->launches += 1;
@@ -1433,6 +1443,8 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->linkB);
     dfree(ctx->L0link);
     dfree(ctx->linkState);
+    dfree(ctx->linkSlotA);
+    dfree(ctx->linkSlotB);
     dfree(ctx->plStart);
     dfree(ctx->plLink);
     dfree(ctx->plEnd);
@@ -1631,6 +1643,8 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     TRY(dalloc(ctx, &deg, n + 1));
     TRY(dalloc(ctx, &cursor, n + 1));
     TRY(dalloc(ctx, &ctx->linkState, std::max<long long>(L, 1)));
+    TRY(dalloc(ctx, &ctx->linkSlotA, std::max<long long>(L, 1)));
+    TRY(dalloc(ctx, &ctx->linkSlotB, std::max<long long>(L, 1)));
     uint8_t *lstate = ctx->linkState;
     CK(cudaMemsetAsync(deg, 0, 4 * (size_t)(n + 1), st));
     CK(cudaMemsetAsync(cursor, 0, 4 * (size_t)(n + 1), st));

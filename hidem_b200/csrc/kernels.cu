@@ -1125,8 +1125,8 @@ __global__ void k_integrate(const Consts<LP> c, PRec<LP> *__restrict__ rec,
 // flag-and-select append of the links that broke.
 template <class LP>
 __global__ void k_link_break(const Consts<LP> c, const PRec<LP> *__restrict__ rec,
-                             const int *__restrict__ slotOf, const int *__restrict__ linkA,
-                             const int *__restrict__ linkB, const int *__restrict__ sideSlot,
+                             const int *__restrict__ endA, const int *__restrict__ endB,
+                             const int *__restrict__ sideSlot,
                              uint8_t *__restrict__ sState, uint8_t *__restrict__ linkState,
                              const LP *__restrict__ L0link, long long L, long long step,
                              int2 *__restrict__ events, unsigned long long *__restrict__ eventCount,
@@ -1137,8 +1137,8 @@ __global__ void k_link_break(const Consts<LP> c, const PRec<LP> *__restrict__ re
         // state and initial length in link order (coalesced); the side copies only on a change
         uint8_t st = linkState[l];
         if (st != 0) {
-            const PRec<LP> pa = load_rec(rec + slotOf[__ldg(linkA + l)]);
-            const PRec<LP> pb = load_rec(rec + slotOf[__ldg(linkB + l)]);
+            const PRec<LP> pa = load_rec(rec + __ldg(endA + l));
+            const PRec<LP> pb = load_rec(rec + __ldg(endB + l));
             uint8_t nst = break_link<LP>(c, pa, pb, st, __ldg(L0link + l));
             if (nst != st) {
                 linkState[l] = nst;
@@ -1356,13 +1356,12 @@ void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, c
 }
 
 template <class LP>
-void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slotOf,
-                       const int *linkA, const int *linkB, const int *sideSlot, uint8_t *sState,
-                       uint8_t *linkState, const LP *L0link, long long L, long long step,
-                       int2 *events, unsigned long long *eventCount, long long eventCap,
-                       cudaStream_t s) {
+void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *endA, const int *endB,
+                       const int *sideSlot, uint8_t *sState, uint8_t *linkState, const LP *L0link,
+                       long long L, long long step, int2 *events, unsigned long long *eventCount,
+                       long long eventCap, cudaStream_t s) {
     if (L <= 0) return;
-    k_link_break<LP><<<nblk(L, 256), 256, 0, s>>>(c, rec, slotOf, linkA, linkB, sideSlot, sState,
+    k_link_break<LP><<<nblk(L, 256), 256, 0, s>>>(c, rec, endA, endB, sideSlot, sState,
                                                   linkState, L0link, L, step, events, eventCount,
                                                   eventCap);
 }
@@ -1524,7 +1523,7 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \
-                                        const int *, const int *, const int *, uint8_t *, uint8_t *, \
+                                        const int *, const int *, uint8_t *, uint8_t *,            \
                                         const LP *, long long, long long, int2 *,                  \
                                         unsigned long long *, long long, cudaStream_t);            \
     template void launch_max_diff<LP>(const PRec<LP> *, int, unsigned long long *, int,            \
@@ -1713,6 +1712,24 @@ void launch_link_keys_identity(const long long *keyA, const long long *keyB, lon
 
 __global__ void k_iota32(int *out, int count) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) out[i] = i;
+}
+
+// slots of both ends of every link in the current storage order (after a rebuild's permute)
+__global__ void k_link_slots(const int *__restrict__ linkA, const int *__restrict__ linkB,
+                             const int *__restrict__ slotOf, long long L, int *__restrict__ slotA,
+                             int *__restrict__ slotB) {
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < L;
+         l += (long long)gridDim.x * blockDim.x) {
+        slotA[l] = slotOf[linkA[l]];
+        slotB[l] = slotOf[linkB[l]];
+    }
+}
+
+void launch_link_slots(const int *linkA, const int *linkB, const int *slotOf, long long L, int *slotA,
+                       int *slotB, cudaStream_t st) {
+    if (L <= 0) return;
+    const int nb = (int)std::min<long long>((L + 255LL) / 256, 148LL * 32);
+    k_link_slots<<<nb, 256, 0, st>>>(linkA, linkB, slotOf, L, slotA, slotB);
 }
 
 void launch_iota32(int *out, int count, cudaStream_t st) {

@@ -166,11 +166,14 @@ template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,
                       int n, cudaStream_t s);
 template <class LP>
-void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *slotOf,
-                       const int *linkA, const int *linkB, const int *sideSlot, uint8_t *sState,
-                       uint8_t *linkState, const LP *L0link, long long L, long long step,
-                       int2 *events, unsigned long long *eventCount, long long eventCap,
-                       cudaStream_t s);
+// endA / endB: the storage slots of every link's two ends
+void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *endA, const int *endB,
+                       const int *sideSlot, uint8_t *sState, uint8_t *linkState, const LP *L0link,
+                       long long L, long long step, int2 *events, unsigned long long *eventCount,
+                       long long eventCap, cudaStream_t s);
+// slotA[l] = slotOf[linkA[l]], slotB[l] = slotOf[linkB[l]]
+void launch_link_slots(const int *linkA, const int *linkB, const int *slotOf, long long L, int *slotA,
+                       int *slotB, cudaStream_t st);
 // Kinetic energy of the particles (double precision): out[0] translational, out[1]
 // rotational, out[2] largest squared speed; `partial` holds 3 * nb doubles
 template <class LP>
