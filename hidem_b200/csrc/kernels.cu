@@ -1106,6 +1106,129 @@ __global__ void __launch_bounds__(KIND == HIDEM_STEP_KERNEL_ITEMS ? kItemThreads
     }
 }
 
+// ---- the two-pass step over a batch (three launches per step and group) ----
+
+// the entry whose CTA range holds block b (last entry with firstBlocks[e] <= b) and the
+// run's launch counter, in shared memory
+__device__ __forceinline__ void batch_locate(const int *firstBlocks, int nentries, const BatchCounter *ctr,
+                                             int &run, int &entry) {
+    __shared__ int sRun, sEntry;
+    if (threadIdx.x == 0) {
+        sRun = *reinterpret_cast<const volatile int *>(&ctr->s);
+        int lo = 0, hi = nentries - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(firstBlocks + mid) <= (int)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        sEntry = lo;
+    }
+    __syncthreads();
+    run = sRun;
+    entry = sEntry;
+}
+
+template <class LP>
+__global__ void __launch_bounds__(kStepThreads, kCapBlocksForces<LP>)
+    k_force_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
+                  const int *__restrict__ firstBlocks, int nentries, const BatchCounter *__restrict__ ctr) {
+    int s, ei;
+    batch_locate(firstBlocks, nentries, ctr, s, ei);
+    const BatchEntry<LP> &e = entries[ei];
+    StepArgs<LP> a = e.a;
+    a.in = e.rec[e.cur0];
+    a.out = e.rec[e.cur0];
+    a.step = e.step0 + s;
+    a.breakPending = 0;
+    a.reduceDiff = 0;
+    const int lb = (int)blockIdx.x - __ldg(firstBlocks + ei);
+    step_thread_particle<LP, false>(c, a, lb * kStepThreads + threadIdx.x);
+}
+
+template <class LP>
+__global__ void __launch_bounds__(kStepThreads)
+    k_integrate_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
+                      const int *__restrict__ firstBlocks, int nentries, const BatchCounter *__restrict__ ctr) {
+    int s, ei;
+    batch_locate(firstBlocks, nentries, ctr, s, ei);
+    const BatchEntry<LP> &e = entries[ei];
+    const long long step = e.step0 + s;
+    const int lb = (int)blockIdx.x - __ldg(firstBlocks + ei);
+    const int i = lb * kStepThreads + threadIdx.x;
+    const int n = e.a.n;
+    PRec<LP> *rec = e.rec[e.cur0];
+    if (e.reduceEvery10 && step % 10 == 0 && lb == 0 && threadIdx.x < 3) e.a.diffMax[threadIdx.x] = 0ull;
+    LP dmax[3] = {LP(0), LP(0), LP(0)};
+    if (i < n) {
+        PRec<LP> me = load_rec(rec + i);
+        LP F[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) F[q] = e.a.force[(long long)q * n + i];
+        integrate_particle<LP>(c, me, e.a.type[i], F);
+        store_rec(rec + i, me);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) dmax[q] = me.d[q] > LP(0) ? me.d[q] : LP(0);
+    }
+    if (e.reduceEvery10 && (step + 1) % 10 == 0) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            LP m = dmax[q];
+            for (int o = 16; o > 0; o >>= 1) {
+                LP u = __shfl_xor_sync(0xffffffffu, m, o);
+                m = (u > m) ? u : m;
+            }
+            if ((threadIdx.x & 31) == 0 && m > LP(0)) atomicMax(e.a.diffMax + q, max_bits(m));
+        }
+    }
+}
+
+template <class LP>
+__global__ void __launch_bounds__(kStepThreads)
+    k_break_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
+                  const int *__restrict__ firstBlocks, int nentries, BatchCounter *__restrict__ ctr,
+                  int totalBlocks) {
+    int s, ei;
+    batch_locate(firstBlocks, nentries, ctr, s, ei);
+    const BatchEntry<LP> &e = entries[ei];
+    const long long step = e.step0 + s;
+    // the sample main's gate t dt > breakTime (MainMeshBlock.cpp:312), in lp
+    if ((LP)((LP)step * c.dt) > c.breakTime && e.L > 0) {
+        const int b0 = __ldg(firstBlocks + ei);
+        const int nb = __ldg(firstBlocks + ei + 1) - b0;
+        const long long chunk = (e.L + nb - 1) / nb;
+        const long long l0 = (long long)((int)blockIdx.x - b0) * chunk;
+        const long long l1 = min(e.L, l0 + chunk);
+        const PRec<LP> *rec = e.rec[e.cur0];
+        for (long long l = l0 + threadIdx.x; l < l1; l += kStepThreads) {
+            const uint8_t st = e.a.linkState[l];
+            if (st == 0) continue;
+            const PRec<LP> pa = load_rec(rec + __ldg(e.slotA + l));
+            const PRec<LP> pb = load_rec(rec + __ldg(e.slotB + l));
+            const uint8_t nst = break_link<LP>(e.a.bendBreak, e.a.maxLoad, pa, pb, st, __ldg(e.L0link + l));
+            if (nst != st) {
+                e.a.linkState[l] = nst;
+                e.a.sState[e.sideSlot[2 * l]] = nst;
+                e.a.sState[e.sideSlot[2 * l + 1]] = nst;
+                if (nst == 0) {
+                    const unsigned long long slot = atomicAdd(e.a.eventCount, 1ull);
+                    if ((long long)slot < e.a.eventCap) e.a.events[slot] = make_int2((int)l, (int)step);
+                }
+            }
+        }
+    }
+    // the last CTA to finish advances the counter for the next step of the run
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int prev = atomicAdd(&ctr->done, 1u);
+        if (prev == (unsigned int)totalBlocks - 1u) {
+            ctr->done = 0u;
+            ctr->s = s + 1;
+            __threadfence();
+        }
+    }
+}
+
 // HiDEMLib::applyForce with the integrate step, in place (split path).
 template <class LP>
 __global__ void k_integrate(const Consts<LP> c, PRec<LP> *__restrict__ rec,
@@ -1350,6 +1473,14 @@ void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const
 }
 
 template <class LP>
+void launch_two_pass_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
+                           int nentries, BatchCounter *ctr, int totalBlocks, cudaStream_t s) {
+    k_force_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, nentries, ctr);
+    k_integrate_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, nentries, ctr);
+    k_break_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, nentries, ctr, totalBlocks);
+}
+
+template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,
                       int n, cudaStream_t s) {
     k_integrate<LP><<<nblk(n, 256), 256, 0, s>>>(c, rec, type, force, n);
@@ -1520,6 +1651,8 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
     template void prepare_step_batch<LP>();                                                        \
     template void launch_step_batch<LP>(const Consts<LP> &, const BatchEntry<LP> *, const int *,     \
                                         int, BatchCounter *, int, int, int, int, cudaStream_t);    \
+    template void launch_two_pass_batch<LP>(const Consts<LP> &, const BatchEntry<LP> *, const int *, \
+                                            int, BatchCounter *, int, cudaStream_t);               \
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \

@@ -140,6 +140,10 @@ struct BatchEntry {
     int cur0;           // record buffer holding the state at launch 0
     int pend0;          // link update of step0 - 1 still to apply at launch 0
     int reduceEvery10;  // gridService reads the diff maxima every 10 steps
+    // the break pass of two-pass runs: both ends' slots, side slots, initial lengths
+    const int *slotA, *slotB, *sideSlot;
+    const LP *L0link;
+    long long L;
 };
 // Launch counter shared by a run of batched launches: launch s reads s; the last CTA to
 // finish sets s + 1 for the next launch in the stream.
@@ -161,6 +165,13 @@ template <class LP>
 void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
                        int nentries, BatchCounter *ctr, int totalBlocks, int maxContacts,
                        int maxEnds, int kernel, cudaStream_t s);
+
+// the two-pass step over a run's entries: force pass, integrate pass (in place, with the
+// diff maxima every 10 steps), break pass (when t dt > breakTime; it advances the run's
+// counter); totalBlocks as for the thread kernels
+template <class LP>
+void launch_two_pass_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
+                           int nentries, BatchCounter *ctr, int totalBlocks, cudaStream_t s);
 
 template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,

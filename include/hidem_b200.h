@@ -437,14 +437,16 @@ int32_t hidem_get_step_kernel(const hidem_ctx *ctx);
 
 /* No counterpart in the reference (one HiDEMLib instance runs one particle set per
  * rank). Many independent contexts (ice blocks of uneven sizes) on one device and of one
- * precision advance together: every timestep is one kernel launch over all contexts
- * that share their constants apart from the break thresholds (maxLoad, bendBreak may
- * differ per context; contexts that differ in anything else form further launches), and
- * the launches between two gridService points (at most 10 steps) are replayed from a
- * CUDA graph when HIDEM_BATCH_GRAPHS is set. Each context's results are bit-identical to
- * hidem_step on that context alone: the batch runs the same gridService policy, the same
- * fused step and the same deferred link update per context. The step kernel is the first
- * context's (hidem_set_step_kernel; AUTO or untimed means THREAD_CAPPED).
+ * precision advance together: every timestep is one launch (three for the two-pass
+ * step: force, integrate and break passes) over all contexts that share their constants
+ * apart from the break thresholds (maxLoad, bendBreak may differ per context; contexts
+ * that differ in anything else form further launches), and the launches between two
+ * gridService points (at most 10 steps) are replayed from a CUDA graph when
+ * HIDEM_BATCH_GRAPHS is set. Each context's results are bit-identical to hidem_step on
+ * that context alone: the batch runs the same gridService policy and the same step and
+ * link update per context. The step kernel is the first context's
+ * (hidem_set_step_kernel; AUTO or untimed means TWO_PASS, THREAD_ASYNC runs as
+ * THREAD_CAPPED).
  * HIDEM_BATCH_PER_CONTEXT runs the single-context launch sequence context after context
  * instead (the same results, for comparison); rows too wide for the ITEMS kernel's shared
  * memory take that path too. During a batch call the contexts' work runs on the batch's

@@ -74,7 +74,8 @@ def assert_same(a, b):
 
 
 @pytest.mark.parametrize("precision", PRECS)
-@pytest.mark.parametrize("mode", ["graphs", "launches", "per_context", "items", "thread"])
+@pytest.mark.parametrize("mode", ["graphs", "launches", "per_context", "items", "thread", "two_pass",
+                                  "two_pass_launches"])
 def test_batch_equals_individual_runs(gpu, precision, mode):
     blocks = mixed_blocks(precision)
     alone = []
@@ -85,9 +86,12 @@ def test_batch_equals_individual_runs(gpu, precision, mode):
         alone.append(snapshot(lib))
         lib.close()
     libs = [open_lib(P, p, l, start) for P, p, l, start in blocks]
-    if mode in ("items", "thread"):  # the batch runs the first context's step kernel
-        libs[0].set_step_kernel(abi.STEP_KERNEL_ITEMS if mode == "items" else abi.STEP_KERNEL_THREAD)
-    batch = HiDEMBatch(libs, graphs=(mode != "launches"), per_context=(mode == "per_context"))
+    kernels = {"items": abi.STEP_KERNEL_ITEMS, "thread": abi.STEP_KERNEL_THREAD,
+               "two_pass": abi.STEP_KERNEL_TWO_PASS, "two_pass_launches": abi.STEP_KERNEL_TWO_PASS}
+    if mode in kernels:  # the batch runs the first context's step kernel
+        libs[0].set_step_kernel(kernels[mode])
+    batch = HiDEMBatch(libs, graphs=(mode not in ("launches", "two_pass_launches")),
+                       per_context=(mode == "per_context"))
     batch.step(13)
     batch.step(24)
     counts = batch.counts()
@@ -99,9 +103,9 @@ def test_batch_equals_individual_runs(gpu, precision, mode):
         assert counts["launches"] == 37 * len(blocks)
     else:
         # three groups of shared constants: the falling block (g, no fixed layer), the
-        # block with another E, and the rest
-        assert counts["launches"] == 37 * 3
-    if mode in ("graphs", "items", "thread"):
+        # block with another E, and the rest; the two-pass step is three launches
+        assert counts["launches"] == 37 * 3 * (3 if mode.startswith("two_pass") else 1)
+    if mode in ("graphs", "items", "thread", "two_pass"):
         assert counts["graph_launches"] > 0
     assert sum(r[3] for r in alone) > len(blocks)  # rebuilds happened inside the runs
 
