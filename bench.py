@@ -373,7 +373,9 @@ def main_ensemble(args):
     achieved = bytes_step / kern_step_s / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                "kernel": "k_step_batch (" + KERNEL_NAMES[kernel if kernel else abi.STEP_KERNEL_THREAD_CAPPED] + ")",
+                "kernel": ("batched two-pass step (k_force_batch, k_integrate_batch, k_break_batch)"
+                           if kernel in (abi.STEP_KERNEL_AUTO, abi.STEP_KERNEL_TWO_PASS)
+                           else "k_step_batch (" + KERNEL_NAMES[kernel] + ")"),
                 "kernel_ms": kern_step_s * 1e3,
                 "algorithmic_bytes_per_launch": bytes_step}
 
