@@ -194,10 +194,18 @@ def links_keys(parts: list, layout: SlabLayout, L: int) -> dict:
     return {"globalKeyEndA": ka, "globalKeyEndB": kb}
 
 
-def halo_width(search_distance: float, interact_distance: float, max_radius: float) -> float:
+def contact_reach(search_distance: float, interact_distance: float, max_radius: float) -> float:
     """Reach of a contact-list pair at a rebuild (NeighAccel.h:104-114:
     d - (r_i + r_j) < interactDist), with 1 % to spare for the rounding of d."""
     return 1.01 * max(search_distance, 2.0 * max_radius + interact_distance)
+
+
+def halo_width(search_distance: float, interact_distance: float, max_radius: float,
+               slack: float = 0.5) -> float:
+    """The contact reach plus `slack` of it, the room particles may move in x between two
+    distributions (rebuilds in between keep the held sets while no particle has moved
+    more than half the room)."""
+    return (1.0 + slack) * contact_reach(search_distance, interact_distance, max_radius)
 
 
 # ---------------------------------------------------------------------------------------
@@ -292,7 +300,8 @@ class SlabRun:
     every process. Steps follow the sample main: gridService, computePartForce (with the
     halo force exchange), applyForce, linkUpdate when t*dt > breakTime, finalizeTs."""
 
-    def __init__(self, comm, libs: list, particles: dict, links: dict, halo: float | None = None):
+    def __init__(self, comm, libs: list, particles: dict, links: dict, halo: float | None = None,
+                 slack: float = 0.5):
         import torch
         if len(libs) != len(comm.ranks):
             raise ValueError("one context per rank of this process")
@@ -302,27 +311,32 @@ class SlabRun:
         self.precision = int(self.libs[0].precision)
         self.lp = abi.lp_dtype(self.precision)
         self._tdtype = torch.float32 if self.lp == np.float32 else torch.float64
-        self._halo = halo
+        self._halo, self._slack = halo, float(slack)
         self.redistributions = 0
+        self.kept = 0           # rebuilds that kept the held sets (no redistribution)
         self.exchanged = 0      # halo force records moved so far (all ranks of this process)
         self._distribute(particles, links)
 
     # -- state movement
-    def _halo_width(self, particles: dict) -> float:
-        if self._halo is not None:
-            return float(self._halo)
+    def _widths(self, particles: dict) -> tuple[float, float]:
+        """(contact reach, halo width)."""
         s = self.libs[0].stats()
         rmax = float(np.max(particles["radius"])) if self.n else 0.0
         rmax = float(self.comm.allmax([np.array([rmax])])[0])
-        return halo_width(s["search_distance"], s["interact_distance"], rmax)
+        reach = contact_reach(s["search_distance"], s["interact_distance"], rmax)
+        width = float(self._halo) if self._halo is not None else (1.0 + self._slack) * reach
+        return reach, width
 
     def _distribute(self, particles: dict, links: dict) -> None:
         import torch
         a, b = link_ends(particles, links)
-        self.layout = slab_layout(particles["xCord"], a, b, self.comm.size, self._halo_width(particles))
+        self._reach, self._width = self._widths(particles)
+        self.layout = slab_layout(particles["xCord"], a, b, self.comm.size, self._width)
         self.send_bufs, self.recv_bufs = [], []
+        self._x0 = []
         for lib, r in zip(self.libs, self.comm.ranks):
             p, l = split_state(particles, links, self.layout, r)
+            self._x0.append(p["xCord"].copy())
             lib.set_particles(p)
             lib.set_links(l)
             snd, rcv = self.layout.send_list(r), self.layout.recv_list(r)
@@ -345,9 +359,19 @@ class SlabRun:
         regen = [np.array([1.0 if lib.grid_service_decide(mx) else 0.0]) for lib in self.libs]
         if not self.comm.allmax(regen)[0]:
             return
-        # rebalance: every particle to the owner of its slab, recut, halos rebuilt
-        particles, links = self.gather()
-        self._distribute(particles, links)
+        # Each rank's held set contains every contact partner of its own particles while
+        # no particle has moved more than half the halo's room in x since the last
+        # distribution (partners lie within the reach; each end moved at most that much):
+        # then the rebuild keeps the held sets, else every particle goes to the owner of
+        # its slab, the slabs are recut and the halos rebuilt.
+        moved = [np.array([float(np.max(np.abs(lib.get_particles()["xCord"] - x0))) if x0.size else 0.0])
+                 for lib, x0 in zip(self.libs, self._x0)]
+        delta = float(self.comm.allmax(moved)[0])
+        if 2.0 * delta > self._width - self._reach:
+            particles, links = self.gather()
+            self._distribute(particles, links)
+        else:
+            self.kept += 1
         bounds = [lib.local_bounds() for lib in self.libs]
         lo = -self.comm.allmax([-b[0] for b in bounds])
         hi = self.comm.allmax([b[1] for b in bounds])
