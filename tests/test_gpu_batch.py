@@ -103,8 +103,9 @@ def test_batch_equals_individual_runs(gpu, precision, mode):
         assert counts["launches"] == 37 * len(blocks)
     else:
         # three groups of shared constants: the falling block (g, no fixed layer), the
-        # block with another E, and the rest; the two-pass step is three launches
-        assert counts["launches"] == 37 * 3 * (3 if mode.startswith("two_pass") else 1)
+        # block with another E, and the rest; the two-pass step (the default) is three
+        # launches, the fused kernels one
+        assert counts["launches"] == 37 * 3 * (1 if mode in ("items", "thread") else 3)
     if mode in ("graphs", "items", "thread", "two_pass"):
         assert counts["graph_launches"] > 0
     assert sum(r[3] for r in alone) > len(blocks)  # rebuilds happened inside the runs
