@@ -5,7 +5,8 @@ Method names follow ``HiDEMLib<PDataT, LDataT>`` (HiDEMLib/HiDEMLib.h): ``gridSe
 ``applyForce`` (303-314) with the sample integrate step, ``linkUpdate`` (256-269) with the
 default break functor, ``finalizeTs`` (495-530), ``getCurrentTimestep`` (245-247), ``run``
 (234-240). ``step(n)`` runs n whole timesteps of the sample main loop
-(HiDEM/MeshBlock/MainMeshBlock.cpp:274-323) as one fused kernel per step.
+(HiDEM/MeshBlock/MainMeshBlock.cpp:274-323) on the device, each as the context's step kernel
+(one fused kernel, or the two-pass step's passes).
 
 Errors follow the C ABI: every failing call raises ``HidemError`` carrying the status and
 ``hidem_last_error`` text (the reference would print and ``exit(1)``).
@@ -224,7 +225,7 @@ class HiDEMLib:
         return int(self._lib.hidem_get_step_kernel(self._ctx))
 
     def profile(self, enable: bool = True) -> None:
-        """CUDA-event timing of the fused step kernel on the context's stream."""
+        """CUDA-event timing of each step's kernels on the context's stream."""
         self._check(self._lib.hidem_profile(self._ctx, 1 if enable else 0))
 
     def profile_read(self) -> tuple[float, int]:

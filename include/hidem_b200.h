@@ -241,8 +241,10 @@ hidem_status hidem_pack_halo_forces(hidem_ctx *ctx, void *device_out);
  * wait for the data (CommunicatorPacked::unpackAllCommData). */
 hidem_status hidem_unpack_halo_forces(hidem_ctx *ctx, const void *device_in);
 /* n whole timesteps of the sample main loop (MainMeshBlock.cpp:274-323):
- * gridService, forces, integrate, gated link update, finalizeTs — as one fused
- * kernel per step, graph-launched between rebuild checks. */
+ * gridService, forces, integrate, gated link update, finalizeTs — each step as the
+ * context's step kernel (hidem_set_step_kernel: one fused kernel, or the two-pass step's
+ * force and integrate passes and break pass), launched back to back between the
+ * gridService checks without host synchronisation. */
 hidem_status hidem_step(hidem_ctx *ctx, int32_t nsteps);
 /* The default functors as a caller's main constructs them (HiDEM/Common/
  * HiDEMDefaultFunctions.h): HiDEMDefNeighForceFunc(invDt, attractDistance,
@@ -266,8 +268,9 @@ hidem_status hidem_synchronize(hidem_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work
  * on it (e.g. CUDA events recorded on the same stream). */
 void *hidem_get_stream(hidem_ctx *ctx);
-/* Turns CUDA-event timing of the fused step kernel on (1) or off (0) and clears the
- * record; hidem_profile_read sums the kernel time of the launches since then. */
+/* Turns CUDA-event timing of each step's kernels (the fused kernel, or the two-pass
+ * step's passes) on (1) or off (0) and clears the record; hidem_profile_read sums their
+ * time over the steps since then and returns the number of steps timed. */
 hidem_status hidem_profile(hidem_ctx *ctx, int32_t enable);
 hidem_status hidem_profile_read(hidem_ctx *ctx, double *step_kernel_ms, int64_t *launches);
 
