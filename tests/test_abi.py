@@ -79,6 +79,18 @@ def test_null_context_calls_return_arg_error():
     assert lib.hidem_grid_service(None) == 1
     assert lib.hidem_compute_forces(None) == 1
     assert lib.hidem_last_error(None) == b"null context"
+    # the slab decomposition hooks
+    import ctypes as C
+    import numpy as np
+    mx, lo, hi = np.zeros(3), np.zeros(3), np.ones(3)
+    flag = C.c_int32()
+    assert lib.hidem_grid_service_local(None, mx.ctypes.data, C.byref(flag)) == 1
+    assert lib.hidem_grid_service_decide(None, mx.ctypes.data, C.byref(flag)) == 1
+    assert lib.hidem_local_bounds(None, lo.ctypes.data, hi.ctypes.data) == 1
+    assert lib.hidem_regenerate_frame(None, lo.ctypes.data, hi.ctypes.data) == 1
+    assert lib.hidem_set_halo_exchange(None, None, 0, None, 0) == 1
+    assert lib.hidem_pack_halo_forces(None, None) == 1
+    assert lib.hidem_unpack_halo_forces(None, None) == 1
 
 
 def test_soa_checks_dtypes_and_sizes():
