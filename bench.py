@@ -1,8 +1,8 @@
 """Benchmark of the HiDEM hot path: particle-steps/s on the 5.7M-particle calving slab.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
-                    [--impl ours|reference] [--workload slab|block|ensemble]
-                    [--kernel auto|items|thread|thread-capped]
+                    [--impl ours|reference] [--workload slab|block|ensemble|settle|topo|mesh|ranks]
+                    [--kernel auto|items|thread|thread-capped|thread-async|two-pass]
 
 A "step" is one timestep of the sample main loop (gridService, forces, integrate, link
 update) over the whole slab. `value` times K steps with the state resident in HBM (CUDA
@@ -11,7 +11,10 @@ C ABI from host arrays: upload of the particle and link state, the K steps, down
 the particle state. `roofline` divides the byte model of the step by the event-timed
 duration of the step's kernels (the force, integrate and break passes of the two-pass
 step, or the one kernel of a fused step). `cpu_baseline` times the reference's own CPU path
-(oracle/_ref, built from its sources with its own flags) on the same slab.
+(oracle/_ref, built from its sources with its own flags) on the same slab. The mixed-precision
+slab line also carries `rebuild_amortised` (the configuration's 2000-step run from step 0,
+its rebuilds included), `fp64` (the same slab in the plain FP64 build) and `settle` (the
+learned warm start's settling steps, cold against surrogate-seeded).
 With --gpus N > 1 (torchrun) every rank advances its own replica of the slab (the path
 has no exchange on one node for this workload; weak scaling).
 --impl reference times the reference's CPU implementation on this host's cores.
@@ -71,6 +74,10 @@ def parse():
                     help="slab size in metres x,y,z (smaller slabs for profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="slab: skip the plain-FP64 run")
+    ap.add_argument("--no-settle", action="store_true", help="slab: skip the warm-start settling experiment")
+    ap.add_argument("--amortised-steps", type=int, default=2000,
+                    help="slab: steps of the run with its rebuilds (the configuration's 2000; 0 skips)")
     return ap.parse_args()
 
 
@@ -101,7 +108,9 @@ class ClockSampler:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+              "utilization.gpu")
+    PERIOD_MS = 50
 
     def __init__(self, device: int):
         self.device = device
@@ -112,7 +121,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -131,7 +140,7 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], 0.0, set()
+        sm, busy, mx, reasons = [], [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
@@ -140,6 +149,8 @@ class ClockSampler:
             try:
                 sm.append(float(f[1]))
                 mx = max(mx, float(f[2]))
+                if len(f) > 9 and float(f[9]) >= 50.0:
+                    busy.append(float(f[1]))
             except ValueError:
                 continue
             for nm, v in zip(names, f[5:9]):
@@ -147,8 +158,10 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        under_load = busy if busy else sm
+        return {"sm_mhz": float(np.median(under_load)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm), "samples_under_load": len(busy), "period_ms": self.PERIOD_MS,
+                "span": "from the warm-up through the timed steps and the rebuild-amortised run"}
 
 
 def measured_peak():
@@ -216,20 +229,44 @@ def cpu_baseline(P, p, l, n):
             "kind": "port", "sample": f"3 timesteps of the full workload ({n} particles)"}
 
 
+def make_workload_np(args):
+    """make_workload's slab or block built in numpy (hidem_b200.inputs_np), so that the
+    reference arm's process maps none of this library's native code; the arrays and
+    parameters are the same bit for bit."""
+    from hidem_b200 import abi, inputs_np, workloads
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    if args.workload == "slab":
+        size = tuple(float(v) for v in args.slab.split(","))
+        P, p, l = inputs_np.calving_slab(size=size, precision=prec, jitter=0.0)
+        cells = tuple(max(1, int(round(s / workloads.SQRT2))) for s in size)
+        name = (f"calving slab {size[0]:g}x{size[1]:g}x{size[2]:g} m FCC d=1 m "
+                f"({cells[0]}x{cells[1]}x{cells[2]} cells), bed, water 90 m, 1% pre-broken")
+        return prec, P, p, l, name
+    p = inputs_np.fcc_particles(20, 20, 20, prec, jitter=0.01, seed=1)
+    z0 = p["zCord"].min()
+    p["type"][p["zCord"] < z0 + 0.25 * workloads.SQRT2] |= abi.TYPE_FIXED
+    l = inputs_np.distance_links(p, prec, 1.01)
+    P = inputs_np.default_params(**workloads.block_overrides(prec, useFixed=1))
+    return prec, P, p, l, "ice block 20^3 FCC cells, jitter 0.01 d, bottom fixed"
+
+
 def run_reference(args):
-    """--impl reference: the reference's CPU implementation, K timed steps after W warm-up."""
+    """--impl reference: the reference's CPU implementation (oracle/_ref, its own sources
+    and flags, all host threads), timed steps after W warm-up, on inputs built without this
+    library."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
     from oracle import oracle
-    prec, P, p, l, name = make_workload(args)
+    prec, P, p, l, name = make_workload_np(args)
     n = p["xCord"].shape[0]
     fast_ok = oracle.reference_available(prec, fast=True)
     sess = oracle.RefSession(P, p, l, fast=True) if fast_ok else None
     if sess is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
         return
-    warm_s = sess.advance(max(args.warmup, 1)) / max(args.warmup, 1)
+    warm_n = max(args.warmup, 1)
+    warm_s = sess.advance(warm_n) / warm_n
     # timed steps bounded to about a minute of host time (the rate is what is reported)
     timed = int(min(args.steps, max(3, 60.0 / max(warm_s, 1e-6))))
     secs = sess.advance(timed)
@@ -237,18 +274,18 @@ def run_reference(args):
     sess.close()
     value = n * timed / secs
     line = {
-        "metric": "particle-steps/s (5.7M slab)" if args.workload == "slab" else "particle-steps/s (32k block)",
-        "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * secs / timed, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None,
+        "metric": slab_metric(args),
+        "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": timed,
+        "steps_requested": args.steps, "warmup": warm_n, "ms_per_step": 1e3 * secs / timed,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64pos" if prec == 1 else "f64", "data": "synthetic",
-        "config": {"workload": name, "particles": n, "links": int(l["state"].shape[0]),
-                   "precision": args.precision},
+        "config": slab_config(args, name, n, int(l["state"].shape[0]), world),
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
                          "kind": "reference", "cpu": cpu_model(), "host_threads": os.cpu_count(),
                          "sample": f"{timed} timesteps of the full workload (of the {args.steps} asked, "
-                                   f"bounded to about a minute) after {max(args.warmup, 1)} warm-up"},
+                                   f"bounded to about a minute) after {warm_n} warm-up; inputs "
+                                   f"generated in numpy (hidem_b200.inputs_np)"},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -847,6 +884,270 @@ def main_ranks(args):
         torch.distributed.destroy_process_group()
 
 
+def slab_config(args, name: str, n: int, L: int, world: int) -> dict:
+    """The `config` of the slab line, identical in both arms at the same N."""
+    return {"workload": name, "particles": n, "links": L, "precision": args.precision,
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (records + link ends > 126 MB)"}
+
+
+def slab_metric(args) -> str:
+    return "particle-steps/s (5.7M slab)" if args.workload == "slab" else "particle-steps/s (32k block)"
+
+
+def timed_steps(lib, stream, steps: int, pg=None):
+    """K timesteps between CUDA events on the library's stream (a barrier and device
+    synchronisation on both sides); returns (ms, step-kernel ms per step, launches, stats
+    before, stats after)."""
+    import torch
+    st0 = lib.stats()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    lib.profile(True)
+    e0.record(stream)
+    lib.step(steps)
+    e1.record(stream)
+    lib.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    kern_ms, kern_n = lib.profile_read()
+    lib.profile(False)
+    st1 = lib.stats()
+    return ms, kern_ms / max(kern_n, 1), int(st1["kernel_launches"] - st0["kernel_launches"]), st0, st1
+
+
+def roofline_of(n, L, pairs, prec, kern_step_ms, precision: str, step_kernel: int) -> dict:
+    from hidem_b200 import workloads
+    bytes_step = workloads.algorithmic_bytes(n, L, pairs, prec)["total"]
+    peak, peak_kind = measured_peak()
+    achieved = bytes_step / (kern_step_ms / 1e3) / 1e9
+    dpps = profile_traffic(precision, step_kernel == KERNELS["two-pass"])
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": (dpps * n) if dpps else None,
+            "peak_source": peak_kind, "kernel": step_label(step_kernel),
+            "kernel_ms": kern_step_ms, "algorithmic_bytes_per_launch": bytes_step}
+
+
+def main_slab(args):
+    """The default line: the calving slab in the requested precision (K timed steps, the
+    end-to-end job through the C ABI, the 2000-step run of the configuration with its
+    rebuilds, the roofline, the CPU baseline); with mixed precision also the plain-FP64 run
+    of the same slab and the learned warm start's settling experiment, the two other halves
+    of the metric."""
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    from hidem_b200 import abi
+    from hidem_b200.hidemlib import HiDEMLib
+
+    prec, P, p, l, name = make_workload(args)
+    n = p["xCord"].shape[0]
+    L = l["state"].shape[0]
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    lib = HiDEMLib(P, device=local)
+    lib.set_step_kernel(KERNELS[args.kernel])
+    lib.set_particles(p)
+    lib.set_links(l)
+    stream = torch.cuda.ExternalStream(lib.stream_handle)
+    # warm-up: at least the autotuner's rounds, so the timed steps use its choice
+    warm = max(args.warmup, 15) if args.kernel == "auto" else args.warmup
+    lib.step(warm)
+    lib.synchronize()
+    ms, kern_step_ms, launches, st0, st1 = timed_steps(lib, stream, args.steps, pg)
+    pairs = st1["num_neighbour_pairs"]
+    step_kernel = lib.step_kernel()
+    if pg:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    lib.close()
+    value = world * n * args.steps / (ms / 1e3)
+    roofline = roofline_of(n, L, pairs, prec, kern_step_ms, args.precision, step_kernel)
+
+    # the configuration's whole run (2000 steps from step 0, its rebuilds included), the
+    # step kernel fixed to the tuned one
+    amortised = None
+    if args.amortised_steps > 0:
+        lib = HiDEMLib(P, device=local)
+        lib.set_step_kernel(step_kernel)
+        lib.set_particles(p)
+        lib.set_links(l)
+        s2 = torch.cuda.ExternalStream(lib.stream_handle)
+        ams, akern, alaunch, a0, a1 = timed_steps(lib, s2, args.amortised_steps, pg)
+        if pg:
+            t = torch.tensor([ams], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ams = float(t.item())
+        lib.close()
+        amortised = {"steps": args.amortised_steps, "value": world * n * args.amortised_steps / (ams / 1e3),
+                     "ms_per_step": ams / args.amortised_steps,
+                     "rebuilds": int(a1["regen_count"] - a0["regen_count"]),
+                     "step_kernel_ms_per_step": akern, "gpu_launches": alaunch,
+                     "what": "a fresh context: steps 0..K-1 of the configuration's run, the first "
+                             "step's rebuild and the rebuild policy's later ones included"}
+    clk = clocks.stop()
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n)
+
+    fp64 = None
+    if args.precision == "mixed" and args.workload == "slab" and not args.no_fp64:
+        a64 = argparse.Namespace(**{**vars(args), "precision": "fp64"})
+        prec64, P64, p64, l64, _ = make_workload(a64)
+        lib = HiDEMLib(P64, device=local)
+        lib.set_step_kernel(KERNELS[args.kernel])
+        lib.set_particles(p64)
+        lib.set_links(l64)
+        s64 = torch.cuda.ExternalStream(lib.stream_handle)
+        lib.step(warm)
+        lib.synchronize()
+        ms64, k64, la64, _, b64 = timed_steps(lib, s64, args.steps, pg)
+        sk64 = lib.step_kernel()
+        if pg:
+            t = torch.tensor([ms64], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms64 = float(t.item())
+        lib.close()
+        del p64, l64
+        v64 = world * n * args.steps / (ms64 / 1e3)
+        fp64 = {"value": v64, "unit": "particle-steps/s", "ms_per_step": ms64 / args.steps,
+                "mixed_over_fp64": value / v64, "gpu_launches": la64,
+                "roofline": roofline_of(n, L, b64["num_neighbour_pairs"], prec64, k64, "fp64", sk64),
+                "what": "the same slab and steps in the plain FP64 build (lp = ct = double)"}
+
+    settle = None
+    if args.precision == "mixed" and args.workload == "slab" and not args.no_settle and rank == 0:
+        settle = settle_summary(args)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(P, p, l, n)
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
+                   "sample": f"failed: {ex}"}
+
+    if pg:
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": slab_metric(args),
+        "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": (value / PUBLISHED_MIXED) if (prec == abi.PREC_MIXED and args.workload == "slab") else None,
+        "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
+        "config": slab_config(args, name, n, L, world),
+        "contact_pairs": pairs,
+        "baseline_number": "RTX 5090 1.108e9 particle-steps/s, HiDEM/Docs/Performance.md:68",
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "rebuilds_in_timed_steps": int(st1["regen_count"] - st0["regen_count"]),
+        "rebuild_amortised": amortised, "fp64": fp64, "settle": settle,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
+def e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n):
+    """The same K steps through the C ABI from pinned host buffers: upload of the particle
+    and link state, K steps, download of the particle state; wall time, devices synchronised
+    on both sides."""
+    import torch
+    from hidem_b200 import abi
+    from hidem_b200.hidemlib import HiDEMLib
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.from_numpy(a[:1]).dtype, pin_memory=True)
+        out = t.numpy()
+        out[...] = a
+        return out, t
+    keep = []
+    pp, ll = {}, {}
+    for k, v in p.items():
+        pp[k], t = pinned(v)
+        keep.append(t)
+    # a fresh job's link ends carry no history (CT all zero): like the reference's own
+    # start, which generates its links in place, it uploads none (the library zeroes CT)
+    fresh = not any(l[k].any() for k in ("CT0", "CT1", "CT2", "CT3", "CT4", "CT5") if k in l)
+    for k, v in l.items():
+        if fresh and k.startswith("CT"):
+            continue
+        ll[k], t = pinned(v)
+        keep.append(t)
+    outp = {}
+    for k, v in abi.empty_particles(n, prec).items():
+        outp[k], t = pinned(v)
+        keep.append(t)
+    lib2 = HiDEMLib(P, device=local)
+    lib2.set_step_kernel(step_kernel)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    lib2.set_particles(pp)
+    ta = time.perf_counter()
+    lib2.set_links(ll)
+    tb = time.perf_counter()
+    lib2.step(args.steps)
+    tc = time.perf_counter()
+    lib2.get_particles(outp)
+    lib2.synchronize()
+    t1 = time.perf_counter()
+    el = t1 - t0
+    parts = {"set_particles_s": ta - t0, "set_links_s": tb - ta, "steps_s": tc - tb,
+             "get_particles_s": t1 - tc}
+    if pg:
+        t = torch.tensor([el], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        el = float(t.item())
+    lib2.close()
+    h2d = sum(v.nbytes for v in pp.values()) + sum(v.nbytes for v in ll.values())
+    d2h = sum(v.nbytes for v in outp.values())
+    return {"value": world * n * args.steps / el, "unit": "particle-steps/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "step": f"one C-ABI job from pinned host arrays: upload state (particles, links"
+                    f"{'; side history zero, not uploaded' if fresh else ', side history'}), "
+                    f"{args.steps} timesteps, download particles", "breakdown": parts}
+
+
+def settle_summary(args) -> dict:
+    """The learned warm start's experiment (the settle workload's defaults): held-out
+    tongues settled cold and from the surrogate's prediction, steps to the plain method's
+    convergence test."""
+    import dataclasses
+    from hidem_b200 import settle
+    size = tuple(float(v) for v in args.tongue.split(","))
+    t0 = time.perf_counter()
+    rep = settle.warm_start_experiment(n_train=args.train_tongues, n_test=args.test_tongues, size=size,
+                                       base_thickness=6.0, amplitude=2.0, train_steps=args.train_steps,
+                                       inputs=args.surrogate_inputs)
+    d = dataclasses.asdict(rep)
+    return {"metric": "settle steps, cold / surrogate-warm (KE < 1e-6 J per particle)",
+            "step_ratio": d["step_ratio"],
+            "cold_steps_mean": float(np.mean(d["cold_steps"])),
+            "warm_steps_mean": float(np.mean(d["warm_steps"])),
+            "prediction_rel_error_mean": float(np.mean(d["prediction_rel_error"])),
+            "settled_error_over_d_max": float(np.max(d["settled_error_over_d"])),
+            "converged": {"cold": int(np.sum(d["cold_converged"])), "warm": int(np.sum(d["warm_converged"]))},
+            "tongues": {"size_m": list(size), "train": args.train_tongues, "held_out": args.test_tongues,
+                        "particles_per_tongue": d["particles_per_tongue"]},
+            "seconds": time.perf_counter() - t0}
+
+
 def main():
     args = parse()
     if args.workload == "ranks":
@@ -886,161 +1187,7 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
-    import torch
-    world, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        pg = dist
-    from hidem_b200 import abi, workloads
-    from hidem_b200.hidemlib import HiDEMLib
-
-    prec, P, p, l, name = make_workload(args)
-    n = p["xCord"].shape[0]
-    L = l["state"].shape[0]
-
-    lib = HiDEMLib(P, device=local)
-    lib.set_step_kernel(KERNELS[args.kernel])
-    lib.set_particles(p)
-    lib.set_links(l)
-    stream = torch.cuda.ExternalStream(lib.stream_handle)
-    # warm-up: at least the autotuner's rounds, so the timed steps use its choice
-    warm = max(args.warmup, 15) if args.kernel == "auto" else args.warmup
-    lib.step(warm)
-    lib.synchronize()
-    st0 = lib.stats()
-    pairs = st0["num_neighbour_pairs"]
-
-    clocks = ClockSampler(local)
-    clocks.start()
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    lib.profile(True)
-    e0.record(stream)
-    lib.step(args.steps)
-    e1.record(stream)
-    lib.synchronize()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    kern_ms, kern_n = lib.profile_read()
-    lib.profile(False)
-    clk = clocks.stop()
-    st1 = lib.stats()
-    step_kernel = lib.step_kernel()
-    launches = int(st1["kernel_launches"] - st0["kernel_launches"])
-    if pg:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-        pg.barrier()
-    lib.close()
-
-    value = world * n * args.steps / (ms / 1e3)
-    bytes_step = workloads.algorithmic_bytes(n, L, pairs, prec)["total"]
-    kern_avg_s = (kern_ms / max(kern_n, 1)) / 1e3
-    peak, peak_kind = measured_peak()
-    achieved = bytes_step / kern_avg_s / 1e9
-    two_pass = step_kernel == KERNELS["two-pass"]
-    dpps = profile_traffic(args.precision, two_pass)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": (dpps * n) if dpps else None,
-                "peak_source": peak_kind,
-                "kernel": step_label(step_kernel),
-                "kernel_ms": kern_ms / max(kern_n, 1),
-                "algorithmic_bytes_per_launch": bytes_step}
-
-    e2e = None
-    if not args.no_e2e:
-        # host copies of the inputs and outputs in pinned memory
-        def pinned(a):
-            t = torch.empty(a.shape, dtype=torch.from_numpy(a[:1]).dtype, pin_memory=True)
-            out = t.numpy()
-            out[...] = a
-            return out, t
-        keep = []
-        pp, ll = {}, {}
-        for k, v in p.items():
-            pp[k], t = pinned(v)
-            keep.append(t)
-        # a fresh job's link ends carry no history (CT all zero): like the reference's own
-        # start, which generates its links in place, it uploads none (the library zeroes CT)
-        fresh = not any(l[k].any() for k in ("CT0", "CT1", "CT2", "CT3", "CT4", "CT5") if k in l)
-        for k, v in l.items():
-            if fresh and k.startswith("CT"):
-                continue
-            ll[k], t = pinned(v)
-            keep.append(t)
-        outp = {}
-        for k, v in abi.empty_particles(n, prec).items():
-            outp[k], t = pinned(v)
-            keep.append(t)
-        # the same K steps through the C ABI from host buffers (state upload, K steps,
-        # particle state download)
-        lib2 = HiDEMLib(P, device=local)
-        lib2.set_step_kernel(step_kernel)
-        torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
-        t0 = time.perf_counter()
-        lib2.set_particles(pp)
-        ta = time.perf_counter()
-        lib2.set_links(ll)
-        tb = time.perf_counter()
-        lib2.step(args.steps)
-        tc = time.perf_counter()
-        lib2.get_particles(outp)
-        lib2.synchronize()
-        t1 = time.perf_counter()
-        el = t1 - t0
-        parts = {"set_particles_s": ta - t0, "set_links_s": tb - ta, "steps_s": tc - tb,
-                 "get_particles_s": t1 - tc}
-        if pg:
-            t = torch.tensor([el], device="cuda", dtype=torch.float64)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            el = float(t.item())
-        lib2.close()
-        h2d = sum(v.nbytes for v in pp.values()) + sum(v.nbytes for v in ll.values())
-        d2h = sum(v.nbytes for v in outp.values())
-        e2e = {"value": world * n * args.steps / el, "unit": "particle-steps/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "step": f"one C-ABI job from pinned host arrays: upload state (particles, links"
-                       f"{'; side history zero, not uploaded' if fresh else ', side history'}), "
-                       f"{args.steps} timesteps, download particles", "breakdown": parts}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            cpu = cpu_baseline(P, p, l, n)
-        except Exception as ex:  # reported, not fatal
-            cpu = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
-                   "sample": f"failed: {ex}"}
-
-    if pg:
-        pg.destroy_process_group()
-    if rank != 0:
-        return
-    line = {
-        "metric": "particle-steps/s (5.7M slab)" if args.workload == "slab" else "particle-steps/s (32k block)",
-        "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": (value / PUBLISHED_MIXED) if (prec == abi.PREC_MIXED and args.workload == "slab") else None,
-        "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
-        "config": {"workload": name, "particles": n, "links": L, "contact_pairs": pairs,
-                   "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (records + link ends > 126 MB)",
-                   "baseline_number": "RTX 5090 1.108e9 particle-steps/s, HiDEM/Docs/Performance.md:68"},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "rebuilds_in_timed_steps": int(st1["regen_count"] - st0["regen_count"]),
-        "clocks": clk,
-    }
-    print(json.dumps(line))
+    main_slab(args)
 
 
 if __name__ == "__main__":

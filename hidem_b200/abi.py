@@ -24,6 +24,8 @@ TYPE_FIXED = 0x40
 TYPE_FRONT = 0x80
 BATCH_GRAPHS = 1
 BATCH_PER_CONTEXT = 2
+CHECK_GRID_GROWTH = 1
+
 STEP_KERNEL_AUTO = 0
 STEP_KERNEL_ITEMS = 1
 STEP_KERNEL_THREAD = 2
@@ -82,7 +84,7 @@ class HidemStats(C.Structure):
                 ("max_links_per_particle", _i64), ("grid_dims", _i64 * 3), ("grid_min", _d * 3),
                 ("regen_count", _i64), ("last_regen_step", _i64), ("accumulated_dist", _d),
                 ("search_distance", _d), ("interact_distance", _d), ("broken_links", _i64),
-                ("kernel_launches", _i64)]
+                ("kernel_launches", _i64), ("grid_growth_events", _i64)]
 
     def as_dict(self) -> dict:
         out = {}
@@ -278,6 +280,7 @@ _PROTOS = [
     ("hidem_get_mesh_accel", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_void_p, _i64, C.POINTER(_i64)]),
     ("hidem_set_step_kernel", C.c_int, [C.c_void_p, _i32]),
+    ("hidem_set_checks", C.c_int, [C.c_void_p, _i32]),
     ("hidem_get_step_kernel", _i32, [C.c_void_p]),
     ("hidem_batch_create", C.c_int, [C.POINTER(C.c_void_p), _i32, _i32, C.POINTER(C.c_void_p)]),
     ("hidem_batch_destroy", None, [C.c_void_p]),

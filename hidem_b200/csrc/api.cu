@@ -63,6 +63,7 @@ struct hidem_ctx {
     int32_t *cellOf[2] = {nullptr, nullptr};
     int32_t *slotOf = nullptr;
     int32_t *perm = nullptr;
+    int32_t *bigCells = nullptr;  // crowded cells of a rebuild's sort (n / 32 + 2 entries, count last)
     void *force = nullptr;
 
     // grid
@@ -114,6 +115,8 @@ struct hidem_ctx {
 
     double accumulatedDist = 0;
     long long regenCount = 0, lastRegen = -1;
+    long long prevTotalCells = 0, gridGrowthEvents = 0;  // NeighbourGrid.cpp:89-92 warning
+    int32_t checks = 0;                                 // HIDEM_CHECK_* bits
     long long launches = 0;
     int smCount = 148;
 
@@ -323,8 +326,9 @@ hidem_status check_device_error(hidem_ctx *ctx) {
                            : flag == 2 ? "more than 65535 contacts for one particle"
                            : flag == 3 ? "more than 65535 link ends for one particle"
                            : flag == 4 ? "shared-memory staging copies did not complete in time"
+                           : flag == 5 ? "more than 4096 particles in one neighbour-grid cell"
                                        : "device check failed";
-        return fail(ctx, HIDEM_ERR_DEVICE, "device check %d: %s", flag, what);
+        return fail(ctx, flag == 5 ? HIDEM_ERR_CAPACITY : HIDEM_ERR_DEVICE, "device check %d: %s", flag, what);
     }
     return HIDEM_OK;
 }
@@ -398,8 +402,11 @@ hidem_status rebuild(hidem_ctx *ctx) {
     double b[6];
     CK(cudaMemcpyAsync(b, ctx->boundsOut, sizeof b, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (!(b[0] <= b[3] && b[1] <= b[4] && b[2] <= b[5]))
-        return fail(ctx, HIDEM_ERR_DEVICE, "non-finite particle coordinates");
+    // the bounds carry a NaN of any coordinate; an infinite one shows as an infinite bound
+    for (int k = 0; k < 6; ++k)
+        if (!std::isfinite(b[k]))
+            return fail(ctx, HIDEM_ERR_DEVICE, "non-finite particle coordinates (NaN or infinite %c)",
+                        "xyz"[k % 3]);
     if (ctx->frameOnce) {
         // the box spanning every rank's particles (hidem_regenerate_frame)
         const double *f = ctx->frame;
@@ -424,6 +431,17 @@ hidem_status rebuild(hidem_ctx *ctx) {
     g.total = (long long)g.X * g.Y * g.Z;
     if (g.total >= (1ll << 31))
         return fail(ctx, HIDEM_ERR_CAPACITY, "grid has %lld cells (limit 2^31)", g.total);
+    // NeighbourGrid::generateNeighbourGrid's explosion warning (NeighbourGrid.cpp:89-92): a
+    // grid more than 10x the last one's cells is counted; with HIDEM_CHECK_GRID_GROWTH the
+    // rebuild is refused instead
+    if (ctx->prevTotalCells != 0 && g.total / 10 > ctx->prevTotalCells) {
+        ctx->gridGrowthEvents += 1;
+        if (ctx->checks & HIDEM_CHECK_GRID_GROWTH)
+            return fail(ctx, HIDEM_ERR_DEVICE,
+                        "grid of %lld cells is more than 10x the last rebuild's %lld: did something explode?",
+                        g.total, ctx->prevTotalCells);
+    }
+    ctx->prevTotalCells = g.total;
     int k = 0;
     for (int zD = -1; zD < 2; ++zD)
         for (int yD = -1; yD < 2; ++yD)
@@ -447,7 +465,9 @@ hidem_status rebuild(hidem_ctx *ctx) {
     ctx->launches += launch_scan<int, int>(ctx->cellCount, g.total, 1, ctx->cellStart,
                                            ctx->scanSums32, nullptr, st);
     launch_scatter(ctx->cellOf[od], n, ctx->cellStart, ctx->cursor, ctx->perm, st);
-    launch_sort_cells(ctx->cellStart, ctx->cellCount, g.total, ctx->orig[od], ctx->perm, st);
+    ctx->launches += launch_sort_cells(ctx->cellStart, ctx->cellCount, g.total, ctx->orig[od], ctx->perm,
+                                       ctx->bigCells, ctx->bigCells + ctx->n / kSmallCell + 1,
+                                       ctx->errorFlag, 5, ctx->smCount, st);
     launch_permute<LP>(ctx->perm, n, recp<LP>(ctx, cur), recp<LP>(ctx, nxt), ctx->type[od],
                        ctx->type[nd], ctx->orig[od], ctx->orig[nd], ctx->cellOf[od],
                        ctx->cellOf[nd], ctx->slotOf, st);
@@ -1447,6 +1467,7 @@ void hidem_destroy(hidem_ctx *ctx) {
     }
     dfree(ctx->slotOf);
     dfree(ctx->perm);
+    dfree(ctx->bigCells);
     dfree(ctx->force);
     dfree(ctx->cellCount);
     dfree(ctx->cellStart);
@@ -1539,6 +1560,7 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     }
     TRY(dalloc(ctx, &ctx->slotOf, n));
     TRY(dalloc(ctx, &ctx->perm, n));
+    TRY(dalloc(ctx, &ctx->bigCells, n / kSmallCell + 2));
     TRY(dalloc_bytes(ctx, &ctx->force, 6 * lp * (size_t)n));
     TRY(dalloc(ctx, &ctx->counts, n));
     const long long nb32 = nblocks32(n);
@@ -1811,6 +1833,10 @@ hidem_status hidem_local_bounds(hidem_ctx *ctx, double lower[3], double upper[3]
     double b[6];
     CK(cudaMemcpyAsync(b, ctx->boundsOut, sizeof b, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 6; ++k)
+        if (!std::isfinite(b[k]))
+            return fail(ctx, HIDEM_ERR_DEVICE, "non-finite particle coordinates (NaN or infinite %c)",
+                        "xyz"[k % 3]);
     for (int k = 0; k < 3; ++k) {
         lower[k] = b[k];
         upper[k] = b[3 + k];
@@ -2121,6 +2147,13 @@ hidem_status hidem_get_break_events(hidem_ctx *ctx, int64_t *link_index, int64_t
     return HIDEM_OK;
 }
 
+hidem_status hidem_set_checks(hidem_ctx *ctx, int32_t flags) {
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (flags & ~HIDEM_CHECK_GRID_GROWTH) return fail(ctx, HIDEM_ERR_ARG, "unknown check flags 0x%x", flags);
+    ctx->checks = flags;
+    return HIDEM_OK;
+}
+
 hidem_status hidem_get_stats(hidem_ctx *ctx, hidem_stats *o) {
     if (!ctx || !o) return HIDEM_ERR_ARG;
     std::memset(o, 0, sizeof *o);
@@ -2142,6 +2175,7 @@ hidem_status hidem_get_stats(hidem_ctx *ctx, hidem_stats *o) {
     o->search_distance = ctx->searchDistance;
     o->interact_distance = ctx->interactDist;
     o->kernel_launches = ctx->launches;
+    o->grid_growth_events = ctx->gridGrowthEvents;
     if (ctx->haveLinks && ctx->L > 0) {
         unsigned long long total = 0;
         CK(cudaMemcpyAsync(&total, ctx->eventCount, sizeof total, cudaMemcpyDeviceToHost, ctx->stream));

@@ -51,6 +51,17 @@ __device__ __forceinline__ void set_error(int *flag, int code) {
 
 // ------------------------------------------------------------------ binning
 
+// min / max that keep a NaN: fmin / fmax drop NaN operands, so one particle with a NaN
+// coordinate would vanish from the bounds and then be binned from floor(NaN). With these
+// a NaN anywhere reaches the result and the host refuses the rebuild. Equal to fmin /
+// fmax for numbers.
+__device__ __forceinline__ double nan_min(double a, double b) {
+    return (a != a) ? a : ((b != b) ? b : fmin(a, b));
+}
+__device__ __forceinline__ double nan_max(double a, double b) {
+    return (a != a) ? a : ((b != b) ? b : fmax(a, b));
+}
+
 // Per-block min / max of the three coordinates over all particles
 // (ParticleData::getLimits, PLiB/ParticleData.h:47-59).
 template <class LP>
@@ -62,15 +73,15 @@ __global__ void k_bounds(const PRec<LP> *__restrict__ rec, int n, double *__rest
         double v[3] = {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            mn[k] = fmin(mn[k], v[k]);
-            mx[k] = fmax(mx[k], v[k]);
+            mn[k] = nan_min(mn[k], v[k]);
+            mx[k] = nan_max(mx[k], v[k]);
         }
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         for (int o = 16; o > 0; o >>= 1) {
-            mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
-            mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+            mn[k] = nan_min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = nan_max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
         }
     }
     __shared__ double sm[32][6];
@@ -87,8 +98,8 @@ __global__ void k_bounds(const PRec<LP> *__restrict__ rec, int n, double *__rest
         for (int k = 0; k < 3; ++k) {
             double a = sm[0][k], b = sm[0][3 + k];
             for (int j = 1; j < nw; ++j) {
-                a = fmin(a, sm[j][k]);
-                b = fmax(b, sm[j][3 + k]);
+                a = nan_min(a, sm[j][k]);
+                b = nan_max(b, sm[j][3 + k]);
             }
             partial[blockIdx.x * 6 + k] = a;
             partial[blockIdx.x * 6 + 3 + k] = b;
@@ -109,7 +120,7 @@ __global__ void k_bounds_final(const double *__restrict__ partial, int nb, doubl
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             const double u = partial[b * 6 + k];
-            v[k] = (k < 3) ? fmin(v[k], u) : fmax(v[k], u);
+            v[k] = (k < 3) ? nan_min(v[k], u) : nan_max(v[k], u);
         }
 #pragma unroll
     for (int k = 0; k < 6; ++k) red[k][t] = v[k];
@@ -118,7 +129,7 @@ __global__ void k_bounds_final(const double *__restrict__ partial, int nb, doubl
         if (t < w)
 #pragma unroll
             for (int k = 0; k < 6; ++k)
-                red[k][t] = (k < 3) ? fmin(red[k][t], red[k][t + w]) : fmax(red[k][t], red[k][t + w]);
+                red[k][t] = (k < 3) ? nan_min(red[k][t], red[k][t + w]) : nan_max(red[k][t], red[k][t + w]);
         __syncthreads();
     }
     if (t < 6) out[t] = red[t][0];
@@ -249,23 +260,84 @@ __global__ void k_scatter(const int *__restrict__ cellOf, int n, const int *__re
 }
 
 // Orders each cell's members by input index: the (colour, index) order of
-// NeighbourGrid::generateIterationList (NeighbourGrid.cpp:163-184).
+// NeighbourGrid::generateIterationList (NeighbourGrid.cpp:163-184). One thread per cell
+// sorts a cell of at most kSmallCell members by insertion (a lattice cell holds a few);
+// a larger cell goes to a list that k_sort_big_cells sorts with one CTA per cell, so that
+// no thread's work grows with the square of a crowded cell's population.
 __global__ void k_sort_cells(const int *__restrict__ cellStart, const int *__restrict__ cellCount,
-                             long long total, const int *__restrict__ origOld, int *__restrict__ perm) {
+                             long long total, const int *__restrict__ origOld, int *__restrict__ perm,
+                             int *__restrict__ bigList, int *__restrict__ bigCount) {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= total) return;
     int cnt = cellCount[c];
     if (cnt < 2) return;
+    if (cnt > kSmallCell) {
+        bigList[atomicAdd(bigCount, 1)] = (int)c;
+        return;
+    }
     int s = cellStart[c];
     for (int a = 1; a < cnt; ++a) {
         int v = perm[s + a];
-        int key = origOld[v];
+        int key = origOld ? origOld[v] : v;
         int b = a - 1;
-        while (b >= 0 && origOld[perm[s + b]] > key) {
+        while (b >= 0 && (origOld ? origOld[perm[s + b]] : perm[s + b]) > key) {
             perm[s + b + 1] = perm[s + b];
             --b;
         }
         perm[s + b + 1] = v;
+    }
+}
+
+// One CTA per listed cell (grid-stride over the list): the (key, member) pairs of the cell
+// in shared memory, a bitonic sort over the next power of two, the members written back in
+// key order. Keys are input indices (non-negative, distinct), so the order is the one the
+// insertion sort gives. A cell of more than kBigCellCap members is left unsorted and sets
+// `errorCode` in the error flag: the caller refuses the result.
+__global__ void __launch_bounds__(kBigCellThreads)
+    k_sort_big_cells(const int *__restrict__ cellStart, const int *__restrict__ cellCount,
+                     const int *__restrict__ origOld, int *__restrict__ perm,
+                     const int *__restrict__ bigList, const int *__restrict__ bigCount,
+                     int *errorFlag, int errorCode) {
+    __shared__ unsigned long long sk[kBigCellCap];
+    const int nbig = *bigCount;
+    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+        const int c = bigList[b];
+        const int cnt = cellCount[c];
+        const int s = cellStart[c];
+        if (cnt > kBigCellCap) {
+            if (threadIdx.x == 0) set_error(errorFlag, errorCode);
+            continue;
+        }
+        int m = kSmallCell;
+        while (m < cnt) m <<= 1;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            if (i < cnt) {
+                const int v = perm[s + i];
+                const unsigned key = (unsigned)(origOld ? origOld[v] : v);
+                sk[i] = ((unsigned long long)key << 32) | (unsigned)v;
+            } else {
+                sk[i] = ~0ull;
+            }
+        }
+        __syncthreads();
+        for (int k = 2; k <= m; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                    const int p = i ^ j;
+                    if (p > i) {
+                        const unsigned long long x = sk[i], y = sk[p];
+                        const bool up = (i & k) == 0;
+                        if (up ? (x > y) : (x < y)) {
+                            sk[i] = y;
+                            sk[p] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) perm[s + i] = (int)(unsigned)(sk[i] & 0xffffffffull);
+        __syncthreads();
     }
 }
 
@@ -340,8 +412,13 @@ __global__ void k_nbr_count(const PRec<LP> *__restrict__ rec, int n, const int *
                             int *errorFlag) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int c = 0;
+    // a failed check earlier in the rebuild (a particle outside the grid, a cell too crowded
+    // to sort) ends the rebuild at the next host check: skip the walk, whose cost grows with
+    // the square of a crowded cell's population
+    const bool failed = *reinterpret_cast<volatile int *>(errorFlag) != 0;
     if (i < n) {
-        c = walk_cells<LP, false>(rec, i, cellOf[i], g, cellStart, cellCount, interactDist, nullptr, 0);
+        if (!failed)
+            c = walk_cells<LP, false>(rec, i, cellOf[i], g, cellStart, cellCount, interactDist, nullptr, 0);
         if (c > 0xffff) {
             set_error(errorFlag, 2);
             c = 0xffff;
@@ -1340,9 +1417,15 @@ void launch_scatter(const int *cellOf, int n, const int *cellStart, int *cursor,
     k_scatter<<<nblk(n, 256), 256, 0, s>>>(cellOf, n, cellStart, cursor, perm);
 }
 
-void launch_sort_cells(const int *cellStart, const int *cellCount, long long total,
-                       const int *origOld, int *perm, cudaStream_t s) {
-    k_sort_cells<<<nblk(total, 256), 256, 0, s>>>(cellStart, cellCount, total, origOld, perm);
+int launch_sort_cells(const int *cellStart, const int *cellCount, long long total,
+                      const int *origOld, int *perm, int *bigList, int *bigCount, int *errorFlag,
+                      int errorCode, int smCount, cudaStream_t s) {
+    cudaMemsetAsync(bigCount, 0, sizeof(int), s);
+    k_sort_cells<<<nblk(total, 256), 256, 0, s>>>(cellStart, cellCount, total, origOld, perm,
+                                                  bigList, bigCount);
+    k_sort_big_cells<<<2 * smCount, kBigCellThreads, 0, s>>>(cellStart, cellCount, origOld, perm,
+                                                             bigList, bigCount, errorFlag, errorCode);
+    return 2;
 }
 
 template <class LP>

@@ -94,8 +94,16 @@ template <class TI, class TO>
 int launch_scan(const TI *in, long long n, TO scaleBy, TO *out, TO *sums, TO *total, cudaStream_t s);
 void launch_scatter(const int *cellOf, int n, const int *cellStart, int *cursor, int *perm,
                     cudaStream_t s);
-void launch_sort_cells(const int *cellStart, const int *cellCount, long long total,
-                       const int *origOld, int *perm, cudaStream_t s);
+// Members of a neighbour-grid cell of at most kSmallCell are sorted by one thread; larger
+// cells (listed in bigList, which holds n / kSmallCell + 1 entries) by one CTA each, up to
+// kBigCellCap members: a larger cell sets errorCode in errorFlag. origOld == nullptr sorts
+// by the member values themselves. Returns the number of kernel launches.
+constexpr int kSmallCell = 32;
+constexpr int kBigCellCap = 4096;
+constexpr int kBigCellThreads = 512;
+int launch_sort_cells(const int *cellStart, const int *cellCount, long long total,
+                      const int *origOld, int *perm, int *bigList, int *bigCount, int *errorFlag,
+                      int errorCode, int smCount, cudaStream_t s);
 template <class LP>
 void launch_permute(const int *perm, int n, const PRec<LP> *recOld, PRec<LP> *recNew,
                     const uint8_t *typeOld, uint8_t *typeNew, const int *origOld, int *origNew,

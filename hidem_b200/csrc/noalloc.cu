@@ -4,14 +4,13 @@
 // counters and cursors, the per-cell start offsets and the scan's block sums — lives in
 // one file-scope __device__ array of fixed size, so the call itself never allocates.
 //
-// Every GPU that loads this library holds that array (about 3.1 MB) until the process
+// Every GPU that loads this library holds that array (about 4.1 MB) until the process
 // exits. All calls on a device share it and it keeps the last call's contents, so the
 // entry point clears what must start at zero on every call, and calls that overlap on
 // the GPU (two streams, two host threads) race on it.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 #include <string>
 
 #include "kernels.h"
@@ -33,16 +32,24 @@ struct NoAllocScratch {
     int count[kNoAllocMaxCells];
     int cursor[kNoAllocMaxCells];
     int start[kNoAllocMaxCells];
+    int big[kNoAllocMaxCells];  // cells of more than 32 members, sorted one CTA each
     int sums[kNoAllocSums];
     int total[4];
+    int bigCount[4];
+    int status[4];              // status[0]: nonzero when a cell held too many members to sort
 };
 
 // The only storage the entry point uses besides the caller's buffers.
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// Device address of g_noalloc_scratch per device, looked up once with the device current.
-std::mutex g_noalloc_mutex;
-NoAllocScratch *g_noalloc_ptr[64] = {};
+// min / max that keep a NaN (fmin / fmax drop one), so that a single NaN coordinate reaches
+// the bounds and the call refuses the input; equal to fmin / fmax for numbers
+__device__ __forceinline__ double na_min(double a, double b) {
+    return (a != a) ? a : ((b != b) ? b : fmin(a, b));
+}
+__device__ __forceinline__ double na_max(double a, double b) {
+    return (a != a) ? a : ((b != b) ? b : fmax(a, b));
+}
 
 __global__ void k_na_bounds(const double *__restrict__ x, const double *__restrict__ y,
                             const double *__restrict__ z, int n, double *__restrict__ partial) {
@@ -51,14 +58,14 @@ __global__ void k_na_bounds(const double *__restrict__ x, const double *__restri
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double v[3] = {x[i], y[i], z[i]};
         for (int k = 0; k < 3; ++k) {
-            mn[k] = fmin(mn[k], v[k]);
-            mx[k] = fmax(mx[k], v[k]);
+            mn[k] = na_min(mn[k], v[k]);
+            mx[k] = na_max(mx[k], v[k]);
         }
     }
     for (int k = 0; k < 3; ++k) {
         for (int o = 16; o > 0; o >>= 1) {
-            mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
-            mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+            mn[k] = na_min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = na_max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
         }
     }
     __shared__ double sm[32][6];
@@ -73,8 +80,8 @@ __global__ void k_na_bounds(const double *__restrict__ x, const double *__restri
         for (int k = 0; k < 3; ++k) {
             double a = sm[0][k], b = sm[0][3 + k];
             for (int j = 1; j < (int)(blockDim.x >> 5); ++j) {
-                a = fmin(a, sm[j][k]);
-                b = fmax(b, sm[j][3 + k]);
+                a = na_min(a, sm[j][k]);
+                b = na_max(b, sm[j][3 + k]);
             }
             partial[blockIdx.x * 6 + k] = a;
             partial[blockIdx.x * 6 + 3 + k] = b;
@@ -88,7 +95,7 @@ __global__ void k_na_bounds_final(const double *__restrict__ partial, int nb, do
         double v = partial[k];
         for (int b = 1; b < nb; ++b) {
             double u = partial[b * 6 + k];
-            v = (k < 3) ? fmin(v, u) : fmax(v, u);
+            v = (k < 3) ? na_min(v, u) : na_max(v, u);
         }
         out[k] = v;
     }
@@ -118,26 +125,6 @@ __global__ void k_na_scatter(const int *__restrict__ cellOf, int n, const int *_
     order[start[c] + atomicAdd(cursor + c, 1)] = i;
 }
 
-// inside each cell, ascending input index: the order of
-// NeighbourGrid::generateIterationList (PLiB/NeighbourGrid.cpp:163-184)
-__global__ void k_na_sort(const int *__restrict__ start, const int *__restrict__ count,
-                          long long total, int *__restrict__ order) {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= total) return;
-    const int cnt = count[c];
-    if (cnt < 2) return;
-    const int s = start[c];
-    for (int a = 1; a < cnt; ++a) {
-        const int v = order[s + a];
-        int b = a - 1;
-        while (b >= 0 && order[s + b] > v) {
-            order[s + b + 1] = order[s + b];
-            --b;
-        }
-        order[s + b + 1] = v;
-    }
-}
-
 hidem_status na_fail(hidem_status s, const std::string &msg) {
     hidem::g_nocontext_error = msg;
     return s;
@@ -161,21 +148,22 @@ extern "C" hidem_status hidem_bin_cells_noalloc(const double *x, const double *y
     if (e != cudaSuccess || dev < 0 || dev >= 64)
         return na_fail(HIDEM_ERR_CUDA, std::string("hidem_bin_cells_noalloc: no current device: ") +
                                            cudaGetErrorString(e));
+    // The array's name is a host-side stand-in in this code; its device address comes from
+    // the runtime with the device current. It is looked up on every call (it allocates
+    // nothing), so that it is valid again after the caller resets the device.
     NoAllocScratch *S = nullptr;
     {
-        // first call on this device: resolve the device address of the scratch array
-        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev]) {
-            void *p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess || !p)
-                return na_fail(HIDEM_ERR_CUDA, std::string("hidem_bin_cells_noalloc: "
-                                                           "cudaGetSymbolAddress failed: ") +
-                                                   cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = static_cast<NoAllocScratch *>(p);
-        }
-        S = g_noalloc_ptr[dev];
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return na_fail(HIDEM_ERR_CUDA, std::string("hidem_bin_cells_noalloc: "
+                                                       "cudaGetSymbolAddress failed: ") +
+                                               cudaGetErrorString(e));
+        S = static_cast<NoAllocScratch *>(p);
     }
+    int smCount = 148;
+    if (cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || smCount < 1)
+        smCount = 148;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int ni = (int)n;
 
@@ -188,8 +176,10 @@ extern "C" hidem_status hidem_bin_cells_noalloc(const double *x, const double *y
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess)
         return na_fail(HIDEM_ERR_CUDA, std::string("hidem_bin_cells_noalloc: ") + cudaGetErrorString(e));
-    if (!(b[0] <= b[3] && b[1] <= b[4] && b[2] <= b[5]))
-        return na_fail(HIDEM_ERR_ARG, "hidem_bin_cells_noalloc: non-finite coordinates");
+    // the bounds carry a NaN of any coordinate; an infinite one shows as an infinite bound
+    for (int k = 0; k < 6; ++k)
+        if (!std::isfinite(b[k]))
+            return na_fail(HIDEM_ERR_ARG, "hidem_bin_cells_noalloc: non-finite coordinates (NaN or infinite)");
 
     // 2. grid dims (NeighbourGrid::getGridSize, PLiB/NeighbourGrid.cpp:40-46)
     const double ex = std::floor((b[3] - b[0]) / cell_size);
@@ -216,6 +206,7 @@ extern "C" hidem_status hidem_bin_cells_noalloc(const double *x, const double *y
     // 3. counters start at zero on every call: the array keeps the previous call's values
     e = cudaMemsetAsync(S->count, 0, sizeof(int) * (size_t)total, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(S->cursor, 0, sizeof(int) * (size_t)total, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->status, 0, sizeof S->status, st);
     if (e != cudaSuccess)
         return na_fail(HIDEM_ERR_CUDA, std::string("hidem_bin_cells_noalloc: ") + cudaGetErrorString(e));
 
@@ -224,9 +215,18 @@ extern "C" hidem_status hidem_bin_cells_noalloc(const double *x, const double *y
                                                  total, cell_of, S->count);
     hidem::launch_scan<int, int>(S->count, total, 1, S->start, S->sums, S->total, st);
     k_na_scatter<<<(ni + 255) / 256, 256, 0, st>>>(cell_of, ni, S->start, S->cursor, order);
-    k_na_sort<<<(int)((total + 255) / 256), 256, 0, st>>>(S->start, S->count, total, order);
+    // inside each cell ascending input index, the order of NeighbourGrid::generateIterationList
+    // (PLiB/NeighbourGrid.cpp:163-184); cells of more than 4096 members are refused
+    hidem::launch_sort_cells(S->start, S->count, total, nullptr, order, S->big, S->bigCount, S->status,
+                             1, smCount, st);
     e = cudaGetLastError();
+    int status = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, S->status, sizeof status, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess)
         return na_fail(HIDEM_ERR_CUDA, std::string("hidem_bin_cells_noalloc: ") + cudaGetErrorString(e));
+    if (status != 0)
+        return na_fail(HIDEM_ERR_CAPACITY, "hidem_bin_cells_noalloc: a cell holds more than 4096 "
+                                           "particles; use a smaller cell_size");
     return HIDEM_OK;
 }

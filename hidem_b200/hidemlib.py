@@ -221,6 +221,11 @@ class HiDEMLib:
         """abi.STEP_KERNEL_* (AUTO: timed on the first fused steps)."""
         self._check(self._lib.hidem_set_step_kernel(self._ctx, int(kernel)))
 
+    def set_checks(self, flags: int) -> None:
+        """abi.CHECK_* bits (hidem_set_checks): CHECK_GRID_GROWTH refuses a rebuild whose
+        grid has more than 10x the previous one's cells."""
+        self._check(self._lib.hidem_set_checks(self._ctx, int(flags)))
+
     def step_kernel(self) -> int:
         return int(self._lib.hidem_get_step_kernel(self._ctx))
 

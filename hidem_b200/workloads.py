@@ -1,9 +1,10 @@
 """Synthetic workloads: FCC ice blocks and slabs with distance-rule links.
 
-The reference's MeshBlock benchmark reads HDF5 point files (HiDEM/Benchmark/*/particles.h5)
-that cannot be read here, so seeded FCC lattices with the same density, particle size
-and link rule stand in for them. Generation runs in the library's host code
-(``hidem_lattice_fcc``, ``hidem_links_by_distance``).
+Seeded FCC lattices with the density, particle size and link rule of the reference's
+MeshBlock benchmark inputs stand in for its HDF5 point files in the named configurations.
+Generation runs in the library's host code (``hidem_lattice_fcc``,
+``hidem_links_by_distance``); ``inputs_np`` restates it in numpy for processes that must not
+load the library.
 
 Parameter mapping of the named configurations (the reference keys they set):
   d = 1 m, a = sqrt(2) d            lattice.particleRadius = 0.5, fccSpacing = sqrt(2)
@@ -64,8 +65,9 @@ def distance_links(p: dict, precision: int, scale: float = 1.01, lean: bool = Fa
     return links
 
 
-def block_params(precision: int, **over) -> abi.HidemParams:
-    """Material and contact parameters of the ice-block configurations."""
+def block_overrides(precision: int, **over) -> dict:
+    """Material and contact parameters of the ice-block configurations, as overrides of
+    the MeshBlock defaults."""
     dt = 1e-4
     mass = 910.0 * 1.0 ** 3
     base = dict(dt=dt, scale=1.0, E=1e9, rhoIce=910.0, g=9.81, maxLoad=5e-4, bendBreak=0.01,
@@ -73,7 +75,19 @@ def block_params(precision: int, **over) -> abi.HidemParams:
                 damping=1e-3 * mass / dt, dampingRotation=1e-3 * mass / dt,
                 searchDistanceScale=1.2, maxRadius=0.5, waterLevel=-1.0e3, precision=precision)
     base.update(over)
-    return abi.default_params(**base)
+    return base
+
+
+def block_params(precision: int, **over) -> abi.HidemParams:
+    """Material and contact parameters of the ice-block configurations."""
+    return abi.default_params(**block_overrides(precision, **over))
+
+
+def slab_params_overrides(precision: int, water_level: float, zmin: float, **over) -> dict:
+    """The calving slab's parameters: the block's, on a flat bed half a diameter below the
+    lowest centres (bed friction 0.3), water line, front pressure."""
+    return block_overrides(precision, waterLevel=water_level, useBed=1, bedHeight=zmin + 0.5,
+                           bedFriction=0.3, useFrontPressure=1, **over)
 
 
 def ice_block(cells=(20, 20, 20), precision: int = abi.PREC_MIXED, seed: int = 1,
@@ -148,8 +162,7 @@ def calving_slab(size=(400.0, 100.0, 100.0), precision: int = abi.PREC_MIXED, se
     if k:
         links["state"][rng.choice(L, size=k, replace=False)] = 0
     zmin = float(p["zCord"].min())
-    params = block_params(precision, waterLevel=water_level, useBed=1, bedHeight=zmin + 0.5,
-                          bedFriction=0.3, useFrontPressure=1, **param_over)
+    params = abi.default_params(**slab_params_overrides(precision, water_level, zmin, **param_over))
     return params, p, links
 
 

@@ -120,6 +120,8 @@ typedef struct hidem_stats {
     double search_distance, interact_distance;
     int64_t broken_links;      /* links with state == 0 */
     int64_t kernel_launches;   /* kernels launched by this context so far */
+    int64_t grid_growth_events; /* rebuilds whose grid had more than 10x the previous one's
+                                   cells (NeighbourGrid.cpp:89-92 prints a warning there) */
 } hidem_stats;
 
 /* ---- defaults -------------------------------------------------------- */
@@ -263,6 +265,17 @@ typedef struct hidem_functor_params {
 } hidem_functor_params;
 hidem_status hidem_set_functor_params(hidem_ctx *ctx, const hidem_functor_params *f);
 hidem_status hidem_get_functor_params(hidem_ctx *ctx, hidem_functor_params *out);
+/* Run-time checks beyond the reference's behaviour. The reference prints "grid 10x larger
+ * than old, did something explode?" when a rebuild's grid has more than ten times the
+ * cells of the previous one and carries on (PLiB/NeighbourGrid.cpp:89-92); the library
+ * counts such rebuilds in hidem_stats.grid_growth_events, and with HIDEM_CHECK_GRID_GROWTH
+ * set the rebuild fails with HIDEM_ERR_DEVICE instead. Always on, whatever the flags:
+ * non-finite coordinates (NaN or infinite) fail a rebuild with HIDEM_ERR_DEVICE; a
+ * neighbour-grid cell of more than 4096 particles fails it with HIDEM_ERR_CAPACITY; a link
+ * end that names no particle fails hidem_set_links with HIDEM_ERR_NOT_FOUND
+ * (LinkData::makeLocalPartEnds, PLiB/LinkData.h:102-108, exits there). */
+#define HIDEM_CHECK_GRID_GROWTH 1
+hidem_status hidem_set_checks(hidem_ctx *ctx, int32_t flags);
 /* Blocks until the context's stream is idle; reports device-side check failures. */
 hidem_status hidem_synchronize(hidem_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work
@@ -530,13 +543,15 @@ hidem_status hidem_surrogate_gradients(hidem_surrogate *s, const float *inputs, 
  * cell colour ix + iy*X + iz*X*Y of each particle (cell_of), and `order` = particle
  * indices sorted by (cell, index). x, y, z, cell_of, order are caller-owned device
  * arrays of n elements; dims and mins are host arrays; work is queued on `stream`
- * (a cudaStream_t, 0 for the default stream) and the call returns after the bounds
- * are known on the host. Scratch is one fixed device array in the library (about
- * 3.1 MB, held on every GPU that loads the library until exit), so grids of more than
- * HIDEM_NOALLOC_MAX_CELLS cells are refused with HIDEM_ERR_CAPACITY. The first call on
- * a device looks up that array's device address (cudaGetSymbolAddress) and should come
- * before any stream capture. All calls share the array: calls that overlap on the GPU
- * race. On failure the text is in hidem_create_error(). */
+ * (a cudaStream_t, 0 for the default stream). The call waits on `stream` twice: for the
+ * bounds, which size the grid, and at the end for the status of the per-cell sort, so it
+ * returns with cell_of and order complete. Scratch is one fixed device array in the
+ * library (about 4.1 MB, held on every GPU that loads the library until exit), so grids
+ * of more than HIDEM_NOALLOC_MAX_CELLS cells, and cells of more than 4096 particles,
+ * are refused with HIDEM_ERR_CAPACITY. Every call looks up that array's device address
+ * (cudaGetSymbolAddress) with the caller's device current. A NaN or infinite coordinate
+ * is refused with HIDEM_ERR_ARG. All calls share the array: calls that overlap on the
+ * GPU race. On failure the text is in hidem_create_error(). */
 #define HIDEM_NOALLOC_MAX_CELLS 262144
 hidem_status hidem_bin_cells_noalloc(const double *x, const double *y, const double *z,
                                      int64_t n, double cell_size, int32_t *cell_of,

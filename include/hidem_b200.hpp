@@ -131,6 +131,7 @@ public:
     }
     // step kernel (HIDEM_STEP_KERNEL_*; AUTO times the candidates on the first steps)
     void setStepKernel(int32_t kernel) { check(hidem_set_step_kernel(ctx_, kernel)); }
+    void setChecks(int32_t flags) { check(hidem_set_checks(ctx_, flags)); }
     int32_t stepKernel() { return hidem_get_step_kernel(ctx_); }
 
 private:

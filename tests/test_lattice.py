@@ -56,3 +56,39 @@ def test_link_set_matches_reference_link_generator(precision):
     our_set = {(int(a), int(b)): float(x) for a, b, x in
                zip(ours["globalKeyEndA"], ours["globalKeyEndB"], ours["initialLen"])}
     assert our_set == ref_set
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_MIXED, abi.PREC_FP64])
+@pytest.mark.parametrize("jitter", [0.0, 0.01])
+def test_numpy_inputs_equal_the_library_generators(precision, jitter):
+    """hidem_b200.inputs_np (the reference arm's inputs, built without the library) gives the
+    library generators' arrays and parameters bit for bit."""
+    from hidem_b200 import inputs_np
+    P, p, l = workloads.calving_slab(size=(30.0, 12.0, 9.0), precision=precision, jitter=jitter, seed=3)
+    Q, q, m = inputs_np.calving_slab(size=(30.0, 12.0, 9.0), precision=precision, jitter=jitter, seed=3)
+    for k in p:
+        assert np.array_equal(p[k], q[k]), k
+    for k in l:
+        assert np.array_equal(l[k], m[k]), k
+    assert bytes(P) == bytes(Q)
+    assert bytes(inputs_np.default_params()) == bytes(abi.default_params())
+
+
+def test_reference_arm_maps_no_library_code(tmp_path):
+    """bench.py --impl reference runs the reference's CPU path on inputs it builds in numpy:
+    its process never maps libhidem_b200.so."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--slab', '20,9,9', "
+            "'--steps', '2', '--warmup', '1']; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('MAPPED' if 'libhidem_b200.so' in maps else 'CLEAN'); "
+            "print('REF' if 'libhidem_ref_fast' in maps else 'NOREF')")
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    out = r.stdout.strip().splitlines()
+    if "unavailable" in out[0]:
+        pytest.skip("oracle/_ref not built")
+    assert out[-2] == "CLEAN" and out[-1] == "REF"

@@ -89,3 +89,43 @@ def test_noalloc_refuses_grids_beyond_the_fixed_scratch(gpu):
                                      out.data_ptr(), out.data_ptr(), dims, mins, 0)
     assert st == 4  # HIDEM_ERR_CAPACITY: 101^3 cells > HIDEM_NOALLOC_MAX_CELLS
     assert b"HIDEM_NOALLOC_MAX_CELLS" in lib.hidem_create_error()
+
+
+def _device_xyz(p):
+    import torch
+    dev = torch.device("cuda", 0)
+    return [torch.from_numpy(np.ascontiguousarray(p[k])).to(dev) for k in ("xCord", "yCord", "zCord")]
+
+
+def _call(xyz, h):
+    import torch
+    lib = abi.load()
+    n = xyz[0].numel()
+    cell_of = torch.full((n,), -1, dtype=torch.int32, device=xyz[0].device)
+    order = torch.full((n,), -1, dtype=torch.int32, device=xyz[0].device)
+    dims = (C.c_int64 * 3)()
+    mins = (C.c_double * 3)()
+    st = lib.hidem_bin_cells_noalloc(xyz[0].data_ptr(), xyz[1].data_ptr(), xyz[2].data_ptr(), n, h,
+                                     cell_of.data_ptr(), order.data_ptr(), dims, mins, 0)
+    return st, lib.hidem_create_error(), cell_of.cpu().numpy(), order.cpu().numpy()
+
+
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_noalloc_refuses_non_finite_coordinates(gpu, bad):
+    """One NaN (or infinite) coordinate written into the host input before upload."""
+    p = cloud(3000, 5)
+    p["yCord"][1234] = bad
+    st, msg, _, _ = _call(_device_xyz(p), 1.2)
+    assert st == abi.HIDEM_ERR_ARG and b"non-finite" in msg
+
+
+def test_noalloc_orders_a_crowded_cell_and_refuses_an_overcrowded_one(gpu):
+    """A cell_size that puts the whole cloud into one cell: up to 4096 members the order is
+    still ascending input index; beyond, the call is refused instead of sorting for long."""
+    p = cloud(4000, 6)
+    st, msg, cell_of, order = _call(_device_xyz(p), 100.0)
+    assert st == abi.HIDEM_OK, msg
+    assert np.all(cell_of == 0) and np.array_equal(order, np.arange(4000, dtype=np.int32))
+    p = cloud(4097, 6)
+    st, msg, _, _ = _call(_device_xyz(p), 100.0)
+    assert st == abi.HIDEM_ERR_CAPACITY and b"4096" in msg
