@@ -54,8 +54,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle", "topo", "mesh", "ranks"],
-                    default="slab")
+    ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle", "topo", "mesh", "ranks",
+                                           "meshblock"], default="slab")
+    ap.add_argument("--config", default=None,
+                    help="meshblock: the reference's run config (default data/meshblock_5700k/config_mesh_5700k.toml)")
+    ap.add_argument("--particle-file", default=None,
+                    help="meshblock: the File lattice's HDF5 points (default: particles.h5 beside the config)")
+    ap.add_argument("--meshblock-start", type=int, default=25000,
+                    help="meshblock: untimed steps before the timed ones (the published run times 25000-30000)")
     ap.add_argument("--ranks", type=int, default=2,
                     help="ranks: slab ranks held as contexts of this process (one GPU)")
     ap.add_argument("--topo", default="1200,200,150",
@@ -290,6 +296,19 @@ def run_reference(args):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def run_reference_meshblock(args):
+    """--impl reference --workload meshblock: the reference's CPU path on its own benchmark
+    input, timed steps from the initial state (its per-step cost does not depend on the step
+    reached; the GPU arm's state at step 25,000 cannot be handed to this process without
+    this library). The input is read by the C restatement's harness-free numpy path."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    print(json.dumps({"impl": "reference", "unavailable":
+                      "the meshblock line carries the reference CPU path on the same state in cpu_baseline; "
+                      "reading its HDF5 input needs this library's reader"}))
 
 
 def run_reference_ensemble(args):
@@ -1062,7 +1081,7 @@ def main_slab(args):
     print(json.dumps(line))
 
 
-def e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n):
+def e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n, start_step: int = 0):
     """The same K steps through the C ABI from pinned host buffers: upload of the particle
     and link state, K steps, download of the particle state; wall time, devices synchronised
     on both sides."""
@@ -1094,6 +1113,8 @@ def e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n):
         keep.append(t)
     lib2 = HiDEMLib(P, device=local)
     lib2.set_step_kernel(step_kernel)
+    if start_step:
+        lib2.set_timestep(start_step)
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
@@ -1142,14 +1163,121 @@ def settle_summary(args) -> dict:
             "warm_steps_mean": float(np.mean(d["warm_steps"])),
             "prediction_rel_error_mean": float(np.mean(d["prediction_rel_error"])),
             "settled_error_over_d_max": float(np.max(d["settled_error_over_d"])),
-            "converged": {"cold": int(np.sum(d["cold_converged"])), "warm": int(np.sum(d["warm_converged"]))},
+            "all_converged": {"cold": bool(d["cold_converged"]), "warm": bool(d["warm_converged"])},
             "tongues": {"size_m": list(size), "train": args.train_tongues, "held_out": args.test_tongues,
                         "particles_per_tongue": d["particles_per_tongue"]},
             "seconds": time.perf_counter() - t0}
 
 
+def meshblock_paths(args):
+    cfg = Path(args.config) if args.config else ROOT / "data" / "meshblock_5700k" / "config_mesh_5700k.toml"
+    pf = Path(args.particle_file) if args.particle_file else cfg.parent / "particles.h5"
+    if not cfg.exists() or not pf.exists():
+        raise SystemExit(f"meshblock: {cfg} / {pf} not found: copy HiDEM/Benchmark/5700k/"
+                         f"{{config_mesh_5700k.toml,particles.h5}} of the reference there, or pass "
+                         f"--config / --particle-file")
+    return cfg, pf
+
+
+def main_meshblock(args):
+    """The reference's own benchmark run (HiDEM/Benchmark/5700k: MeshBlock sample, File
+    lattice of 5,723,826 particles, config_mesh_5700k.toml): the run advances untimed to
+    --meshblock-start (the reference's published time covers steps 25,000-30,000, with link
+    breaking active from t = breakTime), then K timesteps are timed. vs_baseline divides by
+    the published RTX 5090 figure of that run (HiDEM/Docs/Performance.md:68)."""
+    import torch
+    from hidem_b200 import abi, workloads
+    from hidem_b200.hidemlib import HiDEMLib
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    cfg, pf = meshblock_paths(args)
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    t0 = time.perf_counter()
+    P, p, l, info = workloads.meshblock(str(cfg), str(pf), prec)
+    gen_s = time.perf_counter() - t0
+    n, L = p["xCord"].shape[0], l["state"].shape[0]
+    clocks = ClockSampler(local)
+    lib = HiDEMLib(P, device=local)
+    lib.set_step_kernel(KERNELS[args.kernel])
+    lib.set_particles(p)
+    lib.set_links(l)
+    stream = torch.cuda.ExternalStream(lib.stream_handle)
+    start = max(args.meshblock_start, args.warmup, 15 if args.kernel == "auto" else 0)
+    t0 = time.perf_counter()
+    lib.step(start)
+    lib.synchronize()
+    adv_s = time.perf_counter() - t0
+    # the state where the timed region starts, for the legs that start there (untimed)
+    sp, sl = lib.get_particles(), lib.get_links()
+    clocks.start()
+    ms, kern_ms, launches, st0, st1 = timed_steps(lib, stream, args.steps)
+    clk = clocks.stop()
+    step_kernel = lib.step_kernel()
+    state_p = lib.get_particles()
+    state_l = lib.get_links()
+    lib.close()
+    value = n * args.steps / (ms / 1e3)
+    pairs = st1["num_neighbour_pairs"]
+    roofline = roofline_of(n, L, pairs, prec, kern_ms, args.precision, step_kernel)
+    roofline["traffic"] = None  # the committed DRAM figures are of the synthetic slab
+
+    e2e = None
+    if not args.no_e2e:
+        # the job from host arrays: the state at the timed region's start uploaded (particles,
+        # links with their CT history), K steps, the particle state downloaded
+        e2e = e2e_job(args, P, sp, sl, prec, step_kernel, local, None, 1, n, start_step=start)
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import oracle
+            if not oracle.reference_available(prec, fast=True):
+                raise RuntimeError("oracle/_ref not built")
+            sess = oracle.RefSession(P, sp, sl, fast=True, start_step=start)
+            sess.advance(1)
+            k = 5
+            secs = sess.advance(k)
+            cpu = {"value": n * k / secs, "unit": "particle-steps/s", "cores": sess.threads(),
+                   "kind": "reference", "cpu": cpu_model(), "host_threads": os.cpu_count(),
+                   "sample": f"{k} timesteps from step {start + 1} of the same run (the GPU's state at "
+                             f"step {start} handed over) after 1 warm-up step, reference CPU path built with "
+                             f"-O3 -ffast-math -march=x86-64-v3 -fopenmp"}
+            sess.close()
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
+                   "sample": f"failed: {ex}"}
+    broken = int((state_l["state"] == 0).sum())
+    line = {
+        "metric": "particle-steps/s (MeshBlock 5700k benchmark run)", "value": value,
+        "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": start,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / PUBLISHED_MIXED if prec == abi.PREC_MIXED else None,
+        "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64",
+        "data": "the reference's own benchmark input (HiDEM/Benchmark/5700k/particles.h5, config_mesh_5700k.toml)",
+        "config": {"workload": f"MeshBlock File lattice {pf.parent.name}: steps {start}-{start + args.steps}",
+                   "particles": n, "links": L, "precision": args.precision, "parallelism": "replicas x1",
+                   "l2": "inputs larger than L2 (records + link ends > 126 MB)"},
+        "baseline_number": "RTX 5090 25.83 s for steps 25000-30000 = 1.108e9 particle-steps/s, HiDEM/Docs/Performance.md:68",
+        "contact_pairs": pairs, "broken_links_at_end": broken,
+        "rebuilds_in_timed_steps": int(st1["regen_count"] - st0["regen_count"]),
+        "rebuilds_total": int(st1["regen_count"]),
+        "setup_s": {"read_and_links": gen_s, "advance_to_start": adv_s},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.workload == "meshblock":
+        if args.impl == "reference":
+            run_reference_meshblock(args)
+        else:
+            main_meshblock(args)
+        return
     if args.workload == "ranks":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable":

@@ -315,6 +315,9 @@ _PROTOS = [
                                     _i32, C.POINTER(HidemParticleSoA)]),
     ("hidem_links_by_distance", C.c_int, [C.POINTER(HidemParticleSoA), _i64, _i32, _d,
                                           C.POINTER(HidemLinkSoA), _i64, C.POINTER(_i64)]),
+    ("hidem_read_particle_file", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                                           C.c_char_p, _i32, C.POINTER(HidemParticleSoA), _i64,
+                                           C.POINTER(_i64)]),
 ]
 
 EXPORTED = [name for name, _, _ in _PROTOS]

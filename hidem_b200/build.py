@@ -21,7 +21,7 @@ LIB = PKG / "libhidem_b200.so"
 OBJ = PKG / "_build"
 
 CU_SOURCES = ["kernels.cu", "api.cu", "noalloc.cu", "surrogate.cu", "mesh.cu"]
-CPP_SOURCES = ["lattice.cpp", "config.cpp", "h5lite.cpp", "checkpoint.cpp"]
+CPP_SOURCES = ["lattice.cpp", "config.cpp", "h5lite.cpp", "checkpoint.cpp", "particle_file.cpp"]
 HEADERS = ["internal.h", "kernels.h", "physics.cuh", "h5lite.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -73,7 +73,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *objs, "-Xcompiler", "-fopenmp",
-          f"-ccbin={gxx}"])
+          f"-ccbin={gxx}", "-lz"])
     os.replace(tmp, LIB)
     if verbose:
         print(f"built {LIB}")

@@ -1,10 +1,14 @@
-// Minimal HDF5 writer / reader for the checkpoint layout (written from the public HDF5
-// file-format specification): superblock version 2, version-2 object headers, groups with
-// compact link storage (Link Info + Group Info + Link messages), 1-D contiguous datasets,
-// version-3 attribute messages, little-endian integer and IEEE float types, Jenkins
-// lookup3 checksums. The reader accepts files with that structure; it reports anything
-// else (older superblocks, dense link storage, chunked or filtered datasets) as
-// unsupported rather than guessing.
+// Minimal HDF5 writer / reader for the checkpoint layout and the reference's input files
+// (written from the public HDF5 file-format specification).
+// Writer: superblock version 2, version-2 object headers, groups with compact link storage
+// (Link Info + Group Info + Link messages), 1-D contiguous datasets, version-3 attribute
+// messages, little-endian integer and IEEE float types, Jenkins lookup3 checksums.
+// Reader: that layout, and what libhdf5 writes by default — superblock version 0 / 1,
+// version-1 object headers with continuation blocks, symbol-table groups (version-1 group
+// B-tree, symbol nodes, local heap), contiguous, compact and chunked datasets (version-1
+// chunk B-tree) with the deflate (zlib) and shuffle filters, attribute messages 1-3.
+// Anything else (dense link storage, version-4 layouts, other filters, big-endian or
+// compound types, shared messages) is reported as unsupported rather than guessed.
 #pragma once
 #include <cstdint>
 #include <cstdio>
@@ -25,13 +29,27 @@ struct Attr {
     std::vector<uint8_t> data;   // little-endian element bytes
 };
 
+struct Filter {
+    uint16_t id = 0;              // 1 deflate, 2 shuffle
+    bool optional = false;
+    std::vector<uint32_t> values; // client data (deflate level; shuffle element size)
+};
+
 struct Dataset {
     std::string name;
     Type type = Type::F64;
     uint64_t count = 0;
     const void *data = nullptr;  // writer: element bytes (count * type_size)
-    uint64_t fileOffset = 0;     // reader: where the elements are
+    uint64_t fileOffset = 0;     // reader: where the elements are (contiguous storage)
     std::vector<Attr> attrs;
+    // reader: storage of the dataset
+    int layout = 1;                          // 0 compact, 1 contiguous, 2 chunked
+    std::vector<uint64_t> dims;              // dataspace extent, row-major
+    uint64_t storedBytes = ~0ull;            // contiguous: bytes stored
+    std::vector<uint8_t> compact;            // compact: the element bytes
+    std::vector<uint64_t> chunk;             // chunked: chunk extent per dimension
+    uint64_t chunkIndex = ~0ull;             // chunked: version-1 B-tree of the chunks
+    std::vector<Filter> filters;             // chunked: the filter pipeline in order
 };
 
 struct Group {

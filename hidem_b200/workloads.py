@@ -65,6 +65,52 @@ def distance_links(p: dict, precision: int, scale: float = 1.01, lean: bool = Fa
     return links
 
 
+def read_particle_file(path: str, precision: int, names=(None, None, None, None)) -> dict:
+    """The reference's File lattice (hidem_read_particle_file; FileParticleGenerator,
+    PLiB/Generators/FileParticleGenerator.h:23-105): particles from an HDF5 point file."""
+    lib = abi.load()
+    enc = [n.encode() if n else None for n in names]
+    cnt = C.c_int64()
+    st = lib.hidem_read_particle_file(str(path).encode(), *enc, precision, None, 0, C.byref(cnt))
+    if st != abi.HIDEM_OK:
+        raise abi.HidemError(st, lib.hidem_create_error().decode())
+    n = cnt.value
+    p = abi.empty_particles(n, precision)
+    soa = abi.particle_soa(p, precision, n)
+    st = lib.hidem_read_particle_file(str(path).encode(), *enc, precision, C.byref(soa), n, C.byref(cnt))
+    if st != abi.HIDEM_OK:
+        raise abi.HidemError(st, lib.hidem_create_error().decode())
+    return p
+
+
+def meshblock(config_path: str, particle_file: str | None = None, precision: int | None = None):
+    """The reference's MeshBlock benchmark input (HiDEM/Benchmark/<size>/config_mesh_<size>.toml
+    with its particles.h5, the run every published number is quoted on): run parameters from
+    the TOML file (the library's front-end), particles from the File lattice, links by the
+    distance rule with lattice.linkGenScale (LinkGenerator, PLiB/Generators/LinkGenerator.h:
+    60-110; every particle is of ice type 0, linkWith [0], probability 1). `particle_file`
+    overrides lattice.path (which the reference resolves against its working directory).
+    Returns (params, particles, links, run info)."""
+    import tomllib
+    from pathlib import Path
+    from .config import params_from_toml
+    over = [] if precision is None else [f"--general.precision={'mixed' if precision == abi.PREC_MIXED else 'fp64'}"]
+    P, time_steps = params_from_toml(str(config_path), over)
+    prec = int(P.precision)
+    cfg = tomllib.loads(Path(config_path).read_text())
+    lat = cfg.get("lattice", {})
+    if lat.get("type") != "File":
+        raise ValueError(f"{config_path}: lattice.type is {lat.get('type')!r}, not 'File'")
+    path = particle_file or lat["path"]
+    names = (lat.get("xCords"), lat.get("yCords"), lat.get("zCords"), lat.get("radius"))
+    p = read_particle_file(path, prec, names)
+    links = distance_links(p, prec, float(lat["linkGenScale"]))
+    info = {"time_steps": time_steps, "linkGenScale": float(lat["linkGenScale"]),
+            "statIntervals": cfg.get("output", {}).get("statIntervals"),
+            "particle_file": str(path)}
+    return P, p, links, info
+
+
 def block_overrides(precision: int, **over) -> dict:
     """Material and contact parameters of the ice-block configurations, as overrides of
     the MeshBlock defaults."""

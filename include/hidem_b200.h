@@ -150,7 +150,7 @@ hidem_status hidem_create(const hidem_params *params, int device, hidem_ctx **ou
 void hidem_destroy(hidem_ctx *ctx);
 const char *hidem_last_error(const hidem_ctx *ctx);
 /* Per-thread text of the last failure of a call that has no context
- * (hidem_create, hidem_params_from_toml, hidem_bin_cells_noalloc). */
+ * (hidem_create, hidem_params_from_toml, hidem_read_particle_file, hidem_bin_cells_noalloc). */
 const char *hidem_create_error(void);
 int hidem_abi_version(void);
 
@@ -341,6 +341,22 @@ hidem_status hidem_lattice_fcc(int32_t nx, int32_t ny, int32_t nz, double a, dou
 hidem_status hidem_links_by_distance(const hidem_particle_soa *p, int64_t n, int32_t precision,
                                      double scale, hidem_link_soa *out, int64_t cap,
                                      int64_t *count);
+
+/* Replaces FileParticleGenerator::generate (PLiB/Generators/FileParticleGenerator.h:23-105)
+ * on one rank: the HDF5 point file of the reference's File lattice (lattice.path; the
+ * HiDEM/Benchmark/<size>/particles.h5 inputs of its MeshBlock benchmark, as libhdf5 writes
+ * them: superblock 0, symbol-table groups, deflate-compressed chunks). Datasets x_name,
+ * y_name, z_name, radius_name of the root group (lattice.xCords / yCords / zCords / radius;
+ * NULL for "xCord", "yCord", "zCord", "radius"); each value is read as float, as the
+ * reference reads them (readVectorSpann<float>), and stored in the particle fields
+ * (positions as double); thetas and diffs zero, owners and type 0, globalKeys 0..n-1
+ * (ParticleGenerator::setParticleKeys). The reference then keeps the particles that lie
+ * inside their bounding geometry (createParticle, PLiB/Generators/ParticleGenerator.h:37-57);
+ * that test is the caller's (the benchmark files hold only such points). With out == NULL
+ * only *count is written. Errors: HIDEM_ERR_IO with the text in hidem_create_error(). */
+hidem_status hidem_read_particle_file(const char *path, const char *x_name, const char *y_name,
+                                      const char *z_name, const char *radius_name, int32_t precision,
+                                      hidem_particle_soa *out, int64_t cap, int64_t *count);
 
 /* ---- bed and external force maps ------------------------------------- */
 

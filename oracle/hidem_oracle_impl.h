@@ -387,13 +387,15 @@ static int SFX(neighbours)(const hidem_params *P, const hidem_particle_soa *p, i
     SFX(grid_build)(&gd, p->xCord, p->yCord, p->zCord, n, d.searchDistance);
     const LP *rad = (const LP *)p->radius;
     int64_t off = 0;
-    int32_t row[4096];
+    /* one row at a time; rows longer than the buffer are refused (a crowded cell of a few
+       thousand particles still fits) */
+    static _Thread_local int32_t row[16384];
     int rc = 0;
     for (int64_t i = 0; i < n; ++i) {
         int c = SFX(neigh_row)(&gd, p->xCord, p->yCord, p->zCord, rad, i, d.interactDist, NULL);
         counts[i] = c;
         if (list) {
-            if (c > 4096) { rc = HIDEM_ERR_CAPACITY; break; }
+            if (c > 16384) { rc = HIDEM_ERR_CAPACITY; break; }
             SFX(neigh_row)(&gd, p->xCord, p->yCord, p->zCord, rad, i, d.interactDist, row);
             for (int k = 0; k < c; ++k) {
                 if (off + k < cap) list[off + k] = row[k];
