@@ -78,6 +78,17 @@ class HidemLinkSoA(C.Structure):
                 ("CT", _p * 6)]
 
 
+class HidemDeviceView(C.Structure):
+    """hidem_device_view: the context's device arrays (include/hidem_b200_iterate.cuh)."""
+    _fields_ = [("precision", _i32), ("record_bytes", _i32), ("n", _i64), ("L", _i64), ("step", _i64),
+                ("records", _p), ("force", _p), ("type", _p), ("input_index", _p), ("slot_of", _p),
+                ("counts", _p), ("contact_offsets", _p), ("contacts", _p), ("end_offsets", _p),
+                ("end_partner", _p), ("end_ct", _p * 6), ("end_state", _p), ("end_initial_length", _p),
+                ("end_link", _p), ("link_state", _p), ("link_slot_a", _p), ("link_slot_b", _p),
+                ("link_initial_length", _p), ("link_end_index", _p), ("events", _p),
+                ("event_count", _p), ("event_capacity", _i64), ("stream", _p)]
+
+
 class HidemStats(C.Structure):
     _fields_ = [("step", _i64), ("num_particles", _i64), ("num_links", _i64),
                 ("num_neighbour_pairs", _i64), ("max_neighbours", _i64),
@@ -315,6 +326,7 @@ _PROTOS = [
                                     _i32, C.POINTER(HidemParticleSoA)]),
     ("hidem_links_by_distance", C.c_int, [C.POINTER(HidemParticleSoA), _i64, _i32, _d,
                                           C.POINTER(HidemLinkSoA), _i64, C.POINTER(_i64)]),
+    ("hidem_get_device_view", C.c_int, [C.c_void_p, C.c_void_p]),
     ("hidem_read_particle_file", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                            C.c_char_p, _i32, C.POINTER(HidemParticleSoA), _i64,
                                            C.POINTER(_i64)]),

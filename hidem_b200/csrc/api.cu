@@ -14,11 +14,23 @@
 #include <type_traits>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kernels.h"
 
 using namespace hidem;
 
 namespace hidem {
+
+// NVTX range around a host call, named after the reference's phase (its xvtxRangePush
+// ranges, Iterators/DevPortabilityLayer.h:298-332): visible in Nsight timelines, free
+// when no profiler is attached (NVTX forwards to nothing then).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 // per-thread text of the last failure of a call that has no context
 thread_local std::string g_nocontext_error;
 }  // namespace hidem
@@ -391,6 +403,7 @@ hidem_status ensure_scan(hidem_ctx *ctx, long long n) {
 // permutation of the particle records, contact list, link-end layout.
 template <class LP>
 hidem_status rebuild(hidem_ctx *ctx) {
+    NvtxRange nvtx_range("generateNeighbourGrid + contact list + link ends");
     cudaStream_t st = ctx->stream;
     const int n = (int)ctx->n;
     const int cur = ctx->cur, nxt = 1 - cur;
@@ -1544,6 +1557,7 @@ hidem_status hidem_set_timestep(hidem_ctx *ctx, int64_t step) {
 }
 
 hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, int64_t n) {
+    NvtxRange nvtx_range("set_particles");
     if (!ctx) return HIDEM_ERR_ARG;
     if (!p || n <= 0) return fail(ctx, HIDEM_ERR_ARG, "need at least one particle");
     if (n >= (1ll << 31) - 64) return fail(ctx, HIDEM_ERR_CAPACITY, "n = %lld exceeds int32 indexing", (long long)n);
@@ -1601,6 +1615,7 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
 }
 
 hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L) {
+    NvtxRange nvtx_range("set_links");
     if (!ctx) return HIDEM_ERR_ARG;
     if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "set particles before links");
     if (L < 0 || (L > 0 && (!l || !l->globalKeyEndA || !l->globalKeyEndB || !l->initialLen || !l->state)))
@@ -1731,6 +1746,7 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
 }
 
 hidem_status hidem_grid_service(hidem_ctx *ctx) {
+    NvtxRange nvtx_range("gridService");
     if (!ctx) return HIDEM_ERR_ARG;
     if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
     CK(cudaSetDevice(ctx->device));
@@ -1746,6 +1762,7 @@ hidem_status hidem_regenerate(hidem_ctx *ctx) {
 }
 
 hidem_status hidem_compute_forces(hidem_ctx *ctx) {
+    NvtxRange nvtx_range("computePartForce");
     if (!ctx) return HIDEM_ERR_ARG;
     if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
     CK(cudaSetDevice(ctx->device));
@@ -1766,6 +1783,7 @@ hidem_status hidem_compute_forces(hidem_ctx *ctx) {
 }
 
 hidem_status hidem_integrate(hidem_ctx *ctx) {
+    NvtxRange nvtx_range("applyForce");
     if (!ctx) return HIDEM_ERR_ARG;
     if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
     CK(cudaSetDevice(ctx->device));
@@ -1781,6 +1799,7 @@ hidem_status hidem_integrate(hidem_ctx *ctx) {
 }
 
 hidem_status hidem_link_update(hidem_ctx *ctx) {
+    NvtxRange nvtx_range("linkUpdate");
     if (!ctx) return HIDEM_ERR_ARG;
     if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
     CK(cudaSetDevice(ctx->device));
@@ -1916,6 +1935,7 @@ hidem_status hidem_unpack_halo_forces(hidem_ctx *ctx, const void *device_in) {
 }
 
 hidem_status hidem_step(hidem_ctx *ctx, int32_t nsteps) {
+    NvtxRange nvtx_range("hidem_step");
     if (!ctx) return HIDEM_ERR_ARG;
     if (nsteps < 0) return fail(ctx, HIDEM_ERR_ARG, "negative step count");
     if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
@@ -2035,6 +2055,44 @@ hidem_status hidem_get_links(hidem_ctx *ctx, hidem_link_soa *out) {
     CK(cudaStreamSynchronize(st));
     dfree(stage);
     dfree(lstate);
+    return HIDEM_OK;
+}
+
+hidem_status hidem_get_device_view(hidem_ctx *ctx, hidem_device_view *o) {
+    if (!ctx || !o) return HIDEM_ERR_ARG;
+    if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->built) TRY(do_rebuild(ctx));
+    std::memset(o, 0, sizeof *o);
+    SideSet &s = ctx->side[ctx->curSide];
+    o->precision = ctx->P.precision;
+    o->record_bytes = ctx->mixed ? (int32_t)sizeof(PRec<float>) : (int32_t)sizeof(PRec<double>);
+    o->n = ctx->n;
+    o->L = ctx->L;
+    o->step = ctx->step;
+    o->records = ctx->rec[ctx->cur];
+    o->force = ctx->force;
+    o->type = ctx->type[ctx->ord];
+    o->input_index = ctx->orig[ctx->ord];
+    o->slot_of = ctx->slotOf;
+    o->counts = ctx->counts;
+    o->contact_offsets = reinterpret_cast<const int64_t *>(ctx->nOff);
+    o->contacts = ctx->nbr;
+    o->end_offsets = reinterpret_cast<const int64_t *>(ctx->sOff);
+    o->end_partner = s.partner;
+    for (int k = 0; k < 6; ++k) o->end_ct[k] = s.ct[k];
+    o->end_state = s.state;
+    o->end_initial_length = s.L0;
+    o->end_link = s.link;
+    o->link_state = ctx->linkState;
+    o->link_slot_a = ctx->linkSlotA;
+    o->link_slot_b = ctx->linkSlotB;
+    o->link_initial_length = ctx->L0link;
+    o->link_end_index = ctx->sideSlot[ctx->curSide];
+    o->events = ctx->events;
+    o->event_count = ctx->eventCount;
+    o->event_capacity = ctx->eventCap;
+    o->stream = ctx->stream;
     return HIDEM_OK;
 }
 
@@ -2727,6 +2785,7 @@ const char *hidem_batch_last_error(const hidem_batch *b) { return b ? b->err.c_s
 void *hidem_batch_get_stream(hidem_batch *b) { return b ? (void *)b->stream : nullptr; }
 
 hidem_status hidem_batch_step(hidem_batch *b, int32_t nsteps) {
+    NvtxRange nvtx_range("hidem_batch_step");
     if (!b) return HIDEM_ERR_ARG;
     b->err.clear();
     if (nsteps < 0) return bfail(b, HIDEM_ERR_ARG, "negative step count");

@@ -221,6 +221,13 @@ class HiDEMLib:
         """abi.STEP_KERNEL_* (AUTO: timed on the first fused steps)."""
         self._check(self._lib.hidem_set_step_kernel(self._ctx, int(kernel)))
 
+    def device_view(self) -> abi.HidemDeviceView:
+        """The context's device arrays (hidem_get_device_view), valid until the next call
+        that rebuilds or steps."""
+        v = abi.HidemDeviceView()
+        self._check(self._lib.hidem_get_device_view(self._ctx, C.byref(v)))
+        return v
+
     def set_checks(self, flags: int) -> None:
         """abi.CHECK_* bits (hidem_set_checks): CHECK_GRID_GROWTH refuses a rebuild whose
         grid has more than 10x the previous one's cells."""

@@ -287,6 +287,60 @@ void *hidem_get_stream(hidem_ctx *ctx);
 hidem_status hidem_profile(hidem_ctx *ctx, int32_t enable);
 hidem_status hidem_profile_read(hidem_ctx *ctx, double *step_kernel_ms, int64_t *launches);
 
+/* ---- device view (for the templated operator surface) ------------------ */
+
+/* The context's device arrays as the templated CUDA header include/hidem_b200_iterate.cuh
+ * reads them: the counterpart of the reference handing its ParticleData / LinkData objects
+ * (managed memory, Iterators/Allocator.h:18-76) to Iterator::iterate and to the functors of
+ * computePartForce / linkUpdate / applyForce (HiDEMLib.h:256-382). Particles are in storage
+ * ("slot") order, the order the reference's own pInd indices follow after its
+ * redistribution reorder: neighbour-grid cell, then input index.
+ *   record of slot s at records + s * record_bytes: x y z (f64), xDiff yDiff zDiff uDiff
+ *     vDiff wDiff (lp), radius (lp), xTheta yTheta zTheta (lp) [FP64: 3 doubles of padding]
+ *   force: 6 lp arrays of n (xForce..wForce, slot order), what computePartForce writes and
+ *     applyForce reads
+ *   contact k of slot s at contacts[contact_offsets[s / 32] + 32 k + s % 32] (a partner slot),
+ *     counts[s] & 0xffff contacts; link end k at end_offsets[s / 32] + 32 k + s % 32,
+ *     counts[s] >> 16 ends in ascending link index: end_partner (partner slot, bit 31 set
+ *     when this is end B of the link), end_ct[0..5] (CT0..CT5), end_state (the link's state
+ *     as the force loop reads it), end_initial_length, end_link (input link index)
+ *   per link (input order): link_state, link_slot_a / link_slot_b (the ends' slots),
+ *     link_initial_length, link_end_index[2 l + e] (the end storage index of end e)
+ * Taking the view builds the neighbour structures if none exist. It stays valid until the
+ * next call that rebuilds them or swaps the particle records (hidem_grid_service,
+ * hidem_regenerate, hidem_step, hidem_set_particles / hidem_set_links): take it again after
+ * each. Work on it is ordered on `stream`, the context's stream. */
+typedef struct hidem_device_view {
+    int32_t precision;         /* hidem_precision: lp = float (mixed) or double (FP64) */
+    int32_t record_bytes;      /* 64 (mixed) or 128 (FP64) */
+    int64_t n, L, step;
+    void *records;
+    void *force;
+    uint8_t *type;             /* per slot */
+    const int32_t *input_index;/* slot -> input index */
+    const int32_t *slot_of;    /* input index -> slot */
+    const uint32_t *counts;
+    const int64_t *contact_offsets;
+    const int32_t *contacts;
+    const int64_t *end_offsets;
+    const uint32_t *end_partner;
+    void *end_ct[6];
+    uint8_t *end_state;
+    void *end_initial_length;
+    const int32_t *end_link;
+    uint8_t *link_state;
+    const int32_t *link_slot_a, *link_slot_b;
+    void *link_initial_length;
+    const int32_t *link_end_index;
+    /* link-break events (input link index, timestep), the same list hidem_get_break_events
+       reads: an event is added at events[atomicAdd(event_count, 1)] when below event_capacity */
+    void *events;
+    unsigned long long *event_count;
+    int64_t event_capacity;
+    void *stream;              /* cudaStream_t */
+} hidem_device_view;
+hidem_status hidem_get_device_view(hidem_ctx *ctx, hidem_device_view *out);
+
 /* ---- readback (input order: index i is the i-th particle / link given) -- */
 
 hidem_status hidem_get_particles(hidem_ctx *ctx, hidem_particle_soa *out);

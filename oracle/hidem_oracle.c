@@ -31,6 +31,12 @@ void hidem_oracle_set_maps(const hidem_map2d *bed, const hidem_map2d *friction,
         for (int k = 0; k < 6; ++k) { g_maps[2 + k] = ext[k]; g_map_set[2 + k] = 1; }
 }
 
+/* Link functor of the next runs: 0 the default (HiDEMDefLinkForceFunc), 1 the IceBlock
+ * sample's own (HiDEM/IceBlock/MainIceBlock.cpp:173-262). */
+static int g_link_variant;
+
+void hidem_oracle_set_link_variant(int variant) { g_link_variant = variant; }
+
 static int clampi_(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 /* Collision mesh of the next runs (the caller keeps its arrays alive) and the face forces

@@ -45,6 +45,8 @@ void hidem_oracle_set_maps(const hidem_map2d *bed, const hidem_map2d *friction,
  * HiDEM/MeshConstrainedDem/MainMeshDem.cpp:111-113, 220-235 uses it; the arrays must
  * stay alive while they run. */
 void hidem_oracle_set_mesh(const hidem_mesh *mesh);
+/* 0: HiDEMDefLinkForceFunc; 1: the IceBlock sample's link functor */
+void hidem_oracle_set_link_variant(int variant);
 /* Face forces accumulated over the last run with a mesh (summed in particle order),
  * lp [triangles] each. */
 int hidem_oracle_mesh_face_forces(void *x, void *y, void *z);

@@ -292,6 +292,66 @@ static inline void SFX(beam)(const SFX(derived) *d, LP mask, LP xDist, LP yDist,
     F[5] = F[5] + (-(T02 * CT[3] + T22 * CT[5])) * mask;
 }
 
+/* The IceBlock sample's own link functor (HiDEM/IceBlock/MainIceBlock.cpp:173-262), the
+ * variant a caller passes through the templated computePartForce: no guard for exactly
+ * vertical links, LI and LP as square roots, invLILP = 1 / (LI * LP), LIDiv6 =
+ * 1 / (6 * LI); the rest as the default functor. */
+static inline void SFX(beam_iceblock)(const SFX(derived) *d, LP mask, LP xDist, LP yDist, LP zDist,
+                                      const LP *s, const LP *o, LP *CT, LP *F) {
+    F[0] = F[0] + (-d->damping * ((s[0] - o[0]) * d->invDt)) * mask;
+    F[1] = F[1] + (-d->damping * ((s[1] - o[1]) * d->invDt)) * mask;
+    F[2] = F[2] + (-d->damping * ((s[2] - o[2]) * d->invDt)) * mask;
+    F[3] = F[3] + (-d->dampingRotation * ((s[3] - o[3]) * d->invDt)) * mask;
+    F[4] = F[4] + (-d->dampingRotation * ((s[4] - o[4]) * d->invDt)) * mask;
+    F[5] = F[5] + (-d->dampingRotation * ((s[5] - o[5]) * d->invDt)) * mask;
+    LP xDist2 = xDist * xDist;
+    LP yDist2 = yDist * yDist;
+    LP zDist2 = zDist * zDist;
+    LP LI = LSQRT(xDist2 + yDist2 + zDist2);
+    LP LPl = LSQRT(xDist2 + yDist2);
+    LP invLI = (LP)1 / LI;
+    LP invLP = (LP)1 / LPl;
+    LP invLILP = (LP)1 / (LI * LPl);
+    LP T00 = xDist * invLI, T01 = yDist * invLI, T02 = zDist * invLI;
+    LP T10 = -yDist * invLP, T11 = xDist * invLP;
+    LP T20 = -(zDist * xDist) * invLILP;
+    LP T21 = -(zDist * yDist) * invLILP;
+    LP T22 = (xDist2 + yDist2) * invLILP;
+    LP B0 = T00 * s[0] + T01 * s[1] + T02 * s[2];
+    LP B1 = T10 * s[0] + T11 * s[1];
+    LP B2 = T20 * s[0] + T21 * s[1] + T22 * s[2];
+    LP B4 = T10 * s[3] + T11 * s[4];
+    LP B5 = T20 * s[3] + T21 * s[4] + T22 * s[5];
+    LP B6 = T00 * o[0] + T01 * o[1] + T02 * o[2];
+    LP B7 = T10 * o[0] + T11 * o[1];
+    LP B8 = T20 * o[0] + T21 * o[1] + T22 * o[2];
+    LP B10 = T10 * o[3] + T11 * o[4];
+    LP B11 = T20 * o[3] + T21 * o[4] + T22 * o[5];
+    LP L2 = LI * LI;
+    LP L3 = LI * LI * LI;
+    LP LIDiv6 = (LP)1 / ((LP)6 * LI);
+    LP K0 = d->E * d->W2 * invLI;
+    LP K1 = d->E * d->W4 / L3;
+    LP K5 = d->E * d->W4 / ((LP)2 * L2);
+    CT[0] = CT[0] + (K0 * B0 + (-K0) * B6);
+    CT[1] = CT[1] + (K1 * B1 + K5 * B5 + (-K1) * B7 + K5 * B11);
+    CT[2] = CT[2] + (K1 * B2 + (-K5) * B4 + (-K1) * B8 + (-K5) * B10);
+    F[0] = F[0] + (-(T00 * CT[0] + T10 * CT[1] + T20 * CT[2])) * mask;
+    F[1] = F[1] + (-(T01 * CT[0] + T11 * CT[1] + T21 * CT[2])) * mask;
+    F[2] = F[2] + (-(T02 * CT[0] + T22 * CT[2])) * mask;
+    LP K2 = d->G * d->W4 * LIDiv6;
+    LP K3 = d->E * d->W4 * LIDiv6 * (LP)2;
+    LP K4 = d->E * d->W4 * LIDiv6;
+    LP B3 = T00 * s[3] + T01 * s[4] + T02 * s[5];
+    LP B9 = T00 * o[3] + T01 * o[4] + T02 * o[5];
+    CT[3] = CT[3] + (K2 * B3 + (-K2) * B9);
+    CT[4] = CT[4] + ((-K5) * B2 + K3 * B4 + K5 * B8 + K4 * B10);
+    CT[5] = CT[5] + (K5 * B1 + K3 * B5 + (-K5) * B7 + K4 * B11);
+    F[3] = F[3] + (-(T00 * CT[3] + T10 * CT[4] + T20 * CT[5])) * mask;
+    F[4] = F[4] + (-(T01 * CT[3] + T11 * CT[4] + T21 * CT[5])) * mask;
+    F[5] = F[5] + (-(T02 * CT[3] + T22 * CT[5])) * mask;
+}
+
 /* HiDEMDefLinkBreakFunc::operator() (HiDEMDefaultFunctions.h:207-242). Returns the
  * new state. */
 static inline uint8_t SFX(break_test)(const SFX(derived) *d, double x1, double y1, double z1,
@@ -740,8 +800,12 @@ static int SFX(run)(const hidem_params *P, hidem_particle_soa *p, int64_t n, hid
                 for (int c = 0; c < 6; ++c) other[c] = df[c][q];
                 other[6] = rad[q];
                 LP mask = state[adj.link[k]] == 0 ? (LP)0 : (LP)1;
-                SFX(beam)(&d, mask, (LP)(xc - x[q]), (LP)(yc - y[q]), (LP)(zc - z[q]), self, other,
-                          CT + (int64_t)adj.side[k] * 6, f);
+                if (g_link_variant == 1)
+                    SFX(beam_iceblock)(&d, mask, (LP)(xc - x[q]), (LP)(yc - y[q]), (LP)(zc - z[q]), self,
+                                       other, CT + (int64_t)adj.side[k] * 6, f);
+                else
+                    SFX(beam)(&d, mask, (LP)(xc - x[q]), (LP)(yc - y[q]), (LP)(zc - z[q]), self, other,
+                              CT + (int64_t)adj.side[k] * 6, f);
             }
             for (int c = 0; c < 6; ++c) F[c * n + i] = f[c];
         }

@@ -147,3 +147,36 @@ int main() {
     assert out.returncode == 0
     if not cuda_available():
         assert "status=2" in out.stdout
+
+
+def test_device_view_struct_matches_the_header(tmp_path):
+    """hidem_device_view's size and field offsets as a C compiler lays them out."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc") or "/usr/bin/gcc"
+    src = tmp_path / "v.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "hidem_b200.h"\n'
+                   'int main(void){printf("%zu %zu %zu %zu\\n", sizeof(hidem_device_view),'
+                   ' offsetof(hidem_device_view, end_ct), offsetof(hidem_device_view, event_capacity),'
+                   ' offsetof(hidem_device_view, stream)); return 0;}\n')
+    exe = tmp_path / "v"
+    r = subprocess.run([gcc, f"-I{HEADER.parent}", str(src), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()
+    V = abi.HidemDeviceView
+    assert [int(x) for x in out] == [C.sizeof(V), V.end_ct.offset, V.event_capacity.offset, V.stream.offset]
+
+
+def test_iterate_header_compiles_for_sm100a(tmp_path):
+    """include/hidem_b200_iterate.cuh with a caller's functors (tests/iterate_harness.cu)
+    cross-compiles for sm_100a (the GPU tests run it)."""
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(nvcc).exists():
+        pytest.skip("no nvcc")
+    src = Path(__file__).with_name("iterate_harness.cu")
+    r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O1",
+                        "-fmad=false", f"-I{HEADER.parent}", "-c", str(src), "-o", str(tmp_path / "h.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
