@@ -72,6 +72,13 @@ def parse():
     ap.add_argument("--test-tongues", type=int, default=16, help="settle: held-out geometries")
     ap.add_argument("--train-steps", type=int, default=20000, help="settle: surrogate Adam steps")
     ap.add_argument("--tongue", default="40,12", help="settle: tongue plan size in metres x,y")
+    ap.add_argument("--tongue-thickness", type=float, default=6.0, help="settle: base ice thickness (m)")
+    ap.add_argument("--tongue-amplitude", type=float, default=2.0,
+                    help="settle: total amplitude of each heightfield's 8 Fourier modes (m)")
+    ap.add_argument("--settle-max-steps", type=int, default=40000, help="settle: step cap of each settle")
+    ap.add_argument("--settle-check", type=int, default=20, help="settle: steps between kinetic-energy reads")
+    ap.add_argument("--max-train-rows", type=int, default=None,
+                    help="settle: seeded sample of at most this many training rows")
     ap.add_argument("--blocks", type=int, default=256, help="ensemble: number of blocks")
     ap.add_argument("--no-graphs", action="store_true", help="ensemble: plain launches")
     ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped", "thread-async", "two-pass"],
@@ -545,10 +552,11 @@ def main_settle(args):
         return
     torch.cuda.set_device(local)
     size = tuple(float(v) for v in args.tongue.split(","))
-    thick, amp = 6.0, 2.0
+    thick, amp = args.tongue_thickness, args.tongue_amplitude
     rep = settle.warm_start_experiment(n_train=args.train_tongues, n_test=args.test_tongues, size=size,
                                        base_thickness=thick, amplitude=amp, train_steps=args.train_steps,
-                                       inputs=args.surrogate_inputs)
+                                       inputs=args.surrogate_inputs, max_steps=args.settle_max_steps,
+                                       max_train_rows=args.max_train_rows, check=args.settle_check)
     # tensor-core forward throughput of the trained network's shape on 2M rows
     lattice = args.surrogate_inputs == "lattice"
     nin = settle.N_LATTICE_INPUTS if lattice else 5

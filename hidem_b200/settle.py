@@ -378,12 +378,15 @@ def warm_start_experiment(n_train: int = 256, n_test: int = 16, size=(40.0, 12.0
                           base_thickness: float = 6.0, amplitude: float = 2.0,
                           train_steps: int = 20000, batch: int = 8192, seed: int = 1000,
                           tol: float = 1e-6, max_steps: int = 40000, surrogate_cfg: dict | None = None,
-                          with_rotation: bool = True, mirror: bool = True, inputs: str = "lattice"):
+                          with_rotation: bool = True, mirror: bool = True, inputs: str = "lattice",
+                          max_train_rows: int | None = None, check: int = 20):
     """Cold settles of the training tongues, surrogate training on their settled
     displacements, then cold and warm settles of held-out tongues, compared by the plain
     method's convergence test. inputs: "lattice" (lattice_inputs, 4 Fourier bands, the
     learning rate decayed along a half cosine) or "coords" (the 5 coordinate inputs of
-    surrogate_inputs, 6 bands, constant rate)."""
+    surrogate_inputs, 6 bands, constant rate). max_train_rows: a seeded uniform sample of
+    at most that many training rows (large tongues); check: steps between the kinetic-energy
+    reads of the settles."""
     import time
     from . import surrogate as sg
     sec = {}
@@ -392,7 +395,7 @@ def warm_start_experiment(n_train: int = 256, n_test: int = 16, size=(40.0, 12.0
     test = [glacier_tongue(seed + 100000 + i, size, base_thickness, amplitude=amplitude) for i in range(n_test)]
     sec["geometry"] = time.time() - t0
     t0 = time.time()
-    cold_train = settle_many(train, tol=tol, max_steps=max_steps)
+    cold_train = settle_many(train, tol=tol, max_steps=max_steps, check=check)
     sec["cold_train_settles"] = time.time() - t0
     if inputs not in ("lattice", "coords"):
         raise ValueError(f"inputs {inputs!r}: 'lattice' or 'coords'")
@@ -410,6 +413,9 @@ def warm_start_experiment(n_train: int = 256, n_test: int = 16, size=(40.0, 12.0
     mirrors = ((1, 1), (-1, 1), (1, -1), (-1, -1)) if mirror else ((1, 1),)
     xs = np.concatenate([feats(t, m) for m in mirrors for t in train])
     ys = np.concatenate([ys * np.array([m[0], m[1], 1]) for m in mirrors])
+    if max_train_rows is not None and xs.shape[0] > max_train_rows:
+        pick = np.sort(np.random.default_rng(seed).choice(xs.shape[0], size=max_train_rows, replace=False))
+        xs, ys = xs[pick], ys[pick]
     sec["features"] = time.time() - t0
     t0 = time.time()
     base = {"fourier_bands": 4, "cosine_decay": 1} if inputs == "lattice" else {"fourier_bands": 6}
@@ -420,11 +426,11 @@ def warm_start_experiment(n_train: int = 256, n_test: int = 16, size=(40.0, 12.0
         preds = [net.predict(feats(t)).astype(np.float64) * DISP_SCALE for t in test]
     sec["training"] = time.time() - t0
     t0 = time.time()
-    cold = settle_many(test, tol=tol, max_steps=max_steps)
+    cold = settle_many(test, tol=tol, max_steps=max_steps, check=check)
     sec["cold_test_settles"] = time.time() - t0
     t0 = time.time()
     warm = settle_many(test, [warm_state(t, d, rotation_from_displacement(t, d) if with_rotation else None)
-                              for t, d in zip(test, preds)], tol=tol, max_steps=max_steps)
+                              for t, d in zip(test, preds)], tol=tol, max_steps=max_steps, check=check)
     sec["warm_test_settles"] = time.time() - t0
     rel, err = [], []
     for t, d, c, w in zip(test, preds, cold, warm):
