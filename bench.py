@@ -15,8 +15,8 @@ step, or the one kernel of a fused step). `cpu_baseline` times the reference's o
 slab line also carries `rebuild_amortised` (the configuration's 2000-step run from step 0,
 its rebuilds included), `fp64` (the same slab in the plain FP64 build) and `settle` (the
 learned warm start's settling steps, cold against surrogate-seeded).
-With --gpus N > 1 (torchrun) every rank advances its own replica of the slab (the path
-has no exchange on one node for this workload; weak scaling).
+With --gpus N > 1 (torchrun) the slab is decomposed into N x-slabs, one per GPU, with the
+halo force exchange over NCCL (strong scaling); --replicas runs N independent copies instead.
 --impl reference times the reference's CPU implementation on this host's cores.
 --workload ensemble: 256 independent FCC blocks of 5k-80k particles advanced by one
 batched launch per timestep (runs of launches replayed from CUDA graphs); with --gpus N
@@ -85,6 +85,8 @@ def parse():
                     default="auto", help="step kernel (auto: timed on the first steps)")
     ap.add_argument("--slab", default="400,100,100",
                     help="slab size in metres x,y,z (smaller slabs for profiling captures)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="slab with --gpus N > 1: N independent replicas instead of the x-slab decomposition")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="slab: skip the plain-FP64 run")
@@ -807,6 +809,105 @@ def main_mesh(args):
     print(json.dumps(line))
 
 
+def main_slab_decomposed(args):
+    """The default slab line on N > 1 GPUs (torchrun, one rank per GPU): the slab is
+    decomposed into N x-slabs (hidem_b200.slab, the reference's MPI distribution with its
+    halo force exchange, HiDEMDistribution.h:99-234), NCCL point-to-point for the halo
+    forces and all-reduces for gridService. Strong scaling: the whole 5.7M slab over N GPUs;
+    `value` = particles x steps / the slowest rank's time."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from hidem_b200 import abi, slab
+    from hidem_b200.hidemlib import HiDEMLib
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    prec, P, p, l, name = make_workload(args)
+    n, L = p["xCord"].shape[0], l["state"].shape[0]
+    comm = slab.DistComm()
+    kernel = KERNELS["thread-capped" if prec == abi.PREC_MIXED else "thread-async"]
+
+    def timed(body, steps):
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        body(steps)
+        torch.cuda.synchronize()
+        e1.record()
+        e1.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    lib = HiDEMLib(P, device=local)
+    lib.set_step_kernel(kernel)
+    run = slab.SlabRun(comm, [lib], p, l)
+    run.step(max(args.warmup, 3))
+    st0 = lib.stats()
+    red0, ex0 = run.redistributions, run.exchanged
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = timed(run.step, args.steps)
+    clk = clocks.stop()
+    st1 = lib.stats()
+    launches = int(st1["kernel_launches"] - st0["kernel_launches"])
+    held = int(st1["num_particles"])
+    lib.close()
+
+    e2e = None
+    if not args.no_e2e:
+        # a fresh decomposed job: this rank's share uploaded from host arrays, K steps,
+        # this rank's particles downloaded; the slowest rank's wall time
+        lib2 = HiDEMLib(P, device=local)
+        lib2.set_step_kernel(kernel)
+        torch.cuda.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        run2 = slab.SlabRun(comm, [lib2], p, l)
+        run2.step(args.steps)
+        out = lib2.get_particles()
+        lib2.synchronize()
+        el = time.perf_counter() - t0
+        t = torch.tensor([el], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+        held2 = int(lib2.stats()["num_particles"])
+        nb = torch.tensor([held2 * 77.0, sum(v.nbytes for v in out.values())], device="cuda", dtype=torch.float64)
+        dist.all_reduce(nb)
+        lib2.close()
+        e2e = {"value": n * args.steps / el, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": int(nb[0].item()), "d2h_bytes_per_step": int(nb[1].item()),
+               "step": f"one decomposed job over {world} ranks: partition, each rank's share uploaded "
+                       f"from host arrays, {args.steps} timesteps with halo exchanges, each rank's "
+                       f"particles downloaded"}
+    halo = torch.tensor([held - 0.0], device="cuda", dtype=torch.float64)
+    dist.all_reduce(halo)
+    dist.destroy_process_group()
+    if rank != 0:
+        return
+    value = n * args.steps / (ms / 1e3)
+    cfg = slab_config(args, name, n, L, world)
+    line = {
+        "metric": slab_metric(args), "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": (value / PUBLISHED_MIXED) if (prec == abi.PREC_MIXED and args.workload == "slab") else None,
+        "dtype": "f32+f64pos" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
+        "config": cfg,
+        "decomposition": {"transport": "NCCL point-to-point (halo forces), all-reduce (gridService)",
+                          "particles_held_all_ranks": int(halo.item()),
+                          "halo_fraction": float(halo.item()) / n - 1.0,
+                          "force_records_rank0_per_step": (run.exchanged - ex0) / max(args.steps, 1),
+                          "redistributions_in_timed_steps": run.redistributions - red0},
+        "roofline": None, "cpu_baseline": None, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
 def main_ranks(args):
     """The slab decomposed over ranks (hidem_b200.slab): with one process, --ranks contexts
     on its GPU exchange halo forces by device copies; under torchrun, one rank per GPU over
@@ -913,9 +1014,9 @@ def main_ranks(args):
 
 def slab_config(args, name: str, n: int, L: int, world: int) -> dict:
     """The `config` of the slab line, identical in both arms at the same N."""
+    par = f"x-slabs{world}" if (world > 1 and not args.replicas) else f"replicas x{world}"
     return {"workload": name, "particles": n, "links": L, "precision": args.precision,
-            "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (records + link ends > 126 MB)"}
+            "parallelism": par, "l2": "inputs larger than L2 (records + link ends > 126 MB)"}
 
 
 def slab_metric(args) -> str:
@@ -1322,6 +1423,9 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args)
+        return
+    if dist_env()[0] > 1 and not args.replicas:
+        main_slab_decomposed(args)
         return
     main_slab(args)
 

@@ -1998,19 +1998,17 @@ hidem_status hidem_get_particles(hidem_ctx *ctx, hidem_particle_soa *out) {
                      out->radius, out->xTheta, out->yTheta, out->zTheta};
     for (int k = 0; k < 10; ++k)
         if (lpf[k]) CK(cudaMemcpyAsync(lpf[k], lpb + lp * (size_t)n * k, lp * (size_t)n, cudaMemcpyDeviceToHost, st));
-    std::vector<int32_t> orig;
-    std::vector<uint8_t> ty;
     if (out->type) {
-        orig.resize((size_t)n);
-        ty.resize((size_t)n);
-        CK(cudaMemcpyAsync(orig.data(), ctx->orig[ctx->ord], 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(ty.data(), ctx->type[ctx->ord], (size_t)n, cudaMemcpyDeviceToHost, st));
+        // the type bytes in caller order, staged in the rebuild's permutation scratch
+        uint8_t *tstage = reinterpret_cast<uint8_t *>(ctx->perm);
+        launch_scatter_u8(ctx->type[ctx->ord], ctx->orig[ctx->ord], (int)n, tstage, st);
+        ctx->launches += 1;
+        CK(cudaMemcpyAsync(out->type, tstage, (size_t)n, cudaMemcpyDeviceToHost, st));
     }
-    CK(cudaStreamSynchronize(st));
-    if (out->type)
-        for (long long s2 = 0; s2 < n; ++s2) out->type[orig[s2]] = ty[s2];
+    // the host-held fields while the copies run
     if (out->owners) std::memcpy(out->owners, ctx->owners.data(), 4 * (size_t)n);
     if (out->globalKeys) std::memcpy(out->globalKeys, ctx->keys.data(), 8 * (size_t)n);
+    CK(cudaStreamSynchronize(st));
     return HIDEM_OK;
 }
 

@@ -1412,6 +1412,16 @@ template int launch_scan<int, int>(const int *, long long, int, int *, int *, in
 template int launch_scan<int, long long>(const int *, long long, long long, long long *, long long *,
                                          long long *, cudaStream_t);
 
+__global__ void k_scatter_u8(const uint8_t *__restrict__ in, const int *__restrict__ to, int n,
+                             uint8_t *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[to[i]] = in[i];
+}
+
+void launch_scatter_u8(const uint8_t *in, const int *to, int n, uint8_t *out, cudaStream_t s) {
+    if (n > 0) k_scatter_u8<<<nblk(n, 256), 256, 0, s>>>(in, to, n, out);
+}
+
 void launch_scatter(const int *cellOf, int n, const int *cellStart, int *cursor, int *perm,
                     cudaStream_t s) {
     k_scatter<<<nblk(n, 256), 256, 0, s>>>(cellOf, n, cellStart, cursor, perm);

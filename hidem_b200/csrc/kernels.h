@@ -94,6 +94,8 @@ template <class TI, class TO>
 int launch_scan(const TI *in, long long n, TO scaleBy, TO *out, TO *sums, TO *total, cudaStream_t s);
 void launch_scatter(const int *cellOf, int n, const int *cellStart, int *cursor, int *perm,
                     cudaStream_t s);
+// out[to[i]] = in[i] for i < n (slot-order bytes into caller order)
+void launch_scatter_u8(const uint8_t *in, const int *to, int n, uint8_t *out, cudaStream_t s);
 // Members of a neighbour-grid cell of at most kSmallCell are sorted by one thread; larger
 // cells (listed in bigList, which holds n / kSmallCell + 1 entries) by one CTA each, up to
 // kBigCellCap members: a larger cell sets errorCode in errorFlag. origOld == nullptr sorts
