@@ -327,6 +327,7 @@ _PROTOS = [
     ("hidem_links_by_distance", C.c_int, [C.POINTER(HidemParticleSoA), _i64, _i32, _d,
                                           C.POINTER(HidemLinkSoA), _i64, C.POINTER(_i64)]),
     ("hidem_get_device_view", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("hidem_compute_forces_packed", C.c_int, [C.c_void_p, C.c_void_p]),
     ("hidem_read_particle_file", C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                            C.c_char_p, _i32, C.POINTER(HidemParticleSoA), _i64,
                                            C.POINTER(_i64)]),

@@ -76,6 +76,7 @@ struct hidem_ctx {
     int32_t *slotOf = nullptr;
     int32_t *perm = nullptr;
     int32_t *bigCells = nullptr;  // crowded cells of a rebuild's sort (n / 32 + 2 entries, count last)
+    int32_t *haloSendPos = nullptr;  // per slot: position in the halo send list, or -1
     void *force = nullptr;
 
     // grid
@@ -487,6 +488,10 @@ hidem_status rebuild(hidem_ctx *ctx) {
     ctx->launches += 3;
     if (ctx->L > 0) {
         launch_link_slots(ctx->linkA, ctx->linkB, ctx->slotOf, ctx->L, ctx->linkSlotA, ctx->linkSlotB, st);
+        ctx->launches += 1;
+    }
+    if (ctx->nHaloSend > 0 && ctx->haloSendPos) {
+        launch_send_pos(ctx->slotOf, ctx->haloSend, ctx->nHaloSend, n, ctx->haloSendPos, st);
         ctx->launches += 1;
     }
     ctx->cur = nxt;
@@ -1481,6 +1486,7 @@ void hidem_destroy(hidem_ctx *ctx) {
     dfree(ctx->slotOf);
     dfree(ctx->perm);
     dfree(ctx->bigCells);
+    dfree(ctx->haloSendPos);
     dfree(ctx->force);
     dfree(ctx->cellCount);
     dfree(ctx->cellStart);
@@ -1761,25 +1767,51 @@ hidem_status hidem_regenerate(hidem_ctx *ctx) {
     return do_rebuild(ctx);
 }
 
-hidem_status hidem_compute_forces(hidem_ctx *ctx) {
-    NvtxRange nvtx_range("computePartForce");
+hidem_status halo_forces(hidem_ctx *ctx, void *buf, bool pack);
+
+// the split force pass; with sendBuf, the halo send records come out of the same kernel
+// where the force pass is the thread-per-particle one, else from the pack kernel after it
+static hidem_status compute_forces_into(hidem_ctx *ctx, void *sendBuf) {
     if (!ctx) return HIDEM_ERR_ARG;
     if (!ctx->haveParticles || !ctx->haveLinks) return fail(ctx, HIDEM_ERR_STATE, "particles and links must be set");
     CK(cudaSetDevice(ctx->device));
     if (!ctx->built) TRY(do_rebuild(ctx));
     const int kern = force_kernel(step_kernel_settled(ctx));
+    const bool fusedPack = sendBuf && ctx->nHaloSend > 0 && ctx->haloSendPos &&
+                           (kern == HIDEM_STEP_KERNEL_THREAD || kern == HIDEM_STEP_KERNEL_THREAD_CAPPED);
     if (ctx->mixed) {
         StepArgs<float> a = step_args<float>(ctx);
+        if (fusedPack) {
+            a.sendPos = ctx->haloSendPos;
+            a.sendBuf = static_cast<float *>(sendBuf);
+        }
         launch_step<float>(ctx->cf, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, kern,
                            ctx->stream);
     } else {
         StepArgs<double> a = step_args<double>(ctx);
+        if (fusedPack) {
+            a.sendPos = ctx->haloSendPos;
+            a.sendBuf = static_cast<double *>(sendBuf);
+        }
         launch_step<double>(ctx->cd, a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP, kern,
                             ctx->stream);
     }
     ctx->launches += 1;
     CK(cudaGetLastError());
+    if (sendBuf && !fusedPack) TRY(halo_forces(ctx, sendBuf, true));
     return HIDEM_OK;
+}
+
+hidem_status hidem_compute_forces(hidem_ctx *ctx) {
+    NvtxRange nvtx_range("computePartForce");
+    return compute_forces_into(ctx, nullptr);
+}
+
+hidem_status hidem_compute_forces_packed(hidem_ctx *ctx, void *device_out) {
+    NvtxRange nvtx_range("computePartForce + halo pack");
+    if (!ctx) return HIDEM_ERR_ARG;
+    if (ctx->nHaloSend > 0 && !device_out) return fail(ctx, HIDEM_ERR_ARG, "null halo buffer");
+    return compute_forces_into(ctx, ctx->nHaloSend > 0 ? device_out : nullptr);
 }
 
 hidem_status hidem_integrate(hidem_ctx *ctx) {
@@ -1904,13 +1936,18 @@ hidem_status hidem_set_halo_exchange(hidem_ctx *ctx, const int32_t *send_index, 
         TRY(dalloc(ctx, &ctx->haloRecv, n_recv));
         CK(cudaMemcpyAsync(ctx->haloRecv, recv_index, 4 * (size_t)n_recv, cudaMemcpyHostToDevice, ctx->stream));
     }
+    if (n_send > 0) {
+        TRY(dalloc(ctx, &ctx->haloSendPos, ctx->n));
+        launch_send_pos(ctx->slotOf, ctx->haloSend, n_send, (int)ctx->n, ctx->haloSendPos, ctx->stream);
+        ctx->launches += 1;
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->nHaloSend = n_send;
     ctx->nHaloRecv = n_recv;
     return HIDEM_OK;
 }
 
-static hidem_status halo_forces(hidem_ctx *ctx, void *buf, bool pack) {
+hidem_status halo_forces(hidem_ctx *ctx, void *buf, bool pack) {
     if (!ctx) return HIDEM_ERR_ARG;
     if (!ctx->haveParticles) return fail(ctx, HIDEM_ERR_STATE, "no particles set");
     const long long m = pack ? ctx->nHaloSend : ctx->nHaloRecv;

@@ -148,6 +148,10 @@ struct StepArgs {
     int *errorFlag;
     int maxContacts, maxEnds; // widest rows of this layout
     LP bendBreak, maxLoad;    // HiDEMDefLinkBreakFunc thresholds (per context in a batch)
+    // halo send records written by the force pass itself (split path; null: none): the
+    // slot's position in the send list or -1, and the packed buffer of 6 lp per position
+    const int32_t *sendPos;
+    LP *sendBuf;
 };
 
 }  // namespace hidem

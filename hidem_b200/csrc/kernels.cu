@@ -655,6 +655,14 @@ __device__ __forceinline__ void step_thread_particle(const Consts<LP> &c, const 
         } else {
 #pragma unroll
             for (int q = 0; q < 6; ++q) a.force[(long long)q * a.n + i] = F[q];
+            // a particle another rank integrates: its record of the halo send buffer too
+            if (a.sendPos) {
+                const int sp = __ldg(a.sendPos + i);
+                if (sp >= 0) {
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) a.sendBuf[6ll * sp + q] = F[q];
+                }
+            }
         }
     }
     if (FUSED && a.reduceDiff) {
@@ -1411,6 +1419,18 @@ int launch_scan(const TI *in, long long n, TO scaleBy, TO *out, TO *sums, TO *to
 template int launch_scan<int, int>(const int *, long long, int, int *, int *, int *, cudaStream_t);
 template int launch_scan<int, long long>(const int *, long long, long long, long long *, long long *,
                                          long long *, cudaStream_t);
+
+// position of each slot in the halo send list (-1: not sent): pos[slotOf[index[k]]] = k
+__global__ void k_send_pos(const int *__restrict__ slotOf, const int *__restrict__ index, long long m,
+                           int *__restrict__ pos) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) pos[slotOf[index[k]]] = (int)k;
+}
+
+void launch_send_pos(const int *slotOf, const int *index, long long m, int n, int *pos, cudaStream_t s) {
+    cudaMemsetAsync(pos, 0xff, sizeof(int) * (size_t)n, s);
+    if (m > 0) k_send_pos<<<nblk(m, 256), 256, 0, s>>>(slotOf, index, m, pos);
+}
 
 __global__ void k_scatter_u8(const uint8_t *__restrict__ in, const int *__restrict__ to, int n,
                              uint8_t *__restrict__ out) {

@@ -94,6 +94,8 @@ template <class TI, class TO>
 int launch_scan(const TI *in, long long n, TO scaleBy, TO *out, TO *sums, TO *total, cudaStream_t s);
 void launch_scatter(const int *cellOf, int n, const int *cellStart, int *cursor, int *perm,
                     cudaStream_t s);
+// pos[s] = position of slot s in the halo send list `index` (particle indices), else -1
+void launch_send_pos(const int *slotOf, const int *index, long long m, int n, int *pos, cudaStream_t s);
 // out[to[i]] = in[i] for i < n (slot-order bytes into caller order)
 void launch_scatter_u8(const uint8_t *in, const int *to, int n, uint8_t *out, cudaStream_t s);
 // Members of a neighbour-grid cell of at most kSmallCell are sorted by one thread; larger

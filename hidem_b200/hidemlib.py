@@ -160,6 +160,11 @@ class HiDEMLib:
         self._check(self._lib.hidem_set_halo_exchange(self._ctx, snd.ctypes.data, snd.shape[0],
                                                       rcv.ctypes.data, rcv.shape[0]))
 
+    def compute_forces_packed(self, device_ptr: int) -> None:
+        """computePartForce with the halo send records written by the force pass itself
+        (hidem_compute_forces_packed)."""
+        self._check(self._lib.hidem_compute_forces_packed(self._ctx, C.c_void_p(device_ptr)))
+
     def pack_halo_forces(self, device_ptr: int) -> None:
         self._check(self._lib.hidem_pack_halo_forces(self._ctx, C.c_void_p(device_ptr)))
 

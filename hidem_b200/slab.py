@@ -380,8 +380,11 @@ class SlabRun:
 
     def _forces(self) -> None:
         for lib, buf in zip(self.libs, self.send_bufs):
-            lib.computePartForce()
-            lib.pack_halo_forces(buf.data_ptr())
+            if hasattr(lib, "compute_forces_packed"):
+                lib.compute_forces_packed(buf.data_ptr())  # the pack in the force pass
+            else:
+                lib.computePartForce()
+                lib.pack_halo_forces(buf.data_ptr())
         for lib in self.libs:
             lib.synchronize()
         self.comm.exchange(self.layout, self.send_bufs, self.recv_bufs)

@@ -238,6 +238,11 @@ hidem_status hidem_set_halo_exchange(hidem_ctx *ctx, const int32_t *send_index, 
  * particle), from the last hidem_compute_forces to `device_out` (device memory), on the
  * context's stream (CommunicatorPacked::packAllCommData). */
 hidem_status hidem_pack_halo_forces(hidem_ctx *ctx, void *device_out);
+/* hidem_compute_forces followed by hidem_pack_halo_forces into `device_out`, with the send
+ * records written by the force pass itself as it finishes each listed particle (the pack
+ * fused into its epilogue; after the item and asynchronous-copy force kernels the pack
+ * kernel runs instead). The same forces and records as the two calls. */
+hidem_status hidem_compute_forces_packed(hidem_ctx *ctx, void *device_out);
 /* Overwrites the forces of the receive list with n_recv x 6 lp values read from
  * `device_in` (device memory), on the context's stream; the caller has made the stream
  * wait for the data (CommunicatorPacked::unpackAllCommData). */

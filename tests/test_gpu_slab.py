@@ -103,3 +103,44 @@ def test_halo_exchange_entry_points_check_their_arguments(gpu):
         assert np.allclose(lib.stats()["grid_min"], lo - 3.0)
     finally:
         lib.close()
+
+
+@pytest.mark.parametrize("precision", PRECS)
+@pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_THREAD_CAPPED, abi.STEP_KERNEL_ITEMS])
+def test_pack_in_the_force_pass_equals_the_pack_kernel(gpu, precision, kernel):
+    """hidem_compute_forces_packed: the send records written by the force pass's epilogue
+    (the item kernel: by the pack kernel after it) equal hidem_compute_forces followed by
+    hidem_pack_halo_forces, before and after a rebuild that moves the slots."""
+    import torch
+    P, p, l, _ = case("calving_slab", precision)
+    n = p["xCord"].shape[0]
+    rng = np.random.default_rng(3)
+    send = np.sort(rng.choice(n, size=n // 7, replace=False)).astype(np.int32)
+    recv = np.sort(rng.choice(n, size=n // 9, replace=False)).astype(np.int32)
+    dt = torch.float32 if precision == abi.PREC_MIXED else torch.float64
+    libs = []
+    for _ in range(2):
+        lib = HiDEMLib(P)
+        lib.set_step_kernel(kernel)
+        lib.set_particles(p)
+        lib.set_links(l)
+        lib.set_halo_exchange(send, recv)
+        libs.append(lib)
+    a, b = libs
+    for rnd in range(3):
+        ba = torch.zeros(6 * send.size, dtype=dt, device="cuda")
+        bb = torch.full((6 * send.size,), -7.0, dtype=dt, device="cuda")
+        a.computePartForce()
+        a.pack_halo_forces(ba.data_ptr())
+        b.compute_forces_packed(bb.data_ptr())
+        a.synchronize()
+        b.synchronize()
+        assert torch.equal(ba, bb)
+        assert np.array_equal(a.get_forces(), b.get_forces())
+        for lib in libs:
+            lib.applyForce()
+            lib.finalizeTs()
+            if rnd == 1:
+                lib.regenerate()
+    for lib in libs:
+        lib.close()
