@@ -328,14 +328,19 @@ class SlabRun:
         return reach, width
 
     def _distribute(self, particles: dict, links: dict) -> None:
-        import torch
+        """The first distribution, from the whole set (every process has it)."""
         a, b = link_ends(particles, links)
+        self._a, self._b = a.astype(np.int64), b.astype(np.int64)  # link ends never change
         self._reach, self._width = self._widths(particles)
         self.layout = slab_layout(particles["xCord"], a, b, self.comm.size, self._width)
+        self._install([split_state(particles, links, self.layout, r) for r in self.comm.ranks])
+
+    def _install(self, states: list) -> None:
+        """Sets this process's contexts to their held sets of self.layout."""
+        import torch
         self.send_bufs, self.recv_bufs = [], []
         self._x0 = []
-        for lib, r in zip(self.libs, self.comm.ranks):
-            p, l = split_state(particles, links, self.layout, r)
+        for lib, r, (p, l) in zip(self.libs, self.comm.ranks, states):
             self._x0.append(p["xCord"].copy())
             lib.set_particles(p)
             lib.set_links(l)
@@ -345,6 +350,95 @@ class SlabRun:
             self.send_bufs.append(torch.zeros(6 * max(1, snd.size), dtype=self._tdtype, device=dev))
             self.recv_bufs.append(torch.zeros(6 * max(1, rcv.size), dtype=self._tdtype, device=dev))
         self.redistributions += 1
+
+    def _redistribute(self) -> None:
+        """A new distribution from the ranks' current state, moving only what changes hands
+        (the reference's ParticleTransporter / LinkTransporter, HiDEMDistribution.h:188-234):
+        every rank publishes the x of the particles it owns, every process recomputes the
+        same layout from them (slab_layout is deterministic), and each rank receives only
+        the particles and links it did not hold before — each from a rank that held it:
+        particles from their old owner, links from the old owner of their end A. Halo
+        copies and every held link's two sides are bit-equal to their originals (forces
+        are exchanged; a side's history depends only on the two end records), so what a
+        rank already holds stays as it is. The result equals splitting the gathered whole
+        set by the new layout, array for array."""
+        old = self.layout
+        R = self.comm.size
+        states, mine = [], []
+        for lib, r in zip(self.libs, self.comm.ranks):
+            p, l = lib.get_particles(), lib.get_links()
+            states.append((p, l))
+            own = old.owner[old.local[r]] == r
+            mine.append((old.local[r][own], p["xCord"][own]))
+        x_all = np.empty(self.n, np.float64)
+        seen = np.zeros(self.n, bool)
+        for idx, x in self.comm.allgather(mine):
+            x_all[idx] = x
+            seen[idx] = True
+        if not seen.all():
+            raise RuntimeError("a particle has no owner")
+        new = slab_layout(x_all, self._a, self._b, R, self._width)
+        # what each destination lacks, from the ranks of this process that can supply it
+        payloads = []
+        for (p, l), r in zip(states, self.comm.ranks):
+            pay = {}
+            for d in range(R):
+                if d == r:
+                    continue
+                need_p = np.setdiff1d(new.local[d], old.local[d], assume_unique=True)
+                need_p = need_p[old.owner[need_p] == r]
+                need_l = np.setdiff1d(new.links[d], old.links[d], assume_unique=True)
+                need_l = need_l[old.owner[self._a[need_l]] == r]
+                if need_p.size == 0 and need_l.size == 0:
+                    continue
+                pi = old.local_index(r, need_p)
+                li = np.searchsorted(old.links[r], need_l)
+                side = np.stack([2 * li, 2 * li + 1], axis=1).reshape(-1)
+                pay[d] = (need_p, {k: v[pi] for k, v in p.items()}, need_l,
+                          {k: (v[side] if k in abi.SIDE_FIELDS else v[li]) for k, v in l.items()})
+            payloads.append(pay)
+        received = self.comm.allgather(payloads)
+        out = []
+        for (p, l), r in zip(states, self.comm.ranks):
+            gp, gl = new.local[r], new.links[r]
+            np_ = {k: np.zeros(gp.size, v.dtype) for k, v in p.items()}
+            nl = {k: np.zeros(2 * gl.size if k in abi.SIDE_FIELDS else gl.size, v.dtype) for k, v in l.items()}
+            # kept: what this rank held before
+            pos = np.minimum(np.searchsorted(old.local[r], gp), max(old.local[r].size - 1, 0))
+            kept = old.local[r][pos] == gp if old.local[r].size else np.zeros(gp.size, bool)
+            for k, v in p.items():
+                np_[k][kept] = v[pos[kept]]
+            lpos = np.minimum(np.searchsorted(old.links[r], gl), max(old.links[r].size - 1, 0))
+            lkept = old.links[r][lpos] == gl if old.links[r].size else np.zeros(gl.size, bool)
+            for k, v in l.items():
+                if k in abi.SIDE_FIELDS:
+                    nl[k].reshape(-1, 2)[lkept] = v.reshape(-1, 2)[lpos[lkept]]
+                else:
+                    nl[k][lkept] = v[lpos[lkept]]
+            got_p, got_l = kept.copy(), lkept.copy()
+            for pays in received:
+                if r not in pays:
+                    continue
+                idx, vals, lidx, lvals = pays[r]
+                if idx.size:
+                    at = np.searchsorted(gp, idx)
+                    for k, v in vals.items():
+                        np_[k][at] = v
+                    got_p[at] = True
+                if lidx.size:
+                    at = np.searchsorted(gl, lidx)
+                    for k, v in lvals.items():
+                        if k in abi.SIDE_FIELDS:
+                            nl[k].reshape(-1, 2)[at] = v.reshape(-1, 2)
+                        else:
+                            nl[k][at] = v
+                    got_l[at] = True
+            if not (got_p.all() and got_l.all()):
+                raise RuntimeError(f"rank {r}: particles or links missing after the redistribution")
+            np_["owners"] = np.ascontiguousarray(new.owner[gp].astype(np.int32))
+            out.append((np_, nl))
+        self.layout = new
+        self._install(out)
 
     def gather(self) -> tuple[dict, dict]:
         """The whole set's particles and links (every process gets them)."""
@@ -368,8 +462,7 @@ class SlabRun:
                  for lib, x0 in zip(self.libs, self._x0)]
         delta = float(self.comm.allmax(moved)[0])
         if 2.0 * delta > self._width - self._reach:
-            particles, links = self.gather()
-            self._distribute(particles, links)
+            self._redistribute()
         else:
             self.kept += 1
         bounds = [lib.local_bounds() for lib in self.libs]

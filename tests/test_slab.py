@@ -234,3 +234,24 @@ def test_driver_on_two_gloo_ranks_moves_every_halo_force():
     assert [r[0] for r in res] == [0, 1]
     assert all(r[1] is True for r in res), res
     assert all(r[2] > 0 and r[3] > 0 for r in res)
+
+
+@pytest.mark.parametrize("nranks", [2, 3, 4])
+def test_incremental_redistribution_equals_the_whole_set_split(nranks):
+    """After a redistribution (every particle moved past the halo's room) each rank holds
+    exactly what splitting the gathered whole set by the new layout gives, array for array,
+    although it received only the particles and links it did not hold before."""
+    P, p, l = _block()
+    fakes = [FakeRank(r) for r in range(nranks)]
+    run = slab.SlabRun(slab.LocalComm(nranks), fakes, p, l, halo=1.3)
+    run.step(5)  # redistributes at step 4
+    assert run.redistributions == 2
+    whole_p, whole_l = run.gather()
+    for r, f in enumerate(fakes):
+        ep, el = slab.split_state(whole_p, whole_l, run.layout, r)
+        for k, v in ep.items():
+            assert np.array_equal(f.p[k], v), (r, k)
+        for k, v in el.items():
+            assert np.array_equal(f.l[k], v), (r, k)
+        assert np.array_equal(f.snd, run.layout.send_list(r))
+        assert np.array_equal(f.rcv, run.layout.recv_list(r))
