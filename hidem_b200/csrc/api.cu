@@ -31,6 +31,28 @@ struct NvtxRange {
     NvtxRange(const NvtxRange &) = delete;
     NvtxRange &operator=(const NvtxRange &) = delete;
 };
+
+// Host-side work over large arrays (the per-particle fields kept on the host) split over a
+// few threads, so that it keeps pace with the host-device copies it overlaps.
+template <class F>
+void host_parallel(long long n, F body) {
+    const long long chunk = 1ll << 20;
+    const int threads = (int)std::min<long long>(8, (n + chunk - 1) / chunk);
+    if (threads <= 1) {
+        body(0ll, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([=] { body(n * t / threads, n * (t + 1) / threads); });
+    for (auto &th : pool) th.join();
+}
+
+inline void host_copy(void *dst, const void *src, size_t bytes) {
+    host_parallel((long long)bytes, [=](long long a, long long b) {
+        std::memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, (size_t)(b - a));
+    });
+}
 // per-thread text of the last failure of a call that has no context
 thread_local std::string g_nocontext_error;
 }  // namespace hidem
@@ -1600,9 +1622,9 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     CK(cudaMemsetAsync(ctx->counts, 0, 4 * (size_t)n, ctx->stream));
     CK(cudaMemsetAsync(ctx->force, 0, 6 * lp * (size_t)n, ctx->stream));
     ctx->owners.assign((size_t)n, 0);
-    if (p->owners) std::memcpy(ctx->owners.data(), p->owners, 4 * (size_t)n);
+    if (p->owners) host_copy(ctx->owners.data(), p->owners, 4 * (size_t)n);
     ctx->keys.resize((size_t)n);
-    if (p->globalKeys) std::memcpy(ctx->keys.data(), p->globalKeys, 8 * (size_t)n);
+    if (p->globalKeys) host_copy(ctx->keys.data(), p->globalKeys, 8 * (size_t)n);
     else for (int64_t i = 0; i < n; ++i) ctx->keys[i] = i;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
@@ -1634,7 +1656,15 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     // on the device when the keys are 0..n-1 in order, else through a sorted key table on
     // the host
     bool identity = true;
-    for (long long i = 0; i < n && identity; ++i) identity = ctx->keys[i] == i;
+    {
+        std::atomic<bool> all(true);
+        const int64_t *k = ctx->keys.data();
+        host_parallel(n, [&all, k](long long a, long long b) {
+            for (long long i = a; i < b && all.load(std::memory_order_relaxed); ++i)
+                if (k[i] != i) all.store(false, std::memory_order_relaxed);
+        });
+        identity = all.load();
+    }
     cudaStream_t st = ctx->stream;
     TRY(dalloc(ctx, &ctx->linkA, L));
     TRY(dalloc(ctx, &ctx->linkB, L));
@@ -2043,8 +2073,8 @@ hidem_status hidem_get_particles(hidem_ctx *ctx, hidem_particle_soa *out) {
         CK(cudaMemcpyAsync(out->type, tstage, (size_t)n, cudaMemcpyDeviceToHost, st));
     }
     // the host-held fields while the copies run
-    if (out->owners) std::memcpy(out->owners, ctx->owners.data(), 4 * (size_t)n);
-    if (out->globalKeys) std::memcpy(out->globalKeys, ctx->keys.data(), 8 * (size_t)n);
+    if (out->owners) host_copy(out->owners, ctx->owners.data(), 4 * (size_t)n);
+    if (out->globalKeys) host_copy(out->globalKeys, ctx->keys.data(), 8 * (size_t)n);
     CK(cudaStreamSynchronize(st));
     return HIDEM_OK;
 }
