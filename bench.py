@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["slab", "block", "ensemble", "settle", "topo", "mesh", "ranks",
-                                           "meshblock"], default="slab")
+                                           "meshblock", "surrogate"], default="slab")
+    ap.add_argument("--surrogate-batch", type=int, default=65536, help="surrogate: rows per Adam step")
     ap.add_argument("--config", default=None,
                     help="meshblock: the reference's run config (default data/meshblock_5700k/config_mesh_5700k.toml)")
     ap.add_argument("--particle-file", default=None,
@@ -610,6 +611,79 @@ def main_settle(args):
                               "device_seconds": dev, "device_tflops": flops / dev / 1e12,
                               "device_frac_of_bf16_peak": flops / dev / 1e12 / peak,
                               "device_includes": "features and the fused network (k_mlp_fwd), inputs in device memory"},
+    }
+    print(json.dumps(line))
+
+
+def main_surrogate(args):
+    """The learned warm start's network alone, at the settle experiment's shape (82 lattice
+    inputs, 4 Fourier bands -> 768 features, 4 x 256 SiLU, 3 outputs): Adam training steps
+    of --surrogate-batch rows (features, the fused forward pass that keeps activations, the
+    backward GEMMs k_umma_gemm, the CUDA-core reductions and Adam) and the forward pass alone
+    on 2M device-resident rows; tensor-core FLOP/s against the measured BF16 peak."""
+    import torch
+    from hidem_b200 import settle
+    from hidem_b200 import surrogate as sg
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    nin = settle.N_LATTICE_INPUTS
+    batch = args.surrogate_batch
+    cfg = sg.default_config(inputs=nin, fourier_bands=4, batch=batch)
+    k0 = sg.feature_width(nin, cfg.fourier_bands)
+    W, Lh = cfg.width, cfg.hidden_layers
+    rng = np.random.default_rng(0)
+    rows = max(4 * batch, 1 << 18)
+    x = rng.uniform(-1, 1, (rows, nin)).astype(np.float32)
+    y = rng.normal(0, 0.1, (rows, 3)).astype(np.float32)
+    fwd_flops = 2.0 * (k0 * W + (Lh - 1) * W * W + 3 * W)
+    # backward: data gradients of layers 1.. and weight gradients of every layer
+    bwd_flops = 2.0 * ((Lh - 1) * W * W + 3 * W) + 2.0 * (k0 * W + (Lh - 1) * W * W + 3 * W)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    with sg.Surrogate(cfg) as net:
+        net.set_data(x, y)
+        net.train(max(args.warmup, 3))
+        stream = torch.cuda.ExternalStream(net.stream_handle)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        loss = net.train(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        train_s = e0.elapsed_time(e1) / 1e3
+        n_fwd = 1 << 21
+        u = rng.uniform(-1, 1, (n_fwd, nin)).astype(np.float32)
+        du = torch.from_numpy(u).cuda()
+        dy = torch.empty((n_fwd, 3), dtype=torch.float32, device="cuda")
+        net.predict_device(du.data_ptr(), n_fwd, dy.data_ptr())
+        best = float("inf")
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(stream)
+            net.predict_device(du.data_ptr(), n_fwd, dy.data_ptr())
+            b.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b) / 1e3)
+    step_flops = batch * (fwd_flops + bwd_flops)
+    value = step_flops * args.steps / train_s / 1e12
+    line = {
+        "metric": "surrogate training TFLOP/s (BF16 tensor cores, FP32 accumulation)", "value": value,
+        "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": 1e3 * train_s / args.steps, "higher_is_better": True, "scaling": "none",
+        "vs_baseline": None, "dtype": "bf16 (f32 accumulate)", "data": "synthetic",
+        "config": {"workload": f"surrogate {nin} inputs -> {k0} Fourier features -> {Lh} x {W} SiLU -> 3, "
+                               f"Adam steps of {batch} rows", "rows": rows, "batch": batch},
+        "frac_of_bf16_peak": value / peak, "final_loss": loss,
+        "forward": {"rows": n_fwd, "seconds": best, "tflops": n_fwd * fwd_flops / best / 1e12,
+                    "frac_of_bf16_peak": n_fwd * fwd_flops / best / 1e12 / peak,
+                    "includes": "features and the fused network (k_mlp_fwd), inputs in device memory"},
+        "roofline": {"bound": "tensor", "achieved": value, "peak": peak, "unit": "TFLOP/s",
+                     "frac": value / peak, "traffic": None,
+                     "peak_source": "measured" if peaks else "fallback",
+                     "kernel": "training step (k_mlp_fwd, k_umma_gemm, CUDA-core kernels)"},
     }
     print(json.dumps(line))
 
@@ -1381,6 +1455,13 @@ def main_meshblock(args):
 
 def main():
     args = parse()
+    if args.workload == "surrogate":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no learned warm start"}))
+        else:
+            main_surrogate(args)
+        return
     if args.workload == "meshblock":
         if args.impl == "reference":
             run_reference_meshblock(args)
