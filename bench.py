@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--settle-check", type=int, default=20, help="settle: steps between kinetic-energy reads")
     ap.add_argument("--max-train-rows", type=int, default=None,
                     help="settle: seeded sample of at most this many training rows")
+    ap.add_argument("--lattice-offsets", default="1.5,3,6",
+                    help="settle: distances (m) at which the surrogate's inputs sample the heightfields")
     ap.add_argument("--blocks", type=int, default=256, help="ensemble: number of blocks")
     ap.add_argument("--no-graphs", action="store_true", help="ensemble: plain launches")
     ap.add_argument("--kernel", choices=["auto", "items", "thread", "thread-capped", "thread-async", "two-pass"],
@@ -559,10 +561,11 @@ def main_settle(args):
     rep = settle.warm_start_experiment(n_train=args.train_tongues, n_test=args.test_tongues, size=size,
                                        base_thickness=thick, amplitude=amp, train_steps=args.train_steps,
                                        inputs=args.surrogate_inputs, max_steps=args.settle_max_steps,
-                                       max_train_rows=args.max_train_rows, check=args.settle_check)
+                                       max_train_rows=args.max_train_rows, check=args.settle_check,
+                                       offsets=tuple(float(v) for v in args.lattice_offsets.split(",")))
     # tensor-core forward throughput of the trained network's shape on 2M rows
     lattice = args.surrogate_inputs == "lattice"
-    nin = settle.N_LATTICE_INPUTS if lattice else 5
+    nin = settle.n_lattice_inputs(tuple(float(v) for v in args.lattice_offsets.split(","))) if lattice else 5
     cfg = sg.default_config(inputs=nin, fourier_bands=4 if lattice else 6)
     k0 = sg.feature_width(nin, cfg.fourier_bands)
     rows = 1 << 21

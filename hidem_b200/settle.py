@@ -121,14 +121,18 @@ LATTICE_COLUMNS = tuple((i, j) for i in range(-2, 3) for j in range(-2, 3) if (i
 N_LATTICE_INPUTS = 5 + 8 * len(LATTICE_OFFSETS) + 5 + 2 * len(LATTICE_COLUMNS)
 
 
-def lattice_inputs(t: Tongue, mirror: tuple[int, int] = (1, 1)) -> np.ndarray:
+def n_lattice_inputs(offsets=LATTICE_OFFSETS) -> int:
+    return 5 + 8 * len(offsets) + 5 + 2 * len(LATTICE_COLUMNS)
+
+
+def lattice_inputs(t: Tongue, mirror: tuple[int, int] = (1, 1), offsets=LATTICE_OFFSETS) -> np.ndarray:
     """The surrogate's lattice-neighbourhood inputs of every particle (N_LATTICE_INPUTS
     columns), optionally of the tongue's mirror image (x -> Lx - x for mirror[0] = -1,
     y -> Ly - y for mirror[1] = -1, the particles keeping their order):
 
     * the 5 coordinate inputs of surrogate_inputs;
     * ice thickness (0 outside the plan) and bed height at x +- d and y +- d for each d of
-      LATTICE_OFFSETS (d-major, then the axis, then +d before -d);
+      `offsets` (LATTICE_OFFSETS by default; d-major, then the axis, then +d before -d);
     * the particle's lattice column (particles sharing x and y): its bond count, the
       particles above it, the free particles below it, and its height below the column's
       top and above the column's lowest free particle;
@@ -151,7 +155,7 @@ def lattice_inputs(t: Tongue, mirror: tuple[int, int] = (1, 1)) -> np.ndarray:
 
     cols = [2 * x / t.size[0] - 1, 2 * y / t.size[1] - 1, 2 * (z - t.bed) / t.thick - 1,
             t.thick / THICK_SCALE - 1, t.bed / BED_SCALE]
-    for d in LATTICE_OFFSETS:
+    for d in offsets:
         for ax in (0, 1):
             for sgn in (1, -1):
                 th, bd = geo(x + sgn * d, y) if ax == 0 else geo(x, y + sgn * d)
@@ -195,7 +199,7 @@ def lattice_inputs(t: Tongue, mirror: tuple[int, int] = (1, 1)) -> np.ndarray:
         cols.append(np.where(ex, (top[q] - z) / 5.0, -2.0))
         cols.append(np.where(ex, (low_or_top[q] - z) / 5.0, -2.0))
     out = np.stack(cols, axis=1).astype(np.float32)
-    assert out.shape[1] == N_LATTICE_INPUTS
+    assert out.shape[1] == n_lattice_inputs(offsets)
     return out
 
 
@@ -379,14 +383,16 @@ def warm_start_experiment(n_train: int = 256, n_test: int = 16, size=(40.0, 12.0
                           train_steps: int = 20000, batch: int = 8192, seed: int = 1000,
                           tol: float = 1e-6, max_steps: int = 40000, surrogate_cfg: dict | None = None,
                           with_rotation: bool = True, mirror: bool = True, inputs: str = "lattice",
-                          max_train_rows: int | None = None, check: int = 20):
+                          max_train_rows: int | None = None, check: int = 20,
+                          offsets=LATTICE_OFFSETS):
     """Cold settles of the training tongues, surrogate training on their settled
     displacements, then cold and warm settles of held-out tongues, compared by the plain
     method's convergence test. inputs: "lattice" (lattice_inputs, 4 Fourier bands, the
     learning rate decayed along a half cosine) or "coords" (the 5 coordinate inputs of
     surrogate_inputs, 6 bands, constant rate). max_train_rows: a seeded uniform sample of
     at most that many training rows (large tongues); check: steps between the kinetic-energy
-    reads of the settles."""
+    reads of the settles; offsets: the distances at which lattice_inputs samples the
+    heightfields (longer ones for larger tongues)."""
     import time
     from . import surrogate as sg
     sec = {}
@@ -402,7 +408,7 @@ def warm_start_experiment(n_train: int = 256, n_test: int = 16, size=(40.0, 12.0
 
     def feats(t, m=(1, 1)):
         if inputs == "lattice":
-            return lattice_inputs(t, m)
+            return lattice_inputs(t, m, offsets)
         return surrogate_inputs(t) * np.array([m[0], m[1], 1, 1, 1], np.float32)
 
     t0 = time.time()
