@@ -287,14 +287,22 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             __syncwarp();
             const int col = c0 + lane;
             const float bias = g.bias ? g.bias[col] : 0.f;
+            if (EPI == EPI_F32) {
 #pragma unroll 4
-            for (int r = 0; r < 32; ++r) {
-                const float acc = stage[r * 33 + lane];
-                const long long o = (long long)(rowBase + r) * g.ldo + col;
-                if (EPI == EPI_F32) {
-                    g.outF[blockIdx.y * g.splitStride + o] = acc + bias;
-                } else {
-                    g.outH[o] = __float2bfloat16_rn(acc * silu_grad(g.zIn[o]));
+                for (int r = 0; r < 32; ++r) {
+                    const long long o = (long long)(rowBase + r) * g.ldo + col;
+                    g.outF[blockIdx.y * g.splitStride + o] = stage[r * 33 + lane] + bias;
+                }
+            } else {
+                // the 32 rows' pre-activations all in flight at once: each load is a
+                // coalesced 128-byte row segment, and the warp's latency is paid once
+                float z[32];
+#pragma unroll
+                for (int r = 0; r < 32; ++r) z[r] = __ldg(g.zIn + (long long)(rowBase + r) * g.ldo + col);
+#pragma unroll
+                for (int r = 0; r < 32; ++r) {
+                    const long long o = (long long)(rowBase + r) * g.ldo + col;
+                    g.outH[o] = __float2bfloat16_rn(stage[r * 33 + lane] * silu_grad(z[r]));
                 }
             }
             __syncwarp();
