@@ -265,6 +265,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             for (int j = i; j < issued; ++j) mb_wait(full + (j % S), (uint32_t)((j / S) & 1));
         }
     }
+    // the producer's own warp waits for it here rather than polling the accumulator
+    // barrier beside it: polling lanes of a diverged warp delay the lane that issues
+    if (warp == 0) __syncwarp();
     const bool accReady = mb_wait(done, 0);
     tc_fence_after();
     __syncthreads();
