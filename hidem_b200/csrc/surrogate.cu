@@ -179,10 +179,15 @@ constexpr size_t gemm_smem_bytes() {
 // [kTiles * blockIdx.y, +kTiles). Thread 0 streams A / B tiles with TMA and issues the
 // MMAs (4 of K = 16 per 64-wide tile); the eight warps then read the accumulator (warp w:
 // lanes / rows 32 (w % 4) .. +31, column half w / 4) and apply the epilogue.
+// EPI_SILU_GRAD: the CTA's 128 x BN pre-activation tile comes into shared memory by TMA
+// (FP32 boxes of 64 columns x 128 rows, no swizzle) once the MMAs have released the
+// pipeline stages, behind the eight warps' transpose buffers
+constexpr uint32_t kZOff = 36864;
+
 template <int BN, int EPI>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_umma_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
-                const GemmArgs g) {
+                const __grid_constant__ CUtensorMap tz, const GemmArgs g) {
     constexpr int S = kGemmStages;
     constexpr uint32_t ABYTES = 128 * 128, BBYTES = BN * 128, STAGE = ABYTES + BBYTES;
     constexpr uint32_t COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
@@ -192,7 +197,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     uint64_t *full = reinterpret_cast<uint64_t *>(sm + S * STAGE);
     uint64_t *empty = full + S;
     uint64_t *done = empty + S;
-    uint32_t *slot = reinterpret_cast<uint32_t *>(done + 1);
+    uint64_t *zbar = done + 1;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(zbar + 1);
+    static_assert(kZOff + 128u * BN * 4u <= (uint32_t)S * STAGE, "pre-activation tile exceeds the stages");
     __shared__ int sFail;
     const int tid = threadIdx.x, warp = tid >> 5;
 
@@ -202,6 +209,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             mb_init(empty + s, 1);
         }
         mb_init(done, 1);
+        mb_init(zbar, 1);
         sFail = 0;
         mb_fence_init();
     }
@@ -271,7 +279,20 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const bool accReady = mb_wait(done, 0);
     tc_fence_after();
     __syncthreads();
-    if (accReady && !sFail) {
+    // the MMAs have completed: their stages take the pre-activation tile
+    bool zReady = true, zIssued = false;
+    if (EPI == EPI_SILU_GRAD && accReady && !sFail) {
+        zIssued = true;
+        if (tid == 0) {
+            mb_expect_tx(zbar, 128u * BN * 4u);
+#pragma unroll
+            for (int c = 0; c < BN / 64; ++c)
+                tma_load_2d(sm + kZOff + c * (128 * 64 * 4), &tz, c * 64, m0, zbar);
+        }
+        zReady = mb_wait(zbar, 0);
+        if (!zReady && tid == 0) set_err(g.err, 3);
+    }
+    if (accReady && !sFail && zReady) {
         // The accumulator lane of a thread is one row; stores are made coalesced by
         // passing each 32 x 32 block through shared memory (the pipeline stages are free
         // now): lane j then writes column c0 + j of 32 consecutive rows.
@@ -299,13 +320,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             } else {
                 // the 32 rows' pre-activations all in flight at once: each load is a
                 // coalesced 128-byte row segment, and the warp's latency is paid once
-                float z[32];
-#pragma unroll
-                for (int r = 0; r < 32; ++r) z[r] = __ldg(g.zIn + (long long)(rowBase + r) * g.ldo + col);
-#pragma unroll
+                const float *zt = reinterpret_cast<const float *>(sm + kZOff + (col >> 6) * (128 * 64 * 4)) +
+                                  quarter * 32 * 64 + (col & 63);
+#pragma unroll 4
                 for (int r = 0; r < 32; ++r) {
                     const long long o = (long long)(rowBase + r) * g.ldo + col;
-                    g.outH[o] = __float2bfloat16_rn(stage[r * 33 + lane] * silu_grad(z[r]));
+                    g.outH[o] = __float2bfloat16_rn(stage[r * 33 + lane] * silu_grad(zt[r * 64]));
                 }
             }
             __syncwarp();
@@ -313,6 +333,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     } else if (tid == 0 && !accReady) {
         set_err(g.err, 2);
     }
+    // a pre-activation copy that did not complete in time still lands in this CTA's
+    // shared memory: a second bounded wait before the CTA exits
+    if (zIssued && !zReady && tid == 0) mb_wait(zbar, 0);
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tm_dealloc(tmem, COLS);
@@ -794,6 +817,19 @@ bool make_map(CUtensorMap *m, const void *base, long long rows, long long cols, 
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// FP32 [rows][cols] row-major, boxes of 64 columns x boxRows rows, no swizzle
+bool make_map_f32(CUtensorMap *m, const void *base, long long rows, long long cols, int boxRows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * sizeof(float)};
+    cuuint32_t box[2] = {64u, (cuuint32_t)boxRows};
+    cuuint32_t es[2] = {1u, 1u};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 hidem_status sfail(hidem_surrogate *s, hidem_status st, const char *fmt, ...) {
     char buf[512];
     va_list ap;
@@ -832,15 +868,21 @@ hidem_status gemm(hidem_surrogate *s, const bf16 *A, int M, int K, const bf16 *B
     }
     if (M % 128 || K % 64 || (K / 64) % splits)
         return sfail(s, HIDEM_ERR_ARG, "GEMM shape %d x %d x %d (splits %d) is not tile-aligned", M, BN, K, splits);
-    CUtensorMap ta, tb;
+    CUtensorMap ta, tb, tz;
     if (!make_map(&ta, A, M, K, 128) || !make_map(&tb, Bm, BN, K, BN))
         return sfail(s, HIDEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    if (EPI == EPI_SILU_GRAD) {
+        if (g.ldo != BN || !make_map_f32(&tz, g.zIn, M, BN, 128))
+            return sfail(s, HIDEM_ERR_CUDA, "cuTensorMapEncodeTiled failed (pre-activations)");
+    } else {
+        tz = ta;  // not read
+    }
     g.M = M;
     g.N = BN;
     g.K = K;
     g.kTiles = K / 64 / splits;
     g.err = s->dErr;
-    k_umma_gemm<BN, EPI><<<dim3(M / 128, splits), kGemmThreads, gemm_smem_bytes<BN>(), s->stream>>>(ta, tb, g);
+    k_umma_gemm<BN, EPI><<<dim3(M / 128, splits), kGemmThreads, gemm_smem_bytes<BN>(), s->stream>>>(ta, tb, tz, g);
     SCK(cudaGetLastError());
     return HIDEM_OK;
 }
@@ -992,8 +1034,9 @@ hidem_status check_err(hidem_surrogate *s) {
     if (flag) {
         SCK(cudaMemsetAsync(s->dErr, 0, sizeof(int), s->stream));
         return sfail(s, HIDEM_ERR_DEVICE, "tensor-core GEMM: %s",
-                     flag == 1 ? "tile copies did not complete in time"
-                               : "accumulator did not complete in time");
+                     flag == 1   ? "tile copies did not complete in time"
+                     : flag == 2 ? "accumulator did not complete in time"
+                                 : "pre-activation copies did not complete in time");
     }
     return HIDEM_OK;
 }
