@@ -134,6 +134,18 @@ public:
     void setChecks(int32_t flags) { check(hidem_set_checks(ctx_, flags)); }
     int32_t stepKernel() { return hidem_get_step_kernel(ctx_); }
 
+    // the context's device arrays, for hidem_b200_iterate.cuh (take it again after a
+    // call that rebuilds or steps)
+    hidem_device_view deviceView() {
+        hidem_device_view v;
+        check(hidem_get_device_view(ctx_, &v));
+        return v;
+    }
+    // computePartForce with the halo send records written by the force pass (slab ranks)
+    void computePartForcePacked(void *deviceSendBuffer) {
+        check(hidem_compute_forces_packed(ctx_, deviceSendBuffer));
+    }
+
 private:
     void check(hidem_status s) {
         if (s != HIDEM_OK) throw Error(s, hidem_last_error(ctx_));
