@@ -32,6 +32,9 @@ STEP_KERNEL_THREAD = 2
 STEP_KERNEL_THREAD_CAPPED = 3
 STEP_KERNEL_THREAD_ASYNC = 4
 STEP_KERNEL_TWO_PASS = 5
+SURROGATE_FORWARD_AUTO = 0
+SURROGATE_FORWARD_BLOCK = 1
+SURROGATE_FORWARD_PINGPONG = 2
 
 _d = C.c_double
 _i32 = C.c_int32
@@ -303,6 +306,7 @@ _PROTOS = [
     ("hidem_surrogate_config_default", None, [C.POINTER(HidemSurrogateConfig)]),
     ("hidem_surrogate_predict_device", C.c_int, [C.c_void_p, C.c_void_p, _i64, C.c_void_p]),
     ("hidem_surrogate_get_stream", C.c_void_p, [C.c_void_p]),
+    ("hidem_surrogate_set_forward", C.c_int, [C.c_void_p, _i32]),
     ("hidem_surrogate_create", C.c_int, [C.POINTER(HidemSurrogateConfig), C.c_int,
                                          C.POINTER(C.c_void_p)]),
     ("hidem_surrogate_destroy", None, [C.c_void_p]),

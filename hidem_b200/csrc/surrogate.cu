@@ -126,6 +126,24 @@ __device__ __forceinline__ void tm_ld16(uint32_t taddr, float *v) {
     for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// 32 consecutive FP32 columns of this thread's tensor-memory lane, one load and one wait
+__device__ __forceinline__ void tm_ld32(uint32_t taddr, float *v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+        "%30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
 // Shared-memory matrix descriptor of a K-major tile written by TMA with the 128-byte
 // swizzle: rows of 64 BF16 (128 B), 8-row atoms 1024 B apart (stride byte offset),
 // descriptor version 1, layout type 2 (128-byte swizzle). Moving 16 elements along K
@@ -565,6 +583,332 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
     if (warp == 0) tm_dealloc(tmem, COLS);
 }
 
+// ------------------------------------------------------------------ persistent ping-pong forward pass
+
+constexpr int kPPStages = 3;
+constexpr int kPPEpiWarps = 16;
+constexpr int kPPThreads = 32 * (2 + kPPEpiWarps);  // warp 0: copies, warp 1: MMAs, 2-17: epilogues
+
+// both blocks' activation tiles (128 x 256 BF16), the weight ring, barriers and alignment
+constexpr size_t pp_smem_bytes() {
+    return (size_t)2 * 128 * 256 * 2 + (size_t)kPPStages * 256 * 128 + 1024 + 256;
+}
+
+__device__ __forceinline__ void mb_arrive(uint64_t *b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+// a bounded wait that also gives up once another role of the CTA has recorded a failure
+__device__ __forceinline__ bool mb_wait_or_fail(uint64_t *b, uint32_t parity, const volatile int *fail) {
+    for (int i = 0; i < kSpins; ++i) {
+        if (mb_try(b, parity)) return true;
+        if ((i & 255) == 255 && *fail) return false;
+    }
+    return false;
+}
+
+// One epilogue thread's share of a unit of k_mlp_pp: its row's 64 columns starting at
+// c0s, 32 at a time, from tensor memory (taddr: the row's lane, the block's accumulator):
+// bias + SiLU -> BF16. KEEP (training): pre-activations and activations to global memory.
+// LAST: the output layer's partial sums over these columns, in k order, into o; otherwise
+// the activations into the next layer's swizzled K-major A tile. The two flags are template
+// parameters so that neither path costs the other instructions.
+template <int BN, bool LAST, bool KEEP>
+__device__ __forceinline__ void pp_epilogue(uint32_t taddr, int c0s, int row, long long grow, bool live,
+                                            const float *__restrict__ bias, float *zo, bf16 *ho,
+                                            const float *__restrict__ wo, unsigned char *ab, float *o) {
+    constexpr uint32_t ACT_BLOCK = 128 * 128;
+#pragma unroll 1
+    for (int c0 = c0s; c0 < c0s + BN / 4; c0 += 16) {
+        float v[16];
+        tm_ld16(taddr + (uint32_t)c0, v);
+        uint32_t hp[8];
+        const float4 *b4 = reinterpret_cast<const float4 *>(bias + c0);
+#pragma unroll
+        for (int j = 0; j < 16; j += 4) {
+            const float4 bb = __ldg(b4 + (j >> 2));
+            const float z0 = v[j] + bb.x, z1 = v[j + 1] + bb.y, z2 = v[j + 2] + bb.z, z3 = v[j + 3] + bb.w;
+            if (KEEP && live)
+                reinterpret_cast<float4 *>(zo + grow * BN + c0)[j >> 2] = make_float4(z0, z1, z2, z3);
+            const __nv_bfloat162 h01 = __floats2bfloat162_rn(silu_fast(z0), silu_fast(z1));
+            const __nv_bfloat162 h23 = __floats2bfloat162_rn(silu_fast(z2), silu_fast(z3));
+            hp[j >> 1] = *reinterpret_cast<const uint32_t *>(&h01);
+            hp[(j >> 1) + 1] = *reinterpret_cast<const uint32_t *>(&h23);
+            if (LAST) {
+                const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+#pragma unroll
+                for (int jj = 0; jj < kOutCols; ++jj) {
+                    const float4 w = __ldg(reinterpret_cast<const float4 *>(wo + jj * BN + c0 + j));
+                    o[jj] += f01.x * w.x;
+                    o[jj] += f01.y * w.y;
+                    o[jj] += f23.x * w.z;
+                    o[jj] += f23.y * w.w;
+                }
+            }
+        }
+        if (KEEP && live) {
+            uint4 *hq = reinterpret_cast<uint4 *>(ho + grow * BN + c0);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) hq[u] = make_uint4(hp[4 * u], hp[4 * u + 1], hp[4 * u + 2], hp[4 * u + 3]);
+        }
+        if (!LAST) {
+            // 16-byte chunks of 8 columns into the swizzled K-major tile
+            const int kb = c0 >> 6;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int ch = ((c0 & 63) >> 3) + u;
+                uint4 *dst = reinterpret_cast<uint4 *>(ab + kb * ACT_BLOCK + row * 128 + ((ch ^ (row & 7)) << 4));
+                *dst = make_uint4(hp[4 * u], hp[4 * u + 1], hp[4 * u + 2], hp[4 * u + 3]);
+            }
+        }
+    }
+}
+
+// The forward pass of a 256-wide network as a persistent kernel. Each CTA takes pairs of
+// 128-row blocks and runs the two blocks through the layers in ping-pong, so that one
+// block's epilogue (tensor memory -> bias + SiLU -> BF16 activations in shared memory)
+// runs while the tensor cores compute the other block's layer. Tensor memory holds both
+// blocks' accumulators (2 x 256 FP32 columns); shared memory holds both blocks'
+// activation tiles (128 x 256 BF16, 128-byte-swizzled K-major: the next layer's A
+// operand) and a 3-stage ring of weight k-tiles (256 x 64 BF16). The first layer's A
+// operand, the block's feature tile 64 columns at a time, comes by TMA straight into the
+// block's activation tile, cycling through its four 64-column slots. Roles:
+//   warp 0 (one lane)  the TMA copies;
+//   warp 1 (one lane)  tcgen05.mma and the commits;
+//   warps 2-17         the epilogues: warp w reads accumulator lanes 32 (w % 4) .. +31
+//                      (its rows) and the 64 columns 64 ((w - 2) / 4) .. +63.
+// Unit (l, b) is layer l of block b, in the order (0, 0), (0, 1), (1, 0), ... of each pair.
+// Its MMAs wait until the block's previous epilogue has released the accumulator and the
+// activation tile (accFree[b]); its epilogue waits for its MMAs (accFull[b]). The 3-wide
+// output layer runs in the last layer's epilogue: each warp sums its 64 columns in k order
+// per row, and the four partial sums of a row are added in column order. The hidden layers'
+// arithmetic is that of k_mlp_fwd (same MMAs in the same order, same epilogue).
+template <int BN>
+__global__ void __launch_bounds__(kPPThreads, 1)
+    k_mlp_pp(const __grid_constant__ MlpMaps maps, const MlpArgs g, int rows) {
+    static_assert(BN == 256, "the ping-pong forward pass is built for 256-wide layers");
+    constexpr int S = kPPStages;
+    constexpr uint32_t ACT_BLOCK = 128 * 128;  // 128 rows x 64 BF16 columns
+    constexpr uint32_t ACT = 128 * BN * 2;     // one block's activation tile
+    constexpr uint32_t BBYTES = BN * 128;      // one 64-wide weight k-tile
+    constexpr int NA = BN / 64;                // feature slots of an activation tile
+    // a feature slot is reused NA loads later; the copy into it starts only after the
+    // producer has seen the MMAs of the load S earlier complete
+    static_assert(NA >= S, "feature slots must not be reused before their MMAs complete");
+    constexpr uint32_t EPI = 32 * kPPEpiWarps;
+    extern __shared__ unsigned char dyn[];
+    unsigned char *sm =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
+    unsigned char *act = sm;
+    unsigned char *ring = sm + 2 * ACT;
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + S * BBYTES);
+    uint64_t *empty = full + S;
+    uint64_t *accFull = empty + S;
+    uint64_t *accFree = accFull + 2;
+    uint64_t *outBar = accFree + 2;
+    uint64_t *fin = outBar + 2;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(fin + 1);
+    __shared__ int sFail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int L = g.layers;
+    const int nk0 = g.k0 / 64, nkw = BN / 64;
+    const int nPairs = (rows / 128 + 1) / 2;
+
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mb_init(full + s, 1);
+            mb_init(empty + s, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mb_init(accFull + b, 1);
+            mb_init(accFree + b, EPI);
+            mb_init(outBar + b, EPI);
+        }
+        mb_init(fin, 1);
+        sFail = 0;
+        mb_fence_init();
+    }
+    if (warp == 0) {
+        tm_alloc(slot, 2 * BN);
+        tm_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    volatile int *fail = &sFail;
+
+    if (warp == 0 && lane == 0) {
+        // ---- copies: k counts the loads, n[b] the units of block b
+        uint32_t k = 0, n[2] = {0, 0};
+        bool ok = true;
+        for (int p = blockIdx.x; ok && p < nPairs; p += gridDim.x) {
+            for (int l = 0; ok && l < L; ++l) {
+                for (int b = 0; ok && b < 2; ++b) {
+                    const int m0 = (2 * p + b) * 128;
+                    unsigned char *ab = act + b * ACT;
+                    // the feature tiles overwrite the block's activation tile: wait for the
+                    // epilogue of the block's previous unit to release it
+                    if (l == 0 && n[b] > 0 && !mb_wait_or_fail(accFree + b, (n[b] - 1) & 1, fail)) {
+                        ok = false;
+                        break;
+                    }
+                    const int nk = l == 0 ? nk0 : nkw;
+                    for (int kt = 0; kt < nk; ++kt) {
+                        const int s = (int)(k % S);
+                        const uint32_t r = k / S;
+                        if (r > 0 && !mb_wait_or_fail(empty + s, (r - 1) & 1, fail)) {
+                            ok = false;
+                            break;
+                        }
+                        unsigned char *bt = ring + s * BBYTES;
+                        if (l == 0) {
+                            mb_expect_tx(full + s, ACT_BLOCK + BBYTES);
+                            tma_load_2d(ab + (kt % NA) * ACT_BLOCK, &maps.x, kt * 64, m0, full + s);
+                            tma_load_2d(bt, &maps.w[0], kt * 64, 0, full + s);
+                        } else {
+                            mb_expect_tx(full + s, BBYTES);
+                            tma_load_2d(bt, &maps.w[l], kt * 64, 0, full + s);
+                        }
+                        ++k;
+                    }
+                    ++n[b];
+                }
+            }
+        }
+        if (!ok) {
+            *fail = 1;
+            set_err(g.err, 1);
+            // copies still in flight land in this CTA's shared memory: a bounded wait for the
+            // last S loads (each earlier one was consumed before its stage was reused)
+            for (uint32_t j = k > (uint32_t)S ? k - S : 0u; j < k; ++j) mb_wait(full + j % S, (j / S) & 1);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMAs: kind::f16, D FP32, A and B BF16 K-major, N = BN, M = 128
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(128 >> 4) << 24);
+        uint32_t k = 0, n[2] = {0, 0};
+        bool ok = true;
+        for (int p = blockIdx.x; ok && p < nPairs; p += gridDim.x) {
+            for (int l = 0; ok && l < L; ++l) {
+                for (int b = 0; ok && b < 2; ++b) {
+                    if (n[b] > 0 && !mb_wait_or_fail(accFree + b, (n[b] - 1) & 1, fail)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t d = tmem + (uint32_t)(b * BN);
+                    const unsigned char *ab = act + b * ACT;
+                    const int nk = l == 0 ? nk0 : nkw;
+                    for (int kt = 0; kt < nk; ++kt) {
+                        const int s = (int)(k % S);
+                        if (!mb_wait_or_fail(full + s, (k / S) & 1, fail)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t a0 = su32(ab + (l == 0 ? kt % NA : kt) * ACT_BLOCK);
+                        const uint32_t b0 = su32(ring + s * BBYTES);
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk)
+                            tc_mma(d, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), idesc,
+                                   (kt > 0 || kk > 0) ? 1u : 0u);
+                        tc_commit(empty + s);
+                        ++k;
+                    }
+                    if (!ok) break;
+                    tc_commit(accFull + b);
+                    ++n[b];
+                }
+            }
+        }
+        if (!ok) {
+            *fail = 1;
+            set_err(g.err, 1);
+        }
+        // every MMA issued has completed before the CTA releases tensor memory
+        tc_commit(fin);
+        mb_wait(fin, 0);
+    } else if (warp >= 2) {
+        // ---- epilogues
+        const int q = warp & 3, cg = (warp - 2) >> 2;
+        const int row = q * 32 + lane;
+        const uint32_t tl = (uint32_t)(q * 32) << 16;
+        uint32_t n[2] = {0, 0}, no[2] = {0, 0};
+        bool ok = true;
+        for (int p = blockIdx.x; ok && p < nPairs; p += gridDim.x) {
+            for (int l = 0; ok && l < L; ++l) {
+                for (int b = 0; ok && b < 2; ++b) {
+                    if (!mb_wait_or_fail(accFull + b, n[b] & 1, fail)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const long long grow = (long long)(2 * p + b) * 128 + row;
+                    const bool live = grow < rows;
+                    const bool last = l == L - 1;
+                    unsigned char *ab = act + b * ACT;
+                    const float *bias = g.bias[l];
+                    float *zo = g.z[l];
+                    bf16 *ho = g.h[l];
+                    float o[kOutCols] = {0.f, 0.f, 0.f};
+                    const uint32_t taddr = tmem + tl + (uint32_t)(b * BN);
+                    const int c0s = cg * (BN / 4);
+                    if (zo) {
+                        if (last)
+                            pp_epilogue<BN, true, true>(taddr, c0s, row, grow, live, bias, zo, ho, g.wo, ab, o);
+                        else
+                            pp_epilogue<BN, false, true>(taddr, c0s, row, grow, live, bias, zo, ho, g.wo, ab, o);
+                    } else {
+                        if (last)
+                            pp_epilogue<BN, true, false>(taddr, c0s, row, grow, live, bias, zo, ho, g.wo, ab, o);
+                        else
+                            pp_epilogue<BN, false, false>(taddr, c0s, row, grow, live, bias, zo, ho, g.wo, ab, o);
+                    }
+                    if (last) {
+                        // the layer's MMAs have completed, so the activation tile is free: it
+                        // carries the partial sums of column groups 1-3 to group 0's threads
+                        float4 *part = reinterpret_cast<float4 *>(ab);
+                        if (cg > 0) part[cg * 128 + row] = make_float4(o[0], o[1], o[2], 0.f);
+                        mb_arrive(outBar + b);
+                        if (cg == 0) {
+                            if (!mb_wait_or_fail(outBar + b, no[b] & 1, fail)) {
+                                ok = false;
+                            } else if (live) {
+#pragma unroll
+                                for (int c = 1; c < 4; ++c) {
+                                    const float4 pv = part[c * 128 + row];
+                                    o[0] += pv.x;
+                                    o[1] += pv.y;
+                                    o[2] += pv.z;
+                                }
+#pragma unroll
+                                for (int jj = 0; jj < kOutCols; ++jj) g.y[grow * kOutCols + jj] = o[jj] + g.bo[jj];
+                            }
+                        }
+                        ++no[b];
+                    }
+                    // the activation writes (and reads) before the tensor cores' and the
+                    // copies' next use of the tile, the accumulator reads before the next MMAs
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    tc_fence_before();
+                    mb_arrive(accFree + b);
+                    ++n[b];
+                }
+            }
+        }
+        if (!ok) {
+            *fail = 1;
+            set_err(g.err, 2);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tm_dealloc(tmem, 2 * BN);
+    }
+}
+
 }  // namespace
 
 namespace {
@@ -582,30 +926,31 @@ int feature_width(int nin, int bands) {
 
 // Fourier features of the rows idx[b] (or b when idx is null) of `in` [n][nin]:
 // u_i, then sin(2^f pi u_i), cos(2^f pi u_i) for f < bands (f-major), zero padding to K0.
-// One warp per row: the lanes take the row's inputs, then its (input, band) pairs, each
-// with one hardware sine / cosine pair (the features are rounded to BF16, far coarser than
-// the approximation), then the padding.
+// One warp per row: lane j takes inputs j, j + 32, ..., and for each of them its bands,
+// one hardware sine / cosine pair per band (the features are rounded to BF16, far coarser
+// than the approximation); for a fixed band the lanes' (sin, cos) pairs are consecutive
+// 4-byte words of the row. Then the padding.
 __global__ void k_features(const float *__restrict__ in, const int *__restrict__ idx, int rows,
                            int nin, int bands, int K0, bf16 *__restrict__ X) {
-    __shared__ float su[8][kMaxIn];
     const int b = blockIdx.x * blockDim.y + threadIdx.y;
     if (b >= rows) return;
     const int src = idx ? idx[b] : b;
-    float *u = su[threadIdx.y];
     bf16 *x = X + (long long)b * K0;
+    const bool pairs = (nin & 1) == 0;  // (sin, cos) pairs start on 4-byte boundaries
     for (int i = threadIdx.x; i < nin; i += blockDim.x) {
         const float v = in[(long long)src * nin + i];
-        u[i] = v;
         x[i] = __float2bfloat16_rn(v);
-    }
-    __syncwarp();
-    for (int p = threadIdx.x; p < nin * bands; p += blockDim.x) {
-        const int f = p / nin, i = p - f * nin;
-        float sv, cv;
-        __sincosf((float)(1 << f) * 3.14159265358979f * u[i], &sv, &cv);
-        const int c = nin + 2 * p;  // nin + 2 (nin f + i)
-        x[c] = __float2bfloat16_rn(sv);
-        x[c + 1] = __float2bfloat16_rn(cv);
+        for (int f = 0; f < bands; ++f) {
+            float sv, cv;
+            __sincosf((float)(1 << f) * 3.14159265358979f * v, &sv, &cv);
+            const int c = nin + 2 * (nin * f + i);
+            if (pairs) {
+                *reinterpret_cast<__nv_bfloat162 *>(x + c) = __floats2bfloat162_rn(sv, cv);
+            } else {
+                x[c] = __float2bfloat16_rn(sv);
+                x[c + 1] = __float2bfloat16_rn(cv);
+            }
+        }
     }
     for (int c = nin * (1 + 2 * bands) + threadIdx.x; c < K0; c += blockDim.x) x[c] = __float2bfloat16_rn(0.f);
 }
@@ -783,6 +1128,8 @@ struct hidem_surrogate {
     float *predIn = nullptr, *predY = nullptr;    // predict chunk: inputs [PB][nin], outputs [PB][3]
     bf16 *predX = nullptr;                        // predict chunk features [PB][K0]
     long long steps = 0;
+    int smCount = 0;                              // SMs of the device (persistent grids)
+    int forwardKind = HIDEM_SURROGATE_FORWARD_AUTO;
 };
 
 namespace {
@@ -948,7 +1295,46 @@ hidem_status mlp_forward_t(hidem_surrogate *s, const bf16 *X, int rows, float *Y
     return HIDEM_OK;
 }
 
+// The same pass as the persistent ping-pong kernel (k_mlp_pp, 256-wide networks): one CTA
+// per SM at most, each taking pairs of 128-row blocks.
+hidem_status mlp_forward_pp(hidem_surrogate *s, const bf16 *X, int rows, float *Y, bool keepZ) {
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured.load() & bit)) {
+        cudaFuncSetAttribute(k_mlp_pp<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pp_smem_bytes());
+        configured.fetch_or(bit);
+    }
+    if (rows % 128) return sfail(s, HIDEM_ERR_ARG, "forward rows %d not a multiple of 128", rows);
+    if (rows == 0) return HIDEM_OK;
+    MlpMaps maps;
+    std::memset(&maps, 0, sizeof maps);
+    if (!make_map(&maps.x, X, rows, s->K0, 128)) return sfail(s, HIDEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    MlpArgs a{};
+    a.layers = s->L;
+    a.k0 = s->K0;
+    for (int l = 0; l < s->L; ++l) {
+        if (!make_map(&maps.w[l], s->Wb[l], 256, s->Kl[l], 256))
+            return sfail(s, HIDEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+        a.bias[l] = s->P + s->offB[l];
+        a.z[l] = keepZ ? s->Z[l] : nullptr;
+        a.h[l] = keepZ ? s->H[l] : nullptr;
+    }
+    a.wo = s->P + s->offWo;
+    a.bo = s->P + s->offBo;
+    a.y = Y;
+    a.err = s->dErr;
+    const int pairs = (rows / 128 + 1) / 2;
+    const int grid = std::min(pairs, std::max(1, s->smCount));
+    k_mlp_pp<256><<<grid, kPPThreads, pp_smem_bytes(), s->stream>>>(maps, a, rows);
+    SCK(cudaGetLastError());
+    return HIDEM_OK;
+}
+
 hidem_status mlp_forward(hidem_surrogate *s, const bf16 *X, int rows, float *Y, bool keepZ) {
+    if (s->W == 256 && s->forwardKind != HIDEM_SURROGATE_FORWARD_BLOCK)
+        return mlp_forward_pp(s, X, rows, Y, keepZ);
     return s->W == 256 ? mlp_forward_t<256>(s, X, rows, Y, keepZ) : mlp_forward_t<128>(s, X, rows, Y, keepZ);
 }
 
@@ -1127,6 +1513,7 @@ hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device,
         return HIDEM_ERR_CUDA;
     };
     cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->smCount, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     auto dm = [&](void **p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, bytes);
@@ -1159,7 +1546,9 @@ hidem_status hidem_surrogate_create(const hidem_surrogate_config *c, int device,
     dm((void **)&s->idx, sizeof(int) * B);
     dm((void **)&s->scratchIn, sizeof(float) * (size_t)B * s->nin);
     dm((void **)&s->scratchT, sizeof(float) * (size_t)B * kOut);
-    s->PB = std::max(B, 65536);
+    // rows per predict chunk: with the persistent forward pass, 1,024 block pairs per chunk
+    // keep the last round of pairs over the SMs a small share of a chunk
+    s->PB = std::max(B, 262144);
     dm((void **)&s->predIn, sizeof(float) * (size_t)s->PB * s->nin);
     dm((void **)&s->predY, sizeof(float) * (size_t)s->PB * kOut);
     dm((void **)&s->predX, sizeof(bf16) * (size_t)s->PB * K0);
@@ -1305,6 +1694,17 @@ hidem_status hidem_surrogate_predict_device(hidem_surrogate *s, const float *inp
 }
 
 void *hidem_surrogate_get_stream(hidem_surrogate *s) { return s ? (void *)s->stream : nullptr; }
+
+hidem_status hidem_surrogate_set_forward(hidem_surrogate *s, int32_t kind) {
+    if (!s) return HIDEM_ERR_ARG;
+    if (kind != HIDEM_SURROGATE_FORWARD_AUTO && kind != HIDEM_SURROGATE_FORWARD_BLOCK &&
+        kind != HIDEM_SURROGATE_FORWARD_PINGPONG)
+        return sfail(s, HIDEM_ERR_ARG, "forward kind %d (0 auto, 1 block, 2 ping-pong)", kind);
+    if (kind == HIDEM_SURROGATE_FORWARD_PINGPONG && s->W != 256)
+        return sfail(s, HIDEM_ERR_ARG, "the ping-pong forward pass needs width 256");
+    s->forwardKind = kind;
+    return HIDEM_OK;
+}
 
 hidem_status hidem_surrogate_gradients(hidem_surrogate *s, const float *inputs, const float *targets,
                                        int64_t n, float *grads, double *loss) {

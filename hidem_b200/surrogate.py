@@ -113,6 +113,10 @@ class Surrogate:
         and [n][3] FP32 arrays, e.g. torch tensors' data_ptr())."""
         self._check(self._lib.hidem_surrogate_predict_device(self._s, inputs_ptr, int(n), out_ptr))
 
+    def set_forward(self, kind: int) -> None:
+        """The forward pass's kernel: abi.SURROGATE_FORWARD_AUTO, _BLOCK or _PINGPONG."""
+        self._check(self._lib.hidem_surrogate_set_forward(self._s, int(kind)))
+
     @property
     def stream_handle(self) -> int:
         """The cudaStream_t the surrogate's work runs on."""

@@ -603,6 +603,17 @@ hidem_status hidem_surrogate_predict(hidem_surrogate *s, const float *inputs, in
  * and the call returns when it has completed. */
 hidem_status hidem_surrogate_predict_device(hidem_surrogate *s, const float *inputs, int64_t n, float *out);
 void *hidem_surrogate_get_stream(hidem_surrogate *s);
+/* The forward pass's kernel: AUTO (default) takes PINGPONG for width 256 and BLOCK for
+ * width 128. BLOCK: one CTA per 128-row block runs the block through every layer.
+ * PINGPONG (width 256 only): a persistent CTA per SM takes pairs of 128-row blocks and
+ * alternates them, so one block's epilogue runs while the tensor cores compute the other
+ * block's layer. Both give the same hidden layers bit for bit; the 3-wide output layer's
+ * FP32 sums are added in a different order (BLOCK: one sum over all 256 columns;
+ * PINGPONG: four sums of 64 columns, added in column order). */
+#define HIDEM_SURROGATE_FORWARD_AUTO 0
+#define HIDEM_SURROGATE_FORWARD_BLOCK 1
+#define HIDEM_SURROGATE_FORWARD_PINGPONG 2
+hidem_status hidem_surrogate_set_forward(hidem_surrogate *s, int32_t kind);
 /* loss and gradient of all parameters (flat order above) on exactly these n rows, no
  * update; n a multiple of 128 and at most `batch` */
 hidem_status hidem_surrogate_gradients(hidem_surrogate *s, const float *inputs, const float *targets,

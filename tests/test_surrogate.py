@@ -117,7 +117,7 @@ def test_gpu_predict_from_device_memory_equals_host_predict(gpu):
     from hidem_b200 import surrogate as sg
     cfg = sg.default_config(width=256, hidden_layers=4, fourier_bands=4, batch=1024, seed=7, inputs=40)
     rng = np.random.default_rng(8)
-    u, _ = _rows(rng, 70000, 40)  # one full 65,536-row chunk and a ragged one
+    u, _ = _rows(rng, 300000, 40)  # one full 262,144-row chunk and a ragged one
     with sg.Surrogate(cfg) as s:
         y = s.predict(u)
         du = torch.from_numpy(u).cuda()
@@ -159,3 +159,48 @@ def test_gpu_training_with_cosine_decay_and_wide_inputs(gpu):
         uv, tv = _rows(rng, 4096, 40)
         mse = float(np.mean((s.predict(uv) - tv) ** 2))
     assert mse < 0.2 * float(np.mean(tv ** 2)) and mse < first
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows", [128, 384, 1500, 37888 + 256, 300000])
+def test_gpu_pingpong_forward_equals_block_forward(gpu, rows):
+    """The persistent ping-pong forward pass against the one-CTA-per-block pass: one block,
+    an odd number of blocks (the last pair's second block empty), a ragged row count, more
+    pairs than SMs (each CTA takes several), and a full predict chunk plus a ragged one.
+    The hidden layers are the same arithmetic; the output layer's FP32 sums are added in
+    another order, so the outputs agree to FP32 rounding of the 256-term sums."""
+    from hidem_b200 import abi
+    from hidem_b200 import surrogate as sg
+    cfg = sg.default_config(width=256, hidden_layers=4, fourier_bands=4, batch=1024, seed=9, inputs=82)
+    rng = np.random.default_rng(rows)
+    u, t = _rows(rng, rows, 82)
+    with sg.Surrogate(cfg) as s:
+        p = small_params(rng, 4, 256, so.feature_width(82, 4))
+        s.set_params(sg.flatten(p, cfg))
+        s.set_forward(abi.SURROGATE_FORWARD_BLOCK)
+        y_block = s.predict(u)
+        s.set_forward(abi.SURROGATE_FORWARD_PINGPONG)
+        y_pp = s.predict(u)
+        scale = np.abs(y_block).max() + 1e-6
+        assert np.max(np.abs(y_pp - y_block)) <= 1e-5 * scale
+        assert not np.array_equal(y_pp, np.zeros_like(y_pp))
+        if rows % 128 == 0 and rows <= 1024:
+            # training's forward pass too: the gradients agree to FP32 rounding of the loss
+            g_pp, l_pp = s.gradients(u, t)
+            s.set_forward(abi.SURROGATE_FORWARD_BLOCK)
+            g_bl, l_bl = s.gradients(u, t)
+            assert abs(l_pp - l_bl) <= 1e-5 * l_bl
+            assert np.linalg.norm(g_pp - g_bl) <= 1e-4 * np.linalg.norm(g_bl)
+
+
+@pytest.mark.gpu
+def test_gpu_pingpong_forward_is_refused_for_width_128(gpu):
+    from hidem_b200 import abi
+    from hidem_b200 import surrogate as sg
+    cfg = sg.default_config(width=128, hidden_layers=2, fourier_bands=2, batch=1024, seed=1)
+    with sg.Surrogate(cfg) as s:
+        with pytest.raises(abi.HidemError):
+            s.set_forward(abi.SURROGATE_FORWARD_PINGPONG)
+        s.set_forward(abi.SURROGATE_FORWARD_AUTO)
+        with pytest.raises(abi.HidemError):
+            s.set_forward(7)
