@@ -109,10 +109,11 @@ class HiDEMLib:
     def run(self) -> bool:
         return self.end_timestep is None or self.getCurrentTimestep() < self.end_timestep
 
-    def breakActive(self) -> bool:
-        """The sample main's gate ``getCurrentTimestep() * dt > breakTime`` in lp."""
+    def breakActive(self, step: int | None = None) -> bool:
+        """The sample main's gate ``getCurrentTimestep() * dt > breakTime`` in lp (at
+        ``step`` when given, which saves reading the context's statistics)."""
         lp = self.lp
-        t = lp(self.getCurrentTimestep())
+        t = lp(self.getCurrentTimestep() if step is None else step)
         return bool(lp(t * lp(self.params.dt)) > lp(self.params.breakTime))
 
     def timestep_split(self) -> None:

@@ -238,9 +238,9 @@ class LocalComm:
                     src = send_bufs[r][6 * soff[r][s]: 6 * (soff[r][s] + cnt)]
                     dst = recv_bufs[s][6 * roff[s][r]: 6 * (roff[s][r] + cnt)]
                     dst.copy_(src, non_blocking=False)
-        for t in recv_bufs:
-            if t.is_cuda:
-                torch.cuda.synchronize(t.device)
+        # device buffers: the copies run on the devices' current streams, which the caller
+        # orders between its contexts' packs and unpacks; host buffers are copied already
+        del torch
 
 
 class DistComm:
@@ -281,10 +281,10 @@ class DistComm:
             if rc[s]:
                 ops.append(self.dist.P2POp(self.dist.irecv, recv_bufs[0][6 * roff[s]: 6 * roff[s + 1]], s))
         if ops:
+            # with NCCL, wait() orders the current stream after the transfers (no host wait);
+            # the caller orders its contexts' streams after the current stream
             for w in self.dist.batch_isend_irecv(ops):
                 w.wait()
-        if recv_bufs[0].is_cuda:
-            torch.cuda.current_stream(recv_bufs[0].device).synchronize()
 
 
 # ---------------------------------------------------------------------------------------
@@ -449,10 +449,19 @@ class SlabRun:
     # -- one timestep
     def _grid_service(self) -> None:
         loc = [lib.grid_service_local() for lib in self.libs]
-        mx = self.comm.allmax([m for m, _ in loc])
-        regen = [np.array([1.0 if lib.grid_service_decide(mx) else 0.0]) for lib in self.libs]
-        if not self.comm.allmax(regen)[0]:
-            return
+        if any(w for _, w in loc):
+            # a step where gridService reads the displacement maxima (every 10th): their
+            # maximum over all ranks, and the rebuild if any rank's policy asks for it
+            mx = self.comm.allmax([m for m, _ in loc])
+            regen = [np.array([1.0 if lib.grid_service_decide(mx) else 0.0]) for lib in self.libs]
+            if not self.comm.allmax(regen)[0]:
+                return
+        else:
+            # no maxima are read at this step, on any rank (every rank is at the same step
+            # with the same policy): the decision depends only on the step and on whether
+            # the context is built, which all ranks share, so it takes no collective
+            if not any([lib.grid_service_decide(np.zeros(3)) for lib in self.libs]):
+                return
         # Each rank's held set contains every contact partner of its own particles while
         # no particle has moved more than half the halo's room in x since the last
         # distribution (partners lie within the reach; each end moved at most that much):
@@ -471,6 +480,20 @@ class SlabRun:
         for lib in self.libs:
             lib.regenerate_frame(lo, hi)
 
+    def _streams(self):
+        """(context stream, the device's current stream) per context, when the halo buffers
+        live in device memory and the contexts expose their streams; else None."""
+        import torch
+        if not (self.send_bufs and self.send_bufs[0].is_cuda):
+            return None
+        if not all(hasattr(lib, "stream_handle") for lib in self.libs):
+            return None
+        out = []
+        for lib, buf in zip(self.libs, self.send_bufs):
+            dev = buf.device
+            out.append((torch.cuda.ExternalStream(lib.stream_handle, device=dev), torch.cuda.current_stream(dev)))
+        return out
+
     def _forces(self) -> None:
         for lib, buf in zip(self.libs, self.send_bufs):
             if hasattr(lib, "compute_forces_packed"):
@@ -478,18 +501,31 @@ class SlabRun:
             else:
                 lib.computePartForce()
                 lib.pack_halo_forces(buf.data_ptr())
-        for lib in self.libs:
-            lib.synchronize()
+        streams = self._streams()
+        if streams is None:
+            for lib in self.libs:
+                lib.synchronize()
+        else:
+            # ordered on the devices instead of the host: the exchange (on the current
+            # streams) after each context's pack, each context's unpack after the exchange
+            for ctx_stream, cur in streams:
+                cur.wait_stream(ctx_stream)
         self.comm.exchange(self.layout, self.send_bufs, self.recv_bufs)
+        if streams is not None:
+            for ctx_stream, cur in streams:
+                ctx_stream.wait_stream(cur)
         for lib, r, buf in zip(self.libs, self.comm.ranks, self.recv_bufs):
             lib.unpack_halo_forces(buf.data_ptr())
             self.exchanged += sum(self.layout.recv_counts(r))
 
     def step(self, nsteps: int = 1) -> None:
-        for _ in range(nsteps):
+        # the sample main's break gate (getCurrentTimestep() * dt > breakTime) from a step
+        # count kept here, so that a timestep makes no host round trip for it
+        t0 = self.libs[0].getCurrentTimestep()
+        for k in range(nsteps):
             self._grid_service()
             self._forces()
-            brk = self.libs[0].breakActive()
+            brk = self.libs[0].breakActive(t0 + k)
             for lib in self.libs:
                 lib.applyForce()
                 if brk:
@@ -497,6 +533,7 @@ class SlabRun:
                 lib.finalizeTs()
         for lib in self.libs:
             lib.synchronize()
+
 
 
 def _lib_device(lib):

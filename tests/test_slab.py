@@ -157,7 +157,11 @@ class FakeRank:
     def synchronize(self):
         pass
 
-    def breakActive(self):
+    def getCurrentTimestep(self):
+        return self.step_
+
+    def breakActive(self, step=None):
+        assert step is None or step == self.step_
         return False
 
     def applyForce(self):
