@@ -204,3 +204,26 @@ def test_gpu_pingpong_forward_is_refused_for_width_128(gpu):
         s.set_forward(abi.SURROGATE_FORWARD_AUTO)
         with pytest.raises(abi.HidemError):
             s.set_forward(7)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layers,nin,bands", [(1, 5, 8), (8, 5, 8), (2, 40, 4)])
+def test_gpu_pingpong_forward_other_depths_and_widths(gpu, layers, nin, bands):
+    """One hidden layer (the output layer's partial sums share the activation tile with the
+    feature slots), the deepest network, and a 384-wide first layer, against the
+    one-CTA-per-block pass and the oracle."""
+    from hidem_b200 import abi
+    from hidem_b200 import surrogate as sg
+    cfg = sg.default_config(width=256, hidden_layers=layers, fourier_bands=bands, batch=1024, seed=4,
+                            inputs=nin)
+    rng = np.random.default_rng(10 + layers)
+    u, t = _rows(rng, 1500, nin)
+    with sg.Surrogate(cfg) as s:
+        p = small_params(rng, layers, 256, so.feature_width(nin, bands))
+        s.set_params(sg.flatten(p, cfg))
+        y_pp = s.predict(u)
+        s.set_forward(abi.SURROGATE_FORWARD_BLOCK)
+        y_block = s.predict(u)
+    assert np.max(np.abs(y_pp - y_block)) <= 1e-5 * (np.abs(y_block).max() + 1e-6)
+    _, _, y_ref = so.forward_backward(p, layers, u, t, bands)
+    assert np.max(np.abs(y_pp - y_ref)) <= 2e-2 * (np.max(np.abs(y_ref)) + 1e-3)
