@@ -950,7 +950,11 @@ struct hidem_batch {
     int flags = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    void *entries = nullptr;                 // device BatchEntry<LP>[nctx], then int[2 * nctx]
+    void *entries = nullptr;                 // device BatchEntry<LP>[nctx], then int[4 * nctx]:
+                                             // the groups' particle CTA offsets, then their
+                                             // link CTA offsets
+    int *tbl = nullptr;                      // device: the entry of every CTA of each group's
+    long long tblCap = 0;                    // particle launches, then of its link launch
     void *staging = nullptr;                 // pinned host copy of the entries
     BatchCounter *ctr = nullptr;             // device launch counters, one per group
     unsigned long long *diff = nullptr;      // device diff maxima, 3 words per context
@@ -964,7 +968,9 @@ struct hidem_batch {
     struct Group {
         int first = 0, count = 0;             // entries [first, first + count)
         int fbOffset = 0;                     // its CTA offsets in the offset array
-        long long blocks = 0;                 // CTAs of its launch
+        long long blocks = 0;                 // CTAs of its particle launches
+        long long linkBlocks = 0;             // CTAs of its break pass (at least 1)
+        long long tblOffset = 0, ltblOffset = 0;  // its CTA-entry tables in tbl
         int maxC = 0, maxE = 0;
         std::vector<unsigned char> consts;    // Consts<LP> of the group
     };
@@ -1079,20 +1085,35 @@ void batch_group(hidem_batch *b, int kernel) {
             const hidem_ctx *c = b->ctxs[j];
             b->order.push_back(j);
             g.blocks += (c->n + per - 1) / per;
+            g.linkBlocks += (c->L + kStepThreads - 1) / kStepThreads;
             g.maxC = std::max(g.maxC, (int)c->maxNeigh);
             g.maxE = std::max(g.maxE, (int)c->maxLinksPP);
         }
         g.count = (int)b->order.size() - g.first;
+        // a group without links still launches one break CTA: it advances the run counter
+        g.linkBlocks = std::max<long long>(g.linkBlocks, 1);
         fb += g.count + 1;
         b->groups.push_back(std::move(g));
+    }
+    long long t = 0;
+    for (auto &g : b->groups) {
+        g.tblOffset = t;
+        t += g.blocks;
+    }
+    for (auto &g : b->groups) {
+        g.ltblOffset = t;
+        t += g.linkBlocks;
     }
 }
 
 // what identifies the launches of a run: graphs are re-captured when it changes
 std::string batch_shape(const hidem_batch *b, int kernel) {
     std::string sh(reinterpret_cast<const char *>(&kernel), sizeof kernel);
+    const long long tp = (long long)reinterpret_cast<uintptr_t>(b->tbl);
+    sh.append(reinterpret_cast<const char *>(&tp), sizeof tp);
     for (const auto &g : b->groups) {
-        const long long v[6] = {g.first, g.count, g.fbOffset, g.blocks, g.maxC, g.maxE};
+        const long long v[9] = {g.first, g.count, g.fbOffset, g.blocks, g.maxC, g.maxE,
+                                g.linkBlocks, g.tblOffset, g.ltblOffset};
         sh.append(reinterpret_cast<const char *>(v), sizeof v);
         sh.append(g.consts.begin(), g.consts.end());
     }
@@ -1105,9 +1126,10 @@ hidem_status batch_upload(hidem_batch *b, const std::vector<char> &pending, int 
     if (b->uploadPending) BCK(cudaEventSynchronize(b->uploaded));
     BatchEntry<LP> *h = static_cast<BatchEntry<LP> *>(b->staging);
     int *fb = reinterpret_cast<int *>(h + nc);
+    int *lfb = fb + 2 * nc;
     const int per = batch_particles_per_cta(kernel);
     for (const auto &g : b->groups) {
-        int firstBlock = 0;
+        int firstBlock = 0, firstLink = 0;
         for (int q = 0; q < g.count; ++q) {
             const int idx = b->order[g.first + q];
             hidem_ctx *c = b->ctxs[idx];
@@ -1129,12 +1151,34 @@ hidem_status batch_upload(hidem_batch *b, const std::vector<char> &pending, int 
             h[g.first + q] = e;
             fb[g.fbOffset + q] = firstBlock;
             firstBlock += (int)((c->n + per - 1) / per);
+            lfb[g.fbOffset + q] = firstLink;
+            firstLink += (int)((c->L + kStepThreads - 1) / kStepThreads);
         }
         fb[g.fbOffset + g.count] = firstBlock;
+        lfb[g.fbOffset + g.count] = firstLink;
     }
-    BCK(cudaMemcpyAsync(b->entries, h, sizeof(BatchEntry<LP>) * nc + sizeof(int) * 2 * nc,
+    BCK(cudaMemcpyAsync(b->entries, h, sizeof(BatchEntry<LP>) * nc + sizeof(int) * 4 * nc,
                         cudaMemcpyHostToDevice, b->stream));
     BCK(cudaEventRecord(b->uploaded, b->stream));
+    // the entry of every CTA: one table per group and launch grid, filled on the device from
+    // the offsets just uploaded (a group without links keeps its one break CTA on entry 0)
+    long long need = 0;
+    for (const auto &g : b->groups) need = std::max(need, g.ltblOffset + g.linkBlocks);
+    if (need > b->tblCap) {
+        BCK(cudaStreamSynchronize(b->stream));
+        if (b->tbl) BCK(cudaFree(b->tbl));
+        b->tbl = nullptr;
+        b->tblCap = 0;
+        BCK(cudaMalloc((void **)&b->tbl, sizeof(int) * (size_t)need));
+        b->tblCap = need;
+    }
+    BCK(cudaMemsetAsync(b->tbl, 0, sizeof(int) * (size_t)need, b->stream));
+    const int *dfb = reinterpret_cast<const int *>(static_cast<const BatchEntry<LP> *>(b->entries) + nc);
+    for (const auto &g : b->groups) {
+        launch_block_table(dfb + g.fbOffset, g.count, b->tbl + g.tblOffset, b->stream);
+        launch_block_table(dfb + 2 * nc + g.fbOffset, g.count, b->tbl + g.ltblOffset, b->stream);
+    }
+    BCK(cudaGetLastError());
     b->uploadPending = true;
     BCK(cudaMemsetAsync(b->ctr, 0, sizeof(BatchCounter) * b->groups.size(), b->stream));
     b->uploads += 1;
@@ -1152,10 +1196,11 @@ void batch_enqueue_step(hidem_batch *b, int kernel) {
         Consts<LP> c;
         std::memcpy(&c, g.consts.data(), sizeof c);
         if (kernel == HIDEM_STEP_KERNEL_TWO_PASS)
-            launch_two_pass_batch<LP>(c, ent + g.first, fb + g.fbOffset, g.count, b->ctr + gi, (int)g.blocks,
-                                      b->stream);
+            launch_two_pass_batch<LP>(c, ent + g.first, fb + g.fbOffset, b->tbl + g.tblOffset,
+                                      fb + 2 * nc + g.fbOffset, b->tbl + g.ltblOffset, b->ctr + gi,
+                                      (int)g.blocks, (int)g.linkBlocks, b->stream);
         else
-            launch_step_batch<LP>(c, ent + g.first, fb + g.fbOffset, g.count, b->ctr + gi,
+            launch_step_batch<LP>(c, ent + g.first, fb + g.fbOffset, b->tbl + g.tblOffset, b->ctr + gi,
                                   (int)g.blocks, g.maxC, g.maxE, kernel, b->stream);
     }
 }
@@ -1299,6 +1344,8 @@ hidem_status batch_run(hidem_batch *b, int nsteps) {
             for (const auto &g : b->groups) {
                 if (g.blocks > 0x7fffffffLL)
                     return bfail(b, HIDEM_ERR_CAPACITY, "too many particles for one batched launch");
+                if (g.linkBlocks > 0x7fffffffLL)
+                    return bfail(b, HIDEM_ERR_CAPACITY, "too many links for one batched launch");
                 if (kernel == HIDEM_STEP_KERNEL_ITEMS && !batch_fits<LP>(g.maxC, g.maxE))
                     oneLaunch = false;
             }
@@ -2807,7 +2854,7 @@ hidem_status hidem_batch_create(hidem_ctx *const *ctxs, int32_t nctx, int32_t fl
     b->device = ctxs[0]->device;
     b->flags = flags;
     const size_t eb = (b->mixed ? sizeof(BatchEntry<float>) : sizeof(BatchEntry<double>)) * (size_t)nctx +
-                      sizeof(int) * 2 * (size_t)nctx;
+                      sizeof(int) * 4 * (size_t)nctx;
     cudaError_t e = cudaSetDevice(b->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&b->entries, eb);
@@ -2837,6 +2884,7 @@ void hidem_batch_destroy(hidem_batch *b) {
     batch_clear_graphs(b);
     if (b->uploaded) cudaEventDestroy(b->uploaded);
     if (b->entries) cudaFree(b->entries);
+    if (b->tbl) cudaFree(b->tbl);
     if (b->staging) cudaFreeHost(b->staging);
     if (b->ctr) cudaFree(b->ctr);
     if (b->diff) cudaFree(b->diff);

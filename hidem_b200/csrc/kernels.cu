@@ -1129,7 +1129,7 @@ __global__ void __launch_bounds__(kItemThreads)
 }
 
 // One fused step of many independent contexts in one launch. CTA b belongs to the entry
-// whose CTA range [firstBlocks[e], firstBlocks[e + 1]) holds b; all entries share the
+// blockEntry[b], whose CTA range is [firstBlocks[e], firstBlocks[e + 1]); all entries share the
 // launch's constants except the break thresholds (in each entry's arguments), and each
 // entry's per-step arguments are derived from the run counter the way the single-context
 // host loop sets them: records alternate between the two buffers, the link update of the
@@ -1145,20 +1145,14 @@ __global__ void __launch_bounds__(KIND == HIDEM_STEP_KERNEL_ITEMS ? kItemThreads
                                   : KIND == HIDEM_STEP_KERNEL_THREAD      ? kThreadBlocks<LP>
                                                                           : 1)
     k_step_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
-                 const int *__restrict__ firstBlocks, int nentries, BatchCounter *__restrict__ ctr,
-                 int totalBlocks) {
+                 const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry,
+                 BatchCounter *__restrict__ ctr, int totalBlocks) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int sRun, sEntry;
     const int b = blockIdx.x;
     if (threadIdx.x == 0) {
         sRun = *reinterpret_cast<volatile int *>(&ctr->s);
-        int lo = 0, hi = nentries - 1;
-        while (lo < hi) {  // last entry with firstBlocks[e] <= b
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(firstBlocks + mid) <= b) lo = mid;
-            else hi = mid - 1;
-        }
-        sEntry = lo;
+        sEntry = __ldg(blockEntry + b);
     }
     __syncthreads();
     const int s = sRun;
@@ -1193,32 +1187,35 @@ __global__ void __launch_bounds__(KIND == HIDEM_STEP_KERNEL_ITEMS ? kItemThreads
 
 // ---- the two-pass step over a batch (three launches per step and group) ----
 
-// the entry whose CTA range holds block b (last entry with firstBlocks[e] <= b) and the
-// run's launch counter, in shared memory
-__device__ __forceinline__ void batch_locate(const int *firstBlocks, int nentries, const BatchCounter *ctr,
-                                             int &run, int &entry) {
+// The entry whose CTA range holds this CTA (a table of one entry index per CTA, filled when
+// the batch's entries are uploaded: one load where a search over the offsets took several
+// dependent ones at the start of every CTA) and the run's current step.
+__device__ __forceinline__ void batch_locate(const int *blockEntry, const BatchCounter *ctr, int &run,
+                                             int &entry) {
     __shared__ int sRun, sEntry;
     if (threadIdx.x == 0) {
         sRun = *reinterpret_cast<const volatile int *>(&ctr->s);
-        int lo = 0, hi = nentries - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(firstBlocks + mid) <= (int)blockIdx.x) lo = mid;
-            else hi = mid - 1;
-        }
-        sEntry = lo;
+        sEntry = __ldg(blockEntry + blockIdx.x);
     }
     __syncthreads();
     run = sRun;
     entry = sEntry;
 }
 
+// tbl[offs[e] .. offs[e + 1]) = e for each of the `count` entries (one CTA per entry)
+__global__ void k_block_table(const int *__restrict__ offs, int *__restrict__ tbl) {
+    const int e = blockIdx.x;
+    const int a = __ldg(offs + e), b = __ldg(offs + e + 1);
+    for (int i = a + threadIdx.x; i < b; i += blockDim.x) tbl[i] = e;
+}
+
 template <class LP>
 __global__ void __launch_bounds__(kStepThreads, kCapBlocksForces<LP>)
     k_force_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
-                  const int *__restrict__ firstBlocks, int nentries, const BatchCounter *__restrict__ ctr) {
+                  const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry,
+                  const BatchCounter *__restrict__ ctr) {
     int s, ei;
-    batch_locate(firstBlocks, nentries, ctr, s, ei);
+    batch_locate(blockEntry, ctr, s, ei);
     const BatchEntry<LP> &e = entries[ei];
     StepArgs<LP> a = e.a;
     a.in = e.rec[e.cur0];
@@ -1233,9 +1230,10 @@ __global__ void __launch_bounds__(kStepThreads, kCapBlocksForces<LP>)
 template <class LP>
 __global__ void __launch_bounds__(kStepThreads)
     k_integrate_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
-                      const int *__restrict__ firstBlocks, int nentries, const BatchCounter *__restrict__ ctr) {
+                      const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry,
+                      const BatchCounter *__restrict__ ctr) {
     int s, ei;
-    batch_locate(firstBlocks, nentries, ctr, s, ei);
+    batch_locate(blockEntry, ctr, s, ei);
     const BatchEntry<LP> &e = entries[ei];
     const long long step = e.step0 + s;
     const int lb = (int)blockIdx.x - __ldg(firstBlocks + ei);
@@ -1267,26 +1265,25 @@ __global__ void __launch_bounds__(kStepThreads)
     }
 }
 
+// The break pass of the batch: one thread per link over a grid of its own (the links of
+// entry e take CTAs [linkFirst[e], linkFirst[e + 1]), linkEntry maps a CTA to its entry),
+// so that each thread's two record gathers are in flight beside every other thread's, as
+// in the single-context pass.
 template <class LP>
 __global__ void __launch_bounds__(kStepThreads)
     k_break_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
-                  const int *__restrict__ firstBlocks, int nentries, BatchCounter *__restrict__ ctr,
-                  int totalBlocks) {
+                  const int *__restrict__ linkFirst, const int *__restrict__ linkEntry,
+                  BatchCounter *__restrict__ ctr, int totalBlocks) {
     int s, ei;
-    batch_locate(firstBlocks, nentries, ctr, s, ei);
+    batch_locate(linkEntry, ctr, s, ei);
     const BatchEntry<LP> &e = entries[ei];
     const long long step = e.step0 + s;
+    const long long l = (long long)((int)blockIdx.x - __ldg(linkFirst + ei)) * kStepThreads + threadIdx.x;
     // the sample main's gate t dt > breakTime (MainMeshBlock.cpp:312), in lp
-    if ((LP)((LP)step * c.dt) > c.breakTime && e.L > 0) {
-        const int b0 = __ldg(firstBlocks + ei);
-        const int nb = __ldg(firstBlocks + ei + 1) - b0;
-        const long long chunk = (e.L + nb - 1) / nb;
-        const long long l0 = (long long)((int)blockIdx.x - b0) * chunk;
-        const long long l1 = min(e.L, l0 + chunk);
-        const PRec<LP> *rec = e.rec[e.cur0];
-        for (long long l = l0 + threadIdx.x; l < l1; l += kStepThreads) {
-            const uint8_t st = e.a.linkState[l];
-            if (st == 0) continue;
+    if ((LP)((LP)step * c.dt) > c.breakTime && l < e.L) {
+        const uint8_t st = e.a.linkState[l];
+        if (st != 0) {
+            const PRec<LP> *rec = e.rec[e.cur0];
             const PRec<LP> pa = load_rec(rec + __ldg(e.slotA + l));
             const PRec<LP> pb = load_rec(rec + __ldg(e.slotB + l));
             const uint8_t nst = break_link<LP>(e.a.bendBreak, e.a.maxLoad, pa, pb, st, __ldg(e.L0link + l));
@@ -1568,29 +1565,35 @@ int batch_particles_per_cta(int kernel) {
     return kernel == HIDEM_STEP_KERNEL_ITEMS ? 32 : kStepThreads;
 }
 
+void launch_block_table(const int *offs, int count, int *tbl, cudaStream_t s) {
+    if (count > 0) k_block_table<<<count, 256, 0, s>>>(offs, tbl);
+}
+
 template <class LP>
 void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
-                       int nentries, BatchCounter *ctr, int totalBlocks, int maxContacts,
+                       const int *blockEntry, BatchCounter *ctr, int totalBlocks, int maxContacts,
                        int maxEnds, int kernel, cudaStream_t s) {
     if (kernel == HIDEM_STEP_KERNEL_ITEMS) {
         const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds);
         k_step_batch<LP, HIDEM_STEP_KERNEL_ITEMS><<<totalBlocks, kItemThreads, L.total, s>>>(
-            c, entries, firstBlocks, nentries, ctr, totalBlocks);
+            c, entries, firstBlocks, blockEntry, ctr, totalBlocks);
     } else if (kernel == HIDEM_STEP_KERNEL_THREAD_CAPPED) {
         k_step_batch<LP, HIDEM_STEP_KERNEL_THREAD_CAPPED><<<totalBlocks, kStepThreads, 0, s>>>(
-            c, entries, firstBlocks, nentries, ctr, totalBlocks);
+            c, entries, firstBlocks, blockEntry, ctr, totalBlocks);
     } else {
         k_step_batch<LP, HIDEM_STEP_KERNEL_THREAD><<<totalBlocks, kStepThreads, 0, s>>>(
-            c, entries, firstBlocks, nentries, ctr, totalBlocks);
+            c, entries, firstBlocks, blockEntry, ctr, totalBlocks);
     }
 }
 
 template <class LP>
 void launch_two_pass_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
-                           int nentries, BatchCounter *ctr, int totalBlocks, cudaStream_t s) {
-    k_force_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, nentries, ctr);
-    k_integrate_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, nentries, ctr);
-    k_break_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, nentries, ctr, totalBlocks);
+                           const int *blockEntry, const int *linkFirst, const int *linkEntry,
+                           BatchCounter *ctr, int totalBlocks, int totalLinkBlocks, cudaStream_t s) {
+    k_force_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, blockEntry, ctr);
+    k_integrate_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, blockEntry, ctr);
+    k_break_batch<LP><<<totalLinkBlocks, kStepThreads, 0, s>>>(c, entries, linkFirst, linkEntry, ctr,
+                                                               totalLinkBlocks);
 }
 
 template <class LP>
@@ -1763,9 +1766,11 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
     template bool batch_fits<LP>(int, int);                                                        \
     template void prepare_step_batch<LP>();                                                        \
     template void launch_step_batch<LP>(const Consts<LP> &, const BatchEntry<LP> *, const int *,     \
-                                        int, BatchCounter *, int, int, int, int, cudaStream_t);    \
+                                        const int *, BatchCounter *, int, int, int, int,           \
+                                        cudaStream_t);                                             \
     template void launch_two_pass_batch<LP>(const Consts<LP> &, const BatchEntry<LP> *, const int *, \
-                                            int, BatchCounter *, int, cudaStream_t);               \
+                                            const int *, const int *, const int *, BatchCounter *, \
+                                            int, int, cudaStream_t);                               \
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \

@@ -171,19 +171,25 @@ template <class LP>
 void prepare_step_batch();
 // particles per CTA of the batch kernel `kernel` (HIDEM_STEP_KERNEL_*, not AUTO)
 int batch_particles_per_cta(int kernel);
-// entries, firstBlocks (nentries + 1 CTA offsets): device arrays; maxContacts / maxEnds:
-// the widest rows over all entries (shared memory of the item kernel)
+// tbl[offs[e] .. offs[e + 1]) = e for e < count: the entry of every CTA of a batch launch
+void launch_block_table(const int *offs, int count, int *tbl, cudaStream_t s);
+// entries, firstBlocks (nentries + 1 CTA offsets), blockEntry (the entry of each CTA):
+// device arrays; maxContacts / maxEnds: the widest rows over all entries (shared memory of
+// the item kernel)
 template <class LP>
 void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
-                       int nentries, BatchCounter *ctr, int totalBlocks, int maxContacts,
+                       const int *blockEntry, BatchCounter *ctr, int totalBlocks, int maxContacts,
                        int maxEnds, int kernel, cudaStream_t s);
 
 // the two-pass step over a run's entries: force pass, integrate pass (in place, with the
-// diff maxima every 10 steps), break pass (when t dt > breakTime; it advances the run's
-// counter); totalBlocks as for the thread kernels
+// diff maxima every 10 steps) over the particles' CTAs (firstBlocks, blockEntry,
+// totalBlocks as for the thread kernels); break pass (when t dt > breakTime; it advances the
+// run's counter) over the links' CTAs (linkFirst, linkEntry, totalLinkBlocks: kStepThreads
+// links per CTA)
 template <class LP>
 void launch_two_pass_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
-                           int nentries, BatchCounter *ctr, int totalBlocks, cudaStream_t s);
+                           const int *blockEntry, const int *linkFirst, const int *linkEntry,
+                           BatchCounter *ctr, int totalBlocks, int totalLinkBlocks, cudaStream_t s);
 
 template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,

@@ -173,3 +173,33 @@ def test_batch_argument_errors(gpu):
             batch.step(-1)
     for x in (a, b, c):
         x.close()
+
+
+@pytest.mark.parametrize("with_links", [True, False])
+def test_batch_with_contexts_without_links(gpu, with_links):
+    """Blocks whose link set is empty beside one with links, and (with_links False) a batch
+    in which no context has links: the break pass's own grid keeps one CTA to advance the
+    run counter, and every block matches its run alone."""
+    blocks = []
+    for k, (cells, seed) in enumerate([((3, 3, 3), 21), ((4, 3, 3), 22), ((2, 3, 2), 23)]):
+        P, p, l = workloads.ice_block(cells=cells, precision=abi.PREC_MIXED, seed=seed,
+                                      fixed_bottom=False, g=-9.81e3, waterLevel=-1e3)
+        if k > 0 or not with_links:
+            l = {key: v[:0] for key, v in l.items()}
+        blocks.append((P, p, l, 0))
+    alone = []
+    for P, p, l, start in blocks:
+        lib = open_lib(P, p, l, start)
+        lib.step(13)
+        lib.step(12)
+        alone.append(snapshot(lib))
+        lib.close()
+    libs = [open_lib(P, p, l, start) for P, p, l, start in blocks]
+    batch = HiDEMBatch(libs, graphs=True)
+    batch.step(13)
+    batch.step(12)
+    batch.close()
+    for lib, ref in zip(libs, alone):
+        assert_same(snapshot(lib), ref)
+        lib.close()
+    assert alone[1][0]["zDiff"].min() < 0  # the blocks moved
