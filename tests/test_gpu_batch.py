@@ -202,4 +202,4 @@ def test_batch_with_contexts_without_links(gpu, with_links):
     for lib, ref in zip(libs, alone):
         assert_same(snapshot(lib), ref)
         lib.close()
-    assert alone[1][0]["zDiff"].min() < 0  # the blocks moved
+    assert np.abs(alone[1][0]["zDiff"]).min() > 0  # the blocks moved
