@@ -956,7 +956,6 @@ struct hidem_batch {
     int *tbl = nullptr;                      // device: the entry of every CTA of each group's
     long long tblCap = 0;                    // particle launches, then of its link launch
     void *staging = nullptr;                 // pinned host copy of the entries
-    BatchCounter *ctr = nullptr;             // device launch counters, one per group
     unsigned long long *diff = nullptr;      // device diff maxima, 3 words per context
     unsigned long long *diffHost = nullptr;  // pinned
     cudaEvent_t uploaded = nullptr;
@@ -1177,16 +1176,16 @@ hidem_status batch_upload(hidem_batch *b, const std::vector<char> &pending, int 
     for (const auto &g : b->groups) {
         launch_block_table(dfb + g.fbOffset, g.count, b->tbl + g.tblOffset, b->stream);
         launch_block_table(dfb + 2 * nc + g.fbOffset, g.count, b->tbl + g.ltblOffset, b->stream);
+        b->ctxs[0]->launches += 2;
     }
     BCK(cudaGetLastError());
     b->uploadPending = true;
-    BCK(cudaMemsetAsync(b->ctr, 0, sizeof(BatchCounter) * b->groups.size(), b->stream));
     b->uploads += 1;
     return HIDEM_OK;
 }
 
 template <class LP>
-void batch_enqueue_step(hidem_batch *b, int kernel) {
+void batch_enqueue_step(hidem_batch *b, int kernel, int run) {
     const int nc = (int)b->ctxs.size();
     const BatchEntry<LP> *ent = static_cast<const BatchEntry<LP> *>(b->entries);
     const int *fb = reinterpret_cast<const int *>(ent + nc);
@@ -1197,10 +1196,10 @@ void batch_enqueue_step(hidem_batch *b, int kernel) {
         std::memcpy(&c, g.consts.data(), sizeof c);
         if (kernel == HIDEM_STEP_KERNEL_TWO_PASS)
             launch_two_pass_batch<LP>(c, ent + g.first, fb + g.fbOffset, b->tbl + g.tblOffset,
-                                      fb + 2 * nc + g.fbOffset, b->tbl + g.ltblOffset, b->ctr + gi,
+                                      fb + 2 * nc + g.fbOffset, b->tbl + g.ltblOffset, run,
                                       (int)g.blocks, (int)g.linkBlocks, b->stream);
         else
-            launch_step_batch<LP>(c, ent + g.first, fb + g.fbOffset, b->tbl + g.tblOffset, b->ctr + gi,
+            launch_step_batch<LP>(c, ent + g.first, fb + g.fbOffset, b->tbl + g.tblOffset, run,
                                   (int)g.blocks, g.maxC, g.maxE, kernel, b->stream);
     }
 }
@@ -1215,7 +1214,7 @@ hidem_status batch_launch_run(hidem_batch *b, int run, int kernel) {
         b->shape = sh;
     }
     if (!(b->flags & HIDEM_BATCH_GRAPHS)) {
-        for (int j = 0; j < run; ++j) batch_enqueue_step<LP>(b, kernel);
+        for (int j = 0; j < run; ++j) batch_enqueue_step<LP>(b, kernel, j);
         BCK(cudaGetLastError());
         return HIDEM_OK;
     }
@@ -1223,7 +1222,7 @@ hidem_status batch_launch_run(hidem_batch *b, int run, int kernel) {
     if (it == b->graphs.end()) {
         cudaGraph_t g = nullptr;
         BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        for (int j = 0; j < run; ++j) batch_enqueue_step<LP>(b, kernel);
+        for (int j = 0; j < run; ++j) batch_enqueue_step<LP>(b, kernel, j);
         const cudaError_t le = cudaGetLastError();
         const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
         if (le != cudaSuccess || ce != cudaSuccess) {
@@ -1367,7 +1366,10 @@ hidem_status batch_run(hidem_batch *b, int nsteps) {
                 }
         }
         if (oneLaunch) {
-            if (dirty) TRY(batch_upload<LP>(b, pending, kernel));
+            // every run's launches take their steps as 0 .. run - 1 after the entries' first
+            // step (parameters fixed in a captured run): each run starts from the host's step
+            // state, laid out again
+            TRY(batch_upload<LP>(b, pending, kernel));
             dirty = false;
             TRY(batch_launch_run<LP>(b, (int)run, kernel));
             const long long per = twoPass ? 3 : 1;
@@ -2859,7 +2861,6 @@ hidem_status hidem_batch_create(hidem_ctx *const *ctxs, int32_t nctx, int32_t fl
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&b->entries, eb);
     if (e == cudaSuccess) e = cudaMallocHost(&b->staging, eb);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&b->ctr, sizeof(BatchCounter) * (size_t)nctx);
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->diff, 3 * sizeof(unsigned long long) * (size_t)nctx);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&b->diffHost, 3 * sizeof(unsigned long long) * (size_t)nctx);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->uploaded, cudaEventDisableTiming);
@@ -2886,7 +2887,6 @@ void hidem_batch_destroy(hidem_batch *b) {
     if (b->entries) cudaFree(b->entries);
     if (b->tbl) cudaFree(b->tbl);
     if (b->staging) cudaFreeHost(b->staging);
-    if (b->ctr) cudaFree(b->ctr);
     if (b->diff) cudaFree(b->diff);
     if (b->diffHost) cudaFreeHost(b->diffHost);
     if (b->stream) cudaStreamDestroy(b->stream);

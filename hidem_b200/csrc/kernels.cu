@@ -1131,7 +1131,8 @@ __global__ void __launch_bounds__(kItemThreads)
 // One fused step of many independent contexts in one launch. CTA b belongs to the entry
 // blockEntry[b], whose CTA range is [firstBlocks[e], firstBlocks[e + 1]); all entries share the
 // launch's constants except the break thresholds (in each entry's arguments), and each
-// entry's per-step arguments are derived from the run counter the way the single-context
+// entry's per-step arguments are derived from the launch's step s within the run (a
+// parameter of the launch, fixed in a captured run) the way the single-context
 // host loop sets them: records alternate between the two buffers, the link update of the
 // previous step is applied first once the break gate t * dt > breakTime was open at that
 // step (MainMeshBlock.cpp:312), the diff maxima are folded on steps t with
@@ -1145,18 +1146,11 @@ __global__ void __launch_bounds__(KIND == HIDEM_STEP_KERNEL_ITEMS ? kItemThreads
                                   : KIND == HIDEM_STEP_KERNEL_THREAD      ? kThreadBlocks<LP>
                                                                           : 1)
     k_step_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
-                 const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry,
-                 BatchCounter *__restrict__ ctr, int totalBlocks) {
+                 const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry, int s) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ int sRun, sEntry;
     const int b = blockIdx.x;
-    if (threadIdx.x == 0) {
-        sRun = *reinterpret_cast<volatile int *>(&ctr->s);
-        sEntry = __ldg(blockEntry + b);
-    }
-    __syncthreads();
-    const int s = sRun;
-    const BatchEntry<LP> &e = entries[sEntry];
+    const int ei = __ldg(blockEntry + b);
+    const BatchEntry<LP> &e = entries[ei];
     StepArgs<LP> a = e.a;
     const int par = (e.cur0 + s) & 1;
     a.in = e.rec[par];
@@ -1165,42 +1159,21 @@ __global__ void __launch_bounds__(KIND == HIDEM_STEP_KERNEL_ITEMS ? kItemThreads
     a.breakStep = a.step - 1;
     a.breakPending = (s > 0) ? ((LP)((LP)a.breakStep * c.dt) > c.breakTime ? 1 : 0) : e.pend0;
     a.reduceDiff = (e.reduceEvery10 && (a.step + 1) % 10 == 0) ? 1 : 0;
-    const int lb = b - __ldg(firstBlocks + sEntry);
+    const int lb = b - __ldg(firstBlocks + ei);
     if (e.reduceEvery10 && a.step % 10 == 0 && lb == 0 && threadIdx.x < 3)
         a.diffMax[threadIdx.x] = 0ull;
     if (KIND == HIDEM_STEP_KERNEL_ITEMS)
         step_items_block<LP, true>(c, a, lb, smem);
     else
         step_thread_particle<LP, true>(c, a, lb * kStepThreads + threadIdx.x);
-    // the last CTA to finish advances the counter for the next launch of the run
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned int prev = atomicAdd(&ctr->done, 1u);
-        if (prev == (unsigned int)totalBlocks - 1u) {
-            ctr->done = 0u;
-            ctr->s = s + 1;
-            __threadfence();
-        }
-    }
 }
 
 // ---- the two-pass step over a batch (three launches per step and group) ----
 
-// The entry whose CTA range holds this CTA (a table of one entry index per CTA, filled when
-// the batch's entries are uploaded: one load where a search over the offsets took several
-// dependent ones at the start of every CTA) and the run's current step.
-__device__ __forceinline__ void batch_locate(const int *blockEntry, const BatchCounter *ctr, int &run,
-                                             int &entry) {
-    __shared__ int sRun, sEntry;
-    if (threadIdx.x == 0) {
-        sRun = *reinterpret_cast<const volatile int *>(&ctr->s);
-        sEntry = __ldg(blockEntry + blockIdx.x);
-    }
-    __syncthreads();
-    run = sRun;
-    entry = sEntry;
-}
+// The entry whose CTA range holds this CTA: a table of one entry index per CTA, filled when
+// the batch's entries are uploaded (one load, where a search over the offsets took several
+// dependent ones at the start of every CTA).
+__device__ __forceinline__ int batch_entry(const int *blockEntry) { return __ldg(blockEntry + blockIdx.x); }
 
 // tbl[offs[e] .. offs[e + 1]) = e for each of the `count` entries (one CTA per entry)
 __global__ void k_block_table(const int *__restrict__ offs, int *__restrict__ tbl) {
@@ -1212,10 +1185,8 @@ __global__ void k_block_table(const int *__restrict__ offs, int *__restrict__ tb
 template <class LP>
 __global__ void __launch_bounds__(kStepThreads, kCapBlocksForces<LP>)
     k_force_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
-                  const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry,
-                  const BatchCounter *__restrict__ ctr) {
-    int s, ei;
-    batch_locate(blockEntry, ctr, s, ei);
+                  const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry, int s) {
+    const int ei = batch_entry(blockEntry);
     const BatchEntry<LP> &e = entries[ei];
     StepArgs<LP> a = e.a;
     a.in = e.rec[e.cur0];
@@ -1230,10 +1201,8 @@ __global__ void __launch_bounds__(kStepThreads, kCapBlocksForces<LP>)
 template <class LP>
 __global__ void __launch_bounds__(kStepThreads)
     k_integrate_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
-                      const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry,
-                      const BatchCounter *__restrict__ ctr) {
-    int s, ei;
-    batch_locate(blockEntry, ctr, s, ei);
+                      const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry, int s) {
+    const int ei = batch_entry(blockEntry);
     const BatchEntry<LP> &e = entries[ei];
     const long long step = e.step0 + s;
     const int lb = (int)blockIdx.x - __ldg(firstBlocks + ei);
@@ -1272,10 +1241,8 @@ __global__ void __launch_bounds__(kStepThreads)
 template <class LP>
 __global__ void __launch_bounds__(kStepThreads)
     k_break_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
-                  const int *__restrict__ linkFirst, const int *__restrict__ linkEntry,
-                  BatchCounter *__restrict__ ctr, int totalBlocks) {
-    int s, ei;
-    batch_locate(linkEntry, ctr, s, ei);
+                  const int *__restrict__ linkFirst, const int *__restrict__ linkEntry, int s) {
+    const int ei = batch_entry(linkEntry);
     const BatchEntry<LP> &e = entries[ei];
     const long long step = e.step0 + s;
     const long long l = (long long)((int)blockIdx.x - __ldg(linkFirst + ei)) * kStepThreads + threadIdx.x;
@@ -1296,17 +1263,6 @@ __global__ void __launch_bounds__(kStepThreads)
                     if ((long long)slot < e.a.eventCap) e.a.events[slot] = make_int2((int)l, (int)step);
                 }
             }
-        }
-    }
-    // the last CTA to finish advances the counter for the next step of the run
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned int prev = atomicAdd(&ctr->done, 1u);
-        if (prev == (unsigned int)totalBlocks - 1u) {
-            ctr->done = 0u;
-            ctr->s = s + 1;
-            __threadfence();
         }
     }
 }
@@ -1571,29 +1527,28 @@ void launch_block_table(const int *offs, int count, int *tbl, cudaStream_t s) {
 
 template <class LP>
 void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
-                       const int *blockEntry, BatchCounter *ctr, int totalBlocks, int maxContacts,
-                       int maxEnds, int kernel, cudaStream_t s) {
+                       const int *blockEntry, int run, int totalBlocks, int maxContacts, int maxEnds,
+                       int kernel, cudaStream_t s) {
     if (kernel == HIDEM_STEP_KERNEL_ITEMS) {
         const StageLayout L = stage_layout(sizeof(PRec<LP>), sizeof(LP), maxContacts, maxEnds);
         k_step_batch<LP, HIDEM_STEP_KERNEL_ITEMS><<<totalBlocks, kItemThreads, L.total, s>>>(
-            c, entries, firstBlocks, blockEntry, ctr, totalBlocks);
+            c, entries, firstBlocks, blockEntry, run);
     } else if (kernel == HIDEM_STEP_KERNEL_THREAD_CAPPED) {
         k_step_batch<LP, HIDEM_STEP_KERNEL_THREAD_CAPPED><<<totalBlocks, kStepThreads, 0, s>>>(
-            c, entries, firstBlocks, blockEntry, ctr, totalBlocks);
+            c, entries, firstBlocks, blockEntry, run);
     } else {
         k_step_batch<LP, HIDEM_STEP_KERNEL_THREAD><<<totalBlocks, kStepThreads, 0, s>>>(
-            c, entries, firstBlocks, blockEntry, ctr, totalBlocks);
+            c, entries, firstBlocks, blockEntry, run);
     }
 }
 
 template <class LP>
 void launch_two_pass_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
-                           const int *blockEntry, const int *linkFirst, const int *linkEntry,
-                           BatchCounter *ctr, int totalBlocks, int totalLinkBlocks, cudaStream_t s) {
-    k_force_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, blockEntry, ctr);
-    k_integrate_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, blockEntry, ctr);
-    k_break_batch<LP><<<totalLinkBlocks, kStepThreads, 0, s>>>(c, entries, linkFirst, linkEntry, ctr,
-                                                               totalLinkBlocks);
+                           const int *blockEntry, const int *linkFirst, const int *linkEntry, int run,
+                           int totalBlocks, int totalLinkBlocks, cudaStream_t s) {
+    k_force_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, blockEntry, run);
+    k_integrate_batch<LP><<<totalBlocks, kStepThreads, 0, s>>>(c, entries, firstBlocks, blockEntry, run);
+    k_break_batch<LP><<<totalLinkBlocks, kStepThreads, 0, s>>>(c, entries, linkFirst, linkEntry, run);
 }
 
 template <class LP>
@@ -1766,11 +1721,10 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
     template bool batch_fits<LP>(int, int);                                                        \
     template void prepare_step_batch<LP>();                                                        \
     template void launch_step_batch<LP>(const Consts<LP> &, const BatchEntry<LP> *, const int *,     \
-                                        const int *, BatchCounter *, int, int, int, int,           \
-                                        cudaStream_t);                                             \
+                                        const int *, int, int, int, int, int, cudaStream_t);       \
     template void launch_two_pass_batch<LP>(const Consts<LP> &, const BatchEntry<LP> *, const int *, \
-                                            const int *, const int *, const int *, BatchCounter *, \
-                                            int, int, cudaStream_t);                               \
+                                            const int *, const int *, const int *, int, int, int,  \
+                                            cudaStream_t);                                         \
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \

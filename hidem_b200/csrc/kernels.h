@@ -157,12 +157,6 @@ struct BatchEntry {
     const LP *L0link;
     long long L;
 };
-// Launch counter shared by a run of batched launches: launch s reads s; the last CTA to
-// finish sets s + 1 for the next launch in the stream.
-struct BatchCounter {
-    int s;
-    unsigned int done;
-};
 // whether rows of these widths run in the item kernel (else: per-context launches)
 template <class LP>
 bool batch_fits(int maxContacts, int maxEnds);
@@ -174,22 +168,22 @@ int batch_particles_per_cta(int kernel);
 // tbl[offs[e] .. offs[e + 1]) = e for e < count: the entry of every CTA of a batch launch
 void launch_block_table(const int *offs, int count, int *tbl, cudaStream_t s);
 // entries, firstBlocks (nentries + 1 CTA offsets), blockEntry (the entry of each CTA):
-// device arrays; maxContacts / maxEnds: the widest rows over all entries (shared memory of
+// device arrays; run: the launch's step within the run (each entry's step is its first
+// step + run); maxContacts / maxEnds: the widest rows over all entries (shared memory of
 // the item kernel)
 template <class LP>
 void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
-                       const int *blockEntry, BatchCounter *ctr, int totalBlocks, int maxContacts,
-                       int maxEnds, int kernel, cudaStream_t s);
+                       const int *blockEntry, int run, int totalBlocks, int maxContacts, int maxEnds,
+                       int kernel, cudaStream_t s);
 
 // the two-pass step over a run's entries: force pass, integrate pass (in place, with the
 // diff maxima every 10 steps) over the particles' CTAs (firstBlocks, blockEntry,
-// totalBlocks as for the thread kernels); break pass (when t dt > breakTime; it advances the
-// run's counter) over the links' CTAs (linkFirst, linkEntry, totalLinkBlocks: kStepThreads
-// links per CTA)
+// totalBlocks as for the thread kernels); break pass (when t dt > breakTime) over the links'
+// CTAs (linkFirst, linkEntry, totalLinkBlocks: kStepThreads links per CTA)
 template <class LP>
 void launch_two_pass_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
-                           const int *blockEntry, const int *linkFirst, const int *linkEntry,
-                           BatchCounter *ctr, int totalBlocks, int totalLinkBlocks, cudaStream_t s);
+                           const int *blockEntry, const int *linkFirst, const int *linkEntry, int run,
+                           int totalBlocks, int totalLinkBlocks, cudaStream_t s);
 
 template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,

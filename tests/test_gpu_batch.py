@@ -203,3 +203,33 @@ def test_batch_with_contexts_without_links(gpu, with_links):
         assert_same(snapshot(lib), ref)
         lib.close()
     assert np.abs(alone[1][0]["zDiff"]).min() > 0  # the blocks moved
+
+
+@pytest.mark.parametrize("kernel", [abi.STEP_KERNEL_TWO_PASS, abi.STEP_KERNEL_THREAD_CAPPED])
+def test_batch_runs_without_grid_service_between_them(gpu, kernel):
+    """Every context rebuilds on a fixed interval longer than the longest run (10 steps),
+    so consecutive runs meet no gridService point: each run still starts from the host's
+    step state (step, record buffer, owed link update)."""
+    blocks = []
+    for cells, seed in [((4, 3, 3), 31), ((3, 3, 4), 32)]:
+        P, p, l = workloads.ice_block(cells=cells, precision=abi.PREC_MIXED, seed=seed,
+                                      gridRegenInterval=50, maxLoad=5e-5)
+        blocks.append((P, p, l, 0))
+    alone = []
+    for P, p, l, start in blocks:
+        lib = open_lib(P, p, l, start)
+        lib.set_step_kernel(kernel)
+        lib.step(13)
+        lib.step(24)
+        alone.append(snapshot(lib))
+        lib.close()
+    libs = [open_lib(P, p, l, start) for P, p, l, start in blocks]
+    libs[0].set_step_kernel(kernel)
+    batch = HiDEMBatch(libs, graphs=True)
+    batch.step(13)
+    batch.step(24)
+    batch.close()
+    for lib, ref in zip(libs, alone):
+        assert_same(snapshot(lib), ref)
+        lib.close()
+    assert sum(len(r[2]) for r in alone) > 0  # links broke inside the runs
