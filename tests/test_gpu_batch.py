@@ -213,7 +213,7 @@ def test_batch_runs_without_grid_service_between_them(gpu, kernel):
     blocks = []
     for cells, seed in [((4, 3, 3), 31), ((3, 3, 4), 32)]:
         P, p, l = workloads.ice_block(cells=cells, precision=abi.PREC_MIXED, seed=seed,
-                                      gridRegenInterval=50, maxLoad=5e-5)
+                                      gridRegenInterval=50, maxLoad=2e-5)
         blocks.append((P, p, l, 0))
     alone = []
     for P, p, l, start in blocks:
