@@ -1084,7 +1084,7 @@ void batch_group(hidem_batch *b, int kernel) {
             const hidem_ctx *c = b->ctxs[j];
             b->order.push_back(j);
             g.blocks += (c->n + per - 1) / per;
-            g.linkBlocks += (c->L + kBreakLinksPerCta - 1) / kBreakLinksPerCta;
+            g.linkBlocks += (c->L + kStepThreads - 1) / kStepThreads;
             g.maxC = std::max(g.maxC, (int)c->maxNeigh);
             g.maxE = std::max(g.maxE, (int)c->maxLinksPP);
         }
@@ -1151,7 +1151,7 @@ hidem_status batch_upload(hidem_batch *b, const std::vector<char> &pending, int 
             fb[g.fbOffset + q] = firstBlock;
             firstBlock += (int)((c->n + per - 1) / per);
             lfb[g.fbOffset + q] = firstLink;
-            firstLink += (int)((c->L + kBreakLinksPerCta - 1) / kBreakLinksPerCta);
+            firstLink += (int)((c->L + kStepThreads - 1) / kStepThreads);
         }
         fb[g.fbOffset + g.count] = firstBlock;
         lfb[g.fbOffset + g.count] = firstLink;

@@ -1234,70 +1234,34 @@ __global__ void __launch_bounds__(kStepThreads)
     }
 }
 
-// Position and rotation of a record: what the break functor reads of it.
-template <class LP>
-__device__ __forceinline__ PRec<LP> load_pos_rot(const PRec<LP> *p) {
-    PRec<LP> r;
-    r.x = __ldg(&p->x);
-    r.y = __ldg(&p->y);
-    r.z = __ldg(&p->z);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) r.th[k] = __ldg(&p->th[k]);
-    return r;
-}
-
-// The break pass of the batch over a grid of its own (the links of entry e take CTAs
-// [linkFirst[e], linkFirst[e + 1]), linkEntry maps a CTA to its entry), kBreakLinksPerThread
-// links per thread, strided by the CTA's width so that each load is coalesced: the links'
-// states and end slots are loaded for all of them, then the live links' end records, then
-// the break functor runs on each, so that a thread's dependent loads overlap.
+// The break pass of the batch: one thread per link over a grid of its own (the links of
+// entry e take CTAs [linkFirst[e], linkFirst[e + 1]), linkEntry maps a CTA to its entry),
+// so that each thread's two record gathers are in flight beside every other thread's, as
+// in the single-context pass.
 template <class LP>
 __global__ void __launch_bounds__(kStepThreads)
     k_break_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
                   const int *__restrict__ linkFirst, const int *__restrict__ linkEntry, int s) {
-    constexpr int K = kBreakLinksPerThread;
     const int ei = batch_entry(linkEntry);
     const BatchEntry<LP> &e = entries[ei];
     const long long step = e.step0 + s;
+    const long long l = (long long)((int)blockIdx.x - __ldg(linkFirst + ei)) * kStepThreads + threadIdx.x;
     // the sample main's gate t dt > breakTime (MainMeshBlock.cpp:312), in lp
-    if (!((LP)((LP)step * c.dt) > c.breakTime)) return;
-    const long long L = e.L;
-    const long long base =
-        (long long)((int)blockIdx.x - __ldg(linkFirst + ei)) * kBreakLinksPerCta + threadIdx.x;
-    uint8_t st[K];
-    int sa[K], sb[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const long long l = base + (long long)k * kStepThreads;
-        st[k] = l < L ? e.a.linkState[l] : uint8_t(0);
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const long long l = base + (long long)k * kStepThreads;
-        sa[k] = st[k] ? __ldg(e.slotA + l) : 0;
-        sb[k] = st[k] ? __ldg(e.slotB + l) : 0;
-    }
-    const PRec<LP> *rec = e.rec[e.cur0];
-    PRec<LP> pa[K], pb[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (st[k]) {
-            pa[k] = load_pos_rot(rec + sa[k]);
-            pb[k] = load_pos_rot(rec + sb[k]);
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (!st[k]) continue;
-        const long long l = base + (long long)k * kStepThreads;
-        const uint8_t nst = break_link<LP>(e.a.bendBreak, e.a.maxLoad, pa[k], pb[k], st[k], __ldg(e.L0link + l));
-        if (nst != st[k]) {
-            e.a.linkState[l] = nst;
-            e.a.sState[e.sideSlot[2 * l]] = nst;
-            e.a.sState[e.sideSlot[2 * l + 1]] = nst;
-            if (nst == 0) {
-                const unsigned long long slot = atomicAdd(e.a.eventCount, 1ull);
-                if ((long long)slot < e.a.eventCap) e.a.events[slot] = make_int2((int)l, (int)step);
+    if ((LP)((LP)step * c.dt) > c.breakTime && l < e.L) {
+        const uint8_t st = e.a.linkState[l];
+        if (st != 0) {
+            const PRec<LP> *rec = e.rec[e.cur0];
+            const PRec<LP> pa = load_rec(rec + __ldg(e.slotA + l));
+            const PRec<LP> pb = load_rec(rec + __ldg(e.slotB + l));
+            const uint8_t nst = break_link<LP>(e.a.bendBreak, e.a.maxLoad, pa, pb, st, __ldg(e.L0link + l));
+            if (nst != st) {
+                e.a.linkState[l] = nst;
+                e.a.sState[e.sideSlot[2 * l]] = nst;
+                e.a.sState[e.sideSlot[2 * l + 1]] = nst;
+                if (nst == 0) {
+                    const unsigned long long slot = atomicAdd(e.a.eventCount, 1ull);
+                    if ((long long)slot < e.a.eventCap) e.a.events[slot] = make_int2((int)l, (int)step);
+                }
             }
         }
     }

@@ -5,9 +5,6 @@
 namespace hidem {
 
 constexpr int kStepThreads = 128;
-// links per thread and per CTA of the batched break pass
-constexpr int kBreakLinksPerThread = 4;
-constexpr int kBreakLinksPerCta = kStepThreads * kBreakLinksPerThread;
 constexpr int kItemThreads = 256;
 constexpr size_t kItemSmemLimit = 200 * 1024;
 // Byte offsets of the item kernel's shared-memory regions (same for all CTAs of a launch):
@@ -182,7 +179,7 @@ void launch_step_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const
 // the two-pass step over a run's entries: force pass, integrate pass (in place, with the
 // diff maxima every 10 steps) over the particles' CTAs (firstBlocks, blockEntry,
 // totalBlocks as for the thread kernels); break pass (when t dt > breakTime) over the links'
-// CTAs (linkFirst, linkEntry, totalLinkBlocks: kBreakLinksPerCta links per CTA)
+// CTAs (linkFirst, linkEntry, totalLinkBlocks: kStepThreads links per CTA)
 template <class LP>
 void launch_two_pass_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, const int *firstBlocks,
                            const int *blockEntry, const int *linkFirst, const int *linkEntry, int run,
