@@ -1148,24 +1148,30 @@ __global__ void __launch_bounds__(KIND == HIDEM_STEP_KERNEL_ITEMS ? kItemThreads
     k_step_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
                  const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry, int s) {
     extern __shared__ __align__(128) unsigned char smem[];
+    // the context's arguments in shared memory (read as the loops go, not held in registers)
+    __shared__ StepArgs<LP> sa;
     const int b = blockIdx.x;
     const int ei = __ldg(blockEntry + b);
     const BatchEntry<LP> &e = entries[ei];
-    StepArgs<LP> a = e.a;
-    const int par = (e.cur0 + s) & 1;
-    a.in = e.rec[par];
-    a.out = e.rec[par ^ 1];
-    a.step = e.step0 + s;
-    a.breakStep = a.step - 1;
-    a.breakPending = (s > 0) ? ((LP)((LP)a.breakStep * c.dt) > c.breakTime ? 1 : 0) : e.pend0;
-    a.reduceDiff = (e.reduceEvery10 && (a.step + 1) % 10 == 0) ? 1 : 0;
     const int lb = b - __ldg(firstBlocks + ei);
-    if (e.reduceEvery10 && a.step % 10 == 0 && lb == 0 && threadIdx.x < 3)
-        a.diffMax[threadIdx.x] = 0ull;
+    if (threadIdx.x == 0) {
+        StepArgs<LP> a = e.a;
+        const int par = (e.cur0 + s) & 1;
+        a.in = e.rec[par];
+        a.out = e.rec[par ^ 1];
+        a.step = e.step0 + s;
+        a.breakStep = a.step - 1;
+        a.breakPending = (s > 0) ? ((LP)((LP)a.breakStep * c.dt) > c.breakTime ? 1 : 0) : e.pend0;
+        a.reduceDiff = (e.reduceEvery10 && (a.step + 1) % 10 == 0) ? 1 : 0;
+        sa = a;
+    }
+    __syncthreads();
+    if (e.reduceEvery10 && sa.step % 10 == 0 && lb == 0 && threadIdx.x < 3)
+        sa.diffMax[threadIdx.x] = 0ull;
     if (KIND == HIDEM_STEP_KERNEL_ITEMS)
-        step_items_block<LP, true>(c, a, lb, smem);
+        step_items_block<LP, true>(c, sa, lb, smem);
     else
-        step_thread_particle<LP, true>(c, a, lb * kStepThreads + threadIdx.x);
+        step_thread_particle<LP, true>(c, sa, lb * kStepThreads + threadIdx.x);
 }
 
 // ---- the two-pass step over a batch (three launches per step and group) ----
@@ -1186,16 +1192,24 @@ template <class LP>
 __global__ void __launch_bounds__(kStepThreads, kCapBlocksForces<LP>)
     k_force_batch(const Consts<LP> c, const BatchEntry<LP> *__restrict__ entries,
                   const int *__restrict__ firstBlocks, const int *__restrict__ blockEntry, int s) {
+    // the context's arguments in shared memory, where the per-particle loop reads them as
+    // it goes (as it reads a single context's from the parameter bank), rather than in
+    // registers held across the loop
+    __shared__ StepArgs<LP> sa;
     const int ei = batch_entry(blockEntry);
     const BatchEntry<LP> &e = entries[ei];
-    StepArgs<LP> a = e.a;
-    a.in = e.rec[e.cur0];
-    a.out = e.rec[e.cur0];
-    a.step = e.step0 + s;
-    a.breakPending = 0;
-    a.reduceDiff = 0;
+    if (threadIdx.x == 0) {
+        StepArgs<LP> a = e.a;
+        a.in = e.rec[e.cur0];
+        a.out = e.rec[e.cur0];
+        a.step = e.step0 + s;
+        a.breakPending = 0;
+        a.reduceDiff = 0;
+        sa = a;
+    }
+    __syncthreads();
     const int lb = (int)blockIdx.x - __ldg(firstBlocks + ei);
-    step_thread_particle<LP, false>(c, a, lb * kStepThreads + threadIdx.x);
+    step_thread_particle<LP, false>(c, sa, lb * kStepThreads + threadIdx.x);
 }
 
 template <class LP>
