@@ -226,8 +226,9 @@ class LocalComm:
         return list(objs)
 
     def exchange(self, layout: SlabLayout, send_bufs: list, recv_bufs: list) -> None:
-        """recv_bufs[s]'s run from r <- send_bufs[r]'s run for s (torch tensors)."""
-        import torch
+        """recv_bufs[s]'s run from r <- send_bufs[r]'s run for s (torch tensors). Device
+        buffers are copied on the devices' current streams, which the caller orders between
+        its contexts' packs and unpacks; host buffers are copied when this returns."""
         R = self.size
         soff = [np.concatenate([[0], np.cumsum(layout.send_counts(r))]) for r in range(R)]
         roff = [np.concatenate([[0], np.cumsum(layout.recv_counts(s))]) for s in range(R)]
@@ -238,9 +239,6 @@ class LocalComm:
                     src = send_bufs[r][6 * soff[r][s]: 6 * (soff[r][s] + cnt)]
                     dst = recv_bufs[s][6 * roff[s][r]: 6 * (roff[s][r] + cnt)]
                     dst.copy_(src, non_blocking=False)
-        # device buffers: the copies run on the devices' current streams, which the caller
-        # orders between its contexts' packs and unpacks; host buffers are copied already
-        del torch
 
 
 class DistComm:
