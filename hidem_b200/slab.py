@@ -268,7 +268,6 @@ class DistComm:
         return out
 
     def exchange(self, layout: SlabLayout, send_bufs: list, recv_bufs: list) -> None:
-        import torch
         r = self.ranks[0]
         sc, rc = layout.send_counts(r), layout.recv_counts(r)
         soff, roff = np.concatenate([[0], np.cumsum(sc)]), np.concatenate([[0], np.cumsum(rc)])
