@@ -856,27 +856,16 @@ hidem_status run_steps(hidem_ctx *ctx, int nsteps) {
         }
         diffReady = false;
         if (kern == HIDEM_STEP_KERNEL_TWO_PASS) {
-            // force pass, then integrate pass and break pass (MainMeshBlock.cpp:295-320): with
-            // the break gate open, one launch that integrates out of place into the other
-            // record buffer and runs the break functor on each link from its end A; else the
-            // integrate pass in place
+            // force pass, integrate pass (in place), break pass (MainMeshBlock.cpp:295-320)
             if (ctx->profile) TRY(profile_pair(ctx, &e0, &e1));
             if (e0) CK(cudaEventRecord(e0, ctx->stream));
             if (t0) CK(cudaEventRecord(t0, ctx->stream));
-            const StepArgs<LP> a = step_args<LP>(ctx);
-            launch_step<LP>(consts<LP>(ctx), a, false, (int)ctx->maxNeigh, (int)ctx->maxLinksPP,
-                            HIDEM_STEP_KERNEL_THREAD_CAPPED, ctx->stream);
-            // (a collision mesh accumulates face forces in the integrate step: there the
-            // passes stay separate, so that each particle's contact is counted once)
-            if (break_active<LP>(ctx, t) && ctx->L > 0 && !consts<LP>(ctx).useMesh) {
-                launch_integrate_break<LP>(consts<LP>(ctx), a, recp<LP>(ctx, 1 - ctx->cur),
-                                           ctx->sideSlot[ctx->curSide], t, ctx->stream);
-                ctx->cur = 1 - ctx->cur;  // the slot order (type / orig / cellOf) is unchanged
-            } else {
-                launch_integrate<LP>(consts<LP>(ctx), recp<LP>(ctx, ctx->cur), ctx->type[ctx->ord],
-                                     static_cast<const LP *>(ctx->force), (int)ctx->n, ctx->stream);
-            }
+            launch_step<LP>(consts<LP>(ctx), step_args<LP>(ctx), false, (int)ctx->maxNeigh,
+                            (int)ctx->maxLinksPP, HIDEM_STEP_KERNEL_THREAD_CAPPED, ctx->stream);
+            launch_integrate<LP>(consts<LP>(ctx), recp<LP>(ctx, ctx->cur), ctx->type[ctx->ord],
+                                 static_cast<const LP *>(ctx->force), (int)ctx->n, ctx->stream);
             ctx->launches += 2;
+            if (break_active<LP>(ctx, t)) TRY(link_update_now<LP>(ctx, t));
             if (t1) CK(cudaEventRecord(t1, ctx->stream));
             if (e1) CK(cudaEventRecord(e1, ctx->stream));
             ctx->step = t + 1;

@@ -1295,57 +1295,6 @@ __global__ void k_integrate(const Consts<LP> c, PRec<LP> *__restrict__ rec,
     store_rec(rec + i, me);
 }
 
-// The integrate pass of a two-pass step with the step's break pass folded in (the break
-// gate open): HiDEMLib::applyForce for particle i out of place (a.in -> out), then the break
-// functor (HiDEMDefLinkBreakFunc, as linkUpdate runs it after applyForce) on each link whose
-// end A is i. The functor needs both ends' positions after the integrate step: end A's are
-// this thread's, end B's are computed again here from its record, force and type in a.in
-// — the same function of the same inputs as its own thread's, so the same bits — rather
-// than read after a second launch (not with a collision mesh, whose face forces the integrate
-// step accumulates). Each link is evaluated once, by its end A; a change of state goes to the
-// link's state and to both of its sides' mirrors, a break to the event list.
-template <class LP>
-__global__ void __launch_bounds__(256)
-    k_integrate_break(const Consts<LP> c, const StepArgs<LP> a, PRec<LP> *__restrict__ out,
-                      const int *__restrict__ sideSlot, long long step) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < a.n) {
-        const int n = a.n;
-        PRec<LP> me = load_rec(a.in + i);
-        LP F[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) F[q] = a.force[(long long)q * n + i];
-        integrate_particle<LP>(c, me, __ldg(a.type + i), F);
-        store_rec(out + i, me);
-        const int ns = (int)(__ldg(a.counts + i) >> 16);
-        const long long sbase = __ldg(a.sOff + (i >> 5)) + (i & 31);
-        for (int k = 0; k < ns; ++k) {
-            const long long si = sbase + (long long)k * kWarp;
-            const uint32_t pw = __ldg(a.sPartner + si);
-            if (pw & kSideIsB) continue;
-            const uint8_t st = a.sState[si];
-            if (st == 0) continue;
-            const int j = (int)(pw & kSlotMask);
-            PRec<LP> o = load_rec(a.in + j);
-            LP Fj[6];
-#pragma unroll
-            for (int q = 0; q < 6; ++q) Fj[q] = a.force[(long long)q * n + j];
-            integrate_particle<LP>(c, o, __ldg(a.type + j), Fj);
-            const uint8_t nst = break_link<LP>(a.bendBreak, a.maxLoad, me, o, st, __ldg(a.sL0 + si));
-            if (nst != st) {
-                const int l = __ldg(a.sLink + si);
-                a.linkState[l] = nst;
-                a.sState[sideSlot[2 * l]] = nst;
-                a.sState[sideSlot[2 * l + 1]] = nst;
-                if (nst == 0) {
-                    unsigned long long slot = atomicAdd(a.eventCount, 1ull);
-                    if ((long long)slot < a.eventCap) a.events[slot] = make_int2(l, (int)step);
-                }
-            }
-        }
-    }
-}
-
 // HiDEMLib::linkUpdate: the break functor over every link
 // (CombinedAccel::iterateLinks, CombinedAccel.h:200-235), with a warp-compacted
 // flag-and-select append of the links that broke.
@@ -1623,13 +1572,6 @@ void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, c
 }
 
 template <class LP>
-void launch_integrate_break(const Consts<LP> &c, const StepArgs<LP> &a, PRec<LP> *out,
-                            const int *sideSlot, long long step, cudaStream_t s) {
-    if (a.n <= 0) return;
-    k_integrate_break<LP><<<nblk(a.n, 256), 256, 0, s>>>(c, a, out, sideSlot, step);
-}
-
-template <class LP>
 void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *endA, const int *endB,
                        const int *sideSlot, uint8_t *sState, uint8_t *linkState, const LP *L0link,
                        long long L, long long step, int2 *events, unsigned long long *eventCount,
@@ -1799,8 +1741,6 @@ void launch_max_diff(const PRec<LP> *rec, int n, unsigned long long *out, int nb
                                             cudaStream_t);                                         \
     template void launch_integrate<LP>(const Consts<LP> &, PRec<LP> *, const uint8_t *,            \
                                        const LP *, int, cudaStream_t);                             \
-    template void launch_integrate_break<LP>(const Consts<LP> &, const StepArgs<LP> &, PRec<LP> *, \
-                                             const int *, long long, cudaStream_t);                \
     template void launch_link_break<LP>(const Consts<LP> &, const PRec<LP> *, const int *,         \
                                         const int *, const int *, uint8_t *, uint8_t *,            \
                                         const LP *, long long, long long, int2 *,                  \

@@ -188,12 +188,6 @@ void launch_two_pass_batch(const Consts<LP> &c, const BatchEntry<LP> *entries, c
 template <class LP>
 void launch_integrate(const Consts<LP> &c, PRec<LP> *rec, const uint8_t *type, const LP *force,
                       int n, cudaStream_t s);
-// the integrate pass out of place (a.in -> out) with the break functor on every link, each
-// evaluated by its end A (two-pass steps whose break gate is open); sideSlot: both sides'
-// storage slots of each link
-template <class LP>
-void launch_integrate_break(const Consts<LP> &c, const StepArgs<LP> &a, PRec<LP> *out,
-                            const int *sideSlot, long long step, cudaStream_t s);
 template <class LP>
 // endA / endB: the storage slots of every link's two ends
 void launch_link_break(const Consts<LP> &c, const PRec<LP> *rec, const int *endA, const int *endB,
