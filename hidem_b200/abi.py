@@ -142,19 +142,34 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def _field_ptr(kind: str, k: str, a, dt, count: int | None):
+    """The address of a field array — a numpy array, or a torch tensor in host or device
+    memory (the library copies from / to either) — checked for dtype, layout and size."""
+    if hasattr(a, "data_ptr"):  # torch tensor
+        import torch
+        want = getattr(torch, np.dtype(dt).name)
+        if a.dtype != want or not a.is_contiguous() or a.dim() != 1:
+            raise TypeError(f"{kind} field {k}: need a contiguous 1-D {want} tensor, got {a.dtype}")
+        if count is not None and a.shape[0] != count:
+            raise ValueError(f"{kind} field {k}: {a.shape[0]} elements, expected {count}")
+        return C.c_void_p(a.data_ptr()) if a.numel() else None
+    if a.dtype != dt or not a.flags.c_contiguous:
+        raise TypeError(f"{kind} field {k}: need contiguous {np.dtype(dt)}, got {a.dtype}")
+    if count is not None and a.shape[0] != count:
+        raise ValueError(f"{kind} field {k}: {a.shape[0]} elements, expected {count}")
+    return _ptr(a)
+
+
 def particle_soa(arrays: dict, precision: int, n: int | None = None) -> HidemParticleSoA:
-    """A particle SoA struct pointing into `arrays` (numpy, checked for dtype / size)."""
+    """A particle SoA struct pointing into `arrays` (numpy arrays or torch tensors, host or
+    device memory; checked for dtype / size)."""
     s = HidemParticleSoA()
     dts = particle_dtypes(precision)
     for k in PARTICLE_FIELDS:
         a = arrays.get(k)
         if a is None:
             continue
-        if a.dtype != dts[k] or not a.flags.c_contiguous:
-            raise TypeError(f"particle field {k}: need contiguous {np.dtype(dts[k])}, got {a.dtype}")
-        if n is not None and a.shape[0] != n:
-            raise ValueError(f"particle field {k}: {a.shape[0]} elements, expected {n}")
-        setattr(s, k, _ptr(a))
+        setattr(s, k, _field_ptr("particle", k, a, dts[k], n))
     return s
 
 
@@ -165,20 +180,12 @@ def link_soa(arrays: dict, precision: int, L: int | None = None) -> HidemLinkSoA
         a = arrays.get(k)
         if a is None:
             continue
-        if a.dtype != dts[k] or not a.flags.c_contiguous:
-            raise TypeError(f"link field {k}: need contiguous {np.dtype(dts[k])}, got {a.dtype}")
-        if L is not None and a.shape[0] != L:
-            raise ValueError(f"link field {k}: {a.shape[0]} elements, expected {L}")
-        setattr(s, k, _ptr(a))
+        setattr(s, k, _field_ptr("link", k, a, dts[k], L))
     for i, k in enumerate(SIDE_FIELDS):
         a = arrays.get(k)
         if a is None:
             continue
-        if a.dtype != dts[k] or not a.flags.c_contiguous:
-            raise TypeError(f"side field {k}: need contiguous {np.dtype(dts[k])}, got {a.dtype}")
-        if L is not None and a.shape[0] != 2 * L:
-            raise ValueError(f"side field {k}: {a.shape[0]} elements, expected {2 * L}")
-        s.CT[i] = _ptr(a)
+        s.CT[i] = _field_ptr("side", k, a, dts[k], None if L is None else 2 * L)
     return s
 
 
@@ -191,6 +198,20 @@ def empty_links(L: int, precision: int) -> dict:
     for k, dt in link_dtypes(precision).items():
         out[k] = np.zeros(2 * L if k in SIDE_FIELDS else L, dt)
     return out
+
+
+def empty_particles_torch(n: int, precision: int, device) -> dict:
+    """Particle fields as torch tensors on `device` (readback targets that stay there)."""
+    import torch
+    return {k: torch.empty(n, dtype=getattr(torch, np.dtype(dt).name), device=device)
+            for k, dt in particle_dtypes(precision).items()}
+
+
+def empty_links_torch(L: int, precision: int, device) -> dict:
+    import torch
+    return {k: torch.empty(2 * L if k in SIDE_FIELDS else L, dtype=getattr(torch, np.dtype(dt).name),
+                           device=device)
+            for k, dt in link_dtypes(precision).items()}
 
 
 _lib = None

@@ -53,6 +53,26 @@ inline void host_copy(void *dst, const void *src, size_t bytes) {
         std::memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, (size_t)(b - a));
     });
 }
+// whether a caller's array lives in device memory (which the host cannot read directly)
+inline bool on_device(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice;
+}
+// bytes between a caller's array (host or device memory) and host memory
+inline cudaError_t from_caller(void *hostDst, const void *src, size_t bytes) {
+    if (on_device(src)) return cudaMemcpy(hostDst, src, bytes, cudaMemcpyDeviceToHost);
+    host_copy(hostDst, src, bytes);
+    return cudaSuccess;
+}
+inline cudaError_t to_caller(void *dst, const void *hostSrc, size_t bytes) {
+    if (on_device(dst)) return cudaMemcpy(dst, hostSrc, bytes, cudaMemcpyHostToDevice);
+    host_copy(dst, hostSrc, bytes);
+    return cudaSuccess;
+}
 // per-thread text of the last failure of a call that has no context
 thread_local std::string g_nocontext_error;
 }  // namespace hidem
@@ -919,18 +939,18 @@ hidem_status upload_particles(hidem_ctx *ctx, const hidem_particle_soa *p, long 
     cudaStream_t st = ctx->stream;
     // stage the caller's arrays in the second record buffer, pack into the first
     SoaIn<LP> s = soa_layout<LP>(ctx->rec[1], n);
-    CK(cudaMemcpyAsync((void *)s.x, p->xCord, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync((void *)s.y, p->yCord, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync((void *)s.z, p->zCord, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)s.x, p->xCord, 8 * (size_t)n, cudaMemcpyDefault, st));
+    CK(cudaMemcpyAsync((void *)s.y, p->yCord, 8 * (size_t)n, cudaMemcpyDefault, st));
+    CK(cudaMemcpyAsync((void *)s.z, p->zCord, 8 * (size_t)n, cudaMemcpyDefault, st));
     const void *d[6] = {p->xDiff, p->yDiff, p->zDiff, p->uDiff, p->vDiff, p->wDiff};
     const void *th[3] = {p->xTheta, p->yTheta, p->zTheta};
     for (int k = 0; k < 6; ++k) {
-        if (d[k]) CK(cudaMemcpyAsync((void *)s.d[k], d[k], sizeof(LP) * (size_t)n, cudaMemcpyHostToDevice, st));
+        if (d[k]) CK(cudaMemcpyAsync((void *)s.d[k], d[k], sizeof(LP) * (size_t)n, cudaMemcpyDefault, st));
         else s.d[k] = nullptr;
     }
-    CK(cudaMemcpyAsync((void *)s.r, p->radius, sizeof(LP) * (size_t)n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void *)s.r, p->radius, sizeof(LP) * (size_t)n, cudaMemcpyDefault, st));
     for (int k = 0; k < 3; ++k) {
-        if (th[k]) CK(cudaMemcpyAsync((void *)s.th[k], th[k], sizeof(LP) * (size_t)n, cudaMemcpyHostToDevice, st));
+        if (th[k]) CK(cudaMemcpyAsync((void *)s.th[k], th[k], sizeof(LP) * (size_t)n, cudaMemcpyDefault, st));
         else s.th[k] = nullptr;
     }
     launch_pack_records<LP>(s, (int)n, static_cast<PRec<LP> *>(ctx->rec[0]), st);
@@ -1662,7 +1682,7 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     ctx->ord = 0;
     TRY(ctx->mixed ? upload_particles<float>(ctx, p, n) : upload_particles<double>(ctx, p, n));
     if (p->type)
-        CK(cudaMemcpyAsync(ctx->type[0], p->type, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->type[0], p->type, (size_t)n, cudaMemcpyDefault, ctx->stream));
     else
         CK(cudaMemsetAsync(ctx->type[0], 0, (size_t)n, ctx->stream));
     launch_iota32(ctx->orig[0], (int)n, ctx->stream);
@@ -1671,9 +1691,9 @@ hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, in
     CK(cudaMemsetAsync(ctx->counts, 0, 4 * (size_t)n, ctx->stream));
     CK(cudaMemsetAsync(ctx->force, 0, 6 * lp * (size_t)n, ctx->stream));
     ctx->owners.assign((size_t)n, 0);
-    if (p->owners) host_copy(ctx->owners.data(), p->owners, 4 * (size_t)n);
+    if (p->owners) CK(from_caller(ctx->owners.data(), p->owners, 4 * (size_t)n));
     ctx->keys.resize((size_t)n);
-    if (p->globalKeys) host_copy(ctx->keys.data(), p->globalKeys, 8 * (size_t)n);
+    if (p->globalKeys) CK(from_caller(ctx->keys.data(), p->globalKeys, 8 * (size_t)n));
     else for (int64_t i = 0; i < n; ++i) ctx->keys[i] = i;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
@@ -1720,8 +1740,8 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     TRY(dalloc(ctx, &ctx->dLinkKeyA, L));
     TRY(dalloc(ctx, &ctx->dLinkKeyB, L));
     if (L > 0) {
-        CK(cudaMemcpyAsync(ctx->dLinkKeyA, l->globalKeyEndA, 8 * (size_t)L, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(ctx->dLinkKeyB, l->globalKeyEndB, 8 * (size_t)L, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->dLinkKeyA, l->globalKeyEndA, 8 * (size_t)L, cudaMemcpyDefault, st));
+        CK(cudaMemcpyAsync(ctx->dLinkKeyB, l->globalKeyEndB, 8 * (size_t)L, cudaMemcpyDefault, st));
     }
     long long bad = -1, self = -1;
     if (identity) {
@@ -1737,6 +1757,19 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
         if (h[0] != ~0ull) bad = (long long)h[0];
         if (h[1] != ~0ull) self = (long long)h[1];
     } else {
+        // the caller's keys, where the host can read them
+        std::vector<int64_t> hostKeyA, hostKeyB;
+        const int64_t *keyA = l->globalKeyEndA, *keyB = l->globalKeyEndB;
+        if (L > 0 && on_device(keyA)) {
+            hostKeyA.resize((size_t)L);
+            CK(cudaMemcpy(hostKeyA.data(), keyA, 8 * (size_t)L, cudaMemcpyDeviceToHost));
+            keyA = hostKeyA.data();
+        }
+        if (L > 0 && on_device(keyB)) {
+            hostKeyB.resize((size_t)L);
+            CK(cudaMemcpy(hostKeyB.data(), keyB, 8 * (size_t)L, cudaMemcpyDeviceToHost));
+            keyB = hostKeyB.data();
+        }
         std::vector<std::pair<int64_t, int32_t>> km((size_t)n);
         for (long long i = 0; i < n; ++i) km[i] = {ctx->keys[i], (int32_t)i};
         std::sort(km.begin(), km.end());
@@ -1749,8 +1782,8 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
         std::unique_ptr<int32_t[]> B(new int32_t[(size_t)std::max<long long>(L, 1)]);
 #pragma omp parallel for schedule(static)
         for (long long i = 0; i < L; ++i) {
-            A[i] = find(l->globalKeyEndA[i]);
-            B[i] = find(l->globalKeyEndB[i]);
+            A[i] = find(keyA[i]);
+            B[i] = find(keyB[i]);
             if (A[i] < 0 || B[i] < 0) {
 #pragma omp critical
                 if (bad < 0 || i < bad) bad = i;
@@ -1765,9 +1798,13 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
             CK(cudaStreamSynchronize(st));
         }
     }
-    if (bad >= 0)
+    if (bad >= 0) {
+        int64_t ka = 0, kb = 0;
+        CK(from_caller(&ka, l->globalKeyEndA + bad, 8));
+        CK(from_caller(&kb, l->globalKeyEndB + bad, 8));
         return fail(ctx, HIDEM_ERR_NOT_FOUND, "link %lld: dangling end (keys %lld, %lld)", bad,
-                    (long long)l->globalKeyEndA[bad], (long long)l->globalKeyEndB[bad]);
+                    (long long)ka, (long long)kb);
+    }
     if (self >= 0) return fail(ctx, HIDEM_ERR_ARG, "link %lld joins a particle to itself", self);
 
     TRY(dalloc_bytes(ctx, &ctx->L0link, lp * (size_t)std::max<long long>(L, 1)));
@@ -1793,11 +1830,11 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     CK(cudaMemsetAsync(deg, 0, 4 * (size_t)(n + 1), st));
     CK(cudaMemsetAsync(cursor, 0, 4 * (size_t)(n + 1), st));
     if (L > 0) {
-        CK(cudaMemcpyAsync(ctx->L0link, l->initialLen, lp * (size_t)L, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(lstate, l->state, (size_t)L, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->L0link, l->initialLen, lp * (size_t)L, cudaMemcpyDefault, st));
+        CK(cudaMemcpyAsync(lstate, l->state, (size_t)L, cudaMemcpyDefault, st));
         for (int k = 0; k < 6; ++k) {
             if (l->CT[k])
-                CK(cudaMemcpyAsync(ctx->side[0].ct[k], l->CT[k], lp * (size_t)(2 * L), cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(ctx->side[0].ct[k], l->CT[k], lp * (size_t)(2 * L), cudaMemcpyDefault, st));
             else
                 CK(cudaMemsetAsync(ctx->side[0].ct[k], 0, lp * (size_t)(2 * L), st));
         }
@@ -1813,11 +1850,11 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     TRY(dalloc(ctx, &ctx->dLinkNum, L));
     TRY(dalloc(ctx, &ctx->dLinkKeys, L));
     if (L > 0) {
-        if (l->owners) CK(cudaMemcpyAsync(ctx->dLinkOwners, l->owners, 4 * (size_t)L, cudaMemcpyHostToDevice, st));
+        if (l->owners) CK(cudaMemcpyAsync(ctx->dLinkOwners, l->owners, 4 * (size_t)L, cudaMemcpyDefault, st));
         else CK(cudaMemsetAsync(ctx->dLinkOwners, 0, 4 * (size_t)L, st));
-        if (l->particleLinkNum) CK(cudaMemcpyAsync(ctx->dLinkNum, l->particleLinkNum, 4 * (size_t)L, cudaMemcpyHostToDevice, st));
+        if (l->particleLinkNum) CK(cudaMemcpyAsync(ctx->dLinkNum, l->particleLinkNum, 4 * (size_t)L, cudaMemcpyDefault, st));
         else CK(cudaMemsetAsync(ctx->dLinkNum, 0, 4 * (size_t)L, st));
-        if (l->globalKeys) CK(cudaMemcpyAsync(ctx->dLinkKeys, l->globalKeys, 8 * (size_t)L, cudaMemcpyHostToDevice, st));
+        if (l->globalKeys) CK(cudaMemcpyAsync(ctx->dLinkKeys, l->globalKeys, 8 * (size_t)L, cudaMemcpyDefault, st));
         else launch_iota64(ctx->dLinkKeys, L, st);
     }
     CK(cudaStreamSynchronize(st));
@@ -2108,22 +2145,22 @@ hidem_status hidem_get_particles(hidem_ctx *ctx, hidem_particle_soa *out) {
     const char *b = static_cast<const char *>(stage);
     double *xyz[3] = {out->xCord, out->yCord, out->zCord};
     for (int k = 0; k < 3; ++k)
-        if (xyz[k]) CK(cudaMemcpyAsync(xyz[k], b + 8 * (size_t)n * k, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
+        if (xyz[k]) CK(cudaMemcpyAsync(xyz[k], b + 8 * (size_t)n * k, 8 * (size_t)n, cudaMemcpyDefault, st));
     const char *lpb = b + 24 * (size_t)n;
     void *lpf[10] = {out->xDiff, out->yDiff, out->zDiff, out->uDiff, out->vDiff, out->wDiff,
                      out->radius, out->xTheta, out->yTheta, out->zTheta};
     for (int k = 0; k < 10; ++k)
-        if (lpf[k]) CK(cudaMemcpyAsync(lpf[k], lpb + lp * (size_t)n * k, lp * (size_t)n, cudaMemcpyDeviceToHost, st));
+        if (lpf[k]) CK(cudaMemcpyAsync(lpf[k], lpb + lp * (size_t)n * k, lp * (size_t)n, cudaMemcpyDefault, st));
     if (out->type) {
         // the type bytes in caller order, staged in the rebuild's permutation scratch
         uint8_t *tstage = reinterpret_cast<uint8_t *>(ctx->perm);
         launch_scatter_u8(ctx->type[ctx->ord], ctx->orig[ctx->ord], (int)n, tstage, st);
         ctx->launches += 1;
-        CK(cudaMemcpyAsync(out->type, tstage, (size_t)n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(out->type, tstage, (size_t)n, cudaMemcpyDefault, st));
     }
     // the host-held fields while the copies run
-    if (out->owners) host_copy(out->owners, ctx->owners.data(), 4 * (size_t)n);
-    if (out->globalKeys) host_copy(out->globalKeys, ctx->keys.data(), 8 * (size_t)n);
+    if (out->owners) CK(to_caller(out->owners, ctx->owners.data(), 4 * (size_t)n));
+    if (out->globalKeys) CK(to_caller(out->globalKeys, ctx->keys.data(), 8 * (size_t)n));
     CK(cudaStreamSynchronize(st));
     return HIDEM_OK;
 }
@@ -2149,7 +2186,7 @@ hidem_status hidem_get_links(hidem_ctx *ctx, hidem_link_soa *out) {
             launch_gather_sides<float>(slot, L, static_cast<const float *>(s.ct[k]), static_cast<float *>(stage), nullptr, nullptr, st);
         else
             launch_gather_sides<double>(slot, L, static_cast<const double *>(s.ct[k]), static_cast<double *>(stage), nullptr, nullptr, st);
-        CK(cudaMemcpyAsync(out->CT[k], stage, lp * (size_t)(2 * L), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(out->CT[k], stage, lp * (size_t)(2 * L), cudaMemcpyDefault, st));
         ctx->launches += 1;
     }
     if (out->state) {
@@ -2157,15 +2194,15 @@ hidem_status hidem_get_links(hidem_ctx *ctx, hidem_link_soa *out) {
             launch_gather_sides<float>(slot, L, nullptr, nullptr, s.state, lstate, st);
         else
             launch_gather_sides<double>(slot, L, nullptr, nullptr, s.state, lstate, st);
-        CK(cudaMemcpyAsync(out->state, lstate, (size_t)L, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(out->state, lstate, (size_t)L, cudaMemcpyDefault, st));
         ctx->launches += 1;
     }
-    if (out->initialLen) CK(cudaMemcpyAsync(out->initialLen, ctx->L0link, lp * (size_t)L, cudaMemcpyDeviceToHost, st));
-    if (out->owners) CK(cudaMemcpyAsync(out->owners, ctx->dLinkOwners, 4 * (size_t)L, cudaMemcpyDeviceToHost, st));
-    if (out->globalKeys) CK(cudaMemcpyAsync(out->globalKeys, ctx->dLinkKeys, 8 * (size_t)L, cudaMemcpyDeviceToHost, st));
-    if (out->globalKeyEndA) CK(cudaMemcpyAsync(out->globalKeyEndA, ctx->dLinkKeyA, 8 * (size_t)L, cudaMemcpyDeviceToHost, st));
-    if (out->globalKeyEndB) CK(cudaMemcpyAsync(out->globalKeyEndB, ctx->dLinkKeyB, 8 * (size_t)L, cudaMemcpyDeviceToHost, st));
-    if (out->particleLinkNum) CK(cudaMemcpyAsync(out->particleLinkNum, ctx->dLinkNum, 4 * (size_t)L, cudaMemcpyDeviceToHost, st));
+    if (out->initialLen) CK(cudaMemcpyAsync(out->initialLen, ctx->L0link, lp * (size_t)L, cudaMemcpyDefault, st));
+    if (out->owners) CK(cudaMemcpyAsync(out->owners, ctx->dLinkOwners, 4 * (size_t)L, cudaMemcpyDefault, st));
+    if (out->globalKeys) CK(cudaMemcpyAsync(out->globalKeys, ctx->dLinkKeys, 8 * (size_t)L, cudaMemcpyDefault, st));
+    if (out->globalKeyEndA) CK(cudaMemcpyAsync(out->globalKeyEndA, ctx->dLinkKeyA, 8 * (size_t)L, cudaMemcpyDefault, st));
+    if (out->globalKeyEndB) CK(cudaMemcpyAsync(out->globalKeyEndB, ctx->dLinkKeyB, 8 * (size_t)L, cudaMemcpyDefault, st));
+    if (out->particleLinkNum) CK(cudaMemcpyAsync(out->particleLinkNum, ctx->dLinkNum, 4 * (size_t)L, cudaMemcpyDefault, st));
     CK(cudaStreamSynchronize(st));
     dfree(stage);
     dfree(lstate);

@@ -276,11 +276,26 @@ class HiDEMLib:
         self._check(self._lib.hidem_get_particles(self._ctx, C.byref(soa)))
         return out
 
-    def get_links(self) -> dict:
-        out = abi.empty_links(self.L, self.precision)
+    def get_links(self, out: dict | None = None) -> dict:
+        if out is None:
+            out = abi.empty_links(self.L, self.precision)
         soa = abi.link_soa(out, self.precision, self.L)
         self._check(self._lib.hidem_get_links(self._ctx, C.byref(soa)))
         return out
+
+    def get_particles_device(self, fields=None) -> dict:
+        """Particle state in input order as torch tensors on the context's GPU (copied on
+        the device); only `fields` when given."""
+        import torch
+        out = abi.empty_particles_torch(self.n, self.precision, torch.device("cuda", self.device))
+        if fields is not None:
+            out = {k: out[k] for k in fields}
+        return self.get_particles(out)
+
+    def get_links_device(self) -> dict:
+        """Link state in input order as torch tensors on the context's GPU."""
+        import torch
+        return self.get_links(abi.empty_links_torch(self.L, self.precision, torch.device("cuda", self.device)))
 
     def get_forces(self) -> np.ndarray:
         f = np.zeros((6, self.n), self.lp)

@@ -225,6 +225,10 @@ class LocalComm:
     def allgather(self, objs: list) -> list:
         return list(objs)
 
+    def exchange_tensors(self, sends: dict, recv_sizes: dict, devices: list) -> dict:
+        """Byte buffers keyed (source, destination) between ranks of this process."""
+        return _local_exchange_tensors(sends, recv_sizes, devices, self.ranks)
+
     def exchange(self, layout: SlabLayout, send_bufs: list, recv_bufs: list) -> None:
         """recv_bufs[s]'s run from r <- send_bufs[r]'s run for s (torch tensors). Device
         buffers are copied on the devices' current streams, which the caller orders between
@@ -239,6 +243,18 @@ class LocalComm:
                     src = send_bufs[r][6 * soff[r][s]: 6 * (soff[r][s] + cnt)]
                     dst = recv_bufs[s][6 * roff[s][r]: 6 * (roff[s][r] + cnt)]
                     dst.copy_(src, non_blocking=False)
+
+
+def _local_exchange_tensors(sends: dict, recv_sizes: dict, devices: list, ranks: list) -> dict:
+    """Every send is to a rank of this process: the destination's device gets the buffer."""
+    dev_of = dict(zip(ranks, devices))
+    out = {}
+    for (s, r), n in recv_sizes.items():
+        buf = sends[(s, r)]
+        if buf.numel() != n:
+            raise RuntimeError(f"redistribution buffer {s} -> {r}: {buf.numel()} bytes, expected {n}")
+        out[(s, r)] = buf.to(dev_of[r])
+    return out
 
 
 class DistComm:
@@ -266,6 +282,28 @@ class DistComm:
         out = [None] * self.size
         self.dist.all_gather_object(out, objs[0])
         return out
+
+    def exchange_tensors(self, sends: dict, recv_sizes: dict, devices: list) -> dict:
+        """Byte buffers keyed (source, destination): this rank's sends to the other ranks,
+        its receives from them, point to point (NCCL moves device tensors between GPUs;
+        gloo host tensors). Both sides know every size, so no size travels first."""
+        import torch
+        dev = self._dev()
+        r = self.ranks[0]
+        ops, out = [], {}
+        for (s, d), buf in sorted(sends.items()):
+            ops.append(self.dist.P2POp(self.dist.isend, buf.to(dev), d))
+        for (s, d), n in sorted(recv_sizes.items()):
+            t = torch.empty(n, dtype=torch.uint8, device=dev)
+            out[(s, d)] = t
+            ops.append(self.dist.P2POp(self.dist.irecv, t, s))
+        if ops:
+            for w in self.dist.batch_isend_irecv(ops):
+                w.wait()
+        if dev.type == "cuda":
+            torch.cuda.current_stream(dev).synchronize()
+        target = devices[0] if devices else dev
+        return {k: v.to(target) for k, v in out.items()}
 
     def exchange(self, layout: SlabLayout, send_bufs: list, recv_bufs: list) -> None:
         r = self.ranks[0]
@@ -337,13 +375,20 @@ class SlabRun:
         import torch
         self.send_bufs, self.recv_bufs = [], []
         self._x0 = []
+        if any(hasattr(p["xCord"], "is_cuda") and p["xCord"].is_cuda for p, _ in states):
+            torch.cuda.synchronize()  # device arrays are complete before the library reads them
         for lib, r, (p, l) in zip(self.libs, self.comm.ranks, states):
-            self._x0.append(p["xCord"].copy())
+            dev = _lib_device(lib)
+            x = p["xCord"]
+            if dev.type == "cuda" and hasattr(lib, "get_particles_device"):
+                # the x at distribution, where the moved-distance check reads it back
+                self._x0.append(torch.as_tensor(x).to(dev).clone())
+            else:
+                self._x0.append(x.clone() if hasattr(x, "clone") else x.copy())
             lib.set_particles(p)
             lib.set_links(l)
             snd, rcv = self.layout.send_list(r), self.layout.recv_list(r)
             lib.set_halo_exchange(snd, rcv)
-            dev = _lib_device(lib)
             self.send_bufs.append(torch.zeros(6 * max(1, snd.size), dtype=self._tdtype, device=dev))
             self.recv_bufs.append(torch.zeros(6 * max(1, rcv.size), dtype=self._tdtype, device=dev))
         self.redistributions += 1
@@ -359,6 +404,8 @@ class SlabRun:
         are exchanged; a side's history depends only on the two end records), so what a
         rank already holds stays as it is. The result equals splitting the gathered whole
         set by the new layout, array for array."""
+        if self._on_device():
+            return self._redistribute_device()
         old = self.layout
         R = self.comm.size
         states, mine = [], []
@@ -437,6 +484,147 @@ class SlabRun:
         self.layout = new
         self._install(out)
 
+    def _on_device(self) -> bool:
+        """Whether the redistribution can keep the state on the GPUs: contexts that read back
+        to device memory, halo buffers there, and a transport that moves device tensors."""
+        return (bool(self.send_bufs) and self.send_bufs[0].is_cuda
+                and all(hasattr(lib, "get_particles_device") for lib in self.libs)
+                and hasattr(self.comm, "exchange_tensors"))
+
+    def _moves(self, old: "SlabLayout", new: "SlabLayout", r: int, d: int):
+        """What rank r sends rank d at a redistribution from `old` to `new` — the particles d
+        did not hold and r owned, the links d did not hold whose end A r owned — as global
+        indices and as positions in r's old held arrays. Every process computes the same."""
+        need_p = np.setdiff1d(new.local[d], old.local[d], assume_unique=True)
+        need_p = need_p[old.owner[need_p] == r]
+        need_l = np.setdiff1d(new.links[d], old.links[d], assume_unique=True)
+        need_l = need_l[old.owner[self._a[need_l]] == r]
+        return need_p, old.local_index(r, need_p), need_l, np.searchsorted(old.links[r], need_l)
+
+    def _redistribute_device(self) -> None:
+        """_redistribute with the particle and link state kept in device memory: each
+        context reads its held set back into device arrays; the moves are gathered, packed
+        into one byte buffer per destination and sent by the transport's device exchange
+        (device copies between contexts of this process, NCCL point-to-point between
+        processes); the new held sets are assembled on the device and handed to the contexts
+        from there. Only the owned particles' x (for the new cut) and index arrays travel
+        through host memory."""
+        import torch
+        old = self.layout
+        R = self.comm.size
+        states, mine = [], []
+        for lib, r in zip(self.libs, self.comm.ranks):
+            p, l = lib.get_particles_device(), lib.get_links_device()
+            states.append((p, l))
+            own = old.owner[old.local[r]] == r
+            dev = p["xCord"].device
+            mine.append((old.local[r][own], p["xCord"][torch.from_numpy(np.flatnonzero(own)).to(dev)].cpu().numpy()))
+        x_all = np.empty(self.n, np.float64)
+        seen = np.zeros(self.n, bool)
+        for idx, x in self.comm.allgather(mine):
+            x_all[idx] = x
+            seen[idx] = True
+        if not seen.all():
+            raise RuntimeError("a particle has no owner")
+        new = slab_layout(x_all, self._a, self._b, R, self._width)
+        pkeys = sorted(states[0][0].keys())
+        lkeys = sorted(states[0][1].keys())
+        p_dt = {k: states[0][0][k].dtype for k in pkeys}
+        l_dt = {k: states[0][1][k].dtype for k in lkeys}
+
+        def nbytes(np_count, nl_count):
+            tot = 0
+            for k in pkeys:
+                tot += np_count * p_dt[k].itemsize
+            for k in lkeys:
+                tot += (2 if k in abi.SIDE_FIELDS else 1) * nl_count * l_dt[k].itemsize
+            return tot
+
+        # pack: one byte buffer per (source rank of this process, destination)
+        sends = {}
+        for (p, l), r in zip(states, self.comm.ranks):
+            dev = p["xCord"].device
+            for d in range(R):
+                if d == r:
+                    continue
+                need_p, pi, need_l, li = self._moves(old, new, r, d)
+                if need_p.size == 0 and need_l.size == 0:
+                    continue
+                pit = torch.from_numpy(pi.astype(np.int64)).to(dev)
+                lit = torch.from_numpy(li.astype(np.int64)).to(dev)
+                side = torch.stack([2 * lit, 2 * lit + 1], dim=1).reshape(-1)
+                parts = [p[k].index_select(0, pit).view(torch.uint8) for k in pkeys]
+                parts += [l[k].index_select(0, side if k in abi.SIDE_FIELDS else lit).view(torch.uint8)
+                          for k in lkeys]
+                sends[(r, d)] = torch.cat(parts)
+        # what each rank of this process receives, and its size
+        recv_sizes = {}
+        for r in self.comm.ranks:
+            for s_ in range(R):
+                if s_ == r:
+                    continue
+                need_p, _, need_l, _ = self._moves(old, new, s_, r)
+                if need_p.size or need_l.size:
+                    recv_sizes[(s_, r)] = (need_p, need_l, nbytes(need_p.size, need_l.size))
+        got = self.comm.exchange_tensors(sends, {k: v[2] for k, v in recv_sizes.items()},
+                                         [st[0]["xCord"].device for st in states])
+        # assemble each rank's new held set on its device
+        out = []
+        for (p, l), r in zip(states, self.comm.ranks):
+            dev = p["xCord"].device
+            gp, gl = new.local[r], new.links[r]
+            np_ = {k: torch.zeros(gp.size, dtype=p_dt[k], device=dev) for k in pkeys}
+            nl = {k: torch.zeros((2 if k in abi.SIDE_FIELDS else 1) * gl.size, dtype=l_dt[k], device=dev)
+                  for k in lkeys}
+            pos = np.minimum(np.searchsorted(old.local[r], gp), max(old.local[r].size - 1, 0))
+            kept = old.local[r][pos] == gp if old.local[r].size else np.zeros(gp.size, bool)
+            at_t = torch.from_numpy(np.flatnonzero(kept)).to(dev)
+            from_t = torch.from_numpy(pos[kept].astype(np.int64)).to(dev)
+            for k in pkeys:
+                np_[k][at_t] = p[k].index_select(0, from_t)
+            lpos = np.minimum(np.searchsorted(old.links[r], gl), max(old.links[r].size - 1, 0))
+            lkept = old.links[r][lpos] == gl if old.links[r].size else np.zeros(gl.size, bool)
+            lat = torch.from_numpy(np.flatnonzero(lkept)).to(dev)
+            lfrom = torch.from_numpy(lpos[lkept].astype(np.int64)).to(dev)
+            lat2 = torch.stack([2 * lat, 2 * lat + 1], dim=1).reshape(-1)
+            lfrom2 = torch.stack([2 * lfrom, 2 * lfrom + 1], dim=1).reshape(-1)
+            for k in lkeys:
+                if k in abi.SIDE_FIELDS:
+                    nl[k][lat2] = l[k].index_select(0, lfrom2)
+                else:
+                    nl[k][lat] = l[k].index_select(0, lfrom)
+            got_p, got_l = kept.copy(), lkept.copy()
+            for s_ in range(R):
+                if (s_, r) not in recv_sizes:
+                    continue
+                need_p, need_l, _ = recv_sizes[(s_, r)]
+                buf = got[(s_, r)]
+                off = 0
+                at = torch.from_numpy(np.searchsorted(gp, need_p)).to(dev)
+                for k in pkeys:
+                    nb = need_p.size * p_dt[k].itemsize
+                    np_[k][at] = buf[off: off + nb].view(p_dt[k])
+                    off += nb
+                lat = torch.from_numpy(np.searchsorted(gl, need_l)).to(dev)
+                lat2 = torch.stack([2 * lat, 2 * lat + 1], dim=1).reshape(-1)
+                for k in lkeys:
+                    m = (2 if k in abi.SIDE_FIELDS else 1) * need_l.size
+                    nb = m * l_dt[k].itemsize
+                    vals = buf[off: off + nb].view(l_dt[k])
+                    if k in abi.SIDE_FIELDS:
+                        nl[k][lat2] = vals
+                    else:
+                        nl[k][lat] = vals
+                    off += nb
+                got_p[np.searchsorted(gp, need_p)] = True
+                got_l[np.searchsorted(gl, need_l)] = True
+            if not (got_p.all() and got_l.all()):
+                raise RuntimeError(f"rank {r}: particles or links missing after the redistribution")
+            np_["owners"] = torch.from_numpy(new.owner[gp].astype(np.int32)).to(dev)
+            out.append((np_, nl))
+        self.layout = new
+        self._install(out)
+
     def gather(self) -> tuple[dict, dict]:
         """The whole set's particles and links (every process gets them)."""
         mine = [(lib.get_particles(), lib.get_links()) for lib in self.libs]
@@ -464,8 +652,7 @@ class SlabRun:
         # distribution (partners lie within the reach; each end moved at most that much):
         # then the rebuild keeps the held sets, else every particle goes to the owner of
         # its slab, the slabs are recut and the halos rebuilt.
-        moved = [np.array([float(np.max(np.abs(lib.get_particles()["xCord"] - x0))) if x0.size else 0.0])
-                 for lib, x0 in zip(self.libs, self._x0)]
+        moved = [np.array([_max_moved(lib, x0)]) for lib, x0 in zip(self.libs, self._x0)]
         delta = float(self.comm.allmax(moved)[0])
         if 2.0 * delta > self._width - self._reach:
             self._redistribute()
@@ -531,6 +718,16 @@ class SlabRun:
         for lib in self.libs:
             lib.synchronize()
 
+
+
+def _max_moved(lib, x0) -> float:
+    """The largest |x - x0| over a context's held particles, on the device when x0 is there."""
+    if x0.shape[0] == 0:
+        return 0.0
+    if hasattr(x0, "is_cuda") and x0.is_cuda:
+        x = lib.get_particles_device(fields=["xCord"])["xCord"]
+        return float((x - x0).abs().max().item())
+    return float(np.max(np.abs(lib.get_particles()["xCord"] - x0)))
 
 
 def _lib_device(lib):

@@ -155,7 +155,12 @@ const char *hidem_create_error(void);
 int hidem_abi_version(void);
 
 /* Replaces ParticleDataHandler::appendInitParticles / fromCheckpoint
- * (PLiB/ParticleDataHandler.h:215-267): copies n particles to the device. */
+ * (PLiB/ParticleDataHandler.h:215-267): copies n particles to the device.
+ * The arrays of hidem_set_particles / hidem_set_links and of the readbacks
+ * hidem_get_particles / hidem_get_links may be host memory (pageable or pinned) or device
+ * memory of the context's GPU (the copies stay on the device); device arrays handed in must
+ * be complete when the call is made (the caller has synchronised the work that wrote
+ * them), and the readbacks' arrays are complete when the call returns. */
 hidem_status hidem_set_particles(hidem_ctx *ctx, const hidem_particle_soa *p, int64_t n);
 /* Replaces LinkDataHandler::appendInitLinks + LinkData::makeLocalPartEnds
  * (PLiB/LinkDataHandler.h:212-241, PLiB/LinkData.h:91-115): copies L links,

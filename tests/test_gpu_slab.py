@@ -52,6 +52,7 @@ def test_decomposed_run_matches_one_context(gpu, precision, name, nranks, slack)
     libs = [HiDEMLib(P) for _ in range(nranks)]
     try:
         run = slab.SlabRun(slab.LocalComm(nranks), libs, p, l, slack=slack)
+        assert run._on_device()  # redistributions keep the state on the GPU
         assert all(0 < lib.n < p["xCord"].shape[0] for lib in libs)
         run.step(steps)
         gp, gl = run.gather()
@@ -144,3 +145,41 @@ def test_pack_in_the_force_pass_equals_the_pack_kernel(gpu, precision, kernel):
                 lib.regenerate()
     for lib in libs:
         lib.close()
+
+
+@pytest.mark.parametrize("precision", PRECS)
+@pytest.mark.parametrize("keys", ["identity", "shuffled"])
+def test_state_from_and_to_device_arrays(gpu, precision, keys):
+    """hidem_set_particles / hidem_set_links from arrays in device memory and the readbacks
+    into device memory give the state the host arrays give, bit for bit; with global keys
+    that are not 0..n-1 the link ends are resolved through the host key table."""
+    import torch
+    P, p, l = workloads.ice_block(cells=(5, 4, 4), precision=precision, seed=21, fixed_bottom=False,
+                                  g=-9.81e4, waterLevel=-1e3, maxLoad=2e-5, breakTime=0.0)
+    if keys == "shuffled":
+        rng = np.random.default_rng(5)
+        perm = rng.permutation(p["xCord"].shape[0]).astype(np.int64) * 3 + 7
+        p = dict(p, globalKeys=perm)
+        l = dict(l, globalKeyEndA=perm[l["globalKeyEndA"]], globalKeyEndB=perm[l["globalKeyEndB"]])
+    dev = torch.device("cuda", 0)
+    tp = {k: torch.from_numpy(v).to(dev) for k, v in p.items()}
+    tl = {k: torch.from_numpy(v).to(dev) for k, v in l.items()}
+    torch.cuda.synchronize()
+    a, b = HiDEMLib(P), HiDEMLib(P)
+    try:
+        a.set_particles(p)
+        a.set_links(l)
+        b.set_particles(tp)
+        b.set_links(tl)
+        for lib in (a, b):
+            lib.step(25)
+        ha, hl = a.get_particles(), a.get_links()
+        db, dl = b.get_particles_device(), b.get_links_device()
+        for k, v in ha.items():
+            assert np.array_equal(db[k].cpu().numpy(), v), k
+        for k, v in hl.items():
+            assert np.array_equal(dl[k].cpu().numpy(), v), k
+        assert (hl["state"] == 0).any()  # links broke in the run
+    finally:
+        a.close()
+        b.close()
