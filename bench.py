@@ -1075,12 +1075,16 @@ def main_ranks(args):
     launches = sum(int(b["kernel_launches"] - a["kernel_launches"]) for a, b in zip(st0, st1))
     # one redistribution of the current state, outside the timed steps: what it costs to
     # recut the slabs and move what changes hands (wall time, every rank)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    run._redistribute()
-    for lib in libs:
-        lib.synchronize()
-    redist_s = time.perf_counter() - t0
+    redist_s = {}
+    for mode in (True, False):
+        run.device_redistribution = mode
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run._redistribute()
+        for lib in libs:
+            lib.synchronize()
+        redist_s["device" if mode else "host"] = time.perf_counter() - t0
+    run.device_redistribution = True
     if rank == 0:
         lay = run.layout
         halo = int(sum(len(lay.local[r]) for r in range(nranks)) - n)
@@ -1099,10 +1103,10 @@ def main_ranks(args):
                      "exchange_bytes_per_step": (run.exchanged - ex0) / max(args.steps, 1) * 6 * (4 if prec == abi.PREC_MIXED else 8),
                      "particles_held_per_rank": held if world == 1 else None},
             "redistributions_in_timed_steps": run.redistributions - red0,
-            "redistribution": {"seconds": redist_s, "on_device": run._on_device(),
-                               "what": "one recut of the current state after the timed steps: "
-                                       "held sets read back, moves packed and exchanged, new "
-                                       "held sets installed (their rebuild comes at the next step)"},
+            "redistribution_s": dict(redist_s, what="one recut of the current state after the timed "
+                                     "steps, with the state kept in device memory and through host "
+                                     "arrays: held sets read back, moves packed and exchanged, new "
+                                     "held sets installed (their rebuild comes at the next step)"),
             "one_context_ms_per_step": single or None,
             "gpu_launches": launches, "clocks": clk,
         }

@@ -336,7 +336,7 @@ class SlabRun:
     halo force exchange), applyForce, linkUpdate when t*dt > breakTime, finalizeTs."""
 
     def __init__(self, comm, libs: list, particles: dict, links: dict, halo: float | None = None,
-                 slack: float = 0.5):
+                 slack: float = 0.5, device_redistribution: bool = True):
         import torch
         if len(libs) != len(comm.ranks):
             raise ValueError("one context per rank of this process")
@@ -347,6 +347,9 @@ class SlabRun:
         self.lp = abi.lp_dtype(self.precision)
         self._tdtype = torch.float32 if self.lp == np.float32 else torch.float64
         self._halo, self._slack = halo, float(slack)
+        # redistribute with the state in device memory where the contexts and the transport
+        # allow it (else, or when False, through host arrays)
+        self.device_redistribution = bool(device_redistribution)
         self.redistributions = 0
         self.kept = 0           # rebuilds that kept the held sets (no redistribution)
         self.exchanged = 0      # halo force records moved so far (all ranks of this process)
@@ -487,7 +490,7 @@ class SlabRun:
     def _on_device(self) -> bool:
         """Whether the redistribution can keep the state on the GPUs: contexts that read back
         to device memory, halo buffers there, and a transport that moves device tensors."""
-        return (bool(self.send_bufs) and self.send_bufs[0].is_cuda
+        return (self.device_redistribution and bool(self.send_bufs) and self.send_bufs[0].is_cuda
                 and all(hasattr(lib, "get_particles_device") for lib in self.libs)
                 and hasattr(self.comm, "exchange_tensors"))
 
