@@ -494,16 +494,6 @@ class SlabRun:
                 and all(hasattr(lib, "get_particles_device") for lib in self.libs)
                 and hasattr(self.comm, "exchange_tensors"))
 
-    def _moves(self, old: "SlabLayout", new: "SlabLayout", r: int, d: int):
-        """What rank r sends rank d at a redistribution from `old` to `new` — the particles d
-        did not hold and r owned, the links d did not hold whose end A r owned — as global
-        indices and as positions in r's old held arrays. Every process computes the same."""
-        need_p = np.setdiff1d(new.local[d], old.local[d], assume_unique=True)
-        need_p = need_p[old.owner[need_p] == r]
-        need_l = np.setdiff1d(new.links[d], old.links[d], assume_unique=True)
-        need_l = need_l[old.owner[self._a[need_l]] == r]
-        return need_p, old.local_index(r, need_p), need_l, np.searchsorted(old.links[r], need_l)
-
     def _redistribute_device(self) -> None:
         """_redistribute with the particle and link state kept in device memory: each
         context reads its held set back into device arrays; the moves are gathered, packed
@@ -530,6 +520,27 @@ class SlabRun:
         if not seen.all():
             raise RuntimeError("a particle has no owner")
         new = slab_layout(x_all, self._a, self._b, R, self._width)
+        # what each rank held before (masks over the whole set) and, for this process's
+        # ranks, where each held particle / link sat in their arrays (inverse maps): every
+        # set difference and position below is one gather
+        held_p = [_mask(old.local[q], self.n) for q in range(R)]
+        held_l = [_mask(old.links[q], self.L) for q in range(R)]
+        inv_p = {r: _inverse(old.local[r], self.n) for r in self.comm.ranks}
+        inv_l = {r: _inverse(old.links[r], self.L) for r in self.comm.ranks}
+        owner_a = old.owner[self._a]
+        moves = {}
+
+        def move(r, d):
+            """What rank r sends rank d — the particles d did not hold and r owned, the
+            links d did not hold whose end A r owned — as whole-set indices; every process
+            computes the same."""
+            if (r, d) not in moves:
+                gp_, gl_ = new.local[d], new.links[d]
+                need_p = gp_[~held_p[d][gp_]]
+                need_l = gl_[~held_l[d][gl_]]
+                moves[(r, d)] = (need_p[old.owner[need_p] == r], need_l[owner_a[need_l] == r])
+            return moves[(r, d)]
+
         pkeys = sorted(states[0][0].keys())
         lkeys = sorted(states[0][1].keys())
         p_dt = {k: states[0][0][k].dtype for k in pkeys}
@@ -550,9 +561,10 @@ class SlabRun:
             for d in range(R):
                 if d == r:
                     continue
-                need_p, pi, need_l, li = self._moves(old, new, r, d)
+                need_p, need_l = move(r, d)
                 if need_p.size == 0 and need_l.size == 0:
                     continue
+                pi, li = inv_p[r][need_p], inv_l[r][need_l]
                 pit = torch.from_numpy(pi.astype(np.int64)).to(dev)
                 lit = torch.from_numpy(li.astype(np.int64)).to(dev)
                 side = torch.stack([2 * lit, 2 * lit + 1], dim=1).reshape(-1)
@@ -566,7 +578,7 @@ class SlabRun:
             for s_ in range(R):
                 if s_ == r:
                     continue
-                need_p, _, need_l, _ = self._moves(old, new, s_, r)
+                need_p, need_l = move(s_, r)
                 if need_p.size or need_l.size:
                     recv_sizes[(s_, r)] = (need_p, need_l, nbytes(need_p.size, need_l.size))
         got = self.comm.exchange_tensors(sends, {k: v[2] for k, v in recv_sizes.items()},
@@ -579,14 +591,14 @@ class SlabRun:
             np_ = {k: torch.zeros(gp.size, dtype=p_dt[k], device=dev) for k in pkeys}
             nl = {k: torch.zeros((2 if k in abi.SIDE_FIELDS else 1) * gl.size, dtype=l_dt[k], device=dev)
                   for k in lkeys}
-            pos = np.minimum(np.searchsorted(old.local[r], gp), max(old.local[r].size - 1, 0))
-            kept = old.local[r][pos] == gp if old.local[r].size else np.zeros(gp.size, bool)
+            pos = inv_p[r][gp]
+            kept = pos >= 0
             at_t = torch.from_numpy(np.flatnonzero(kept)).to(dev)
             from_t = torch.from_numpy(pos[kept].astype(np.int64)).to(dev)
             for k in pkeys:
                 np_[k][at_t] = p[k].index_select(0, from_t)
-            lpos = np.minimum(np.searchsorted(old.links[r], gl), max(old.links[r].size - 1, 0))
-            lkept = old.links[r][lpos] == gl if old.links[r].size else np.zeros(gl.size, bool)
+            lpos = inv_l[r][gl]
+            lkept = lpos >= 0
             lat = torch.from_numpy(np.flatnonzero(lkept)).to(dev)
             lfrom = torch.from_numpy(lpos[lkept].astype(np.int64)).to(dev)
             lat2 = torch.stack([2 * lat, 2 * lat + 1], dim=1).reshape(-1)
@@ -721,6 +733,19 @@ class SlabRun:
         for lib in self.libs:
             lib.synchronize()
 
+
+
+def _mask(idx: np.ndarray, size: int) -> np.ndarray:
+    m = np.zeros(size, bool)
+    m[idx] = True
+    return m
+
+
+def _inverse(idx: np.ndarray, size: int) -> np.ndarray:
+    """inv[idx[k]] = k, -1 elsewhere."""
+    inv = np.full(size, -1, np.int32)
+    inv[idx] = np.arange(idx.size, dtype=np.int32)
+    return inv
 
 
 def _max_moved(lib, x0) -> float:
