@@ -1722,17 +1722,20 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
     const long long n = ctx->n;
     const size_t lp = ctx->lp;
     // globalKey -> input index (LinkData::makeLocalPartEnds, PLiB/LinkData.h:91-115):
-    // on the device when the keys are 0..n-1 in order, else through a sorted key table on
-    // the host
-    bool identity = true;
+    // on the device when the keys are 0..n-1 in order or strictly ascending (a binary
+    // search of the key table), else through a sorted key table on the host
+    bool identity = true, ascending = true;
     {
-        std::atomic<bool> all(true);
+        std::atomic<bool> all(true), up(true);
         const int64_t *k = ctx->keys.data();
-        host_parallel(n, [&all, k](long long a, long long b) {
-            for (long long i = a; i < b && all.load(std::memory_order_relaxed); ++i)
+        host_parallel(n, [&all, &up, k](long long a, long long b) {
+            for (long long i = a; i < b && (all.load(std::memory_order_relaxed) || up.load(std::memory_order_relaxed)); ++i) {
                 if (k[i] != i) all.store(false, std::memory_order_relaxed);
+                if (i > 0 && !(k[i - 1] < k[i])) up.store(false, std::memory_order_relaxed);
+            }
         });
         identity = all.load();
+        ascending = up.load();
     }
     cudaStream_t st = ctx->stream;
     TRY(dalloc(ctx, &ctx->linkA, L));
@@ -1744,16 +1747,26 @@ hidem_status hidem_set_links(hidem_ctx *ctx, const hidem_link_soa *l, int64_t L)
         CK(cudaMemcpyAsync(ctx->dLinkKeyB, l->globalKeyEndB, 8 * (size_t)L, cudaMemcpyDefault, st));
     }
     long long bad = -1, self = -1;
-    if (identity) {
+    if (identity || ascending) {
         unsigned long long *mins = nullptr;
+        long long *dkeys = nullptr;
         TRY(dalloc(ctx, &mins, 2));
         CK(cudaMemsetAsync(mins, 0xff, 2 * sizeof(unsigned long long), st));
-        launch_link_keys_identity(ctx->dLinkKeyA, ctx->dLinkKeyB, L, n, ctx->linkA, ctx->linkB, mins,
-                                  mins + 1, st);
+        if (identity) {
+            launch_link_keys_identity(ctx->dLinkKeyA, ctx->dLinkKeyB, L, n, ctx->linkA, ctx->linkB, mins,
+                                      mins + 1, st);
+        } else {
+            TRY(dalloc(ctx, &dkeys, n));
+            CK(cudaMemcpyAsync(dkeys, ctx->keys.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, st));
+            launch_link_keys_sorted(dkeys, n, ctx->dLinkKeyA, ctx->dLinkKeyB, L, ctx->linkA, ctx->linkB,
+                                    mins, mins + 1, st);
+        }
+        ctx->launches += 1;
         unsigned long long h[2];
         CK(cudaMemcpyAsync(h, mins, sizeof h, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         dfree(mins);
+        if (dkeys) dfree(dkeys);
         if (h[0] != ~0ull) bad = (long long)h[0];
         if (h[1] != ~0ull) self = (long long)h[1];
     } else {

@@ -1915,6 +1915,45 @@ __global__ void k_link_keys_identity(const long long *__restrict__ ka, const lon
     }
 }
 
+// link ends from particle keys in strictly ascending order (not 0..n-1): each end's index
+// by a binary search of the key table
+__device__ __forceinline__ int find_key(const long long *__restrict__ keys, long long n, long long k) {
+    long long lo = 0, hi = n;  // first position with keys[pos] >= k
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (__ldg(keys + mid) < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && __ldg(keys + lo) == k) ? (int)lo : -1;
+}
+
+__global__ void k_link_keys_sorted(const long long *__restrict__ keys, long long n,
+                                   const long long *__restrict__ ka, const long long *__restrict__ kb,
+                                   long long L, int *__restrict__ A, int *__restrict__ B,
+                                   unsigned long long *badMin, unsigned long long *selfMin) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int a = find_key(keys, n, ka[i]), b = find_key(keys, n, kb[i]);
+        if (a < 0 || b < 0) {
+            atomicMin(badMin, (unsigned long long)i);
+            A[i] = 0;
+            B[i] = 0;
+            continue;
+        }
+        A[i] = a;
+        B[i] = b;
+        if (a == b) atomicMin(selfMin, (unsigned long long)i);
+    }
+}
+
+void launch_link_keys_sorted(const long long *keys, long long n, const long long *keyA,
+                             const long long *keyB, long long L, int *A, int *B,
+                             unsigned long long *badMin, unsigned long long *selfMin, cudaStream_t st) {
+    if (L <= 0) return;
+    const int nb = (int)std::min<long long>((L + 255) / 256, 148LL * 32);
+    k_link_keys_sorted<<<nb, 256, 0, st>>>(keys, n, keyA, keyB, L, A, B, badMin, selfMin);
+}
+
 __global__ void k_iota64(long long *out, long long count) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
          i += (long long)gridDim.x * blockDim.x)

@@ -73,6 +73,11 @@ void launch_side_init(const uint8_t *linkState, long long L, int *sideSlot, uint
 void launch_link_keys_identity(const long long *keyA, const long long *keyB, long long L,
                                long long n, int *A, int *B, unsigned long long *badMin,
                                unsigned long long *selfMin, cudaStream_t st);
+// the same from particle keys in strictly ascending order (keys: n device words): each end
+// found by binary search
+void launch_link_keys_sorted(const long long *keys, long long n, const long long *keyA,
+                             const long long *keyB, long long L, int *A, int *B,
+                             unsigned long long *badMin, unsigned long long *selfMin, cudaStream_t st);
 // out[i] = i (int64 / int32)
 void launch_iota64(long long *out, long long count, cudaStream_t st);
 void launch_iota32(int *out, int count, cudaStream_t st);

@@ -588,8 +588,9 @@ class SlabRun:
         for (p, l), r in zip(states, self.comm.ranks):
             dev = p["xCord"].device
             gp, gl = new.local[r], new.links[r]
-            np_ = {k: torch.zeros(gp.size, dtype=p_dt[k], device=dev) for k in pkeys}
-            nl = {k: torch.zeros((2 if k in abi.SIDE_FIELDS else 1) * gl.size, dtype=l_dt[k], device=dev)
+            # every position is filled below, from what was kept or what was received
+            np_ = {k: torch.empty(gp.size, dtype=p_dt[k], device=dev) for k in pkeys}
+            nl = {k: torch.empty((2 if k in abi.SIDE_FIELDS else 1) * gl.size, dtype=l_dt[k], device=dev)
                   for k in lkeys}
             pos = inv_p[r][gp]
             kept = pos >= 0

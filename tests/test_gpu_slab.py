@@ -148,17 +148,20 @@ def test_pack_in_the_force_pass_equals_the_pack_kernel(gpu, precision, kernel):
 
 
 @pytest.mark.parametrize("precision", PRECS)
-@pytest.mark.parametrize("keys", ["identity", "shuffled"])
+@pytest.mark.parametrize("keys", ["identity", "ascending", "shuffled"])
 def test_state_from_and_to_device_arrays(gpu, precision, keys):
     """hidem_set_particles / hidem_set_links from arrays in device memory and the readbacks
     into device memory give the state the host arrays give, bit for bit; with global keys
-    that are not 0..n-1 the link ends are resolved through the host key table."""
+    that are not 0..n-1 the link ends are resolved by a search of the key table (on the device
+    when the keys ascend, on the host otherwise)."""
     import torch
     P, p, l = workloads.ice_block(cells=(5, 4, 4), precision=precision, seed=21, fixed_bottom=False,
                                   g=-9.81e4, waterLevel=-1e3, maxLoad=2e-5, breakTime=0.0)
-    if keys == "shuffled":
+    if keys != "identity":
+        # keys in ascending order (ends found on the device) or shuffled (on the host)
         rng = np.random.default_rng(5)
-        perm = rng.permutation(p["xCord"].shape[0]).astype(np.int64) * 3 + 7
+        n = p["xCord"].shape[0]
+        perm = (np.arange(n) if keys == "ascending" else rng.permutation(n)).astype(np.int64) * 3 + 7
         p = dict(p, globalKeys=perm)
         l = dict(l, globalKeyEndA=perm[l["globalKeyEndA"]], globalKeyEndB=perm[l["globalKeyEndB"]])
     dev = torch.device("cuda", 0)
