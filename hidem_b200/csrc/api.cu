@@ -1109,7 +1109,8 @@ void batch_group(hidem_batch *b, int kernel) {
             g.maxE = std::max(g.maxE, (int)c->maxLinksPP);
         }
         g.count = (int)b->order.size() - g.first;
-        // a group without links still launches one break CTA: it advances the run counter
+        // a group without links still launches one (idle) break CTA: a launch of no CTAs is
+        // an error
         g.linkBlocks = std::max<long long>(g.linkBlocks, 1);
         fb += g.count + 1;
         b->groups.push_back(std::move(g));

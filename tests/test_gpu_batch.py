@@ -178,8 +178,8 @@ def test_batch_argument_errors(gpu):
 @pytest.mark.parametrize("with_links", [True, False])
 def test_batch_with_contexts_without_links(gpu, with_links):
     """Blocks whose link set is empty beside one with links, and (with_links False) a batch
-    in which no context has links: the break pass's own grid keeps one CTA to advance the
-    run counter, and every block matches its run alone."""
+    in which no context has links (the break pass's own grid keeps one idle CTA): every block
+    matches its run alone."""
     blocks = []
     for k, (cells, seed) in enumerate([((3, 3, 3), 21), ((4, 3, 3), 22), ((2, 3, 2), 23)]):
         P, p, l = workloads.ice_block(cells=cells, precision=abi.PREC_MIXED, seed=seed,
