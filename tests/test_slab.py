@@ -240,6 +240,46 @@ def test_driver_on_two_gloo_ranks_moves_every_halo_force():
     assert all(r[2] > 0 and r[3] > 0 for r in res)
 
 
+def _gloo_exchange_rank(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import torch
+        comm = slab.DistComm()
+        # rank r sends (r + 1) * 10 + d bytes of value 16 r + d to every other rank d
+        sends = {(rank, d): torch.full(((rank + 1) * 10 + d,), 16 * rank + d, dtype=torch.uint8)
+                 for d in range(world) if d != rank}
+        sizes = {(s_, rank): (s_ + 1) * 10 + rank for s_ in range(world) if s_ != rank}
+        got = comm.exchange_tensors(sends, sizes, [torch.device("cpu")])
+        ok = sorted(got) == sorted(sizes)
+        ok &= all(int(t.numel()) == sizes[k] and bool((t == 16 * k[0] + k[1]).all()) for k, t in got.items())
+        q.put((rank, ok))
+    except Exception as e:  # reported to the parent instead of a queue timeout
+        q.put((rank, repr(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_tensor_exchange_on_gloo_ranks(world):
+    """The redistribution's byte-buffer exchange between processes (point to point, every
+    size known to both sides) delivers each buffer to its destination intact."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gloo_exchange_rank, args=(r, world, port, q)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    res = sorted(q.get(timeout=180) for _ in procs)
+    for pr in procs:
+        pr.join(timeout=60)
+    assert [r[0] for r in res] == list(range(world))
+    assert all(r[1] is True for r in res), res
+
+
 @pytest.mark.parametrize("nranks", [2, 3, 4])
 def test_incremental_redistribution_equals_the_whole_set_split(nranks):
     """After a redistribution (every particle moved past the halo's room) each rank holds
