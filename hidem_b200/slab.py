@@ -123,6 +123,40 @@ def slab_layout(x: np.ndarray, link_a: np.ndarray, link_b: np.ndarray, nranks: i
     return SlabLayout(cuts=cuts, owner=owner, local=local, links=links, send=send)
 
 
+def slab_layout_torch(x, link_a, link_b, nranks: int, halo: float) -> SlabLayout:
+    """slab_layout computed with torch on the device the tensors live on (x float64[N],
+    link_a / link_b int64[L]); the same cuts, owners and index sets, returned as numpy."""
+    import torch
+    n = x.shape[0]
+    if nranks < 1:
+        raise ValueError("need at least one rank")
+    xs = torch.sort(x).values
+    inner = [float(xs[min(n - 1, (k * n) // nranks)]) for k in range(1, nranks)] if n else [0.0] * (nranks - 1)
+    cuts = np.array([-np.inf, *inner, np.inf])
+    cuts_t = torch.tensor(cuts, dtype=torch.float64, device=x.device)
+    owner = torch.searchsorted(cuts_t[1:-1].contiguous(), x, right=True).to(torch.int32)
+    oa, ob = owner[link_a], owner[link_b]
+    local, links, held_sets = [], [], []
+    for r in range(nranks):
+        near = (x >= cuts[r] - halo) & (x < cuts[r + 1] + halo)
+        mine = (oa == r) | (ob == r)
+        held = near | (owner == r)
+        held[link_a[mine]] = True
+        held[link_b[mine]] = True
+        loc = torch.nonzero(held).flatten()
+        held_sets.append(loc)
+        local.append(loc.cpu().numpy())
+        links.append(torch.nonzero(mine).flatten().cpu().numpy())
+    send = [[np.zeros(0, np.int64) for _ in range(nranks)] for _ in range(nranks)]
+    for s_ in range(nranks):
+        held = held_sets[s_]
+        ow = owner[held]
+        for r in range(nranks):
+            if r != s_:
+                send[r][s_] = held[ow == r].cpu().numpy()
+    return SlabLayout(cuts=cuts, owner=owner.cpu().numpy(), local=local, links=links, send=send)
+
+
 def key_index(keys: np.ndarray, wanted: np.ndarray) -> np.ndarray:
     """Positions of the particle keys `wanted` in `keys` (globalKey -> index)."""
     keys = np.asarray(keys, np.int64)
@@ -350,6 +384,7 @@ class SlabRun:
         # redistribute with the state in device memory where the contexts and the transport
         # allow it (else, or when False, through host arrays)
         self.device_redistribution = bool(device_redistribution)
+        self._a_dev = self._b_dev = None  # link ends on the device, for the device recut
         self.redistributions = 0
         self.kept = 0           # rebuilds that kept the held sets (no redistribution)
         self.exchanged = 0      # halo force records moved so far (all ranks of this process)
@@ -519,7 +554,11 @@ class SlabRun:
             seen[idx] = True
         if not seen.all():
             raise RuntimeError("a particle has no owner")
-        new = slab_layout(x_all, self._a, self._b, R, self._width)
+        dev0 = states[0][0]["xCord"].device
+        if self._a_dev is None or self._a_dev.device != dev0:
+            self._a_dev = torch.from_numpy(self._a).to(dev0)
+            self._b_dev = torch.from_numpy(self._b).to(dev0)
+        new = slab_layout_torch(torch.from_numpy(x_all).to(dev0), self._a_dev, self._b_dev, R, self._width)
         # what each rank held before (masks over the whole set) and, for this process's
         # ranks, where each held particle / link sat in their arrays (inverse maps): every
         # set difference and position below is one gather

@@ -299,3 +299,23 @@ def test_incremental_redistribution_equals_the_whole_set_split(nranks):
             assert np.array_equal(f.l[k], v), (r, k)
         assert np.array_equal(f.snd, run.layout.send_list(r))
         assert np.array_equal(f.rcv, run.layout.recv_list(r))
+
+
+@pytest.mark.parametrize("nranks", [1, 2, 3, 5])
+def test_layout_with_torch_equals_numpy(nranks):
+    """The recut computed with torch (on the device in a run; here on the host) gives the
+    numpy layout's cuts, owners and index sets exactly."""
+    import torch
+    P, p, l = _block()
+    a, b = slab.link_ends(p, l)
+    a, b = a.astype(np.int64), b.astype(np.int64)
+    x = p["xCord"] + np.random.default_rng(nranks).normal(0, 0.3, p["xCord"].shape[0])
+    want = slab.slab_layout(x, a, b, nranks, 1.3)
+    got = slab.slab_layout_torch(torch.from_numpy(x), torch.from_numpy(a), torch.from_numpy(b), nranks, 1.3)
+    assert np.array_equal(got.cuts, want.cuts)
+    assert np.array_equal(got.owner, want.owner)
+    for r in range(nranks):
+        assert np.array_equal(got.local[r], want.local[r])
+        assert np.array_equal(got.links[r], want.links[r])
+        for s_ in range(nranks):
+            assert np.array_equal(got.send[r][s_], want.send[r][s_])
