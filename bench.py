@@ -92,6 +92,8 @@ def parse():
                     help="slab with --gpus N > 1: N independent replicas instead of the x-slab decomposition")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-numa-bind", action="store_true",
+                    help="run the end-to-end job on every allowed CPU, not only the GPU's NUMA node")
     ap.add_argument("--no-fp64", action="store_true", help="slab: skip the plain-FP64 run")
     ap.add_argument("--no-settle", action="store_true", help="slab: skip the warm-start settling experiment")
     ap.add_argument("--amortised-steps", type=int, default=2000,
@@ -1295,10 +1297,46 @@ def main_slab(args):
     print(json.dumps(line))
 
 
+def gpu_local_cpus(device: int):
+    """The host CPUs next to the GPU (NVML's CPU affinity of the device: its NUMA node) that
+    this process may run on; None when NVML cannot tell or when they are all of them."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByIndex(device)
+        words = ((os.cpu_count() or 64) + 63) // 64
+        mask = pynvml.nvmlDeviceGetCpuAffinity(h, words)
+        cpus = {w * 64 + b for w, m in enumerate(mask) for b in range(64) if (int(m) >> b) & 1}
+        allowed = os.sched_getaffinity(0)
+        cpus &= allowed
+        return cpus if cpus and cpus != allowed else None
+    except Exception:
+        return None
+
+
 def e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n, start_step: int = 0):
     """The same K steps through the C ABI from pinned host buffers: upload of the particle
     and link state, K steps, download of the particle state; wall time, devices synchronised
     on both sides."""
+    import torch
+    from hidem_b200 import abi
+    from hidem_b200.hidemlib import HiDEMLib
+    # the job's host side on the CPUs next to the GPU, so that its pinned buffers sit in that
+    # NUMA node's memory and the copies do not cross between sockets (the affinity a serving
+    # process would take; restored after the job)
+    near = None if getattr(args, "no_numa_bind", False) else gpu_local_cpus(local)
+    prev = os.sched_getaffinity(0)
+    if near:
+        os.sched_setaffinity(0, near)
+    try:
+        return _e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n, start_step,
+                        len(near) if near else len(prev), bool(near))
+    finally:
+        if near:
+            os.sched_setaffinity(0, prev)
+
+
+def _e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n, start_step, host_cpus, bound):
     import torch
     from hidem_b200 import abi
     from hidem_b200.hidemlib import HiDEMLib
@@ -1368,7 +1406,8 @@ def e2e_job(args, P, p, l, prec, step_kernel, local, pg, world, n, start_step: i
             "warmup": "one untimed job (5 steps) before the timed one",
             "step": f"one C-ABI job from pinned host arrays: upload state (particles, links"
                     f"{'; side history zero, not uploaded' if fresh else ', side history'}), "
-                    f"{args.steps} timesteps, download particles", "breakdown": parts}
+                    f"{args.steps} timesteps, download particles", "breakdown": parts,
+            "host_cpus": host_cpus, "bound_to_gpu_numa_node": bound}
 
 
 def settle_summary(args) -> dict:
