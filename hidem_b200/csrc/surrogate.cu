@@ -976,6 +976,9 @@ __global__ void k_sum_splits(const float *__restrict__ part, int splits, long lo
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= count) return;
     float acc = 0.f;
+    // unrolled so that the loads of several splits are in flight at once (the sum stays in
+    // split order)
+#pragma unroll 8
     for (int s = 0; s < splits; ++s) acc += part[s * count + e];
     out[e] = acc;
 }
@@ -987,9 +990,11 @@ __global__ void k_colsum_bf16(const bf16 *__restrict__ A, int rows, int N, float
     const int c = blockIdx.x * 32 + threadIdx.x;
     const int r0 = blockIdx.y * kChunk;
     float acc = 0.f;
-    if (c < N)
-        for (int r = r0 + threadIdx.y; r < min(rows, r0 + kChunk); r += 8)
-            acc += __bfloat162float(A[(long long)r * N + c]);
+    if (c < N) {
+        const int r1 = min(rows, r0 + kChunk);
+#pragma unroll 8
+        for (int r = r0 + threadIdx.y; r < r1; r += 8) acc += __bfloat162float(A[(long long)r * N + c]);
+    }
     red[threadIdx.y][threadIdx.x] = acc;
     __syncthreads();
     if (threadIdx.y == 0 && c < N) {
@@ -1029,9 +1034,10 @@ __global__ void k_loss(const float *__restrict__ Y, const float *__restrict__ ta
 // dZ[b][k] = (sum_j dY[b][j] Wo[j][k]) * SiLU'(Z[b][k]), stored BF16
 __global__ void k_out_bwd(const float *__restrict__ dY, const float *__restrict__ Wo,
                           const float *__restrict__ Z, int rows, int W, bf16 *__restrict__ dZ) {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (long long)rows * W) return;
-    const int b = (int)(e / W), k = (int)(e % W);
+    // one CTA row per batch row (blockIdx.x), its columns over blockIdx.y
+    const int b = blockIdx.x, k = blockIdx.y * blockDim.x + threadIdx.x;
+    if (b >= rows || k >= W) return;
+    const long long e = (long long)b * W + k;
     float g = 0.f;
 #pragma unroll
     for (int j = 0; j < kOut; ++j) g += dY[(long long)b * kOut + j] * Wo[j * W + k];
@@ -1044,9 +1050,12 @@ __global__ void k_out_grad(const float *__restrict__ dY, const bf16 *__restrict_
                            float *__restrict__ part) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;  // 0..W (W = bias)
     if (k > W) return;
-    const int r0 = blockIdx.y * kChunk;
+    const int r0 = blockIdx.y * kChunk, r1 = min(rows, r0 + kChunk);
     float acc[kOut] = {0.f, 0.f, 0.f};
-    for (int b = r0; b < min(rows, r0 + kChunk); ++b) {
+    // unrolled so that the loads of several rows are in flight at once (the sums stay in
+    // row order)
+#pragma unroll 8
+    for (int b = r0; b < r1; ++b) {
         const float h = (k < W) ? __bfloat162float(H[(long long)b * W + k]) : 1.f;
 #pragma unroll
         for (int j = 0; j < kOut; ++j) acc[j] += dY[(long long)b * kOut + j] * h;
@@ -1360,9 +1369,8 @@ hidem_status backward(hidem_surrogate *s, int rows, const float *targets, const 
         SCK(cudaMemcpyAsync(s->G + s->offBo + j, outBlock + (long long)j * (W + 1) + W, sizeof(float),
                             cudaMemcpyDeviceToDevice, s->stream));
     }
-    const long long e = (long long)rows * W;
     bf16 *dZ = s->dZa, *dZn = s->dZb;
-    k_out_bwd<<<(unsigned)((e + 255) / 256), 256, 0, s->stream>>>(s->dY, s->P + s->offWo, s->Z[L - 1], rows, W, dZ);
+    k_out_bwd<<<dim3((unsigned)rows, (unsigned)((W + 255) / 256)), 256, 0, s->stream>>>(s->dY, s->P + s->offWo, s->Z[L - 1], rows, W, dZ);
     SCK(cudaGetLastError());
     // hidden layers, last to first
     for (int l = L - 1; l >= 0; --l) {
