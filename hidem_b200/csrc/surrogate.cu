@@ -955,18 +955,49 @@ __global__ void k_features(const float *__restrict__ in, const int *__restrict__
     for (int c = nin * (1 + 2 * bands) + threadIdx.x; c < K0; c += blockDim.x) x[c] = __float2bfloat16_rn(0.f);
 }
 
-// out[c][r] = in[r][c] for a [R][C] BF16 matrix (32 x 32 tiles through shared memory)
-__global__ void k_transpose(const bf16 *__restrict__ in, int R, int C, bf16 *__restrict__ out) {
-    __shared__ bf16 t[32][33];
-    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-        const int r = r0 + j, c = c0 + threadIdx.x;
-        if (r < R && c < C) t[j][threadIdx.x] = in[(long long)r * C + c];
+// out[c][r] = in[r][c] for a [R][C] BF16 matrix: 64 x 64 tiles through shared memory, 256
+// threads; rows are read and written as BF16 pairs (4-byte words, 128 bytes per warp), and the
+// tile's row pitch of 65 elements keeps both the pair writes and the column reads free of
+// bank conflicts. Odd R or C fall back to single elements at the edges they affect.
+constexpr int kTrTile = 64, kTrPitch = kTrTile + 1;
+__global__ void __launch_bounds__(256) k_transpose(const bf16 *__restrict__ in, int R, int C,
+                                                   bf16 *__restrict__ out) {
+    __shared__ bf16 t[kTrTile * kTrPitch];
+    const int c0 = blockIdx.x * kTrTile, r0 = blockIdx.y * kTrTile;
+    const bool evenC = (C & 1) == 0, evenR = (R & 1) == 0;
+    for (int k = threadIdx.x; k < kTrTile * (kTrTile / 2); k += blockDim.x) {
+        const int r = k >> 5, w = k & 31;
+        const int gr = r0 + r, gc = c0 + 2 * w;
+        bf16 a = __float2bfloat16_rn(0.f), b = a;
+        if (gr < R) {
+            const bf16 *src = in + (long long)gr * C + gc;
+            if (evenC && gc + 1 < C) {
+                const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162 *>(src);
+                a = v.x;
+                b = v.y;
+            } else {
+                if (gc < C) a = src[0];
+                if (gc + 1 < C) b = src[1];
+            }
+        }
+        t[r * kTrPitch + 2 * w] = a;
+        t[r * kTrPitch + 2 * w + 1] = b;
     }
     __syncthreads();
-    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-        const int c = c0 + j, r = r0 + threadIdx.x;
-        if (r < R && c < C) out[(long long)c * R + r] = t[threadIdx.x][j];
+    for (int k = threadIdx.x; k < kTrTile * (kTrTile / 2); k += blockDim.x) {
+        const int c = k >> 5, w = k & 31;
+        const int orow = c0 + c, ocol = r0 + 2 * w;
+        if (orow >= C || ocol >= R) continue;
+        __nv_bfloat162 v;
+        v.x = t[(2 * w) * kTrPitch + c];
+        v.y = t[(2 * w + 1) * kTrPitch + c];
+        bf16 *dst = out + (long long)orow * R + ocol;
+        if (evenR && ocol + 1 < R) {
+            *reinterpret_cast<__nv_bfloat162 *>(dst) = v;
+        } else {
+            dst[0] = v.x;
+            if (ocol + 1 < R) dst[1] = v.y;
+        }
     }
 }
 
@@ -1377,8 +1408,8 @@ hidem_status backward(hidem_surrogate *s, int rows, const float *targets, const 
         const int K = s->Kl[l];
         const bf16 *in = l == 0 ? s->X0 : s->H[l - 1];
         // dW_l = dZ^T * in: both operands transposed to K-major [.][rows], split over rows
-        k_transpose<<<dim3((W + 31) / 32, (rows + 31) / 32), dim3(32, 8), 0, s->stream>>>(dZ, rows, W, s->dZT);
-        k_transpose<<<dim3((K + 31) / 32, (rows + 31) / 32), dim3(32, 8), 0, s->stream>>>(in, rows, K, s->inT);
+        k_transpose<<<dim3((W + kTrTile - 1) / kTrTile, (rows + kTrTile - 1) / kTrTile), 256, 0, s->stream>>>(dZ, rows, W, s->dZT);
+        k_transpose<<<dim3((K + kTrTile - 1) / kTrTile, (rows + kTrTile - 1) / kTrTile), 256, 0, s->stream>>>(in, rows, K, s->inT);
         int splits = s->splits;
         while (splits > 1 && ((rows / 64) % splits)) splits >>= 1;
         STRY(ensure_part(s, (long long)splits * W * K));
