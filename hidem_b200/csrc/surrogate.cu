@@ -1001,37 +1001,57 @@ __global__ void __launch_bounds__(256) k_transpose(const bf16 *__restrict__ in, 
     }
 }
 
-// out[e] = sum over s (in order) of part[s * count + e]
-__global__ void k_sum_splits(const float *__restrict__ part, int splits, long long count,
-                             float *__restrict__ out) {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= count) return;
-    float acc = 0.f;
-    // unrolled so that the loads of several splits are in flight at once (the sum stays in
-    // split order)
-#pragma unroll 8
-    for (int s = 0; s < splits; ++s) acc += part[s * count + e];
-    out[e] = acc;
-}
-
-// Column sums of a BF16 [rows][N] matrix over row chunks of kChunk: part[chunk][N]
-constexpr int kChunk = 256;
-__global__ void k_colsum_bf16(const bf16 *__restrict__ A, int rows, int N, float *__restrict__ part) {
+// out[e] = sum over s of part[s * count + e]: a block of 32 x 8 threads per 32 elements, the
+// 8 thread rows summing every 8th split (their loads of 32 consecutive elements coalesced),
+// then the 8 partial sums added in order
+__global__ void __launch_bounds__(256) k_sum_splits(const float *__restrict__ part, int splits,
+                                                    long long count, float *__restrict__ out) {
     __shared__ float red[8][33];
-    const int c = blockIdx.x * 32 + threadIdx.x;
-    const int r0 = blockIdx.y * kChunk;
+    const long long e = (long long)blockIdx.x * 32 + threadIdx.x;
     float acc = 0.f;
-    if (c < N) {
-        const int r1 = min(rows, r0 + kChunk);
-#pragma unroll 8
-        for (int r = r0 + threadIdx.y; r < r1; r += 8) acc += __bfloat162float(A[(long long)r * N + c]);
+    if (e < count) {
+#pragma unroll 4
+        for (int s = threadIdx.y; s < splits; s += 8) acc += part[s * count + e];
     }
     red[threadIdx.y][threadIdx.x] = acc;
     __syncthreads();
-    if (threadIdx.y == 0 && c < N) {
-        float s = 0.f;
-        for (int j = 0; j < 8; ++j) s += red[j][threadIdx.x];
-        part[(long long)blockIdx.y * N + c] = s;
+    if (threadIdx.y == 0 && e < count) {
+        float t = 0.f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) t += red[j][threadIdx.x];
+        out[e] = t;
+    }
+}
+inline dim3 sum_splits_grid(long long count) { return dim3((unsigned)((count + 31) / 32)); }
+
+// Column sums of a BF16 [rows][N] matrix (N even) over row chunks of kChunk: part[chunk][N].
+// A block of 32 x 8 threads per 64 columns: each thread takes a column pair (one 4-byte load
+// per row, 128 bytes per warp) and every 8th row of the chunk; the 8 partial sums are added
+// in order.
+constexpr int kChunk = 256;
+__global__ void __launch_bounds__(256) k_colsum_bf16(const bf16 *__restrict__ A, int rows, int N,
+                                                     float *__restrict__ part) {
+    __shared__ float red[8][65];
+    const int c = blockIdx.x * 64 + 2 * threadIdx.x;
+    const int r0 = blockIdx.y * kChunk, r1 = min(rows, r0 + kChunk);
+    float a0 = 0.f, a1 = 0.f;
+    if (c < N) {
+#pragma unroll 4
+        for (int r = r0 + threadIdx.y; r < r1; r += 8) {
+            const float2 v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(A + (long long)r * N + c));
+            a0 += v.x;
+            a1 += v.y;
+        }
+    }
+    red[threadIdx.y][2 * threadIdx.x] = a0;
+    red[threadIdx.y][2 * threadIdx.x + 1] = a1;
+    __syncthreads();
+    for (int q = threadIdx.y * 32 + threadIdx.x; q < 64; q += 256) {
+        if (blockIdx.x * 64 + q >= N) continue;
+        float t = 0.f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) t += red[j][q];
+        part[(long long)blockIdx.y * N + blockIdx.x * 64 + q] = t;
     }
 }
 
@@ -1076,23 +1096,33 @@ __global__ void k_out_bwd(const float *__restrict__ dY, const float *__restrict_
 }
 
 // Output layer weight / bias gradients over row chunks of kChunk:
-// part[chunk][j][W + 1]: column k < W holds sum dY[b][j] H[b][k], column W sum dY[b][j]
-__global__ void k_out_grad(const float *__restrict__ dY, const bf16 *__restrict__ H, int rows, int W,
-                           float *__restrict__ part) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;  // 0..W (W = bias)
-    if (k > W) return;
+// part[chunk][j][W + 1]: column k < W holds sum dY[b][j] H[b][k], column W sum dY[b][j].
+// A block of 32 x 8 threads per 32 columns: each thread takes every 8th row of the chunk for
+// its column; the 8 partial sums are added in order.
+__global__ void __launch_bounds__(256) k_out_grad(const float *__restrict__ dY, const bf16 *__restrict__ H,
+                                                  int rows, int W, float *__restrict__ part) {
+    __shared__ float red[kOut][8][33];
+    const int k = blockIdx.x * 32 + threadIdx.x;  // 0..W (W = bias)
     const int r0 = blockIdx.y * kChunk, r1 = min(rows, r0 + kChunk);
     float acc[kOut] = {0.f, 0.f, 0.f};
-    // unrolled so that the loads of several rows are in flight at once (the sums stay in
-    // row order)
-#pragma unroll 8
-    for (int b = r0; b < r1; ++b) {
-        const float h = (k < W) ? __bfloat162float(H[(long long)b * W + k]) : 1.f;
+    if (k <= W) {
+#pragma unroll 4
+        for (int b = r0 + threadIdx.y; b < r1; b += 8) {
+            const float h = (k < W) ? __bfloat162float(H[(long long)b * W + k]) : 1.f;
 #pragma unroll
-        for (int j = 0; j < kOut; ++j) acc[j] += dY[(long long)b * kOut + j] * h;
+            for (int j = 0; j < kOut; ++j) acc[j] += dY[(long long)b * kOut + j] * h;
+        }
     }
 #pragma unroll
-    for (int j = 0; j < kOut; ++j) part[((long long)blockIdx.y * kOut + j) * (W + 1) + k] = acc[j];
+    for (int j = 0; j < kOut; ++j) red[j][threadIdx.y][threadIdx.x] = acc[j];
+    __syncthreads();
+    if (threadIdx.y < kOut && k <= W) {
+        const int j = threadIdx.y;
+        float t = 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) t += red[j][q][threadIdx.x];
+        part[((long long)blockIdx.y * kOut + j) * (W + 1) + k] = t;
+    }
 }
 
 // Adam on a flat FP32 parameter array (t = step count after this update)
@@ -1390,10 +1420,10 @@ hidem_status backward(hidem_surrogate *s, int rows, const float *targets, const 
     // output layer
     const int chunks = (rows + kChunk - 1) / kChunk;
     STRY(ensure_part(s, (long long)(chunks + 1) * kOut * (W + 1)));
-    k_out_grad<<<dim3((W + 1 + 127) / 128, chunks), 128, 0, s->stream>>>(s->dY, s->H[L - 1], rows, W, s->part);
+    k_out_grad<<<dim3((W + 1 + 31) / 32, chunks), dim3(32, 8), 0, s->stream>>>(s->dY, s->H[L - 1], rows, W, s->part);
     // sum the chunk partials into a [3][W + 1] block, then split weights and biases
     float *outBlock = s->part + (long long)chunks * kOut * (W + 1);
-    k_sum_splits<<<(unsigned)((kOut * (W + 1) + 255) / 256), 256, 0, s->stream>>>(s->part, chunks, (long long)kOut * (W + 1), outBlock);
+    k_sum_splits<<<sum_splits_grid((long long)kOut * (W + 1)), dim3(32, 8), 0, s->stream>>>(s->part, chunks, (long long)kOut * (W + 1), outBlock);
     for (int j = 0; j < kOut; ++j) {
         SCK(cudaMemcpyAsync(s->G + s->offWo + (long long)j * W, outBlock + (long long)j * (W + 1),
                             sizeof(float) * W, cudaMemcpyDeviceToDevice, s->stream));
@@ -1423,11 +1453,11 @@ hidem_status backward(hidem_surrogate *s, int rows, const float *targets, const 
             STRY(gemm_n<EPI_F32>(s, bn, s->dZT, W, rows, s->inT + (long long)n0 * rows, splits, g));
             n0 += bn;
         }
-        k_sum_splits<<<(unsigned)(((long long)W * K + 255) / 256), 256, 0, s->stream>>>(s->part, splits, (long long)W * K, s->G + s->offW[l]);
+        k_sum_splits<<<sum_splits_grid((long long)W * K), dim3(32, 8), 0, s->stream>>>(s->part, splits, (long long)W * K, s->G + s->offW[l]);
         // db_l = column sums of dZ
         STRY(ensure_part(s, (long long)chunks * W + W));
-        k_colsum_bf16<<<dim3((W + 31) / 32, chunks), dim3(32, 8), 0, s->stream>>>(dZ, rows, W, s->part);
-        k_sum_splits<<<(W + 255) / 256, 256, 0, s->stream>>>(s->part, chunks, W, s->G + s->offB[l]);
+        k_colsum_bf16<<<dim3((W + 63) / 64, chunks), dim3(32, 8), 0, s->stream>>>(dZ, rows, W, s->part);
+        k_sum_splits<<<sum_splits_grid(W), dim3(32, 8), 0, s->stream>>>(s->part, chunks, W, s->G + s->offB[l]);
         if (l > 0) {
             // dZ_{l-1} = (dZ_l * W_l) . SiLU'(Z_{l-1}); B operand W_l^T is [K_l][W]
             GemmArgs gd{};
