@@ -7,7 +7,7 @@ displacement (3 components, normalised).
 Training and inference run in the library's own kernels: BF16 tensor-core GEMMs for the
 hidden layers, CUDA-core kernels for the output layer, loss, reductions and Adam. No
 counterpart in the reference, which settles every geometry from rest; the plain settling
-run stays the judge of every prediction (see ``hidem_b200.settle``).
+run still decides when a warm-started geometry has settled (see ``hidem_b200.settle``).
 """
 from __future__ import annotations
 
