@@ -319,3 +319,16 @@ def test_layout_with_torch_equals_numpy(nranks):
         assert np.array_equal(got.links[r], want.links[r])
         for s_ in range(nranks):
             assert np.array_equal(got.send[r][s_], want.send[r][s_])
+
+
+def test_local_tensor_exchange_checks_sizes():
+    """Between ranks of one process the redistribution's buffers go to the destination's
+    device as they are; a buffer whose size differs from the one both sides computed is an
+    error, not a silent short copy."""
+    import torch
+    comm = slab.LocalComm(2)
+    buf = torch.arange(7, dtype=torch.uint8)
+    got = comm.exchange_tensors({(0, 1): buf}, {(0, 1): 7}, [torch.device("cpu")] * 2)
+    assert torch.equal(got[(0, 1)], buf)
+    with pytest.raises(RuntimeError):
+        comm.exchange_tensors({(0, 1): buf}, {(0, 1): 8}, [torch.device("cpu")] * 2)
